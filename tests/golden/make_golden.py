@@ -1,0 +1,128 @@
+"""Regenerate the golden fixtures in this directory from the reference's own
+known-answer tests.
+
+Run in an environment that has the mwa_hyperdrive source tree (pass its root
+as argv[1]); the outputs are committed so that nothing reads the reference at
+test time.
+
+* model_kats.json  -- expected no-beam visibilities (f32, epsilon 0 in the
+  reference) from src/model/tests/mod.rs: the zenith / off-zenith list,
+  power-law and curved-power-law cases (lines 351-444, 600-731, 887-1018), the
+  two-component Gaussian and shapelet cases (1393-1569) and the shapelet UVWs
+  (1530-1568).  Values are parsed from the Rust source text.
+* shapelet_basis_samples.json -- samples of the shapelet basis table produced
+  by the reference's generator script src/model/make_shapelet_basis_values.py
+  (imported, its gen_shape_basis evaluated at the sampled points), plus the
+  reference's own table KATs (src/model/shapelets.rs:44-59).
+"""
+
+import importlib.util
+import json
+import re
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+
+CPLX = re.compile(r"Complex::new\(\s*([-+0-9.eE]+)\s*,\s*([-+0-9.eE]+)\s*\)")
+UVW = re.compile(r"UVW\s*\{\s*u:\s*([-+0-9.eE]+),\s*v:\s*([-+0-9.eE]+),\s*w:\s*([-+0-9.eE]+),?\s*\}")
+IDENT = re.compile(r"Jones::identity\(\)(?:\s*\*\s*([-+0-9.eE]+))?")
+
+
+def fn_body(src: str, name: str) -> str:
+    start = src.index(f"fn {name}(")
+    end = src.index("\n}\n", start)
+    return src[start:end]
+
+
+def parse_rows(body: str, nbl: int = 3):
+    """Rows of Jones (as [re, im] * 4) for a test function that states its
+    expectation per frequency row (`let expected_*` blocks)."""
+    rows = []
+    blocks = re.split(r"let expected", body)[1:]
+    for blk in blocks:
+        blk = blk.split("assert_abs_diff_eq")[0]
+        cs = CPLX.findall(blk)
+        if cs:
+            vals = [[float(a), float(b)] for a, b in cs]
+            assert len(vals) % 4 == 0
+            jones = [vals[i : i + 4] for i in range(0, len(vals), 4)]
+            rows.extend(jones[i : i + nbl] for i in range(0, len(jones), nbl))
+        else:
+            m = IDENT.search(blk)
+            assert m, blk[:200]
+            s = float(m.group(1)) if m.group(1) else 1.0
+            j = [[s, 0.0], [0.0, 0.0], [0.0, 0.0], [s, 0.0]]
+            rows.append([j] * nbl)
+    return rows
+
+
+def main(ref_root: str) -> None:
+    ref = Path(ref_root)
+    src = (ref / "src/model/tests/mod.rs").read_text()
+    out = {
+        "source": "src/model/tests/mod.rs (mwa_hyperdrive 0.8.0)",
+        "obs": {
+            "phase_centre_deg": [0.0, -27.0],
+            "off_phase_centre_deg": [1.0, -27.0],
+            "freqs_hz": [150e6, 175e6, 200e6],
+            "lst_rad": 0.0,
+            "xyzs": [[0.0, 1.0, 0.0], [0.0, -1.0, 0.0], [1.0, 0.0, 0.0]],
+        },
+        "cases": {},
+    }
+    for name in [
+        "test_list_zenith_visibilities",
+        "test_list_off_zenith_visibilities",
+        "test_power_law_zenith_visibilities",
+        "test_power_law_off_zenith_visibilities",
+        "test_curved_power_law_zenith_visibilities",
+        "test_curved_power_law_off_zenith_visibilities",
+        "test_multiple_gaussian_components",
+    ]:
+        rows = parse_rows(fn_body(src, name))
+        assert len(rows) == 3 and all(len(r) == 3 for r in rows), name
+        out["cases"][name] = rows
+
+    body = fn_body(src, "test_multiple_shapelet_components")
+    vis_part, uvw_part = body.split("assert_abs_diff_eq!(expected, vis", 1)
+    cs = [[float(a), float(b)] for a, b in CPLX.findall(vis_part)]
+    jones = [cs[i : i + 4] for i in range(0, len(cs), 4)]
+    out["cases"]["test_multiple_shapelet_components"] = [jones[i : i + 3] for i in range(0, 9, 3)]
+    uvws = [[float(a), float(b), float(c)] for a, b, c in UVW.findall(uvw_part)]
+    assert len(uvws) == 6
+    out["shapelet_uvws_bl_comp"] = [uvws[i : i + 2] for i in range(0, 6, 2)]
+    (HERE / "model_kats.json").write_text(json.dumps(out, indent=1))
+
+    # Shapelet basis: evaluate the reference generator's basis function.
+    spec = importlib.util.spec_from_file_location("mk", ref / "src/model/make_shapelet_basis_values.py")
+    gen_src = (ref / "src/model/make_shapelet_basis_values.py").read_text()
+    # Import only the function definition (the script body writes files).
+    ns: dict = {}
+    exec(gen_src.split("max_x = 50")[0], ns)
+    gen = ns["gen_shape_basis"]
+    xlocs = np.linspace(-50, 50, 10001)
+    rng = np.random.default_rng(7)
+    samples = []
+    for n in [0, 1, 2, 3, 5, 8, 13, 21, 40, 70, 100]:
+        vals = gen(n, xlocs, beta=1.0)
+        idx = sorted(set(rng.integers(3500, 6500, size=24).tolist() + [5000, 5001, 4999, 0, 10000]))
+        for i in idx:
+            samples.append([n, int(i), float(vals[i])])
+    (HERE / "shapelet_basis_samples.json").write_text(
+        json.dumps(
+            {
+                "source": "src/model/make_shapelet_basis_values.py gen_shape_basis; KATs src/model/shapelets.rs:44-59",
+                "kat": {"index_5000": 1.0, "index_5001": 0.99995, "eps_5000": 1e-10, "eps_5001": 1e-8},
+                "samples_n_index_value": samples,
+            },
+            indent=0,
+        )
+    )
+    del spec
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
