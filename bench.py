@@ -1,0 +1,371 @@
+"""Benchmark: sky-model predict throughput (vis x components / s) on the
+mixed-component configuration (128 tiles, 4 timesteps, 384 channels, 4000
+points + 500 Gaussians + 100 shapelets, analytic beam), synthetic seeded
+inputs.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+A step predicts all 4 timesteps of the configuration.  `value` is the
+device-resident throughput (inputs and tables in HBM, L2 flushed between
+steps, CUDA events on the launching stream, max over ranks); `e2e` is the
+same metric through the trait-style C-ABI call with host buffers (H2D of the
+accumulated visibilities and D2H of the result inside the timed region).
+Multi-GPU runs are independent replicas (the predict shards by timestep and
+channel with no exchange), so scaling is weak.
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "predict vis·components/s"
+UNIT = "vis·comp/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="hdc", choices=["hdc", "reference"])
+    ap.add_argument("--form", default="auto", choices=["auto", "direct", "tensor"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+def workload():
+    from mwa_hyperdrive_b200 import synth
+
+    obs, sky = synth.config2()
+    return obs, sky
+
+
+def vis_comp_per_step(obs, sky):
+    return obs.num_baselines * obs.freqs.size * obs.lsts.size * sky.num_components
+
+
+def config_dict(obs, sky, form):
+    return {
+        "workload": "mixed-component predict: 128 tiles (8128 baselines), 4 timesteps x 8 s, 384 x 80 kHz channels "
+                    "from 167 MHz, 4000 points + 500 Gaussians + 100 shapelets (20 coeffs), curved power laws, "
+                    "analytic dipole-array beam",
+        "tiles": int(obs.num_tiles), "baselines": int(obs.num_baselines), "timesteps": int(obs.lsts.size),
+        "channels": int(obs.freqs.size), "components": int(sky.num_components),
+        "points": int(np.sum(sky.comp_type == 0)), "gaussians": int(np.sum(sky.comp_type == 1)),
+        "shapelets": int(np.sum(sky.comp_type == 2)), "form": form,
+        "l2": "flushed between steps (256 MiB write)",
+    }
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        if self.proc is None:
+            return out
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        rows = []
+        for line in Path(self.path).read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return out
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for k, n in enumerate(names):
+                if r[5 + k].lower() == "active":
+                    reasons.add(n)
+        out["sm_mhz"] = statistics.median(sm) if sm else None
+        out["sm_max_mhz"] = max(mx) if mx else None
+        out["reasons"] = sorted(reasons)
+        out["samples"] = len(rows)
+        return out
+
+
+# --------------------------------------------------------- reference arm
+def reference_arm(args, rank):
+    """The reference's CPU predictor (the oracle's C++ restatement of
+    SkyModellerCpu, OpenMP over baselines) on bounded samples of the same
+    workload: one timestep x a channel subset per step."""
+    if rank != 0:
+        return
+    from oracle import oracle as orc
+
+    orc.build()
+    obs, sky = workload()
+    threads = os.cpu_count() or 1
+    orc.set_num_threads(threads)
+    beam = orc.beam_struct(1)
+    nch = 2
+    # size the per-step sample to ~ a few seconds
+    t0 = time.perf_counter()
+    orc.model_timestep(sky, obs.tile_xyzs, obs.freqs[:nch], obs.phase_centre, obs.lsts[0], obs.latitude, beam=beam)
+    dt = time.perf_counter() - t0
+    nch = int(max(1, min(obs.freqs.size, round(nch * 3.0 / max(dt, 1e-3)))))
+    for _ in range(max(args.warmup, 0)):
+        orc.model_timestep(sky, obs.tile_xyzs, obs.freqs[:1], obs.phase_centre, obs.lsts[0], obs.latitude, beam=beam)
+    times = []
+    for k in range(args.steps):
+        t0 = time.perf_counter()
+        orc.model_timestep(sky, obs.tile_xyzs, obs.freqs[:nch], obs.phase_centre, obs.lsts[k % obs.lsts.size],
+                           obs.latitude, beam=beam)
+        times.append(time.perf_counter() - t0)
+    work = obs.num_baselines * nch * sky.num_components
+    value = work * len(times) / sum(times)
+    sample = f"1 timestep x {nch} of 384 channels x 4600 components x 8128 baselines per step"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config_dict(obs, sky, "reference CPU (C++ restatement of SkyModellerCpu, OpenMP)"),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(obs, sky, seconds):
+    from oracle import oracle as orc
+
+    orc.build()
+    threads = os.cpu_count() or 1
+    orc.set_num_threads(threads)
+    beam = orc.beam_struct(1)
+    t0 = time.perf_counter()
+    orc.model_timestep(sky, obs.tile_xyzs, obs.freqs[:1], obs.phase_centre, obs.lsts[0], obs.latitude, beam=beam)
+    dt = time.perf_counter() - t0
+    nch = int(max(1, min(obs.freqs.size, math.floor(seconds / max(dt, 1e-3)))))
+    t0 = time.perf_counter()
+    orc.model_timestep(sky, obs.tile_xyzs, obs.freqs[:nch], obs.phase_centre, obs.lsts[0], obs.latitude, beam=beam)
+    dt = time.perf_counter() - t0
+    work = obs.num_baselines * nch * sky.num_components
+    return {"value": work / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"1 timestep x {nch} channels x {sky.num_components} components x {obs.num_baselines} baselines "
+                      f"({dt:.1f} s)"}
+
+
+# ------------------------------------------------------------ GPU arm
+def gpu_arm(args, rank, world, local_rank):
+    import torch
+
+    from mwa_hyperdrive_b200 import _lib
+    from mwa_hyperdrive_b200.model import SkyModeller
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    L = _lib.lib()
+    obs, sky = workload()
+    form = args.form
+    if form == "auto":
+        form = "direct"
+        try:
+            SkyModeller(sky.select(sky.comp_type == 0), obs.tile_xyzs, obs.freqs[:1], obs.phase_centre, obs.latitude,
+                        form="tensor").close()
+            form = "tensor"
+        except _lib.HdcError:
+            form = "direct"
+    stream = torch.cuda.current_stream()
+    nf, nbl, nt = obs.freqs.size, obs.num_baselines, obs.lsts.size
+
+    def make(fm):
+        m = SkyModeller(sky, obs.tile_xyzs, obs.freqs, obs.phase_centre, obs.latitude, beam="analytic", form=fm)
+        return m
+
+    vis = torch.zeros((nt, nf, nbl, 8), dtype=torch.float32, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def step(m):
+        vis.zero_()
+        for t in range(nt):
+            m.model_timestep_with(float(obs.lsts[t]), vis[t], stream=stream, return_uvws=False)
+
+    def timed(m, steps, warmup):
+        for _ in range(warmup):
+            step(m)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        evs = []
+        launches0 = L.hdc_kernel_launches()
+        for k in range(steps):
+            flush.fill_(float(k))
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            step(m)
+            b.record(stream)
+            evs.append((a, b))
+        torch.cuda.synchronize()
+        launches = L.hdc_kernel_launches() - launches0
+        ms = [a.elapsed_time(b) for a, b in evs]
+        total = sum(ms)
+        if dist:
+            t = torch.tensor([total], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            total = float(t.item())
+        if dist:
+            dist.barrier()
+        return total / steps, launches // steps
+
+    results = {}
+    plain = make("direct")
+    clocks = ClockSampler(local_rank)
+    ms_plain, launches_plain = timed(plain, args.steps, args.warmup)
+    results["direct"] = ms_plain
+    chosen = plain
+    if form == "tensor":
+        chosen = make("tensor")
+    L.hdc_modeller_set_profiling(chosen._h, 1)
+    clocks.start()
+    ms_chosen, launches = timed(chosen, args.steps, args.warmup)
+    clk = clocks.stop()
+    prof = (ctypes.c_double * 4)()
+    L.hdc_modeller_profile(chosen._h, prof, 1)
+    L.hdc_modeller_set_profiling(chosen._h, 0)
+
+    work = vis_comp_per_step(obs, sky)
+    value = work * world / (ms_chosen * 1e-3)
+
+    # e2e: trait-style host-buffer calls (pinned host memory)
+    hvis = torch.zeros((nt, nf, nbl, 8), dtype=torch.float32).pin_memory()
+    hnp = hvis.numpy()
+    for _ in range(max(1, args.warmup)):
+        for t in range(nt):
+            chosen.model_timestep_with_host(float(obs.lsts[t]), hnp[t], stream=stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    e2e_steps = max(2, args.steps)
+    for _ in range(e2e_steps):
+        hnp[:] = 0.0
+        for t in range(nt):
+            chosen.model_timestep_with_host(float(obs.lsts[t]), hnp[t], stream=stream)
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    if dist:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    bytes_vis = nt * nf * nbl * 32
+
+    # roofline of the dominant kernel class
+    names = ["points", "gaussians", "shapelets", "prep"]
+    per_step_ms = [prof[k] / args.steps for k in range(4)]
+    dom = int(np.argmax(per_step_ms[:3]))
+    npts = int(np.sum(sky.comp_type == 0))
+    nga = int(np.sum(sky.comp_type == 1))
+    nsh = int(np.sum(sky.comp_type == 2))
+    ncoef = int(np.sum(sky.coeff_count))
+    vis_per_launch = nbl * nf
+    launches_per_step = nt
+    if dom == 0 and form == "tensor":
+        # useful complex-GEMM flops: 3 products (XX, XY, YY) of 8 x 128 x 128 x Nc per (t, f)
+        flops = 3 * 8 * obs.num_tiles * obs.num_tiles * npts * nf
+        peak = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["bf16_tflops"] if (
+            ROOT / "MEASURED_PEAKS.json").exists() else 1590.0
+        bound, unit = "tensor", "TFLOP/s"
+        achieved = flops / (per_step_ms[0] / launches_per_step * 1e-3) / 1e12
+    else:
+        fl_per = {0: 37.0, 1: 37.0 + 10.0, 2: 37.0 + 12.0 * ncoef / max(nsh, 1)}[dom]
+        ncomp = [npts, nga, nsh][dom]
+        flops = fl_per * vis_per_launch * ncomp
+        g = ctypes.c_double()
+        _lib.check(L.hdc_probe_fp64_gflops(ctypes.byref(g)), "fp64 probe")
+        peak = g.value / 1e3
+        bound, unit = "fp64", "TFLOP/s"
+        achieved = flops / (per_step_ms[dom] / launches_per_step * 1e-3) / 1e12
+    roofline = {"bound": bound, "kernel": f"{names[dom]} ({form if dom == 0 else 'direct'})",
+                "achieved": achieved, "peak": peak, "unit": unit, "frac": achieved / peak, "traffic": None,
+                "peak_source": "MEASURED_PEAKS.json bf16 burst" if bound == "tensor" else
+                "FP64 FMA probe kernel measured in this run",
+                "per_step_ms_by_class": dict(zip(names, per_step_ms))}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_chosen, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if form == "direct" else "f64 phases / split-precision tensor",
+            "data": "synthetic (seeded)", "config": config_dict(obs, sky, form),
+            "plain": {"form": "direct", "value": work * world / (ms_plain * 1e-3), "ms_per_step": ms_plain},
+            "e2e": {"value": work * world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": bytes_vis,
+                    "d2h_bytes_per_step": bytes_vis},
+            "roofline": roofline, "gpu_launches": int(launches), "clocks": clk,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(obs, sky, args.cpu_seconds)
+        print(json.dumps(line), flush=True)
+    plain.close()
+    if chosen is not plain:
+        chosen.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", str(args.gpus if args.gpus == 1 else 1)))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, rank)
+        return
+    gpu_arm(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,351 @@
+/*
+ * hdc.h -- C ABI of libhdc, the B200 (sm_100a) sky-model predictor,
+ * DI calibration and peeling library.
+ *
+ * Two layers:
+ *
+ *  1. Drop-in layer.  The structs and entry points of mwa_hyperdrive's GPU FFI
+ *     with the same names, field order and argument meaning, FP64 build
+ *     (gpu/types.h, gpu/model.h:33-56, gpu/peel.h:13-35).  A Rust host that
+ *     binds those headers with bindgen binds these unchanged.  Like the
+ *     reference they return NULL on success or a static error string, run on
+ *     the legacy default stream of the current device and accumulate (+=)
+ *     into visibility buffers.
+ *
+ *  2. Native layer (hdc_*).  The SkyModeller trait (model/mod.rs:123-204),
+ *     calibrate_timeblock (di_calibrate/mod.rs:387-618) and the peel loop
+ *     (params/peel/gpu.rs:25-757) as C entry points with explicit streams.
+ *     They return an int status (HDC_OK == 0) and leave a message in
+ *     hdc_last_error().
+ *
+ * Pointers named d_* are device pointers; h_* are host pointers.  Visibility
+ * layouts are the reference's: [time][freq][baseline], baselines in
+ * upper-triangle order (tile1 < tile2, row-major; math/mod.rs:94-109).
+ */
+#pragma once
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------------- */
+/* Types (gpu/types.h, FP64 build: FLOAT = double, JONES = JonesF64)       */
+/* ---------------------------------------------------------------------- */
+
+typedef struct RADec {
+    double ra;  /* [rad] */
+    double dec; /* [rad] */
+} RADec;
+
+typedef struct HADec {
+    double ha;
+    double dec;
+} HADec;
+
+typedef struct XYZ {
+    double x, y, z; /* [m] */
+} XYZ;
+
+typedef struct UVW {
+    double u, v, w; /* [m] */
+} UVW;
+
+/* LMN prepared for the RIME: (2 pi l, 2 pi m, 2 pi (n - 1)). */
+typedef struct LmnRime {
+    double l, m, n;
+} LmnRime;
+
+typedef struct GaussianParams {
+    double maj, min, pa; /* [rad] */
+} GaussianParams;
+
+typedef struct ShapeletCoeff {
+    double value;
+    unsigned char n1;
+    unsigned char n2;
+} ShapeletCoeff;
+
+typedef struct ShapeletUV {
+    double u, v; /* [m] */
+} ShapeletUV;
+
+typedef struct JonesF32 {
+    float j00_re, j00_im, j01_re, j01_im, j10_re, j10_im, j11_re, j11_im;
+} JonesF32;
+
+typedef struct JonesF64 {
+    double j00_re, j00_im, j01_re, j01_im, j10_re, j10_im, j11_re, j11_im;
+} JonesF64;
+
+/* gpu/types.h:172-183 */
+typedef struct Addresses {
+    const int num_freqs;
+    const int num_vis;
+    const int num_baselines;
+    const double *d_freqs;
+    const double *d_shapelet_basis_values;
+    const int num_unique_beam_freqs;
+    const int *d_tile_map;
+    const int *d_freq_map;
+    const int *d_tile_index_to_unflagged_tile_index_map;
+} Addresses;
+
+/* gpu/types.h:187-205 */
+typedef struct Points {
+    const int num_power_laws;
+    const LmnRime *power_law_lmns;
+    const JonesF64 *power_law_fds; /* instrumental, at 150 MHz */
+    const double *power_law_sis;
+    const int num_curved_power_laws;
+    const LmnRime *curved_power_law_lmns;
+    const JonesF64 *curved_power_law_fds;
+    const double *curved_power_law_sis;
+    const double *curved_power_law_qs;
+    const int num_lists;
+    const LmnRime *list_lmns;
+    const JonesF64 *list_fds; /* [freq][num_lists] */
+} Points;
+
+/* gpu/types.h:210-233 */
+typedef struct Gaussians {
+    const int num_power_laws;
+    const LmnRime *power_law_lmns;
+    const JonesF64 *power_law_fds;
+    const double *power_law_sis;
+    const GaussianParams *power_law_gps;
+    const int num_curved_power_laws;
+    const LmnRime *curved_power_law_lmns;
+    const JonesF64 *curved_power_law_fds;
+    const double *curved_power_law_sis;
+    const double *curved_power_law_qs;
+    const GaussianParams *curved_power_law_gps;
+    const int num_lists;
+    const LmnRime *list_lmns;
+    const JonesF64 *list_fds;
+    const GaussianParams *list_gps;
+} Gaussians;
+
+/* gpu/types.h:238-267 */
+typedef struct Shapelets {
+    const int num_power_laws;
+    const LmnRime *power_law_lmns;
+    const JonesF64 *power_law_fds;
+    const double *power_law_sis;
+    const GaussianParams *power_law_gps;
+    const ShapeletUV *power_law_shapelet_uvs; /* [baseline][num_power_laws] */
+    const ShapeletCoeff *power_law_shapelet_coeffs;
+    const int *power_law_num_shapelet_coeffs;
+    const int num_curved_power_laws;
+    const LmnRime *curved_power_law_lmns;
+    const JonesF64 *curved_power_law_fds;
+    const double *curved_power_law_sis;
+    const double *curved_power_law_qs;
+    const GaussianParams *curved_power_law_gps;
+    const ShapeletUV *curved_power_law_shapelet_uvs;
+    const ShapeletCoeff *curved_power_law_shapelet_coeffs;
+    const int *curved_power_law_num_shapelet_coeffs;
+    const int num_lists;
+    const LmnRime *list_lmns;
+    const JonesF64 *list_fds;
+    const GaussianParams *list_gps;
+    const ShapeletUV *list_shapelet_uvs;
+    const ShapeletCoeff *list_shapelet_coeffs;
+    const int *list_num_shapelet_coeffs;
+} Shapelets;
+
+/* gpu/types.h:280-287 */
+typedef struct IonoConsts {
+    double alpha;
+    double beta;
+    double gain;
+} IonoConsts;
+
+/* ---------------------------------------------------------------------- */
+/* Drop-in layer                                                           */
+/* ---------------------------------------------------------------------- */
+
+/* Replaces gpu/model.h:33 model_points.  Cross-correlation visibilities of
+ * point components for one timestep, accumulated into d_vis_fb [freq][bl].
+ * Power-law fluxes are given at 150 MHz (POWER_LAW_FD_REF_FREQ). */
+const char *model_points(const Points *comps, const Addresses *a, const UVW *d_uvws, const JonesF64 *d_beam_jones,
+                         JonesF32 *d_vis_fb);
+
+/* Replaces gpu/model.h:40 model_gaussians. */
+const char *model_gaussians(const Gaussians *comps, const Addresses *a, const UVW *d_uvws,
+                            const JonesF64 *d_beam_jones, JonesF32 *d_vis_fb);
+
+/* Replaces gpu/model.h:47 model_shapelets. */
+const char *model_shapelets(const Shapelets *comps, const Addresses *a, const UVW *d_uvws,
+                            const JonesF64 *d_beam_jones, JonesF32 *d_vis_fb);
+
+/* Replaces gpu/model.h:53 model_autos.  vis_fb is [freq][tile]. */
+const char *model_autos(int num_tiles, int num_freqs, const double *freqs, const Points *points,
+                        const Gaussians *gaussians, const Shapelets *shapelets, const JonesF64 *beam_jones,
+                        const int *tile_map, const int *freq_map, int num_fee_freqs,
+                        const int *tile_index_to_unflagged_tile_index_map, JonesF32 *vis_fb);
+
+/* Replaces gpu/peel.h:13 xyzs_to_uvws: d_xyzs [t][tile], d_lmsts [t],
+ * d_uvws [t][bl]. */
+const char *xyzs_to_uvws(const XYZ *d_xyzs, const double *d_lmsts, UVW *d_uvws, RADec pointing_centre, int num_tiles,
+                         int num_baselines, int num_timesteps);
+
+/* Replaces gpu/peel.h:16 rotate (in place, [t][f][bl]). */
+const char *rotate(JonesF32 *vis_fb, const int num_timesteps, const int num_baselines, const int num_freqs,
+                   const UVW *uvws_from, const UVW *uvws_to, const double *lambdas);
+
+/* Replaces gpu/peel.h:19 average (time and freq_average_factor channels). */
+const char *average(const JonesF32 *d_high_res_vis, const float *d_high_res_weights, JonesF32 *d_low_res_vis,
+                    const int num_timesteps, const int num_baselines, const int num_freqs,
+                    const int freq_average_factor);
+
+/* Replaces gpu/peel.h:23 iono_loop.  *iono_consts is read and updated. */
+const char *iono_loop(const JonesF32 *d_vis_residual, const float *d_vis_weights, const JonesF32 *d_vis_model,
+                      JonesF32 *d_vis_model_rotated, JonesF64 *d_iono_fits, IonoConsts *iono_consts,
+                      const int num_baselines, const int num_freqs, const int num_iterations, const UVW *d_uvws,
+                      const double *d_lambdas_m, const double convergence);
+
+/* Replaces gpu/peel.h:29 subtract_iono. */
+const char *subtract_iono(JonesF32 *d_vis_residual, const JonesF32 *d_vis_model, const IonoConsts iono_consts,
+                          const IonoConsts old_iono_consts, const UVW *d_uvws, const double *d_lambdas_m,
+                          const int num_timesteps, const int num_baselines, const int num_freqs);
+
+/* Replaces gpu/peel.cu:737 add_model.  The argument order is the one of the
+ * reference's definition (peel.cu:737-740: ..., num_timesteps, num_freqs,
+ * num_baselines), which is also how params/peel/gpu.rs:465-475 calls it;
+ * gpu/peel.h:33 declares the last two the other way round. */
+const char *add_model(JonesF32 *d_vis_residual, const JonesF32 *d_vis_model, const IonoConsts iono_consts,
+                      const double *d_lambdas_m, const UVW *d_uvws, const int num_timesteps, const int num_freqs,
+                      const int num_baselines);
+
+/* ---------------------------------------------------------------------- */
+/* Native layer                                                            */
+/* ---------------------------------------------------------------------- */
+
+#define HDC_OK 0
+#define HDC_ERR_ARG 1
+#define HDC_ERR_CUDA 2
+#define HDC_ERR_ALLOC 3
+#define HDC_ERR_TIMEOUT 4
+#define HDC_ERR_UNSUPPORTED 5
+
+/* A cudaStream_t without requiring the CUDA headers. NULL = legacy default. */
+typedef struct CUstream_st *hdcStream_t;
+
+/* Message for the last non-OK status on this thread ("" if none). */
+const char *hdc_last_error(void);
+
+/* Library and device description, e.g. for the solutions' MODELLER string
+ * (di_calibrate/mod.rs:258-260; gpu/utils.cu:43-68). */
+int hdc_device_info(char *buf, int buf_len);
+
+/* Component type and flux-model codes of HdcSkyModel. */
+#define HDC_POINT 0
+#define HDC_GAUSSIAN 1
+#define HDC_SHAPELET 2
+#define HDC_FLUX_LIST 0
+#define HDC_FLUX_POWER_LAW 1
+#define HDC_FLUX_CURVED_POWER_LAW 2
+
+/* A sky model as a struct of arrays over components (host memory), in the
+ * reference's modelling order (srclist/types/components/mod.rs:169-272).
+ * fds holds 5 doubles per entry (freq [Hz], I, Q, U, V) [Jy]; a component's
+ * entries are fds[fd_start .. fd_start + fd_count).  (Curved) power laws have
+ * one entry, the reference flux density.  Shapelet coefficients are
+ * coeff_*[coeff_start .. coeff_start + coeff_count). */
+typedef struct HdcSkyModel {
+    int num_components;
+    const int *comp_type;
+    const double *ra;
+    const double *dec;
+    const double *maj;
+    const double *min;
+    const double *pa;
+    const int *flux_type;
+    const double *si;
+    const double *q;
+    const int *fd_start;
+    const int *fd_count;
+    const double *fds;
+    const int *coeff_start;
+    const int *coeff_count;
+    const int *coeff_n1;
+    const int *coeff_n2;
+    const double *coeff_value;
+} HdcSkyModel;
+
+/* Beam used by the native modeller. */
+#define HDC_BEAM_NONE 0          /* identity Jones (beam/mod.rs:255-388 NoBeam) */
+#define HDC_BEAM_ANALYTIC_DIPOLE 1 /* 4x4 dipole tile over a ground plane, shared by all tiles */
+
+/* Precision form of the point-source predict. */
+#define HDC_PREDICT_DIRECT 0     /* FP64 direct per-baseline kernel (the plain form) */
+#define HDC_PREDICT_TENSOR 1     /* factored tcgen05 contraction (points only) */
+
+/* Polarisations (context/mod.rs:26): 0 XX_XY_YX_YY, 1 XX, 2 YY, 3 XX_YY,
+ * 4 XX_YY_XY. */
+
+typedef struct HdcModeller HdcModeller;
+
+/* new_sky_modeller / SkyModellerGpu::new (model/mod.rs:215-261,
+ * model/gpu.rs:150-520) for the unflagged tiles and channels.  The tile XYZs
+ * are used for every timestep unless hdc_modeller_set_tile_xyzs replaces them
+ * (e.g. with precessed positions). */
+int hdc_modeller_new(const HdcSkyModel *sky, int pols, const XYZ *h_unflagged_tile_xyzs, int num_tiles,
+                     const double *h_freqs, int num_freqs, RADec phase_centre, double array_latitude_rad,
+                     int beam_kind, int predict_form, HdcModeller **out);
+void hdc_modeller_free(HdcModeller *m);
+
+int hdc_modeller_set_tile_xyzs(HdcModeller *m, const XYZ *h_tile_xyzs);
+
+/* SkyModeller::model_timestep_with at a given LMST (the device-level form the
+ * reference's peel loop calls, model/gpu.rs:1152-1166): d_vis_fb [freq][bl]
+ * is accumulated into (not cleared); h_uvws_out [bl] may be NULL. */
+int hdc_modeller_model_timestep_with(HdcModeller *m, double lst_rad, JonesF32 *d_vis_fb, UVW *h_uvws_out,
+                                     hdcStream_t stream);
+
+/* As above with an FP64 visibility buffer (no f32 demotion; parity mode). */
+int hdc_modeller_model_timestep_with_f64(HdcModeller *m, double lst_rad, JonesF64 *d_vis_fb, UVW *h_uvws_out,
+                                         hdcStream_t stream);
+
+/* SkyModeller::model_timestep_with with host buffers, as the trait is called
+ * (model/gpu.rs:1476-1496): copies h_vis_fb in, accumulates, copies back. */
+int hdc_modeller_model_timestep_with_host(HdcModeller *m, double lst_rad, JonesF32 *h_vis_fb, UVW *h_uvws_out,
+                                          hdcStream_t stream);
+
+/* SkyModeller::update_with_a_source (model/mod.rs:174): replace the sky model
+ * and the phase centre. */
+int hdc_modeller_update_with_a_source(HdcModeller *m, const HdcSkyModel *source, RADec phase_centre);
+
+/* SkyModeller::model_timestep_autos_with (model/mod.rs:199): d_vis_fb is
+ * [freq][tile], accumulated. */
+int hdc_modeller_model_timestep_autos_with(HdcModeller *m, double lst_rad, JonesF32 *d_vis_fb, hdcStream_t stream);
+
+/* Diagnostics.  Number of kernels libhdc has launched in this process. */
+long long hdc_kernel_launches(void);
+
+/* Per-kernel-class device time of a modeller's last calls, measured with
+ * CUDA events on the launching stream when profiling is enabled.
+ * out_ms[0..3] = points, Gaussians, shapelets, geometry/beam prep [ms],
+ * accumulated since the last reset. */
+int hdc_modeller_set_profiling(HdcModeller *m, int enable);
+int hdc_modeller_profile(HdcModeller *m, double *out_ms, int reset);
+
+/* Achievable FP64 FMA rate of the current device [GFLOP/s], measured by a
+ * register-resident FMA-chain kernel over all SMs (the FP64 roofline
+ * denominator; a measurement, not a datasheet value). */
+int hdc_probe_fp64_gflops(double *out_gflops);
+
+/* Per-chanblock calibration outcome (di_calibrate/mod.rs:620-632). */
+typedef struct HdcCalResult {
+    int num_iterations;
+    int converged;
+    double max_precision;
+    int num_failed;
+} HdcCalResult;
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif

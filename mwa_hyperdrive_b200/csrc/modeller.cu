@@ -1,0 +1,625 @@
+// Native sky modeller: the SkyModeller trait (model/mod.rs:123-204) over the
+// direct FP64 kernels (and the tensor-core point path), with all per-timestep
+// geometry, beam and flux work on the device.
+//
+// Construction (SkyModellerGpu::new / update_source_list,
+// model/gpu.rs:150-861; ComponentList::new, components/mod.rs:181-272):
+// components are split by type in the given order; per type the device holds
+//   lmn   [nc]      (l, m, n - 1) in turn units (the reference's LmnRime / 2 pi)
+//   S     [nf][nc]  instrumental flux per channel (list fluxes tabulated on the
+//                   host with estimate_at_freq, power laws extrapolated on the
+//                   device from the catalogue reference frequency, as the CPU
+//                   modeller does)
+//   gp    [nc]      envelope parameters
+// Per timestep (model_timestep_with, model/cpu.rs:787-812): baseline UVWs from
+// the tile XYZs at the phase centre's hour angle (tile UVW differences, as
+// marlu's xyzs_to_cross_uvws), per-tile shapelet UVs at each shapelet's own
+// hour angle (components/mod.rs:279-298), the beam-weighted flux
+// W = B S B^H when a beam is set, then the per-type direct kernels.
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "modeller.cuh"
+#include "predict.cuh"
+
+namespace hdc {
+
+// ---------------------------------------------------------------------------
+// Host restatement of the flux-density models (srclist/types/flux_density/
+// mod.rs:158-275) used to tabulate list-type fluxes.
+// ---------------------------------------------------------------------------
+struct Stokes {
+    double freq, i, q, u, v;
+};
+
+static Stokes fd_entry(const HdcSkyModel* s, int idx) {
+    const double* p = s->fds + 5 * (size_t)idx;
+    return Stokes{p[0], p[1], p[2], p[3], p[4]};
+}
+static Stokes scale(Stokes a, double r) { return Stokes{a.freq, a.i * r, a.q * r, a.u * r, a.v * r}; }
+static double signum_rs(double x) { return std::isnan(x) ? NAN : (std::signbit(x) ? -1.0 : 1.0); }
+
+Stokes estimate_list(const HdcSkyModel* s, int c, double freq) {
+    const int start = s->fd_start[c], count = s->fd_count[c];
+    double si;
+    Stokes smaller;
+    if (count == 1) {
+        si = -0.8;  // DEFAULT_SPEC_INDEX (constants.rs)
+        smaller = fd_entry(s, start);
+    } else {
+        Stokes a = fd_entry(s, start), b = fd_entry(s, start + 1);
+        for (int w = 0; w + 1 < count; w++) {
+            const Stokes w0 = fd_entry(s, start + w), w1 = fd_entry(s, start + w + 1);
+            a = w0;
+            b = w1;
+            if (std::fabs(w0.freq - freq) < 1e-3) return w0;
+            if (std::fabs(w1.freq - freq) < 1e-3) return w1;
+            if (freq < w1.freq) break;
+        }
+        if (signum_rs(a.i) != signum_rs(b.i)) {
+            const double run = b.freq - a.freq, df = freq - a.freq;
+            return Stokes{freq, a.i + (b.i - a.i) / run * df, a.q + (b.q - a.q) / run * df,
+                          a.u + (b.u - a.u) / run * df, a.v + (b.v - a.v) / run * df};
+        }
+        si = std::log(b.i / a.i) / std::log(b.freq / a.freq);
+        smaller = (b.freq < freq) ? b : a;
+    }
+    Stokes out = smaller;
+    out.freq = freq;
+    return scale(out, std::pow(freq / smaller.freq, si));
+}
+
+static JonesF64 inst_stokes(const Stokes& f) {
+    return JonesF64{f.i - f.q, 0.0, f.u, -f.v, f.u, f.v, f.i + f.q, 0.0};
+}
+
+// ---------------------------------------------------------------------------
+// Device kernels
+// ---------------------------------------------------------------------------
+struct FluxComp {
+    int flux_type;  // 1 power law, 2 curved power law (lists are host-tabulated)
+    double freq, i, q, u, v, si, cq;
+};
+
+__global__ void flux_kernel(const FluxComp* comps, int nc, const double* freqs, int nf, JonesF64* S) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int f = blockIdx.y;
+    if (c >= nc) return;
+    const FluxComp k = comps[c];
+    if (k.flux_type == 0) return;
+    const double nu = freqs[f];
+    const double ratio = pow(nu / k.freq, k.si);
+    double i = k.i * ratio, q = k.q * ratio, u = k.u * ratio, v = k.v * ratio;
+    if (k.flux_type == 2) {
+        const double lr = log(nu / k.freq);
+        const double curved = exp(k.cq * (lr * lr));
+        i *= curved;
+        q *= curved;
+        u *= curved;
+        v *= curved;
+    }
+    S[(size_t)f * nc + c] = JonesF64{i - q, 0.0, u, -v, u, v, i + q, 0.0};
+}
+
+// Baseline UVWs (m) as tile-UVW differences at one hour angle / declination.
+__global__ void baseline_uvw_kernel(const XYZ* xyzs, int ntiles, int nbl, double s_ha, double c_ha, double s_dec,
+                                    double c_dec, UVW* uvws) {
+    const int bl = blockIdx.x * blockDim.x + threadIdx.x;
+    if (bl >= nbl) return;
+    int t1, t2;
+    baseline_to_tiles(bl, ntiles, t1, t2);
+    const XYZ a = xyzs[t1], b = xyzs[t2];
+    const double u1 = s_ha * a.x + c_ha * a.y;
+    const double v1 = -s_dec * c_ha * a.x + s_dec * s_ha * a.y + c_dec * a.z;
+    const double w1 = c_dec * c_ha * a.x - c_dec * s_ha * a.y + s_dec * a.z;
+    const double u2 = s_ha * b.x + c_ha * b.y;
+    const double v2 = -s_dec * c_ha * b.x + s_dec * s_ha * b.y + c_dec * b.z;
+    const double w2 = c_dec * c_ha * b.x - c_dec * s_ha * b.y + s_dec * b.z;
+    uvws[bl] = UVW{u1 - u2, v1 - v2, w1 - w2};
+}
+
+// Per (shapelet component, tile) UV [m] at the component's hour angle.
+__global__ void shapelet_tile_uv_kernel(const double2* radec, int nc, const XYZ* xyzs, int ntiles, double lst,
+                                        double2* out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nc * ntiles) return;
+    const int c = i / ntiles, t = i % ntiles;
+    const double2 rd = radec[c];
+    double s_ha, c_ha, s_dec, c_dec;
+    sincos(lst - rd.x, &s_ha, &c_ha);
+    sincos(rd.y, &s_dec, &c_dec);
+    const XYZ a = xyzs[t];
+    out[i] = make_double2(s_ha * a.x + c_ha * a.y, -s_dec * c_ha * a.x + s_dec * s_ha * a.y + c_dec * a.z);
+}
+
+// Analytic 4x4 dipole-array tile over a ground plane (a model of this
+// project; mwa_hyperdrive has no analytic beam): for direction (az, za),
+// J = A R(az)^T diag(cos za, 1) R(az), A = AFx(l) AFy(m) GP(za) / |GP(0)|,
+// l = sin za sin az, m = sin za cos az, AFx(l) = (cos(k 0.55 l) + cos(k 1.65 l))/2
+// (1.1 m dipole spacing), GP = 1 - exp(-2 i k h cos za), h = 0.278 m.
+__device__ J2 analytic_beam(double az, double el, double freq) {
+    if (el <= 0.0) return jzero();
+    const double za = FRAC_PI_2 - el;
+    const double k = TAU * freq / VEL_C;
+    double sza, cza, saz, caz;
+    sincos(za, &sza, &cza);
+    sincos(az, &saz, &caz);
+    const double l = sza * saz, m = sza * caz;
+    const double afx = 0.5 * (cos(k * 0.55 * l) + cos(k * 1.65 * l));
+    const double afy = 0.5 * (cos(k * 0.55 * m) + cos(k * 1.65 * m));
+    const double h = 0.278;
+    double sp, cp;
+    sincos(2.0 * k * h * cza, &sp, &cp);
+    const double gp0 = 2.0 * fabs(sin(k * h));
+    const double a = afx * afy / gp0;
+    const cplx amp = cplx{1.0 - cp, sp} * a;
+    const double p00 = cza * saz * saz + caz * caz;
+    const double p01 = (cza - 1.0) * saz * caz;
+    const double p11 = cza * caz * caz + saz * saz;
+    return J2{amp * p00, amp * p01, amp * p01, amp * p11};
+}
+
+// ERFA hd2ae (marlu HADec::to_azel).
+__device__ void hadec_to_azel(double ha, double dec, double lat, double& az, double& el) {
+    double s_ha, c_ha, s_dec, c_dec, s_lat, c_lat;
+    sincos(ha, &s_ha, &c_ha);
+    sincos(dec, &s_dec, &c_dec);
+    sincos(lat, &s_lat, &c_lat);
+    const double x = -s_ha * c_dec;
+    const double y = -c_ha * c_dec * s_lat + s_dec * c_lat;
+    const double z = c_ha * c_dec * c_lat + s_dec * s_lat;
+    const double r = hypot(x, y);
+    const double a = (r == 0.0) ? 0.0 : atan2(x, y);
+    az = (a < 0.0) ? a + TAU : a;
+    el = atan2(z, r);
+}
+
+// W[f][c] = B S B^H for a beam shared by all tiles (model/cpu.rs:187-230,
+// 336-337 with B1 == B2).
+__global__ void beam_weight_kernel(const double2* radec, int nc, const double* freqs, int nf, double lst, double lat,
+                                   const JonesF64* S, JonesF64* W) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int f = blockIdx.y;
+    if (c >= nc) return;
+    const double2 rd = radec[c];
+    double az, el;
+    hadec_to_azel(lst - rd.x, rd.y, lat, az, el);
+    const J2 b = analytic_beam(az, el, freqs[f]);
+    const J2 s = load_j(S[(size_t)f * nc + c]);
+    W[(size_t)f * nc + c] = store_j((b * s) * herm(b));
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+template <class T>
+static cudaError_t dalloc(T** p, size_t n) {
+    *p = nullptr;
+    if (n == 0) return cudaSuccess;
+    return cudaMalloc((void**)p, sizeof(T) * n);
+}
+template <class T>
+static void dfree(T*& p) {
+    if (p) cudaFree((void*)p);
+    p = nullptr;
+}
+
+void TypeTables::release() {
+    dfree(d_lmn);
+    dfree(d_S);
+    dfree(d_W);
+    dfree(d_gp);
+    dfree(d_radec);
+    dfree(d_coeffs);
+    dfree(d_cstart);
+    dfree(d_ccount);
+    dfree(d_suv_tile);
+    nc = 0;
+}
+
+static void lmn_turns(double ra, double dec, double pc_ra, double pc_dec, double out[3]) {
+    // marlu RADec::to_lmn; prepare_for_rime's 2 pi is applied in the kernel's
+    // turn-based phase instead.
+    const double d_ra = ra - pc_ra;
+    const double s_d_ra = std::sin(d_ra), c_d_ra = std::cos(d_ra);
+    const double s_dec = std::sin(dec), c_dec = std::cos(dec);
+    const double pc_s = std::sin(pc_dec), pc_c = std::cos(pc_dec);
+    out[0] = c_dec * s_d_ra;
+    out[1] = s_dec * pc_c - c_dec * pc_s * c_d_ra;
+    out[2] = (s_dec * pc_s + c_dec * pc_c * c_d_ra) - 1.0;
+}
+
+int Modeller::build_tables(const HdcSkyModel* sky) {
+    for (int ty = 0; ty < 3; ty++) t[ty].release();
+    std::vector<int> idx[3];
+    for (int c = 0; c < sky->num_components; c++) {
+        const int ty = sky->comp_type[c];
+        if (ty < 0 || ty > 2) {
+            set_error("component %d has unknown type %d", c, ty);
+            return HDC_ERR_ARG;
+        }
+        const int ft = sky->flux_type[c];
+        if (ft < 0 || ft > 2 || sky->fd_count[c] < 1) {
+            set_error("component %d has an invalid flux model", c);
+            return HDC_ERR_ARG;
+        }
+        idx[ty].push_back(c);
+    }
+    std::vector<double> hfreqs(freqs);
+    for (int ty = 0; ty < 3; ty++) {
+        TypeTables& tt = t[ty];
+        const int nc = (int)idx[ty].size();
+        tt.nc = nc;
+        if (nc == 0) continue;
+        std::vector<double4> lmn(nc), gp(nc);
+        std::vector<double2> radec(nc);
+        std::vector<JonesF64> S((size_t)nf * nc);
+        std::vector<FluxComp> fc(nc);
+        std::vector<ShapeletCoeff> coeffs;
+        std::vector<int> cstart(nc), ccount(nc);
+        for (int k = 0; k < nc; k++) {
+            const int c = idx[ty][k];
+            double l3[3];
+            lmn_turns(sky->ra[c], sky->dec[c], pc.ra, pc.dec, l3);
+            lmn[k] = make_double4(l3[0], l3[1], l3[2], 0.0);
+            radec[k] = make_double2(sky->ra[c], sky->dec[c]);
+            if (ty >= 1) {
+                const double sp = std::sin(sky->pa[c]), cp = std::cos(sky->pa[c]);
+                if (ty == 1)
+                    gp[k] = make_double4(GAUSSIAN_EXP_CONST * (sky->maj[c] * sky->maj[c]),
+                                         GAUSSIAN_EXP_CONST * (sky->min[c] * sky->min[c]), sp, cp);
+                else
+                    gp[k] = make_double4(sky->maj[c] * SHAPELET_CONST, -sky->min[c] * SHAPELET_CONST, sp, cp);
+            }
+            const int ft = sky->flux_type[c];
+            FluxComp f = {};
+            f.flux_type = ft;
+            if (ft == HDC_FLUX_LIST) {
+                for (int fi = 0; fi < nf; fi++) S[(size_t)fi * nc + k] = inst_stokes(estimate_list(sky, c, hfreqs[fi]));
+            } else {
+                const Stokes r = fd_entry(sky, sky->fd_start[c]);
+                f.freq = r.freq;
+                f.i = r.i;
+                f.q = r.q;
+                f.u = r.u;
+                f.v = r.v;
+                f.si = sky->si[c];
+                f.cq = (ft == HDC_FLUX_CURVED_POWER_LAW) ? sky->q[c] : 0.0;
+            }
+            fc[k] = f;
+            if (ty == 2) {
+                cstart[k] = (int)coeffs.size();
+                ccount[k] = sky->coeff_count[c];
+                for (int q = 0; q < sky->coeff_count[c]; q++) {
+                    const int ci = sky->coeff_start[c] + q;
+                    const int n1 = sky->coeff_n1[ci], n2 = sky->coeff_n2[ci];
+                    if (n1 < 0 || n1 >= SBF_N || n2 < 0 || n2 >= SBF_N) {
+                        set_error("shapelet coefficient order (%d, %d) outside 0..%d", n1, n2, SBF_N - 1);
+                        return HDC_ERR_ARG;
+                    }
+                    ShapeletCoeff sc;
+                    std::memset(&sc, 0, sizeof(sc));
+                    sc.value = sky->coeff_value[ci];
+                    sc.n1 = (unsigned char)n1;
+                    sc.n2 = (unsigned char)n2;
+                    coeffs.push_back(sc);
+                }
+            }
+        }
+        HDC_CUDA_RET_INT(dalloc(&tt.d_lmn, nc));
+        HDC_CUDA_RET_INT(dalloc(&tt.d_S, (size_t)nf * nc));
+        HDC_CUDA_RET_INT(dalloc(&tt.d_gp, nc));
+        HDC_CUDA_RET_INT(dalloc(&tt.d_radec, nc));
+        HDC_CUDA_RET_INT(cudaMemcpy(tt.d_lmn, lmn.data(), sizeof(double4) * nc, cudaMemcpyHostToDevice));
+        HDC_CUDA_RET_INT(cudaMemcpy(tt.d_gp, gp.data(), sizeof(double4) * nc, cudaMemcpyHostToDevice));
+        HDC_CUDA_RET_INT(cudaMemcpy(tt.d_radec, radec.data(), sizeof(double2) * nc, cudaMemcpyHostToDevice));
+        HDC_CUDA_RET_INT(cudaMemcpy(tt.d_S, S.data(), sizeof(JonesF64) * S.size(), cudaMemcpyHostToDevice));
+        FluxComp* d_fc = nullptr;
+        HDC_CUDA_RET_INT(dalloc(&d_fc, nc));
+        HDC_CUDA_RET_INT(cudaMemcpy(d_fc, fc.data(), sizeof(FluxComp) * nc, cudaMemcpyHostToDevice));
+        dim3 g((nc + 127) / 128, nf);
+        flux_kernel<<<g, 128>>>(d_fc, nc, d_freqs, nf, tt.d_S);
+        count_launches(1);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+        cudaFree(d_fc);
+        HDC_CUDA_RET_INT(e);
+        if (beam_kind != HDC_BEAM_NONE) HDC_CUDA_RET_INT(dalloc(&tt.d_W, (size_t)nf * nc));
+        if (ty == 2) {
+            HDC_CUDA_RET_INT(dalloc(&tt.d_coeffs, coeffs.size() + 1));
+            if (!coeffs.empty())
+                HDC_CUDA_RET_INT(cudaMemcpy(tt.d_coeffs, coeffs.data(), sizeof(ShapeletCoeff) * coeffs.size(),
+                                            cudaMemcpyHostToDevice));
+            HDC_CUDA_RET_INT(dalloc(&tt.d_cstart, nc));
+            HDC_CUDA_RET_INT(dalloc(&tt.d_ccount, nc));
+            HDC_CUDA_RET_INT(cudaMemcpy(tt.d_cstart, cstart.data(), sizeof(int) * nc, cudaMemcpyHostToDevice));
+            HDC_CUDA_RET_INT(cudaMemcpy(tt.d_ccount, ccount.data(), sizeof(int) * nc, cudaMemcpyHostToDevice));
+            HDC_CUDA_RET_INT(dalloc(&tt.d_suv_tile, (size_t)nc * ntiles));
+        }
+    }
+    return HDC_OK;
+}
+
+int Modeller::geometry(double lst, cudaStream_t s) {
+    const double ha = lst - pc.ra;
+    const double s_ha = std::sin(ha), c_ha = std::cos(ha);
+    const double s_dec = std::sin(pc.dec), c_dec = std::cos(pc.dec);
+    baseline_uvw_kernel<<<(nbl + 255) / 256, 256, 0, s>>>(d_xyzs, ntiles, nbl, s_ha, c_ha, s_dec, c_dec, d_uvws);
+    count_launches(1);
+    HDC_CUDA_RET_INT(cudaGetLastError());
+    if (t[2].nc > 0) {
+        const int n = t[2].nc * ntiles;
+        shapelet_tile_uv_kernel<<<(n + 255) / 256, 256, 0, s>>>(t[2].d_radec, t[2].nc, d_xyzs, ntiles, lst,
+                                                                 t[2].d_suv_tile);
+        count_launches(1);
+        HDC_CUDA_RET_INT(cudaGetLastError());
+    }
+    if (beam_kind != HDC_BEAM_NONE) {
+        for (int ty = 0; ty < 3; ty++) {
+            if (t[ty].nc == 0) continue;
+            dim3 g((t[ty].nc + 127) / 128, nf);
+            beam_weight_kernel<<<g, 128, 0, s>>>(t[ty].d_radec, t[ty].nc, d_freqs, nf, lst, lat, t[ty].d_S, t[ty].d_W);
+            count_launches(1);
+            HDC_CUDA_RET_INT(cudaGetLastError());
+        }
+    }
+    return HDC_OK;
+}
+
+const JonesF64* Modeller::weights(int ty) const { return beam_kind != HDC_BEAM_NONE ? t[ty].d_W : t[ty].d_S; }
+
+DirectParams Modeller::direct_params(int ty, void* vis) const {
+    DirectParams p = {};
+    p.nbl = nbl;
+    p.nf = nf;
+    p.ntiles = ntiles;
+    p.nc = t[ty].nc;
+    p.freqs = d_freqs;
+    p.uvws = d_uvws;
+    p.lmn = t[ty].d_lmn;
+    p.flux = weights(ty);
+    p.gp = t[ty].d_gp;
+    p.sbf = d_sbf;
+    p.coeffs = t[ty].d_coeffs;
+    p.coeff_start = t[ty].d_cstart;
+    p.coeff_count = t[ty].d_ccount;
+    p.suv_bl = nullptr;
+    p.suv_tile = t[ty].d_suv_tile;
+    p.vis = vis;
+    p.err = d_err;
+    return p;
+}
+
+void Modeller::prof_begin(int cls, cudaStream_t s, EvPair& e) {
+    if (!profiling) return;
+    if (!ev_free.empty()) {
+        e = ev_free.back();
+        ev_free.pop_back();
+    } else {
+        cudaEventCreate(&e.a);
+        cudaEventCreate(&e.b);
+    }
+    e.cls = cls;
+    cudaEventRecord(e.a, s);
+}
+
+void Modeller::prof_end(cudaStream_t s, EvPair& e) {
+    if (!profiling) return;
+    cudaEventRecord(e.b, s);
+    ev_pending.push_back(e);
+}
+
+void Modeller::prof_collect() {
+    for (EvPair& e : ev_pending) {
+        float ms = 0.f;
+        cudaEventSynchronize(e.b);
+        if (cudaEventElapsedTime(&ms, e.a, e.b) == cudaSuccess) prof_ms[e.cls] += ms;
+        ev_free.push_back(e);
+    }
+    ev_pending.clear();
+}
+
+int Modeller::model(double lst, void* d_vis, bool out64, UVW* h_uvws, cudaStream_t s) {
+    EvPair e{};
+    prof_begin(3, s, e);
+    int rc = geometry(lst, s);
+    if (rc) return rc;
+    prof_end(s, e);
+    for (int ty = 0; ty < 3; ty++) {
+        if (t[ty].nc == 0) continue;
+        prof_begin(ty, s, e);
+        if (ty == 0 && form == HDC_PREDICT_TENSOR) {
+            rc = tensor_points(lst, d_vis, out64, s);
+            if (rc) return rc;
+        } else {
+            HDC_CUDA_RET_INT(launch_direct(ty, false, out64, direct_params(ty, d_vis), s));
+        }
+        prof_end(s, e);
+    }
+    if (!out64) HDC_CUDA_RET_INT(launch_mask_pols((JonesF32*)d_vis, (size_t)nf * nbl, pols, s));
+    if (h_uvws) {
+        HDC_CUDA_RET_INT(cudaMemcpyAsync(h_uvws, d_uvws, sizeof(UVW) * nbl, cudaMemcpyDeviceToHost, s));
+        HDC_CUDA_RET_INT(cudaStreamSynchronize(s));
+    }
+    return HDC_OK;
+}
+
+int Modeller::autos(double lst, JonesF32* d_vis, cudaStream_t s) {
+    int rc = geometry(lst, s);
+    if (rc) return rc;
+    for (int ty = 0; ty < 3; ty++) {
+        if (t[ty].nc == 0) continue;
+        AutosParams p = {};
+        p.ntiles = ntiles;
+        p.nf = nf;
+        p.nc_total = t[ty].nc;
+        p.flux = weights(ty);  // with a shared beam, B S B^H is already the auto term
+        p.beam = nullptr;
+        p.vis = d_vis;
+        HDC_CUDA_RET_INT(launch_autos(p, s));
+    }
+    return HDC_OK;
+}
+
+Modeller::~Modeller() {
+    for (int ty = 0; ty < 3; ty++) t[ty].release();
+    dfree(d_freqs);
+    dfree(d_xyzs);
+    dfree(d_uvws);
+    dfree(d_host_vis);
+    tensor_release();
+    for (EvPair& e : ev_pending) ev_free.push_back(e);
+    for (EvPair& e : ev_free) {
+        cudaEventDestroy(e.a);
+        cudaEventDestroy(e.b);
+    }
+}
+
+}  // namespace hdc
+
+using hdc::Modeller;
+
+extern "C" int hdc_modeller_new(const HdcSkyModel* sky, int pols, const XYZ* h_xyzs, int num_tiles,
+                                const double* h_freqs, int num_freqs, RADec phase_centre, double array_latitude_rad,
+                                int beam_kind, int predict_form, HdcModeller** out) {
+    if (!sky || !h_xyzs || !h_freqs || !out || num_tiles < 2 || num_freqs < 1) {
+        hdc::set_error("hdc_modeller_new: invalid arguments");
+        return HDC_ERR_ARG;
+    }
+    if (pols < 0 || pols > 4 || beam_kind < 0 || beam_kind > 1 || predict_form < 0 || predict_form > 1) {
+        hdc::set_error("hdc_modeller_new: invalid pols/beam/form code");
+        return HDC_ERR_ARG;
+    }
+    Modeller* m = new Modeller();
+    cudaGetDevice(&m->device);
+    m->pols = pols;
+    m->ntiles = num_tiles;
+    m->nbl = num_tiles * (num_tiles - 1) / 2;
+    m->nf = num_freqs;
+    m->pc = phase_centre;
+    m->lat = array_latitude_rad;
+    m->beam_kind = beam_kind;
+    m->form = predict_form;
+    m->freqs.assign(h_freqs, h_freqs + num_freqs);
+    m->xyzs.assign(h_xyzs, h_xyzs + num_tiles);
+    int rc = HDC_OK;
+    auto fail = [&](int r) {
+        delete m;
+        return r;
+    };
+    if (cudaMalloc(&m->d_freqs, sizeof(double) * num_freqs) != cudaSuccess ||
+        cudaMalloc(&m->d_xyzs, sizeof(XYZ) * num_tiles) != cudaSuccess ||
+        cudaMalloc(&m->d_uvws, sizeof(UVW) * m->nbl) != cudaSuccess) {
+        cudaGetLastError();
+        hdc::set_error("hdc_modeller_new: device allocation failed");
+        return fail(HDC_ERR_ALLOC);
+    }
+    cudaMemcpy(m->d_freqs, h_freqs, sizeof(double) * num_freqs, cudaMemcpyHostToDevice);
+    cudaMemcpy(m->d_xyzs, h_xyzs, sizeof(XYZ) * num_tiles, cudaMemcpyHostToDevice);
+    m->d_sbf = hdc::device_shapelet_basis();
+    m->d_err = hdc::device_error_word();
+    if (!m->d_sbf || !m->d_err) {
+        hdc::set_error("hdc_modeller_new: device tables unavailable");
+        return fail(HDC_ERR_ALLOC);
+    }
+    rc = m->build_tables(sky);
+    if (rc) return fail(rc);
+    if (predict_form == HDC_PREDICT_TENSOR) {
+        rc = m->tensor_setup();
+        if (rc) return fail(rc);
+    }
+    *out = reinterpret_cast<HdcModeller*>(m);
+    return HDC_OK;
+}
+
+extern "C" void hdc_modeller_free(HdcModeller* m) { delete reinterpret_cast<Modeller*>(m); }
+
+extern "C" int hdc_modeller_set_tile_xyzs(HdcModeller* hm, const XYZ* h_xyzs) {
+    Modeller* m = reinterpret_cast<Modeller*>(hm);
+    if (!m || !h_xyzs) return HDC_ERR_ARG;
+    m->xyzs.assign(h_xyzs, h_xyzs + m->ntiles);
+    HDC_CUDA_RET_INT(cudaMemcpy(m->d_xyzs, h_xyzs, sizeof(XYZ) * m->ntiles, cudaMemcpyHostToDevice));
+    return HDC_OK;
+}
+
+extern "C" int hdc_modeller_model_timestep_with(HdcModeller* hm, double lst, JonesF32* d_vis, UVW* h_uvws,
+                                                hdcStream_t stream) {
+    Modeller* m = reinterpret_cast<Modeller*>(hm);
+    if (!m || !d_vis) {
+        hdc::set_error("hdc_modeller_model_timestep_with: invalid arguments");
+        return HDC_ERR_ARG;
+    }
+    return m->model(lst, d_vis, false, h_uvws, (cudaStream_t)stream);
+}
+
+extern "C" int hdc_modeller_model_timestep_with_f64(HdcModeller* hm, double lst, JonesF64* d_vis, UVW* h_uvws,
+                                                    hdcStream_t stream) {
+    Modeller* m = reinterpret_cast<Modeller*>(hm);
+    if (!m || !d_vis) {
+        hdc::set_error("hdc_modeller_model_timestep_with_f64: invalid arguments");
+        return HDC_ERR_ARG;
+    }
+    return m->model(lst, d_vis, true, h_uvws, (cudaStream_t)stream);
+}
+
+extern "C" int hdc_modeller_model_timestep_with_host(HdcModeller* hm, double lst, JonesF32* h_vis, UVW* h_uvws,
+                                                     hdcStream_t stream) {
+    Modeller* m = reinterpret_cast<Modeller*>(hm);
+    if (!m || !h_vis) {
+        hdc::set_error("hdc_modeller_model_timestep_with_host: invalid arguments");
+        return HDC_ERR_ARG;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t bytes = sizeof(JonesF32) * (size_t)m->nf * m->nbl;
+    if (m->host_vis_bytes < bytes) {
+        if (m->d_host_vis) cudaFree(m->d_host_vis);
+        m->d_host_vis = nullptr;
+        m->host_vis_bytes = 0;
+        HDC_CUDA_RET_INT(cudaMalloc(&m->d_host_vis, bytes));
+        m->host_vis_bytes = bytes;
+    }
+    HDC_CUDA_RET_INT(cudaMemcpyAsync(m->d_host_vis, h_vis, bytes, cudaMemcpyHostToDevice, s));
+    int rc = m->model(lst, m->d_host_vis, false, nullptr, s);
+    if (rc) return rc;
+    HDC_CUDA_RET_INT(cudaMemcpyAsync(h_vis, m->d_host_vis, bytes, cudaMemcpyDeviceToHost, s));
+    if (h_uvws) HDC_CUDA_RET_INT(cudaMemcpyAsync(h_uvws, m->d_uvws, sizeof(UVW) * m->nbl, cudaMemcpyDeviceToHost, s));
+    HDC_CUDA_RET_INT(cudaStreamSynchronize(s));
+    return HDC_OK;
+}
+
+extern "C" int hdc_modeller_update_with_a_source(HdcModeller* hm, const HdcSkyModel* source, RADec phase_centre) {
+    Modeller* m = reinterpret_cast<Modeller*>(hm);
+    if (!m || !source) return HDC_ERR_ARG;
+    cudaDeviceSynchronize();
+    m->pc = phase_centre;
+    int rc = m->build_tables(source);
+    if (rc) return rc;
+    if (m->form == HDC_PREDICT_TENSOR) return m->tensor_setup();
+    return HDC_OK;
+}
+
+extern "C" int hdc_modeller_set_profiling(HdcModeller* hm, int enable) {
+    Modeller* m = reinterpret_cast<Modeller*>(hm);
+    if (!m) return HDC_ERR_ARG;
+    m->profiling = enable != 0;
+    return HDC_OK;
+}
+
+extern "C" int hdc_modeller_profile(HdcModeller* hm, double* out_ms, int reset) {
+    Modeller* m = reinterpret_cast<Modeller*>(hm);
+    if (!m || !out_ms) return HDC_ERR_ARG;
+    m->prof_collect();
+    for (int k = 0; k < 4; k++) out_ms[k] = m->prof_ms[k];
+    if (reset)
+        for (int k = 0; k < 4; k++) m->prof_ms[k] = 0.0;
+    return HDC_OK;
+}
+
+extern "C" int hdc_modeller_model_timestep_autos_with(HdcModeller* hm, double lst, JonesF32* d_vis,
+                                                      hdcStream_t stream) {
+    Modeller* m = reinterpret_cast<Modeller*>(hm);
+    if (!m || !d_vis) return HDC_ERR_ARG;
+    return m->autos(lst, d_vis, (cudaStream_t)stream);
+}

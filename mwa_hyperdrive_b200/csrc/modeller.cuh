@@ -1,0 +1,68 @@
+// Native modeller state (host side).
+#pragma once
+
+#include <vector>
+
+#include "predict.cuh"
+
+namespace hdc {
+
+struct TypeTables {
+    int nc = 0;
+    double4* d_lmn = nullptr;    // [nc]
+    JonesF64* d_S = nullptr;     // [nf][nc] instrumental flux
+    JonesF64* d_W = nullptr;     // [nf][nc] B S B^H (beam set)
+    double4* d_gp = nullptr;     // [nc]
+    double2* d_radec = nullptr;  // [nc]
+    ShapeletCoeff* d_coeffs = nullptr;
+    int* d_cstart = nullptr;
+    int* d_ccount = nullptr;
+    double2* d_suv_tile = nullptr;  // [nc][ntiles]
+    void release();
+};
+
+struct TensorState;
+
+struct Modeller {
+    int device = 0;
+    int pols = 0, ntiles = 0, nbl = 0, nf = 0, beam_kind = 0, form = 0;
+    RADec pc{0, 0};
+    double lat = 0;
+    std::vector<double> freqs;
+    std::vector<XYZ> xyzs;
+    double* d_freqs = nullptr;
+    XYZ* d_xyzs = nullptr;
+    UVW* d_uvws = nullptr;
+    const double* d_sbf = nullptr;
+    int* d_err = nullptr;
+    TypeTables t[3];
+    JonesF32* d_host_vis = nullptr;
+    size_t host_vis_bytes = 0;
+    TensorState* tc = nullptr;
+
+    // Optional CUDA-event timing of each kernel class on the launching stream:
+    // class 0..2 = the per-type predict kernels, 3 = geometry/beam prep.
+    bool profiling = false;
+    struct EvPair {
+        cudaEvent_t a, b;
+        int cls;
+    };
+    std::vector<EvPair> ev_pending, ev_free;
+    double prof_ms[4] = {0, 0, 0, 0};
+    void prof_begin(int cls, cudaStream_t s, EvPair& e);
+    void prof_end(cudaStream_t s, EvPair& e);
+    void prof_collect();
+
+    int build_tables(const HdcSkyModel* sky);
+    int geometry(double lst, cudaStream_t s);
+    const JonesF64* weights(int ty) const;
+    DirectParams direct_params(int ty, void* vis) const;
+    int model(double lst, void* d_vis, bool out64, UVW* h_uvws, cudaStream_t s);
+    int autos(double lst, JonesF32* d_vis, cudaStream_t s);
+    int tensor_setup();
+    int tensor_points(double lst, void* d_vis, bool out64, cudaStream_t s);
+    void tensor_release();
+    ~Modeller();
+};
+
+}  // namespace hdc

@@ -1,0 +1,600 @@
+// Direct FP64 sky-model predictor for sm_100a and the drop-in model_* entry
+// points (replacing gpu/model.cu of mwa_hyperdrive).
+//
+// Kernel shape: one thread per (baseline, channel); a CTA covers 256
+// consecutive baselines of one channel, so component data is uniform across
+// the CTA.  Component tables (LMN, per-channel flux or B S B^H, envelope
+// parameters) are streamed through shared memory in chunks by the TMA engine
+// (cp.async.bulk) with a two-stage mbarrier pipeline; every thread reads them
+// as broadcasts.  The phase 2 pi (u l + v m + w (n - 1)) is formed in turns
+// and range-reduced exactly in FP64 (t - rint(t)) before sincospi; the
+// accumulation is FP64 and the visibility is updated once per type, as the
+// reference does (model/cpu.rs:341-348, gpu/model.cu:171).
+
+#include <cstdio>
+
+#include "predict.cuh"
+
+namespace hdc {
+
+constexpr int DT = 256;  // threads (baselines) per CTA
+constexpr int CH = 64;   // components per staged chunk
+
+template <int TYPE>
+__device__ __forceinline__ cplx shapelet_envelope(const DirectParams& p, int c, double4 g, double su, double sv) {
+    const double x = su * g.z + sv * g.w;
+    const double y = su * g.w - sv * g.z;
+    const double x_pos = x * g.x + SBF_C;
+    const double y_pos = y * g.y + SBF_C;
+    const double fx = floor(x_pos), fy = floor(y_pos);
+    // Negative positions clamp to 0 as in the reference (gpu/model.cu:63-64;
+    // on the CPU path the saturating usize cast does the same); positions past
+    // the table end clamp to the last interval so no read leaves the table.
+    int xi = fx > 0.0 ? (int)fmin(fx, (double)(SBF_L - 2)) : 0;
+    int yi = fy > 0.0 ? (int)fmin(fy, (double)(SBF_L - 2)) : 0;
+    const double xfrac = x_pos - fx, yfrac = y_pos - fy;
+    const int start = __ldg(p.coeff_start + c), count = __ldg(p.coeff_count + c);
+    cplx env = {0.0, 0.0};
+    for (int i = 0; i < count; i++) {
+        const ShapeletCoeff co = p.coeffs[start + i];
+        const double* bx = p.sbf + (size_t)SBF_L * co.n1 + xi;
+        const double* by = p.sbf + (size_t)SBF_L * co.n2 + yi;
+        const double x_low = __ldg(bx), x_high = __ldg(bx + 1);
+        const double y_low = __ldg(by), y_high = __ldg(by + 1);
+        const double u_value = x_low + (x_high - x_low) * xfrac;
+        const double v_value = y_low + (y_high - y_low) * yfrac;
+        const double rest = co.value * u_value * v_value;
+        switch ((co.n1 + co.n2) & 3) {
+            case 0: env.re += rest; break;
+            case 1: env.im += rest; break;
+            case 2: env.re -= rest; break;
+            default: env.im -= rest; break;
+        }
+    }
+    return env;
+}
+
+template <int TYPE, bool TILE_BEAM, bool OUT64>
+__global__ void __launch_bounds__(DT) direct_kernel(const DirectParams p) {
+    __shared__ alignas(128) double4 s_lmn[2][CH];
+    __shared__ alignas(128) JonesF64 s_flux[2][CH];
+    __shared__ alignas(128) double4 s_gp[2][CH];
+    __shared__ alignas(8) uint64_t bar[2];
+
+    const int f = blockIdx.y;
+    const int bl = blockIdx.x * DT + threadIdx.x;
+    const bool active = bl < p.nbl;
+    int t1 = 0, t2 = 1;
+    if (active) baseline_to_tiles(bl, p.ntiles, t1, t2);
+
+    const double freq = p.freqs[f];
+    const double ool = freq / VEL_C;
+    double u = 0.0, v = 0.0, w = 0.0;
+    if (active) {
+        const UVW q = p.uvws[bl];
+        if (TYPE == 2) {
+            u = q.u * ool;
+            v = q.v * ool;
+            w = q.w * ool;
+        } else {
+            u = q.u * freq / VEL_C;
+            v = q.v * freq / VEL_C;
+            w = q.w * freq / VEL_C;
+        }
+    }
+    const JonesF64* b1 = nullptr;
+    const JonesF64* b2 = nullptr;
+    if (TILE_BEAM && active) {
+        int u1 = p.unflagged_map ? p.unflagged_map[t1] : t1;
+        int u2 = p.unflagged_map ? p.unflagged_map[t2] : t2;
+        const int col = p.freq_map[f];
+        b1 = p.beam + (size_t)p.nc * ((size_t)p.n_uniq_freq * p.tile_map[u1] + col);
+        b2 = p.beam + (size_t)p.nc * ((size_t)p.n_uniq_freq * p.tile_map[u2] + col);
+    }
+
+    const int nchunks = (p.nc + CH - 1) / CH;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+
+    auto issue = [&](int k) {
+        const int st = k & 1;
+        const int c0 = k * CH;
+        const int n = min(CH, p.nc - c0);
+        const uint32_t bytes = n * 32u + n * 64u + (TYPE ? n * 32u : 0u);
+        mbar_arrive_expect_tx(&bar[st], bytes);
+        bulk_g2s(s_lmn[st], p.lmn + c0, n * 32u, &bar[st]);
+        bulk_g2s(s_flux[st], p.flux + (size_t)f * p.nc + c0, n * 64u, &bar[st]);
+        if (TYPE) bulk_g2s(s_gp[st], p.gp + c0, n * 32u, &bar[st]);
+    };
+    if (threadIdx.x == 0) {
+        fence_proxy_async_smem();
+        if (nchunks > 0) issue(0);
+        if (nchunks > 1) issue(1);
+    }
+
+    J2 acc = jzero();
+    for (int k = 0; k < nchunks; k++) {
+        const int st = k & 1;
+        const bool ok = mbar_wait_bounded(&bar[st], (k >> 1) & 1, p.err);
+        if (__syncthreads_or(!ok)) break;
+        const int c0 = k * CH;
+        const int n = min(CH, p.nc - c0);
+        if (active) {
+            for (int c = 0; c < n; c++) {
+                const double4 lmn = s_lmn[st][c];
+                J2 wj = load_j(s_flux[st][c]);
+                if (TILE_BEAM) {
+                    const J2 j1 = ldg_j(b1 + c0 + c);
+                    const J2 j2 = ldg_j(b2 + c0 + c);
+                    wj = (j1 * wj) * herm(j2);
+                }
+                const double t = u * lmn.x + v * lmn.y + w * lmn.z;
+                const cplx ph = phasor_turns(t);
+                if (TYPE == 0) {
+                    acc = acc + wj * ph;
+                } else if (TYPE == 1) {
+                    const double4 g = s_gp[st][c];
+                    const double kx = u * g.z + v * g.w;
+                    const double ky = u * g.w - v * g.z;
+                    const double env = exp(g.x * (kx * kx) + g.y * (ky * ky));
+                    acc = acc + (wj * ph) * env;
+                } else {
+                    const double4 g = s_gp[st][c];
+                    double su, sv;
+                    if (p.suv_bl) {
+                        const ShapeletUV q = p.suv_bl[(size_t)bl * p.nc + c0 + c];
+                        su = q.u;
+                        sv = q.v;
+                    } else {
+                        const double2 a = __ldg(p.suv_tile + (size_t)(c0 + c) * p.ntiles + t1);
+                        const double2 b = __ldg(p.suv_tile + (size_t)(c0 + c) * p.ntiles + t2);
+                        su = a.x - b.x;
+                        sv = a.y - b.y;
+                    }
+                    const cplx env = shapelet_envelope<TYPE>(p, c0 + c, g, su * ool, sv * ool);
+                    acc = acc + (wj * ph) * env;
+                }
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0 && k + 2 < nchunks) {
+            fence_proxy_async_smem();
+            issue(k + 2);
+        }
+    }
+
+    if (!active) return;
+    const size_t o = (size_t)f * p.nbl + bl;
+    if (OUT64) {
+        double2* q = reinterpret_cast<double2*>(reinterpret_cast<JonesF64*>(p.vis) + o);
+        double2 a = q[0], b = q[1], c = q[2], d = q[3];
+        q[0] = make_double2(a.x + acc.a.re, a.y + acc.a.im);
+        q[1] = make_double2(b.x + acc.b.re, b.y + acc.b.im);
+        q[2] = make_double2(c.x + acc.c.re, c.y + acc.c.im);
+        q[3] = make_double2(d.x + acc.d.re, d.y + acc.d.im);
+    } else {
+        float4* q = reinterpret_cast<float4*>(reinterpret_cast<JonesF32*>(p.vis) + o);
+        float4 a = q[0], b = q[1];
+        a.x += (float)acc.a.re;
+        a.y += (float)acc.a.im;
+        a.z += (float)acc.b.re;
+        a.w += (float)acc.b.im;
+        b.x += (float)acc.c.re;
+        b.y += (float)acc.c.im;
+        b.z += (float)acc.d.re;
+        b.w += (float)acc.d.im;
+        q[0] = a;
+        q[1] = b;
+    }
+}
+
+template <int TYPE>
+static cudaError_t launch_t(bool tile_beam, bool out64, const DirectParams& p, cudaStream_t s) {
+    dim3 grid((p.nbl + DT - 1) / DT, p.nf);
+    if (tile_beam) {
+        if (out64)
+            direct_kernel<TYPE, true, true><<<grid, DT, 0, s>>>(p);
+        else
+            direct_kernel<TYPE, true, false><<<grid, DT, 0, s>>>(p);
+    } else {
+        if (out64)
+            direct_kernel<TYPE, false, true><<<grid, DT, 0, s>>>(p);
+        else
+            direct_kernel<TYPE, false, false><<<grid, DT, 0, s>>>(p);
+    }
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_direct(int ty, bool tile_beam, bool out64, const DirectParams& p, cudaStream_t s) {
+    if (p.nc <= 0 || p.nbl <= 0 || p.nf <= 0) return cudaSuccess;
+    if (ty == 0) return launch_t<0>(tile_beam, out64, p, s);
+    if (ty == 1) return launch_t<1>(tile_beam, out64, p, s);
+    return launch_t<2>(tile_beam, out64, p, s);
+}
+
+// Auto-correlations: one thread per (tile, channel) (gpu/model.cu:368-485;
+// the envelope is 1 for every component type).
+__global__ void autos_kernel(const AutosParams p) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.ntiles * p.nf) return;
+    const int f = i % p.nf;
+    const int tile = i / p.nf;
+    J2 acc = jzero();
+    const JonesF64* bj = nullptr;
+    if (p.beam) {
+        const int ut = p.unflagged_map ? p.unflagged_map[tile] : tile;
+        bj = p.beam + (size_t)p.nc_total * ((size_t)p.n_uniq_freq * p.tile_map[ut] + p.freq_map[f]);
+    }
+    for (int c = 0; c < p.nc_total; c++) {
+        J2 sj = ldg_j(p.flux + (size_t)f * p.nc_total + c);
+        if (bj) {
+            const J2 b = ldg_j(bj + c);
+            sj = (b * sj) * herm(b);
+        }
+        acc = acc + sj;
+    }
+    JonesF32* o = p.vis + (size_t)f * p.ntiles + tile;
+    o->j00_re += (float)acc.a.re;
+    o->j00_im += (float)acc.a.im;
+    o->j01_re += (float)acc.b.re;
+    o->j01_im += (float)acc.b.im;
+    o->j10_re += (float)acc.c.re;
+    o->j10_im += (float)acc.c.im;
+    o->j11_re += (float)acc.d.re;
+    o->j11_im += (float)acc.d.im;
+}
+
+cudaError_t launch_autos(const AutosParams& p, cudaStream_t s) {
+    if (p.ntiles * p.nf == 0 || p.nc_total == 0) return cudaSuccess;
+    const int n = p.ntiles * p.nf;
+    autos_kernel<<<(n + 255) / 256, 256, 0, s>>>(p);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+__global__ void mask_pols_kernel(JonesF32* vis, size_t n, int pols) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    JonesF32 j = vis[i];
+    const bool k0 = pols == 1 || pols == 3 || pols == 4;
+    const bool k1 = pols == 4;
+    const bool k3 = pols == 2 || pols == 3 || pols == 4;
+    if (!k0) j.j00_re = j.j00_im = 0.0f;
+    if (!k1) j.j01_re = j.j01_im = 0.0f;
+    j.j10_re = j.j10_im = 0.0f;
+    if (!k3) j.j11_re = j.j11_im = 0.0f;
+    vis[i] = j;
+}
+
+cudaError_t launch_mask_pols(JonesF32* vis, size_t n, int pols, cudaStream_t s) {
+    if (pols == 0 || n == 0) return cudaSuccess;
+    mask_pols_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(vis, n, pols);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Drop-in layer: the reference's component tables -> per-type direct tables.
+// ---------------------------------------------------------------------------
+
+// One flux-model group of a component type as the reference passes it.
+struct GroupIn {
+    int n;
+    const LmnRime* lmns;
+    const JonesF64* fds;  // PL/CPL: [n] at 150 MHz; list: [nf][n]
+    const double* sis;
+    const double* qs;
+    const GaussianParams* gps;
+    const ShapeletUV* suvs;  // [nbl][n]
+    const ShapeletCoeff* coeffs;
+    const int* num_coeffs;
+};
+
+struct PrepIn {
+    GroupIn g[3];  // power law, curved power law, list
+    int nc, nf, nbl, type;
+    const double* freqs;
+    double4* lmn;
+    JonesF64* flux;   // [nf][flux_ld]
+    int flux_ld;
+    double4* gp;
+    ShapeletUV* suv;  // [nbl][nc]
+};
+
+// Per (channel, component): instrumental flux at the channel as the reference
+// GPU kernels extrapolate it from 150 MHz (gpu/model.cu:16-28), plus the
+// component's LMN in turns and envelope parameters.
+__global__ void dropin_prep_kernel(const PrepIn in) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int f = blockIdx.y;
+    if (c >= in.nc) return;
+    int grp = 0, k = c;
+    if (k >= in.g[0].n) {
+        k -= in.g[0].n;
+        grp = 1;
+        if (k >= in.g[1].n) {
+            k -= in.g[1].n;
+            grp = 2;
+        }
+    }
+    const GroupIn& g = in.g[grp];
+    const double freq = in.freqs[f];
+    JonesF64 s;
+    if (grp == 2) {
+        s = g.fds[(size_t)f * g.n + k];
+    } else {
+        const double ratio = pow(freq / POWER_LAW_FD_REF_FREQ, g.sis[k]);
+        J2 j = load_j(g.fds[k]) * ratio;
+        if (grp == 1) {
+            const double lt = log(freq / POWER_LAW_FD_REF_FREQ);
+            j = j * exp(g.qs[k] * lt * lt);
+        }
+        s = store_j(j);
+    }
+    in.flux[(size_t)f * in.flux_ld + c] = s;
+    if (f == 0) {
+        const LmnRime l = g.lmns[k];
+        in.lmn[c] = make_double4(l.l * INV_TAU, l.m * INV_TAU, l.n * INV_TAU, 0.0);
+        if (in.type >= 1) {
+            const GaussianParams gp = g.gps[k];
+            double sp, cp;
+            sincos(gp.pa, &sp, &cp);
+            if (in.type == 1)
+                in.gp[c] = make_double4(GAUSSIAN_EXP_CONST * (gp.maj * gp.maj), GAUSSIAN_EXP_CONST * (gp.min * gp.min), sp, cp);
+            else
+                in.gp[c] = make_double4(gp.maj * SHAPELET_CONST, -gp.min * SHAPELET_CONST, sp, cp);
+        }
+    }
+}
+
+__global__ void dropin_suv_kernel(const PrepIn in) {
+    // gather the three groups' [nbl][n_g] shapelet UVs into [nbl][nc]
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)in.nbl * in.nc) return;
+    const int bl = (int)(i / in.nc);
+    int k = (int)(i % in.nc);
+    int grp = 0;
+    if (k >= in.g[0].n) {
+        k -= in.g[0].n;
+        grp = 1;
+        if (k >= in.g[1].n) {
+            k -= in.g[1].n;
+            grp = 2;
+        }
+    }
+    in.suv[i] = in.g[grp].suvs[(size_t)bl * in.g[grp].n + k];
+}
+
+// Exclusive scan of per-component coefficient counts (single thread; the
+// component counts here are small) and repacking of the three groups'
+// coefficient arrays into one table.
+__global__ void dropin_coeff_kernel(const PrepIn in, int* start, int* count, ShapeletCoeff* out) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    int off = 0, c = 0;
+    for (int grp = 0; grp < 3; grp++) {
+        int goff = 0;
+        for (int k = 0; k < in.g[grp].n; k++, c++) {
+            const int nk = in.g[grp].num_coeffs[k];
+            start[c] = off;
+            count[c] = nk;
+            for (int i = 0; i < nk; i++) out[off + i] = in.g[grp].coeffs[goff + i];
+            off += nk;
+            goff += nk;
+        }
+    }
+}
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Sum of per-component coefficient counts needs a device read; the drop-in
+// entry point copies the counts back (small) to size the repacked table.
+static const char* dropin_model(int type, const GroupIn g[3], const Addresses* a, const UVW* d_uvws,
+                                const JonesF64* d_beam_jones, JonesF32* d_vis_fb) {
+    const int nc = g[0].n + g[1].n + g[2].n;
+    if (nc == 0) return NULL;
+    const int nf = a->num_freqs, nbl = a->num_baselines;
+    int total_coeffs = 0;
+    if (type == 2) {
+        for (int grp = 0; grp < 3; grp++) {
+            if (g[grp].n == 0) continue;
+            int* h = (int*)malloc(sizeof(int) * g[grp].n);
+            if (!h) return "host allocation failed";
+            cudaError_t e = cudaMemcpy(h, g[grp].num_coeffs, sizeof(int) * g[grp].n, cudaMemcpyDeviceToHost);
+            if (e != cudaSuccess) {
+                free(h);
+                set_error("model_shapelets: %s", cudaGetErrorString(e));
+                return cudaGetErrorString(e);
+            }
+            for (int k = 0; k < g[grp].n; k++) total_coeffs += h[k];
+            free(h);
+        }
+    }
+    size_t off_lmn = 0;
+    size_t off_flux = align256(off_lmn + sizeof(double4) * nc);
+    size_t off_gp = align256(off_flux + sizeof(JonesF64) * (size_t)nf * nc);
+    size_t off_suv = align256(off_gp + sizeof(double4) * nc);
+    size_t off_cs = align256(off_suv + (type == 2 ? sizeof(ShapeletUV) * (size_t)nbl * nc : 0));
+    size_t off_cc = align256(off_cs + sizeof(int) * nc);
+    size_t off_co = align256(off_cc + sizeof(int) * nc);
+    size_t total = align256(off_co + sizeof(ShapeletCoeff) * (size_t)(total_coeffs + 1));
+    char* ws = (char*)device_scratch(total);
+    if (!ws) return "out of device memory";
+
+    PrepIn in;
+    for (int i = 0; i < 3; i++) in.g[i] = g[i];
+    in.nc = nc;
+    in.nf = nf;
+    in.nbl = nbl;
+    in.type = type;
+    in.freqs = a->d_freqs;
+    in.lmn = (double4*)(ws + off_lmn);
+    in.flux = (JonesF64*)(ws + off_flux);
+    in.flux_ld = nc;
+    in.gp = (double4*)(ws + off_gp);
+    in.suv = (ShapeletUV*)(ws + off_suv);
+    dim3 pg((nc + 127) / 128, nf);
+    dropin_prep_kernel<<<pg, 128>>>(in);
+    count_launches(1);
+    HDC_CUDA_RET_STR(cudaGetLastError());
+    int* cstart = (int*)(ws + off_cs);
+    int* ccount = (int*)(ws + off_cc);
+    ShapeletCoeff* co = (ShapeletCoeff*)(ws + off_co);
+    if (type == 2) {
+        size_t n = (size_t)nbl * nc;
+        dropin_suv_kernel<<<(unsigned)((n + 255) / 256), 256>>>(in);
+        count_launches(1);
+        HDC_CUDA_RET_STR(cudaGetLastError());
+        dropin_coeff_kernel<<<1, 1>>>(in, cstart, ccount, co);
+        count_launches(1);
+        HDC_CUDA_RET_STR(cudaGetLastError());
+    }
+    DirectParams p = {};
+    p.nbl = nbl;
+    p.nf = nf;
+    p.ntiles = (int)((1.0 + sqrt(1.0 + 8.0 * nbl)) / 2.0 + 0.5);
+    p.nc = nc;
+    p.freqs = a->d_freqs;
+    p.uvws = d_uvws;
+    p.lmn = in.lmn;
+    p.flux = in.flux;
+    p.gp = in.gp;
+    p.beam = d_beam_jones;
+    p.tile_map = a->d_tile_map;
+    p.unflagged_map = a->d_tile_index_to_unflagged_tile_index_map;
+    p.freq_map = a->d_freq_map;
+    p.n_uniq_freq = a->num_unique_beam_freqs;
+    p.sbf = a->d_shapelet_basis_values ? a->d_shapelet_basis_values : device_shapelet_basis();
+    p.coeffs = co;
+    p.coeff_start = cstart;
+    p.coeff_count = ccount;
+    p.suv_bl = type == 2 ? in.suv : nullptr;
+    p.suv_tile = nullptr;
+    p.vis = d_vis_fb;
+    p.err = device_error_word();
+    const bool tile_beam = d_beam_jones != nullptr;
+    HDC_CUDA_RET_STR(launch_direct(type, tile_beam, false, p, 0));
+#ifdef HDC_DEBUG_SYNC
+    HDC_CUDA_RET_STR(cudaDeviceSynchronize());
+#endif
+    return NULL;
+}
+
+}  // namespace hdc
+
+using namespace hdc;
+
+extern "C" const char* model_points(const Points* comps, const Addresses* a, const UVW* d_uvws,
+                                    const JonesF64* d_beam_jones, JonesF32* d_vis_fb) {
+    GroupIn g[3] = {};
+    g[0] = GroupIn{comps->num_power_laws, comps->power_law_lmns, comps->power_law_fds, comps->power_law_sis};
+    g[1] = GroupIn{comps->num_curved_power_laws, comps->curved_power_law_lmns, comps->curved_power_law_fds,
+                   comps->curved_power_law_sis, comps->curved_power_law_qs};
+    g[2] = GroupIn{comps->num_lists, comps->list_lmns, comps->list_fds};
+    return dropin_model(0, g, a, d_uvws, d_beam_jones, d_vis_fb);
+}
+
+extern "C" const char* model_gaussians(const Gaussians* comps, const Addresses* a, const UVW* d_uvws,
+                                       const JonesF64* d_beam_jones, JonesF32* d_vis_fb) {
+    GroupIn g[3] = {};
+    g[0] = GroupIn{comps->num_power_laws, comps->power_law_lmns, comps->power_law_fds, comps->power_law_sis, nullptr,
+                   comps->power_law_gps};
+    g[1] = GroupIn{comps->num_curved_power_laws, comps->curved_power_law_lmns, comps->curved_power_law_fds,
+                   comps->curved_power_law_sis, comps->curved_power_law_qs, comps->curved_power_law_gps};
+    g[2] = GroupIn{comps->num_lists, comps->list_lmns, comps->list_fds, nullptr, nullptr, comps->list_gps};
+    return dropin_model(1, g, a, d_uvws, d_beam_jones, d_vis_fb);
+}
+
+extern "C" const char* model_shapelets(const Shapelets* comps, const Addresses* a, const UVW* d_uvws,
+                                       const JonesF64* d_beam_jones, JonesF32* d_vis_fb) {
+    GroupIn g[3] = {};
+    g[0] = GroupIn{comps->num_power_laws,           comps->power_law_lmns,          comps->power_law_fds,
+                   comps->power_law_sis,            nullptr,                        comps->power_law_gps,
+                   comps->power_law_shapelet_uvs,   comps->power_law_shapelet_coeffs, comps->power_law_num_shapelet_coeffs};
+    g[1] = GroupIn{comps->num_curved_power_laws,
+                   comps->curved_power_law_lmns,
+                   comps->curved_power_law_fds,
+                   comps->curved_power_law_sis,
+                   comps->curved_power_law_qs,
+                   comps->curved_power_law_gps,
+                   comps->curved_power_law_shapelet_uvs,
+                   comps->curved_power_law_shapelet_coeffs,
+                   comps->curved_power_law_num_shapelet_coeffs};
+    g[2] = GroupIn{comps->num_lists,          comps->list_lmns,           comps->list_fds,
+                   nullptr,                   nullptr,                    comps->list_gps,
+                   comps->list_shapelet_uvs,  comps->list_shapelet_coeffs, comps->list_num_shapelet_coeffs};
+    return dropin_model(2, g, a, d_uvws, d_beam_jones, d_vis_fb);
+}
+
+extern "C" const char* model_autos(int num_tiles, int num_freqs, const double* freqs, const Points* points,
+                                   const Gaussians* gaussians, const Shapelets* shapelets, const JonesF64* beam_jones,
+                                   const int* tile_map, const int* freq_map, int num_fee_freqs,
+                                   const int* tile_index_to_unflagged_tile_index_map, JonesF32* vis_fb) {
+    // Build one concatenated flux table over all nine groups, in the
+    // reference's direction order (gpu/model.cu:380-470).
+    GroupIn gs[9] = {};
+    gs[0] = GroupIn{points->num_power_laws, points->power_law_lmns, points->power_law_fds, points->power_law_sis};
+    gs[1] = GroupIn{points->num_curved_power_laws, points->curved_power_law_lmns, points->curved_power_law_fds,
+                    points->curved_power_law_sis, points->curved_power_law_qs};
+    gs[2] = GroupIn{points->num_lists, points->list_lmns, points->list_fds};
+    gs[3] = GroupIn{gaussians->num_power_laws, gaussians->power_law_lmns, gaussians->power_law_fds,
+                    gaussians->power_law_sis};
+    gs[4] = GroupIn{gaussians->num_curved_power_laws, gaussians->curved_power_law_lmns,
+                    gaussians->curved_power_law_fds, gaussians->curved_power_law_sis, gaussians->curved_power_law_qs};
+    gs[5] = GroupIn{gaussians->num_lists, gaussians->list_lmns, gaussians->list_fds};
+    gs[6] = GroupIn{shapelets->num_power_laws, shapelets->power_law_lmns, shapelets->power_law_fds,
+                    shapelets->power_law_sis};
+    gs[7] = GroupIn{shapelets->num_curved_power_laws, shapelets->curved_power_law_lmns,
+                    shapelets->curved_power_law_fds, shapelets->curved_power_law_sis, shapelets->curved_power_law_qs};
+    gs[8] = GroupIn{shapelets->num_lists, shapelets->list_lmns, shapelets->list_fds};
+    int nc_total = 0;
+    for (int i = 0; i < 9; i++) nc_total += gs[i].n;
+    if (nc_total == 0) return NULL;
+    size_t flux_bytes = align256(sizeof(JonesF64) * (size_t)num_freqs * nc_total);
+    size_t lmn_bytes = align256(sizeof(double4) * (size_t)nc_total);
+    char* ws = (char*)device_scratch(flux_bytes + 3 * lmn_bytes + 256);
+    if (!ws) return "out of device memory";
+    JonesF64* flux = (JonesF64*)ws;
+    // Prepare each component type's three groups as one table, then copy its
+    // columns into the concatenated table.
+    int col = 0;
+    for (int ty = 0; ty < 3; ty++) {
+        PrepIn in = {};
+        int nty = 0;
+        for (int i = 0; i < 3; i++) {
+            in.g[i] = gs[3 * ty + i];
+            nty += in.g[i].n;
+        }
+        if (nty == 0) continue;
+        in.nc = nty;
+        in.nf = num_freqs;
+        in.type = 0;  // envelope parameters are not needed for autos
+        in.freqs = freqs;
+        in.lmn = (double4*)(ws + flux_bytes);
+        in.gp = (double4*)(ws + flux_bytes + lmn_bytes);
+        in.flux = flux + col;
+        in.flux_ld = nc_total;
+        dim3 pg((nty + 127) / 128, num_freqs);
+        dropin_prep_kernel<<<pg, 128>>>(in);
+        count_launches(1);
+        HDC_CUDA_RET_STR(cudaGetLastError());
+        col += nty;
+    }
+    AutosParams p;
+    p.ntiles = num_tiles;
+    p.nf = num_freqs;
+    p.nc_total = nc_total;
+    p.flux = flux;
+    p.beam = beam_jones;
+    p.tile_map = tile_map;
+    p.unflagged_map = tile_index_to_unflagged_tile_index_map;
+    p.freq_map = freq_map;
+    p.n_uniq_freq = num_fee_freqs;
+    p.vis = vis_fb;
+    HDC_CUDA_RET_STR(launch_autos(p, 0));
+    return NULL;
+}

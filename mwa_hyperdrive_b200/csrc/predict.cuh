@@ -1,0 +1,59 @@
+// Direct FP64 predictor kernels (shared by the drop-in entry points and the
+// native modeller).
+#pragma once
+
+#include "common.cuh"
+
+namespace hdc {
+
+// Per-type component tables consumed by the direct kernel.  Component order
+// is the modelling order; for the drop-in layer it is power laws, curved
+// power laws, lists (gpu/types.h:187-267), which is also the beam-direction
+// order of d_beam_jones.
+struct DirectParams {
+    int nbl, nf, ntiles, nc;
+    const double* freqs;  // [nf] Hz
+    const UVW* uvws;      // [nbl] m
+    const double4* lmn;   // [nc] (l, m, n - 1, 0), dimensionless (turn units)
+    const JonesF64* flux; // [nf][nc]: B S B^H when the beam is shared (or none), S when per tile
+    const double4* gp;    // [nc] Gaussian: (C maj^2, C min^2, sin pa, cos pa); shapelet: (maj K, -min K, sin pa, cos pa)
+    // per-tile beam, reference layout [uniq_tile][uniq_freq][nc]
+    const JonesF64* beam;
+    const int* tile_map;
+    const int* unflagged_map;
+    const int* freq_map;
+    int n_uniq_freq;
+    // shapelets
+    const double* sbf;  // [SBF_N][SBF_L]
+    const ShapeletCoeff* coeffs;
+    const int* coeff_start;
+    const int* coeff_count;
+    const ShapeletUV* suv_bl;  // [nbl][nc] m, or NULL
+    const double2* suv_tile;   // [nc][ntiles] m, or NULL (then suv = tile1 - tile2)
+    void* vis;                 // [nf][nbl] JonesF32 or JonesF64, accumulated
+    int* err;
+};
+
+// Launch the direct kernel for component type ty (0 point, 1 Gaussian,
+// 2 shapelet).  tile_beam selects per-tile beam Jones; out64 an FP64 output.
+cudaError_t launch_direct(int ty, bool tile_beam, bool out64, const DirectParams& p, cudaStream_t s);
+
+struct AutosParams {
+    int ntiles, nf;
+    int nc_total;
+    // up to 3 type tables concatenated by the caller into one [nf][nc] flux
+    // table (S) and a beam table [uniq_tile][uniq_freq][nc] (NULL: identity)
+    const JonesF64* flux;
+    const JonesF64* beam;
+    const int* tile_map;
+    const int* unflagged_map;
+    const int* freq_map;
+    int n_uniq_freq;
+    JonesF32* vis;  // [nf][ntiles]
+};
+cudaError_t launch_autos(const AutosParams& p, cudaStream_t s);
+
+// mask_pols over a [n] JonesF32 buffer (model/mod.rs:264-285)
+cudaError_t launch_mask_pols(JonesF32* vis, size_t n, int pols, cudaStream_t s);
+
+}  // namespace hdc

@@ -1,0 +1,130 @@
+"""Seeded synthetic observations with the shapes of the benchmark
+configurations (the reference publishes no dataset for this path).
+
+Arrays: tiles uniform in a disk in the local east/north plane, converted to
+geodetic XYZ at the MWA latitude.  Sky models: components uniform in a
+spherical cap around the phase centre.
+"""
+
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+from typing import List, Optional
+
+import numpy as np
+
+from . import srclist as sl
+
+MWA_LAT_RAD = -0.4660608448386394
+SIDEREAL_RATE = 7.292115855306589e-5  # rad / s
+VEL_C = 299792458.0
+
+
+def enu_to_xyz(e, n, u, lat=MWA_LAT_RAD):
+    """Local east/north/up [m] -> geodetic XYZ [m] (X in the meridian plane)."""
+    sl_, cl = math.sin(lat), math.cos(lat)
+    x = -sl_ * n + cl * u
+    y = e
+    z = cl * n + sl_ * u
+    return np.stack([x, y, z], axis=-1)
+
+
+def tiles_in_disk(num_tiles: int, radius_m: float, seed: int) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    r = radius_m * np.sqrt(rng.random(num_tiles))
+    th = rng.random(num_tiles) * 2 * math.pi
+    return enu_to_xyz(r * np.cos(th), r * np.sin(th), np.zeros(num_tiles))
+
+
+def cap_positions(n: int, centre, radius_rad: float, rng) -> np.ndarray:
+    """Uniform positions (ra, dec) within a cap of angular radius around centre."""
+    cosr = math.cos(radius_rad)
+    z = 1.0 - rng.random(n) * (1.0 - cosr)  # cos of offset angle
+    rho = np.arccos(z)
+    phi = rng.random(n) * 2 * math.pi
+    # offset direction in the tangent frame of the centre
+    ra0, dec0 = centre
+    sd, cd = math.sin(dec0), math.cos(dec0)
+    sr, cr = np.sin(rho), np.cos(rho)
+    dec = np.arcsin(sd * cr + cd * sr * np.cos(phi))
+    ra = ra0 + np.arctan2(np.sin(phi) * sr * cd, cr - sd * np.sin(dec))
+    return np.stack([ra, dec], axis=-1)
+
+
+@dataclass
+class Obs:
+    tile_xyzs: np.ndarray
+    freqs: np.ndarray
+    phase_centre: tuple
+    lsts: np.ndarray
+    latitude: float = MWA_LAT_RAD
+
+    @property
+    def num_tiles(self):
+        return self.tile_xyzs.shape[0]
+
+    @property
+    def num_baselines(self):
+        n = self.num_tiles
+        return n * (n - 1) // 2
+
+
+def point_sky(n: int, centre, radius_deg: float, seed: int, curved_q_sigma: Optional[float] = None,
+              ref_freq: float = 150e6) -> List[sl.SourceComponent]:
+    rng = np.random.default_rng(seed)
+    pos = cap_positions(n, centre, math.radians(radius_deg), rng)
+    flux_i = rng.lognormal(0.0, 1.0, n)
+    si = rng.normal(-0.8, 0.2, n)
+    qs = rng.normal(0.0, curved_q_sigma, n) if curved_q_sigma else None
+    comps = []
+    for k in range(n):
+        fd = sl.FluxDensity(ref_freq, float(flux_i[k]))
+        ft = sl.CurvedPowerLaw(float(si[k]), fd, float(qs[k])) if qs is not None else sl.PowerLaw(float(si[k]), fd)
+        comps.append(sl.SourceComponent(float(pos[k, 0]), float(pos[k, 1]), sl.Point(), ft))
+    return comps
+
+
+def config1():
+    """Plain point-source predict, f64: 128 tiles in a 1.5 km disk, 1
+    timestep at HA 0, 32 channels of 40 kHz from 170 MHz, 200 points within
+    10 deg of (0, -27 deg), lognormal(0, 1) Jy at 150 MHz, SI N(-0.8, 0.2),
+    no beam."""
+    pc = (0.0, math.radians(-27.0))
+    obs = Obs(tiles_in_disk(128, 750.0, 1), 170.0e6 + np.arange(32) * 40e3, pc, np.array([pc[0]]))
+    sky = sl.SkyModelArrays.from_components(point_sky(200, pc, 10.0, 1))
+    return obs, sky
+
+
+def gaussians_and_shapelets(n_g: int, n_s: int, centre, seed: int, q_sigma: float = 0.2, ncoeff: int = 20):
+    rng = np.random.default_rng(seed)
+    arcmin = math.radians(1.0 / 60.0)
+    comps = []
+    pos = cap_positions(n_g + n_s, centre, math.radians(10.0), rng)
+    for k in range(n_g + n_s):
+        maj = rng.uniform(0.5, 5.0) * arcmin
+        mn = maj * rng.uniform(0.3, 1.0)
+        pa = rng.uniform(0.0, math.pi)
+        fd = sl.FluxDensity(150e6, float(rng.lognormal(0.0, 1.0)))
+        ft = sl.CurvedPowerLaw(float(rng.normal(-0.8, 0.2)), fd, float(rng.normal(0.0, q_sigma)))
+        if k < n_g:
+            ct = sl.Gaussian(maj, mn, pa)
+        else:
+            coeffs = [sl.ShapeletCoeff(int(rng.integers(0, 6)), int(rng.integers(0, 6)), float(rng.normal() * 0.1))
+                      for _ in range(ncoeff)]
+            ct = sl.Shapelet(maj, mn, pa, coeffs)
+        comps.append(sl.SourceComponent(float(pos[k, 0]), float(pos[k, 1]), ct, ft))
+    return comps
+
+
+def config2(n_points=4000, n_gauss=500, n_shapelets=100, n_freqs=384, n_times=4):
+    """Mixed-component predict: 128 tiles, 4 timesteps 8 s apart, 384
+    channels of 80 kHz from 167 MHz, 4000 points + 500 Gaussians + 100
+    shapelets (20 coefficients, n1, n2 <= 5), curved power laws with q ~
+    N(0, 0.2), analytic dipole-array beam shared by all tiles."""
+    pc = (0.0, math.radians(-27.0))
+    lsts = pc[0] + np.arange(n_times) * 8.0 * SIDEREAL_RATE
+    obs = Obs(tiles_in_disk(128, 750.0, 2), 167.0e6 + np.arange(n_freqs) * 80e3, pc, lsts)
+    comps = point_sky(n_points, pc, 10.0, 2, curved_q_sigma=0.2)
+    comps += gaussians_and_shapelets(n_gauss, n_shapelets, pc, 22)
+    return obs, sl.SkyModelArrays.from_components(comps)
