@@ -237,6 +237,9 @@ def gpu_arm(args, rank, world, local_rank):
         for _ in range(warmup):
             step(m)
         torch.cuda.synchronize()
+        # discard event timings recorded during warm-up
+        discard = (ctypes.c_double * 4)()
+        L.hdc_modeller_profile(m._h, discard, 1)
         if dist:
             dist.barrier()
         torch.cuda.synchronize()

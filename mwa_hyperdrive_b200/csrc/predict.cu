@@ -373,7 +373,10 @@ __global__ void dropin_suv_kernel(const PrepIn in) {
 // Exclusive scan of per-component coefficient counts (single thread; the
 // component counts here are small) and repacking of the three groups'
 // coefficient arrays into one table.
-__global__ void dropin_coeff_kernel(const PrepIn in, int* start, int* count, ShapeletCoeff* out) {
+// Coefficients whose orders fall outside the basis table (n >= SBF_N) would
+// index past it; they are replaced by a zero coefficient and flagged in *err
+// (KERR_INDEX) so that the entry point can return an error.
+__global__ void dropin_coeff_kernel(const PrepIn in, int* start, int* count, ShapeletCoeff* out, int* err) {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
     int off = 0, c = 0;
     for (int grp = 0; grp < 3; grp++) {
@@ -382,7 +385,16 @@ __global__ void dropin_coeff_kernel(const PrepIn in, int* start, int* count, Sha
             const int nk = in.g[grp].num_coeffs[k];
             start[c] = off;
             count[c] = nk;
-            for (int i = 0; i < nk; i++) out[off + i] = in.g[grp].coeffs[goff + i];
+            for (int i = 0; i < nk; i++) {
+                ShapeletCoeff co = in.g[grp].coeffs[goff + i];
+                if (co.n1 >= SBF_N || co.n2 >= SBF_N) {
+                    *err |= KERR_INDEX;
+                    co.value = 0.0;
+                    co.n1 = 0;
+                    co.n2 = 0;
+                }
+                out[off + i] = co;
+            }
             off += nk;
             goff += nk;
         }
@@ -449,9 +461,18 @@ static const char* dropin_model(int type, const GroupIn g[3], const Addresses* a
         dropin_suv_kernel<<<(unsigned)((n + 255) / 256), 256>>>(in);
         count_launches(1);
         HDC_CUDA_RET_STR(cudaGetLastError());
-        dropin_coeff_kernel<<<1, 1>>>(in, cstart, ccount, co);
+        int* flag = device_error_word();
+        if (!flag) return "device error word unavailable";
+        dropin_coeff_kernel<<<1, 1>>>(in, cstart, ccount, co, flag);
         count_launches(1);
         HDC_CUDA_RET_STR(cudaGetLastError());
+        int h = 0;
+        HDC_CUDA_RET_STR(cudaMemcpy(&h, flag, sizeof(int), cudaMemcpyDeviceToHost));
+        if (h & KERR_INDEX) {
+            cudaMemset(flag, 0, sizeof(int));
+            set_error("model_shapelets: a shapelet coefficient order is outside 0..%d", SBF_N - 1);
+            return "model_shapelets: shapelet coefficient order outside the basis table";
+        }
     }
     DirectParams p = {};
     p.nbl = nbl;

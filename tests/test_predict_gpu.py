@@ -307,9 +307,9 @@ def test_dropin_model_functions_per_tile_beam(oracle, ctype):
     co["value"] = [0.5, -0.2]
     co["n1"] = [1, 2]
     co["n2"] = [0, 3]
-    co3 = np.concatenate([co, co, co])
+    co3 = np.concatenate([co] * 9)  # 3 groups x 3 components x 2 coefficients
     coeffs = put("co", co3.view(np.uint8), np.uint8)
-    ncoef = put("nco", np.array([2, 2, 2], np.int32), np.int32)
+    ncoef = put("nco", np.array([2] * 9, np.int32), np.int32)
     freqs = put("freqs", obs.freqs)
     tm = put("tm", tile_map, np.int32)
     fm = put("fm", freq_map, np.int32)
@@ -329,8 +329,8 @@ def test_dropin_model_functions_per_tile_beam(oracle, ctype):
         res = L.model_gaussians(ctypes.byref(p), ctypes.byref(a), d_uvws, bj, vis.data_ptr())
     else:
         p = _lib.Shapelets(3, o3(0), fds, sis, gpar, suv_pl, coeffs, ncoef,
-                           3, o3(3), fds + 3 * 64, sis + 3 * 8, qs, gpar + 72, suv_cpl, coeffs + 32, ncoef + 12,
-                           3, o3(6), lf, gpar + 144, suv_l, coeffs + 64, ncoef + 24)
+                           3, o3(3), fds + 3 * 64, sis + 3 * 8, qs, gpar + 72, suv_cpl, coeffs + 96, ncoef + 12,
+                           3, o3(6), lf, gpar + 144, suv_l, coeffs + 192, ncoef + 24)
         res = L.model_shapelets(ctypes.byref(p), ctypes.byref(a), d_uvws, bj, vis.data_ptr())
     _lib.check_str(res, "model_*")
     torch.cuda.synchronize()
