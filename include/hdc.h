@@ -173,6 +173,21 @@ typedef struct IonoConsts {
 const char *model_points(const Points *comps, const Addresses *a, const UVW *d_uvws, const JonesF64 *d_beam_jones,
                          JonesF32 *d_vis_fb);
 
+/* No counterpart in the reference.  model_points for callers that cannot
+ * allocate device memory (hosts that reserve the whole device for their own
+ * memory pool, or streaming loops that must not call cudaMalloc because of its
+ * implicit device synchronisation).  Same arguments and result as
+ * model_points, but its scratch is a fixed array compiled into the library
+ * (HDC_NOALLOC_SCRATCH_BYTES per device, held until exit): it needs
+ * 32 B per component + 64 B per (channel, component), and larger problems
+ * are rejected with an error.  Every call on a device shares that array, so
+ * calls whose kernels overlap on the GPU race and must be serialised.  The
+ * first call on a device looks up the array's device address and should come
+ * before any stream capture. */
+#define HDC_NOALLOC_SCRATCH_BYTES (16u * 1024u * 1024u)
+const char *model_points_noalloc(const Points *comps, const Addresses *a, const UVW *d_uvws,
+                                 const JonesF64 *d_beam_jones, JonesF32 *d_vis_fb);
+
 /* Replaces gpu/model.h:40 model_gaussians. */
 const char *model_gaussians(const Gaussians *comps, const Addresses *a, const UVW *d_uvws,
                             const JonesF64 *d_beam_jones, JonesF32 *d_vis_fb);

@@ -85,6 +85,8 @@ class Shapelets(ctypes.Structure):
 # Every symbol include/hdc.h declares, with its argument and result types.
 SIGNATURES = {
     "model_points": (c_char_p, [ctypes.POINTER(Points), ctypes.POINTER(Addresses), c_void_p, c_void_p, c_void_p]),
+    "model_points_noalloc": (c_char_p, [ctypes.POINTER(Points), ctypes.POINTER(Addresses), c_void_p, c_void_p,
+                                        c_void_p]),
     "model_gaussians": (c_char_p, [ctypes.POINTER(Gaussians), ctypes.POINTER(Addresses), c_void_p, c_void_p,
                                    c_void_p]),
     "model_shapelets": (c_char_p, [ctypes.POINTER(Shapelets), ctypes.POINTER(Addresses), c_void_p, c_void_p,

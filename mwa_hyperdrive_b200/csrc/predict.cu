@@ -505,6 +505,65 @@ static const char* dropin_model(int type, const GroupIn g[3], const Addresses* a
     return NULL;
 }
 
+// Bytes of workspace the point-source drop-in path needs for nc components
+// and nf channels (derived LMN and per-channel flux tables).
+size_t points_workspace_bytes(int nc, int nf) {
+    size_t off_flux = align256(sizeof(double4) * (size_t)nc);
+    size_t off_gp = align256(off_flux + sizeof(JonesF64) * (size_t)nf * nc);
+    return align256(off_gp + sizeof(double4) * (size_t)nc);
+}
+
+// The point-source drop-in path over a workspace and kernel error word the
+// caller provides.  Allocates nothing and runs on the legacy default stream.
+const char* points_with_workspace(const Points* comps, const Addresses* a, const UVW* d_uvws,
+                                  const JonesF64* d_beam_jones, JonesF32* d_vis_fb, void* ws, size_t ws_bytes,
+                                  int* err_word) {
+    GroupIn g[3] = {};
+    g[0] = GroupIn{comps->num_power_laws, comps->power_law_lmns, comps->power_law_fds, comps->power_law_sis};
+    g[1] = GroupIn{comps->num_curved_power_laws, comps->curved_power_law_lmns, comps->curved_power_law_fds,
+                   comps->curved_power_law_sis, comps->curved_power_law_qs};
+    g[2] = GroupIn{comps->num_lists, comps->list_lmns, comps->list_fds};
+    const int nc = g[0].n + g[1].n + g[2].n;
+    if (nc == 0) return NULL;
+    const int nf = a->num_freqs, nbl = a->num_baselines;
+    if (points_workspace_bytes(nc, nf) > ws_bytes) return "workspace too small for this many channels x components";
+    char* w = (char*)ws;
+    PrepIn in = {};
+    for (int i = 0; i < 3; i++) in.g[i] = g[i];
+    in.nc = nc;
+    in.nf = nf;
+    in.nbl = nbl;
+    in.type = 0;
+    in.freqs = a->d_freqs;
+    in.lmn = (double4*)w;
+    in.flux = (JonesF64*)(w + align256(sizeof(double4) * (size_t)nc));
+    in.flux_ld = nc;
+    in.gp = (double4*)(w + align256(align256(sizeof(double4) * (size_t)nc) + sizeof(JonesF64) * (size_t)nf * nc));
+    dim3 pg((nc + 127) / 128, nf);
+    dropin_prep_kernel<<<pg, 128>>>(in);
+    count_launches(1);
+    HDC_CUDA_RET_STR(cudaGetLastError());
+    DirectParams p = {};
+    p.nbl = nbl;
+    p.nf = nf;
+    p.ntiles = (int)((1.0 + sqrt(1.0 + 8.0 * nbl)) / 2.0 + 0.5);
+    p.nc = nc;
+    p.freqs = a->d_freqs;
+    p.uvws = d_uvws;
+    p.lmn = in.lmn;
+    p.flux = in.flux;
+    p.gp = in.gp;
+    p.beam = d_beam_jones;
+    p.tile_map = a->d_tile_map;
+    p.unflagged_map = a->d_tile_index_to_unflagged_tile_index_map;
+    p.freq_map = a->d_freq_map;
+    p.n_uniq_freq = a->num_unique_beam_freqs;
+    p.vis = d_vis_fb;
+    p.err = err_word;
+    HDC_CUDA_RET_STR(launch_direct(0, d_beam_jones != nullptr, false, p, 0));
+    return NULL;
+}
+
 }  // namespace hdc
 
 using namespace hdc;
