@@ -46,13 +46,22 @@ def parse():
     ap.add_argument("--form", default="auto", choices=["auto", "direct", "tensor"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
-    return ap.parse_args()
+    ap.add_argument("--channels", type=int, default=384, help="reduced case for profiling (default: full 384)")
+    ap.add_argument("--timesteps", type=int, default=4, help="reduced case for profiling (default: full 4)")
+    ap.add_argument("--skip-e2e", action="store_true")
+    args = ap.parse_args()
+    global SHAPE
+    SHAPE = (args.channels, args.timesteps)
+    return args
+
+
+SHAPE = (384, 4)
 
 
 def workload():
     from mwa_hyperdrive_b200 import synth
 
-    obs, sky = synth.config2()
+    obs, sky = synth.config2(n_freqs=SHAPE[0], n_times=SHAPE[1])
     return obs, sky
 
 
@@ -285,6 +294,8 @@ def gpu_arm(args, rank, world, local_rank):
     value = work * world / (ms_chosen * 1e-3)
 
     # e2e: trait-style host-buffer calls (pinned host memory)
+    if args.skip_e2e:
+        return
     hvis = torch.zeros((nt, nf, nbl, 8), dtype=torch.float32).pin_memory()
     hnp = hvis.numpy()
     for _ in range(max(1, args.warmup)):

@@ -361,6 +361,22 @@ typedef struct HdcCalResult {
     int num_failed;
 } HdcCalResult;
 
+#define HDC_CAL_PLAIN 0 /* stream data and model every iteration */
+
+/* calibrate_timeblock (di_calibrate/mod.rs:387-618): calibrate every
+ * chanblock of one timeblock, then re-calibrate failed chanblocks from
+ * neighbour-interpolated starts until no more converge.  d_data_tfb and
+ * d_model_tfb are [num_timesteps][num_chanblocks][num_baselines] (pre-weighted
+ * as CalVis::scale_by_weights leaves them); the timeblock is timesteps
+ * [timeblock_start, timeblock_end).  d_di_jones is this timeblock's
+ * [tile][chanblock] slice of the solutions (model -> data, not inverted): the
+ * initial guesses in, the solutions out (NaN where failed).  h_results gets
+ * one entry per chanblock.  Up to 256 tiles. */
+int hdc_calibrate_timeblock(const JonesF32 *d_data_tfb, const JonesF32 *d_model_tfb, int num_timesteps,
+                            int timeblock_start, int timeblock_end, int num_chanblocks, int num_baselines,
+                            JonesF64 *d_di_jones, int max_iterations, double stop_threshold, double min_threshold,
+                            int pols, HdcCalResult *h_results, int form, hdcStream_t stream);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

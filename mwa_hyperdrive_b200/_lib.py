@@ -112,6 +112,8 @@ SIGNATURES = {
     "hdc_modeller_model_timestep_with_host": (c_int, [c_void_p, c_double, c_void_p, c_void_p, c_void_p]),
     "hdc_modeller_update_with_a_source": (c_int, [c_void_p, c_void_p, RADec]),
     "hdc_modeller_model_timestep_autos_with": (c_int, [c_void_p, c_double, c_void_p, c_void_p]),
+    "hdc_calibrate_timeblock": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p, c_int,
+                                        c_double, c_double, c_int, ctypes.POINTER(HdcCalResult), c_int, c_void_p]),
     "hdc_kernel_launches": (ctypes.c_longlong, []),
     "hdc_modeller_set_profiling": (c_int, [c_void_p, c_int]),
     "hdc_modeller_profile": (c_int, [c_void_p, c_void_p, c_int]),

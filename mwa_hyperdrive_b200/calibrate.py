@@ -1,0 +1,83 @@
+"""Direction-independent calibration: the host-side mirror of
+mwa_hyperdrive's calibrate_timeblocks / calibrate_timeblock
+(di_calibrate/mod.rs:272-618) over libhdc's GPU solver.
+
+Visibilities are ``[timestep][chanblock][baseline][8]`` float32 (torch CUDA
+tensors for the device entry point, numpy arrays for the host-buffer
+convenience); solutions follow the reference's layout
+``di_jones[timeblock][tile][chanblock][8]`` float64, holding the model->data
+gains (not inverted) with NaN where calibration failed.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from typing import List, Sequence, Tuple
+
+import numpy as np
+
+from . import _lib
+from .model import POLS, _stream_ptr
+
+FORMS = {"plain": 0}
+
+
+@dataclass
+class CalibrationResult:
+    """di_calibrate/mod.rs:620-632"""
+
+    num_iterations: int
+    converged: bool
+    max_precision: float
+    num_failed: int
+    chanblock: int = -1
+
+
+def num_tiles_from_baselines(nbl: int) -> int:
+    n = int(round((1 + (1 + 8 * nbl) ** 0.5) / 2))
+    if n * (n - 1) // 2 != nbl:
+        raise ValueError(f"{nbl} is not a triangular number of baselines")
+    return n
+
+
+def calibrate_timeblock(d_data, d_model, d_di_jones_tc, timeblock: Tuple[int, int], max_iterations: int = 50,
+                        stop_threshold: float = 1e-8, min_threshold: float = 1e-4, pols: str = "XX_XY_YX_YY",
+                        form: str = "plain", stream=None) -> List[CalibrationResult]:
+    """Calibrate one timeblock on the device.  ``d_di_jones_tc`` is a CUDA
+    float64 tensor [tile][chanblock][8] holding the initial guesses; it is
+    overwritten with the solutions."""
+    nt, nch, nbl = int(d_data.shape[0]), int(d_data.shape[1]), int(d_data.shape[2])
+    res = (_lib.HdcCalResult * nch)()
+    rc = _lib.lib().hdc_calibrate_timeblock(d_data.data_ptr(), d_model.data_ptr(), nt, int(timeblock[0]),
+                                            int(timeblock[1]), nch, nbl, d_di_jones_tc.data_ptr(),
+                                            int(max_iterations), float(stop_threshold), float(min_threshold),
+                                            POLS[pols], res, FORMS[form], _stream_ptr(stream))
+    _lib.check(rc, "hdc_calibrate_timeblock")
+    return [CalibrationResult(r.num_iterations, bool(r.converged), r.max_precision, r.num_failed, i)
+            for i, r in enumerate(res)]
+
+
+def calibrate_timeblocks(vis_data_tfb, vis_model_tfb, timeblocks: Sequence[Tuple[int, int]],
+                         max_iterations: int = 50, stop_threshold: float = 1e-8, min_threshold: float = 1e-4,
+                         pols: str = "XX_XY_YX_YY", form: str = "plain"):
+    """calibrate_timeblocks (di_calibrate/mod.rs:272-361).  Accepts host
+    (numpy) or device (torch) visibilities; returns (di_jones
+    [timeblock][tile][chanblock][8] numpy, results [timeblock][chanblock])."""
+    import torch
+
+    host = isinstance(vis_data_tfb, np.ndarray)
+    d_data = torch.from_numpy(np.ascontiguousarray(vis_data_tfb, np.float32)).cuda() if host else vis_data_tfb
+    d_model = torch.from_numpy(np.ascontiguousarray(vis_model_tfb, np.float32)).cuda() if host else vis_model_tfb
+    nt, nch, nbl = d_data.shape[:3]
+    ntiles = num_tiles_from_baselines(int(nbl))
+    out = np.zeros((len(timeblocks), ntiles, nch, 8))
+    results = []
+    for k, tb in enumerate(timeblocks):
+        dj = torch.zeros((ntiles, nch, 8), dtype=torch.float64, device=d_data.device)
+        dj[..., 0] = 1.0
+        dj[..., 6] = 1.0
+        results.append(calibrate_timeblock(d_data, d_model, dj, tb, max_iterations, stop_threshold, min_threshold,
+                                           pols, form))
+        out[k] = dj.cpu().numpy()
+    return out, results

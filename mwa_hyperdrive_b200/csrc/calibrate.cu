@@ -1,0 +1,446 @@
+// Direction-independent calibration (MitchCal / StefCal) for sm_100a:
+// calibrate_timeblock of mwa_hyperdrive (di_calibrate/mod.rs:387-968).
+//
+// Plain form: one CTA per chanblock runs that chanblock's whole iteration
+// loop on the device -- every chanblock converges (or fails) independently,
+// so the grid needs no inter-CTA synchronisation and each CTA keeps its own
+// iteration count, exactly as the reference's rayon loop over chanblocks.
+// Per iteration a CTA streams the chanblock's timeblock of data and model
+// (f32, promoted to f64) once: each thread owns one baseline for all
+// timesteps and forms both tiles' contributions (MitchCal eq. 11,
+// calibration_loop, mod.rs:900-968):
+//     tile1: top += D (G2 M^H),     bot += (G2 M^H)^H (G2 M^H)
+//     tile2: top += D^H (G1 M),     bot += (G1 M)^H (G1 M)
+// in registers; tile1 sums are combined across the warp with a segmented
+// shuffle reduction (consecutive baselines mostly share tile1) and added to
+// shared-memory accumulators, tile2 sums are added with shared-memory
+// atomics.  bot is Hermitian with a real diagonal and is kept as 4 reals.
+// The per-tile update (top bot^-1), the NaN/failed-tile rules, the
+// even-iteration averaging and convergence test and the final failure rules
+// follow calibrate() (mod.rs:640-893) with block-wide votes.
+
+#include <vector>
+
+#include "common.cuh"
+
+namespace hdc {
+
+constexpr int CT = 256;  // threads per CTA; supports up to CT tiles
+
+struct CalParams {
+    const JonesF32* data;  // [nt_total][nchan][nbl]
+    const JonesF32* model;
+    int t0, t1, nchan, nbl, ntiles;
+    JonesF64* di_jones;  // [ntiles][nchan]
+    const int* chan_list;  // chanblocks to calibrate (blockIdx.x -> chanblock)
+    int max_iter;
+    double stop, min_thr;
+    int pols;
+    HdcCalResult* results;  // [nchan]
+};
+
+struct Herm {  // [a b; conj(b) d], a and d real
+    double a, d;
+    cplx b;
+};
+
+__device__ __forceinline__ J2 load_vis(const JonesF32* p) {
+    const float4* q = reinterpret_cast<const float4*>(p);
+    const float4 x = __ldg(q), y = __ldg(q + 1);
+    return J2{{x.x, x.y}, {x.z, x.w}, {y.x, y.y}, {y.z, y.w}};
+}
+
+// Z^H Z for Z = [z0 z1; z2 z3]
+__device__ __forceinline__ void add_zhz(Herm& h, const J2& z) {
+    h.a += z.a.re * z.a.re + z.a.im * z.a.im + z.c.re * z.c.re + z.c.im * z.c.im;
+    h.d += z.b.re * z.b.re + z.b.im * z.b.im + z.d.re * z.d.re + z.d.im * z.d.im;
+    h.b = h.b + conj(z.a) * z.b + conj(z.c) * z.d;
+}
+
+__device__ __forceinline__ double warp_seg_sum(double v, int key, int lane) {
+    // inclusive suffix sum over lanes with the same key; keys are
+    // non-decreasing with lane, so each key is a contiguous run
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const double other = __shfl_down_sync(0xffffffffu, v, o);
+        const int ok = __shfl_down_sync(0xffffffffu, key, o);
+        if (lane + o < 32 && ok == key) v += other;
+    }
+    return v;
+}
+
+__device__ __forceinline__ cplx cdiv(cplx a, cplx b) {
+    const double n = b.re * b.re + b.im * b.im;
+    return {(a.re * b.re + a.im * b.im) / n, (a.im * b.re - a.re * b.im) / n};
+}
+
+// marlu Jones::inv and Jones division (top * bot^-1)
+__device__ __forceinline__ J2 jdiv(const J2& top, const J2& bot, int pols) {
+    if (pols == 1) return J2{cdiv(top.a, bot.a), {0, 0}, {0, 0}, {0, 0}};
+    if (pols == 2) return J2{{0, 0}, {0, 0}, {0, 0}, cdiv(top.d, bot.d)};
+    const cplx det = bot.a * bot.d - bot.b * bot.c;
+    const cplx inv_det = cdiv(cplx{1.0, 0.0}, det);
+    const cplx m = cplx{-inv_det.re, -inv_det.im};
+    const J2 inv = J2{inv_det * bot.d, m * bot.b, m * bot.c, inv_det * bot.a};
+    return top * inv;
+}
+
+__device__ __forceinline__ bool any_nan(const J2& j) {
+    return isnan(j.a.re) || isnan(j.a.im) || isnan(j.b.re) || isnan(j.b.im) || isnan(j.c.re) || isnan(j.c.im) ||
+           isnan(j.d.re) || isnan(j.d.im);
+}
+
+__device__ __forceinline__ double cnorm(cplx a) { return a.re * a.re + a.im * a.im; }
+
+__global__ void __launch_bounds__(CT) mitchcal_kernel(const CalParams P) {
+    extern __shared__ double smem[];
+    const int n = P.ntiles;
+    J2* G = reinterpret_cast<J2*>(smem);          // current gains
+    J2* Gold = G + n;                              // previous gains
+    J2* top = Gold + n;                            // accumulators
+    Herm* bot = reinterpret_cast<Herm*>(top + n);
+    double* prec = reinterpret_cast<double*>(bot + n);  // [n][4]
+    int* failed = reinterpret_cast<int*>(prec + 4 * n);
+
+    const int ch = P.chan_list ? P.chan_list[blockIdx.x] : blockIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int nt = P.t1 - P.t0;
+    const size_t tstride = (size_t)P.nchan * P.nbl;
+    const JonesF32* D0 = P.data + ((size_t)P.t0 * P.nchan + ch) * P.nbl;
+    const JonesF32* M0 = P.model + ((size_t)P.t0 * P.nchan + ch) * P.nbl;
+
+    for (int i = tid; i < n; i += CT) {
+        G[i] = load_j(P.di_jones[(size_t)i * P.nchan + ch]);
+        Gold[i] = jzero();
+        for (int k = 0; k < 4; k++) prec[4 * i + k] = 0.0;
+        failed[i] = 0;
+    }
+    __syncthreads();
+
+    int iteration = 0;
+    while (iteration < P.max_iter) {
+        iteration++;
+        for (int i = tid; i < n; i += CT) {
+            top[i] = jzero();
+            bot[i] = Herm{0.0, 0.0, {0.0, 0.0}};
+        }
+        __syncthreads();
+
+        // ---- accumulate top / bot (calibration_loop) ----
+        const int nwarp_bl = (P.nbl + 31) & ~31;
+        for (int base = tid & ~31; base < nwarp_bl; base += CT) {
+            const int bl = base + lane;
+            const bool active = bl < P.nbl;
+            int p = -1 - lane, q = 0;  // unique keys for inactive lanes
+            J2 t1 = jzero(), t2 = jzero();
+            Herm h1{0, 0, {0, 0}}, h2{0, 0, {0, 0}};
+            if (active) {
+                baseline_to_tiles(bl, n, p, q);
+                const J2 gp = G[p], gq = G[q];
+                for (int t = 0; t < nt; t++) {
+                    const J2 d = load_vis(D0 + t * tstride + bl);
+                    const J2 m = load_vis(M0 + t * tstride + bl);
+                    const J2 z1 = gq * herm(m);
+                    t1 = t1 + d * z1;
+                    add_zhz(h1, z1);
+                    const J2 z2 = gp * m;
+                    t2 = t2 + herm(d) * z2;
+                    add_zhz(h2, z2);
+                }
+            }
+            // tile1 (row) sums: segmented reduction, head lane adds
+            double v[12] = {t1.a.re, t1.a.im, t1.b.re, t1.b.im, t1.c.re, t1.c.im,
+                            t1.d.re, t1.d.im, h1.a,    h1.d,    h1.b.re, h1.b.im};
+#pragma unroll
+            for (int k = 0; k < 12; k++) v[k] = warp_seg_sum(v[k], p, lane);
+            const int prev = __shfl_up_sync(0xffffffffu, p, 1);
+            const bool head = active && (lane == 0 || prev != p);
+            if (head) {
+                double* tp = reinterpret_cast<double*>(&top[p]);
+                for (int k = 0; k < 8; k++) atomicAdd(tp + k, v[k]);
+                atomicAdd(&bot[p].a, v[8]);
+                atomicAdd(&bot[p].d, v[9]);
+                atomicAdd(&bot[p].b.re, v[10]);
+                atomicAdd(&bot[p].b.im, v[11]);
+            }
+            if (active) {
+                double* tq = reinterpret_cast<double*>(&top[q]);
+                atomicAdd(tq + 0, t2.a.re);
+                atomicAdd(tq + 1, t2.a.im);
+                atomicAdd(tq + 2, t2.b.re);
+                atomicAdd(tq + 3, t2.b.im);
+                atomicAdd(tq + 4, t2.c.re);
+                atomicAdd(tq + 5, t2.c.im);
+                atomicAdd(tq + 6, t2.d.re);
+                atomicAdd(tq + 7, t2.d.im);
+                atomicAdd(&bot[q].a, h2.a);
+                atomicAdd(&bot[q].d, h2.d);
+                atomicAdd(&bot[q].b.re, h2.b.re);
+                atomicAdd(&bot[q].b.im, h2.b.im);
+            }
+        }
+        __syncthreads();
+
+        // ---- iteration-1 check: top == bot (and zeros) (mod.rs:701-750) ----
+        if (iteration == 1) {
+            int eq = 1, small = 1;
+            for (int i = tid; i < n; i += CT) {
+                const J2 tp = top[i];
+                const Herm b = bot[i];
+                const J2 bj = J2{{b.a, 0.0}, b.b, conj(b.b), {b.d, 0.0}};
+                const J2 df = tp - bj;
+                const double e[8] = {df.a.re, df.a.im, df.b.re, df.b.im, df.c.re, df.c.im, df.d.re, df.d.im};
+                for (int k = 0; k < 8; k++)
+                    if (fabs(e[k]) > P.stop) eq = 0;
+                const double tv[8] = {tp.a.re, tp.a.im, tp.b.re, tp.b.im, tp.c.re, tp.c.im, tp.d.re, tp.d.im};
+                const double bv[8] = {bj.a.re, bj.a.im, bj.b.re, bj.b.im, bj.c.re, bj.c.im, bj.d.re, bj.d.im};
+                for (int k = 0; k < 8; k++)
+                    if (fabs(tv[k]) > 2.220446049250313e-16 || fabs(bv[k]) > 2.220446049250313e-16) small = 0;
+            }
+            const int all_eq = __syncthreads_and(eq);
+            const int all_small = __syncthreads_and(small);
+            if (all_eq) {
+                if (all_small)
+                    for (int i = tid; i < n; i += CT) failed[i] = 1;
+                __syncthreads();
+                break;
+            }
+        }
+
+        // ---- new gains (mod.rs:753-778) ----
+        for (int i = tid; i < n; i += CT) {
+            if (failed[i]) continue;
+            const Herm b = bot[i];
+            const J2 bj = J2{{b.a, 0.0}, b.b, conj(b.b), {b.d, 0.0}};
+            const J2 div = jdiv(top[i], bj, P.pols);
+            if (any_nan(div)) {
+                failed[i] = 1;
+                G[i] = jzero();
+                Gold[i] = jzero();
+            } else {
+                G[i] = div;
+            }
+        }
+        int my_failed = 0;
+        for (int i = tid; i < n; i += CT) my_failed += failed[i];
+        __shared__ int s_count;
+        if (tid == 0) s_count = 0;
+        __syncthreads();
+        if (my_failed) atomicAdd(&s_count, my_failed);
+        __syncthreads();
+        const int nfail = s_count;
+        if (n - nfail <= 4) break;
+
+        // ---- even iterations: precision, average, convergence (mod.rs:787-840) ----
+        if (iteration % 2 == 0) {
+            int below = 1;
+            for (int i = tid; i < n; i += CT) {
+                if (!failed[i]) {
+                    const J2 g = G[i], o = Gold[i];
+                    const J2 df = g - o;
+                    prec[4 * i + 0] = cnorm(df.a);
+                    prec[4 * i + 1] = cnorm(df.b);
+                    prec[4 * i + 2] = cnorm(df.c);
+                    prec[4 * i + 3] = cnorm(df.d);
+                    G[i] = (g + o) * 0.5;
+                }
+                for (int k = 0; k < 4; k++)
+                    if (!(prec[4 * i + k] < P.stop)) below = 0;
+            }
+            if (__syncthreads_and(below)) break;
+        }
+        for (int i = tid; i < n; i += CT) Gold[i] = G[i];
+        __syncthreads();
+    }
+    __syncthreads();
+
+    // ---- finalise (mod.rs:843-893) ----
+    __shared__ double s_max[CT / 32];
+    __shared__ int s_nfail;
+    if (tid == 0) s_nfail = 0;
+    __syncthreads();
+    double mx = -1.7976931348623157e308;  // f64::MIN
+    int nf_local = 0;
+    for (int i = tid; i < n; i += CT) {
+        if (failed[i]) {
+            nf_local++;
+            continue;
+        }
+        for (int k = 3; k >= 0; k--) mx = fmax(mx, prec[4 * i + k]);  // fmax ignores NaN like f64::max
+    }
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (lane == 0) s_max[tid >> 5] = mx;
+    if (nf_local) atomicAdd(&s_nfail, nf_local);
+    __syncthreads();
+    double max_precision = s_max[0];
+    for (int w = 1; w < CT / 32; w++) max_precision = fmax(max_precision, s_max[w]);
+    const int num_failed = s_nfail;
+    const bool converged = !(n - num_failed <= 4 || max_precision > P.min_thr);
+    const double qnan = __longlong_as_double(0x7ff8000000000000ll);
+    for (int i = tid; i < n; i += CT) {
+        JonesF64 out;
+        if (!converged || failed[i])
+            out = JonesF64{qnan, qnan, qnan, qnan, qnan, qnan, qnan, qnan};
+        else
+            out = store_j(G[i]);
+        P.di_jones[(size_t)i * P.nchan + ch] = out;
+    }
+    if (tid == 0) P.results[ch] = HdcCalResult{iteration, converged ? 1 : 0, max_precision, num_failed};
+}
+
+// Seed failed chanblocks from converged neighbours (mod.rs:473-520):
+// pairs (l, r) with l = -1 for a leading run of failures.
+__global__ void retry_seed_kernel(JonesF64* dj, int nchan, int ntiles, const int2* pairs, int npairs) {
+    const int tile = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tile >= ntiles) return;
+    for (int k = 0; k < npairs; k++) {
+        const int l = pairs[k].x, r = pairs[k].y;
+        const J2 rs = load_j(dj[(size_t)tile * nchan + r]);
+        if (l >= 0) {
+            const J2 ls = load_j(dj[(size_t)tile * nchan + l]);
+            for (int i = l + 1; i < r; i++) {
+                const double lw = (double)(r - i), rw = (double)(i - l), d = (double)(r - l);
+                const J2 s = ls * lw + rs * rw;
+                dj[(size_t)tile * nchan + i] =
+                    JonesF64{s.a.re / d, s.a.im / d, s.b.re / d, s.b.im / d, s.c.re / d, s.c.im / d, s.d.re / d, s.d.im / d};
+            }
+        } else {
+            for (int i = 0; i < r; i++) dj[(size_t)tile * nchan + i] = store_j(rs);
+        }
+    }
+}
+
+static size_t smem_bytes(int n) { return (size_t)n * (3 * sizeof(J2) + sizeof(Herm) + 4 * sizeof(double) + sizeof(int)); }
+
+static int launch_mitchcal(const CalParams& P, int nblocks, cudaStream_t s) {
+    const size_t sm = smem_bytes(P.ntiles);
+    HDC_CUDA_RET_INT(cudaFuncSetAttribute(mitchcal_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    mitchcal_kernel<<<nblocks, CT, sm, s>>>(P);
+    count_launches(1);
+    HDC_CUDA_RET_INT(cudaGetLastError());
+    return HDC_OK;
+}
+
+}  // namespace hdc
+
+using namespace hdc;
+
+extern "C" int hdc_calibrate_timeblock(const JonesF32* d_data_tfb, const JonesF32* d_model_tfb, int num_timesteps,
+                                       int timeblock_start, int timeblock_end, int num_chanblocks, int num_baselines,
+                                       JonesF64* d_di_jones, int max_iterations, double stop_threshold,
+                                       double min_threshold, int pols, HdcCalResult* h_results, int form,
+                                       hdcStream_t stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    const int ntiles = (int)((1.0 + std::sqrt(1.0 + 8.0 * num_baselines)) / 2.0 + 0.5);
+    if (ntiles * (ntiles - 1) / 2 != num_baselines || ntiles > CT || num_chanblocks <= 0 ||
+        timeblock_start < 0 || timeblock_end > num_timesteps || timeblock_start >= timeblock_end || !h_results ||
+        pols < 0 || pols > 4) {
+        set_error("hdc_calibrate_timeblock: invalid arguments (baselines %d -> %d tiles, max %d)", num_baselines,
+                  ntiles, CT);
+        return HDC_ERR_ARG;
+    }
+    if (form != 0) {
+        set_error("hdc_calibrate_timeblock: unknown form %d", form);
+        return HDC_ERR_ARG;
+    }
+    HdcCalResult* d_res = nullptr;
+    int* d_list = nullptr;
+    int2* d_pairs = nullptr;
+    int rc = HDC_OK;
+    auto cleanup = [&]() {
+        if (d_res) cudaFree(d_res);
+        if (d_list) cudaFree(d_list);
+        if (d_pairs) cudaFree(d_pairs);
+    };
+    if (cudaMalloc(&d_res, sizeof(HdcCalResult) * num_chanblocks) != cudaSuccess ||
+        cudaMalloc(&d_list, sizeof(int) * num_chanblocks) != cudaSuccess ||
+        cudaMalloc(&d_pairs, sizeof(int2) * (num_chanblocks + 1)) != cudaSuccess) {
+        cudaGetLastError();
+        cleanup();
+        set_error("hdc_calibrate_timeblock: device allocation failed");
+        return HDC_ERR_ALLOC;
+    }
+    CalParams P;
+    P.data = d_data_tfb;
+    P.model = d_model_tfb;
+    P.t0 = timeblock_start;
+    P.t1 = timeblock_end;
+    P.nchan = num_chanblocks;
+    P.nbl = num_baselines;
+    P.ntiles = ntiles;
+    P.di_jones = d_di_jones;
+    P.chan_list = nullptr;
+    P.max_iter = max_iterations;
+    P.stop = stop_threshold;
+    P.min_thr = min_threshold;
+    P.pols = pols;
+    P.results = d_res;
+    rc = launch_mitchcal(P, num_chanblocks, s);
+    if (rc) {
+        cleanup();
+        return rc;
+    }
+    std::vector<HdcCalResult> res(num_chanblocks);
+    if (cudaMemcpyAsync(res.data(), d_res, sizeof(HdcCalResult) * num_chanblocks, cudaMemcpyDeviceToHost, s) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+        cleanup();
+        set_error("hdc_calibrate_timeblock: %s", cudaGetErrorString(cudaGetLastError()));
+        return HDC_ERR_CUDA;
+    }
+    // Retry failed chanblocks from interpolated neighbours (mod.rs:468-614).
+    int total = 0;
+    for (auto& r : res) total += r.converged;
+    if (total > 0 && total != num_chanblocks) {
+        int new_conv = 1;
+        while (new_conv > 0 && total != num_chanblocks) {
+            std::vector<int2> pairs;
+            int left = -1;
+            bool in_fail = false;
+            for (int c = 0; c < num_chanblocks; c++) {
+                const bool conv = res[c].converged != 0;
+                if (!in_fail && conv)
+                    left = c;
+                else if (!in_fail && !conv)
+                    in_fail = true;
+                else if (in_fail && conv) {
+                    in_fail = false;
+                    pairs.push_back(make_int2(left, c));
+                    left = c;
+                }
+            }
+            std::vector<int> list;
+            for (int c = 0; c < num_chanblocks; c++)
+                if (!res[c].converged) list.push_back(c);
+            if (!pairs.empty()) {
+                cudaMemcpyAsync(d_pairs, pairs.data(), sizeof(int2) * pairs.size(), cudaMemcpyHostToDevice, s);
+                retry_seed_kernel<<<(ntiles + 127) / 128, 128, 0, s>>>(d_di_jones, num_chanblocks, ntiles, d_pairs,
+                                                                        (int)pairs.size());
+                count_launches(1);
+            }
+            cudaMemcpyAsync(d_list, list.data(), sizeof(int) * list.size(), cudaMemcpyHostToDevice, s);
+            P.chan_list = d_list;
+            rc = launch_mitchcal(P, (int)list.size(), s);
+            if (rc) {
+                cleanup();
+                return rc;
+            }
+            if (cudaMemcpyAsync(res.data(), d_res, sizeof(HdcCalResult) * num_chanblocks, cudaMemcpyDeviceToHost,
+                                s) != cudaSuccess ||
+                cudaStreamSynchronize(s) != cudaSuccess) {
+                cleanup();
+                set_error("hdc_calibrate_timeblock: %s", cudaGetErrorString(cudaGetLastError()));
+                return HDC_ERR_CUDA;
+            }
+            for (int c : list)
+                if (std::fabs(res[c].max_precision) > 1e100) res[c].max_precision = NAN;
+            int tmp = 0;
+            for (auto& r : res) tmp += r.converged;
+            new_conv = tmp - total;
+            total = tmp;
+        }
+    }
+    for (int c = 0; c < num_chanblocks; c++) h_results[c] = res[c];
+    cleanup();
+    return HDC_OK;
+}

@@ -128,3 +128,74 @@ def config2(n_points=4000, n_gauss=500, n_shapelets=100, n_freqs=384, n_times=4)
     comps = point_sky(n_points, pc, 10.0, 2, curved_q_sigma=0.2)
     comps += gaussians_and_shapelets(n_gauss, n_shapelets, pc, 22)
     return obs, sl.SkyModelArrays.from_components(comps)
+
+
+def truth_gains(ntiles: int, nch: int, rng, amp_sigma=0.1, leak_sigma=0.01, phase_slope=None, freqs=None):
+    """Per (tile, chanblock) Jones gains: diagonal amplitude N(1, amp_sigma),
+    phase U(-pi, pi) (or a per-tile linear phase in frequency when
+    phase_slope [rad/Hz] and freqs are given), complex off-diagonal leakage
+    N(0, leak_sigma).  Returns [tile][chanblock][8] float64."""
+    g = np.zeros((ntiles, nch, 8))
+    amp = rng.normal(1.0, amp_sigma, (ntiles, 2))
+    if phase_slope is not None:
+        ph0 = rng.uniform(-np.pi, np.pi, (ntiles, 2))
+        slope = rng.uniform(-phase_slope, phase_slope, (ntiles, 2))
+        ph = ph0[:, None, :] + slope[:, None, :] * (np.asarray(freqs)[None, :, None] - freqs[0])
+    else:
+        ph = np.broadcast_to(rng.uniform(-np.pi, np.pi, (ntiles, 1, 2)), (ntiles, nch, 2))
+    g[..., 0] = amp[:, None, 0] * np.cos(ph[..., 0])
+    g[..., 1] = amp[:, None, 0] * np.sin(ph[..., 0])
+    g[..., 6] = amp[:, None, 1] * np.cos(ph[..., 1])
+    g[..., 7] = amp[:, None, 1] * np.sin(ph[..., 1])
+    g[..., 2:6] = rng.normal(0.0, leak_sigma, (ntiles, nch, 4))
+    return g
+
+
+def _jmul(a, b):
+    """Batched 2x2 complex products of [...][8] arrays."""
+    ac = a[..., 0::2] + 1j * a[..., 1::2]
+    bc = b[..., 0::2] + 1j * b[..., 1::2]
+    r = np.empty_like(ac)
+    r[..., 0] = ac[..., 0] * bc[..., 0] + ac[..., 1] * bc[..., 2]
+    r[..., 1] = ac[..., 0] * bc[..., 1] + ac[..., 1] * bc[..., 3]
+    r[..., 2] = ac[..., 2] * bc[..., 0] + ac[..., 3] * bc[..., 2]
+    r[..., 3] = ac[..., 2] * bc[..., 1] + ac[..., 3] * bc[..., 3]
+    out = np.empty(a.shape[:-1] + (8,))
+    out[..., 0::2] = r.real
+    out[..., 1::2] = r.imag
+    return out
+
+
+def _jh(a):
+    out = a.copy()
+    out[..., 2:4], out[..., 4:6] = a[..., 4:6].copy(), a[..., 2:4].copy()
+    out[..., 1::2] *= -1
+    return out
+
+
+def corrupt(model_tfb, gains_tc, rng=None, snr=None):
+    """data = G_p M G_q^H (+ complex Gaussian noise at per-visibility SNR)."""
+    nt, nch, nbl = model_tfb.shape[:3]
+    ntiles = gains_tc.shape[0]
+    i, j = np.triu_indices(ntiles, 1)
+    gp = gains_tc[i].transpose(1, 0, 2)[None]  # [1][ch][bl][8]
+    gq = gains_tc[j].transpose(1, 0, 2)[None]
+    d = _jmul(_jmul(np.broadcast_to(gp, model_tfb.shape), model_tfb.astype(np.float64)),
+              _jh(np.broadcast_to(gq, model_tfb.shape)))
+    if snr is not None:
+        rms = np.sqrt(np.mean(d[..., [0, 1, 6, 7]] ** 2))
+        d = d + rng.normal(0.0, rms / snr / np.sqrt(2.0), d.shape)
+    return d.astype(np.float32)
+
+
+def random_model(nt, nch, nbl, rng):
+    """A random, Stokes-I dominated model [t][chanblock][bl][8]."""
+    m = np.zeros((nt, nch, nbl, 8))
+    amp = rng.lognormal(0.0, 0.5, (nt, nch, nbl))
+    ph = rng.uniform(-np.pi, np.pi, (nt, nch, nbl))
+    m[..., 0] = amp * np.cos(ph)
+    m[..., 1] = amp * np.sin(ph)
+    m[..., 6] = m[..., 0] * 0.95
+    m[..., 7] = m[..., 1] * 0.95
+    m[..., 2:6] = rng.normal(0.0, 0.02, (nt, nch, nbl, 4)) * amp[..., None]
+    return m.astype(np.float32)
