@@ -1,0 +1,119 @@
+"""Tensor-core factored point predict (tcgen05) against the FP64 oracle.
+
+Error metric (relative visibility error): normwise ||V - V_ref||_F / ||V_ref||_F
+and the 99.9th percentile of |dV| / rms|V_ref| per visibility element.  The
+bound is 1e-6 for both (the fp16 hi/lo split represents the FP64 phasors and
+weights to ~2^-24; accumulation is FP32)."""
+
+import math
+
+import numpy as np
+import pytest
+
+from mwa_hyperdrive_b200 import srclist as sl
+from mwa_hyperdrive_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("no CUDA device", allow_module_level=True)
+
+from mwa_hyperdrive_b200.model import SkyModeller  # noqa: E402
+
+TOL = 1e-6
+
+
+def errors(got, ref):
+    got = np.asarray(got, np.float64)
+    ref = np.asarray(ref, np.float64)
+    norm = np.linalg.norm(ref)
+    rms = norm / math.sqrt(ref.size)
+    d = np.abs(got - ref)
+    return np.linalg.norm(got - ref) / norm, np.percentile(d, 99.9) / rms, d.max() / rms
+
+
+def run(sky, obs, lst, form, beam="none", f64=True):
+    m = SkyModeller(sky, obs.tile_xyzs, obs.freqs, obs.phase_centre, obs.latitude, beam=beam, form=form)
+    vis = torch.zeros((obs.freqs.size, obs.num_baselines, 8), dtype=torch.float64 if f64 else torch.float32,
+                      device="cuda")
+    m.model_timestep_with(lst, vis)
+    torch.cuda.synchronize()
+    return vis.cpu().numpy()
+
+
+def polarised_points(n, centre, seed):
+    rng = np.random.default_rng(seed)
+    pos = synth.cap_positions(n, centre, math.radians(8.0), rng)
+    comps = []
+    for k in range(n):
+        i = float(rng.lognormal(0.0, 1.0))
+        fd = sl.FluxDensity(150e6, i, 0.1 * i * rng.normal(), 0.1 * i * rng.normal(), 0.05 * i * rng.normal())
+        ft = [sl.PowerLaw(float(rng.normal(-0.8, 0.2)), fd),
+              sl.CurvedPowerLaw(float(rng.normal(-0.8, 0.2)), fd, float(rng.normal(0, 0.2))),
+              sl.FluxList([sl.FluxDensity(140e6, 2.0 * i), sl.FluxDensity(210e6, i)])][k % 3]
+        comps.append(sl.SourceComponent(float(pos[k, 0]), float(pos[k, 1]), sl.Point(), ft))
+    return sl.SkyModelArrays.from_components(comps)
+
+
+def test_config1_tensor_vs_fp64_oracle(oracle):
+    obs, sky = synth.config1()
+    got = run(sky, obs, obs.lsts[0], "tensor")
+    ref, _ = oracle.model_timestep(sky, obs.tile_xyzs, obs.freqs, obs.phase_centre, obs.lsts[0], obs.latitude,
+                                   out_f64=True)
+    nrm, p999, mx = errors(got, ref)
+    print(f"config1 tensor: normwise {nrm:.2e}, p99.9 {p999:.2e}, max {mx:.2e}")
+    assert nrm < TOL and p999 < TOL, (nrm, p999, mx)
+
+
+@pytest.mark.parametrize("ntiles,npts,nf,beam", [(128, 1000, 6, "analytic"), (57, 77, 5, "none"), (2, 33, 3, "none"),
+                                                 (128, 31, 4, "analytic")])
+def test_polarised_sky_all_correlations(oracle, ntiles, npts, nf, beam):
+    pc = (0.4, math.radians(-25.0))
+    obs = synth.Obs(synth.tiles_in_disk(ntiles, 1000.0, ntiles), 160e6 + np.arange(nf) * 2.56e6, pc,
+                    np.array([0.42]))
+    sky = polarised_points(npts, pc, npts)
+    got = run(sky, obs, obs.lsts[0], "tensor", beam=beam)
+    b = oracle.beam_struct(1 if beam == "analytic" else 0)
+    ref, _ = oracle.model_timestep(sky, obs.tile_xyzs, obs.freqs, pc, obs.lsts[0], obs.latitude, beam=b,
+                                   out_f64=True)
+    nrm, p999, mx = errors(got, ref)
+    print(f"{ntiles} tiles {npts} comps: normwise {nrm:.2e}, p99.9 {p999:.2e}, max {mx:.2e}")
+    assert nrm < TOL and p999 < TOL, (nrm, p999, mx)
+    # each correlation separately (XY / YX come from the conjugate transpose)
+    for k in range(4):
+        r = ref[..., 2 * k:2 * k + 2]
+        if np.linalg.norm(r) > 0:
+            assert np.linalg.norm(got[..., 2 * k:2 * k + 2] - r) / np.linalg.norm(r) < 10 * TOL
+
+
+def test_mixed_types_tensor_form_keeps_direct_gaussians_and_shapelets(oracle):
+    obs, sky = synth.config2(n_points=300, n_gauss=20, n_shapelets=5, n_freqs=4, n_times=1)
+    got = run(sky, obs, obs.lsts[0], "tensor", beam="analytic")
+    ref, _ = oracle.model_timestep(sky, obs.tile_xyzs, obs.freqs, obs.phase_centre, obs.lsts[0], obs.latitude,
+                                   beam=oracle.beam_struct(1), out_f64=True)
+    nrm, p999, mx = errors(got, ref)
+    assert nrm < TOL and p999 < TOL, (nrm, p999, mx)
+
+
+def test_f32_output_and_accumulate(oracle):
+    obs, sky = synth.config1()
+    obs.freqs = obs.freqs[:3]
+    m = SkyModeller(sky, obs.tile_xyzs, obs.freqs, obs.phase_centre, obs.latitude, form="tensor")
+    vis = torch.ones((3, obs.num_baselines, 8), dtype=torch.float32, device="cuda")
+    m.model_timestep_with(obs.lsts[0], vis)
+    torch.cuda.synchronize()
+    ref, _ = oracle.model_timestep(sky, obs.tile_xyzs, obs.freqs, obs.phase_centre, obs.lsts[0], obs.latitude,
+                                   out_f64=True)
+    nrm, p999, _ = errors(vis.cpu().numpy() - 1.0, ref)
+    assert nrm < 5e-6  # f32 output rounding dominates
+
+
+def test_unsupported_tile_count_is_refused():
+    from mwa_hyperdrive_b200 import _lib
+
+    pc = (0.0, -0.5)
+    obs = synth.Obs(synth.tiles_in_disk(130, 1000.0, 1), np.array([150e6]), pc, np.array([0.0]))
+    sky = polarised_points(3, pc, 1)
+    with pytest.raises(_lib.HdcError):
+        SkyModeller(sky, obs.tile_xyzs, obs.freqs, pc, obs.latitude, form="tensor")
