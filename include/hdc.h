@@ -377,6 +377,33 @@ int hdc_calibrate_timeblock(const JonesF32 *d_data_tfb, const JonesF32 *d_model_
                             JonesF64 *d_di_jones, int max_iterations, double stop_threshold, double min_threshold,
                             int pols, HdcCalResult *h_results, int form, hdcStream_t stream);
 
+/* Peel loop controls (PeelLoopParams and PeelWeightParams' consumers,
+ * params/peel/mod.rs:207-224).  num_passes is the number of passes over all
+ * sources, num_loops the iono-fit iterations per source.  (The reference's
+ * peel_gpu destructures PeelLoopParams::get() with the two swapped,
+ * gpu.rs:41; pass them swapped to reproduce that.) */
+typedef struct HdcPeelParams {
+    int num_passes;
+    int num_loops;
+    double convergence;
+    int freq_average_factor; /* high-res channels per low-res channel */
+    int beam_kind;           /* HDC_BEAM_* for the per-source models */
+    double array_latitude_rad;
+} HdcPeelParams;
+
+/* peel_gpu (params/peel/gpu.rs:25-757): peel num_sources sources from the
+ * residual visibilities d_resid_tfb [t][f][bl] (in place, phase centre
+ * `phase_centre`), weights d_weights_tfb [t][f][bl] (>= 0).  Source i is
+ * h_sources[i] (its components) at weighted position h_source_positions[i];
+ * h_iono_consts[i] holds its (alpha, beta, gain), read and updated.  Low-res
+ * channel wavelengths use the mean frequency of each channel group; the
+ * low-res UVWs use average_lmst (the timeblock's median LMST). */
+int hdc_peel_timeblock(JonesF32 *d_resid_tfb, const float *d_weights_tfb, int num_timesteps, int num_freqs,
+                       const double *h_freqs, const XYZ *h_tile_xyzs, int num_tiles, const double *h_lmsts,
+                       double average_lmst, RADec phase_centre, int num_sources, const HdcSkyModel *h_sources,
+                       const RADec *h_source_positions, IonoConsts *h_iono_consts, const HdcPeelParams *params,
+                       hdcStream_t stream);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

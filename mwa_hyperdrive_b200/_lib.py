@@ -35,6 +35,11 @@ class IonoConsts(ctypes.Structure):
     _fields_ = [("alpha", c_double), ("beta", c_double), ("gain", c_double)]
 
 
+class HdcPeelParams(ctypes.Structure):
+    _fields_ = [("num_passes", c_int), ("num_loops", c_int), ("convergence", c_double),
+                ("freq_average_factor", c_int), ("beam_kind", c_int), ("array_latitude_rad", c_double)]
+
+
 class HdcCalResult(ctypes.Structure):
     _fields_ = [("num_iterations", c_int), ("converged", c_int), ("max_precision", c_double), ("num_failed", c_int)]
 
@@ -114,6 +119,8 @@ SIGNATURES = {
     "hdc_modeller_model_timestep_autos_with": (c_int, [c_void_p, c_double, c_void_p, c_void_p]),
     "hdc_calibrate_timeblock": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p, c_int,
                                         c_double, c_double, c_int, ctypes.POINTER(HdcCalResult), c_int, c_void_p]),
+    "hdc_peel_timeblock": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p, c_int, c_void_p, c_double,
+                                   RADec, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "hdc_kernel_launches": (ctypes.c_longlong, []),
     "hdc_modeller_set_profiling": (c_int, [c_void_p, c_int]),
     "hdc_modeller_profile": (c_int, [c_void_p, c_void_p, c_int]),

@@ -446,6 +446,18 @@ int Modeller::model(double lst, void* d_vis, bool out64, UVW* h_uvws, cudaStream
     return HDC_OK;
 }
 
+int Modeller::model_uvws(double lst, const UVW* d_uvws_ext, JonesF32* d_vis, cudaStream_t s) {
+    int rc = geometry(lst, s);
+    if (rc) return rc;
+    for (int ty = 0; ty < 3; ty++) {
+        if (t[ty].nc == 0) continue;
+        DirectParams p = direct_params(ty, d_vis);
+        p.uvws = d_uvws_ext;
+        HDC_CUDA_RET_INT(launch_direct(ty, false, false, p, s));
+    }
+    return HDC_OK;
+}
+
 int Modeller::autos(double lst, JonesF32* d_vis, cudaStream_t s) {
     int rc = geometry(lst, s);
     if (rc) return rc;

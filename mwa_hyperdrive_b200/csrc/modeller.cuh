@@ -58,6 +58,10 @@ struct Modeller {
     const JonesF64* weights(int ty) const;
     DirectParams direct_params(int ty, void* vis) const;
     int model(double lst, void* d_vis, bool out64, UVW* h_uvws, cudaStream_t s);
+    // model_timestep_with over baseline UVWs the caller computed (as the
+    // reference's peel loop passes its own d_uvws, model/gpu.rs:1152-1166);
+    // direct FP64 kernels, JonesF32 output.
+    int model_uvws(double lst, const UVW* d_uvws_ext, JonesF32* d_vis, cudaStream_t s);
     int autos(double lst, JonesF32* d_vis, cudaStream_t s);
     int tensor_setup();
     int tensor_points(double lst, void* d_vis, bool out64, cudaStream_t s);

@@ -279,6 +279,74 @@ const char* iono_loop_on(const JonesF32* d_resid, const float* d_w, const JonesF
     return NULL;
 }
 
+
+// Stream-aware launchers (the drop-in entry points below use stream 0).
+cudaError_t k_xyzs_to_uvws(const XYZ* xyzs, const double* lmsts, UVW* uvws, RADec pc, int ntiles, int nbl, int nt,
+                           cudaStream_t s) {
+    const size_t n = (size_t)nbl * nt;
+    if (n == 0) return cudaSuccess;
+    xyzs_to_uvws_kernel<<<grid1(n), PT, 0, s>>>(xyzs, lmsts, uvws, pc, ntiles, nbl, nt);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t k_rotate(JonesF32* vis, int nt, int nbl, int nf, const UVW* from, const UVW* to, const double* lambdas,
+                     cudaStream_t s) {
+    const size_t n = (size_t)nt * nf * nbl;
+    if (n == 0) return cudaSuccess;
+    rotate_kernel<<<grid1(n), PT, 0, s>>>(vis, nt, nbl, nf, from, to, lambdas);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t k_average(const JonesF32* hi, const float* w, JonesF32* lo, int nt, int nbl, int nf, int favg,
+                      cudaStream_t s) {
+    const size_t n = (size_t)(nf / favg) * nbl;
+    if (n == 0) return cudaSuccess;
+    average_kernel<<<grid1(n), PT, 0, s>>>(hi, w, lo, nt, nbl, nf, favg);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t k_subtract_iono(JonesF32* resid, const JonesF32* model, IonoConsts c, IonoConsts old, const UVW* uvws,
+                            const double* lambdas, int nt, int nbl, int nf, cudaStream_t s) {
+    const size_t n = (size_t)nt * nf * nbl;
+    if (n == 0) return cudaSuccess;
+    subtract_iono_kernel<<<grid1(n), PT, 0, s>>>(resid, model, c, old, uvws, lambdas, nt, nbl, nf);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t k_add_model(JonesF32* resid, const JonesF32* model, IonoConsts c, const double* lambdas, const UVW* uvws,
+                        int nt, int nf, int nbl, cudaStream_t s) {
+    const size_t n = (size_t)nt * nf * nbl;
+    if (n == 0) return cudaSuccess;
+    add_model_kernel<<<grid1(n), PT, 0, s>>>(resid, model, c, lambdas, uvws, nt, nf, nbl);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+// Low-resolution weights: sum over all timesteps and each channel group,
+// clamped at 0 (params/peel/mod.rs:709-755 weights_average).
+__global__ void weights_average_kernel(const float* w, float* lo, int nt, int nbl, int nf, int favg) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nlo = nf / favg;
+    if (i >= nlo * nbl) return;
+    const int bl = i % nbl, flo = i / nbl;
+    double sum = 0.0;
+    for (int t = 0; t < nt; t++)
+        for (int fc = flo * favg; fc < flo * favg + favg; fc++) sum += (double)w[((size_t)t * nf + fc) * nbl + bl];
+    lo[i] = fmaxf((float)sum, 0.0f);
+}
+
+cudaError_t k_weights_average(const float* w, float* lo, int nt, int nbl, int nf, int favg, cudaStream_t s) {
+    const size_t n = (size_t)(nf / favg) * nbl;
+    if (n == 0) return cudaSuccess;
+    weights_average_kernel<<<grid1(n), PT, 0, s>>>(w, lo, nt, nbl, nf, favg);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
 }  // namespace hdc
 
 using namespace hdc;

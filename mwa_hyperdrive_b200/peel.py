@@ -1,0 +1,83 @@
+"""Peeling: the host-side mirror of mwa_hyperdrive's peel loop
+(params/peel/gpu.rs:25-757 peel_gpu; params/peel/mod.rs:207-224
+PeelLoopParams) over libhdc's native peel.
+
+Residual visibilities are ``[timestep][channel][baseline][8]`` float32
+(CUDA tensor, peeled in place); weights ``[t][f][bl]`` float32 (>= 0).
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from typing import List, Sequence, Tuple
+
+import numpy as np
+
+from . import _lib
+from .model import BEAMS, _as_sky, _stream_ptr
+
+
+@dataclass
+class IonoConsts:
+    """params/peel/mod.rs:56-70 (alpha, beta scale lambda^2; gain)."""
+
+    alpha: float = 0.0
+    beta: float = 0.0
+    gain: float = 1.0
+
+
+@dataclass
+class PeelLoopParams:
+    """params/peel/mod.rs:207-224."""
+
+    num_passes: int = 3
+    num_loops: int = 10
+    convergence: float = 1.0
+
+    def get(self) -> Tuple[int, int, float]:
+        return self.num_passes, self.num_loops, self.convergence
+
+
+def peel_timeblock(d_resid_tfb, d_weights_tfb, freqs, tile_xyzs, lmsts, average_lmst, phase_centre, sources,
+                   source_positions, iono_consts: Sequence[IonoConsts], num_passes: int, num_loops: int,
+                   convergence: float, freq_average_factor: int, array_latitude_rad: float, beam: str = "none",
+                   stream=None) -> List[IonoConsts]:
+    """Peel ``sources`` (a list of SourceList / Source / SkyModelArrays, one per
+    source) with explicit pass and loop counts."""
+    nt, nf, nbl = (int(x) for x in d_resid_tfb.shape[:3])
+    freqs = np.ascontiguousarray(freqs, np.float64)
+    xyzs = np.ascontiguousarray(tile_xyzs, np.float64).reshape(-1, 3)
+    lmsts = np.ascontiguousarray(lmsts, np.float64)
+    skies = [_as_sky(s) for s in sources]
+    n = len(skies)
+    from .srclist import HdcSkyModel
+
+    structs = (HdcSkyModel * max(n, 1))()
+    for i, sk in enumerate(skies):
+        structs[i] = sk.struct()
+    pos = (_lib.RADec * max(n, 1))(*[_lib.RADec(*p) for p in source_positions])
+    consts = (_lib.IonoConsts * max(n, 1))(*[_lib.IonoConsts(c.alpha, c.beta, c.gain) for c in iono_consts])
+    params = _lib.HdcPeelParams(int(num_passes), int(num_loops), float(convergence), int(freq_average_factor),
+                                BEAMS[beam], float(array_latitude_rad))
+    rc = _lib.lib().hdc_peel_timeblock(d_resid_tfb.data_ptr(), d_weights_tfb.data_ptr(), nt, nf, freqs.ctypes.data,
+                                       xyzs.ctypes.data, xyzs.shape[0], lmsts.ctypes.data, float(average_lmst),
+                                       _lib.RADec(*phase_centre), n, ctypes.addressof(structs), ctypes.addressof(pos),
+                                       ctypes.addressof(consts), ctypes.byref(params), _stream_ptr(stream))
+    _lib.check(rc, "hdc_peel_timeblock")
+    return [IonoConsts(consts[i].alpha, consts[i].beta, consts[i].gain) for i in range(n)]
+
+
+def peel_gpu(d_resid_tfb, d_weights_tfb, freqs, tile_xyzs, lmsts, average_lmst, phase_centre, sources,
+             source_positions, iono_consts, peel_loop_params: PeelLoopParams, freq_average_factor: int,
+             array_latitude_rad: float, beam: str = "none", stream=None) -> List[IonoConsts]:
+    """peel_gpu as the reference calls it: it destructures
+    PeelLoopParams::get() as (num_loops, num_passes, convergence)
+    (params/peel/gpu.rs:41) although get() returns (passes, loops, conv), so
+    the configured pass count becomes the iono-loop count and vice versa.
+    This wrapper reproduces that behaviour; call peel_timeblock for the
+    intended meaning."""
+    num_loops, num_passes, convergence = peel_loop_params.get()
+    return peel_timeblock(d_resid_tfb, d_weights_tfb, freqs, tile_xyzs, lmsts, average_lmst, phase_centre, sources,
+                          source_positions, iono_consts, num_passes, num_loops, convergence, freq_average_factor,
+                          array_latitude_rad, beam, stream)
