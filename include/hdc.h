@@ -377,6 +377,36 @@ int hdc_calibrate_timeblock(const JonesF32 *d_data_tfb, const JonesF32 *d_model_
                             JonesF64 *d_di_jones, int max_iterations, double stop_threshold, double min_threshold,
                             int pols, HdcCalResult *h_results, int form, hdcStream_t stream);
 
+/* Per-chanblock calibration residual sum_{t,bl} ||D - G_p M G_q^H||_F^2 for
+ * the gains d_di_jones [tile][chanblock] over timesteps
+ * [timeblock_start, timeblock_end); h_residuals [num_chanblocks].  Used to
+ * judge a proposed starting point for the solver against identity. */
+int hdc_calibration_residuals(const JonesF32 *d_data_tfb, const JonesF32 *d_model_tfb, int num_timesteps,
+                              int timeblock_start, int timeblock_end, int num_chanblocks, int num_baselines,
+                              const JonesF64 *d_di_jones, double *h_residuals, hdcStream_t stream);
+
+/* Learned warm start (no counterpart in the reference): a multilayer
+ * perceptron trained and evaluated by this library's own FP32 kernels.
+ * dims[0..num_layers] are the layer widths; hidden layers use ReLU, the
+ * output layer is linear; if residual_offset >= 0 the output adds the input
+ * slice starting there (width dims[num_layers]).  Parameters are laid out
+ * per layer as W [out][in] then b [out]. */
+typedef struct HdcMlp HdcMlp;
+int hdc_mlp_new(int num_layers, const int *dims, int residual_offset, unsigned long long seed, HdcMlp **out);
+void hdc_mlp_free(HdcMlp *m);
+long long hdc_mlp_num_params(HdcMlp *m);
+int hdc_mlp_get_params(HdcMlp *m, float *h_out);
+int hdc_mlp_set_params(HdcMlp *m, const float *h_in);
+/* d_x [batch][dims[0]] -> d_y [batch][dims[num_layers]] (device pointers) */
+int hdc_mlp_forward(HdcMlp *m, const float *d_x, int batch, float *d_y, hdcStream_t stream);
+/* Mean-squared-error loss and its gradient with respect to every parameter
+ * (h_grads [num_params], may be NULL; h_loss may be NULL). */
+int hdc_mlp_gradients(HdcMlp *m, const float *d_x, const float *d_target, int batch, float *h_grads,
+                      double *h_loss, hdcStream_t stream);
+/* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8) on the MSE loss. */
+int hdc_mlp_train_step(HdcMlp *m, const float *d_x, const float *d_target, int batch, float lr, double *h_loss,
+                       hdcStream_t stream);
+
 /* Peel loop controls (PeelLoopParams and PeelWeightParams' consumers,
  * params/peel/mod.rs:207-224).  num_passes is the number of passes over all
  * sources, num_loops the iono-fit iterations per source.  (The reference's

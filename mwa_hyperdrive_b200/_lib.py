@@ -121,6 +121,16 @@ SIGNATURES = {
                                         c_double, c_double, c_int, ctypes.POINTER(HdcCalResult), c_int, c_void_p]),
     "hdc_peel_timeblock": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p, c_int, c_void_p, c_double,
                                    RADec, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "hdc_calibration_residuals": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p,
+                                          c_void_p]),
+    "hdc_mlp_new": (c_int, [c_int, c_void_p, c_int, ctypes.c_ulonglong, ctypes.POINTER(c_void_p)]),
+    "hdc_mlp_free": (None, [c_void_p]),
+    "hdc_mlp_num_params": (ctypes.c_longlong, [c_void_p]),
+    "hdc_mlp_get_params": (c_int, [c_void_p, c_void_p]),
+    "hdc_mlp_set_params": (c_int, [c_void_p, c_void_p]),
+    "hdc_mlp_forward": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p]),
+    "hdc_mlp_gradients": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
+    "hdc_mlp_train_step": (c_int, [c_void_p, c_void_p, c_void_p, c_int, ctypes.c_float, c_void_p, c_void_p]),
     "hdc_kernel_launches": (ctypes.c_longlong, []),
     "hdc_modeller_set_profiling": (c_int, [c_void_p, c_int]),
     "hdc_modeller_profile": (c_int, [c_void_p, c_void_p, c_int]),

@@ -310,6 +310,37 @@ __global__ void retry_seed_kernel(JonesF64* dj, int nchan, int ntiles, const int
     }
 }
 
+// Per-chanblock calibration residual sum_{t,bl} ||D - G_p M G_q^H||_F^2 for
+// the gains in dj [tile][chanblock] (used to judge a proposed starting point
+// against the identity start).  One CTA per chanblock.
+__global__ void __launch_bounds__(CT) residual_kernel(const CalParams P, const JonesF64* dj, double* out) {
+    const int ch = blockIdx.x;
+    const int nt = P.t1 - P.t0;
+    const size_t tstride = (size_t)P.nchan * P.nbl;
+    const JonesF32* D0 = P.data + ((size_t)P.t0 * P.nchan + ch) * P.nbl;
+    const JonesF32* M0 = P.model + ((size_t)P.t0 * P.nchan + ch) * P.nbl;
+    double acc = 0.0;
+    for (int bl = threadIdx.x; bl < P.nbl; bl += CT) {
+        int p, q;
+        baseline_to_tiles(bl, P.ntiles, p, q);
+        const J2 gp = load_j(dj[(size_t)p * P.nchan + ch]);
+        const J2 gqh = herm(load_j(dj[(size_t)q * P.nchan + ch]));
+        for (int t = 0; t < nt; t++) {
+            const J2 r = load_vis(D0 + t * tstride + bl) - (gp * load_vis(M0 + t * tstride + bl)) * gqh;
+            acc += cnorm(r.a) + cnorm(r.b) + cnorm(r.c) + cnorm(r.d);
+        }
+    }
+    __shared__ double red[CT / 32];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < CT / 32; w++) s += red[w];
+        out[ch] = s;
+    }
+}
+
 static size_t smem_bytes(int n) { return (size_t)n * (3 * sizeof(J2) + sizeof(Herm) + 4 * sizeof(double) + sizeof(int)); }
 
 static int launch_mitchcal(const CalParams& P, int nblocks, cudaStream_t s) {
@@ -442,5 +473,38 @@ extern "C" int hdc_calibrate_timeblock(const JonesF32* d_data_tfb, const JonesF3
     }
     for (int c = 0; c < num_chanblocks; c++) h_results[c] = res[c];
     cleanup();
+    return HDC_OK;
+}
+
+extern "C" int hdc_calibration_residuals(const JonesF32* d_data_tfb, const JonesF32* d_model_tfb, int num_timesteps,
+                                         int timeblock_start, int timeblock_end, int num_chanblocks, int num_baselines,
+                                         const JonesF64* d_di_jones, double* h_residuals, hdcStream_t stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    const int ntiles = (int)((1.0 + std::sqrt(1.0 + 8.0 * num_baselines)) / 2.0 + 0.5);
+    if (ntiles * (ntiles - 1) / 2 != num_baselines || timeblock_start < 0 || timeblock_end > num_timesteps ||
+        timeblock_start >= timeblock_end || num_chanblocks <= 0 || !h_residuals) {
+        set_error("hdc_calibration_residuals: invalid arguments");
+        return HDC_ERR_ARG;
+    }
+    double* d_out = nullptr;
+    HDC_CUDA_RET_INT(cudaMalloc(&d_out, sizeof(double) * num_chanblocks));
+    CalParams P = {};
+    P.data = d_data_tfb;
+    P.model = d_model_tfb;
+    P.t0 = timeblock_start;
+    P.t1 = timeblock_end;
+    P.nchan = num_chanblocks;
+    P.nbl = num_baselines;
+    P.ntiles = ntiles;
+    residual_kernel<<<num_chanblocks, CT, 0, s>>>(P, d_di_jones, d_out);
+    count_launches(1);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h_residuals, d_out, sizeof(double) * num_chanblocks, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(d_out);
+    if (e != cudaSuccess) {
+        set_error("hdc_calibration_residuals: %s", cudaGetErrorString(e));
+        return HDC_ERR_CUDA;
+    }
     return HDC_OK;
 }

@@ -1,0 +1,272 @@
+"""Learned warm start for DI calibration (this project's addition; the
+reference's solver always starts each timeblock from identity,
+di_calibrate/mod.rs:283-287).
+
+A small MLP (trained and evaluated by libhdc's own FP32 CUDA kernels) maps,
+for each (tile, chanblock), the previous timeblock's solutions at chanblocks
+c-2 .. c+2 (5 Jones = 40 reals, gauge-aligned) to a proposed gain for the
+current timeblock.  The network predicts a correction to the centre input
+(its output layer starts at zero, so the untrained net proposes the previous
+solution).  The solver judges every chanblock's proposal by its calibration
+residual and falls back to the identity start wherever the proposal's
+residual is worse, then refines with the unchanged MitchCal iteration.
+
+Gauge: DI solutions are defined up to one unit-modulus phase per chanblock
+(G -> e^{i phi} G leaves G M G^H unchanged).  Features and targets are
+aligned so that the reference tile's XX gain is real and positive;
+comparisons between solvers use the same alignment.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import hashlib
+import struct
+import time
+from dataclasses import dataclass
+from pathlib import Path
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import _lib
+from . import calibrate as cal
+from .model import _stream_ptr
+
+NEIGHBOURS = 2          # chanblocks on each side
+IN_DIM = 8 * (2 * NEIGHBOURS + 1)
+OUT_DIM = 8
+CENTRE = 8 * NEIGHBOURS
+
+
+def gauge_align(sol_tc: np.ndarray, ref_tile: int = 0) -> np.ndarray:
+    """Rotate each chanblock's solutions by one phase so that the reference
+    tile's XX gain is real and positive (NaN chanblocks stay NaN)."""
+    s = np.array(sol_tc, np.float64, copy=True)
+    xx = s[ref_tile, :, 0] + 1j * s[ref_tile, :, 1]
+    ph = np.where(np.abs(xx) > 0, np.conj(xx) / np.maximum(np.abs(xx), 1e-300), 1.0 + 0j)
+    c = s[..., 0::2] + 1j * s[..., 1::2]
+    c = c * ph[None, :, None]
+    s[..., 0::2] = c.real
+    s[..., 1::2] = c.imag
+    return s
+
+
+def features(prev_tc: np.ndarray) -> np.ndarray:
+    """[tile][chanblock][8] previous solutions -> [tile*chanblock][40] float32
+    (neighbours clamped at the band edges; NaN solutions replaced by the
+    identity)."""
+    p = gauge_align(prev_tc)
+    bad = ~np.isfinite(p).all(axis=-1)
+    p[bad] = [1, 0, 0, 0, 0, 0, 1, 0]
+    nt, nc = p.shape[:2]
+    idx = np.clip(np.arange(nc)[:, None] + np.arange(-NEIGHBOURS, NEIGHBOURS + 1)[None, :], 0, nc - 1)
+    f = p[:, idx, :].reshape(nt * nc, IN_DIM)
+    return np.ascontiguousarray(f, np.float32)
+
+
+class WarmStartMLP:
+    """40 -> 256 -> 256 -> 256 -> 8 ReLU MLP with a residual on the centre
+    input (hdc_mlp_*)."""
+
+    def __init__(self, hidden: int = 256, num_hidden: int = 3, seed: int = 0):
+        self.dims = [IN_DIM] + [hidden] * num_hidden + [OUT_DIM]
+        d = (ctypes.c_int * len(self.dims))(*self.dims)
+        h = ctypes.c_void_p()
+        _lib.check(_lib.lib().hdc_mlp_new(len(self.dims) - 1, d, CENTRE, seed, ctypes.byref(h)), "hdc_mlp_new")
+        self._h = h
+        self.losses: List[float] = []
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.lib().hdc_mlp_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def num_params(self) -> int:
+        return int(_lib.lib().hdc_mlp_num_params(self._h))
+
+    def get_params(self) -> np.ndarray:
+        out = np.zeros(self.num_params, np.float32)
+        _lib.check(_lib.lib().hdc_mlp_get_params(self._h, out.ctypes.data), "hdc_mlp_get_params")
+        return out
+
+    def set_params(self, p: np.ndarray) -> None:
+        p = np.ascontiguousarray(p, np.float32)
+        assert p.size == self.num_params
+        _lib.check(_lib.lib().hdc_mlp_set_params(self._h, p.ctypes.data), "hdc_mlp_set_params")
+
+    def forward_device(self, d_x, d_y, stream=None):
+        _lib.check(_lib.lib().hdc_mlp_forward(self._h, d_x.data_ptr(), int(d_x.shape[0]), d_y.data_ptr(),
+                                              _stream_ptr(stream)), "hdc_mlp_forward")
+
+    def gradients(self, d_x, d_t, stream=None):
+        g = np.zeros(self.num_params, np.float32)
+        loss = ctypes.c_double()
+        _lib.check(_lib.lib().hdc_mlp_gradients(self._h, d_x.data_ptr(), d_t.data_ptr(), int(d_x.shape[0]),
+                                                g.ctypes.data, ctypes.byref(loss), _stream_ptr(stream)),
+                   "hdc_mlp_gradients")
+        return loss.value, g
+
+    def train(self, X: np.ndarray, Y: np.ndarray, epochs: int = 20, batch: int = 4096, lr: float = 1e-3,
+              seed: int = 0) -> List[float]:
+        """Mini-batch Adam on the device (inputs moved to HBM once)."""
+        import torch
+
+        d_x = torch.from_numpy(np.ascontiguousarray(X, np.float32)).cuda()
+        d_y = torch.from_numpy(np.ascontiguousarray(Y, np.float32)).cuda()
+        n = X.shape[0]
+        rng = np.random.default_rng(seed)
+        lib = _lib.lib()
+        loss = ctypes.c_double()
+        for ep in range(epochs):
+            perm = torch.from_numpy(rng.permutation(n)).cuda()
+            xs, ys = d_x[perm], d_y[perm]
+            tot, cnt = 0.0, 0
+            for b0 in range(0, n - batch + 1, batch):
+                bx = xs[b0:b0 + batch].contiguous()
+                by = ys[b0:b0 + batch].contiguous()
+                _lib.check(lib.hdc_mlp_train_step(self._h, bx.data_ptr(), by.data_ptr(), batch, float(lr),
+                                                  ctypes.byref(loss), _stream_ptr(None)), "hdc_mlp_train_step")
+                tot += loss.value
+                cnt += 1
+            self.losses.append(tot / max(cnt, 1))
+        return self.losses
+
+    def propose(self, prev_tc: np.ndarray) -> np.ndarray:
+        """Proposed gains [tile][chanblock][8] (gauge of the aligned input)."""
+        import torch
+
+        nt, nc = prev_tc.shape[:2]
+        x = torch.from_numpy(features(prev_tc)).cuda()
+        y = torch.empty((x.shape[0], OUT_DIM), dtype=torch.float32, device="cuda")
+        self.forward_device(x, y)
+        torch.cuda.synchronize()
+        return y.cpu().numpy().astype(np.float64).reshape(nt, nc, OUT_DIM)
+
+    # ---------------------------------------------- persistence
+    MAGIC = b"HDCMLP01"
+
+    def save(self, path) -> None:
+        """Weights file: magic, layer count, dims, float32 parameters, SHA-256."""
+        p = self.get_params()
+        body = struct.pack("<I", len(self.dims)) + struct.pack(f"<{len(self.dims)}I", *self.dims) + p.tobytes()
+        Path(path).write_bytes(self.MAGIC + body + hashlib.sha256(body).digest())
+
+    @classmethod
+    def load(cls, path) -> "WarmStartMLP":
+        raw = Path(path).read_bytes()
+        if raw[:8] != cls.MAGIC:
+            raise ValueError("not a warm-start MLP weights file")
+        body, digest = raw[8:-32], raw[-32:]
+        if hashlib.sha256(body).digest() != digest:
+            raise ValueError("weights file checksum mismatch")
+        (nl,) = struct.unpack("<I", body[:4])
+        dims = list(struct.unpack(f"<{nl}I", body[4:4 + 4 * nl]))
+        m = cls(hidden=dims[1], num_hidden=nl - 2)
+        if m.dims != dims:
+            raise ValueError(f"unsupported layer widths {dims}")
+        m.set_params(np.frombuffer(body[4 + 4 * nl:], np.float32))
+        return m
+
+
+def identity_gains(ntiles: int, nch: int) -> np.ndarray:
+    g = np.zeros((ntiles, nch, 8))
+    g[..., 0] = 1.0
+    g[..., 6] = 1.0
+    return g
+
+
+def judge(d_data, d_model, timeblock, proposal_tc: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
+    """Per chanblock, keep the proposal where its calibration residual is no
+    worse than the identity start's; returns (start gains, chose_proposal)."""
+    import torch
+
+    nt, nch, nbl = (int(x) for x in d_data.shape[:3])
+    ntiles = proposal_tc.shape[0]
+    lib = _lib.lib()
+
+    def residual(g):
+        dg = torch.from_numpy(np.ascontiguousarray(g, np.float64)).cuda()
+        out = np.zeros(nch)
+        _lib.check(lib.hdc_calibration_residuals(d_data.data_ptr(), d_model.data_ptr(), nt, int(timeblock[0]),
+                                                 int(timeblock[1]), nch, nbl, dg.data_ptr(), out.ctypes.data,
+                                                 _stream_ptr(None)), "hdc_calibration_residuals")
+        return out
+
+    ident = identity_gains(ntiles, nch)
+    prop = np.where(np.isfinite(proposal_tc), proposal_tc, ident)
+    r_prop = residual(prop)
+    r_id = residual(ident)
+    use = np.isfinite(r_prop) & (r_prop <= r_id)
+    start = np.where(use[None, :, None], prop, ident)
+    return start, use
+
+
+def calibrate_warm(d_data, d_model, timeblock, prev_tc: Optional[np.ndarray], mlp: Optional[WarmStartMLP],
+                   max_iterations=50, stop_threshold=1e-8, min_threshold=1e-4):
+    """Calibrate one timeblock from the MLP's judged proposal (identity where
+    there is no previous solution or no network)."""
+    import torch
+
+    nt, nch, nbl = (int(x) for x in d_data.shape[:3])
+    ntiles = cal.num_tiles_from_baselines(nbl)
+    t0 = time.perf_counter()
+    if prev_tc is None or mlp is None:
+        start, use = identity_gains(ntiles, nch), np.zeros(nch, bool)
+    else:
+        start, use = judge(d_data, d_model, timeblock, mlp.propose(prev_tc))
+    dj = torch.from_numpy(np.ascontiguousarray(start, np.float64)).cuda()
+    res = cal.calibrate_timeblock(d_data, d_model, dj, timeblock, max_iterations, stop_threshold, min_threshold)
+    torch.cuda.synchronize()
+    return dj.cpu().numpy(), res, use, time.perf_counter() - t0
+
+
+@dataclass
+class DriftSky:
+    """Seeded synthetic calibration sequence: per-tile gains with a phase slope
+    in frequency and a phase that drifts between timeblocks in proportion to
+    the slope (a drifting delay), plus small amplitude jitter."""
+
+    ntiles: int
+    nch: int
+    nt_per_block: int
+    nblocks: int
+    seed: int
+    slope_rad_per_mhz: float = 0.5
+    chan_mhz: float = 0.04
+    drift_per_block: float = 0.15
+    snr: Optional[float] = None
+
+    def generate(self):
+        from . import synth
+
+        rng = np.random.default_rng(self.seed)
+        nbl = self.ntiles * (self.ntiles - 1) // 2
+        f = np.arange(self.nch) * self.chan_mhz
+        phi0 = rng.uniform(-np.pi, np.pi, (self.ntiles, 2))
+        slope = rng.uniform(-self.slope_rad_per_mhz, self.slope_rad_per_mhz, (self.ntiles, 2))
+        amp0 = rng.normal(1.0, 0.1, (self.ntiles, 2))
+        leak = rng.normal(0.0, 0.01, (self.ntiles, self.nch, 4))
+        blocks = []
+        for b in range(self.nblocks):
+            g = np.zeros((self.ntiles, self.nch, 8))
+            # phase(f, b) = phi0 + slope (f + b drift): the delay behind the
+            # slope moves the phase by slope * drift per timeblock
+            ph = phi0[:, None, :] + slope[:, None, :] * (f[None, :, None] + b * self.drift_per_block)
+            amp = amp0[:, None, :] * (1.0 + 0.002 * rng.normal(size=(self.ntiles, 1, 2)))
+            g[..., 0] = amp[..., 0] * np.cos(ph[..., 0])
+            g[..., 1] = amp[..., 0] * np.sin(ph[..., 0])
+            g[..., 6] = amp[..., 1] * np.cos(ph[..., 1])
+            g[..., 7] = amp[..., 1] * np.sin(ph[..., 1])
+            g[..., 2:6] = leak
+            model = synth.random_model(self.nt_per_block, self.nch, nbl, rng)
+            data = synth.corrupt(model, g, rng, self.snr)
+            blocks.append((data, model, g))
+        return blocks

@@ -28,8 +28,23 @@ from mwa_hyperdrive_b200 import peel as P  # noqa: E402
 VEL_C = 299792458.0
 
 
+_KEEP = []
+
+
 def dev(x, dt=np.float64):
-    return torch.from_numpy(np.ascontiguousarray(x, dt)).cuda()
+    """Device copy that stays alive for the test (kernels run asynchronously,
+    so a temporary freed right after .data_ptr() could be reused before the
+    kernel reads it)."""
+    t = torch.from_numpy(np.ascontiguousarray(x, dt)).cuda()
+    _KEEP.append(t)
+    return t
+
+
+@pytest.fixture(autouse=True)
+def _release_kept():
+    yield
+    torch.cuda.synchronize()
+    _KEEP.clear()
 
 
 def rel(a, b):

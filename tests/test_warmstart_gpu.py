@@ -1,0 +1,124 @@
+"""Learned warm start: the MLP's CUDA gradients against the float64 numpy
+oracle, training on solver-produced solutions, the judge-and-fallback rule,
+and what the trained network gains over the identity start."""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("no CUDA device", allow_module_level=True)
+
+from mwa_hyperdrive_b200 import calibrate as cal  # noqa: E402
+from mwa_hyperdrive_b200 import warmstart as ws  # noqa: E402
+from oracle import mlp_ref  # noqa: E402
+
+
+def test_gradients_match_numpy_oracle():
+    rng = np.random.default_rng(0)
+    m = ws.WarmStartMLP(hidden=48, num_hidden=3, seed=3)
+    p = m.get_params()
+    # give the (zero-initialised) output layer values so every gradient is exercised
+    p = p + rng.normal(0, 0.05, p.size).astype(np.float32)
+    m.set_params(p)
+    x = rng.normal(size=(300, ws.IN_DIM)).astype(np.float32)
+    t = rng.normal(size=(300, ws.OUT_DIM)).astype(np.float32)
+    loss, g = m.gradients(torch.from_numpy(x).cuda(), torch.from_numpy(t).cuda())
+    ref_loss, ref_g = mlp_ref.gradients(p, m.dims, x, t, ws.CENTRE)
+    assert abs(loss - ref_loss) <= 1e-5 * ref_loss
+    err = np.linalg.norm(g - ref_g) / np.linalg.norm(ref_g)
+    assert err < 1e-5, err
+    y = torch.empty((300, ws.OUT_DIM), device="cuda")
+    m.forward_device(torch.from_numpy(x).cuda(), y)
+    yr, _ = mlp_ref.forward(p, m.dims, x, ws.CENTRE)
+    np.testing.assert_allclose(y.cpu().numpy(), yr, rtol=1e-4, atol=1e-5)
+
+
+def test_training_reduces_loss():
+    rng = np.random.default_rng(1)
+    m = ws.WarmStartMLP(hidden=64, num_hidden=2, seed=1)
+    x = rng.normal(size=(8192, ws.IN_DIM)).astype(np.float32)
+    # target: centre input plus a smooth function of the neighbours
+    y = x[:, ws.CENTRE:ws.CENTRE + 8] + 0.3 * np.tanh(x[:, :8] - x[:, 32:40])
+    losses = m.train(x, y.astype(np.float32), epochs=30, batch=1024, lr=2e-3)
+    assert losses[-1] < 0.2 * losses[0], losses
+
+
+def test_save_load_roundtrip(tmp_path):
+    m = ws.WarmStartMLP(hidden=32, num_hidden=3, seed=5)
+    p = m.get_params() + 0.01
+    m.set_params(p)
+    m.save(tmp_path / "w.bin")
+    m2 = ws.WarmStartMLP.load(tmp_path / "w.bin")
+    np.testing.assert_array_equal(m2.get_params(), p.astype(np.float32))
+    raw = bytearray((tmp_path / "w.bin").read_bytes())
+    raw[20] ^= 1
+    (tmp_path / "bad.bin").write_bytes(bytes(raw))
+    with pytest.raises(ValueError):
+        ws.WarmStartMLP.load(tmp_path / "bad.bin")
+
+
+def solve_sequence(blocks, mlp, tight):
+    """Solve consecutive timeblocks; timeblock k>0 starts from the judged MLP
+    proposal (mlp) or identity (mlp None).  Returns solutions, iterations."""
+    prev = None
+    sols, iters, chose = [], [], []
+    for data, model, _ in blocks:
+        d = torch.from_numpy(data).cuda()
+        m = torch.from_numpy(model).cuda()
+        sol, res, use, _ = ws.calibrate_warm(d, m, (0, data.shape[0]), prev, mlp, max_iterations=tight[0],
+                                             stop_threshold=tight[1], min_threshold=1e-4)
+        sols.append(sol)
+        iters.append(np.array([r.num_iterations for r in res]))
+        chose.append(use)
+        prev = sol
+    return sols, iters, chose
+
+
+def test_trained_warm_start_saves_iterations_and_matches_identity_solutions():
+    tight = (300, 1e-16)  # solve to the fixed point so the two starts can be compared at 1e-6
+    ntiles, nch = 24, 48
+    # training pairs from the solver's own solutions on seeded sequences
+    X, Y = [], []
+    for seed in range(6):
+        blocks = ws.DriftSky(ntiles, nch, 2, 3, seed=100 + seed, snr=None).generate()
+        sols, _, _ = solve_sequence(blocks, None, (200, 1e-14))
+        for k in range(1, len(sols)):
+            X.append(ws.features(sols[k - 1]))
+            Y.append(ws.gauge_align(sols[k]).reshape(-1, 8).astype(np.float32))
+    X, Y = np.concatenate(X), np.concatenate(Y)
+    ok = np.isfinite(X).all(axis=1) & np.isfinite(Y).all(axis=1)
+    mlp = ws.WarmStartMLP(hidden=128, num_hidden=3, seed=0)
+    losses = mlp.train(X[ok], Y[ok], epochs=60, batch=256, lr=1e-3)
+    assert losses[-1] < losses[0]
+
+    blocks = ws.DriftSky(ntiles, nch, 2, 4, seed=999, snr=None).generate()
+    s_id, it_id, _ = solve_sequence(blocks, None, tight)
+    s_ws, it_ws, chose = solve_sequence(blocks, mlp, tight)
+    # the warm start is used (judged better) on most chanblocks after the first timeblock
+    assert np.mean(np.concatenate(chose[1:])) > 0.8
+    total_id = sum(int(i.sum()) for i in it_id[1:])
+    total_ws = sum(int(i.sum()) for i in it_ws[1:])
+    assert total_ws < 0.6 * total_id, (total_ws, total_id)
+    # same solutions (gauge-aligned) within 1e-6
+    for a, b in zip(s_id, s_ws):
+        a, b = ws.gauge_align(a), ws.gauge_align(b)
+        good = np.isfinite(a).all(axis=-1) & np.isfinite(b).all(axis=-1)
+        err = np.max(np.abs(a[good] - b[good])) / np.max(np.abs(a[good]))
+        assert err < 1e-6, err
+
+
+def test_fallback_to_identity_when_proposal_is_worse():
+    blocks = ws.DriftSky(12, 8, 2, 1, seed=5).generate()
+    data, model, g = blocks[0]
+    d, m = torch.from_numpy(data).cuda(), torch.from_numpy(model).cuda()
+    rng = np.random.default_rng(0)
+    bad = rng.normal(0, 5.0, g.shape)  # a nonsense proposal
+    good = g.copy()
+    prop = bad.copy()
+    prop[:, ::2] = good[:, ::2]  # good on even chanblocks only
+    start, use = ws.judge(d, m, (0, data.shape[0]), prop)
+    assert use[::2].all() and not use[1::2].any()
+    np.testing.assert_array_equal(start[:, 1::2], ws.identity_gains(12, 8)[:, 1::2])
