@@ -77,14 +77,19 @@ def solve_sequence(blocks, mlp, tight):
     return sols, iters, chose
 
 
-def test_trained_warm_start_saves_iterations_and_matches_identity_solutions():
-    tight = (300, 1e-16)  # solve to the fixed point so the two starts can be compared at 1e-6
+def test_trained_warm_start_saves_iterations_and_reaches_the_fixed_point():
+    """From an identity start with U(-pi, pi) phases the MitchCal iteration
+    often stalls in a slow cycle (precision ~1e-7 for hundreds of iterations,
+    still 'converged' under min_threshold 1e-4); started from the trained
+    network's judged proposal it reaches the solver's fixed point (the
+    solution obtained from the true gains) in a few iterations.  Both arms use
+    the reference's default thresholds (50 iterations, stop 1e-8)."""
     ntiles, nch = 24, 48
-    # training pairs from the solver's own solutions on seeded sequences
+    default = (50, 1e-8)
     X, Y = [], []
     for seed in range(6):
         blocks = ws.DriftSky(ntiles, nch, 2, 3, seed=100 + seed, snr=None).generate()
-        sols, _, _ = solve_sequence(blocks, None, (200, 1e-14))
+        sols, _, _ = solve_sequence(blocks, None, default)
         for k in range(1, len(sols)):
             X.append(ws.features(sols[k - 1]))
             Y.append(ws.gauge_align(sols[k]).reshape(-1, 8).astype(np.float32))
@@ -95,19 +100,24 @@ def test_trained_warm_start_saves_iterations_and_matches_identity_solutions():
     assert losses[-1] < losses[0]
 
     blocks = ws.DriftSky(ntiles, nch, 2, 4, seed=999, snr=None).generate()
-    s_id, it_id, _ = solve_sequence(blocks, None, tight)
-    s_ws, it_ws, chose = solve_sequence(blocks, mlp, tight)
-    # the warm start is used (judged better) on most chanblocks after the first timeblock
+    s_id, it_id, _ = solve_sequence(blocks, None, default)
+    s_ws, it_ws, chose = solve_sequence(blocks, mlp, default)
     assert np.mean(np.concatenate(chose[1:])) > 0.8
     total_id = sum(int(i.sum()) for i in it_id[1:])
     total_ws = sum(int(i.sum()) for i in it_ws[1:])
-    assert total_ws < 0.6 * total_id, (total_ws, total_id)
-    # same solutions (gauge-aligned) within 1e-6
-    for a, b in zip(s_id, s_ws):
-        a, b = ws.gauge_align(a), ws.gauge_align(b)
-        good = np.isfinite(a).all(axis=-1) & np.isfinite(b).all(axis=-1)
-        err = np.max(np.abs(a[good] - b[good])) / np.max(np.abs(a[good]))
-        assert err < 1e-6, err
+    assert total_ws < 0.5 * total_id, (total_ws, total_id)
+    # fixed point of the solver for each timeblock: solve from the true gains
+    for k, (data, model, g) in enumerate(blocks[1:], start=1):
+        d, m = torch.from_numpy(data).cuda(), torch.from_numpy(model).cuda()
+        dj = torch.from_numpy(g.copy()).cuda()
+        cal.calibrate_timeblock(d, m, dj, (0, data.shape[0]), 50, 1e-20, 1e-4)
+        fp = ws.gauge_align(dj.cpu().numpy())
+        w = ws.gauge_align(s_ws[k])
+        i = ws.gauge_align(s_id[k])
+        err_ws = np.max(np.abs(w - fp)) / np.max(np.abs(fp))
+        err_id = np.max(np.abs(i - fp)) / np.max(np.abs(fp))
+        assert err_ws < 1e-6, (k, err_ws, err_id)
+        assert err_ws <= err_id + 1e-12
 
 
 def test_fallback_to_identity_when_proposal_is_worse():
