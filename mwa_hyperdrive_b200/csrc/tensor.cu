@@ -1,35 +1,54 @@
-// Tensor-core factored point-source predict (tcgen05, sm_100a).
+// Tensor-core factored point-source predict (tcgen05, sm_100a), exact
+// integer accumulation.
 //
 // For one timestep and channel the baseline UVW is a tile difference
 // (uvw_pq = uvw_p - uvw_q, as marlu's xyzs_to_cross_uvws builds it), so the
 // point-source phasor factors: exp(2 pi i theta_pq,c) = A_pc conj(A_qc) with
 // A_pc = exp(2 pi i (u_p l_c + v_p m_c + w_p (n_c - 1)) f / c).  Each
 // polarisation ab of the visibility matrix is then a weighted Gram product
-//     V^ab = A diag(W^ab) A^H          (tiles x tiles, contracted over components)
+//     V^ab = X Y^H,  X = A diag(W^ab),  Y = A     (tiles x tiles, over components)
 // with W = B S B^H the per-component brightness (shared beam).  W is
 // Hermitian, so V^YX = (V^XY)^H and V^XX, V^YY are Hermitian: three complex
-// products give all four correlations of every baseline.
+// products give all four correlations of every baseline.  In real form
+//     Re V = Xr Yr^T + Xi Yi^T,   Im V = Xi Yr^T + Xr (-Yi)^T.
 //
-// Kernel: one CTA per (channel, polarisation group); group 0 = XX + YY,
-// group 1 = XY.  With X = A diag(W) s (s a power-of-two range scale) and
-// Y = A, the real form is
-//     Re V = Xr Yr^T + Xi Yi^T,   Im V = Xi Yr^T - Xr Yi^T,
-// computed by tcgen05.mma (kind::f16, M = N = 128, K = 16 per instruction,
-// FP32 accumulators in TMEM, the minus sign via the A-negate bit).  Producer
-// warps compute the FP64 per-tile phases (exact turn-domain range reduction,
-// sincospi) for 32 components per stage, form X and Y, split every value into
-// an fp16 pair (hi = fp16(x), lo = fp16(x - hi): 22 bits, inputs exact to
-// ~2^-24) and write them to shared memory in the K-major core-matrix layout;
-// one thread issues the 4 partial products (hi.hi, hi.lo, lo.hi, lo.lo) of
-// every term.  Two stages double-buffer producers against the tensor core.
-// The epilogue reads TMEM with tcgen05.ld and adds the upper-triangle
-// baselines into the visibilities.
+// Numbers.  A tensor core accumulating in FP32 does not round to nearest, and
+// its error grows with every K step.  Here every operand is instead a
+// fixed-point integer split into balanced byte digits, and the digit planes
+// are multiplied on the integer tensor core (kind::i8, s8 x s8, s32
+// accumulators), where every sum is exact:
+//   x = rint(X sx), |x| < 2^31 - 2^24 (sx from the channel's largest |W|):
+//       x = d0 2^24 + d1 2^16 + d2 2^8 + d3, every d_i in [-128, 127];
+//   y = rint(A sy), |y| < 2^23 - 2^16: y = e0 2^16 + e1 2^8 + e2.
+// Balanced digits are the bytes of (x + 0x808080) ^ 0x808080: adding 128 to
+// each lower digit position and flipping its top bit turns excess-128 bytes
+// into two's-complement ones.  They have zero mean, so the products left out
+// below do not bias the sum (unsigned lower bytes would: their dropped
+// products are all positive and grow with the number of components).
+// x y = sum_ij d_i e_j 2^(40 - 8(i + j)); the nine plane products with
+// i + j <= 3 are kept (the rest weigh < 2^-30 of full scale), each into the
+// accumulator of its class w = i + j, and the epilogue forms
+// V = sum_w D_w 2^(40 - 8w) / (sx sy) in FP64.  The only rounding is in the
+// inputs: the FP64-reduced phase, FP32 sincospi with a first-order
+// correction for the low part of the phase, X = W A in FP32, and the two
+// roundings to integers (2^-24 of A, 2^-31 of the channel's largest |X|).
+// A launch covers at most KPASS components, so no s32 sum can overflow.
+//
+// Kernel: one CTA per (channel, polarisation, half of the tile columns); M =
+// 128 tiles (rows of X), N = 64 tiles (rows of Y), K = 32 components per
+// stage.  Eight producer warps compute the per-tile phases (exact FP64 turn
+// reduction), X and Y, the byte planes, and write them to shared memory in
+// the K-major core-matrix layout; one thread issues the 36 MMAs of a stage
+// (9 plane pairs x 4 real products) into 8 TMEM accumulators (4 classes x
+// re/im, 64 columns each = all 512 columns).  Four stages let the producers
+// run ahead of the tensor core.  The epilogue reads TMEM with tcgen05.ld,
+// combines the classes in FP64 and adds the baselines of its columns into
+// the visibilities (XX, YY: q > p; XY: q > p as XY, q < p as YX = conj).
 //
 // Every mbarrier wait is bounded by the global timer; on a timeout the CTA
 // records KERR_TIMEOUT, waits (bounded) for its issued MMAs and frees TMEM.
 
-#include <cuda_fp16.h>
-
+#include <algorithm>
 #include <cmath>
 
 #include "modeller.cuh"
@@ -37,20 +56,27 @@
 namespace hdc {
 namespace tc {
 
-constexpr int NT = 128;   // tiles = M = N
-constexpr int KC = 32;    // components per stage (K elements per operand part)
-constexpr int NSTAGE = 2;
-constexpr int NPW = 8;    // producer / epilogue warps
+constexpr int NT = 128;    // tiles = M
+constexpr int NH = 64;     // tile columns per CTA = N
+constexpr int KC = 32;     // components per stage = MMA K (bytes)
+constexpr int NSTAGE = 4;
+constexpr int NPW = 8;     // producer / epilogue warps
 constexpr int THREADS = (NPW + 1) * 32;
-constexpr int TILE_BYTES = NT * KC * 2;  // one fp16 operand tile, 8 KB
-constexpr int LBO = 128;                 // bytes between 8-element K chunks
-constexpr int SBO = (KC / 8) * 128;      // bytes between 8-row groups
-constexpr int TILES_PER_STAGE = 12;      // Y: 4, X: up to 2 pols x 4
-constexpr int STAGE_BYTES = TILES_PER_STAGE * TILE_BYTES;
+constexpr int XDIG = 4;    // byte planes of x
+constexpr int YDIG = 3;    // byte planes of y
+constexpr int XT_BYTES = NT * KC;                           // one X plane tile, 4 KB
+constexpr int YT_BYTES = NH * KC;                           // one Y plane tile, 2 KB
+constexpr int Y_OFF = 2 * XDIG * XT_BYTES;                  // X: [re, im][4 planes]
+constexpr int STAGE_BYTES = Y_OFF + 3 * YDIG * YT_BYTES;    // Y: [re, im, -im][3 planes]
 constexpr int SMEM_BYTES = NSTAGE * STAGE_BYTES + 1024;
+constexpr int LBO = 128;             // bytes between the two 16-byte K core matrices of a row group
+constexpr int SBO = (KC / 16) * 128; // bytes between 8-row groups
+constexpr int TMEM_COLS = 512;       // 4 classes x (re, im) x NH
+constexpr int KPASS = 16384;         // components per launch: 3 pairs x 2 x 2^14 x KPASS < 2^31
+constexpr float SY = 8257536.0f;     // 2^23 - 2^17: |A| <= 1 -> y + 0x8080 < 2^23
 
 struct Params {
-    int nf, nbl, ntiles, nc;
+    int nf, nbl, ntiles, nc, c0, cn;
     const double* freqs;
     const XYZ* xyzs;
     double s_ha, c_ha, s_dec, c_dec;
@@ -67,17 +93,23 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
            ((uint64_t)1 << 46);
 }
 
-// kind::f16 instruction descriptor: f16 A and B, f32 D, K-major, M=N=128.
-__host__ __device__ constexpr uint32_t idesc(bool neg_a) {
-    return (1u << 4) | (0u << 7) | (0u << 10) | ((neg_a ? 1u : 0u) << 13) | ((uint32_t)(NT >> 3) << 17) |
-           ((uint32_t)(NT >> 4) << 24);
+// kind::i8 instruction descriptor: s32 D (bits 4-5 = 2), A and B signed
+// (bits 7 and 10 = 1), K-major, N at bit 17 (>> 3), M at bit 24 (>> 4).
+__host__ __device__ constexpr uint32_t idesc_s8() {
+    return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NH >> 3) << 17) | ((uint32_t)(NT >> 4) << 24);
 }
 
-__device__ __forceinline__ void mma_f16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t id, uint32_t acc) {
+// integer whose bytes are the balanced base-256 digits of v (lower `low`
+// positions rebalanced, the top byte keeps the sign)
+__device__ __forceinline__ int balanced(int v, uint32_t low) {
+    return (int)(((uint32_t)v + low) ^ low);
+}
+
+__device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t id, uint32_t acc) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
         :
         : "r"(d_tmem), "l"(a), "l"(b), "r"(id), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
 }
@@ -94,47 +126,74 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t addr, float* v) {
-    uint32_t r[16];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(addr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+// 8 columns of 32 lanes (one per thread) from TMEM; the caller waits with
+// tmem_wait_ld before using the registers.
+__device__ __forceinline__ void tmem_ld8(uint32_t addr, int* v) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+                 : "r"(addr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// byte offset of the 16-byte chunk (row, K half) in a K-major core-matrix tile
+__device__ __forceinline__ uint32_t chunk_off(int row, int khalf) {
+    return (uint32_t)((row >> 3) * SBO + khalf * LBO + (row & 7) * 16);
+}
+
+// Byte planes of 16 integers: plane b (byte b of every v[j]) as 16 bytes, v[j]
+// at byte j.  A 4x4 byte transpose per group of four.
+__device__ __forceinline__ void byte_planes(const int* v, uint4* planes, int nplanes) {
+    uint32_t w[4][4];  // [plane][group]
 #pragma unroll
-    for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+    for (int g = 0; g < 4; g++) {
+        const uint32_t a = (uint32_t)v[4 * g], b = (uint32_t)v[4 * g + 1], c = (uint32_t)v[4 * g + 2],
+                       d = (uint32_t)v[4 * g + 3];
+        const uint32_t t0 = __byte_perm(a, b, 0x5140), t1 = __byte_perm(c, d, 0x5140);
+        const uint32_t t2 = __byte_perm(a, b, 0x7362), t3 = __byte_perm(c, d, 0x7362);
+        w[0][g] = __byte_perm(t0, t1, 0x5410);
+        w[1][g] = __byte_perm(t0, t1, 0x7632);
+        w[2][g] = __byte_perm(t2, t3, 0x5410);
+        w[3][g] = __byte_perm(t2, t3, 0x7632);
+    }
+#pragma unroll
+    for (int b = 0; b < 4; b++)
+        if (b < nplanes) planes[b] = make_uint4(w[b][0], w[b][1], w[b][2], w[b][3]);
 }
 
-// byte offset of element (row, k) in a K-major core-matrix tile
-__device__ __forceinline__ uint32_t tile_off(int row, int k) {
-    return (uint32_t)((row >> 3) * SBO + (k >> 3) * LBO + (row & 7) * 16 + (k & 7) * 2);
+// shared-memory tile offsets inside a stage; digit 0 is the signed top byte
+__device__ __forceinline__ uint32_t x_tile(int part, int digit) {
+    return (uint32_t)((part * XDIG + digit) * XT_BYTES);
 }
-
-__device__ __forceinline__ void split16(double x, __half& h, __half& l) {
-    h = __double2half(x);  // round to nearest even
-    l = __double2half(x - (double)__half2float(h));
+__device__ __forceinline__ uint32_t y_tile(int part, int digit) {
+    return (uint32_t)(Y_OFF + (part * YDIG + digit) * YT_BYTES);
 }
-
-// tile index inside a stage
-__device__ __forceinline__ int y_tile(int piece, int part) { return piece * 2 + part; }
-__device__ __forceinline__ int x_tile(int pol, int piece, int part) { return 4 + pol * 4 + piece * 2 + part; }
+// TMEM column of accumulator (class w, re/im)
+__device__ __forceinline__ uint32_t acc_col(int w, int ri) { return (uint32_t)((w * 2 + ri) * NH); }
 
 template <bool OUT64>
-__global__ void __launch_bounds__(THREADS, 1) gram_kernel(const Params P) {
+__global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const Params P) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     __shared__ alignas(8) uint64_t full_bar[NSTAGE], empty_bar[NSTAGE], done_bar;
     __shared__ uint32_t tmem_base_s;
-    __shared__ float red_s[THREADS / 32];
+    __shared__ double red_s[THREADS / 32];
     __shared__ volatile int abort_s;
 
     unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     const int f = blockIdx.x;
-    const int group = blockIdx.y;          // 0: XX+YY, 1: XY
-    const int npol = group == 0 ? 2 : 1;
+    const int pol = blockIdx.y;   // 0: XX, 1: YY, 2: XY
+    const int hcol = blockIdx.z;  // tile columns [hcol * NH, hcol * NH + NH)
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int ncols = group == 0 ? 512 : 256;
+    // W component of this polarisation (JonesF64 as 4 double2: xx, xy, yx, yy)
+    const int wsel = pol == 0 ? 0 : (pol == 1 ? 3 : 1);
 
+    // largest |W| of the pass sets the x scale
+    double mx = 0.0;
+    for (int c = tid; c < P.cn; c += THREADS) {
+        const double2 w = __ldg(reinterpret_cast<const double2*>(P.W + (size_t)f * P.nc + P.c0 + c) + wsel);
+        mx = fmax(mx, hypot(w.x, w.y));
+    }
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (lane == 0) red_s[warp] = mx;
     if (tid == 0) {
         for (int s = 0; s < NSTAGE; s++) {
             mbar_init(&full_bar[s], NPW * 32);
@@ -144,45 +203,37 @@ __global__ void __launch_bounds__(THREADS, 1) gram_kernel(const Params P) {
         abort_s = 0;
         fence_barrier_init();
     }
+    __syncthreads();
+    double wmax = 0.0;
+    for (int i = 0; i < THREADS / 32; i++) wmax = fmax(wmax, red_s[i]);
+    // A polarisation whose weights are all exactly zero (e.g. XY of a
+    // Stokes-I sky) contributes exactly zero; a column half beyond the
+    // last tile has no baselines.
+    if (!(wmax > 0.0) || hcol * NH >= P.ntiles) return;
+    const float sx = (float)((2147483648.0 - 33554432.0) / wmax);  // (2^31 - 2^25) / max|W|
+    const double inv = 1.0 / ((double)sx * (double)SY);
+
     if (warp == 0) {
-        // allocate TMEM (one warp), publish its base address in shared memory
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_s)),
-                     "r"(ncols)
+                     "r"(TMEM_COLS)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
-
-    // range scale: s = 2^e with max |W component| * s in [8192, 16384)
-    const double freq = P.freqs[f];
-    float mx = 0.f;
-    for (int c = tid; c < P.nc; c += THREADS) {
-        const JonesF64 w = P.W[(size_t)f * P.nc + c];
-        if (group == 0)
-            mx = fmaxf(mx, (float)fmax(fmax(fabs(w.j00_re), fabs(w.j00_im)), fmax(fabs(w.j11_re), fabs(w.j11_im))));
-        else
-            mx = fmaxf(mx, (float)fmax(fabs(w.j01_re), fabs(w.j01_im)));
-    }
-    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    if (lane == 0) red_s[warp] = mx;
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    float wmax = 0.f;
-    for (int i = 0; i < THREADS / 32; i++) wmax = fmaxf(wmax, red_s[i]);
-    const double scale = wmax > 0.f ? exp2(floor(log2(16384.0 / (double)wmax))) : 1.0;
-    const double inv_scale = 1.0 / scale;
     const uint32_t tmem = tmem_base_s;
-    // A polarisation group whose weights are all exactly zero (e.g. XY/YX of
-    // a Stokes-I sky) contributes exactly zero: skip its work.
-    const bool skip = !(wmax > 0.f);
-    const int nchunks = skip ? 0 : (P.nc + KC - 1) / KC;
+    const int nchunks = (P.cn + KC - 1) / KC;
+    const double freq = P.freqs[f];
 
     if (warp < NPW) {
         // ------------------------------------------------ producers
-        const int r = tid & (NT - 1);  // tile (row of X and of Y)
-        const int half = tid >> 7;     // which 16 components of the stage
-        double u = 0.0, v = 0.0, w = 0.0;
+        const int r = tid & (NT - 1);  // tile: row of X
+        const int khalf = tid >> 7;    // components [khalf * 16, khalf * 16 + 16) of a stage
+        const int yrow = r - hcol * NH;
         const bool real_tile = r < P.ntiles;
+        const bool in_y = real_tile && yrow >= 0 && yrow < NH;
+        double u = 0.0, v = 0.0, w = 0.0;
         if (real_tile) {
             const XYZ x = P.xyzs[r];
             const double ool = freq / VEL_C;
@@ -190,6 +241,7 @@ __global__ void __launch_bounds__(THREADS, 1) gram_kernel(const Params P) {
             v = (-P.s_dec * P.c_ha * x.x + P.s_dec * P.s_ha * x.y + P.c_dec * x.z) * ool;
             w = (P.c_dec * P.c_ha * x.x - P.c_dec * P.s_ha * x.y + P.s_dec * x.z) * ool;
         }
+        const JonesF64* Wf = P.W + (size_t)f * P.nc + P.c0;
         for (int k = 0; k < nchunks; k++) {
             const int st = k % NSTAGE;
             if (k >= NSTAGE) {
@@ -197,57 +249,58 @@ __global__ void __launch_bounds__(THREADS, 1) gram_kernel(const Params P) {
                 if (!ok) abort_s = 1;
             }
             if (abort_s) break;
-            unsigned char* sb = smem + st * STAGE_BYTES;
-            // two sub-blocks of 8 components -> one 16-byte store per tile each
-            for (int sub = 0; sub < 2; sub++) {
-                const int kbase = half * 16 + sub * 8;  // k offset inside the stage
-                __align__(16) __half yv[4][8];          // [piece*2+part][j]
-                __align__(16) __half xv[2][4][8];       // [pol][piece*2+part][j]
+            int xr[16], xi[16], yr[16], yi[16], yn[16];
 #pragma unroll
-                for (int j = 0; j < 8; j++) {
-                    const int c = k * KC + kbase + j;
-                    double ar = 0.0, ai = 0.0;
-                    double br[2] = {0.0, 0.0}, bi[2] = {0.0, 0.0};
-                    if (c < P.nc && real_tile) {
-                        const double2 lm = __ldg(reinterpret_cast<const double2*>(P.lmn + c));
-                        const double ln = __ldg(reinterpret_cast<const double*>(P.lmn + c) + 2);
-                        const cplx a = phasor_turns(u * lm.x + v * lm.y + w * ln);
-                        ar = a.re;
-                        ai = a.im;
-                        const JonesF64* wp = P.W + (size_t)f * P.nc + c;
-                        if (group == 0) {
-                            const double2 xx = __ldg(reinterpret_cast<const double2*>(wp));
-                            const double2 yy = __ldg(reinterpret_cast<const double2*>(wp) + 3);
-                            const cplx bx = a * cplx{xx.x * scale, xx.y * scale};
-                            const cplx by = a * cplx{yy.x * scale, yy.y * scale};
-                            br[0] = bx.re;
-                            bi[0] = bx.im;
-                            br[1] = by.re;
-                            bi[1] = by.im;
-                        } else {
-                            const double2 xy = __ldg(reinterpret_cast<const double2*>(wp) + 1);
-                            const cplx b = a * cplx{xy.x * scale, xy.y * scale};
-                            br[0] = b.re;
-                            bi[0] = b.im;
-                        }
-                    }
-                    split16(ar, yv[0][j], yv[2][j]);
-                    split16(ai, yv[1][j], yv[3][j]);
-                    for (int p = 0; p < npol; p++) {
-                        split16(br[p], xv[p][0][j], xv[p][2][j]);
-                        split16(bi[p], xv[p][1][j], xv[p][3][j]);
+            for (int j = 0; j < 16; j++) {
+                const int c = k * KC + khalf * 16 + j;
+                xr[j] = xi[j] = yr[j] = yi[j] = yn[j] = 0;
+                if (c < P.cn && real_tile) {
+                    const double2 lm = __ldg(reinterpret_cast<const double2*>(P.lmn + P.c0 + c));
+                    const double ln = __ldg(reinterpret_cast<const double*>(P.lmn + P.c0 + c) + 2);
+                    const double t = u * lm.x + v * lm.y + w * ln;
+                    const double tr = 2.0 * (t - rint(t));  // half-turns in [-1, 1]
+                    const float th = (float)tr;
+                    const float tl = (float)(tr - (double)th);
+                    float s, co;
+                    sincospif(th, &s, &co);
+                    // sin, cos of pi (th + tl) to first order in tl (|tl| <= 2^-24)
+                    const float d = 3.14159265358979f * tl;
+                    const float s1 = fmaf(d, co, s);
+                    const float c1 = fmaf(-d, s, co);
+                    const double2 wd = __ldg(reinterpret_cast<const double2*>(Wf + c) + wsel);
+                    const float wr = (float)wd.x, wi = (float)wd.y;
+                    const float Xr = fmaf(wr, c1, -wi * s1);
+                    const float Xi = fmaf(wr, s1, wi * c1);
+                    xr[j] = balanced(__float2int_rn(Xr * sx), 0x808080u);
+                    xi[j] = balanced(__float2int_rn(Xi * sx), 0x808080u);
+                    if (in_y) {
+                        const int yi0 = __float2int_rn(s1 * SY);
+                        yr[j] = balanced(__float2int_rn(c1 * SY), 0x8080u);
+                        yi[j] = balanced(yi0, 0x8080u);
+                        yn[j] = balanced(-yi0, 0x8080u);
                     }
                 }
-                const uint32_t off = tile_off(r, kbase);
+            }
+            unsigned char* sb = smem + st * STAGE_BYTES;
+            const uint32_t xo = chunk_off(r, khalf);
+            uint4 pl[4];
+            byte_planes(xr, pl, 4);
 #pragma unroll
-                for (int t = 0; t < 4; t++)
-                    *reinterpret_cast<uint4*>(sb + y_tile(t >> 1, t & 1) * TILE_BYTES + off) =
-                        *reinterpret_cast<const uint4*>(yv[t]);
-                for (int p = 0; p < npol; p++)
+            for (int b = 0; b < 4; b++) *reinterpret_cast<uint4*>(sb + x_tile(0, 3 - b) + xo) = pl[b];
+            byte_planes(xi, pl, 4);
 #pragma unroll
-                    for (int t = 0; t < 4; t++)
-                        *reinterpret_cast<uint4*>(sb + x_tile(p, t >> 1, t & 1) * TILE_BYTES + off) =
-                            *reinterpret_cast<const uint4*>(xv[p][t]);
+            for (int b = 0; b < 4; b++) *reinterpret_cast<uint4*>(sb + x_tile(1, 3 - b) + xo) = pl[b];
+            if (yrow >= 0 && yrow < NH) {
+                const uint32_t yo = chunk_off(yrow, khalf);
+                byte_planes(yr, pl, 3);
+#pragma unroll
+                for (int b = 0; b < 3; b++) *reinterpret_cast<uint4*>(sb + y_tile(0, 2 - b) + yo) = pl[b];
+                byte_planes(yi, pl, 3);
+#pragma unroll
+                for (int b = 0; b < 3; b++) *reinterpret_cast<uint4*>(sb + y_tile(1, 2 - b) + yo) = pl[b];
+                byte_planes(yn, pl, 3);
+#pragma unroll
+                for (int b = 0; b < 3; b++) *reinterpret_cast<uint4*>(sb + y_tile(2, 2 - b) + yo) = pl[b];
             }
             fence_proxy_async_smem();  // make the generic-proxy stores visible to the tensor core
             mbar_arrive(&full_bar[st]);
@@ -256,7 +309,6 @@ __global__ void __launch_bounds__(THREADS, 1) gram_kernel(const Params P) {
         // ------------------------------------------------ MMA issuer (one thread)
         if (lane == 0) {
             const uint32_t sbase = smem_u32(smem);
-            int issued = 0;
             for (int k = 0; k < nchunks; k++) {
                 const int st = k % NSTAGE;
                 const bool ok = mbar_wait_bounded(&full_bar[st], (k / NSTAGE) & 1, P.err);
@@ -266,30 +318,26 @@ __global__ void __launch_bounds__(THREADS, 1) gram_kernel(const Params P) {
                 }
                 tc_fence_after();
                 const uint32_t sb = sbase + st * STAGE_BYTES;
-                for (int p = 0; p < npol; p++) {
-                    const uint32_t d_re = tmem + p * 256, d_im = tmem + p * 256 + 128;
-                    // (x part, y part, negate A, accumulator)
-                    const int terms[4][4] = {{0, 0, 0, 0}, {1, 1, 0, 0}, {1, 0, 0, 1}, {0, 1, 1, 1}};
-                    for (int tm = 0; tm < 4; tm++) {
-                        const uint32_t d = terms[tm][3] ? d_im : d_re;
-                        const uint32_t id = idesc(terms[tm][2] != 0);
-                        for (int pa = 0; pa < 2; pa++)
-                            for (int pb = 0; pb < 2; pb++)
-                                for (int kk = 0; kk < KC / 16; kk++) {
-                                    const uint32_t a = sb + x_tile(p, pa, terms[tm][0]) * TILE_BYTES + kk * 2 * LBO;
-                                    const uint32_t b = sb + y_tile(pb, terms[tm][1]) * TILE_BYTES + kk * 2 * LBO;
-                                    // the first product into each accumulator overwrites it
-                                    const bool first = (k == 0) && (tm < 2 ? tm == 0 : tm == 2) && pa == 0 &&
-                                                       pb == 0 && kk == 0;
-                                    mma_f16(d, smem_desc(a), smem_desc(b), id, first ? 0u : 1u);
-                                }
+                uint32_t started = 0;  // accumulators written in this launch (first stage only)
+                for (int i = 0; i < XDIG; i++)
+                    for (int j = 0; j < YDIG; j++) {
+                        const int cls = i + j;
+                        if (cls > 3) continue;
+                        const uint32_t id = idesc_s8();
+                        // (accumulator re/im, X part, Y part): Re += Xr Yr + Xi Yi, Im += Xi Yr + Xr (-Yi)
+                        const int prods[4][3] = {{0, 0, 0}, {0, 1, 1}, {1, 1, 0}, {1, 0, 2}};
+                        for (int q = 0; q < 4; q++) {
+                            const int ri = prods[q][0];
+                            const uint32_t bit = 1u << (cls * 2 + ri);
+                            const bool first = k == 0 && !(started & bit);
+                            started |= bit;
+                            mma_i8(tmem + acc_col(cls, ri), smem_desc(sb + x_tile(prods[q][1], i)),
+                                   smem_desc(sb + y_tile(prods[q][2], j)), id, first ? 0u : 1u);
+                        }
                     }
-                }
                 mma_commit(&empty_bar[st]);  // stage free once these MMAs have read it
-                issued++;
             }
             mma_commit(&done_bar);
-            (void)issued;
         }
     }
 
@@ -298,72 +346,49 @@ __global__ void __launch_bounds__(THREADS, 1) gram_kernel(const Params P) {
     const bool aborted = abort_s != 0;
     const bool ok = mbar_wait_bounded(&done_bar, 0, P.err);
     tc_fence_after();
-    if (!aborted && ok && !skip && warp < NPW) {
-        const int lg = warp & 3;           // TMEM lane group this warp may access
-        const int chalf = warp >> 2;       // column half
-        const int p = lg * 32 + lane;      // row (tile 1 candidate)
+    if (!aborted && ok && warp < NPW && nchunks > 0) {
+        const int lg = warp & 3;       // TMEM lane group this warp may access
+        const int chalf = warp >> 2;   // column half of the NH columns
+        const int p = lg * 32 + lane;  // row: tile p
         const uint32_t lane_addr = tmem + ((uint32_t)(lg * 32) << 16);
         const int n = P.ntiles;
-        for (int q0 = chalf * 64; q0 < chalf * 64 + 64; q0 += 16) {
-            if (group == 0) {
-                float xr[16], xi[16], yr[16], yi[16];
-                tmem_ld16(lane_addr + q0, xr);
-                tmem_ld16(lane_addr + 128 + q0, xi);
-                tmem_ld16(lane_addr + 256 + q0, yr);
-                tmem_ld16(lane_addr + 384 + q0, yi);
-                if (p < n) {
-                    for (int j = 0; j < 16; j++) {
-                        const int q = q0 + j;
-                        if (q <= p || q >= n) continue;
-                        const size_t o = (size_t)f * P.nbl + baseline_index(p, q, n);
-                        if (OUT64) {
-                            JonesF64* vp = reinterpret_cast<JonesF64*>(P.vis) + o;
-                            vp->j00_re += xr[j] * inv_scale;
-                            vp->j00_im += xi[j] * inv_scale;
-                            vp->j11_re += yr[j] * inv_scale;
-                            vp->j11_im += yi[j] * inv_scale;
-                        } else {
-                            JonesF32* vp = reinterpret_cast<JonesF32*>(P.vis) + o;
-                            vp->j00_re += (float)(xr[j] * inv_scale);
-                            vp->j00_im += (float)(xi[j] * inv_scale);
-                            vp->j11_re += (float)(yr[j] * inv_scale);
-                            vp->j11_im += (float)(yi[j] * inv_scale);
-                        }
-                    }
+        for (int c0 = chalf * (NH / 2); c0 < chalf * (NH / 2) + NH / 2; c0 += 8) {
+            int a[8][8];  // [class * 2 + re/im][column]
+#pragma unroll
+            for (int g = 0; g < 8; g++) tmem_ld8(lane_addr + (uint32_t)(g * NH + c0), a[g]);
+            tmem_wait_ld();
+            if (p >= n) continue;
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                const int q = hcol * NH + c0 + j;
+                if (q == p || q >= n) continue;
+                if (pol < 2 && q < p) continue;
+                double re = 0.0, im = 0.0;
+#pragma unroll
+                for (int cls = 0; cls < 4; cls++) {
+                    const double wgt = ldexp(1.0, 40 - 8 * cls);
+                    re += (double)a[cls * 2][j] * wgt;
+                    im += (double)a[cls * 2 + 1][j] * wgt;
                 }
-            } else {
-                float dr[16], di[16];
-                tmem_ld16(lane_addr + q0, dr);
-                tmem_ld16(lane_addr + 128 + q0, di);
-                if (p < n) {
-                    for (int j = 0; j < 16; j++) {
-                        const int q = q0 + j;
-                        if (q == p || q >= n) continue;
-                        // q > p: XY of baseline (p, q); q < p: YX of (q, p) = conj(XY(p, q))
-                        const bool upper = q > p;
-                        const size_t o = (size_t)f * P.nbl + (upper ? baseline_index(p, q, n) : baseline_index(q, p, n));
-                        const double re = dr[j] * inv_scale;
-                        const double im = (upper ? 1.0 : -1.0) * di[j] * inv_scale;
-                        if (OUT64) {
-                            JonesF64* vp = reinterpret_cast<JonesF64*>(P.vis) + o;
-                            if (upper) {
-                                vp->j01_re += re;
-                                vp->j01_im += im;
-                            } else {
-                                vp->j10_re += re;
-                                vp->j10_im += im;
-                            }
-                        } else {
-                            JonesF32* vp = reinterpret_cast<JonesF32*>(P.vis) + o;
-                            if (upper) {
-                                vp->j01_re += (float)re;
-                                vp->j01_im += (float)im;
-                            } else {
-                                vp->j10_re += (float)re;
-                                vp->j10_im += (float)im;
-                            }
-                        }
-                    }
+                re *= inv;
+                im *= inv;
+                const bool upper = q > p;
+                const size_t o = (size_t)f * P.nbl + (upper ? baseline_index(p, q, n) : baseline_index(q, p, n));
+                // XY(p, q) for q > p; YX(q, p) = conj(XY(p, q)) for q < p
+                const int slot = pol == 0 ? 0 : (pol == 1 ? 3 : (upper ? 1 : 2));
+                if (!upper) im = -im;
+                if (OUT64) {
+                    double2* vp = reinterpret_cast<double2*>(reinterpret_cast<JonesF64*>(P.vis) + o) + slot;
+                    double2 cur = *vp;
+                    cur.x += re;
+                    cur.y += im;
+                    *vp = cur;
+                } else {
+                    float2* vp = reinterpret_cast<float2*>(reinterpret_cast<JonesF32*>(P.vis) + o) + slot;
+                    float2 cur = *vp;
+                    cur.x += (float)re;
+                    cur.y += (float)im;
+                    *vp = cur;
                 }
             }
         }
@@ -375,7 +400,7 @@ __global__ void __launch_bounds__(THREADS, 1) gram_kernel(const Params P) {
     __syncthreads();
     if (warp == 0) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
     }
 }
 
@@ -392,9 +417,9 @@ int Modeller::tensor_setup() {
     }
     if (!tc) tc = new TensorState();
     if (!tc->configured) {
-        HDC_CUDA_RET_INT(cudaFuncSetAttribute(tc::gram_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              tc::SMEM_BYTES));
-        HDC_CUDA_RET_INT(cudaFuncSetAttribute(tc::gram_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        HDC_CUDA_RET_INT(cudaFuncSetAttribute(tc::gram_i8_kernel<false>,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES));
+        HDC_CUDA_RET_INT(cudaFuncSetAttribute(tc::gram_i8_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               tc::SMEM_BYTES));
         tc->configured = true;
     }
@@ -419,13 +444,18 @@ int Modeller::tensor_points(double lst, void* d_vis, bool out64, cudaStream_t s)
     P.W = weights(0);
     P.vis = d_vis;
     P.err = d_err;
-    dim3 grid(nf, 2);
-    if (out64)
-        tc::gram_kernel<true><<<grid, tc::THREADS, tc::SMEM_BYTES, s>>>(P);
-    else
-        tc::gram_kernel<false><<<grid, tc::THREADS, tc::SMEM_BYTES, s>>>(P);
-    count_launches(1);
-    HDC_CUDA_RET_INT(cudaGetLastError());
+    // passes of at most KPASS components accumulate into the visibilities in turn
+    const dim3 grid(nf, 3, (ntiles + tc::NH - 1) / tc::NH);
+    for (int c0 = 0; c0 < P.nc; c0 += tc::KPASS) {
+        P.c0 = c0;
+        P.cn = std::min(tc::KPASS, P.nc - c0);
+        if (out64)
+            tc::gram_i8_kernel<true><<<grid, tc::THREADS, tc::SMEM_BYTES, s>>>(P);
+        else
+            tc::gram_i8_kernel<false><<<grid, tc::THREADS, tc::SMEM_BYTES, s>>>(P);
+        count_launches(1);
+        HDC_CUDA_RET_INT(cudaGetLastError());
+    }
     return HDC_OK;
 }
 

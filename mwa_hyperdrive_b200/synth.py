@@ -188,6 +188,23 @@ def corrupt(model_tfb, gains_tc, rng=None, snr=None):
     return d.astype(np.float32)
 
 
+def polarised_model(nt, nch, nbl, rng, cross=0.3):
+    """A random model [t][chanblock][bl][8] whose four correlations have
+    independent phases, XX and YY of similar amplitude and XY, YX at
+    `cross` of it (an apparent sky seen through a polarised beam).  Unlike a
+    Stokes-I dominated model this pins the relative X/Y phase of the gains,
+    so MitchCal converges to a unique fixed point (up to one phase per
+    chanblock)."""
+    m = np.zeros((nt, nch, nbl, 8))
+    amp = rng.lognormal(0.0, 0.5, (nt, nch, nbl))
+    for k in range(4):
+        a = amp * (1.0 if k in (0, 3) else cross) * rng.lognormal(0.0, 0.2, (nt, nch, nbl))
+        ph = rng.uniform(-np.pi, np.pi, (nt, nch, nbl))
+        m[..., 2 * k] = a * np.cos(ph)
+        m[..., 2 * k + 1] = a * np.sin(ph)
+    return m.astype(np.float32)
+
+
 def random_model(nt, nch, nbl, rng):
     """A random, Stokes-I dominated model [t][chanblock][bl][8]."""
     m = np.zeros((nt, nch, nbl, 8))

@@ -4,17 +4,24 @@ di_calibrate/mod.rs:283-287).
 
 A small MLP (trained and evaluated by libhdc's own FP32 CUDA kernels) maps,
 for each (tile, chanblock), the previous timeblock's solutions at chanblocks
-c-2 .. c+2 (5 Jones = 40 reals, gauge-aligned) to a proposed gain for the
-current timeblock.  The network predicts a correction to the centre input
-(its output layer starts at zero, so the untrained net proposes the previous
-solution).  The solver judges every chanblock's proposal by its calibration
+c-2 .. c+2 (5 Jones = 40 reals) to a proposed gain for the current
+timeblock.  The solver judges every chanblock's proposal by its calibration
 residual and falls back to the identity start wherever the proposal's
 residual is worse, then refines with the unchanged MitchCal iteration.
 
-Gauge: DI solutions are defined up to one unit-modulus phase per chanblock
-(G -> e^{i phi} G leaves G M G^H unchanged).  Features and targets are
-aligned so that the reference tile's XX gain is real and positive;
-comparisons between solvers use the same alignment.
+Frames.  DI solutions are defined up to one unit-modulus phase per chanblock
+(G -> e^{i phi} G leaves G M G^H unchanged); solutions are first aligned so
+that the reference tile's XX gain is real and positive.  Each tile's absolute
+X and Y phases are arbitrary (uniform over the circle), which no small
+network learns to rotate; so features and targets are expressed in the frame
+of the previous centre gain: every Jones is right-multiplied by
+diag(1/a, 1/d), a and d the previous centre's XX and YY, which leaves the
+centre's diagonal at 1 and turns neighbours into gain ratios.  The network
+predicts a correction to the centre input (its output layer starts at zero,
+so the untrained net proposes the previous solution), and the proposal is
+mapped back by diag(a, d).  Neighbours beyond the band edge continue the line
+through the centre and the mirrored in-band neighbour (2 N_0 - N_-j), so an
+edge chanblock still sees its phase slope.
 """
 
 from __future__ import annotations
@@ -52,17 +59,57 @@ def gauge_align(sol_tc: np.ndarray, ref_tile: int = 0) -> np.ndarray:
     return s
 
 
-def features(prev_tc: np.ndarray) -> np.ndarray:
-    """[tile][chanblock][8] previous solutions -> [tile*chanblock][40] float32
-    (neighbours clamped at the band edges; NaN solutions replaced by the
-    identity)."""
+def _frame(p_aligned: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
+    """Complex XX and YY of each (tile, chanblock), 1 where unusable."""
+    a = p_aligned[..., 0] + 1j * p_aligned[..., 1]
+    d = p_aligned[..., 6] + 1j * p_aligned[..., 7]
+    ok = np.isfinite(a) & np.isfinite(d) & (np.abs(a) > 1e-6) & (np.abs(d) > 1e-6)
+    return np.where(ok, a, 1.0 + 0j), np.where(ok, d, 1.0 + 0j)
+
+
+def _scale_columns(p: np.ndarray, ca: np.ndarray, cd: np.ndarray) -> np.ndarray:
+    """J diag(ca, cd) for Jones [.., 8] = [xx, xy, yx, yy] (re, im)."""
+    c = p[..., 0::2] + 1j * p[..., 1::2]
+    c[..., 0] *= ca
+    c[..., 2] *= ca
+    c[..., 1] *= cd
+    c[..., 3] *= cd
+    out = np.empty(p.shape)
+    out[..., 0::2] = c.real
+    out[..., 1::2] = c.imag
+    return out
+
+
+def _aligned(prev_tc: np.ndarray) -> np.ndarray:
     p = gauge_align(prev_tc)
     bad = ~np.isfinite(p).all(axis=-1)
     p[bad] = [1, 0, 0, 0, 0, 0, 1, 0]
+    return p
+
+
+def features(prev_tc: np.ndarray) -> np.ndarray:
+    """[tile][chanblock][8] previous solutions -> [tile*chanblock][40] float32
+    in the frame of each previous centre gain (NaN solutions replaced by the
+    identity; out-of-band neighbours extrapolated through the centre)."""
+    p = _aligned(prev_tc)
     nt, nc = p.shape[:2]
-    idx = np.clip(np.arange(nc)[:, None] + np.arange(-NEIGHBOURS, NEIGHBOURS + 1)[None, :], 0, nc - 1)
-    f = p[:, idx, :].reshape(nt * nc, IN_DIM)
-    return np.ascontiguousarray(f, np.float32)
+    a, d = _frame(p)
+    ia, id_ = (1.0 / a)[:, :, None], (1.0 / d)[:, :, None]
+    chans = np.arange(nc)[:, None]
+    raw = chans + np.arange(-NEIGHBOURS, NEIGHBOURS + 1)[None, :]
+    n = _scale_columns(p[:, np.clip(raw, 0, nc - 1), :], ia, id_)
+    mirror = _scale_columns(p[:, np.clip(2 * chans - raw, 0, nc - 1), :], ia, id_)
+    outside = ((raw < 0) | (raw >= nc))[None, :, :, None]
+    n = np.where(outside, 2.0 * n[:, :, NEIGHBOURS:NEIGHBOURS + 1, :] - mirror, n)
+    return np.ascontiguousarray(n.reshape(nt * nc, IN_DIM), np.float32)
+
+
+def targets(prev_tc: np.ndarray, cur_tc: np.ndarray) -> np.ndarray:
+    """The current timeblock's aligned solutions in the frame of the previous
+    centre gains: [tile*chanblock][8] float32 training targets."""
+    a, d = _frame(_aligned(prev_tc))
+    t = _scale_columns(gauge_align(cur_tc), 1.0 / a, 1.0 / d)
+    return np.ascontiguousarray(t.reshape(-1, OUT_DIM), np.float32)
 
 
 class WarmStartMLP:
@@ -115,8 +162,11 @@ class WarmStartMLP:
         return loss.value, g
 
     def train(self, X: np.ndarray, Y: np.ndarray, epochs: int = 20, batch: int = 4096, lr: float = 1e-3,
-              seed: int = 0) -> List[float]:
-        """Mini-batch Adam on the device (inputs moved to HBM once)."""
+              seed: int = 0, schedule: str = "cosine") -> List[float]:
+        """Mini-batch Adam on the device (inputs moved to HBM once).  The
+        learning rate follows a cosine from lr down to lr/100 over the run
+        ("cosine") or stays at lr ("constant"); the decay makes the final fit
+        insensitive to the seed and to rounding differences between runs."""
         import torch
 
         d_x = torch.from_numpy(np.ascontiguousarray(X, np.float32)).cuda()
@@ -125,17 +175,23 @@ class WarmStartMLP:
         rng = np.random.default_rng(seed)
         lib = _lib.lib()
         loss = ctypes.c_double()
+        total = max(epochs * (n // batch), 1)
+        step = 0
         for ep in range(epochs):
             perm = torch.from_numpy(rng.permutation(n)).cuda()
             xs, ys = d_x[perm], d_y[perm]
             tot, cnt = 0.0, 0
             for b0 in range(0, n - batch + 1, batch):
+                rate = lr
+                if schedule == "cosine":
+                    rate = lr * (0.01 + 0.99 * 0.5 * (1.0 + np.cos(np.pi * step / total)))
                 bx = xs[b0:b0 + batch].contiguous()
                 by = ys[b0:b0 + batch].contiguous()
-                _lib.check(lib.hdc_mlp_train_step(self._h, bx.data_ptr(), by.data_ptr(), batch, float(lr),
+                _lib.check(lib.hdc_mlp_train_step(self._h, bx.data_ptr(), by.data_ptr(), batch, float(rate),
                                                   ctypes.byref(loss), _stream_ptr(None)), "hdc_mlp_train_step")
                 tot += loss.value
                 cnt += 1
+                step += 1
             self.losses.append(tot / max(cnt, 1))
         return self.losses
 
@@ -148,7 +204,8 @@ class WarmStartMLP:
         y = torch.empty((x.shape[0], OUT_DIM), dtype=torch.float32, device="cuda")
         self.forward_device(x, y)
         torch.cuda.synchronize()
-        return y.cpu().numpy().astype(np.float64).reshape(nt, nc, OUT_DIM)
+        a, d = _frame(_aligned(prev_tc))
+        return _scale_columns(y.cpu().numpy().astype(np.float64).reshape(nt, nc, OUT_DIM), a, d)
 
     # ---------------------------------------------- persistence
     MAGIC = b"HDCMLP01"
@@ -232,7 +289,8 @@ def calibrate_warm(d_data, d_model, timeblock, prev_tc: Optional[np.ndarray], ml
 class DriftSky:
     """Seeded synthetic calibration sequence: per-tile gains with a phase slope
     in frequency and a phase that drifts between timeblocks in proportion to
-    the slope (a drifting delay), plus small amplitude jitter."""
+    the slope (a drifting delay), plus small amplitude jitter, over a
+    polarised random model (synth.polarised_model)."""
 
     ntiles: int
     nch: int
@@ -243,6 +301,8 @@ class DriftSky:
     chan_mhz: float = 0.04
     drift_per_block: float = 0.15
     snr: Optional[float] = None
+    cross_pol: float = 0.3
+    amp_jitter: float = 0.0005
 
     def generate(self):
         from . import synth
@@ -260,13 +320,13 @@ class DriftSky:
             # phase(f, b) = phi0 + slope (f + b drift): the delay behind the
             # slope moves the phase by slope * drift per timeblock
             ph = phi0[:, None, :] + slope[:, None, :] * (f[None, :, None] + b * self.drift_per_block)
-            amp = amp0[:, None, :] * (1.0 + 0.002 * rng.normal(size=(self.ntiles, 1, 2)))
+            amp = amp0[:, None, :] * (1.0 + self.amp_jitter * rng.normal(size=(self.ntiles, 1, 2)))
             g[..., 0] = amp[..., 0] * np.cos(ph[..., 0])
             g[..., 1] = amp[..., 0] * np.sin(ph[..., 0])
             g[..., 6] = amp[..., 1] * np.cos(ph[..., 1])
             g[..., 7] = amp[..., 1] * np.sin(ph[..., 1])
             g[..., 2:6] = leak
-            model = synth.random_model(self.nt_per_block, self.nch, nbl, rng)
+            model = synth.polarised_model(self.nt_per_block, self.nch, nbl, rng, self.cross_pol)
             data = synth.corrupt(model, g, rng, self.snr)
             blocks.append((data, model, g))
         return blocks

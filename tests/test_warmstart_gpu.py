@@ -77,47 +77,49 @@ def solve_sequence(blocks, mlp, tight):
     return sols, iters, chose
 
 
-def test_trained_warm_start_saves_iterations_and_reaches_the_fixed_point():
-    """From an identity start with U(-pi, pi) phases the MitchCal iteration
-    often stalls in a slow cycle (precision ~1e-7 for hundreds of iterations,
-    still 'converged' under min_threshold 1e-4); started from the trained
-    network's judged proposal it reaches the solver's fixed point (the
-    solution obtained from the true gains) in a few iterations.  Both arms use
-    the reference's default thresholds (50 iterations, stop 1e-8)."""
+def test_trained_warm_start_halves_iterations_to_the_same_solutions():
+    """Both arms run the unchanged MitchCal iteration to stop 1e-15 (tight
+    enough that each lands within 1e-6 of the solver's fixed point: the
+    iteration converges linearly, and at the default stop 1e-8 a solution can
+    still be ~1e-3 from it).  The trained network's judged start must reach
+    the same solutions (within 1e-6, gauge-aligned) in at most half the
+    iterations summed over chanblocks."""
     ntiles, nch = 24, 48
-    default = (50, 1e-8)
+    tight = (400, 1e-15)
     X, Y = [], []
     for seed in range(6):
-        blocks = ws.DriftSky(ntiles, nch, 2, 3, seed=100 + seed, snr=None).generate()
-        sols, _, _ = solve_sequence(blocks, None, default)
+        blocks = ws.DriftSky(ntiles, nch, 2, 3, seed=100 + seed).generate()
+        sols, _, _ = solve_sequence(blocks, None, tight)
         for k in range(1, len(sols)):
             X.append(ws.features(sols[k - 1]))
-            Y.append(ws.gauge_align(sols[k]).reshape(-1, 8).astype(np.float32))
+            Y.append(ws.targets(sols[k - 1], sols[k]))
     X, Y = np.concatenate(X), np.concatenate(Y)
     ok = np.isfinite(X).all(axis=1) & np.isfinite(Y).all(axis=1)
     mlp = ws.WarmStartMLP(hidden=128, num_hidden=3, seed=0)
     losses = mlp.train(X[ok], Y[ok], epochs=60, batch=256, lr=1e-3)
-    assert losses[-1] < losses[0]
+    assert losses[-1] < 0.01 * losses[0], losses
 
-    blocks = ws.DriftSky(ntiles, nch, 2, 4, seed=999, snr=None).generate()
-    s_id, it_id, _ = solve_sequence(blocks, None, default)
-    s_ws, it_ws, chose = solve_sequence(blocks, mlp, default)
+    blocks = ws.DriftSky(ntiles, nch, 2, 4, seed=999).generate()
+    s_id, it_id, _ = solve_sequence(blocks, None, tight)
+    s_ws, it_ws, chose = solve_sequence(blocks, mlp, tight)
     assert np.mean(np.concatenate(chose[1:])) > 0.8
     total_id = sum(int(i.sum()) for i in it_id[1:])
     total_ws = sum(int(i.sum()) for i in it_ws[1:])
-    assert total_ws < 0.5 * total_id, (total_ws, total_id)
-    # fixed point of the solver for each timeblock: solve from the true gains
+    assert 2 * total_ws <= total_id, (total_ws, total_id)
+    worst_id = max(int(i.max()) for i in it_id[1:])
+    worst_ws = max(int(i.max()) for i in it_ws[1:])
+    assert worst_ws < worst_id, (worst_ws, worst_id)
     for k, (data, model, g) in enumerate(blocks[1:], start=1):
+        # the solver's fixed point: iterate from the true gains
         d, m = torch.from_numpy(data).cuda(), torch.from_numpy(model).cuda()
         dj = torch.from_numpy(g.copy()).cuda()
-        cal.calibrate_timeblock(d, m, dj, (0, data.shape[0]), 50, 1e-20, 1e-4)
+        cal.calibrate_timeblock(d, m, dj, (0, data.shape[0]), 60, 1e-30, 1e-4)
         fp = ws.gauge_align(dj.cpu().numpy())
-        w = ws.gauge_align(s_ws[k])
-        i = ws.gauge_align(s_id[k])
-        err_ws = np.max(np.abs(w - fp)) / np.max(np.abs(fp))
-        err_id = np.max(np.abs(i - fp)) / np.max(np.abs(fp))
-        assert err_ws < 1e-6, (k, err_ws, err_id)
-        assert err_ws <= err_id + 1e-12
+        scale = np.max(np.abs(fp))
+        w, i = ws.gauge_align(s_ws[k]), ws.gauge_align(s_id[k])
+        assert np.max(np.abs(w - i)) / scale < 1e-6, k
+        assert np.max(np.abs(w - fp)) / scale < 1e-6, k
+        assert np.max(np.abs(i - fp)) / scale < 1e-6, k
 
 
 def test_fallback_to_identity_when_proposal_is_worse():
