@@ -19,28 +19,35 @@
 // accumulators), where every sum is exact:
 //   x = rint(X sx), |x| < 2^31 - 2^24 (sx from the channel's largest |W|):
 //       x = d0 2^24 + d1 2^16 + d2 2^8 + d3, every d_i in [-128, 127];
-//   y = rint(A sy), |y| < 2^23 - 2^16: y = e0 2^16 + e1 2^8 + e2.
+//   y = rint(A sy), |y| < 2^22: y = e0 2^16 + e1 2^8 + e2.
 // Balanced digits are the bytes of (x + 0x808080) ^ 0x808080: adding 128 to
 // each lower digit position and flipping its top bit turns excess-128 bytes
-// into two's-complement ones.  They have zero mean, so the products left out
+// into two's-complement ones (the flip is applied to four digits of a byte
+// plane at once).  They have zero mean, so the products left out
 // below do not bias the sum (unsigned lower bytes would: their dropped
 // products are all positive and grow with the number of components).
 // x y = sum_ij d_i e_j 2^(40 - 8(i + j)); the nine plane products with
 // i + j <= 3 are kept (the rest weigh < 2^-30 of full scale), each into the
 // accumulator of its class w = i + j, and the epilogue forms
 // V = sum_w D_w 2^(40 - 8w) / (sx sy) in FP64.  The only rounding is in the
-// inputs: the FP64-reduced phase, FP32 sincospi with a first-order
-// correction for the low part of the phase, X = W A in FP32, and the two
-// roundings to integers (2^-24 of A, 2^-31 of the channel's largest |X|).
-// A launch covers at most KPASS components, so no s32 sum can overflow.
+// inputs: the phase, reduced exactly in FP64 to a quadrant q and a remainder
+// r in [-1/2, 1/2] quarter-turns; sin and cos of (pi/2) r from FP32
+// polynomials (least-squares fits, mwa_hyperdrive_b200/phasor_poly.py,
+// < 0.75 ulp); X = W A in FP32; the two roundings to integers (2^-23 of A,
+// 2^-31 of the channel's largest |X|).  A launch covers at most KPASS
+// components, so no s32 sum can overflow.
 //
 // Kernel: one CTA per (channel, polarisation, half of the tile columns); M =
-// 128 tiles (rows of X), N = 64 tiles (rows of Y), K = 32 components per
-// stage.  Eight producer warps compute the per-tile phases (exact FP64 turn
-// reduction), X and Y, the byte planes, and write them to shared memory in
-// the K-major core-matrix layout; one thread issues the 36 MMAs of a stage
-// (9 plane pairs x 4 real products) into 8 TMEM accumulators (4 classes x
-// re/im, 64 columns each = all 512 columns).  Four stages let the producers
+// 128 tiles (rows of X), 64 tile columns (rows of Y), K = 32 components per
+// stage.  Sixteen producer warps compute the per-tile phasors, X and Y, the
+// byte planes, and write them to shared memory in the K-major core-matrix
+// layout (two lanes per 16-byte core-matrix row); the stage's component data
+// (l, m, n, W) is staged in shared memory one stage ahead, so the phasor loop
+// reads no global memory.  One thread issues the 18 MMAs of a stage (9 plane
+// pairs x {Xr, Xi}, N = 128 = [Re | Im] of the 64 columns, which keeps the
+// operand bytes read from shared memory per MAC at half of what separate
+// N = 64 products would need) into 4 TMEM accumulators (one per class, 128
+// columns each = all 512 columns).  Four stages let the producers
 // run ahead of the tensor core.  The epilogue reads TMEM with tcgen05.ld,
 // combines the classes in FP64 and adds the baselines of its columns into
 // the visibilities (XX, YY: q > p; XY: q > p as XY, q < p as YX = conj).
@@ -57,11 +64,14 @@ namespace hdc {
 namespace tc {
 
 constexpr int NT = 128;    // tiles = M
-constexpr int NH = 64;     // tile columns per CTA = N
+constexpr int NH = 64;     // tile columns per CTA
+constexpr int NB = 2 * NH; // MMA N: [Re | Im] of the NH columns
 constexpr int KC = 32;     // components per stage = MMA K (bytes)
 constexpr int NSTAGE = 4;
-constexpr int NPW = 8;     // producer / epilogue warps
-constexpr int THREADS = (NPW + 1) * 32;
+constexpr int NPW = 16;    // producer / epilogue warps
+constexpr int NPT = NPW * 32;   // producer threads
+constexpr int THREADS = NPT + 32;
+constexpr int CPT = 8;     // components per producer thread per stage
 constexpr int XDIG = 4;    // byte planes of x
 constexpr int YDIG = 3;    // byte planes of y
 constexpr int XT_BYTES = NT * KC;                           // one X plane tile, 4 KB
@@ -71,9 +81,29 @@ constexpr int STAGE_BYTES = Y_OFF + 3 * YDIG * YT_BYTES;    // Y: [re, im, -im][
 constexpr int SMEM_BYTES = NSTAGE * STAGE_BYTES + 1024;
 constexpr int LBO = 128;             // bytes between the two 16-byte K core matrices of a row group
 constexpr int SBO = (KC / 16) * 128; // bytes between 8-row groups
-constexpr int TMEM_COLS = 512;       // 4 classes x (re, im) x NH
+constexpr int TMEM_COLS = 512;       // 4 classes x NB
 constexpr int KPASS = 16384;         // components per launch: 3 pairs x 2 x 2^14 x KPASS < 2^31
-constexpr float SY = 8257536.0f;     // 2^23 - 2^17: |A| <= 1 -> y + 0x8080 < 2^23
+constexpr float SY = 4128768.0f;     // 2^22 - 2^16: |A| <= 1 -> |y| < 2^22
+constexpr double QMAGIC = 6755399441055744.0;  // 1.5 * 2^52: adding it rounds to an integer held in the low word
+// y + 0x8080 as FP32 bits: 1.5 * 2^23 rounds |v| < 2^22 to an integer in
+// the mantissa; the extra 0x8080 is the balancing offset of the two lower
+// digits.  The mantissa field then holds 2^22 + 0x8080 + y, so byte 2 is the
+// top digit + 0x40 and bytes 1, 0 the excess-128 lower digits.
+constexpr float YOFF = 12582912.0f + 32896.0f;
+
+// sin(pi/2 r) / r and cos(pi/2 r) in powers of r^2 on |r| <= 1/2
+// (mwa_hyperdrive_b200/phasor_poly.py)
+constexpr float PS0 = 1.570796371e+00f, PS1 = -6.459640861e-01f, PS2 = 7.969257981e-02f,
+                PS3 = -4.681266379e-03f, PS4 = 1.582065161e-04f;
+constexpr float PC0 = 1.000000000e+00f, PC1 = -1.233700514e+00f, PC2 = 2.536695004e-01f,
+                PC3 = -2.086346783e-02f, PC4 = 9.191617719e-04f, PC5 = -2.485098776e-05f;
+
+// component data of one stage, staged in shared memory (structure of arrays
+// so that 16-byte loads of consecutive components are conflict-free)
+struct CompStage {
+    double l[KC], m[KC], n[KC];  // turn units (n - 1 in n)
+    float2 w[KC];                // W of this polarisation
+};
 
 struct Params {
     int nf, nbl, ntiles, nc, c0, cn;
@@ -96,13 +126,7 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
 // kind::i8 instruction descriptor: s32 D (bits 4-5 = 2), A and B signed
 // (bits 7 and 10 = 1), K-major, N at bit 17 (>> 3), M at bit 24 (>> 4).
 __host__ __device__ constexpr uint32_t idesc_s8() {
-    return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NH >> 3) << 17) | ((uint32_t)(NT >> 4) << 24);
-}
-
-// integer whose bytes are the balanced base-256 digits of v (lower `low`
-// positions rebalanced, the top byte keeps the sign)
-__device__ __forceinline__ int balanced(int v, uint32_t low) {
-    return (int)(((uint32_t)v + low) ^ low);
+    return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NB >> 3) << 17) | ((uint32_t)(NT >> 4) << 24);
 }
 
 __device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t id, uint32_t acc) {
@@ -140,12 +164,12 @@ __device__ __forceinline__ uint32_t chunk_off(int row, int khalf) {
     return (uint32_t)((row >> 3) * SBO + khalf * LBO + (row & 7) * 16);
 }
 
-// Byte planes of 16 integers: plane b (byte b of every v[j]) as 16 bytes, v[j]
+// Byte planes of 8 integers: plane b (byte b of every v[j]) as 8 bytes, v[j]
 // at byte j.  A 4x4 byte transpose per group of four.
-__device__ __forceinline__ void byte_planes(const int* v, uint4* planes, int nplanes) {
-    uint32_t w[4][4];  // [plane][group]
+__device__ __forceinline__ void byte_planes8(const int* v, uint2* planes) {
+    uint32_t w[4][2];  // [plane][group]
 #pragma unroll
-    for (int g = 0; g < 4; g++) {
+    for (int g = 0; g < 2; g++) {
         const uint32_t a = (uint32_t)v[4 * g], b = (uint32_t)v[4 * g + 1], c = (uint32_t)v[4 * g + 2],
                        d = (uint32_t)v[4 * g + 3];
         const uint32_t t0 = __byte_perm(a, b, 0x5140), t1 = __byte_perm(c, d, 0x5140);
@@ -156,19 +180,64 @@ __device__ __forceinline__ void byte_planes(const int* v, uint4* planes, int npl
         w[3][g] = __byte_perm(t2, t3, 0x7632);
     }
 #pragma unroll
-    for (int b = 0; b < 4; b++)
-        if (b < nplanes) planes[b] = make_uint4(w[b][0], w[b][1], w[b][2], w[b][3]);
+    for (int b = 0; b < 4; b++) planes[b] = make_uint2(w[b][0], w[b][1]);
+}
+
+// per-byte corrections of four digits at once: excess-128 -> two's
+// complement, and b - 64 for bytes b in [0, 127] (b ^ 0x40 when bit 6 is
+// set, b ^ 0xC0 when it is clear; bit 6 moves to bit 7 inside its byte)
+__device__ __forceinline__ uint2 from_excess128(uint2 p) { return make_uint2(p.x ^ 0x80808080u, p.y ^ 0x80808080u); }
+__device__ __forceinline__ uint32_t minus64(uint32_t w) {
+    return w ^ 0x40404040u ^ ((~w & 0x40404040u) << 1);
+}
+__device__ __forceinline__ uint2 minus64(uint2 p) { return make_uint2(minus64(p.x), minus64(p.y)); }
+
+// sin and cos of 2 pi z for z in quarter-turns: q = rint(z) and r = z - q
+// exactly in FP64, then the FP32 polynomials on r and the quadrant q mod 4.
+__device__ __forceinline__ void phasor_quadrant(double z, float& sn, float& cs) {
+    const double zq = __dadd_rn(z, QMAGIC);
+    const int q = __double2loint(zq);
+    const float r = (float)__dsub_rn(z, __dsub_rn(zq, QMAGIC));
+    const float r2 = r * r;
+    float ps = fmaf(fmaf(fmaf(fmaf(PS4, r2, PS3), r2, PS2), r2, PS1), r2, PS0) * r;
+    float pc = fmaf(fmaf(fmaf(fmaf(fmaf(PC5, r2, PC4), r2, PC3), r2, PC2), r2, PC1), r2, PC0);
+    // angle = (pi/2)(q + r): odd q swaps sin and cos; sin takes the sign of
+    // bit 1 of q, cos that of bit 1 of q + 1 (moved to bit 31 by << 30)
+    const bool odd = q & 1;
+    const float a = odd ? pc : ps, b = odd ? ps : pc;
+    const uint32_t qs = (uint32_t)q << 30;
+    sn = __uint_as_float(__float_as_uint(a) ^ (qs & 0x80000000u));
+    cs = __uint_as_float(__float_as_uint(b) ^ ((qs + 0x40000000u) & 0x80000000u));
+}
+
+// all producer threads: barrier 1, true when any of them passed true
+__device__ __forceinline__ bool producers_sync_or(bool v) {
+    int r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.b32 p, %1, 0;\n\t"
+        "bar.red.or.pred q, 1, %2, p;\n\t"
+        "selp.b32 %0, 1, 0, q;\n\t}"
+        : "=r"(r)
+        : "r"((int)v), "r"(NPT)
+        : "memory");
+    return r != 0;
 }
 
 // shared-memory tile offsets inside a stage; digit 0 is the signed top byte
 __device__ __forceinline__ uint32_t x_tile(int part, int digit) {
     return (uint32_t)((part * XDIG + digit) * XT_BYTES);
 }
+// Y tiles of one digit lie in the order [Yi | Yr | -Yi] (64 rows each), so
+// that [Yr; -Yi] (from the Yr tile) and [Yi; Yr] (from the Yi tile) are
+// 128-row B operands: Xr [Yr; -Yi]^T + Xi [Yi; Yr]^T = [Re | Im] of X Y^H.
+// part: 0 = Yr, 1 = Yi, 2 = -Yi
 __device__ __forceinline__ uint32_t y_tile(int part, int digit) {
-    return (uint32_t)(Y_OFF + (part * YDIG + digit) * YT_BYTES);
+    const int slot = part == 0 ? 1 : (part == 1 ? 0 : 2);
+    return (uint32_t)(Y_OFF + (digit * 3 + slot) * YT_BYTES);
 }
-// TMEM column of accumulator (class w, re/im)
-__device__ __forceinline__ uint32_t acc_col(int w, int ri) { return (uint32_t)((w * 2 + ri) * NH); }
+// TMEM column of accumulator class w ([Re | Im], NB columns)
+__device__ __forceinline__ uint32_t acc_col(int w) { return (uint32_t)(w * NB); }
 
 template <bool OUT64>
 __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const Params P) {
@@ -177,6 +246,7 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const Params P) {
     __shared__ uint32_t tmem_base_s;
     __shared__ double red_s[THREADS / 32];
     __shared__ volatile int abort_s;
+    __shared__ __align__(16) CompStage comp_s[2];
 
     unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     const int f = blockIdx.x;
@@ -228,82 +298,115 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const Params P) {
 
     if (warp < NPW) {
         // ------------------------------------------------ producers
-        const int r = tid & (NT - 1);  // tile: row of X
-        const int khalf = tid >> 7;    // components [khalf * 16, khalf * 16 + 16) of a stage
+        // lanes in pairs: (row, which 8 of the 16 components in the row's
+        // 16-byte core-matrix chunk), so a warp stores 16 whole rows
+        const int h8 = tid & 1;
+        const int r = (tid >> 1) & (NT - 1);  // tile: row of X
+        const int kq = tid >> 8;              // components [kq * 16, kq * 16 + 16) of a stage
+        const int cbase = kq * 16 + h8 * CPT;
         const int yrow = r - hcol * NH;
         const bool real_tile = r < P.ntiles;
-        const bool in_y = real_tile && yrow >= 0 && yrow < NH;
-        double u = 0.0, v = 0.0, w = 0.0;
+        const bool y_row = yrow >= 0 && yrow < NH;
+        const bool in_y = real_tile && y_row;
+        double u = 0.0, v = 0.0, w = 0.0;  // quarter-turns per unit l, m, n - 1
         if (real_tile) {
             const XYZ x = P.xyzs[r];
-            const double ool = freq / VEL_C;
-            u = (P.s_ha * x.x + P.c_ha * x.y) * ool;
-            v = (-P.s_dec * P.c_ha * x.x + P.s_dec * P.s_ha * x.y + P.c_dec * x.z) * ool;
-            w = (P.c_dec * P.c_ha * x.x - P.c_dec * P.s_ha * x.y + P.s_dec * x.z) * ool;
+            const double oq = 4.0 * freq / VEL_C;
+            u = (P.s_ha * x.x + P.c_ha * x.y) * oq;
+            v = (-P.s_dec * P.c_ha * x.x + P.s_dec * P.s_ha * x.y + P.c_dec * x.z) * oq;
+            w = (P.c_dec * P.c_ha * x.x - P.c_dec * P.s_ha * x.y + P.s_dec * x.z) * oq;
         }
+        const double4* lmn = P.lmn + P.c0;
         const JonesF64* Wf = P.W + (size_t)f * P.nc + P.c0;
+        // tiles beyond the array get zero scales: their x and y are exactly 0
+        const float sxr = real_tile ? sx : 0.f;
+        const float syr = in_y ? SY : 0.f;
+        // the first KC threads fetch a stage's component data (zeros past the end)
+        auto fetch = [&](int k, double2& a, double2& b, double2& wd) {
+            const int c = k * KC + tid;
+            if (c < P.cn) {
+                a = __ldg(reinterpret_cast<const double2*>(lmn + c));
+                b = __ldg(reinterpret_cast<const double2*>(lmn + c) + 1);
+                wd = __ldg(reinterpret_cast<const double2*>(Wf + c) + wsel);
+            } else {
+                a = b = wd = make_double2(0.0, 0.0);
+            }
+        };
+        auto stash = [&](int buf, const double2& a, const double2& b, const double2& wd) {
+            comp_s[buf].l[tid] = a.x;
+            comp_s[buf].m[tid] = a.y;
+            comp_s[buf].n[tid] = b.x;
+            comp_s[buf].w[tid] = make_float2((float)wd.x, (float)wd.y);
+        };
+        if (tid < KC) {
+            double2 a, b, wd;
+            fetch(0, a, b, wd);
+            stash(0, a, b, wd);
+        }
+        producers_sync_or(false);
         for (int k = 0; k < nchunks; k++) {
             const int st = k % NSTAGE;
-            if (k >= NSTAGE) {
-                const bool ok = mbar_wait_bounded(&empty_bar[st], ((k / NSTAGE) - 1) & 1, P.err);
-                if (!ok) abort_s = 1;
-            }
-            if (abort_s) break;
-            int xr[16], xi[16], yr[16], yi[16], yn[16];
+            bool bad = false;
+            if (k >= NSTAGE) bad = !mbar_wait_bounded(&empty_bar[st], ((k / NSTAGE) - 1) & 1, P.err);
+            double2 na, nb, nw;  // next stage's component data, in flight during this stage
+            const bool pre = tid < KC && k + 1 < nchunks;
+            if (pre) fetch(k + 1, na, nb, nw);
+            int xr[CPT], xi[CPT], yr[CPT], yi[CPT], yn[CPT];
+            const CompStage& cs_ = comp_s[k & 1];
 #pragma unroll
-            for (int j = 0; j < 16; j++) {
-                const int c = k * KC + khalf * 16 + j;
-                xr[j] = xi[j] = yr[j] = yi[j] = yn[j] = 0;
-                if (c < P.cn && real_tile) {
-                    const double2 lm = __ldg(reinterpret_cast<const double2*>(P.lmn + P.c0 + c));
-                    const double ln = __ldg(reinterpret_cast<const double*>(P.lmn + P.c0 + c) + 2);
-                    const double t = u * lm.x + v * lm.y + w * ln;
-                    const double tr = 2.0 * (t - rint(t));  // half-turns in [-1, 1]
-                    const float th = (float)tr;
-                    const float tl = (float)(tr - (double)th);
-                    float s, co;
-                    sincospif(th, &s, &co);
-                    // sin, cos of pi (th + tl) to first order in tl (|tl| <= 2^-24)
-                    const float d = 3.14159265358979f * tl;
-                    const float s1 = fmaf(d, co, s);
-                    const float c1 = fmaf(-d, s, co);
-                    const double2 wd = __ldg(reinterpret_cast<const double2*>(Wf + c) + wsel);
-                    const float wr = (float)wd.x, wi = (float)wd.y;
-                    const float Xr = fmaf(wr, c1, -wi * s1);
-                    const float Xi = fmaf(wr, s1, wi * c1);
-                    xr[j] = balanced(__float2int_rn(Xr * sx), 0x808080u);
-                    xi[j] = balanced(__float2int_rn(Xi * sx), 0x808080u);
-                    if (in_y) {
-                        const int yi0 = __float2int_rn(s1 * SY);
-                        yr[j] = balanced(__float2int_rn(c1 * SY), 0x8080u);
-                        yi[j] = balanced(yi0, 0x8080u);
-                        yn[j] = balanced(-yi0, 0x8080u);
-                    }
+            for (int j2 = 0; j2 < CPT; j2 += 2) {
+                const double2 l2 = *reinterpret_cast<const double2*>(&cs_.l[cbase + j2]);
+                const double2 m2 = *reinterpret_cast<const double2*>(&cs_.m[cbase + j2]);
+                const double2 n2 = *reinterpret_cast<const double2*>(&cs_.n[cbase + j2]);
+                const float4 w2 = *reinterpret_cast<const float4*>(&cs_.w[cbase + j2]);
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const int j = j2 + h;
+                    const double cl = h ? l2.y : l2.x, cm = h ? m2.y : m2.x, cn = h ? n2.y : n2.x;
+                    const float wr = h ? w2.z : w2.x, wi = h ? w2.w : w2.y;
+                    float sn, cs;
+                    phasor_quadrant(u * cl + v * cm + w * cn, sn, cs);
+                    const float Xr = fmaf(wr, cs, -wi * sn);
+                    const float Xi = fmaf(wr, sn, wi * cs);
+                    // x + 0x808080 (balancing offset of the three lower digits)
+                    xr[j] = __float2int_rn(Xr * sxr) + 0x808080;
+                    xi[j] = __float2int_rn(Xi * sxr) + 0x808080;
+                    // y + 0x8080 + 0x400000 in the FP32 mantissa (one rounding)
+                    yr[j] = __float_as_int(__fmaf_rn(cs, syr, YOFF));
+                    yi[j] = __float_as_int(__fmaf_rn(sn, syr, YOFF));
+                    yn[j] = __float_as_int(__fmaf_rn(-sn, syr, YOFF));
                 }
             }
             unsigned char* sb = smem + st * STAGE_BYTES;
-            const uint32_t xo = chunk_off(r, khalf);
-            uint4 pl[4];
-            byte_planes(xr, pl, 4);
+            const uint32_t xo = chunk_off(r, kq) + h8 * 8;
+            uint2 pl[4];
+            // x planes: bytes 0-2 excess-128 lower digits, byte 3 the signed top digit
 #pragma unroll
-            for (int b = 0; b < 4; b++) *reinterpret_cast<uint4*>(sb + x_tile(0, 3 - b) + xo) = pl[b];
-            byte_planes(xi, pl, 4);
+            for (int part = 0; part < 2; part++) {
+                byte_planes8(part ? xi : xr, pl);
 #pragma unroll
-            for (int b = 0; b < 4; b++) *reinterpret_cast<uint4*>(sb + x_tile(1, 3 - b) + xo) = pl[b];
-            if (yrow >= 0 && yrow < NH) {
-                const uint32_t yo = chunk_off(yrow, khalf);
-                byte_planes(yr, pl, 3);
+                for (int b = 0; b < 4; b++)
+                    *reinterpret_cast<uint2*>(sb + x_tile(part, 3 - b) + xo) = b < 3 ? from_excess128(pl[b]) : pl[b];
+            }
+            // y planes: bytes 0-1 excess-128, byte 2 the top digit + 64
+            if (y_row) {
+                const uint32_t yo = chunk_off(yrow, kq) + h8 * 8;
 #pragma unroll
-                for (int b = 0; b < 3; b++) *reinterpret_cast<uint4*>(sb + y_tile(0, 2 - b) + yo) = pl[b];
-                byte_planes(yi, pl, 3);
-#pragma unroll
-                for (int b = 0; b < 3; b++) *reinterpret_cast<uint4*>(sb + y_tile(1, 2 - b) + yo) = pl[b];
-                byte_planes(yn, pl, 3);
-#pragma unroll
-                for (int b = 0; b < 3; b++) *reinterpret_cast<uint4*>(sb + y_tile(2, 2 - b) + yo) = pl[b];
+                for (int part = 0; part < 3; part++) {
+                    byte_planes8(part == 0 ? yr : (part == 1 ? yi : yn), pl);
+                    *reinterpret_cast<uint2*>(sb + y_tile(part, 2) + yo) = from_excess128(pl[0]);
+                    *reinterpret_cast<uint2*>(sb + y_tile(part, 1) + yo) = from_excess128(pl[1]);
+                    *reinterpret_cast<uint2*>(sb + y_tile(part, 0) + yo) = minus64(pl[2]);
+                }
             }
             fence_proxy_async_smem();  // make the generic-proxy stores visible to the tensor core
             mbar_arrive(&full_bar[st]);
+            if (pre) stash((k + 1) & 1, na, nb, nw);
+            // one decision for all producers: leave together on any timeout
+            if (producers_sync_or(bad || abort_s != 0)) {
+                abort_s = 1;
+                break;
+            }
         }
     } else {
         // ------------------------------------------------ MMA issuer (one thread)
@@ -319,21 +422,18 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const Params P) {
                 tc_fence_after();
                 const uint32_t sb = sbase + st * STAGE_BYTES;
                 uint32_t started = 0;  // accumulators written in this launch (first stage only)
+                const uint32_t id = idesc_s8();
                 for (int i = 0; i < XDIG; i++)
                     for (int j = 0; j < YDIG; j++) {
                         const int cls = i + j;
                         if (cls > 3) continue;
-                        const uint32_t id = idesc_s8();
-                        // (accumulator re/im, X part, Y part): Re += Xr Yr + Xi Yi, Im += Xi Yr + Xr (-Yi)
-                        const int prods[4][3] = {{0, 0, 0}, {0, 1, 1}, {1, 1, 0}, {1, 0, 2}};
-                        for (int q = 0; q < 4; q++) {
-                            const int ri = prods[q][0];
-                            const uint32_t bit = 1u << (cls * 2 + ri);
-                            const bool first = k == 0 && !(started & bit);
-                            started |= bit;
-                            mma_i8(tmem + acc_col(cls, ri), smem_desc(sb + x_tile(prods[q][1], i)),
-                                   smem_desc(sb + y_tile(prods[q][2], j)), id, first ? 0u : 1u);
-                        }
+                        const bool first = k == 0 && !(started & (1u << cls));
+                        started |= 1u << cls;
+                        // [Re | Im] += Xr [Yr; -Yi]^T + Xi [Yi; Yr]^T
+                        mma_i8(tmem + acc_col(cls), smem_desc(sb + x_tile(0, i)), smem_desc(sb + y_tile(0, j)), id,
+                               first ? 0u : 1u);
+                        mma_i8(tmem + acc_col(cls), smem_desc(sb + x_tile(1, i)), smem_desc(sb + y_tile(1, j)), id,
+                               1u);
                     }
                 mma_commit(&empty_bar[st]);  // stage free once these MMAs have read it
             }
@@ -348,14 +448,15 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const Params P) {
     tc_fence_after();
     if (!aborted && ok && warp < NPW && nchunks > 0) {
         const int lg = warp & 3;       // TMEM lane group this warp may access
-        const int chalf = warp >> 2;   // column half of the NH columns
+        const int cq = warp >> 2;      // quarter of the NH columns
         const int p = lg * 32 + lane;  // row: tile p
         const uint32_t lane_addr = tmem + ((uint32_t)(lg * 32) << 16);
         const int n = P.ntiles;
-        for (int c0 = chalf * (NH / 2); c0 < chalf * (NH / 2) + NH / 2; c0 += 8) {
+        for (int c0 = cq * (NH / 4); c0 < cq * (NH / 4) + NH / 4; c0 += 8) {
             int a[8][8];  // [class * 2 + re/im][column]
 #pragma unroll
-            for (int g = 0; g < 8; g++) tmem_ld8(lane_addr + (uint32_t)(g * NH + c0), a[g]);
+            for (int g = 0; g < 8; g++)  // g = class * 2 + (0 Re, 1 Im)
+                tmem_ld8(lane_addr + acc_col(g >> 1) + (uint32_t)((g & 1) * NH + c0), a[g]);
             tmem_wait_ld();
             if (p >= n) continue;
 #pragma unroll
