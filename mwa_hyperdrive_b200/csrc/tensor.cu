@@ -33,7 +33,7 @@
 // inputs: the phase, reduced exactly in FP64 to a quadrant q and a remainder
 // r in [-1/2, 1/2] quarter-turns; sin and cos of (pi/2) r from FP32
 // polynomials (least-squares fits, mwa_hyperdrive_b200/phasor_poly.py,
-// < 0.75 ulp); X = W A in FP32; the two roundings to integers (2^-23 of A,
+// < 0.75 ulp); X = (W sx) A in FP32; the two roundings to integers (2^-23 of A,
 // 2^-31 of the channel's largest |X|).  A launch covers at most KPASS
 // components, so no s32 sum can overflow.
 //
@@ -41,7 +41,7 @@
 // 128 tiles (rows of X), 64 tile columns (rows of Y), K = 32 components per
 // stage.  Sixteen producer warps compute the per-tile phasors, X and Y, the
 // byte planes, and write them to shared memory in the K-major core-matrix
-// layout (two lanes per 16-byte core-matrix row); the stage's component data
+// layout (one warp store = one 128-byte core matrix); the stage's component data
 // (l, m, n, W) is staged in shared memory one stage ahead, so the phasor loop
 // reads no global memory.  One thread issues the 18 MMAs of a stage (9 plane
 // pairs x {Xr, Xi}, N = 128 = [Re | Im] of the 64 columns, which keeps the
@@ -71,7 +71,6 @@ constexpr int NSTAGE = 4;
 constexpr int NPW = 16;    // producer / epilogue warps
 constexpr int NPT = NPW * 32;   // producer threads
 constexpr int THREADS = NPT + 32;
-constexpr int CPT = 8;     // components per producer thread per stage
 constexpr int XDIG = 4;    // byte planes of x
 constexpr int YDIG = 3;    // byte planes of y
 constexpr int XT_BYTES = NT * KC;                           // one X plane tile, 4 KB
@@ -93,16 +92,16 @@ constexpr float YOFF = 12582912.0f + 32896.0f;
 
 // sin(pi/2 r) / r and cos(pi/2 r) in powers of r^2 on |r| <= 1/2
 // (mwa_hyperdrive_b200/phasor_poly.py)
-constexpr float PS0 = 1.570796371e+00f, PS1 = -6.459640861e-01f, PS2 = 7.969257981e-02f,
-                PS3 = -4.681266379e-03f, PS4 = 1.582065161e-04f;
-constexpr float PC0 = 1.000000000e+00f, PC1 = -1.233700514e+00f, PC2 = 2.536695004e-01f,
-                PC3 = -2.086346783e-02f, PC4 = 9.191617719e-04f, PC5 = -2.485098776e-05f;
+constexpr float PS0 = 1.570796371e+00f, PS1 = -6.459634900e-01f, PS2 = 7.968021929e-02f,
+                PS3 = -4.602163099e-03f;
+constexpr float PC0 = 1.000000000e+00f, PC1 = -1.233700514e+00f, PC2 = 2.536692023e-01f,
+                PC3 = -2.086007036e-02f, PC4 = 9.036298725e-04f;
 
 // component data of one stage, staged in shared memory (structure of arrays
 // so that 16-byte loads of consecutive components are conflict-free)
 struct CompStage {
     double l[KC], m[KC], n[KC];  // turn units (n - 1 in n)
-    float2 w[KC];                // W of this polarisation
+    float2 w[KC];                // W of this polarisation times the x scale sx
 };
 
 struct Params {
@@ -164,33 +163,25 @@ __device__ __forceinline__ uint32_t chunk_off(int row, int khalf) {
     return (uint32_t)((row >> 3) * SBO + khalf * LBO + (row & 7) * 16);
 }
 
-// Byte planes of 8 integers: plane b (byte b of every v[j]) as 8 bytes, v[j]
-// at byte j.  A 4x4 byte transpose per group of four.
-__device__ __forceinline__ void byte_planes8(const int* v, uint2* planes) {
-    uint32_t w[4][2];  // [plane][group]
-#pragma unroll
-    for (int g = 0; g < 2; g++) {
-        const uint32_t a = (uint32_t)v[4 * g], b = (uint32_t)v[4 * g + 1], c = (uint32_t)v[4 * g + 2],
-                       d = (uint32_t)v[4 * g + 3];
-        const uint32_t t0 = __byte_perm(a, b, 0x5140), t1 = __byte_perm(c, d, 0x5140);
-        const uint32_t t2 = __byte_perm(a, b, 0x7362), t3 = __byte_perm(c, d, 0x7362);
-        w[0][g] = __byte_perm(t0, t1, 0x5410);
-        w[1][g] = __byte_perm(t0, t1, 0x7632);
-        w[2][g] = __byte_perm(t2, t3, 0x5410);
-        w[3][g] = __byte_perm(t2, t3, 0x7632);
-    }
-#pragma unroll
-    for (int b = 0; b < 4; b++) planes[b] = make_uint2(w[b][0], w[b][1]);
+// Byte planes of 4 integers: word b holds byte b of v[0..3], v[j] at byte j
+// (a 4x4 byte transpose).
+__device__ __forceinline__ void byte_planes4(const int* v, uint32_t* w) {
+    const uint32_t a = (uint32_t)v[0], b = (uint32_t)v[1], c = (uint32_t)v[2], d = (uint32_t)v[3];
+    const uint32_t t0 = __byte_perm(a, b, 0x5140), t1 = __byte_perm(c, d, 0x5140);
+    const uint32_t t2 = __byte_perm(a, b, 0x7362), t3 = __byte_perm(c, d, 0x7362);
+    w[0] = __byte_perm(t0, t1, 0x5410);
+    w[1] = __byte_perm(t0, t1, 0x7632);
+    w[2] = __byte_perm(t2, t3, 0x5410);
+    w[3] = __byte_perm(t2, t3, 0x7632);
 }
 
-// per-byte corrections of four digits at once: excess-128 -> two's
-// complement, and b - 64 for bytes b in [0, 127] (b ^ 0x40 when bit 6 is
-// set, b ^ 0xC0 when it is clear; bit 6 moves to bit 7 inside its byte)
-__device__ __forceinline__ uint2 from_excess128(uint2 p) { return make_uint2(p.x ^ 0x80808080u, p.y ^ 0x80808080u); }
+// per-byte correction of four digits at once: b - 64 for bytes b in [0, 127]
+// (b ^ 0x40 when bit 6 is set, b ^ 0xC0 when it is clear; bit 6 moves to
+// bit 7 inside its byte).  Excess-128 digits become two's complement with
+// a plain XOR 0x80.
 __device__ __forceinline__ uint32_t minus64(uint32_t w) {
     return w ^ 0x40404040u ^ ((~w & 0x40404040u) << 1);
 }
-__device__ __forceinline__ uint2 minus64(uint2 p) { return make_uint2(minus64(p.x), minus64(p.y)); }
 
 // sin and cos of 2 pi z for z in quarter-turns: q = rint(z) and r = z - q
 // exactly in FP64, then the FP32 polynomials on r and the quadrant q mod 4.
@@ -199,8 +190,8 @@ __device__ __forceinline__ void phasor_quadrant(double z, float& sn, float& cs) 
     const int q = __double2loint(zq);
     const float r = (float)__dsub_rn(z, __dsub_rn(zq, QMAGIC));
     const float r2 = r * r;
-    float ps = fmaf(fmaf(fmaf(fmaf(PS4, r2, PS3), r2, PS2), r2, PS1), r2, PS0) * r;
-    float pc = fmaf(fmaf(fmaf(fmaf(fmaf(PC5, r2, PC4), r2, PC3), r2, PC2), r2, PC1), r2, PC0);
+    const float ps = fmaf(fmaf(fmaf(PS3, r2, PS2), r2, PS1), r2, PS0) * r;
+    const float pc = fmaf(fmaf(fmaf(fmaf(PC4, r2, PC3), r2, PC2), r2, PC1), r2, PC0);
     // angle = (pi/2)(q + r): odd q swaps sin and cos; sin takes the sign of
     // bit 1 of q, cos that of bit 1 of q + 1 (moved to bit 31 by << 30)
     const bool odd = q & 1;
@@ -266,7 +257,7 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const Params P) {
     if (lane == 0) red_s[warp] = mx;
     if (tid == 0) {
         for (int s = 0; s < NSTAGE; s++) {
-            mbar_init(&full_bar[s], NPW * 32);
+            mbar_init(&full_bar[s], 1);
             mbar_init(&empty_bar[s], 1);
         }
         mbar_init(&done_bar, 1);
@@ -298,29 +289,34 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const Params P) {
 
     if (warp < NPW) {
         // ------------------------------------------------ producers
-        // lanes in pairs: (row, which 8 of the 16 components in the row's
-        // 16-byte core-matrix chunk), so a warp stores 16 whole rows
-        const int h8 = tid & 1;
-        const int r = (tid >> 1) & (NT - 1);  // tile: row of X
-        const int kq = tid >> 8;              // components [kq * 16, kq * 16 + 16) of a stage
-        const int cbase = kq * 16 + h8 * CPT;
-        const int yrow = r - hcol * NH;
-        const bool real_tile = r < P.ntiles;
-        const bool y_row = yrow >= 0 && yrow < NH;
-        const bool in_y = real_tile && y_row;
-        double u = 0.0, v = 0.0, w = 0.0;  // quarter-turns per unit l, m, n - 1
-        if (real_tile) {
-            const XYZ x = P.xyzs[r];
-            const double oq = 4.0 * freq / VEL_C;
-            u = (P.s_ha * x.x + P.c_ha * x.y) * oq;
-            v = (-P.s_dec * P.c_ha * x.x + P.s_dec * P.s_ha * x.y + P.c_dec * x.z) * oq;
-            w = (P.c_dec * P.c_ha * x.x - P.c_dec * P.s_ha * x.y + P.s_dec * x.z) * oq;
+        // warp = 8 tile rows x 16 components of a stage; lane = (row rl, quad of
+        // 4 components), and every thread also takes the row 64 tiles down, so a
+        // warp's store of one byte plane is one whole 128-byte core matrix and
+        // exactly one of a thread's two rows lies in this CTA's Y half
+        const int g = warp & 7;             // rows 8g .. 8g + 7 (and + 64)
+        const int kq = warp >> 3;           // components [kq * 16, kq * 16 + 16) of a stage
+        const int rl = lane >> 2, quad = lane & 3;
+        const int cb = kq * 16 + quad * 4;  // this thread's 4 components
+        const int r0 = 8 * g + rl;          // rows r0 and r0 + 64; Y row r0 of tile r0 + 64 hcol
+        const int ry = hcol;                // which of the two rows is the Y row
+        // Rows of tiles beyond the array get phase 0 (bounded values, so no
+        // s32 sum can overflow): their products only reach rows and columns
+        // of the accumulators that the epilogue never writes out.
+        double u[2], v[2], w[2];            // quarter-turns per unit l, m, n - 1
+#pragma unroll
+        for (int s2 = 0; s2 < 2; s2++) {
+            const int r = r0 + 64 * s2;
+            u[s2] = v[s2] = w[s2] = 0.0;
+            if (r < P.ntiles) {
+                const XYZ x = P.xyzs[r];
+                const double oq = 4.0 * freq / VEL_C;
+                u[s2] = (P.s_ha * x.x + P.c_ha * x.y) * oq;
+                v[s2] = (-P.s_dec * P.c_ha * x.x + P.s_dec * P.s_ha * x.y + P.c_dec * x.z) * oq;
+                w[s2] = (P.c_dec * P.c_ha * x.x - P.c_dec * P.s_ha * x.y + P.s_dec * x.z) * oq;
+            }
         }
         const double4* lmn = P.lmn + P.c0;
         const JonesF64* Wf = P.W + (size_t)f * P.nc + P.c0;
-        // tiles beyond the array get zero scales: their x and y are exactly 0
-        const float sxr = real_tile ? sx : 0.f;
-        const float syr = in_y ? SY : 0.f;
         // the first KC threads fetch a stage's component data (zeros past the end)
         auto fetch = [&](int k, double2& a, double2& b, double2& wd) {
             const int c = k * KC + tid;
@@ -336,7 +332,7 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const Params P) {
             comp_s[buf].l[tid] = a.x;
             comp_s[buf].m[tid] = a.y;
             comp_s[buf].n[tid] = b.x;
-            comp_s[buf].w[tid] = make_float2((float)wd.x, (float)wd.y);
+            comp_s[buf].w[tid] = make_float2((float)(wd.x * (double)sx), (float)(wd.y * (double)sx));
         };
         if (tid < KC) {
             double2 a, b, wd;
@@ -346,64 +342,80 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const Params P) {
         producers_sync_or(false);
         for (int k = 0; k < nchunks; k++) {
             const int st = k % NSTAGE;
-            bool bad = false;
-            if (k >= NSTAGE) bad = !mbar_wait_bounded(&empty_bar[st], ((k / NSTAGE) - 1) & 1, P.err);
             double2 na, nb, nw;  // next stage's component data, in flight during this stage
             const bool pre = tid < KC && k + 1 < nchunks;
             if (pre) fetch(k + 1, na, nb, nw);
-            int xr[CPT], xi[CPT], yr[CPT], yi[CPT], yn[CPT];
             const CompStage& cs_ = comp_s[k & 1];
+            double cl[4], cm[4], cn[4];
+            float wr[4], wi[4];
 #pragma unroll
-            for (int j2 = 0; j2 < CPT; j2 += 2) {
-                const double2 l2 = *reinterpret_cast<const double2*>(&cs_.l[cbase + j2]);
-                const double2 m2 = *reinterpret_cast<const double2*>(&cs_.m[cbase + j2]);
-                const double2 n2 = *reinterpret_cast<const double2*>(&cs_.n[cbase + j2]);
-                const float4 w2 = *reinterpret_cast<const float4*>(&cs_.w[cbase + j2]);
-#pragma unroll
-                for (int h = 0; h < 2; h++) {
-                    const int j = j2 + h;
-                    const double cl = h ? l2.y : l2.x, cm = h ? m2.y : m2.x, cn = h ? n2.y : n2.x;
-                    const float wr = h ? w2.z : w2.x, wi = h ? w2.w : w2.y;
-                    float sn, cs;
-                    phasor_quadrant(u * cl + v * cm + w * cn, sn, cs);
-                    const float Xr = fmaf(wr, cs, -wi * sn);
-                    const float Xi = fmaf(wr, sn, wi * cs);
-                    // x + 0x808080 (balancing offset of the three lower digits)
-                    xr[j] = __float2int_rn(Xr * sxr) + 0x808080;
-                    xi[j] = __float2int_rn(Xi * sxr) + 0x808080;
-                    // y + 0x8080 + 0x400000 in the FP32 mantissa (one rounding)
-                    yr[j] = __float_as_int(__fmaf_rn(cs, syr, YOFF));
-                    yi[j] = __float_as_int(__fmaf_rn(sn, syr, YOFF));
-                    yn[j] = __float_as_int(__fmaf_rn(-sn, syr, YOFF));
-                }
+            for (int h = 0; h < 2; h++) {
+                const double2 l2 = *reinterpret_cast<const double2*>(&cs_.l[cb + 2 * h]);
+                const double2 m2 = *reinterpret_cast<const double2*>(&cs_.m[cb + 2 * h]);
+                const double2 n2 = *reinterpret_cast<const double2*>(&cs_.n[cb + 2 * h]);
+                const float4 w2 = *reinterpret_cast<const float4*>(&cs_.w[cb + 2 * h]);
+                cl[2 * h] = l2.x, cl[2 * h + 1] = l2.y;
+                cm[2 * h] = m2.x, cm[2 * h + 1] = m2.y;
+                cn[2 * h] = n2.x, cn[2 * h + 1] = n2.y;
+                wr[2 * h] = w2.x, wi[2 * h] = w2.y, wr[2 * h + 1] = w2.z, wi[2 * h + 1] = w2.w;
             }
+            int xr[2][4], xi[2][4], yr[4], yi[4], yn[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+#pragma unroll
+                for (int s2 = 0; s2 < 2; s2++) {
+                    float sn, cs;
+                    phasor_quadrant(u[s2] * cl[j] + v[s2] * cm[j] + w[s2] * cn[j], sn, cs);
+                    const float Xr = fmaf(wr[j], cs, -wi[j] * sn);
+                    const float Xi = fmaf(wr[j], sn, wi[j] * cs);
+                    // x + 0x808080 (balancing offset of the three lower digits)
+                    xr[s2][j] = __float2int_rn(Xr) + 0x808080;
+                    xi[s2][j] = __float2int_rn(Xi) + 0x808080;
+                    if (s2 == ry) {
+                        // y + 0x8080 + 0x400000 in the FP32 mantissa (one rounding)
+                        yr[j] = __float_as_int(__fmaf_rn(cs, SY, YOFF));
+                        yi[j] = __float_as_int(__fmaf_rn(sn, SY, YOFF));
+                        yn[j] = __float_as_int(__fmaf_rn(-sn, SY, YOFF));
+                    }
+                }
             unsigned char* sb = smem + st * STAGE_BYTES;
-            const uint32_t xo = chunk_off(r, kq) + h8 * 8;
-            uint2 pl[4];
+            uint32_t pl[4];
             // x planes: bytes 0-2 excess-128 lower digits, byte 3 the signed top digit
 #pragma unroll
-            for (int part = 0; part < 2; part++) {
-                byte_planes8(part ? xi : xr, pl);
+            for (int s2 = 0; s2 < 2; s2++) {
+                const uint32_t xo = chunk_off(r0 + 64 * s2, kq) + quad * 4;
 #pragma unroll
-                for (int b = 0; b < 4; b++)
-                    *reinterpret_cast<uint2*>(sb + x_tile(part, 3 - b) + xo) = b < 3 ? from_excess128(pl[b]) : pl[b];
+                for (int part = 0; part < 2; part++) {
+                    byte_planes4(part ? xi[s2] : xr[s2], pl);
+#pragma unroll
+                    for (int b = 0; b < 4; b++)
+                        *reinterpret_cast<uint32_t*>(sb + x_tile(part, 3 - b) + xo) = b < 3 ? pl[b] ^ 0x80808080u : pl[b];
+                }
             }
             // y planes: bytes 0-1 excess-128, byte 2 the top digit + 64
-            if (y_row) {
-                const uint32_t yo = chunk_off(yrow, kq) + h8 * 8;
+            {
+                const uint32_t yo = chunk_off(r0, kq) + quad * 4;
 #pragma unroll
                 for (int part = 0; part < 3; part++) {
-                    byte_planes8(part == 0 ? yr : (part == 1 ? yi : yn), pl);
-                    *reinterpret_cast<uint2*>(sb + y_tile(part, 2) + yo) = from_excess128(pl[0]);
-                    *reinterpret_cast<uint2*>(sb + y_tile(part, 1) + yo) = from_excess128(pl[1]);
-                    *reinterpret_cast<uint2*>(sb + y_tile(part, 0) + yo) = minus64(pl[2]);
+                    byte_planes4(part == 0 ? yr : (part == 1 ? yi : yn), pl);
+                    *reinterpret_cast<uint32_t*>(sb + y_tile(part, 2) + yo) = pl[0] ^ 0x80808080u;
+                    *reinterpret_cast<uint32_t*>(sb + y_tile(part, 1) + yo) = pl[1] ^ 0x80808080u;
+                    *reinterpret_cast<uint32_t*>(sb + y_tile(part, 0) + yo) = minus64(pl[2]);
                 }
             }
             fence_proxy_async_smem();  // make the generic-proxy stores visible to the tensor core
-            mbar_arrive(&full_bar[st]);
             if (pre) stash((k + 1) & 1, na, nb, nw);
-            // one decision for all producers: leave together on any timeout
-            if (producers_sync_or(bad || abort_s != 0)) {
+            // before the barrier, thread 0 waits until the next iteration's
+            // stage has been read by the tensor core; the barrier then both
+            // publishes this stage (one arrive on its full barrier) and frees
+            // everyone to write the next.  One decision for all producers:
+            // leave together on any timeout.
+            bool bad = false;
+            if (tid == 0 && k + 1 >= NSTAGE && k + 1 < nchunks)
+                bad = !mbar_wait_bounded(&empty_bar[(k + 1) % NSTAGE], (((k + 1) / NSTAGE) - 1) & 1, P.err);
+            const bool stop = producers_sync_or(bad || abort_s != 0);
+            if (tid == 0) mbar_arrive(&full_bar[st]);
+            if (stop) {
                 abort_s = 1;
                 break;
             }
@@ -412,6 +424,7 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const Params P) {
         // ------------------------------------------------ MMA issuer (one thread)
         if (lane == 0) {
             const uint32_t sbase = smem_u32(smem);
+            const uint32_t id = idesc_s8();
             for (int k = 0; k < nchunks; k++) {
                 const int st = k % NSTAGE;
                 const bool ok = mbar_wait_bounded(&full_bar[st], (k / NSTAGE) & 1, P.err);
@@ -420,20 +433,23 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const Params P) {
                     break;
                 }
                 tc_fence_after();
-                const uint32_t sb = sbase + st * STAGE_BYTES;
-                uint32_t started = 0;  // accumulators written in this launch (first stage only)
-                const uint32_t id = idesc_s8();
+                // straight-line issue: one base descriptor per stage plus
+                // compile-time tile offsets (in 16-byte units, the
+                // descriptor's address field); the first product of each
+                // class in the launch's first stage overwrites its accumulator
+                const uint64_t d0 = smem_desc(sbase + st * STAGE_BYTES);
+                const uint32_t acc0 = k > 0 ? 1u : 0u;
+#pragma unroll
                 for (int i = 0; i < XDIG; i++)
+#pragma unroll
                     for (int j = 0; j < YDIG; j++) {
                         const int cls = i + j;
                         if (cls > 3) continue;
-                        const bool first = k == 0 && !(started & (1u << cls));
-                        started |= 1u << cls;
+                        const bool first = (i == 0) || (i == 1 && j == 2);
                         // [Re | Im] += Xr [Yr; -Yi]^T + Xi [Yi; Yr]^T
-                        mma_i8(tmem + acc_col(cls), smem_desc(sb + x_tile(0, i)), smem_desc(sb + y_tile(0, j)), id,
-                               first ? 0u : 1u);
-                        mma_i8(tmem + acc_col(cls), smem_desc(sb + x_tile(1, i)), smem_desc(sb + y_tile(1, j)), id,
-                               1u);
+                        mma_i8(tmem + acc_col(cls), d0 + (x_tile(0, i) >> 4), d0 + (y_tile(0, j) >> 4), id,
+                               first ? acc0 : 1u);
+                        mma_i8(tmem + acc_col(cls), d0 + (x_tile(1, i) >> 4), d0 + (y_tile(1, j) >> 4), id, 1u);
                     }
                 mma_commit(&empty_bar[st]);  // stage free once these MMAs have read it
             }

@@ -4,8 +4,8 @@ tensor-core point predict (csrc/tensor.cu, `phasor_quadrant`).
 The phase enters as r in quarter-turns, |r| <= 1/2 after the quadrant is
 split off in FP64, so the polynomials approximate
 
-    sin(pi/2 r) = r   * (s0 + s1 r^2 + s2 r^4 + s3 r^6 + s4 r^8)
-    cos(pi/2 r) = c0 + c1 r^2 + c2 r^4 + c3 r^6 + c4 r^8 + c5 r^10
+    sin(pi/2 r) = r   * (s0 + s1 r^2 + s2 r^4 + s3 r^6)
+    cos(pi/2 r) = c0 + c1 r^2 + c2 r^4 + c3 r^6 + c4 r^8
 
 on [-1/2, 1/2].  Method: weighted least squares in float64 on Chebyshev
 nodes of r^2 (relative error weighting for sin), then rounding to float32;
@@ -21,8 +21,8 @@ from __future__ import annotations
 
 import numpy as np
 
-SIN_TERMS = 5
-COS_TERMS = 6
+SIN_TERMS = 4
+COS_TERMS = 5
 
 
 def fit():
