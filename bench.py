@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--channels", type=int, default=384, help="reduced case for profiling (default: full 384)")
     ap.add_argument("--timesteps", type=int, default=4, help="reduced case for profiling (default: full 4)")
     ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--skip-dical", action="store_true", help="leave out the DI-calibration measurement")
+    ap.add_argument("--dical-chanblocks", type=int, default=768, help="reduced DI-cal case for profiling")
     args = ap.parse_args()
     global SHAPE
     SHAPE = (args.channels, args.timesteps)
@@ -198,6 +200,116 @@ def cpu_baseline(obs, sky, seconds):
     return {"value": work / dt, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": f"1 timestep x {nch} channels x {sky.num_components} components x {obs.num_baselines} baselines "
                       f"({dt:.1f} s)"}
+
+
+# ------------------------------------------------------ DI calibration
+DICAL_WORKLOAD = ("DI calibration: 128 tiles (8128 baselines), 1 timeblock of 14 timesteps 8 s apart, 768 chanblocks "
+                  "of 40 kHz from 167 MHz; truth gains |g| ~ N(1, 0.1), phase U(-pi, pi), leakage N(0, 0.01); model "
+                  "predicted from 8000 points (lognormal(0, 1) Jy, 10 deg cap) through the analytic dipole-array beam "
+                  "(an unpolarised sky without a beam gives M proportional to I, for which full-Jones solutions are "
+                  "defined only up to a unitary factor and no chanblock converges); data = G M G^H + noise at "
+                  "per-visibility SNR 10; max 50 iterations, stop 1e-8, min 1e-4")
+
+
+def dical_workload(nch):
+    """Model and data [14][nch][8128][8] float32 on the device, and the truth gains."""
+    import torch
+
+    from mwa_hyperdrive_b200 import synth
+    from mwa_hyperdrive_b200 import srclist as sl
+    from mwa_hyperdrive_b200.model import SkyModeller
+
+    pc = (0.0, math.radians(-27.0))
+    nt = 14
+    lsts = pc[0] + np.arange(nt) * 8.0 * synth.SIDEREAL_RATE
+    obs = synth.Obs(synth.tiles_in_disk(128, 750.0, 3), 167.0e6 + np.arange(nch) * 40e3, pc, lsts)
+    sky = sl.SkyModelArrays.from_components(synth.point_sky(8000, pc, 10.0, 3))
+    nbl = obs.num_baselines
+    model = torch.zeros((nt, nch, nbl, 8), dtype=torch.float32, device="cuda")
+    m = SkyModeller(sky, obs.tile_xyzs, obs.freqs, pc, obs.latitude, beam="analytic", form="tensor")
+    for t in range(nt):
+        m.model_timestep_with(float(lsts[t]), model[t], return_uvws=False)
+    m.close()
+    rng = np.random.default_rng(3)
+    g = synth.truth_gains(128, nch, rng)  # [tile][chanblock][8]
+    gc = torch.from_numpy(g[..., 0::2] + 1j * g[..., 1::2]).to("cuda").reshape(128, nch, 2, 2)
+    i, j = np.triu_indices(128, 1)
+    ii, jj = torch.from_numpy(i).cuda(), torch.from_numpy(j).cuda()
+    data = torch.empty_like(model)
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(3)
+    for t in range(nt):
+        mc = torch.view_as_complex(model[t].reshape(nch, nbl, 4, 2)).reshape(nch, nbl, 2, 2).to(torch.complex128)
+        gp = gc[ii].permute(1, 0, 2, 3)  # [nch][nbl][2][2]
+        gq = gc[jj].permute(1, 0, 2, 3)
+        d = gp @ mc @ gq.conj().transpose(-1, -2)
+        dr = torch.view_as_real(d.reshape(nch, nbl, 4)).reshape(nch, nbl, 8)
+        rms = torch.sqrt(torch.mean(dr[..., [0, 1, 6, 7]] ** 2))
+        noise = torch.randn(dr.shape, generator=gen, device="cuda", dtype=torch.float64) * (rms / 10.0 / math.sqrt(2.0))
+        data[t] = (dr + noise).to(torch.float32)
+    return model, data, g
+
+
+def dical_arm(args):
+    """Plain and collapsed DI calibration of the workload's timeblock, CPU
+    oracle on a bounded sample of its chanblocks."""
+    import torch
+
+    from mwa_hyperdrive_b200 import calibrate as cal
+
+    nch = args.dical_chanblocks
+    model, data, g = dical_workload(nch)
+    nt = model.shape[0]
+    ident = np.zeros((128, nch, 8))
+    ident[..., 0] = 1.0
+    ident[..., 6] = 1.0
+    out = {"workload": DICAL_WORKLOAD, "metric": "DI-cal s/timeblock", "unit": "s", "higher_is_better": False}
+    sols = {}
+    for form in ("plain", "collapsed", "collapsed_f32"):
+        dj = torch.from_numpy(ident.copy()).cuda()
+        cal.calibrate_timeblock(data, model, dj, (0, nt), 50, 1e-8, 1e-4, form=form)  # warm-up
+        times, res = [], None
+        for _ in range(3):
+            dj.copy_(torch.from_numpy(ident))
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            res = cal.calibrate_timeblock(data, model, dj, (0, nt), 50, 1e-8, 1e-4, form=form)
+            torch.cuda.synchronize()
+            times.append(time.perf_counter() - t0)
+        sols[form] = dj.cpu().numpy()
+        it = np.array([r.num_iterations for r in res])
+        out[form] = {"s_per_timeblock": min(times), "iterations_mean": float(it.mean()), "iterations_max": int(it.max()),
+                     "converged": int(sum(r.converged for r in res)), "chanblocks": nch}
+    ok = np.isfinite(sols["plain"])
+    for form in ("collapsed", "collapsed_f32"):
+        a, b = sols[form][ok], sols["plain"][ok]
+        out[form]["solution_rel_err_vs_plain"] = (float(np.linalg.norm(a - b) / np.linalg.norm(b)) if ok.any()
+                                                  else None)
+        out[form]["nan_pattern_equal"] = bool(np.array_equal(np.isnan(sols[form]), np.isnan(sols["plain"])))
+    out["chosen"] = "collapsed_f32"
+    out["speedup_chosen_vs_plain"] = out["plain"]["s_per_timeblock"] / out["collapsed_f32"]["s_per_timeblock"]
+    # roofline of the chosen iteration kernel: covariance bytes per iteration
+    nbl = model.shape[2]
+    it_total = out["collapsed_f32"]["iterations_mean"] * nch
+    out["algorithmic"] = {"plain_bytes_per_iteration_per_chanblock": nt * nbl * 64,
+                          "collapsed_f32_bytes_per_iteration_per_chanblock": nbl * 48 * 4,
+                          "fp64_flop_per_visibility_iteration_plain": 368, "collapsed_iterations_total": it_total}
+    if not args.no_cpu_baseline:
+        from oracle import oracle as orc
+
+        orc.build()
+        threads = os.cpu_count() or 1
+        orc.set_num_threads(threads)
+        ns = min(nch, max(threads, 8))
+        dh = data[:, :ns].cpu().numpy()
+        mh = model[:, :ns].cpu().numpy()
+        t0 = time.perf_counter()
+        orc.calibrate_timeblock(dh, mh, ident[:, :ns], 0, nt, 50, 1e-8, 1e-4, 0)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": dt * nch / ns, "unit": "s", "cores": threads, "kind": "port",
+                               "sample": f"{ns} of {nch} chanblocks x 14 timesteps x {nbl} baselines in {dt:.2f} s, "
+                                         f"scaled to {nch} chanblocks"}
+    return out
 
 
 # ------------------------------------------------------------ GPU arm
@@ -362,6 +474,10 @@ def gpu_arm(args, rank, world, local_rank):
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(obs, sky, args.cpu_seconds)
+        if not args.skip_dical:
+            del vis, flush
+            torch.cuda.empty_cache()
+            line["dical"] = dical_arm(args)
         print(json.dumps(line), flush=True)
     plain.close()
     if chosen is not plain:

@@ -361,7 +361,9 @@ typedef struct HdcCalResult {
     int num_failed;
 } HdcCalResult;
 
-#define HDC_CAL_PLAIN 0 /* stream data and model every iteration */
+#define HDC_CAL_PLAIN 0         /* stream data and model every iteration */
+#define HDC_CAL_COLLAPSED 1     /* sum the timeblock's timesteps once into per-baseline covariances (FP64) */
+#define HDC_CAL_COLLAPSED_F32 2 /* the same with covariances stored in FP32 (half the bytes per iteration) */
 
 /* calibrate_timeblock (di_calibrate/mod.rs:387-618): calibrate every
  * chanblock of one timeblock, then re-calibrate failed chanblocks from

@@ -20,7 +20,7 @@ import numpy as np
 from . import _lib
 from .model import POLS, _stream_ptr
 
-FORMS = {"plain": 0}
+FORMS = {"plain": 0, "collapsed": 1, "collapsed_f32": 2}
 
 
 @dataclass

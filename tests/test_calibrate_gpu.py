@@ -26,11 +26,12 @@ def identity(n, nch=1):
     return j
 
 
-def gpu_timeblock(data, model, dj0, t0, t1, max_iter=50, stop=1e-8, min_thr=1e-4, pols="XX_XY_YX_YY"):
+def gpu_timeblock(data, model, dj0, t0, t1, max_iter=50, stop=1e-8, min_thr=1e-4, pols="XX_XY_YX_YY",
+                  form="plain"):
     d = torch.from_numpy(np.ascontiguousarray(data, np.float32)).cuda()
     m = torch.from_numpy(np.ascontiguousarray(model, np.float32)).cuda()
     dj = torch.from_numpy(np.ascontiguousarray(dj0, np.float64)).cuda()
-    res = cal.calibrate_timeblock(d, m, dj, (t0, t1), max_iter, stop, min_thr, pols)
+    res = cal.calibrate_timeblock(d, m, dj, (t0, t1), max_iter, stop, min_thr, pols, form=form)
     return dj.cpu().numpy(), res
 
 
@@ -169,3 +170,48 @@ def test_failed_chanblock_retry_and_flagged_tile(oracle):
     data[:, 1, sel] = 0
     model[:, 1, sel] = 0
     compare(oracle, data, model, dj0, 0, nt, max_iter=30)
+
+
+def compare_collapsed(oracle, data, model, dj0, t0, t1, form, max_iter=50, stop=1e-8, min_thr=1e-4):
+    """The collapsed forms regroup the timestep sums (FP64: same iteration
+    counts, solutions to rounding; FP32 covariances: solutions to ~1e-7)."""
+    dj_g, res_g = gpu_timeblock(data, model, dj0, t0, t1, max_iter, stop, min_thr, form=form)
+    dj_o, res_o = oracle.calibrate_timeblock(data, model, dj0, t0, t1, max_iter, stop, min_thr, 0)
+    assert [r.converged for r in res_g] == [r["converged"] for r in res_o]
+    it_g = np.array([r.num_iterations for r in res_g])
+    it_o = np.array([r["num_iterations"] for r in res_o])
+    if form == "collapsed":
+        np.testing.assert_array_equal(it_g, it_o)
+    else:
+        assert np.max(np.abs(it_g - it_o)) <= 2, (it_g, it_o)
+    np.testing.assert_array_equal(np.isnan(dj_g), np.isnan(dj_o))
+    ok = ~np.isnan(dj_o)
+    err = np.linalg.norm(dj_g[ok] - dj_o[ok]) / np.linalg.norm(dj_o[ok]) if ok.any() else 0.0
+    return err
+
+
+@pytest.mark.parametrize("form,tol", [("collapsed", 1e-9), ("collapsed_f32", 1e-6)])
+@pytest.mark.parametrize("ntiles,nt,nch,snr", [(8, 2, 5, None), (20, 4, 6, 10.0), (128, 14, 3, 10.0)])
+def test_collapsed_forms_match_oracle(oracle, form, tol, ntiles, nt, nch, snr):
+    rng = np.random.default_rng(ntiles + nt)
+    nbl = ntiles * (ntiles - 1) // 2
+    model = synth.random_model(nt, nch, nbl, rng)
+    g = synth.truth_gains(ntiles, nch, rng)
+    data = synth.corrupt(model, g, rng, snr)
+    err = compare_collapsed(oracle, data, model, identity(ntiles, nch), 0, nt, form)
+    assert err < tol, err
+
+
+@pytest.mark.parametrize("form", ["collapsed", "collapsed_f32"])
+def test_collapsed_forms_retry_and_timeblock_offset(oracle, form):
+    rng = np.random.default_rng(11)
+    ntiles, nt, nch = 10, 4, 7
+    nbl = ntiles * (ntiles - 1) // 2
+    model = synth.random_model(nt, nch, nbl, rng)
+    data = synth.corrupt(model, synth.truth_gains(ntiles, nch, rng), rng, 20.0)
+    data[:, 3] = 0
+    model[:, 3] = 0
+    dj0 = identity(ntiles, nch)
+    dj0[:, 5] = 0
+    err = compare_collapsed(oracle, data, model, dj0, 1, 3, form, max_iter=30)
+    assert err < (1e-9 if form == "collapsed" else 1e-6), err
