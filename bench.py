@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-dical", action="store_true", help="leave out the DI-calibration measurement")
     ap.add_argument("--dical-chanblocks", type=int, default=768, help="reduced DI-cal case for profiling")
+    ap.add_argument("--skip-peel", action="store_true", help="leave out the peeling measurement")
+    ap.add_argument("--peel-channels", type=int, default=384, help="reduced peel case for profiling")
     args = ap.parse_args()
     global SHAPE
     SHAPE = (args.channels, args.timesteps)
@@ -351,6 +353,98 @@ def dical_arm(args):
     return out
 
 
+# ------------------------------------------------------------- peeling
+PEEL_WORKLOAD = ("peeling: 128 tiles (8128 baselines), 8 timesteps 8 s apart, 384 x 80 kHz channels from 167 MHz "
+                 "averaged x16 to 24 for the fits; sky of 20000 points (lognormal(0, 1) Jy, 10 deg cap); the 50 "
+                 "brightest carry ionospheric offsets (alpha, beta) ~ N(0, 2e-5) and gains U(0.9, 1.1); residual = "
+                 "data - model without ionosphere (so only those 50 remain); 3 passes x 10 iono iterations, "
+                 "convergence 1, no beam")
+
+
+def peel_workload(nch):
+    """Residual [8][nch][8128][8] float32 on the device, the 50 sources,
+    their positions and truths."""
+    import torch
+
+    from mwa_hyperdrive_b200 import synth
+    from mwa_hyperdrive_b200 import srclist as sl
+    from mwa_hyperdrive_b200.model import SkyModeller
+
+    pc = (0.0, math.radians(-27.0))
+    nt = 8
+    lsts = pc[0] + np.arange(nt) * 8.0 * synth.SIDEREAL_RATE
+    obs = synth.Obs(synth.tiles_in_disk(128, 750.0, 5), 167.0e6 + np.arange(nch) * 80e3, pc, lsts)
+    comps = synth.point_sky(20000, pc, 10.0, 5)
+    flux = np.array([c.flux_type.fd.i for c in comps])
+    bright = np.argsort(flux)[::-1][:50]
+    rng = np.random.default_rng(5)
+    nbl = obs.num_baselines
+    lam = torch.from_numpy(299792458.0 / obs.freqs).cuda()
+    resid = torch.zeros((nt, nch, nbl, 8), dtype=torch.float32, device="cuda")
+    sources, positions, truths = [], [], []
+    i, j = np.triu_indices(128, 1)
+    for k in bright:
+        sky = sl.SkyModelArrays.from_components([comps[k]])
+        pos = (comps[k].ra, comps[k].dec)
+        tr = (float(rng.normal(0, 2e-5)), float(rng.normal(0, 2e-5)), float(rng.uniform(0.9, 1.1)))
+        sources.append(sky)
+        positions.append(pos)
+        truths.append(tr)
+        m = SkyModeller(sky, obs.tile_xyzs, obs.freqs, pc, obs.latitude, beam="none", form="direct")
+        for t in range(nt):
+            mv = torch.zeros((nch, nbl, 8), dtype=torch.float64, device="cuda")
+            m.model_timestep_with(float(lsts[t]), mv, return_uvws=False)
+            # baseline u, v in the source's frame
+            ha, dec = lsts[t] - pos[0], pos[1]
+            xyz = obs.tile_xyzs
+            d = xyz[i] - xyz[j]
+            u = np.sin(ha) * d[:, 0] + np.cos(ha) * d[:, 1]
+            v = -np.sin(dec) * np.cos(ha) * d[:, 0] + np.sin(dec) * np.sin(ha) * d[:, 1] + np.cos(dec) * d[:, 2]
+            arg = -2 * np.pi * (torch.from_numpy(u * tr[0] + v * tr[1]).cuda()[None, :] * lam[:, None])
+            f = torch.polar(torch.full_like(arg, tr[2]), arg) - 1.0  # iono - 1
+            mc = torch.view_as_complex(mv.reshape(nch, nbl, 4, 2))
+            resid[t] += torch.view_as_real(mc * f[..., None]).reshape(nch, nbl, 8).to(torch.float32)
+        m.close()
+    return obs, resid, sources, positions, truths
+
+
+def peel_arm(args):
+    import torch
+
+    from mwa_hyperdrive_b200 import peel as P
+
+    nch = args.peel_channels
+    obs, resid0, sources, positions, truths = peel_workload(nch)
+    weights = torch.ones(resid0.shape[:3], dtype=torch.float32, device="cuda")
+    avg = float(np.median(obs.lsts))
+    out = {"workload": PEEL_WORKLOAD, "metric": "peel s/timeblock (3 passes, 50 sources)", "unit": "s",
+           "higher_is_better": False}
+    for name, batched in (("sequential", False), ("batched", True)):
+        times, consts = [], None
+        for rep in range(2):  # the first run also builds the models and (batched) autotunes
+            r = resid0.clone()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            consts = P.peel_timeblock(r, weights, obs.freqs, obs.tile_xyzs, obs.lsts, avg, obs.phase_centre, sources,
+                                      positions, [P.IonoConsts() for _ in sources], 3, 10, 1.0, 16,
+                                      obs.latitude, "none", batched=batched)
+            torch.cuda.synchronize()
+            times.append(time.perf_counter() - t0)
+        err_a = max(abs(c.alpha - t[0]) for c, t in zip(consts, truths))
+        err_g = max(abs(c.gain - t[2]) for c, t in zip(consts, truths))
+        out[name] = {"s_per_timeblock": min(times), "first_call_s": times[0],
+                     "residual_rms_ratio": float(r.norm() / resid0.norm()),
+                     "max_alpha_err": err_a, "max_gain_err": err_g}
+        if batched:
+            bx, sy, ms = P.batched_tuning()
+            out[name]["autotuned_accumulate_cta"] = {"bins": bx, "sources": sy, "ms": ms}
+    out["speedup_batched_vs_sequential"] = out["sequential"]["s_per_timeblock"] / out["batched"]["s_per_timeblock"]
+    nvis = int(np.prod(resid0.shape[:3]))
+    out["algorithmic"] = {"hi_res_vis": nvis, "hi_res_bytes": nvis * 32,
+                          "batched_hi_res_bytes_per_pass": "residual read + read/write, weights, 50 model reads x 2"}
+    return out
+
+
 # ------------------------------------------------------------ GPU arm
 def gpu_arm(args, rank, world, local_rank):
     import torch
@@ -505,10 +599,14 @@ def gpu_arm(args, rank, world, local_rank):
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(obs, sky, args.cpu_seconds)
-        if not args.skip_dical:
+        if not args.skip_dical or not args.skip_peel:
             del vis, flush
             torch.cuda.empty_cache()
+        if not args.skip_dical:
             line["dical"] = dical_arm(args)
+            torch.cuda.empty_cache()
+        if not args.skip_peel:
+            line["peel"] = peel_arm(args)
         print(json.dumps(line), flush=True)
     plain.close()
     if chosen is not plain:

@@ -436,6 +436,26 @@ int hdc_peel_timeblock(JonesF32 *d_resid_tfb, const float *d_weights_tfb, int nu
                        const RADec *h_source_positions, IonoConsts *h_iono_consts, const HdcPeelParams *params,
                        hdcStream_t stream);
 
+/* The same timeblock peeled with every source's fit of a pass batched
+ * (this project's chosen form; no counterpart in the reference): one
+ * accumulation sweep over the high-resolution residual for all sources, all
+ * iono fits in one launch per iteration, one sweep applying every source's
+ * update.  Sources fitted in the same pass see the residual as it was at the
+ * start of the pass (Jacobi) instead of each other's updates (the reference's
+ * Gauss-Seidel order); with one source the two coincide.  Needs num_sources
+ * x (timesteps x channels x baselines) JonesF32 of device memory for the
+ * source models. */
+int hdc_peel_timeblock_batched(JonesF32 *d_resid_tfb, const float *d_weights_tfb, int num_timesteps, int num_freqs,
+                               const double *h_freqs, const XYZ *h_tile_xyzs, int num_tiles, const double *h_lmsts,
+                               double average_lmst, RADec phase_centre, int num_sources, const HdcSkyModel *h_sources,
+                               const RADec *h_source_positions, IonoConsts *h_iono_consts, const HdcPeelParams *params,
+                               hdcStream_t stream);
+
+/* The accumulation-sweep launch shape the batched peel's autotuner chose for
+ * the last new problem shape (low-resolution bins and sources per CTA) and
+ * its measured time. */
+int hdc_peel_batched_tuning(int *block_bins, int *block_sources, float *ms);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

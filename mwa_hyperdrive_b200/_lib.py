@@ -121,6 +121,10 @@ SIGNATURES = {
                                         c_double, c_double, c_int, ctypes.POINTER(HdcCalResult), c_int, c_void_p]),
     "hdc_peel_timeblock": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p, c_int, c_void_p, c_double,
                                    RADec, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "hdc_peel_timeblock_batched": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p, c_int, c_void_p,
+                                           c_double, RADec, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
+                                           c_void_p]),
+    "hdc_peel_batched_tuning": (c_int, [ctypes.POINTER(c_int), ctypes.POINTER(c_int), ctypes.POINTER(c_float)]),
     "hdc_calibration_residuals": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p,
                                           c_void_p]),
     "hdc_mlp_new": (c_int, [c_int, c_void_p, c_int, ctypes.c_ulonglong, ctypes.POINTER(c_void_p)]),

@@ -232,6 +232,8 @@ __global__ void __launch_bounds__(CT) mitchcal_kernel(const CalParams P) {
     Herm* Hs = bot + n;                                  // G^H G per tile (collapsed form)
     double* prec = reinterpret_cast<double*>(Hs + n);   // [n][4]
     int* failed = reinterpret_cast<int*>(prec + 4 * n);
+    // collapsed form: 16 x 16 x 12 block-column partial sums (8-byte aligned)
+    double* colbuf = reinterpret_cast<double*>(failed + ((n + 1) & ~1));
 
     const int ch = P.chan_list ? P.chan_list[blockIdx.x] : blockIdx.x;
     const int tid = threadIdx.x, lane = tid & 31;
@@ -263,6 +265,7 @@ __global__ void __launch_bounds__(CT) mitchcal_kernel(const CalParams P) {
         __syncthreads();
 
         // ---- accumulate top / bot (calibration_loop) ----
+        if (FORM == 0) {
         const int nwarp_bl = (P.nbl + 31) & ~31;
         for (int base = tid & ~31; base < nwarp_bl; base += CT) {
             const int bl = base + lane;
@@ -273,23 +276,15 @@ __global__ void __launch_bounds__(CT) mitchcal_kernel(const CalParams P) {
             if (active) {
                 baseline_to_tiles(bl, n, p, q);
                 const J2 gp = G[p], gq = G[q];
-                if (FORM == 0) {
-                    for (int t = 0; t < nt; t++) {
-                        const J2 d = load_vis(D0 + t * tstride + bl);
-                        const J2 m = load_vis(M0 + t * tstride + bl);
-                        const J2 z1 = gq * herm(m);
-                        t1 = t1 + d * z1;
-                        add_zhz(h1, z1);
-                        const J2 z2 = gp * m;
-                        t2 = t2 + herm(d) * z2;
-                        add_zhz(h2, z2);
-                    }
-                } else if (FORM == 1) {
-                    collapsed_terms(static_cast<const double*>(P.cov) + (size_t)ch * NCOV * P.nbl + bl, (size_t)P.nbl,
-                                    gp, gq, Hs[p], Hs[q], t1, t2, h1, h2);
-                } else {
-                    collapsed_terms(static_cast<const float*>(P.cov) + (size_t)ch * NCOV * P.nbl + bl, (size_t)P.nbl,
-                                    gp, gq, Hs[p], Hs[q], t1, t2, h1, h2);
+                for (int t = 0; t < nt; t++) {
+                    const J2 d = load_vis(D0 + t * tstride + bl);
+                    const J2 m = load_vis(M0 + t * tstride + bl);
+                    const J2 z1 = gq * herm(m);
+                    t1 = t1 + d * z1;
+                    add_zhz(h1, z1);
+                    const J2 z2 = gp * m;
+                    t2 = t2 + herm(d) * z2;
+                    add_zhz(h2, z2);
                 }
             }
             // tile1 (row) sums: segmented reduction, head lane adds
@@ -322,6 +317,71 @@ __global__ void __launch_bounds__(CT) mitchcal_kernel(const CalParams P) {
                 atomicAdd(&bot[q].b.re, h2.b.re);
                 atomicAdd(&bot[q].b.im, h2.b.im);
             }
+        }
+        } else {
+            // collapsed: 16 x 16 blocks of tile pairs (p, q), p < q; thread
+            // (bi, bj) takes pair (16 pb + bi, 16 qb + bj).  Tile-1 sums run
+            // along a block row (16 consecutive lanes, shuffles), tile-2 sums
+            // along a block column (through shared memory), so every
+            // accumulator entry has one writer per block and no atomics.
+            const int bi = tid >> 4, bj = tid & 15;
+            const int nb = (n + 15) / 16;
+            for (int pb = 0; pb < nb; pb++)
+                for (int qb = pb; qb < nb; qb++) {
+                    const int p = pb * 16 + bi, q = qb * 16 + bj;
+                    J2 t1 = jzero(), t2 = jzero();
+                    Herm h1{0, 0, {0, 0}}, h2{0, 0, {0, 0}};
+                    if (p < q && q < n) {
+                        const size_t bl = (size_t)baseline_index(p, q, n);
+                        if (FORM == 1)
+                            collapsed_terms(static_cast<const double*>(P.cov) + (size_t)ch * NCOV * P.nbl + bl,
+                                            (size_t)P.nbl, G[p], G[q], Hs[p], Hs[q], t1, t2, h1, h2);
+                        else
+                            collapsed_terms(static_cast<const float*>(P.cov) + (size_t)ch * NCOV * P.nbl + bl,
+                                            (size_t)P.nbl, G[p], G[q], Hs[p], Hs[q], t1, t2, h1, h2);
+                    }
+                    double v[12] = {t1.a.re, t1.a.im, t1.b.re, t1.b.im, t1.c.re, t1.c.im,
+                                    t1.d.re, t1.d.im, h1.a,    h1.d,    h1.b.re, h1.b.im};
+#pragma unroll
+                    for (int k = 0; k < 12; k++) {
+#pragma unroll
+                        for (int o = 8; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+                    }
+                    double* cb = colbuf + (size_t)(bi * 16 + bj) * 12;
+                    cb[0] = t2.a.re, cb[1] = t2.a.im, cb[2] = t2.b.re, cb[3] = t2.b.im;
+                    cb[4] = t2.c.re, cb[5] = t2.c.im, cb[6] = t2.d.re, cb[7] = t2.d.im;
+                    cb[8] = h2.a, cb[9] = h2.d, cb[10] = h2.b.re, cb[11] = h2.b.im;
+                    if (bj == 0 && p < n) {
+                        double* tp = reinterpret_cast<double*>(&top[p]);
+#pragma unroll
+                        for (int k = 0; k < 8; k++) tp[k] += v[k];
+                        bot[p].a += v[8];
+                        bot[p].d += v[9];
+                        bot[p].b.re += v[10];
+                        bot[p].b.im += v[11];
+                    }
+                    __syncthreads();
+                    if (tid < 16 * 12) {
+                        const int j = tid / 12, k = tid - j * 12;
+                        const int qq = qb * 16 + j;
+                        double sum = 0.0;
+#pragma unroll
+                        for (int i = 0; i < 16; i++) sum += colbuf[(i * 16 + j) * 12 + k];
+                        if (qq < n) {
+                            if (k < 8)
+                                reinterpret_cast<double*>(&top[qq])[k] += sum;
+                            else if (k == 8)
+                                bot[qq].a += sum;
+                            else if (k == 9)
+                                bot[qq].d += sum;
+                            else if (k == 10)
+                                bot[qq].b.re += sum;
+                            else
+                                bot[qq].b.im += sum;
+                        }
+                    }
+                    __syncthreads();
+                }
         }
         __syncthreads();
 
@@ -485,13 +545,15 @@ __global__ void __launch_bounds__(CT) residual_kernel(const CalParams P, const J
     }
 }
 
-static size_t smem_bytes(int n) {
-    return (size_t)n * (3 * sizeof(J2) + 2 * sizeof(Herm) + 4 * sizeof(double) + sizeof(int));
+static size_t smem_bytes(int n, int form) {
+    const size_t base = (size_t)n * (3 * sizeof(J2) + 2 * sizeof(Herm) + 4 * sizeof(double)) +
+                        sizeof(int) * (size_t)((n + 1) & ~1);
+    return base + (form != HDC_CAL_PLAIN ? 16 * 16 * 12 * sizeof(double) : 0);
 }
 
 template <int FORM>
 static int launch_mitchcal_form(const CalParams& P, int nblocks, cudaStream_t s) {
-    const size_t sm = smem_bytes(P.ntiles);
+    const size_t sm = smem_bytes(P.ntiles, FORM);
     HDC_CUDA_RET_INT(
         cudaFuncSetAttribute(mitchcal_kernel<FORM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     mitchcal_kernel<FORM><<<nblocks, CT, sm, s>>>(P);

@@ -12,6 +12,8 @@
 // once at the end (the reference copies them back every iteration,
 // peel.cu:709).
 
+#include <vector>
+
 #include "common.cuh"
 
 namespace hdc {
@@ -105,16 +107,15 @@ __device__ __forceinline__ double warp_sum(double v) {
 }
 
 // One iteration's apply + partial sums (peel.cu:437-486 apply_iono and
-// iono_loop_kernel, fused with the baseline reduction of reduce_baselines).
-// grid (ceil(nbl/PT), nf); partials [nf][gridDim.x][7].
-__global__ void __launch_bounds__(PT) iono_partials_kernel(const JonesF32* resid, const float* weights,
-                                                           const JonesF32* model, JonesF32* model_rot,
-                                                           const IonoDev* st, const UVW* uvws, const double* lambdas,
-                                                           int nbl, int nf, double* partials) {
-    if (st->stop) return;
+// iono_loop_kernel, fused with the baseline reduction of reduce_baselines)
+// for one (baseline block, channel) of one source; partials [nblk][7] of
+// that channel.
+__device__ __forceinline__ void iono_partials_body(const JonesF32* resid, const float* weights,
+                                                   const JonesF32* model, JonesF32* model_rot, const IonoDev* st,
+                                                   const UVW* uvws, const double* lambdas, int nbl, int f,
+                                                   int blk, int nblk, double* partials_f) {
     __shared__ double red[PT / 32][7];
-    const int f = blockIdx.y;
-    const int bl = blockIdx.x * PT + threadIdx.x;
+    const int bl = blk * PT + threadIdx.x;
     double v[7] = {0, 0, 0, 0, 0, 0, 0};
     if (bl < nbl) {
         const double u = uvws[bl].u, vv = uvws[bl].v;
@@ -150,15 +151,40 @@ __global__ void __launch_bounds__(PT) iono_partials_kernel(const JonesF32* resid
     if (threadIdx.x < 7) {
         double s = 0.0;
         for (int w = 0; w < PT / 32; w++) s += red[w][threadIdx.x];
-        partials[((size_t)f * gridDim.x + blockIdx.x) * 7 + threadIdx.x] = s;
+        partials_f[(size_t)blk * 7 + threadIdx.x] = s;
     }
 }
 
-// Channel reduction with the lambda scaling and the constants update
-// (peel.cu:327-432).  One CTA.
-__global__ void iono_update_kernel(const double* partials, int nblk, const double* lambdas, int nf, IonoDev* st,
-                                   double convergence) {
+// grid (ceil(nbl/PT), nf); partials [nf][gridDim.x][7].
+__global__ void __launch_bounds__(PT) iono_partials_kernel(const JonesF32* resid, const float* weights,
+                                                           const JonesF32* model, JonesF32* model_rot,
+                                                           const IonoDev* st, const UVW* uvws, const double* lambdas,
+                                                           int nbl, int nf, double* partials) {
     if (st->stop) return;
+    iono_partials_body(resid, weights, model, model_rot, st, uvws, lambdas, nbl, blockIdx.y, blockIdx.x, gridDim.x,
+                       partials + (size_t)blockIdx.y * gridDim.x * 7);
+}
+
+// The same for a batch of sources: grid (ceil(nbl/PT), nf, nsrc); source s
+// reads resid/model/model_rot at s * nf * nbl, weights shared, uvws at
+// s * nbl, state st[s], partials [nsrc][nf][nblk][7].
+__global__ void __launch_bounds__(PT) iono_partials_batched_kernel(const JonesF32* resid, const float* weights,
+                                                                   const JonesF32* model, JonesF32* model_rot,
+                                                                   const IonoDev* st, const UVW* uvws,
+                                                                   const double* lambdas, int nbl, int nf,
+                                                                   double* partials) {
+    const int src = blockIdx.z;
+    if (st[src].stop) return;
+    const size_t off = (size_t)src * nf * nbl;
+    iono_partials_body(resid + off, weights, model + off, model_rot + off, st + src, uvws + (size_t)src * nbl,
+                       lambdas, nbl, blockIdx.y, blockIdx.x, gridDim.x,
+                       partials + ((size_t)src * nf + blockIdx.y) * gridDim.x * 7);
+}
+
+// Channel reduction with the lambda scaling and the constants update
+// (peel.cu:327-432) for one source; one CTA.
+__device__ __forceinline__ void iono_update_body(const double* partials, int nblk, const double* lambdas, int nf,
+                                                 IonoDev* st, double convergence) {
     __shared__ double red[PT / 32][7];
     double v[7] = {0, 0, 0, 0, 0, 0, 0};
     for (int f = threadIdx.x; f < nf; f += blockDim.x) {
@@ -193,6 +219,20 @@ __global__ void iono_update_kernel(const double* partials, int nblk, const doubl
         st->gain *= 1. + convergence * (s_vm / s_mm - 1);
         if (st->gain < 0.0) st->stop = 1;  // peel.cu:711
     }
+}
+
+__global__ void iono_update_kernel(const double* partials, int nblk, const double* lambdas, int nf, IonoDev* st,
+                                   double convergence) {
+    if (st->stop) return;
+    iono_update_body(partials, nblk, lambdas, nf, st, convergence);
+}
+
+// grid (nsrc): source s updates st[s] from partials [s][nf][nblk][7].
+__global__ void iono_update_batched_kernel(const double* partials, int nblk, const double* lambdas, int nf,
+                                           IonoDev* st, double convergence) {
+    const int src = blockIdx.x;
+    if (st[src].stop) return;
+    iono_update_body(partials + (size_t)src * nf * nblk * 7, nblk, lambdas, nf, st + src, convergence);
 }
 
 __global__ void subtract_iono_kernel(JonesF32* resid, const JonesF32* model, IonoConsts c, IonoConsts old,
@@ -279,6 +319,42 @@ const char* iono_loop_on(const JonesF32* d_resid, const float* d_w, const JonesF
     return NULL;
 }
 
+
+// iono_loop for a batch of sources on one stream, every source starting
+// from its own constants in `consts` and writing the fitted ones back; one
+// host read at the end.  Buffers: resid/model/model_rot [nsrc][nf][nbl],
+// uvws [nsrc][nbl]; scratch holds partials [nsrc][nf][nblk][7] then the
+// per-source IonoDev states.
+size_t iono_batched_scratch_bytes(int nsrc, int nbl, int nf) {
+    const int nblk = (nbl + PT - 1) / PT;
+    return sizeof(double) * ((size_t)nsrc * nf * nblk * 7 + 4) + sizeof(IonoDev) * (size_t)nsrc;
+}
+
+const char* iono_loop_batched_on(const JonesF32* d_resid, const float* d_w, const JonesF32* d_model,
+                                 JonesF32* d_model_rot, void* d_scratch, IonoConsts* consts, int nsrc, int nbl, int nf,
+                                 int niter, const UVW* d_uvws, const double* d_lambdas, double convergence,
+                                 cudaStream_t s) {
+    if (nbl <= 0 || nf <= 0 || nsrc <= 0) return NULL;
+    const int nblk = (nbl + PT - 1) / PT;
+    double* partials = reinterpret_cast<double*>(d_scratch);
+    const size_t part_doubles = (size_t)nsrc * nf * nblk * 7;
+    IonoDev* st = reinterpret_cast<IonoDev*>(partials + ((part_doubles + 3) & ~(size_t)3));
+    std::vector<IonoDev> h(nsrc);
+    for (int i = 0; i < nsrc; i++) h[i] = IonoDev{consts[i].alpha, consts[i].beta, consts[i].gain, 0, 0};
+    HDC_CUDA_RET_STR(cudaMemcpyAsync(st, h.data(), sizeof(IonoDev) * nsrc, cudaMemcpyHostToDevice, s));
+    const dim3 g(nblk, nf, nsrc);
+    for (int it = 0; it < niter; it++) {
+        iono_partials_batched_kernel<<<g, PT, 0, s>>>(d_resid, d_w, d_model, d_model_rot, st, d_uvws, d_lambdas, nbl,
+                                                      nf, partials);
+        iono_update_batched_kernel<<<nsrc, PT, 0, s>>>(partials, nblk, d_lambdas, nf, st, convergence);
+        count_launches(2);
+    }
+    HDC_CUDA_RET_STR(cudaGetLastError());
+    HDC_CUDA_RET_STR(cudaMemcpyAsync(h.data(), st, sizeof(IonoDev) * nsrc, cudaMemcpyDeviceToHost, s));
+    HDC_CUDA_RET_STR(cudaStreamSynchronize(s));
+    for (int i = 0; i < nsrc; i++) consts[i] = IonoConsts{h[i].alpha, h[i].beta, h[i].gain};
+    return NULL;
+}
 
 // Stream-aware launchers (the drop-in entry points below use stream 0).
 cudaError_t k_xyzs_to_uvws(const XYZ* xyzs, const double* lmsts, UVW* uvws, RADec pc, int ntiles, int nbl, int nt,

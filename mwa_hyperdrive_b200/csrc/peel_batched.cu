@@ -1,0 +1,393 @@
+// Batched peeling: every source's ionospheric fit of a pass from one pass
+// over the data (this project's chosen form of peel_gpu,
+// params/peel/gpu.rs:25-757).
+//
+// Source models: a source that is one point component at its own position
+// has, in its own frame, the same model on every baseline (phase 1, a beam
+// shared by all tiles), so it is kept as one Jones per (timestep, channel);
+// any other source's model is materialised at high resolution.
+//
+// The reference peels sources one after another (Gauss-Seidel): rotate the
+// whole high-resolution residual to the source, add the source back, average
+// to low resolution, fit (alpha, beta, gain), subtract the re-fitted source,
+// move on -- about ten passes over the high-resolution data per source.
+// Here a pass fits all sources against the same residual (Jacobi), in the
+// phase-centre frame throughout:
+//   1. accumulate sweep: for every low-resolution bin and source s,
+//        D_s = <w (R rot_s + M_s iono_s(old))>,  Mr_s = <w M_s iono_s(old)>
+//      with rot_s = exp(-2 pi i (w_s - w_pc) / lambda) the rotation to the
+//      source and <.> the weighted mean over the timeblock and each channel
+//      group (the reference's rotate, add_model and vis_average_tfb);
+//   2. all sources' iono_loop fits in one launch per iteration
+//      (iono_loop_batched_on, the reference's arithmetic);
+//   3. apply sweep: R += sum_s conj(rot_s) M_s (iono_s(old) - iono_s(new))
+//      (the reference's subtract_iono, rotated back).
+// With one source this is the reference's sequence exactly (up to rounding:
+// FP64 throughout instead of its f32 intermediates); with several, sources
+// fitted in the same pass do not see each other's updates until the next
+// pass.  The source models M_s (high resolution, source frame) are predicted
+// once per timeblock by the modeller and reused by every pass.
+//
+// The accumulate sweep's CTA shape (low-resolution bins x sources per CTA;
+// sources in a CTA share the residual loads through L1) is chosen by timing
+// the candidates on the first call for a problem shape (the sweep only
+// writes its low-resolution outputs, so trial runs have no side effects).
+
+#include <chrono>
+#include <cmath>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <tuple>
+#include <vector>
+
+#include "modeller.cuh"
+
+namespace hdc {
+cudaError_t k_xyzs_to_uvws(const XYZ* xyzs, const double* lmsts, UVW* uvws, RADec pc, int ntiles, int nbl, int nt,
+                           cudaStream_t s);
+cudaError_t k_weights_average(const float* w, float* lo, int nt, int nbl, int nf, int favg, cudaStream_t s);
+size_t iono_batched_scratch_bytes(int nsrc, int nbl, int nf);
+const char* iono_loop_batched_on(const JonesF32* d_resid, const float* d_w, const JonesF32* d_model,
+                                 JonesF32* d_model_rot, void* d_scratch, IonoConsts* consts, int nsrc, int nbl, int nf,
+                                 int niter, const UVW* d_uvws, const double* d_lambdas, double convergence,
+                                 cudaStream_t s);
+
+namespace pb {
+
+struct SweepArgs {
+    const JonesF32* resid;  // [nt][nf][nbl], phase-centre frame
+    const float* w;         // [nt][nf][nbl]
+    const JonesF32* models; // [nsrc][nt][nf][nbl], source frames (general sources)
+    const JonesF32* ptab;   // [nsrc][nt][nf]: point-at-centre sources' models, or null
+    const UVW* uv_pc;       // [nt][nbl]
+    const UVW* uv_src;      // [nsrc][nt][nbl]
+    const double* lambdas;  // [nf]
+    const IonoConsts* old;  // [nsrc]
+    const IonoConsts* neu;  // [nsrc] (apply sweep)
+    JonesF32* d_lo;         // [nsrc][nlo][nbl]
+    JonesF32* m_lo;         // [nsrc][nlo][nbl]
+    int nt, nf, nbl, nsrc, favg;
+};
+
+__device__ __forceinline__ cplx phase(double arg) {
+    double s, c;
+    sincos(arg, &s, &c);
+    return cplx{c, s};
+}
+
+// iono factor g exp(-2 pi i (u alpha + v beta) lambda), as add_model / subtract_iono
+__device__ __forceinline__ cplx iono(const IonoConsts& k, const UVW& q, double lam) {
+    if (k.alpha == 0.0 && k.beta == 0.0) return cplx{k.gain, 0.0};
+    return phase(-TAU * (q.u * k.alpha + q.v * k.beta) * lam) * k.gain;
+}
+
+__device__ __forceinline__ JonesF32 to_f32(const J2& v) {
+    return JonesF32{(float)v.a.re, (float)v.a.im, (float)v.b.re, (float)v.b.im,
+                    (float)v.c.re, (float)v.c.im, (float)v.d.re, (float)v.d.im};
+}
+
+// blockDim (BX, SY): x = low-resolution bins, y = sources of this CTA's chunk
+template <int BX, int SY>
+__global__ void __launch_bounds__(BX* SY) accumulate_kernel(const SweepArgs A) {
+    const int nlo = A.nf / A.favg;
+    const int bin = blockIdx.x * BX + threadIdx.x;
+    const int src = blockIdx.y * SY + threadIdx.y;
+    if (bin >= nlo * A.nbl || src >= A.nsrc) return;
+    const int bl = bin % A.nbl, flo = bin / A.nbl;
+    const IonoConsts k = A.old[src];
+    const size_t nvis = (size_t)A.nt * A.nf * A.nbl;
+    const JonesF32* M = A.ptab ? nullptr : A.models + (size_t)src * nvis;
+    J2 acc_d = jzero(), acc_m = jzero();
+    double ws = 0.0;
+    for (int t = 0; t < A.nt; t++) {
+        const UVW q = A.uv_src[((size_t)src * A.nt + t) * A.nbl + bl];
+        const double dw = q.w - A.uv_pc[(size_t)t * A.nbl + bl].w;
+        for (int fc = flo * A.favg; fc < flo * A.favg + A.favg; fc++) {
+            const size_t i = ((size_t)t * A.nf + fc) * A.nbl + bl;
+            const double wt = A.w[i];
+            const double lam = A.lambdas[fc];
+            const cplx rot = phase(-TAU * dw / lam);
+            const JonesF32 mj = A.ptab ? A.ptab[((size_t)src * A.nt + t) * A.nf + fc] : M[i];
+            const J2 m = load_j32(mj) * iono(k, q, lam);
+            acc_d = acc_d + (load_j32(A.resid[i]) * rot + m) * wt;
+            acc_m = acc_m + m * wt;
+            ws += wt;
+        }
+    }
+    const double d = ws > 0.0 ? ws : 1.0;
+    const size_t o = ((size_t)src * nlo + flo) * A.nbl + bl;
+    A.d_lo[o] = to_f32(acc_d * (1.0 / d));
+    A.m_lo[o] = to_f32(acc_m * (1.0 / d));
+}
+
+// one thread per high-resolution visibility; all sources' updates
+__global__ void __launch_bounds__(256) apply_kernel(JonesF32* resid, const SweepArgs A) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t nvis = (size_t)A.nt * A.nf * A.nbl;
+    if (i >= nvis) return;
+    const int bl = (int)(i % A.nbl);
+    const int f = (int)((i / A.nbl) % A.nf);
+    const int t = (int)(i / ((size_t)A.nbl * A.nf));
+    const double lam = A.lambdas[f];
+    const double wpc = A.uv_pc[(size_t)t * A.nbl + bl].w;
+    J2 r = load_j32(resid[i]);
+    for (int s = 0; s < A.nsrc; s++) {
+        const UVW q = A.uv_src[((size_t)s * A.nt + t) * A.nbl + bl];
+        const cplx d = iono(A.old[s], q, lam) - iono(A.neu[s], q, lam);
+        if (d.re == 0.0 && d.im == 0.0) continue;
+        const cplx back = phase(TAU * (q.w - wpc) / lam);  // conj of the rotation to the source
+        const JonesF32 mj = A.ptab ? A.ptab[((size_t)s * A.nt + t) * A.nf + f] : A.models[(size_t)s * nvis + i];
+        r = r + load_j32(mj) * (back * d);
+    }
+    resid[i] = to_f32(r);
+}
+
+struct Variant {
+    int bx, sy;
+    void (*launch)(const SweepArgs&, cudaStream_t);
+};
+
+template <int BX, int SY>
+void launch_acc(const SweepArgs& A, cudaStream_t s) {
+    const int nbins = (A.nf / A.favg) * A.nbl;
+    const dim3 grid((nbins + BX - 1) / BX, (A.nsrc + SY - 1) / SY);
+    accumulate_kernel<BX, SY><<<grid, dim3(BX, SY), 0, s>>>(A);
+    count_launches(1);
+}
+
+const Variant kVariants[] = {
+    {256, 1, launch_acc<256, 1>}, {128, 2, launch_acc<128, 2>}, {64, 4, launch_acc<64, 4>}, {32, 8, launch_acc<32, 8>}};
+constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
+
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int, int>, int> g_tuned;  // (nt, nf, nbl, nsrc, favg) -> variant
+struct Tuning {
+    int bx = 0, sy = 0;
+    float ms = 0.f;
+} g_last;
+
+// the fastest accumulate variant for this shape (timed once, then cached)
+int choose_variant(const SweepArgs& A, cudaStream_t s) {
+    const auto key = std::make_tuple(A.nt, A.nf, A.nbl, A.nsrc, A.favg);
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tuned.find(key);
+        if (it != g_tuned.end()) return it->second;
+    }
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    int best = 0;
+    float best_ms = 1e30f;
+    for (int v = 0; v < kNumVariants; v++) {
+        kVariants[v].launch(A, s);  // warm
+        cudaEventRecord(a, s);
+        kVariants[v].launch(A, s);
+        cudaEventRecord(b, s);
+        cudaEventSynchronize(b);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        if (cudaGetLastError() == cudaSuccess && ms < best_ms) {
+            best_ms = ms;
+            best = v;
+        }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tuned[key] = best;
+    g_last = Tuning{kVariants[best].bx, kVariants[best].sy, best_ms};
+    return best;
+}
+
+struct DevBuf {
+    void* p = nullptr;
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+    template <class T>
+    T* as() {
+        return reinterpret_cast<T*>(p);
+    }
+};
+
+}  // namespace pb
+}  // namespace hdc
+
+using namespace hdc;
+
+#define PB_CK(call)                                                                    \
+    do {                                                                               \
+        cudaError_t e_ = (call);                                                       \
+        if (e_ != cudaSuccess) {                                                       \
+            set_error("hdc_peel_timeblock_batched: %s: %s", #call, cudaGetErrorString(e_)); \
+            return HDC_ERR_CUDA;                                                       \
+        }                                                                              \
+    } while (0)
+
+extern "C" int hdc_peel_timeblock_batched(JonesF32* d_resid_tfb, const float* d_weights_tfb, int num_timesteps,
+                                          int num_freqs, const double* h_freqs, const XYZ* h_tile_xyzs, int num_tiles,
+                                          const double* h_lmsts, double average_lmst, RADec phase_centre,
+                                          int num_sources, const HdcSkyModel* h_sources,
+                                          const RADec* h_source_positions, IonoConsts* h_iono_consts,
+                                          const HdcPeelParams* params, hdcStream_t stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    if (!d_resid_tfb || !d_weights_tfb || !h_freqs || !h_tile_xyzs || !h_lmsts || !params || num_tiles < 2 ||
+        num_timesteps < 1 || num_freqs < 1 || num_sources < 0 ||
+        (num_sources > 0 && (!h_sources || !h_iono_consts || !h_source_positions))) {
+        set_error("hdc_peel_timeblock_batched: invalid arguments");
+        return HDC_ERR_ARG;
+    }
+    const int favg = params->freq_average_factor;
+    if (favg < 1 || num_freqs % favg != 0) {
+        set_error("hdc_peel_timeblock_batched: %d channels are not a multiple of the averaging factor %d", num_freqs,
+                  favg);
+        return HDC_ERR_ARG;
+    }
+    if (num_sources == 0) return HDC_OK;
+    const int nt = num_timesteps, nf = num_freqs, nbl = num_tiles * (num_tiles - 1) / 2, nlo = nf / favg;
+    const int ns = num_sources;
+    const size_t nvis = (size_t)nt * nf * nbl;
+
+    std::vector<double> lam(nf), lam_lo(nlo);
+    for (int f = 0; f < nf; f++) lam[f] = VEL_C / h_freqs[f];
+    for (int k = 0; k < nlo; k++) {
+        double sum = 0.0;
+        for (int f = k * favg; f < (k + 1) * favg; f++) sum += h_freqs[f];
+        lam_lo[k] = VEL_C / (sum / favg);
+    }
+    std::vector<XYZ> xyz_t((size_t)nt * num_tiles);
+    for (int t = 0; t < nt; t++)
+        for (int i = 0; i < num_tiles; i++) xyz_t[(size_t)t * num_tiles + i] = h_tile_xyzs[i];
+
+    // point-at-centre sources keep a (timestep, channel) table; otherwise
+    // the models need ns x nvis JonesF32 of device memory
+    bool points = true;
+    for (int i = 0; i < ns && points; i++) {
+        const HdcSkyModel& m = h_sources[i];
+        points = m.num_components == 1 && m.comp_type[0] == 0 && std::fabs(m.ra[0] - h_source_positions[i].ra) < 1e-12 &&
+                 std::fabs(m.dec[0] - h_source_positions[i].dec) < 1e-12;
+    }
+    size_t free_b = 0, total_b = 0;
+    PB_CK(cudaMemGetInfo(&free_b, &total_b));
+    const size_t need = points ? sizeof(JonesF32) * (size_t)ns * nt * nf : sizeof(JonesF32) * nvis * (size_t)ns;
+    if (need + (size_t)(1u << 30) > free_b) {
+        set_error("hdc_peel_timeblock_batched: the %d source models need %zu MB of device memory, %zu MB free", ns,
+                  need >> 20, free_b >> 20);
+        return HDC_ERR_ALLOC;
+    }
+    pb::DevBuf b_lam, b_lam_lo, b_lmst, b_avg_lmst, b_xyz, b_uv_pc, b_uv_src, b_uv_lo, b_models, b_dlo, b_mlo, b_mlo_rot,
+        b_wlo, b_scr, b_old, b_new, b_stage;
+    PB_CK(cudaMalloc(&b_lam.p, sizeof(double) * nf));
+    PB_CK(cudaMalloc(&b_lam_lo.p, sizeof(double) * nlo));
+    PB_CK(cudaMalloc(&b_lmst.p, sizeof(double) * nt));
+    PB_CK(cudaMalloc(&b_avg_lmst.p, sizeof(double)));
+    PB_CK(cudaMalloc(&b_xyz.p, sizeof(XYZ) * xyz_t.size()));
+    PB_CK(cudaMalloc(&b_uv_pc.p, sizeof(UVW) * (size_t)nt * nbl));
+    PB_CK(cudaMalloc(&b_uv_src.p, sizeof(UVW) * (size_t)ns * nt * nbl));
+    PB_CK(cudaMalloc(&b_uv_lo.p, sizeof(UVW) * (size_t)ns * nbl));
+    PB_CK(cudaMalloc(&b_models.p, need));
+    PB_CK(cudaMalloc(&b_dlo.p, sizeof(JonesF32) * (size_t)ns * nlo * nbl));
+    PB_CK(cudaMalloc(&b_mlo.p, sizeof(JonesF32) * (size_t)ns * nlo * nbl));
+    PB_CK(cudaMalloc(&b_mlo_rot.p, sizeof(JonesF32) * (size_t)ns * nlo * nbl));
+    PB_CK(cudaMalloc(&b_wlo.p, sizeof(float) * (size_t)nlo * nbl));
+    PB_CK(cudaMalloc(&b_scr.p, iono_batched_scratch_bytes(ns, nbl, nlo)));
+    PB_CK(cudaMalloc(&b_old.p, sizeof(IonoConsts) * ns));
+    PB_CK(cudaMalloc(&b_new.p, sizeof(IonoConsts) * ns));
+    PB_CK(cudaMemcpyAsync(b_lam.p, lam.data(), sizeof(double) * nf, cudaMemcpyHostToDevice, s));
+    PB_CK(cudaMemcpyAsync(b_lam_lo.p, lam_lo.data(), sizeof(double) * nlo, cudaMemcpyHostToDevice, s));
+    PB_CK(cudaMemcpyAsync(b_lmst.p, h_lmsts, sizeof(double) * nt, cudaMemcpyHostToDevice, s));
+    PB_CK(cudaMemcpyAsync(b_avg_lmst.p, &average_lmst, sizeof(double), cudaMemcpyHostToDevice, s));
+    PB_CK(cudaMemcpyAsync(b_xyz.p, xyz_t.data(), sizeof(XYZ) * xyz_t.size(), cudaMemcpyHostToDevice, s));
+    PB_CK(k_weights_average(d_weights_tfb, b_wlo.as<float>(), nt, nbl, nf, favg, s));
+    PB_CK(k_xyzs_to_uvws(b_xyz.as<XYZ>(), b_lmst.as<double>(), b_uv_pc.as<UVW>(), phase_centre, num_tiles, nbl, nt, s));
+    PB_CK(cudaMemsetAsync(b_models.p, 0, need, s));
+    if (points) PB_CK(cudaMalloc(&b_stage.p, sizeof(JonesF32) * (size_t)nf * nbl));
+    // per source: UVWs in its frame and its high-resolution model (once per timeblock)
+    for (int i = 0; i < ns; i++) {
+        UVW* uv = b_uv_src.as<UVW>() + (size_t)i * nt * nbl;
+        PB_CK(k_xyzs_to_uvws(b_xyz.as<XYZ>(), b_lmst.as<double>(), uv, h_source_positions[i], num_tiles, nbl, nt, s));
+        PB_CK(k_xyzs_to_uvws(b_xyz.as<XYZ>(), b_avg_lmst.as<double>(), b_uv_lo.as<UVW>() + (size_t)i * nbl,
+                             h_source_positions[i], num_tiles, nbl, 1, s));
+        HdcModeller* hm = nullptr;
+        int rc = hdc_modeller_new(&h_sources[i], 0, h_tile_xyzs, num_tiles, h_freqs, num_freqs, h_source_positions[i],
+                                  params->array_latitude_rad, params->beam_kind, HDC_PREDICT_DIRECT, &hm);
+        if (rc) return rc;
+        std::unique_ptr<Modeller> m(reinterpret_cast<Modeller*>(hm));
+        for (int t = 0; t < nt; t++) {
+            if (points) {
+                // predict all baselines, keep baseline 0's channel column
+                PB_CK(cudaMemsetAsync(b_stage.p, 0, sizeof(JonesF32) * (size_t)nf * nbl, s));
+                rc = m->model_uvws(h_lmsts[t], uv + (size_t)t * nbl, b_stage.as<JonesF32>(), s);
+                if (rc) return rc;
+                PB_CK(cudaMemcpy2DAsync(b_models.as<JonesF32>() + ((size_t)i * nt + t) * nf, sizeof(JonesF32),
+                                        b_stage.p, sizeof(JonesF32) * nbl, sizeof(JonesF32), nf,
+                                        cudaMemcpyDeviceToDevice, s));
+            } else {
+                rc = m->model_uvws(h_lmsts[t], uv + (size_t)t * nbl,
+                                   b_models.as<JonesF32>() + (size_t)i * nvis + (size_t)t * nf * nbl, s);
+                if (rc) return rc;
+            }
+        }
+    }
+
+    pb::SweepArgs A;
+    A.resid = d_resid_tfb;
+    A.w = d_weights_tfb;
+    A.models = points ? nullptr : b_models.as<JonesF32>();
+    A.ptab = points ? b_models.as<JonesF32>() : nullptr;
+    A.uv_pc = b_uv_pc.as<UVW>();
+    A.uv_src = b_uv_src.as<UVW>();
+    A.lambdas = b_lam.as<double>();
+    A.old = b_old.as<IonoConsts>();
+    A.neu = b_new.as<IonoConsts>();
+    A.d_lo = b_dlo.as<JonesF32>();
+    A.m_lo = b_mlo.as<JonesF32>();
+    A.nt = nt;
+    A.nf = nf;
+    A.nbl = nbl;
+    A.nsrc = ns;
+    A.favg = favg;
+    const size_t nbins = (size_t)nlo * nbl;
+    std::vector<IonoConsts> fit(ns), next(ns);
+    for (int pass = 0; pass < params->num_passes; pass++) {
+        PB_CK(cudaMemcpyAsync(b_old.p, h_iono_consts, sizeof(IonoConsts) * ns, cudaMemcpyHostToDevice, s));
+        const int v = pb::choose_variant(A, s);
+        pb::kVariants[v].launch(A, s);
+        PB_CK(cudaGetLastError());
+        for (int i = 0; i < ns; i++) fit[i] = IonoConsts{0.0, 0.0, 1.0};
+        const char* err = iono_loop_batched_on(b_dlo.as<JonesF32>(), b_wlo.as<float>(), b_mlo.as<JonesF32>(),
+                                               b_mlo_rot.as<JonesF32>(), b_scr.p, fit.data(), ns, nbl, nlo,
+                                               params->num_loops, b_uv_lo.as<UVW>(), b_lam_lo.as<double>(),
+                                               params->convergence, s);
+        if (err) {
+            set_error("hdc_peel_timeblock_batched: %s", err);
+            return HDC_ERR_CUDA;
+        }
+        for (int i = 0; i < ns; i++) {
+            const IonoConsts old = h_iono_consts[i];
+            IonoConsts c = {old.alpha + fit[i].alpha, old.beta + fit[i].beta, old.gain * fit[i].gain};
+            // the reference's revert rule (gpu.rs:541-627)
+            if (std::fabs(c.alpha) > 1e-3 || std::fabs(c.beta) > 1e-3 || c.gain < 0.0 || c.gain > 1.5) c = old;
+            next[i] = c;
+        }
+        PB_CK(cudaMemcpyAsync(b_new.p, next.data(), sizeof(IonoConsts) * ns, cudaMemcpyHostToDevice, s));
+        pb::apply_kernel<<<(unsigned)((nvis + 255) / 256), 256, 0, s>>>(d_resid_tfb, A);
+        count_launches(1);
+        PB_CK(cudaGetLastError());
+        PB_CK(cudaStreamSynchronize(s));  // `next` is read by the copy above
+        for (int i = 0; i < ns; i++) h_iono_consts[i] = next[i];
+    }
+    (void)nbins;
+    PB_CK(cudaStreamSynchronize(s));
+    return HDC_OK;
+}
+
+extern "C" int hdc_peel_batched_tuning(int* block_bins, int* block_sources, float* ms) {
+    std::lock_guard<std::mutex> lk(pb::g_tune_mu);
+    if (block_bins) *block_bins = pb::g_last.bx;
+    if (block_sources) *block_sources = pb::g_last.sy;
+    if (ms) *ms = pb::g_last.ms;
+    return HDC_OK;
+}

@@ -42,9 +42,12 @@ class PeelLoopParams:
 def peel_timeblock(d_resid_tfb, d_weights_tfb, freqs, tile_xyzs, lmsts, average_lmst, phase_centre, sources,
                    source_positions, iono_consts: Sequence[IonoConsts], num_passes: int, num_loops: int,
                    convergence: float, freq_average_factor: int, array_latitude_rad: float, beam: str = "none",
-                   stream=None) -> List[IonoConsts]:
+                   stream=None, batched: bool = False) -> List[IonoConsts]:
     """Peel ``sources`` (a list of SourceList / Source / SkyModelArrays, one per
-    source) with explicit pass and loop counts."""
+    source) with explicit pass and loop counts.  ``batched`` selects
+    hdc_peel_timeblock_batched (all sources of a pass fitted together against
+    the residual at the start of the pass) instead of the reference's
+    source-by-source order."""
     nt, nf, nbl = (int(x) for x in d_resid_tfb.shape[:3])
     freqs = np.ascontiguousarray(freqs, np.float64)
     xyzs = np.ascontiguousarray(tile_xyzs, np.float64).reshape(-1, 3)
@@ -60,11 +63,12 @@ def peel_timeblock(d_resid_tfb, d_weights_tfb, freqs, tile_xyzs, lmsts, average_
     consts = (_lib.IonoConsts * max(n, 1))(*[_lib.IonoConsts(c.alpha, c.beta, c.gain) for c in iono_consts])
     params = _lib.HdcPeelParams(int(num_passes), int(num_loops), float(convergence), int(freq_average_factor),
                                 BEAMS[beam], float(array_latitude_rad))
-    rc = _lib.lib().hdc_peel_timeblock(d_resid_tfb.data_ptr(), d_weights_tfb.data_ptr(), nt, nf, freqs.ctypes.data,
-                                       xyzs.ctypes.data, xyzs.shape[0], lmsts.ctypes.data, float(average_lmst),
-                                       _lib.RADec(*phase_centre), n, ctypes.addressof(structs), ctypes.addressof(pos),
-                                       ctypes.addressof(consts), ctypes.byref(params), _stream_ptr(stream))
-    _lib.check(rc, "hdc_peel_timeblock")
+    fn = _lib.lib().hdc_peel_timeblock_batched if batched else _lib.lib().hdc_peel_timeblock
+    rc = fn(d_resid_tfb.data_ptr(), d_weights_tfb.data_ptr(), nt, nf, freqs.ctypes.data, xyzs.ctypes.data,
+            xyzs.shape[0], lmsts.ctypes.data, float(average_lmst), _lib.RADec(*phase_centre), n,
+            ctypes.addressof(structs), ctypes.addressof(pos), ctypes.addressof(consts), ctypes.byref(params),
+            _stream_ptr(stream))
+    _lib.check(rc, "hdc_peel_timeblock_batched" if batched else "hdc_peel_timeblock")
     return [IonoConsts(consts[i].alpha, consts[i].beta, consts[i].gain) for i in range(n)]
 
 
@@ -81,3 +85,12 @@ def peel_gpu(d_resid_tfb, d_weights_tfb, freqs, tile_xyzs, lmsts, average_lmst, 
     return peel_timeblock(d_resid_tfb, d_weights_tfb, freqs, tile_xyzs, lmsts, average_lmst, phase_centre, sources,
                           source_positions, iono_consts, num_passes, num_loops, convergence, freq_average_factor,
                           array_latitude_rad, beam, stream)
+
+
+def batched_tuning():
+    """(bins per CTA, sources per CTA, ms) the batched peel's autotuner chose
+    for the last new problem shape."""
+    bx, sy, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_float()
+    _lib.check(_lib.lib().hdc_peel_batched_tuning(ctypes.byref(bx), ctypes.byref(sy), ctypes.byref(ms)),
+               "hdc_peel_batched_tuning")
+    return bx.value, sy.value, ms.value

@@ -155,7 +155,7 @@ def test_iono_loop_matches_oracle(oracle):
 
 
 # ---------------------------------------------------------------- peel loop
-def make_peel_problem(seed=3, ntiles=20, nt=2, nf=8, nsrc=3, inject=True):
+def make_peel_problem(seed=3, ntiles=20, nt=2, nf=8, nsrc=3, inject=True, points=False):
     rng, pc, xyzs, freqs, lmsts = setup(ntiles, nt, nf, seed)
     nbl = ntiles * (ntiles - 1) // 2
     lam = VEL_C / freqs
@@ -165,7 +165,7 @@ def make_peel_problem(seed=3, ntiles=20, nt=2, nf=8, nsrc=3, inject=True):
         dec = pc[1] + math.radians(rng.uniform(-3, 3))
         comps = [sl.SourceComponent(ra + math.radians(0.02 * k), dec, sl.Point(),
                                     sl.PowerLaw(-0.8, sl.FluxDensity(150e6, float(rng.uniform(2, 6)))))
-                 for k in range(2)]
+                 for k in range(1 if points else 2)]
         sources.append(sl.SkyModelArrays.from_components(comps))
         positions.append((ra, dec))
         truths.append((rng.normal(0, 2e-5), rng.normal(0, 2e-5), rng.uniform(0.95, 1.05)) if inject else (0, 0, 1))
@@ -264,4 +264,60 @@ def test_native_peel_recovers_injected_iono(oracle):
         assert abs(g.alpha - tr[0]) < 0.02 * abs(tr[0]) + 2e-7, (g, tr)
         assert abs(g.beta - tr[1]) < 0.02 * abs(tr[1]) + 2e-7, (g, tr)
         assert abs(g.gain - tr[2]) < 5e-3, (g, tr)
+    assert after < 0.05 * before, (after, before)
+
+
+# ------------------------------------------------------------ batched peel
+@pytest.mark.parametrize("points", [False, True])
+def test_batched_peel_single_source_equals_sequential(oracle, points):
+    """With one source the batched (Jacobi) pass is the reference's sequence:
+    same constants and residual up to rounding (FP64 instead of f32
+    intermediates).  points: one point at the source position (the
+    per-(timestep, channel) model table) instead of a two-component source
+    (materialised model)."""
+    rng, pc, xyzs, freqs, lmsts, lam, nbl, sources, positions, truths = make_peel_problem(seed=5, nsrc=1,
+                                                                                           points=points)
+    resid = simulate_residual(oracle, pc, xyzs, freqs, lmsts, lam, sources, positions, truths)
+    weights = np.ones(resid.shape[:3], np.float32)
+    weights[:, :, ::5] = 0.5
+    avg_lmst = float(np.median(lmsts))
+    out = {}
+    for batched in (False, True):
+        d_resid = dev(resid, np.float32)
+        c = P.peel_timeblock(d_resid, dev(weights, np.float32), freqs, xyzs, lmsts, avg_lmst, pc, sources, positions,
+                             [P.IonoConsts()], num_passes=2, num_loops=5, convergence=1.0, freq_average_factor=4,
+                             array_latitude_rad=synth.MWA_LAT_RAD, batched=batched)
+        out[batched] = (c[0], d_resid.cpu().numpy())
+    (cs, rs), (cb, rb) = out[False], out[True]
+    assert abs(cb.alpha - cs.alpha) <= 1e-5 * abs(cs.alpha) + 1e-12, (cb, cs)
+    assert abs(cb.beta - cs.beta) <= 1e-5 * abs(cs.beta) + 1e-12, (cb, cs)
+    assert abs(cb.gain - cs.gain) <= 1e-6, (cb, cs)
+    # the peeled residuals are at rounding level; compare on the input's scale
+    assert np.linalg.norm(rb.astype(np.float64) - rs) / np.linalg.norm(resid) < 1e-4
+    bx, sy, ms = P.batched_tuning()
+    assert bx * sy == 256 and ms > 0
+
+
+def test_batched_peel_recovers_injected_iono(oracle):
+    rng, pc, xyzs, freqs, lmsts, lam, nbl, sources, positions, truths = make_peel_problem(seed=7, ntiles=32, nf=16,
+                                                                                           nsrc=4)
+    resid = simulate_residual(oracle, pc, xyzs, freqs, lmsts, lam, sources, positions, truths)
+    before = np.linalg.norm(resid)
+    weights = np.ones(resid.shape[:3], np.float32)
+    got = {}
+    for batched in (False, True):
+        d_resid = dev(resid, np.float32)
+        got[batched] = P.peel_timeblock(d_resid, dev(weights, np.float32), freqs, xyzs, lmsts,
+                                        float(np.median(lmsts)), pc, sources, positions,
+                                        [P.IonoConsts() for _ in sources], num_passes=3, num_loops=10,
+                                        convergence=1.0, freq_average_factor=4,
+                                        array_latitude_rad=synth.MWA_LAT_RAD, batched=batched)
+        if batched:
+            after = np.linalg.norm(d_resid.cpu().numpy())
+    for g, s_, tr in zip(got[True], got[False], truths):
+        assert abs(g.alpha - tr[0]) < 0.02 * abs(tr[0]) + 2e-7, (g, tr)
+        assert abs(g.beta - tr[1]) < 0.02 * abs(tr[1]) + 2e-7, (g, tr)
+        assert abs(g.gain - tr[2]) < 5e-3, (g, tr)
+        # Jacobi and Gauss-Seidel agree once the passes have converged
+        assert abs(g.alpha - s_.alpha) < 0.01 * abs(s_.alpha) + 1e-7, (g, s_)
     assert after < 0.05 * before, (after, before)

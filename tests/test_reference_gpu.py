@@ -117,7 +117,10 @@ def dropin_inputs(oracle, ntiles, nf, ncomp_per_group, ctype, seed, ntile_beams=
     co["n2"] = [0, 3] * n
     coeffs = dev(co.view(np.uint8), np.uint8).data_ptr()
     ncoef = dev(np.full(n, 2, np.int32), np.int32).data_ptr()
-    a = _lib.Addresses(nf, nf * nbl, nbl, dev(obs.freqs).data_ptr(), 0, nfreq_beams,
+    # the reference's shapelet kernel reads the basis table through Addresses
+    sbf = np.zeros(101 * 10001)
+    _lib.lib().hdc_shapelet_basis(sbf.ctypes.data)
+    a = _lib.Addresses(nf, nf * nbl, nbl, dev(obs.freqs).data_ptr(), dev(sbf).data_ptr(), nfreq_beams,
                        dev(tile_map, np.int32).data_ptr(), dev(freq_map, np.int32).data_ptr(),
                        dev(np.arange(ntiles, dtype=np.int32), np.int32).data_ptr())
     o = lambda g: lm + g * m * 24  # noqa: E731
