@@ -166,6 +166,34 @@ __device__ __forceinline__ cplx phasor_turns(double t) {
     return {c, s};
 }
 
+// FP32 phasor for the tensor-core predict and the chosen form's direct
+// kernels: sin and cos of 2 pi z for z in quarter-turns.  q = rint(z) and
+// r = z - q are exact in FP64; sin and cos of (pi/2) r come from
+// least-squares polynomials in r^2 on |r| <= 1/2 (fitted by
+// mwa_hyperdrive_b200/phasor_poly.py, < 0.75 float32 ulp); the quadrant
+// q mod 4 swaps and signs them.
+constexpr double QMAGIC = 6755399441055744.0;  // 1.5 * 2^52: adding it rounds to an integer held in the low word
+constexpr float PS0 = 1.570796371e+00f, PS1 = -6.459634900e-01f, PS2 = 7.968021929e-02f,
+                PS3 = -4.602163099e-03f;
+constexpr float PC0 = 1.000000000e+00f, PC1 = -1.233700514e+00f, PC2 = 2.536692023e-01f,
+                PC3 = -2.086007036e-02f, PC4 = 9.036298725e-04f;
+
+__device__ __forceinline__ void phasor_quarter_f32(double z, float& sn, float& cs) {
+    const double zq = __dadd_rn(z, QMAGIC);
+    const int q = __double2loint(zq);
+    const float r = (float)__dsub_rn(z, __dsub_rn(zq, QMAGIC));
+    const float r2 = r * r;
+    const float ps = fmaf(fmaf(fmaf(PS3, r2, PS2), r2, PS1), r2, PS0) * r;
+    const float pc = fmaf(fmaf(fmaf(fmaf(PC4, r2, PC3), r2, PC2), r2, PC1), r2, PC0);
+    // angle = (pi/2)(q + r): odd q swaps sin and cos; sin takes the sign of
+    // bit 1 of q, cos that of bit 1 of q + 1 (moved to bit 31 by << 30)
+    const bool odd = q & 1;
+    const float a = odd ? pc : ps, b = odd ? ps : pc;
+    const uint32_t qs = (uint32_t)q << 30;
+    sn = __uint_as_float(__float_as_uint(a) ^ (qs & 0x80000000u));
+    cs = __uint_as_float(__float_as_uint(b) ^ ((qs + 0x40000000u) & 0x80000000u));
+}
+
 }  // namespace hdc
 
 // ---------------------------------------------------------------------------
@@ -183,6 +211,7 @@ int* device_error_word();
 int take_device_error(cudaStream_t s);
 // Shapelet basis table on the current device (SBF_N x SBF_L doubles).
 const double* device_shapelet_basis();
+const float* device_shapelet_basis_f32();
 void host_shapelet_basis(double* out);
 // Count of kernel launches made by libhdc (diagnostics).
 void count_launches(int n);

@@ -382,6 +382,7 @@ DirectParams Modeller::direct_params(int ty, void* vis) const {
     p.flux = weights(ty);
     p.gp = t[ty].d_gp;
     p.sbf = d_sbf;
+    p.sbf32 = form == HDC_PREDICT_TENSOR ? device_shapelet_basis_f32() : nullptr;
     p.coeffs = t[ty].d_coeffs;
     p.coeff_start = t[ty].d_cstart;
     p.coeff_count = t[ty].d_ccount;
@@ -434,7 +435,10 @@ int Modeller::model(double lst, void* d_vis, bool out64, UVW* h_uvws, cudaStream
             rc = tensor_points(lst, d_vis, out64, s);
             if (rc) return rc;
         } else {
-            HDC_CUDA_RET_INT(launch_direct(ty, false, out64, direct_params(ty, d_vis), s));
+            // the chosen (tensor) form keeps Gaussians and shapelets in the
+            // direct kernel, in its FP32 form
+            HDC_CUDA_RET_INT(launch_direct(ty, false, out64, direct_params(ty, d_vis), s,
+                                           form == HDC_PREDICT_TENSOR));
         }
         prof_end(s, e);
     }

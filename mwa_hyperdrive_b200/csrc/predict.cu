@@ -54,11 +54,54 @@ __device__ __forceinline__ cplx shapelet_envelope(const DirectParams& p, int c, 
     return env;
 }
 
-template <int TYPE, bool TILE_BEAM, bool OUT64>
+// The chosen form's shapelet envelope: table positions in FP64 (an FP32
+// position near 5000 would move the interpolation point by ~1e-3 of a table
+// step), basis values from the FP32 copy of the table, interpolation and
+// products in FP32.
+__device__ __forceinline__ void shapelet_envelope_f32(const DirectParams& p, int c, double4 g, double su, double sv,
+                                                      float& er, float& ei) {
+    const double x = su * g.z + sv * g.w;
+    const double y = su * g.w - sv * g.z;
+    const double x_pos = x * g.x + SBF_C;
+    const double y_pos = y * g.y + SBF_C;
+    const double fx = floor(x_pos), fy = floor(y_pos);
+    const int xi = fx > 0.0 ? (int)fmin(fx, (double)(SBF_L - 2)) : 0;
+    const int yi = fy > 0.0 ? (int)fmin(fy, (double)(SBF_L - 2)) : 0;
+    const float xfrac = (float)(x_pos - fx), yfrac = (float)(y_pos - fy);
+    const int start = __ldg(p.coeff_start + c), count = __ldg(p.coeff_count + c);
+    float re = 0.f, im = 0.f;
+    for (int i = 0; i < count; i++) {
+        const ShapeletCoeff co = p.coeffs[start + i];
+        const float* bx = p.sbf32 + (size_t)SBF_L * co.n1 + xi;
+        const float* by = p.sbf32 + (size_t)SBF_L * co.n2 + yi;
+        const float2 xv = make_float2(__ldg(bx), __ldg(bx + 1));
+        const float2 yv = make_float2(__ldg(by), __ldg(by + 1));
+        const float u_value = fmaf(xv.y - xv.x, xfrac, xv.x);
+        const float v_value = fmaf(yv.y - yv.x, yfrac, yv.x);
+        const float rest = (float)co.value * u_value * v_value;
+        switch ((co.n1 + co.n2) & 3) {
+            case 0: re += rest; break;
+            case 1: im += rest; break;
+            case 2: re -= rest; break;
+            default: im -= rest; break;
+        }
+    }
+    er = re;
+    ei = im;
+}
+
+// FAST (the chosen form's Gaussians and shapelets, shared beam only): the
+// phasor from the FP32 quarter-turn polynomials after exact FP64 range
+// reduction, envelopes in FP32 (arguments and table positions in FP64),
+// each component's term W ph env in FP32
+// (W staged once per chunk as FP32), summed in FP32 within a 64-component
+// chunk and in FP64 across chunks.  Error ~1e-7 of the visibility.
+template <int TYPE, bool TILE_BEAM, bool OUT64, bool FAST>
 __global__ void __launch_bounds__(DT) direct_kernel(const DirectParams p) {
     __shared__ alignas(128) double4 s_lmn[2][CH];
     __shared__ alignas(128) JonesF64 s_flux[2][CH];
     __shared__ alignas(128) double4 s_gp[2][CH];
+    __shared__ alignas(16) float s_wf[FAST ? CH * 8 : 1];
     __shared__ alignas(8) uint64_t bar[2];
 
     const int f = blockIdx.y;
@@ -123,7 +166,45 @@ __global__ void __launch_bounds__(DT) direct_kernel(const DirectParams p) {
         if (__syncthreads_or(!ok)) break;
         const int c0 = k * CH;
         const int n = min(CH, p.nc - c0);
-        if (active) {
+        if (FAST) {
+            const double* src = reinterpret_cast<const double*>(s_flux[st]);
+            for (int i = threadIdx.x; i < n * 8; i += DT) s_wf[i] = (float)src[i];
+            __syncthreads();
+        }
+        if (FAST && active) {
+            float a[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            for (int c = 0; c < n; c++) {
+                const double4 lmn = s_lmn[st][c];
+                float sn, cs;
+                phasor_quarter_f32(4.0 * (u * lmn.x + v * lmn.y + w * lmn.z), sn, cs);
+                float er = 1.f, ei = 0.f;
+                if (TYPE == 1) {
+                    // the exponent in FP64 (an FP32 exponent's absolute error,
+                    // ~1e-7 of its size, would become the envelope's relative
+                    // error); exp of its FP32 head, first order in the tail
+                    const double4 g = s_gp[st][c];
+                    const double kx = u * g.z + v * g.w;
+                    const double ky = u * g.w - v * g.z;
+                    const double ex = g.x * (kx * kx) + g.y * (ky * ky);
+                    const float exh = (float)ex;
+                    er = expf(exh) * (1.f + (float)(ex - (double)exh));
+                } else if (TYPE == 2) {
+                    const double4 g = s_gp[st][c];
+                    const double2 ta = __ldg(p.suv_tile + (size_t)(c0 + c) * p.ntiles + t1);
+                    const double2 tb = __ldg(p.suv_tile + (size_t)(c0 + c) * p.ntiles + t2);
+                    shapelet_envelope_f32(p, c0 + c, g, (ta.x - tb.x) * ool, (ta.y - tb.y) * ool, er, ei);
+                }
+                // ph * env
+                const float zr = cs * er - sn * ei, zi = fmaf(cs, ei, sn * er);
+                const float* wv = s_wf + c * 8;
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    a[2 * e] += fmaf(wv[2 * e], zr, -wv[2 * e + 1] * zi);
+                    a[2 * e + 1] += fmaf(wv[2 * e], zi, wv[2 * e + 1] * zr);
+                }
+            }
+            acc = acc + J2{{a[0], a[1]}, {a[2], a[3]}, {a[4], a[5]}, {a[6], a[7]}};
+        } else if (active) {
             for (int c = 0; c < n; c++) {
                 const double4 lmn = s_lmn[st][c];
                 J2 wj = load_j(s_flux[st][c]);
@@ -193,28 +274,35 @@ __global__ void __launch_bounds__(DT) direct_kernel(const DirectParams p) {
 }
 
 template <int TYPE>
-static cudaError_t launch_t(bool tile_beam, bool out64, const DirectParams& p, cudaStream_t s) {
+static cudaError_t launch_t(bool tile_beam, bool out64, bool fast, const DirectParams& p, cudaStream_t s) {
     dim3 grid((p.nbl + DT - 1) / DT, p.nf);
     if (tile_beam) {
         if (out64)
-            direct_kernel<TYPE, true, true><<<grid, DT, 0, s>>>(p);
+            direct_kernel<TYPE, true, true, false><<<grid, DT, 0, s>>>(p);
         else
-            direct_kernel<TYPE, true, false><<<grid, DT, 0, s>>>(p);
+            direct_kernel<TYPE, true, false, false><<<grid, DT, 0, s>>>(p);
+    } else if (fast) {
+        if (out64)
+            direct_kernel<TYPE, false, true, true><<<grid, DT, 0, s>>>(p);
+        else
+            direct_kernel<TYPE, false, false, true><<<grid, DT, 0, s>>>(p);
     } else {
         if (out64)
-            direct_kernel<TYPE, false, true><<<grid, DT, 0, s>>>(p);
+            direct_kernel<TYPE, false, true, false><<<grid, DT, 0, s>>>(p);
         else
-            direct_kernel<TYPE, false, false><<<grid, DT, 0, s>>>(p);
+            direct_kernel<TYPE, false, false, false><<<grid, DT, 0, s>>>(p);
     }
     count_launches(1);
     return cudaGetLastError();
 }
 
-cudaError_t launch_direct(int ty, bool tile_beam, bool out64, const DirectParams& p, cudaStream_t s) {
+cudaError_t launch_direct(int ty, bool tile_beam, bool out64, const DirectParams& p, cudaStream_t s, bool fast) {
     if (p.nc <= 0 || p.nbl <= 0 || p.nf <= 0) return cudaSuccess;
-    if (ty == 0) return launch_t<0>(tile_beam, out64, p, s);
-    if (ty == 1) return launch_t<1>(tile_beam, out64, p, s);
-    return launch_t<2>(tile_beam, out64, p, s);
+    // the FP32 form needs per-tile shapelet UVs and the FP32 basis table
+    fast = fast && !tile_beam && (ty != 2 || (p.suv_tile && !p.suv_bl && p.sbf32));
+    if (ty == 0) return launch_t<0>(tile_beam, out64, fast, p, s);
+    if (ty == 1) return launch_t<1>(tile_beam, out64, fast, p, s);
+    return launch_t<2>(tile_beam, out64, fast, p, s);
 }
 
 // Auto-correlations: one thread per (tile, channel) (gpu/model.cu:368-485;

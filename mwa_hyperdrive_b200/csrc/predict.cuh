@@ -25,6 +25,7 @@ struct DirectParams {
     int n_uniq_freq;
     // shapelets
     const double* sbf;  // [SBF_N][SBF_L]
+    const float* sbf32; // the same table in FP32 (chosen form), or NULL
     const ShapeletCoeff* coeffs;
     const int* coeff_start;
     const int* coeff_count;
@@ -35,8 +36,10 @@ struct DirectParams {
 };
 
 // Launch the direct kernel for component type ty (0 point, 1 Gaussian,
-// 2 shapelet).  tile_beam selects per-tile beam Jones; out64 an FP64 output.
-cudaError_t launch_direct(int ty, bool tile_beam, bool out64, const DirectParams& p, cudaStream_t s);
+// 2 shapelet).  tile_beam selects per-tile beam Jones; out64 an FP64 output;
+// fast the FP32 form (errors ~1e-7 of the visibility; shared beam only).
+cudaError_t launch_direct(int ty, bool tile_beam, bool out64, const DirectParams& p, cudaStream_t s,
+                          bool fast = false);
 
 struct AutosParams {
     int ntiles, nf;

@@ -83,19 +83,11 @@ constexpr int SBO = (KC / 16) * 128; // bytes between 8-row groups
 constexpr int TMEM_COLS = 512;       // 4 classes x NB
 constexpr int KPASS = 16384;         // components per launch: 3 pairs x 2 x 2^14 x KPASS < 2^31
 constexpr float SY = 4128768.0f;     // 2^22 - 2^16: |A| <= 1 -> |y| < 2^22
-constexpr double QMAGIC = 6755399441055744.0;  // 1.5 * 2^52: adding it rounds to an integer held in the low word
 // y + 0x8080 as FP32 bits: 1.5 * 2^23 rounds |v| < 2^22 to an integer in
 // the mantissa; the extra 0x8080 is the balancing offset of the two lower
 // digits.  The mantissa field then holds 2^22 + 0x8080 + y, so byte 2 is the
 // top digit + 0x40 and bytes 1, 0 the excess-128 lower digits.
 constexpr float YOFF = 12582912.0f + 32896.0f;
-
-// sin(pi/2 r) / r and cos(pi/2 r) in powers of r^2 on |r| <= 1/2
-// (mwa_hyperdrive_b200/phasor_poly.py)
-constexpr float PS0 = 1.570796371e+00f, PS1 = -6.459634900e-01f, PS2 = 7.968021929e-02f,
-                PS3 = -4.602163099e-03f;
-constexpr float PC0 = 1.000000000e+00f, PC1 = -1.233700514e+00f, PC2 = 2.536692023e-01f,
-                PC3 = -2.086007036e-02f, PC4 = 9.036298725e-04f;
 
 // component data of one stage, staged in shared memory (structure of arrays
 // so that 16-byte loads of consecutive components are conflict-free)
@@ -181,24 +173,6 @@ __device__ __forceinline__ void byte_planes4(const int* v, uint32_t* w) {
 // a plain XOR 0x80.
 __device__ __forceinline__ uint32_t minus64(uint32_t w) {
     return w ^ 0x40404040u ^ ((~w & 0x40404040u) << 1);
-}
-
-// sin and cos of 2 pi z for z in quarter-turns: q = rint(z) and r = z - q
-// exactly in FP64, then the FP32 polynomials on r and the quadrant q mod 4.
-__device__ __forceinline__ void phasor_quadrant(double z, float& sn, float& cs) {
-    const double zq = __dadd_rn(z, QMAGIC);
-    const int q = __double2loint(zq);
-    const float r = (float)__dsub_rn(z, __dsub_rn(zq, QMAGIC));
-    const float r2 = r * r;
-    const float ps = fmaf(fmaf(fmaf(PS3, r2, PS2), r2, PS1), r2, PS0) * r;
-    const float pc = fmaf(fmaf(fmaf(fmaf(PC4, r2, PC3), r2, PC2), r2, PC1), r2, PC0);
-    // angle = (pi/2)(q + r): odd q swaps sin and cos; sin takes the sign of
-    // bit 1 of q, cos that of bit 1 of q + 1 (moved to bit 31 by << 30)
-    const bool odd = q & 1;
-    const float a = odd ? pc : ps, b = odd ? ps : pc;
-    const uint32_t qs = (uint32_t)q << 30;
-    sn = __uint_as_float(__float_as_uint(a) ^ (qs & 0x80000000u));
-    cs = __uint_as_float(__float_as_uint(b) ^ ((qs + 0x40000000u) & 0x80000000u));
 }
 
 // all producer threads: barrier 1, true when any of them passed true
@@ -365,7 +339,7 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const Params P) {
 #pragma unroll
                 for (int s2 = 0; s2 < 2; s2++) {
                     float sn, cs;
-                    phasor_quadrant(u[s2] * cl[j] + v[s2] * cm[j] + w[s2] * cn[j], sn, cs);
+                    phasor_quarter_f32(u[s2] * cl[j] + v[s2] * cm[j] + w[s2] * cn[j], sn, cs);
                     const float Xr = fmaf(wr[j], cs, -wi[j] * sn);
                     const float Xi = fmaf(wr[j], sn, wi[j] * cs);
                     // x + 0x808080 (balancing offset of the three lower digits)

@@ -1,5 +1,6 @@
 """Coefficients of the single-precision phasor polynomials used by the
-tensor-core point predict (csrc/tensor.cu, `phasor_quadrant`).
+tensor-core point predict and the chosen form's direct kernels
+(csrc/common.cuh, `phasor_quarter_f32`).
 
 The phase enters as r in quarter-turns, |r| <= 1/2 after the quadrant is
 split off in FP64, so the polynomials approximate
@@ -14,7 +15,7 @@ rule (fused multiply-adds emulated in float64 then rounded, as the GPU's FMA
 does) against float64 numpy and reports the error in float32 ulps of 1.
 
 Run `python -m mwa_hyperdrive_b200.phasor_poly` to print the constants that
-csrc/tensor.cu holds.
+csrc/common.cuh holds.
 """
 
 from __future__ import annotations

@@ -1,5 +1,5 @@
 """The tensor-core predict's FP32 phasor: polynomial accuracy and the quadrant
-mapping (a numpy emulation of csrc/tensor.cu phasor_quadrant, FP64
+mapping (a numpy emulation of csrc/common.cuh phasor_quarter_f32, FP64
 reduction then FP32 polynomials), no GPU."""
 
 import re
@@ -9,7 +9,7 @@ import numpy as np
 
 from mwa_hyperdrive_b200 import phasor_poly
 
-SRC = Path(__file__).resolve().parents[1] / "mwa_hyperdrive_b200" / "csrc" / "tensor.cu"
+SRC = Path(__file__).resolve().parents[1] / "mwa_hyperdrive_b200" / "csrc" / "common.cuh"
 
 
 def kernel_constants():

@@ -99,6 +99,19 @@ def test_mixed_types_tensor_form_keeps_direct_gaussians_and_shapelets(oracle):
     assert nrm < TOL and p999 < TOL, (nrm, p999, mx)
 
 
+def test_chosen_form_gaussians_and_shapelets_fp32(oracle):
+    """The chosen form runs Gaussians and shapelets in the direct kernel's FP32
+    form (FP32 phasor, envelope and terms; FP64 across chunks): same 1e-6 bars."""
+    obs, _ = synth.config2(n_points=1, n_gauss=1, n_shapelets=1, n_freqs=5, n_times=1)
+    sky = sl.SkyModelArrays.from_components(synth.gaussians_and_shapelets(60, 12, obs.phase_centre, 9))
+    got = run(sky, obs, obs.lsts[0], "tensor", beam="analytic")
+    ref, _ = oracle.model_timestep(sky, obs.tile_xyzs, obs.freqs, obs.phase_centre, obs.lsts[0], obs.latitude,
+                                   beam=oracle.beam_struct(1), out_f64=True)
+    nrm, p999, mx = errors(got, ref)
+    print(f"FP32 Gaussians + shapelets: normwise {nrm:.2e}, p99.9 {p999:.2e}, max {mx:.2e}")
+    assert nrm < TOL and p999 < TOL, (nrm, p999, mx)
+
+
 @pytest.mark.parametrize("ntiles,npts", [(64, 4500), (24, 16500)])
 def test_many_components(oracle, ntiles, npts):
     """Errors must not grow with the component count; 16500 components need
