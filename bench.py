@@ -665,7 +665,7 @@ def gpu_arm(args, rank, world, local_rank):
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_chosen, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64" if form == "direct" else "f64 phases, s8 digit planes with exact s32 accumulation (points); f64 (Gaussians, shapelets)",
+            "vs_baseline": None, "dtype": "f64" if form == "direct" else "f64 phases, s8 digit planes with exact s32 accumulation (points); f32 terms with f64 arguments and chunk sums (Gaussians, shapelets)",
             "data": "synthetic (seeded)", "config": config_dict(obs, sky, form),
             "plain": {"form": "direct", "value": work * world / (ms_plain * 1e-3), "ms_per_step": ms_plain},
             "e2e": None if e2e_s is None else {"value": work * world / e2e_s, "unit": UNIT,
