@@ -409,6 +409,33 @@ int hdc_mlp_gradients(HdcMlp *m, const float *d_x, const float *d_target, int ba
 int hdc_mlp_train_step(HdcMlp *m, const float *d_x, const float *d_target, int batch, float lr, double *h_loss,
                        hdcStream_t stream);
 
+/* Warm-start chain on the device, one stream, no host synchronisation.
+ * d_prev_tc [tile][chanblock] are the previous timeblock's solutions (NaN
+ * where failed).  hdc_warmstart_features writes the network inputs d_x
+ * [tile*chanblock][40] (FP32): per (tile, chanblock) the gauge-aligned
+ * solutions at chanblocks c-2..c+2 in the frame of the centre's XX and YY
+ * gains, band edges extrapolated through the centre.
+ * hdc_warmstart_propose runs features, the network (40 inputs, 8 outputs)
+ * and the mapping back to gains; with d_data_tfb and d_model_tfb non-NULL it
+ * then judges every chanblock's proposal by its calibration residual over
+ * the timeblock against the identity start and writes the chosen start to
+ * d_start_tc [tile][chanblock] (d_use [chanblock], may be NULL: 1 where the
+ * proposal was kept); with both NULL d_start_tc gets the proposal itself.
+ * No counterpart in the reference (its solver starts from identity,
+ * di_calibrate/mod.rs:283-287). */
+int hdc_warmstart_features(const JonesF64 *d_prev_tc, int num_tiles, int num_chanblocks, float *d_x,
+                           hdcStream_t stream);
+/* The judge alone: per chanblock keep d_proposal_tc where its residual is
+ * finite and no larger than the identity start's, else identity, into
+ * d_start_tc (a different buffer); d_use as above. */
+int hdc_warmstart_judge(const JonesF32 *d_data_tfb, const JonesF32 *d_model_tfb, int num_timesteps,
+                        int timeblock_start, int timeblock_end, int num_chanblocks, int num_tiles,
+                        const JonesF64 *d_proposal_tc, JonesF64 *d_start_tc, int *d_use, hdcStream_t stream);
+int hdc_warmstart_propose(HdcMlp *mlp, const JonesF64 *d_prev_tc, int num_tiles, int num_chanblocks,
+                          const JonesF32 *d_data_tfb, const JonesF32 *d_model_tfb, int num_timesteps,
+                          int timeblock_start, int timeblock_end, JonesF64 *d_start_tc, int *d_use,
+                          hdcStream_t stream);
+
 /* Peel loop controls (PeelLoopParams and PeelWeightParams' consumers,
  * params/peel/mod.rs:207-224).  num_passes is the number of passes over all
  * sources, num_loops the iono-fit iterations per source.  (The reference's

@@ -135,6 +135,11 @@ SIGNATURES = {
     "hdc_mlp_forward": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p]),
     "hdc_mlp_gradients": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
     "hdc_mlp_train_step": (c_int, [c_void_p, c_void_p, c_void_p, c_int, ctypes.c_float, c_void_p, c_void_p]),
+    "hdc_warmstart_features": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p]),
+    "hdc_warmstart_judge": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p,
+                                    c_void_p, c_void_p]),
+    "hdc_warmstart_propose": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p, c_int, c_int, c_int,
+                                      c_void_p, c_void_p, c_void_p]),
     "hdc_kernel_launches": (ctypes.c_longlong, []),
     "hdc_modeller_set_profiling": (c_int, [c_void_p, c_int]),
     "hdc_modeller_profile": (c_int, [c_void_p, c_void_p, c_int]),

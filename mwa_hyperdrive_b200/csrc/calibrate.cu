@@ -545,6 +545,74 @@ __global__ void __launch_bounds__(CT) residual_kernel(const CalParams P, const J
     }
 }
 
+// Device-side judge of a proposed start: one pass over the timeblock forms
+// the calibration residuals of the proposal dprop and of the identity start
+// together; the proposal is kept (use[ch] = 1) where its residual is finite
+// and no larger, and the chosen start is written to dstart [tile][chanblock].
+__global__ void __launch_bounds__(CT) judge_kernel(const CalParams P, const JonesF64* dprop, JonesF64* dstart,
+                                                   int* use) {
+    const int ch = blockIdx.x;
+    const int nt = P.t1 - P.t0;
+    const size_t tstride = (size_t)P.nchan * P.nbl;
+    const JonesF32* D0 = P.data + ((size_t)P.t0 * P.nchan + ch) * P.nbl;
+    const JonesF32* M0 = P.model + ((size_t)P.t0 * P.nchan + ch) * P.nbl;
+    double acc_p = 0.0, acc_i = 0.0;
+    for (int bl = threadIdx.x; bl < P.nbl; bl += CT) {
+        int p, q;
+        baseline_to_tiles(bl, P.ntiles, p, q);
+        const J2 gp = load_j(dprop[(size_t)p * P.nchan + ch]);
+        const J2 gqh = herm(load_j(dprop[(size_t)q * P.nchan + ch]));
+        for (int t = 0; t < nt; t++) {
+            const J2 d = load_vis(D0 + t * tstride + bl), m = load_vis(M0 + t * tstride + bl);
+            const J2 r = d - (gp * m) * gqh;
+            const J2 ri = d - m;
+            acc_p += cnorm(r.a) + cnorm(r.b) + cnorm(r.c) + cnorm(r.d);
+            acc_i += cnorm(ri.a) + cnorm(ri.b) + cnorm(ri.c) + cnorm(ri.d);
+        }
+    }
+    __shared__ double red[2][CT / 32];
+    __shared__ int keep;
+    for (int o = 16; o > 0; o >>= 1) {
+        acc_p += __shfl_xor_sync(0xffffffffu, acc_p, o);
+        acc_i += __shfl_xor_sync(0xffffffffu, acc_i, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        red[0][threadIdx.x >> 5] = acc_p;
+        red[1][threadIdx.x >> 5] = acc_i;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double sp = 0.0, si = 0.0;
+        for (int w = 0; w < CT / 32; w++) {
+            sp += red[0][w];
+            si += red[1][w];
+        }
+        keep = isfinite(sp) && sp <= si;
+        if (use) use[ch] = keep;
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < P.ntiles; t += CT) {
+        const size_t i = (size_t)t * P.nchan + ch;
+        dstart[i] = keep ? dprop[i] : JonesF64{1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 1.0, 0.0};
+    }
+}
+
+int launch_judge(const JonesF32* d_data, const JonesF32* d_model, int t0, int t1, int nchan, int nbl, int ntiles,
+                 const JonesF64* d_prop, JonesF64* d_start, int* d_use, cudaStream_t s) {
+    CalParams P = {};
+    P.data = d_data;
+    P.model = d_model;
+    P.t0 = t0;
+    P.t1 = t1;
+    P.nchan = nchan;
+    P.nbl = nbl;
+    P.ntiles = ntiles;
+    judge_kernel<<<nchan, CT, 0, s>>>(P, d_prop, d_start, d_use);
+    count_launches(1);
+    HDC_CUDA_RET_INT(cudaGetLastError());
+    return HDC_OK;
+}
+
 static size_t smem_bytes(int n, int form) {
     const size_t base = (size_t)n * (3 * sizeof(J2) + 2 * sizeof(Herm) + 4 * sizeof(double)) +
                         sizeof(int) * (size_t)((n + 1) & ~1);

@@ -308,6 +308,17 @@ extern "C" int hdc_mlp_new(int num_layers, const int* dims, int residual_offset,
 
 extern "C" void hdc_mlp_free(HdcMlp* m) { delete reinterpret_cast<Net*>(m); }
 
+namespace hdc {
+// input and output widths of a network (for callers that build its inputs)
+int mlp_io_dims(HdcMlp* m, int* in, int* out) {
+    if (!m) return HDC_ERR_ARG;
+    const Net* n = reinterpret_cast<const Net*>(m);
+    *in = n->dims.front();
+    *out = n->dims.back();
+    return HDC_OK;
+}
+}  // namespace hdc
+
 extern "C" long long hdc_mlp_num_params(HdcMlp* m) { return (long long)reinterpret_cast<Net*>(m)->nparams; }
 
 extern "C" int hdc_mlp_get_params(HdcMlp* hm, float* h_out) {

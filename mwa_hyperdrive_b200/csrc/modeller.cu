@@ -216,6 +216,7 @@ void TypeTables::release() {
     dfree(d_cstart);
     dfree(d_ccount);
     dfree(d_suv_tile);
+    dfree(d_sdense);
     nc = 0;
 }
 
@@ -337,6 +338,22 @@ int Modeller::build_tables(const HdcSkyModel* sky) {
             HDC_CUDA_RET_INT(cudaMemcpy(tt.d_cstart, cstart.data(), sizeof(int) * nc, cudaMemcpyHostToDevice));
             HDC_CUDA_RET_INT(cudaMemcpy(tt.d_ccount, ccount.data(), sizeof(int) * nc, cudaMemcpyHostToDevice));
             HDC_CUDA_RET_INT(dalloc(&tt.d_suv_tile, (size_t)nc * ntiles));
+            // dense form: sum of value * sign(i^(n1+n2)) per (n1, n2); the
+            // real part takes even n1 + n2, the imaginary part odd
+            bool dense = true;
+            for (const ShapeletCoeff& sc : coeffs) dense = dense && sc.n1 < SDN && sc.n2 < SDN;
+            if (dense) {
+                std::vector<double> dm((size_t)nc * SDN * SDN, 0.0);
+                for (int k = 0; k < nc; k++)
+                    for (int q = 0; q < ccount[k]; q++) {
+                        const ShapeletCoeff& sc = coeffs[cstart[k] + q];
+                        const double sgn = ((sc.n1 + sc.n2) & 3) < 2 ? 1.0 : -1.0;
+                        dm[((size_t)k * SDN + sc.n1) * SDN + sc.n2] += sgn * sc.value;
+                    }
+                std::vector<float> df(dm.begin(), dm.end());
+                HDC_CUDA_RET_INT(dalloc(&tt.d_sdense, df.size()));
+                HDC_CUDA_RET_INT(cudaMemcpy(tt.d_sdense, df.data(), sizeof(float) * df.size(), cudaMemcpyHostToDevice));
+            }
         }
     }
     return HDC_OK;
@@ -383,6 +400,8 @@ DirectParams Modeller::direct_params(int ty, void* vis) const {
     p.gp = t[ty].d_gp;
     p.sbf = d_sbf;
     p.sbf32 = form == HDC_PREDICT_TENSOR ? device_shapelet_basis_f32() : nullptr;
+    p.sbfp = form == HDC_PREDICT_TENSOR ? device_shapelet_basis_pairs() : nullptr;
+    p.sdense = form == HDC_PREDICT_TENSOR ? t[ty].d_sdense : nullptr;
     p.coeffs = t[ty].d_coeffs;
     p.coeff_start = t[ty].d_cstart;
     p.coeff_count = t[ty].d_ccount;

@@ -18,6 +18,7 @@ struct TypeTables {
     int* d_cstart = nullptr;
     int* d_ccount = nullptr;
     double2* d_suv_tile = nullptr;  // [nc][ntiles]
+    float* d_sdense = nullptr;      // [nc][SDN][SDN] signed dense coefficients, or NULL
     void release();
 };
 

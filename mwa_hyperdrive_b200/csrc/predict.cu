@@ -90,6 +90,47 @@ __device__ __forceinline__ void shapelet_envelope_f32(const DirectParams& p, int
     ei = im;
 }
 
+// The chosen form's dense shapelet envelope (every order below SDN): the
+// basis is interpolated once per order along each axis (one 8-byte gather of
+// a (value, next - value) pair each), then contracted with the component's
+// signed dense coefficient matrix C (shared memory):
+//     env = sum_{n1,n2} C[n1][n2] X[n1] Y[n2],  even n1 + n2 -> re, odd -> im.
+__device__ __forceinline__ void shapelet_envelope_dense(const DirectParams& p, const float* __restrict__ cm,
+                                                        double4 g, double su, double sv, float& er, float& ei) {
+    const double x = su * g.z + sv * g.w;
+    const double y = su * g.w - sv * g.z;
+    const double x_pos = x * g.x + SBF_C;
+    const double y_pos = y * g.y + SBF_C;
+    const double fx = floor(x_pos), fy = floor(y_pos);
+    const int xi = fx > 0.0 ? (int)fmin(fx, (double)(SBF_L - 2)) : 0;
+    const int yi = fy > 0.0 ? (int)fmin(fy, (double)(SBF_L - 2)) : 0;
+    const float xfrac = (float)(x_pos - fx), yfrac = (float)(y_pos - fy);
+    float X[SDN], Y[SDN];
+#pragma unroll
+    for (int n = 0; n < SDN; n++) {
+        const float2 a = __ldg(p.sbfp + (size_t)SBF_L * n + xi);
+        const float2 b = __ldg(p.sbfp + (size_t)SBF_L * n + yi);
+        X[n] = fmaf(a.y, xfrac, a.x);
+        Y[n] = fmaf(b.y, yfrac, b.x);
+    }
+    float re = 0.f, im = 0.f;
+#pragma unroll
+    for (int n1 = 0; n1 < SDN; n1++) {
+        float tr = 0.f, ti = 0.f;
+#pragma unroll
+        for (int n2 = 0; n2 < SDN; n2++) {
+            if ((n1 + n2) & 1)
+                ti = fmaf(cm[n1 * SDN + n2], Y[n2], ti);
+            else
+                tr = fmaf(cm[n1 * SDN + n2], Y[n2], tr);
+        }
+        re = fmaf(X[n1], tr, re);
+        im = fmaf(X[n1], ti, im);
+    }
+    er = re;
+    ei = im;
+}
+
 // FAST (the chosen form's Gaussians and shapelets, shared beam only): the
 // phasor from the FP32 quarter-turn polynomials after exact FP64 range
 // reduction, envelopes in FP32 (arguments and table positions in FP64),
@@ -102,6 +143,7 @@ __global__ void __launch_bounds__(DT) direct_kernel(const DirectParams p) {
     __shared__ alignas(128) JonesF64 s_flux[2][CH];
     __shared__ alignas(128) double4 s_gp[2][CH];
     __shared__ alignas(16) float s_wf[FAST ? CH * 8 : 1];
+    __shared__ alignas(16) float s_dense[(FAST && TYPE == 2) ? CH * SDN * SDN : 1];
     __shared__ alignas(8) uint64_t bar[2];
 
     const int f = blockIdx.y;
@@ -169,6 +211,9 @@ __global__ void __launch_bounds__(DT) direct_kernel(const DirectParams p) {
         if (FAST) {
             const double* src = reinterpret_cast<const double*>(s_flux[st]);
             for (int i = threadIdx.x; i < n * 8; i += DT) s_wf[i] = (float)src[i];
+            if (TYPE == 2 && p.sdense)
+                for (int i = threadIdx.x; i < n * SDN * SDN; i += DT)
+                    s_dense[i] = __ldg(p.sdense + (size_t)c0 * SDN * SDN + i);
             __syncthreads();
         }
         if (FAST && active) {
@@ -192,7 +237,11 @@ __global__ void __launch_bounds__(DT) direct_kernel(const DirectParams p) {
                     const double4 g = s_gp[st][c];
                     const double2 ta = __ldg(p.suv_tile + (size_t)(c0 + c) * p.ntiles + t1);
                     const double2 tb = __ldg(p.suv_tile + (size_t)(c0 + c) * p.ntiles + t2);
-                    shapelet_envelope_f32(p, c0 + c, g, (ta.x - tb.x) * ool, (ta.y - tb.y) * ool, er, ei);
+                    if (p.sdense)
+                        shapelet_envelope_dense(p, s_dense + c * SDN * SDN, g, (ta.x - tb.x) * ool,
+                                                (ta.y - tb.y) * ool, er, ei);
+                    else
+                        shapelet_envelope_f32(p, c0 + c, g, (ta.x - tb.x) * ool, (ta.y - tb.y) * ool, er, ei);
                 }
                 // ph * env
                 const float zr = cs * er - sn * ei, zi = fmaf(cs, ei, sn * er);
@@ -300,6 +349,7 @@ cudaError_t launch_direct(int ty, bool tile_beam, bool out64, const DirectParams
     if (p.nc <= 0 || p.nbl <= 0 || p.nf <= 0) return cudaSuccess;
     // the FP32 form needs per-tile shapelet UVs and the FP32 basis table
     fast = fast && !tile_beam && (ty != 2 || (p.suv_tile && !p.suv_bl && p.sbf32));
+    if (fast && ty == 2 && p.sdense && !p.sbfp) return cudaErrorInvalidValue;
     if (ty == 0) return launch_t<0>(tile_beam, out64, fast, p, s);
     if (ty == 1) return launch_t<1>(tile_beam, out64, fast, p, s);
     return launch_t<2>(tile_beam, out64, fast, p, s);

@@ -10,6 +10,8 @@ namespace hdc {
 // is the modelling order; for the drop-in layer it is power laws, curved
 // power laws, lists (gpu/types.h:187-267), which is also the beam-direction
 // order of d_beam_jones.
+constexpr int SDN = 6;  // orders 0..5 in the dense shapelet form
+
 struct DirectParams {
     int nbl, nf, ntiles, nc;
     const double* freqs;  // [nf] Hz
@@ -26,6 +28,12 @@ struct DirectParams {
     // shapelets
     const double* sbf;  // [SBF_N][SBF_L]
     const float* sbf32; // the same table in FP32 (chosen form), or NULL
+    // chosen form, orders below SDN: the table as FP32 (value, next - value)
+    // pairs [SBF_N][SBF_L] and per component a dense SDN x SDN coefficient
+    // matrix [nc][n1][n2] with the sign of i^(n1+n2) folded in; NULL when
+    // some coefficient's order is SDN or more
+    const float2* sbfp;
+    const float* sdense;
     const ShapeletCoeff* coeffs;
     const int* coeff_start;
     const int* coeff_count;

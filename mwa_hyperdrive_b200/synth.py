@@ -205,6 +205,40 @@ def polarised_model(nt, nch, nbl, rng, cross=0.3):
     return m.astype(np.float32)
 
 
+def polarised_model_device(nt, nch, nbl, gen, cross=0.3):
+    """polarised_model on the CUDA device (torch, generator ``gen``): the
+    same distribution, a different random stream; float32 [t][ch][bl][8]."""
+    import torch
+
+    amp = torch.empty((nt, nch, nbl), dtype=torch.float64, device="cuda").log_normal_(0.0, 0.5, generator=gen)
+    m = torch.empty((nt, nch, nbl, 8), dtype=torch.float32, device="cuda")
+    for k in range(4):
+        a = amp * (1.0 if k in (0, 3) else cross) * torch.empty_like(amp).log_normal_(0.0, 0.2, generator=gen)
+        ph = torch.empty_like(amp).uniform_(-np.pi, np.pi, generator=gen)
+        m[..., 2 * k] = (a * torch.cos(ph)).float()
+        m[..., 2 * k + 1] = (a * torch.sin(ph)).float()
+    return m
+
+
+def corrupt_device(model_tfb, gains_tc):
+    """corrupt() on the device without noise: data = G_p M G_q^H, float32."""
+    import torch
+
+    nt, nch, nbl = (int(x) for x in model_tfb.shape[:3])
+    ntiles = gains_tc.shape[0]
+    i, j = np.triu_indices(ntiles, 1)
+    g = torch.from_numpy(np.ascontiguousarray(gains_tc, np.float64)).cuda()
+    g = torch.view_as_complex(g.reshape(ntiles, nch, 4, 2)).reshape(ntiles, nch, 2, 2)
+    gp = g[torch.from_numpy(i).cuda()].permute(1, 0, 2, 3)  # [ch][bl][2][2]
+    gqh = g[torch.from_numpy(j).cuda()].permute(1, 0, 2, 3).conj().transpose(-1, -2)
+    out = torch.empty_like(model_tfb)
+    for t in range(nt):
+        m = torch.view_as_complex(model_tfb[t].double().reshape(nch, nbl, 4, 2)).reshape(nch, nbl, 2, 2)
+        d = gp @ m @ gqh
+        out[t] = torch.view_as_real(d.reshape(nch, nbl, 4)).reshape(nch, nbl, 8).float()
+    return out
+
+
 def random_model(nt, nch, nbl, rng):
     """A random, Stokes-I dominated model [t][chanblock][bl][8]."""
     m = np.zeros((nt, nch, nbl, 8))

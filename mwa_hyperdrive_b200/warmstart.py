@@ -51,7 +51,8 @@ def gauge_align(sol_tc: np.ndarray, ref_tile: int = 0) -> np.ndarray:
     tile's XX gain is real and positive (NaN chanblocks stay NaN)."""
     s = np.array(sol_tc, np.float64, copy=True)
     xx = s[ref_tile, :, 0] + 1j * s[ref_tile, :, 1]
-    ph = np.where(np.abs(xx) > 0, np.conj(xx) / np.maximum(np.abs(xx), 1e-300), 1.0 + 0j)
+    with np.errstate(invalid="ignore"):  # NaN chanblocks stay NaN
+        ph = np.where(np.abs(xx) > 0, np.conj(xx) / np.maximum(np.abs(xx), 1e-300), 1.0 + 0j)
     c = s[..., 0::2] + 1j * s[..., 1::2]
     c = c * ph[None, :, None]
     s[..., 0::2] = c.real
@@ -161,16 +162,21 @@ class WarmStartMLP:
                    "hdc_mlp_gradients")
         return loss.value, g
 
-    def train(self, X: np.ndarray, Y: np.ndarray, epochs: int = 20, batch: int = 4096, lr: float = 1e-3,
+    def train(self, X, Y, epochs: int = 20, batch: int = 4096, lr: float = 1e-3,
               seed: int = 0, schedule: str = "cosine") -> List[float]:
-        """Mini-batch Adam on the device (inputs moved to HBM once).  The
+        """Mini-batch Adam on the device (X [n][40], Y [n][8]: numpy arrays,
+        moved to HBM once, or CUDA tensors).  The
         learning rate follows a cosine from lr down to lr/100 over the run
         ("cosine") or stays at lr ("constant"); the decay makes the final fit
         insensitive to the seed and to rounding differences between runs."""
         import torch
 
-        d_x = torch.from_numpy(np.ascontiguousarray(X, np.float32)).cuda()
-        d_y = torch.from_numpy(np.ascontiguousarray(Y, np.float32)).cuda()
+        def dev(a):
+            if isinstance(a, torch.Tensor):
+                return a.to(device="cuda", dtype=torch.float32).contiguous()
+            return torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda()
+
+        d_x, d_y = dev(X), dev(Y)
         n = X.shape[0]
         rng = np.random.default_rng(seed)
         lib = _lib.lib()
@@ -195,8 +201,33 @@ class WarmStartMLP:
             self.losses.append(tot / max(cnt, 1))
         return self.losses
 
+    def propose_device(self, d_prev, d_data=None, d_model=None, timeblock=None, stream=None):
+        """The device chain (hdc_warmstart_propose): previous solutions on the
+        device ([tile][chanblock][8] float64) -> proposed starting gains on the
+        device; with the timeblock's data and model also the judge.  Returns
+        (d_start, d_use): d_use [chanblock] int32 (1 = proposal kept), None
+        without a judge.  Nothing is synchronised with the host."""
+        import torch
+
+        d_prev = d_prev.contiguous()
+        nt, nc = int(d_prev.shape[0]), int(d_prev.shape[1])
+        d_start = torch.empty((nt, nc, 8), dtype=torch.float64, device=d_prev.device)
+        if d_data is None:
+            _lib.check(_lib.lib().hdc_warmstart_propose(self._h, d_prev.data_ptr(), nt, nc, None, None, 0, 0, 0,
+                                                        d_start.data_ptr(), None, _stream_ptr(stream)),
+                       "hdc_warmstart_propose")
+            return d_start, None
+        d_use = torch.empty(nc, dtype=torch.int32, device=d_prev.device)
+        _lib.check(_lib.lib().hdc_warmstart_propose(self._h, d_prev.data_ptr(), nt, nc, d_data.data_ptr(),
+                                                    d_model.data_ptr(), int(d_data.shape[0]), int(timeblock[0]),
+                                                    int(timeblock[1]), d_start.data_ptr(), d_use.data_ptr(),
+                                                    _stream_ptr(stream)), "hdc_warmstart_propose")
+        return d_start, d_use
+
     def propose(self, prev_tc: np.ndarray) -> np.ndarray:
-        """Proposed gains [tile][chanblock][8] (gauge of the aligned input)."""
+        """Host restatement of the proposal (numpy features and frames around
+        the device network): gains [tile][chanblock][8] in the gauge of the
+        aligned input."""
         import torch
 
         nt, nc = prev_tc.shape[:2]
@@ -233,6 +264,19 @@ class WarmStartMLP:
         return m
 
 
+def features_device(d_prev, stream=None):
+    """features() on the device (hdc_warmstart_features): [tile][chanblock][8]
+    float64 CUDA tensor -> [tile*chanblock][40] float32 CUDA tensor."""
+    import torch
+
+    d_prev = d_prev.contiguous()
+    nt, nc = int(d_prev.shape[0]), int(d_prev.shape[1])
+    x = torch.empty((nt * nc, IN_DIM), dtype=torch.float32, device=d_prev.device)
+    _lib.check(_lib.lib().hdc_warmstart_features(d_prev.data_ptr(), nt, nc, x.data_ptr(), _stream_ptr(stream)),
+               "hdc_warmstart_features")
+    return x
+
+
 def identity_gains(ntiles: int, nch: int) -> np.ndarray:
     g = np.zeros((ntiles, nch, 8))
     g[..., 0] = 1.0
@@ -242,47 +286,47 @@ def identity_gains(ntiles: int, nch: int) -> np.ndarray:
 
 def judge(d_data, d_model, timeblock, proposal_tc: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
     """Per chanblock, keep the proposal where its calibration residual is no
-    worse than the identity start's; returns (start gains, chose_proposal)."""
+    worse than the identity start's (hdc_warmstart_judge, on the device);
+    non-finite proposal entries are first replaced by the identity's.
+    Returns (start gains, chose_proposal) on the host."""
     import torch
 
     nt, nch, nbl = (int(x) for x in d_data.shape[:3])
     ntiles = proposal_tc.shape[0]
-    lib = _lib.lib()
-
-    def residual(g):
-        dg = torch.from_numpy(np.ascontiguousarray(g, np.float64)).cuda()
-        out = np.zeros(nch)
-        _lib.check(lib.hdc_calibration_residuals(d_data.data_ptr(), d_model.data_ptr(), nt, int(timeblock[0]),
-                                                 int(timeblock[1]), nch, nbl, dg.data_ptr(), out.ctypes.data,
-                                                 _stream_ptr(None)), "hdc_calibration_residuals")
-        return out
-
     ident = identity_gains(ntiles, nch)
-    prop = np.where(np.isfinite(proposal_tc), proposal_tc, ident)
-    r_prop = residual(prop)
-    r_id = residual(ident)
-    use = np.isfinite(r_prop) & (r_prop <= r_id)
-    start = np.where(use[None, :, None], prop, ident)
-    return start, use
+    prop = torch.from_numpy(np.ascontiguousarray(np.where(np.isfinite(proposal_tc), proposal_tc, ident),
+                                                 np.float64)).cuda()
+    start = torch.empty_like(prop)
+    use = torch.empty(nch, dtype=torch.int32, device=prop.device)
+    _lib.check(_lib.lib().hdc_warmstart_judge(d_data.data_ptr(), d_model.data_ptr(), nt, int(timeblock[0]),
+                                              int(timeblock[1]), nch, ntiles, prop.data_ptr(), start.data_ptr(),
+                                              use.data_ptr(), _stream_ptr(None)), "hdc_warmstart_judge")
+    return start.cpu().numpy(), use.cpu().numpy().astype(bool)
 
 
-def calibrate_warm(d_data, d_model, timeblock, prev_tc: Optional[np.ndarray], mlp: Optional[WarmStartMLP],
-                   max_iterations=50, stop_threshold=1e-8, min_threshold=1e-4):
-    """Calibrate one timeblock from the MLP's judged proposal (identity where
-    there is no previous solution or no network)."""
+def calibrate_warm(d_data, d_model, timeblock, d_prev, mlp: Optional[WarmStartMLP], max_iterations=50,
+                   stop_threshold=1e-8, min_threshold=1e-4):
+    """Calibrate one timeblock on the device from the MLP's judged proposal,
+    or from identity where there is no previous solution or no network.
+    d_prev: the previous timeblock's solutions on the device ([tile]
+    [chanblock][8] float64 tensor) or None.  Returns (d_solutions, results,
+    d_use, seconds): the solutions stay on the device for the next
+    timeblock; seconds is the wall time of proposal, judge and solve."""
     import torch
 
     nt, nch, nbl = (int(x) for x in d_data.shape[:3])
     ntiles = cal.num_tiles_from_baselines(nbl)
     t0 = time.perf_counter()
-    if prev_tc is None or mlp is None:
-        start, use = identity_gains(ntiles, nch), np.zeros(nch, bool)
+    d_use = None
+    if d_prev is None or mlp is None:
+        dj = torch.zeros((ntiles, nch, 8), dtype=torch.float64, device=d_data.device)
+        dj[..., 0] = 1.0
+        dj[..., 6] = 1.0
     else:
-        start, use = judge(d_data, d_model, timeblock, mlp.propose(prev_tc))
-    dj = torch.from_numpy(np.ascontiguousarray(start, np.float64)).cuda()
+        dj, d_use = mlp.propose_device(d_prev, d_data, d_model, timeblock)
     res = cal.calibrate_timeblock(d_data, d_model, dj, timeblock, max_iterations, stop_threshold, min_threshold)
     torch.cuda.synchronize()
-    return dj.cpu().numpy(), res, use, time.perf_counter() - t0
+    return dj, res, d_use, time.perf_counter() - t0
 
 
 @dataclass
@@ -304,10 +348,21 @@ class DriftSky:
     cross_pol: float = 0.3
     amp_jitter: float = 0.0005
 
-    def generate(self):
+    def generate(self, device: bool = False):
+        """[(data, model, gains)] per timeblock: numpy arrays, or with
+        ``device`` data and model as CUDA tensors drawn on the device (same
+        distributions, another random stream; no noise) and gains in numpy."""
         from . import synth
 
         rng = np.random.default_rng(self.seed)
+        gen = None
+        if device:
+            import torch
+
+            gen = torch.Generator(device="cuda")
+            gen.manual_seed(self.seed)
+            if self.snr is not None:
+                raise ValueError("device generation has no noise")
         nbl = self.ntiles * (self.ntiles - 1) // 2
         f = np.arange(self.nch) * self.chan_mhz
         phi0 = rng.uniform(-np.pi, np.pi, (self.ntiles, 2))
@@ -326,7 +381,11 @@ class DriftSky:
             g[..., 6] = amp[..., 1] * np.cos(ph[..., 1])
             g[..., 7] = amp[..., 1] * np.sin(ph[..., 1])
             g[..., 2:6] = leak
-            model = synth.polarised_model(self.nt_per_block, self.nch, nbl, rng, self.cross_pol)
-            data = synth.corrupt(model, g, rng, self.snr)
+            if device:
+                model = synth.polarised_model_device(self.nt_per_block, self.nch, nbl, gen, self.cross_pol)
+                data = synth.corrupt_device(model, g)
+            else:
+                model = synth.polarised_model(self.nt_per_block, self.nch, nbl, rng, self.cross_pol)
+                data = synth.corrupt(model, g, rng, self.snr)
             blocks.append((data, model, g))
         return blocks

@@ -112,6 +112,32 @@ def test_chosen_form_gaussians_and_shapelets_fp32(oracle):
     assert nrm < TOL and p999 < TOL, (nrm, p999, mx)
 
 
+@pytest.mark.parametrize("max_order", [5, 9])
+def test_chosen_form_shapelets_dense_and_per_coefficient(oracle, max_order):
+    """Shapelets alone: orders up to 5 take the dense form (basis interpolated
+    once per order, dense coefficient matrix); any order of 6 or more sends
+    the launch through the per-coefficient FP32 loop.  Both within 1e-6."""
+    obs, _ = synth.config2(n_points=1, n_gauss=1, n_shapelets=1, n_freqs=4, n_times=1)
+    rng = np.random.default_rng(17 + max_order)
+    pos = synth.cap_positions(24, obs.phase_centre, math.radians(8.0), rng)
+    comps = []
+    for k in range(24):
+        maj = math.radians(rng.uniform(0.5, 5.0) / 60.0)
+        coeffs = [sl.ShapeletCoeff(int(rng.integers(0, max_order + 1)), int(rng.integers(0, max_order + 1)),
+                                   float(rng.normal() * 0.1)) for _ in range(20)]
+        coeffs.append(sl.ShapeletCoeff(0, 0, 1.0))
+        comps.append(sl.SourceComponent(float(pos[k, 0]), float(pos[k, 1]),
+                                        sl.Shapelet(maj, maj * rng.uniform(0.3, 1.0), rng.uniform(0, math.pi), coeffs),
+                                        sl.PowerLaw(-0.8, sl.FluxDensity(150e6, float(rng.lognormal()), 0.0, 0.0, 0.0))))
+    sky = sl.SkyModelArrays.from_components(comps)
+    got = run(sky, obs, obs.lsts[0], "tensor", beam="analytic")
+    ref, _ = oracle.model_timestep(sky, obs.tile_xyzs, obs.freqs, obs.phase_centre, obs.lsts[0], obs.latitude,
+                                   beam=oracle.beam_struct(1), out_f64=True)
+    nrm, p999, mx = errors(got, ref)
+    print(f"shapelets to order {max_order}: normwise {nrm:.2e}, p99.9 {p999:.2e}, max {mx:.2e}")
+    assert nrm < TOL and p999 < TOL, (nrm, p999, mx)
+
+
 @pytest.mark.parametrize("ntiles,npts", [(64, 4500), (24, 16500)])
 def test_many_components(oracle, ntiles, npts):
     """Errors must not grow with the component count; 16500 components need

@@ -70,9 +70,9 @@ def solve_sequence(blocks, mlp, tight):
         m = torch.from_numpy(model).cuda()
         sol, res, use, _ = ws.calibrate_warm(d, m, (0, data.shape[0]), prev, mlp, max_iterations=tight[0],
                                              stop_threshold=tight[1], min_threshold=1e-4)
-        sols.append(sol)
+        sols.append(sol.cpu().numpy())
         iters.append(np.array([r.num_iterations for r in res]))
-        chose.append(use)
+        chose.append(use.cpu().numpy().astype(bool) if use is not None else np.zeros(data.shape[1], bool))
         prev = sol
     return sols, iters, chose
 
@@ -134,3 +134,57 @@ def test_fallback_to_identity_when_proposal_is_worse():
     start, use = ws.judge(d, m, (0, data.shape[0]), prop)
     assert use[::2].all() and not use[1::2].any()
     np.testing.assert_array_equal(start[:, 1::2], ws.identity_gains(12, 8)[:, 1::2])
+
+
+def awkward_solutions(ntiles, nch, seed):
+    """Previous solutions with the cases the frames must handle: a NaN
+    chanblock, a failed tile, a reference tile with zero XX, tiny YY."""
+    rng = np.random.default_rng(seed)
+    p = rng.normal(size=(ntiles, nch, 8))
+    p[..., 0] += 2.0
+    p[..., 6] += 2.0
+    p[:, 3, :] = np.nan          # a failed chanblock
+    p[5, :, :] = np.nan          # a failed tile
+    p[0, 7, 0:2] = 0.0           # reference tile XX zero: no rotation
+    p[2, 9, 6:8] = 1e-9          # YY below the frame threshold
+    return p
+
+
+def test_device_features_match_host_restatement():
+    p = awkward_solutions(20, 17, 3)
+    x = ws.features_device(torch.from_numpy(p).cuda()).cpu().numpy()
+    ref = ws.features(p)
+    assert x.shape == ref.shape
+    np.testing.assert_allclose(x, ref, rtol=2e-6, atol=2e-6)
+
+
+def test_device_proposal_matches_host_restatement():
+    rng = np.random.default_rng(4)
+    mlp = ws.WarmStartMLP(hidden=64, num_hidden=3, seed=2)
+    q = mlp.get_params()
+    mlp.set_params(q + rng.normal(0, 0.02, q.size).astype(np.float32))
+    p = awkward_solutions(20, 17, 5)
+    d_start, d_use = mlp.propose_device(torch.from_numpy(p).cuda())
+    assert d_use is None
+    host = mlp.propose(p)
+    host = np.where(np.isfinite(host), host, ws.identity_gains(20, 17))
+    np.testing.assert_allclose(d_start.cpu().numpy(), host, rtol=1e-5, atol=1e-5)
+
+
+def test_device_chain_judges_like_the_host():
+    """propose_device with the timeblock's data runs the judge: its choice
+    and starting gains equal the host-driven judge of the same proposal."""
+    blocks = ws.DriftSky(16, 12, 2, 2, seed=8).generate()
+    mlp = ws.WarmStartMLP(hidden=32, num_hidden=2, seed=4)
+    (data0, model0, _), (data1, model1, _) = blocks
+    d0, m0 = torch.from_numpy(data0).cuda(), torch.from_numpy(model0).cuda()
+    sol, _, _, _ = ws.calibrate_warm(d0, m0, (0, data0.shape[0]), None, None, max_iterations=100)
+    sol_np = sol.cpu().numpy()
+    sol_np[:, 4, :] = np.nan  # one failed chanblock: its proposal is the identity
+    d1, m1 = torch.from_numpy(data1).cuda(), torch.from_numpy(model1).cuda()
+    d_start, d_use = mlp.propose_device(torch.from_numpy(sol_np).cuda(), d1, m1, (0, data1.shape[0]))
+    prop, _ = mlp.propose_device(torch.from_numpy(sol_np).cuda())
+    start, use = ws.judge(d1, m1, (0, data1.shape[0]), prop.cpu().numpy())
+    np.testing.assert_array_equal(d_use.cpu().numpy().astype(bool), use)
+    np.testing.assert_array_equal(d_start.cpu().numpy(), start)
+    assert use.sum() >= 8  # the previous solution is a far better start than identity on most chanblocks
