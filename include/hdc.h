@@ -379,6 +379,18 @@ int hdc_calibrate_timeblock(const JonesF32 *d_data_tfb, const JonesF32 *d_model_
                             JonesF64 *d_di_jones, int max_iterations, double stop_threshold, double min_threshold,
                             int pols, HdcCalResult *h_results, int form, hdcStream_t stream);
 
+/* All timeblocks (calibrate_timeblocks, di_calibrate/mod.rs:272-361): every
+ * timeblock k = [h_timeblock_bounds[2k], h_timeblock_bounds[2k+1]) starts
+ * from identity; the first pass of all timeblocks runs as one CUDA graph
+ * (identity start, collapse, persistent MitchCal kernel per timeblock), then
+ * failed chanblocks are retried per timeblock as in hdc_calibrate_timeblock.
+ * d_di_jones [timeblock][tile][chanblock] gets the solutions, h_results
+ * [timeblock][chanblock] the results. */
+int hdc_calibrate_timeblocks(const JonesF32 *d_data_tfb, const JonesF32 *d_model_tfb, int num_timesteps,
+                             const int *h_timeblock_bounds, int num_timeblocks, int num_chanblocks,
+                             int num_baselines, JonesF64 *d_di_jones, int max_iterations, double stop_threshold,
+                             double min_threshold, int pols, HdcCalResult *h_results, int form, hdcStream_t stream);
+
 /* Per-chanblock calibration residual sum_{t,bl} ||D - G_p M G_q^H||_F^2 for
  * the gains d_di_jones [tile][chanblock] over timesteps
  * [timeblock_start, timeblock_end); h_residuals [num_chanblocks].  Used to

@@ -60,8 +60,10 @@ def calibrate_timeblock(d_data, d_model, d_di_jones_tc, timeblock: Tuple[int, in
 
 def calibrate_timeblocks(vis_data_tfb, vis_model_tfb, timeblocks: Sequence[Tuple[int, int]],
                          max_iterations: int = 50, stop_threshold: float = 1e-8, min_threshold: float = 1e-4,
-                         pols: str = "XX_XY_YX_YY", form: str = "plain"):
-    """calibrate_timeblocks (di_calibrate/mod.rs:272-361).  Accepts host
+                         pols: str = "XX_XY_YX_YY", form: str = "plain", stream=None):
+    """calibrate_timeblocks (di_calibrate/mod.rs:272-361) through
+    hdc_calibrate_timeblocks: the first pass of every timeblock runs as one
+    CUDA graph, failed chanblocks are retried per timeblock.  Accepts host
     (numpy) or device (torch) visibilities; returns (di_jones
     [timeblock][tile][chanblock][8] numpy, results [timeblock][chanblock])."""
     import torch
@@ -69,15 +71,16 @@ def calibrate_timeblocks(vis_data_tfb, vis_model_tfb, timeblocks: Sequence[Tuple
     host = isinstance(vis_data_tfb, np.ndarray)
     d_data = torch.from_numpy(np.ascontiguousarray(vis_data_tfb, np.float32)).cuda() if host else vis_data_tfb
     d_model = torch.from_numpy(np.ascontiguousarray(vis_model_tfb, np.float32)).cuda() if host else vis_model_tfb
-    nt, nch, nbl = d_data.shape[:3]
-    ntiles = num_tiles_from_baselines(int(nbl))
-    out = np.zeros((len(timeblocks), ntiles, nch, 8))
-    results = []
-    for k, tb in enumerate(timeblocks):
-        dj = torch.zeros((ntiles, nch, 8), dtype=torch.float64, device=d_data.device)
-        dj[..., 0] = 1.0
-        dj[..., 6] = 1.0
-        results.append(calibrate_timeblock(d_data, d_model, dj, tb, max_iterations, stop_threshold, min_threshold,
-                                           pols, form))
-        out[k] = dj.cpu().numpy()
-    return out, results
+    nt, nch, nbl = (int(x) for x in d_data.shape[:3])
+    ntiles = num_tiles_from_baselines(nbl)
+    ntb = len(timeblocks)
+    dj = torch.empty((ntb, ntiles, nch, 8), dtype=torch.float64, device=d_data.device)
+    bounds = np.ascontiguousarray(np.array(timeblocks, dtype=np.int32).reshape(-1))
+    res = (_lib.HdcCalResult * (ntb * nch))()
+    rc = _lib.lib().hdc_calibrate_timeblocks(d_data.data_ptr(), d_model.data_ptr(), nt, bounds.ctypes.data, ntb, nch,
+                                             nbl, dj.data_ptr(), int(max_iterations), float(stop_threshold),
+                                             float(min_threshold), POLS[pols], res, FORMS[form], _stream_ptr(stream))
+    _lib.check(rc, "hdc_calibrate_timeblocks")
+    results = [[CalibrationResult(r.num_iterations, bool(r.converged), r.max_precision, r.num_failed, i)
+                for i, r in enumerate(res[k * nch:(k + 1) * nch])] for k in range(ntb)]
+    return dj.cpu().numpy(), results

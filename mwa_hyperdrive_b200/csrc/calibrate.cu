@@ -630,6 +630,60 @@ static int launch_mitchcal_form(const CalParams& P, int nblocks, cudaStream_t s)
     return HDC_OK;
 }
 
+// Launch without setting the shared-memory attribute (inside a stream
+// capture, after prepare_mitchcal has set it).
+static void launch_mitchcal_captured(const CalParams& P, int form, int nblocks, cudaStream_t s) {
+    const size_t sm = smem_bytes(P.ntiles, form);
+    if (form == HDC_CAL_COLLAPSED)
+        mitchcal_kernel<1><<<nblocks, CT, sm, s>>>(P);
+    else if (form == HDC_CAL_COLLAPSED_F32)
+        mitchcal_kernel<2><<<nblocks, CT, sm, s>>>(P);
+    else
+        mitchcal_kernel<0><<<nblocks, CT, sm, s>>>(P);
+    count_launches(1);
+}
+
+static int prepare_mitchcal(int ntiles, int form) {
+    const int sm = (int)smem_bytes(ntiles, form);
+    if (form == HDC_CAL_COLLAPSED)
+        HDC_CUDA_RET_INT(cudaFuncSetAttribute(mitchcal_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    else if (form == HDC_CAL_COLLAPSED_F32)
+        HDC_CUDA_RET_INT(cudaFuncSetAttribute(mitchcal_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    else
+        HDC_CUDA_RET_INT(cudaFuncSetAttribute(mitchcal_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    return HDC_OK;
+}
+
+__global__ void identity_kernel(JonesF64* dj, size_t n) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dj[i] = JonesF64{1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 1.0, 0.0};
+}
+
+static void launch_collapse(const CalParams& P, int form, void* cov, cudaStream_t s) {
+    const dim3 grid((P.nbl + 127) / 128, P.nchan);
+    if (form == HDC_CAL_COLLAPSED)
+        collapse_kernel<double><<<grid, 128, 0, s>>>(P, static_cast<double*>(cov));
+    else
+        collapse_kernel<float><<<grid, 128, 0, s>>>(P, static_cast<float*>(cov));
+    count_launches(1);
+}
+
+// A non-blocking stream per device on which the multi-timeblock graph is
+// captured (capture is not possible on the legacy default stream).
+static std::mutex g_cs_mu;
+static cudaStream_t g_cs[16] = {nullptr};
+
+static cudaStream_t capture_stream() {
+    std::lock_guard<std::mutex> lk(g_cs_mu);
+    int d = 0;
+    if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= 16) return nullptr;
+    if (!g_cs[d] && cudaStreamCreateWithFlags(&g_cs[d], cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return g_cs[d];
+}
+
 static int launch_mitchcal(const CalParams& P, int form, int nblocks, cudaStream_t s) {
     if (form == HDC_CAL_COLLAPSED) return launch_mitchcal_form<1>(P, nblocks, s);
     if (form == HDC_CAL_COLLAPSED_F32) return launch_mitchcal_form<2>(P, nblocks, s);
@@ -659,6 +713,63 @@ static void* covariance_buffer(size_t bytes) {
         g_cov_size[d] = bytes;
     }
     return g_cov[d];
+}
+
+// Retry failed chanblocks from interpolated neighbours (mod.rs:468-614):
+// res holds the first pass's results (read back); P.results/P.di_jones point
+// at this timeblock's device results and solutions; for the collapsed forms
+// P.cov must hold this timeblock's covariances.
+static int retry_failed(CalParams P, int form, std::vector<HdcCalResult>& res, int* d_list, int2* d_pairs,
+                        cudaStream_t s) {
+    int rc = HDC_OK;
+    int total = 0;
+    for (auto& r : res) total += r.converged;
+    if (total > 0 && total != P.nchan) {
+        int new_conv = 1;
+        while (new_conv > 0 && total != P.nchan) {
+            std::vector<int2> pairs;
+            int left = -1;
+            bool in_fail = false;
+            for (int c = 0; c < P.nchan; c++) {
+                const bool conv = res[c].converged != 0;
+                if (!in_fail && conv)
+                    left = c;
+                else if (!in_fail && !conv)
+                    in_fail = true;
+                else if (in_fail && conv) {
+                    in_fail = false;
+                    pairs.push_back(make_int2(left, c));
+                    left = c;
+                }
+            }
+            std::vector<int> list;
+            for (int c = 0; c < P.nchan; c++)
+                if (!res[c].converged) list.push_back(c);
+            if (!pairs.empty()) {
+                cudaMemcpyAsync(d_pairs, pairs.data(), sizeof(int2) * pairs.size(), cudaMemcpyHostToDevice, s);
+                retry_seed_kernel<<<(P.ntiles + 127) / 128, 128, 0, s>>>(P.di_jones, P.nchan, P.ntiles, d_pairs,
+                                                                        (int)pairs.size());
+                count_launches(1);
+            }
+            cudaMemcpyAsync(d_list, list.data(), sizeof(int) * list.size(), cudaMemcpyHostToDevice, s);
+            P.chan_list = d_list;
+            rc = launch_mitchcal(P, form, (int)list.size(), s);
+            if (rc) return rc;
+            if (cudaMemcpyAsync(res.data(), P.results, sizeof(HdcCalResult) * P.nchan, cudaMemcpyDeviceToHost,
+                                s) != cudaSuccess ||
+                cudaStreamSynchronize(s) != cudaSuccess) {
+                set_error("calibration retry: %s", cudaGetErrorString(cudaGetLastError()));
+                return HDC_ERR_CUDA;
+            }
+            for (int c : list)
+                if (std::fabs(res[c].max_precision) > 1e100) res[c].max_precision = NAN;
+            int tmp = 0;
+            for (auto& r : res) tmp += r.converged;
+            new_conv = tmp - total;
+            total = tmp;
+        }
+    }
+    return rc;
 }
 
 }  // namespace hdc
@@ -750,59 +861,139 @@ extern "C" int hdc_calibrate_timeblock(const JonesF32* d_data_tfb, const JonesF3
         set_error("hdc_calibrate_timeblock: %s", cudaGetErrorString(cudaGetLastError()));
         return HDC_ERR_CUDA;
     }
-    // Retry failed chanblocks from interpolated neighbours (mod.rs:468-614).
-    int total = 0;
-    for (auto& r : res) total += r.converged;
-    if (total > 0 && total != num_chanblocks) {
-        int new_conv = 1;
-        while (new_conv > 0 && total != num_chanblocks) {
-            std::vector<int2> pairs;
-            int left = -1;
-            bool in_fail = false;
-            for (int c = 0; c < num_chanblocks; c++) {
-                const bool conv = res[c].converged != 0;
-                if (!in_fail && conv)
-                    left = c;
-                else if (!in_fail && !conv)
-                    in_fail = true;
-                else if (in_fail && conv) {
-                    in_fail = false;
-                    pairs.push_back(make_int2(left, c));
-                    left = c;
-                }
-            }
-            std::vector<int> list;
-            for (int c = 0; c < num_chanblocks; c++)
-                if (!res[c].converged) list.push_back(c);
-            if (!pairs.empty()) {
-                cudaMemcpyAsync(d_pairs, pairs.data(), sizeof(int2) * pairs.size(), cudaMemcpyHostToDevice, s);
-                retry_seed_kernel<<<(ntiles + 127) / 128, 128, 0, s>>>(d_di_jones, num_chanblocks, ntiles, d_pairs,
-                                                                        (int)pairs.size());
-                count_launches(1);
-            }
-            cudaMemcpyAsync(d_list, list.data(), sizeof(int) * list.size(), cudaMemcpyHostToDevice, s);
-            P.chan_list = d_list;
-            rc = launch_mitchcal(P, form, (int)list.size(), s);
+    rc = retry_failed(P, form, res, d_list, d_pairs, s);
+    if (rc) {
+        cleanup();
+        return rc;
+    }
+    for (int c = 0; c < num_chanblocks; c++) h_results[c] = res[c];
+    cleanup();
+    return HDC_OK;
+}
+
+// All timeblocks of an observation (calibrate_timeblocks, mod.rs:272-361):
+// the first pass of every timeblock (identity start, collapse for the
+// collapsed forms, the persistent MitchCal kernel over all chanblocks) is
+// captured once into a CUDA graph and launched as one unit; the host reads
+// every timeblock's results once, then runs the reference's retry of failed
+// chanblocks per timeblock where it applies (outside the graph: its shape
+// depends on which chanblocks failed).
+extern "C" int hdc_calibrate_timeblocks(const JonesF32* d_data_tfb, const JonesF32* d_model_tfb, int num_timesteps,
+                                        const int* h_timeblock_bounds, int num_timeblocks, int num_chanblocks,
+                                        int num_baselines, JonesF64* d_di_jones, int max_iterations,
+                                        double stop_threshold, double min_threshold, int pols,
+                                        HdcCalResult* h_results, int form, hdcStream_t stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    const int ntiles = (int)((1.0 + std::sqrt(1.0 + 8.0 * num_baselines)) / 2.0 + 0.5);
+    bool ok = ntiles * (ntiles - 1) / 2 == num_baselines && ntiles <= CT && num_chanblocks > 0 &&
+              num_timeblocks > 0 && h_timeblock_bounds && h_results && pols >= 0 && pols <= 4 &&
+              (form == HDC_CAL_PLAIN || form == HDC_CAL_COLLAPSED || form == HDC_CAL_COLLAPSED_F32);
+    for (int k = 0; ok && k < num_timeblocks; k++) {
+        const int a = h_timeblock_bounds[2 * k], b = h_timeblock_bounds[2 * k + 1];
+        ok = a >= 0 && b <= num_timesteps && a < b;
+    }
+    if (!ok) {
+        set_error("hdc_calibrate_timeblocks: invalid arguments");
+        return HDC_ERR_ARG;
+    }
+    const size_t nres = (size_t)num_timeblocks * num_chanblocks;
+    const size_t nsol = (size_t)ntiles * num_chanblocks;
+    HdcCalResult* d_res = nullptr;
+    int* d_list = nullptr;
+    int2* d_pairs = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    auto cleanup = [&]() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (d_res) cudaFree(d_res);
+        if (d_list) cudaFree(d_list);
+        if (d_pairs) cudaFree(d_pairs);
+    };
+    if (cudaMalloc(&d_res, sizeof(HdcCalResult) * nres) != cudaSuccess ||
+        cudaMalloc(&d_list, sizeof(int) * num_chanblocks) != cudaSuccess ||
+        cudaMalloc(&d_pairs, sizeof(int2) * (num_chanblocks + 1)) != cudaSuccess) {
+        cudaGetLastError();
+        cleanup();
+        set_error("hdc_calibrate_timeblocks: device allocation failed");
+        return HDC_ERR_ALLOC;
+    }
+    void* cov = nullptr;
+    if (form != HDC_CAL_PLAIN) {
+        const size_t elem = form == HDC_CAL_COLLAPSED ? sizeof(double) : sizeof(float);
+        cov = covariance_buffer(elem * NCOV * (size_t)num_chanblocks * num_baselines);
+        if (!cov) {
+            cleanup();
+            set_error("hdc_calibrate_timeblocks: covariance allocation failed");
+            return HDC_ERR_ALLOC;
+        }
+    }
+    int rc = prepare_mitchcal(ntiles, form);
+    cudaStream_t cs = capture_stream();
+    if (rc || !cs) {
+        cleanup();
+        if (!rc) set_error("hdc_calibrate_timeblocks: no capture stream");
+        return rc ? rc : HDC_ERR_CUDA;
+    }
+    auto params = [&](int k) {
+        CalParams P = {};
+        P.data = d_data_tfb;
+        P.model = d_model_tfb;
+        P.t0 = h_timeblock_bounds[2 * k];
+        P.t1 = h_timeblock_bounds[2 * k + 1];
+        P.nchan = num_chanblocks;
+        P.nbl = num_baselines;
+        P.ntiles = ntiles;
+        P.di_jones = d_di_jones + (size_t)k * nsol;
+        P.chan_list = nullptr;
+        P.max_iter = max_iterations;
+        P.stop = stop_threshold;
+        P.min_thr = min_threshold;
+        P.pols = pols;
+        P.results = d_res + (size_t)k * num_chanblocks;
+        P.cov = cov;
+        return P;
+    };
+    cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        for (int k = 0; k < num_timeblocks; k++) {
+            const CalParams P = params(k);
+            identity_kernel<<<(unsigned)((nsol + 255) / 256), 256, 0, cs>>>(P.di_jones, nsol);
+            count_launches(1);
+            if (form != HDC_CAL_PLAIN) launch_collapse(P, form, cov, cs);
+            launch_mitchcal_captured(P, form, num_chanblocks, cs);
+        }
+        const cudaError_t le = cudaGetLastError();
+        e = cudaStreamEndCapture(cs, &graph);
+        if (e == cudaSuccess) e = le;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+    if (e == cudaSuccess) e = cudaGraphLaunch(exec, s);
+    std::vector<HdcCalResult> res(nres);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(res.data(), d_res, sizeof(HdcCalResult) * nres, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        cleanup();
+        set_error("hdc_calibrate_timeblocks: %s", cudaGetErrorString(e));
+        return HDC_ERR_CUDA;
+    }
+    for (int k = 0; k < num_timeblocks; k++) {
+        std::vector<HdcCalResult> rk(res.begin() + (size_t)k * num_chanblocks,
+                                     res.begin() + (size_t)(k + 1) * num_chanblocks);
+        int conv = 0;
+        for (auto& r : rk) conv += r.converged;
+        if (conv > 0 && conv != num_chanblocks) {
+            const CalParams P = params(k);
+            if (form != HDC_CAL_PLAIN) launch_collapse(P, form, cov, s);  // this timeblock's covariances
+            rc = retry_failed(P, form, rk, d_list, d_pairs, s);
             if (rc) {
                 cleanup();
                 return rc;
             }
-            if (cudaMemcpyAsync(res.data(), d_res, sizeof(HdcCalResult) * num_chanblocks, cudaMemcpyDeviceToHost,
-                                s) != cudaSuccess ||
-                cudaStreamSynchronize(s) != cudaSuccess) {
-                cleanup();
-                set_error("hdc_calibrate_timeblock: %s", cudaGetErrorString(cudaGetLastError()));
-                return HDC_ERR_CUDA;
-            }
-            for (int c : list)
-                if (std::fabs(res[c].max_precision) > 1e100) res[c].max_precision = NAN;
-            int tmp = 0;
-            for (auto& r : res) tmp += r.converged;
-            new_conv = tmp - total;
-            total = tmp;
         }
+        for (int c = 0; c < num_chanblocks; c++) h_results[(size_t)k * num_chanblocks + c] = rk[c];
     }
-    for (int c = 0; c < num_chanblocks; c++) h_results[c] = res[c];
     cleanup();
     return HDC_OK;
 }
