@@ -222,8 +222,10 @@ def test_timeblocks_graph_equals_per_timeblock_calls(form):
     """calibrate_timeblocks runs every timeblock's first pass as one CUDA
     graph and the retry of failed chanblocks afterwards; its solutions and
     results equal those of one hdc_calibrate_timeblock call per timeblock,
-    bit for bit, including a chanblock that fails (zero data) and is
-    retried from its neighbours."""
+    including a chanblock that fails (zero data) and is retried from its
+    neighbours: bit for bit for the collapsed forms (deterministic block
+    reductions); to rounding for the plain form, whose shared-memory FP64
+    atomics add in a run-dependent order."""
     rng = np.random.default_rng(21)
     ntiles, nt, nch = 12, 6, 9
     nbl = ntiles * (ntiles - 1) // 2
@@ -237,7 +239,10 @@ def test_timeblocks_graph_equals_per_timeblock_calls(form):
     for k, tb in enumerate(tbs):
         dj = torch.from_numpy(identity(ntiles, nch)).cuda()
         res = cal.calibrate_timeblock(d, m, dj, tb, 40, 1e-8, 1e-4, form=form)
-        np.testing.assert_array_equal(out[k], dj.cpu().numpy())
+        if form == "plain":
+            np.testing.assert_allclose(out[k], dj.cpu().numpy(), rtol=1e-10, atol=1e-12)
+        else:
+            np.testing.assert_array_equal(out[k], dj.cpu().numpy())
         assert [r.num_iterations for r in results[k]] == [r.num_iterations for r in res]
         assert [r.converged for r in results[k]] == [r.converged for r in res]
         assert not res[3].converged and sum(r.converged for r in res) >= nch - 2
