@@ -211,7 +211,7 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const Params P) {
     __shared__ uint32_t tmem_base_s;
     __shared__ double red_s[THREADS / 32];
     __shared__ volatile int abort_s;
-    __shared__ __align__(16) CompStage comp_s[2];
+    __shared__ __align__(16) CompStage comp_s[3];
 
     unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     const int f = blockIdx.x;
@@ -308,18 +308,17 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const Params P) {
             comp_s[buf].n[tid] = b.x;
             comp_s[buf].w[tid] = make_float2((float)(wd.x * (double)sx), (float)(wd.y * (double)sx));
         };
-        if (tid < KC) {
-            double2 a, b, wd;
-            fetch(0, a, b, wd);
-            stash(0, a, b, wd);
-        }
-        producers_sync_or(false);
-        for (int k = 0; k < nchunks; k++) {
-            const int st = k % NSTAGE;
-            double2 na, nb, nw;  // next stage's component data, in flight during this stage
-            const bool pre = tid < KC && k + 1 < nchunks;
-            if (pre) fetch(k + 1, na, nb, nw);
-            const CompStage& cs_ = comp_s[k & 1];
+        // Software pipeline: iteration k writes the byte planes of stage k
+        // from registers and computes the values of stage k + 1 (phasors, X,
+        // Y: FP64, conversion and FMA work) in the same straight-line block,
+        // so the scheduler interleaves the two kinds of work instead of every
+        // producer warp hitting the same pipe at once.  Component data goes
+        // through a 3-deep ring: stage j in comp_s[j % 3], stashed two
+        // iterations ahead, overwritten only after the barrier that follows
+        // its last reader.  Stages past the end read zeros (their values are
+        // never written out).
+        auto compute = [&](int k, int (&xr)[2][4], int (&xi)[2][4], int (&yr)[4], int (&yi)[4], int (&yn)[4]) {
+            const CompStage& cs_ = comp_s[k % 3];
             double cl[4], cm[4], cn[4];
             float wr[4], wi[4];
 #pragma unroll
@@ -333,7 +332,6 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const Params P) {
                 cn[2 * h] = n2.x, cn[2 * h + 1] = n2.y;
                 wr[2 * h] = w2.x, wi[2 * h] = w2.y, wr[2 * h + 1] = w2.z, wi[2 * h + 1] = w2.w;
             }
-            int xr[2][4], xi[2][4], yr[4], yi[4], yn[4];
 #pragma unroll
             for (int j = 0; j < 4; j++)
 #pragma unroll
@@ -352,6 +350,9 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const Params P) {
                         yn[j] = __float_as_int(__fmaf_rn(-sn, SY, YOFF));
                     }
                 }
+        };
+        auto write_planes = [&](int st, const int (&xr)[2][4], const int (&xi)[2][4], const int (&yr)[4],
+                                const int (&yi)[4], const int (&yn)[4]) {
             unsigned char* sb = smem + st * STAGE_BYTES;
             uint32_t pl[4];
             // x planes: bytes 0-2 excess-128 lower digits, byte 3 the signed top digit
@@ -367,18 +368,35 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const Params P) {
                 }
             }
             // y planes: bytes 0-1 excess-128, byte 2 the top digit + 64
-            {
-                const uint32_t yo = chunk_off(r0, kq) + quad * 4;
+            const uint32_t yo = chunk_off(r0, kq) + quad * 4;
 #pragma unroll
-                for (int part = 0; part < 3; part++) {
-                    byte_planes4(part == 0 ? yr : (part == 1 ? yi : yn), pl);
-                    *reinterpret_cast<uint32_t*>(sb + y_tile(part, 2) + yo) = pl[0] ^ 0x80808080u;
-                    *reinterpret_cast<uint32_t*>(sb + y_tile(part, 1) + yo) = pl[1] ^ 0x80808080u;
-                    *reinterpret_cast<uint32_t*>(sb + y_tile(part, 0) + yo) = minus64(pl[2]);
-                }
+            for (int part = 0; part < 3; part++) {
+                byte_planes4(part == 0 ? yr : (part == 1 ? yi : yn), pl);
+                *reinterpret_cast<uint32_t*>(sb + y_tile(part, 2) + yo) = pl[0] ^ 0x80808080u;
+                *reinterpret_cast<uint32_t*>(sb + y_tile(part, 1) + yo) = pl[1] ^ 0x80808080u;
+                *reinterpret_cast<uint32_t*>(sb + y_tile(part, 0) + yo) = minus64(pl[2]);
             }
+        };
+        if (tid < KC) {
+            double2 a, b, wd;
+            fetch(0, a, b, wd);
+            stash(0, a, b, wd);
+            fetch(1, a, b, wd);
+            stash(1, a, b, wd);
+        }
+        producers_sync_or(false);
+        int xr[2][4], xi[2][4], yr[4], yi[4], yn[4];
+        compute(0, xr, xi, yr, yi, yn);
+        for (int k = 0; k < nchunks; k++) {
+            const int st = k % NSTAGE;
+            double2 na, nb, nw;  // stage k + 2's component data, in flight during this stage
+            const bool pre = tid < KC;
+            if (pre) fetch(k + 2, na, nb, nw);
+            int nxr[2][4], nxi[2][4], nyr[4], nyi[4], nyn[4];
+            write_planes(st, xr, xi, yr, yi, yn);
+            compute(k + 1, nxr, nxi, nyr, nyi, nyn);
             fence_proxy_async_smem();  // make the generic-proxy stores visible to the tensor core
-            if (pre) stash((k + 1) & 1, na, nb, nw);
+            if (pre) stash((k + 2) % 3, na, nb, nw);
             // before the barrier, thread 0 waits until the next iteration's
             // stage has been read by the tensor core; the barrier then both
             // publishes this stage (one arrive on its full barrier) and frees
@@ -392,6 +410,11 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const Params P) {
             if (stop) {
                 abort_s = 1;
                 break;
+            }
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                xr[0][j] = nxr[0][j], xr[1][j] = nxr[1][j], xi[0][j] = nxi[0][j], xi[1][j] = nxi[1][j];
+                yr[j] = nyr[j], yi[j] = nyi[j], yn[j] = nyn[j];
             }
         }
     } else {
