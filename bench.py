@@ -632,7 +632,8 @@ def gpu_arm(args, rank, world, local_rank):
         e2e_s = max_over_ranks((time.perf_counter() - t0) / e2e_steps, dist)
     bytes_vis = nt * nf * nbl * 32
 
-    # roofline of the dominant kernel class
+    # roofline of every kernel class of the chosen form; `roofline` is the
+    # dominant one (largest share of the step)
     names = ["points", "gaussians", "shapelets", "prep"]
     per_step_ms = [prof[k] / args.steps for k in range(4)]
     dom = int(np.argmax(per_step_ms[:3]))
@@ -640,29 +641,39 @@ def gpu_arm(args, rank, world, local_rank):
     nga = int(np.sum(sky.comp_type == 1))
     nsh = int(np.sum(sky.comp_type == 2))
     ncoef = int(np.sum(sky.coeff_count))
-    vis_per_launch = nbl * nf
     launches_per_step = nt
-    if dom == 0 and form == "tensor":
-        # useful complex-GEMM flops: 3 products (XX, XY, YY) of 8 x 128 x 128 x Nc per (t, f)
-        flops = 3 * 8 * obs.num_tiles * obs.num_tiles * npts * nf
-        peak = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["bf16_tflops"] if (
-            ROOT / "MEASURED_PEAKS.json").exists() else 1590.0
-        bound, unit = "tensor", "TFLOP/s"
-        achieved = flops / (per_step_ms[0] / launches_per_step * 1e-3) / 1e12
-    else:
-        fl_per = {0: 37.0, 1: 37.0 + 10.0, 2: 37.0 + 12.0 * ncoef / max(nsh, 1)}[dom]
-        ncomp = [npts, nga, nsh][dom]
-        flops = fl_per * vis_per_launch * ncomp
-        g = ctypes.c_double()
-        _lib.check(L.hdc_probe_fp64_gflops(ctypes.byref(g)), "fp64 probe")
-        peak = g.value / 1e3
-        bound, unit = "fp64", "TFLOP/s"
-        achieved = flops / (per_step_ms[dom] / launches_per_step * 1e-3) / 1e12
-    roofline = {"bound": bound, "kernel": f"{names[dom]} ({form if dom == 0 else 'direct'})",
-                "achieved": achieved, "peak": peak, "unit": unit, "frac": achieved / peak, "traffic": None,
-                "peak_source": "MEASURED_PEAKS.json bf16 burst" if bound == "tensor" else
-                "FP64 FMA probe kernel measured in this run",
-                "per_step_ms_by_class": dict(zip(names, per_step_ms))}
+    g64, g32 = ctypes.c_double(), ctypes.c_double()
+    _lib.check(L.hdc_probe_fp64_gflops(ctypes.byref(g64)), "fp64 probe")
+    _lib.check(L.hdc_probe_fp32_gflops(ctypes.byref(g32)), "fp32 probe")
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    by_class = {}
+    for k, ncomp in enumerate([npts, nga, nsh]):
+        if ncomp == 0 or per_step_ms[k] <= 0.0:
+            continue
+        t_launch = per_step_ms[k] / launches_per_step * 1e-3
+        if k == 0 and form == "tensor":
+            # useful complex-GEMM flops: 3 products (XX, XY, YY) of 8 x 128 x 128 x Nc per (t, f)
+            flops = 3 * 8 * obs.num_tiles * obs.num_tiles * npts * nf
+            entry = {"bound": "tensor", "kernel": "gram_i8_kernel (points, tcgen05 kind::i8)",
+                     "peak": peaks.get("bf16_tflops", 1590.0),
+                     "peak_source": "MEASURED_PEAKS.json bf16 burst" if peaks else "fallback 1590 TFLOP/s"}
+        else:
+            # algorithmic FLOPs per visibility-component: phase 5 + Jones x phasor 24 + accumulate 8;
+            # Gaussians +10 (envelope); shapelets +12 per coefficient
+            fl_per = {0: 37.0, 1: 47.0, 2: 37.0 + 12.0 * ncoef / max(nsh, 1)}[k]
+            flops = fl_per * nbl * nf * ncomp
+            fast = form == "tensor"
+            entry = {"bound": "fp32" if fast else "fp64",
+                     "kernel": f"direct_kernel ({names[k]}, {'FP32 form' if fast else 'FP64'})",
+                     "peak": (g32.value if fast else g64.value) / 1e3,
+                     "peak_source": f"{'FP32' if fast else 'FP64'} FMA probe kernel measured in this run"}
+        entry.update({"achieved": flops / t_launch / 1e12, "unit": "TFLOP/s", "traffic": None,
+                      "ms_per_step": per_step_ms[k]})
+        entry["frac"] = entry["achieved"] / entry["peak"]
+        by_class[names[k]] = entry
+    roofline = dict(by_class[names[dom]])
+    roofline["per_step_ms_by_class"] = dict(zip(names, per_step_ms))
+    roofline["by_class"] = by_class
 
     if rank == 0:
         line = {

@@ -352,6 +352,8 @@ int hdc_modeller_profile(HdcModeller *m, double *out_ms, int reset);
  * register-resident FMA-chain kernel over all SMs (the FP64 roofline
  * denominator; a measurement, not a datasheet value). */
 int hdc_probe_fp64_gflops(double *out_gflops);
+/* The same for FP32 FMAs (the chosen form's direct kernels are FP32-bound). */
+int hdc_probe_fp32_gflops(double *out_gflops);
 
 /* Per-chanblock calibration outcome (di_calibrate/mod.rs:620-632). */
 typedef struct HdcCalResult {

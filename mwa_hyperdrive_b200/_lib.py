@@ -146,6 +146,7 @@ SIGNATURES = {
     "hdc_modeller_set_profiling": (c_int, [c_void_p, c_int]),
     "hdc_modeller_profile": (c_int, [c_void_p, c_void_p, c_int]),
     "hdc_probe_fp64_gflops": (c_int, [ctypes.POINTER(c_double)]),
+    "hdc_probe_fp32_gflops": (c_int, [ctypes.POINTER(c_double)]),
 }
 
 # Symbols exported for tests/tools that include/hdc.h does not declare.
