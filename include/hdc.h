@@ -188,13 +188,38 @@ const char *model_points(const Points *comps, const Addresses *a, const UVW *d_u
 const char *model_points_noalloc(const Points *comps, const Addresses *a, const UVW *d_uvws,
                                  const JonesF64 *d_beam_jones, JonesF32 *d_vis_fb);
 
+/* model_points with FP64 output (d_vis_fb JonesF64 [freq][bl], accumulated):
+ * the 1e-10 parity mode.  No counterpart in the reference, whose output
+ * precision is fixed at compile time (gpu/types.h:13-21). */
+const char *model_points_f64out(const Points *comps, const Addresses *a, const UVW *d_uvws,
+                                const JonesF64 *d_beam_jones, JonesF64 *d_vis_fb);
+
+/* model_points on the tensor cores (tcgen05 integer digit planes; results
+ * within 1e-6 of the FP64 predict).  No counterpart in the reference.  Takes
+ * the per-tile XYZs (d_tile_xyzs [tile], metres, the tile order of the
+ * baselines), the LST and the phase centre instead of per-baseline UVWs: the
+ * predict factors per tile because uvw_pq = R (xyz_p - xyz_q).  The beam
+ * must be one for all tiles: d_beam_jones NULL, or the reference's layout
+ * [uniq_tile][uniq_freq][component] with every tile mapped to one row.  Up
+ * to 128 tiles. */
+const char *model_points_tc(const Points *comps, const Addresses *a, const XYZ *d_tile_xyzs, double lst_rad,
+                            RADec phase_centre, const JonesF64 *d_beam_jones, JonesF32 *d_vis_fb);
+
 /* Replaces gpu/model.h:40 model_gaussians. */
 const char *model_gaussians(const Gaussians *comps, const Addresses *a, const UVW *d_uvws,
                             const JonesF64 *d_beam_jones, JonesF32 *d_vis_fb);
 
+/* model_gaussians with FP64 output (see model_points_f64out). */
+const char *model_gaussians_f64out(const Gaussians *comps, const Addresses *a, const UVW *d_uvws,
+                                   const JonesF64 *d_beam_jones, JonesF64 *d_vis_fb);
+
 /* Replaces gpu/model.h:47 model_shapelets. */
 const char *model_shapelets(const Shapelets *comps, const Addresses *a, const UVW *d_uvws,
                             const JonesF64 *d_beam_jones, JonesF32 *d_vis_fb);
+
+/* model_shapelets with FP64 output (see model_points_f64out). */
+const char *model_shapelets_f64out(const Shapelets *comps, const Addresses *a, const UVW *d_uvws,
+                                   const JonesF64 *d_beam_jones, JonesF64 *d_vis_fb);
 
 /* Replaces gpu/model.h:53 model_autos.  vis_fb is [freq][tile]. */
 const char *model_autos(int num_tiles, int num_freqs, const double *freqs, const Points *points,

@@ -92,8 +92,16 @@ SIGNATURES = {
     "model_points": (c_char_p, [ctypes.POINTER(Points), ctypes.POINTER(Addresses), c_void_p, c_void_p, c_void_p]),
     "model_points_noalloc": (c_char_p, [ctypes.POINTER(Points), ctypes.POINTER(Addresses), c_void_p, c_void_p,
                                         c_void_p]),
+    "model_points_f64out": (c_char_p, [ctypes.POINTER(Points), ctypes.POINTER(Addresses), c_void_p, c_void_p,
+                                       c_void_p]),
+    "model_points_tc": (c_char_p, [ctypes.POINTER(Points), ctypes.POINTER(Addresses), c_void_p, c_double, RADec,
+                                   c_void_p, c_void_p]),
     "model_gaussians": (c_char_p, [ctypes.POINTER(Gaussians), ctypes.POINTER(Addresses), c_void_p, c_void_p,
                                    c_void_p]),
+    "model_gaussians_f64out": (c_char_p, [ctypes.POINTER(Gaussians), ctypes.POINTER(Addresses), c_void_p, c_void_p,
+                                          c_void_p]),
+    "model_shapelets_f64out": (c_char_p, [ctypes.POINTER(Shapelets), ctypes.POINTER(Addresses), c_void_p, c_void_p,
+                                          c_void_p]),
     "model_shapelets": (c_char_p, [ctypes.POINTER(Shapelets), ctypes.POINTER(Addresses), c_void_p, c_void_p,
                                    c_void_p]),
     "model_autos": (c_char_p, [c_int, c_int, c_void_p, ctypes.POINTER(Points), ctypes.POINTER(Gaussians),

@@ -54,8 +54,27 @@ struct CalParams {
     double stop, min_thr;
     int pols;
     HdcCalResult* results;  // [nchan]
-    const void* cov;        // collapsed form: [nchan][48][nbl] (X re/im 32, C 16), FP64 or FP32
+    const void* cov;        // collapsed form: [nchan][nblk][48][256] block-major, FP64 or FP32
+    int nblk;               // 16 x 16 tile-pair blocks per chanblock
+    int nring;              // FP32 collapsed form: shared-memory ring depth (0: direct loads)
+    int* err;               // device error word (bounded waits)
 };
+
+// Collapsed covariances are stored block-major: the pairs (p, q) of tile
+// blocks pb <= qb (16 tiles each), enumerated column-major (qb outer, pb
+// inner), each block [48 components][256 lanes] with lane = 16 (p % 16) +
+// q % 16 and zeros where p >= q or q >= n -- so one block is one contiguous
+// run of 48 x 256 values that a single bulk copy brings into shared memory.
+constexpr int BLK = 256;
+__host__ __device__ __forceinline__ int cov_blocks(int n) {
+    const int nb = (n + 15) / 16;
+    return nb * (nb + 1) / 2;
+}
+__device__ __forceinline__ void cov_block_coords(int b, int& pb, int& qb) {
+    qb = 0;
+    while ((qb + 1) * (qb + 2) / 2 <= b) qb++;
+    pb = b - qb * (qb + 1) / 2;
+}
 
 // Covariance components per baseline: X[u][v] re at u*4+v, im at 16+u*4+v;
 // C Hermitian: diagonal reals at 32+u, off-diagonal (u<v) re/im at
@@ -122,10 +141,18 @@ __device__ __forceinline__ double cnorm(cplx a) { return a.re * a.re + a.im * a.
 // baseline, chanblock on blockIdx.y); stored structure-of-arrays so that a
 // warp's loads of one component are contiguous.
 template <typename T>
-__global__ void collapse_kernel(const CalParams P, T* cov) {
-    const int bl = blockIdx.x * blockDim.x + threadIdx.x;
-    const int ch = blockIdx.y;
-    if (bl >= P.nbl) return;
+__global__ void __launch_bounds__(BLK / 2) collapse_kernel(const CalParams P, T* cov) {
+    const int b = blockIdx.x >> 1, ch = blockIdx.y, lane = (blockIdx.x & 1) * (BLK / 2) + threadIdx.x;
+    int pb, qb;
+    cov_block_coords(b, pb, qb);
+    const int p = pb * 16 + (lane >> 4), q = qb * 16 + (lane & 15);
+    T* out = cov + ((size_t)ch * P.nblk + b) * NCOV * BLK + lane;
+    if (!(p < q && q < P.ntiles)) {
+#pragma unroll
+        for (int k = 0; k < NCOV; k++) out[(size_t)k * BLK] = (T)0;
+        return;
+    }
+    const int bl = baseline_index(p, q, P.ntiles);
     const size_t tstride = (size_t)P.nchan * P.nbl;
     const JonesF32* D0 = P.data + ((size_t)P.t0 * P.nchan + ch) * P.nbl + bl;
     const JonesF32* M0 = P.model + ((size_t)P.t0 * P.nchan + ch) * P.nbl + bl;
@@ -157,19 +184,26 @@ __global__ void collapse_kernel(const CalParams P, T* cov) {
             }
         }
     }
-    T* out = cov + (size_t)ch * NCOV * P.nbl + bl;
 #pragma unroll
     for (int k = 0; k < 16; k++) {
-        out[(size_t)k * P.nbl] = (T)xr[k];
-        out[(size_t)(16 + k) * P.nbl] = (T)xi[k];
+        out[(size_t)k * BLK] = (T)xr[k];
+        out[(size_t)(16 + k) * BLK] = (T)xi[k];
     }
 #pragma unroll
-    for (int u = 0; u < 4; u++) out[(size_t)(32 + u) * P.nbl] = (T)cd[u];
+    for (int u = 0; u < 4; u++) out[(size_t)(32 + u) * BLK] = (T)cd[u];
 #pragma unroll
     for (int k = 0; k < 6; k++) {
-        out[(size_t)(36 + 2 * k) * P.nbl] = (T)cr[k];
-        out[(size_t)(37 + 2 * k) * P.nbl] = (T)ci[k];
+        out[(size_t)(36 + 2 * k) * BLK] = (T)cr[k];
+        out[(size_t)(37 + 2 * k) * BLK] = (T)ci[k];
     }
+}
+
+template <typename T, bool SMEM>
+__device__ __forceinline__ double cov_ld(const T* p) {
+    if (SMEM)
+        return (double)*p;
+    else
+        return (double)__ldg(p);
 }
 
 // One baseline's tile1 and tile2 contributions from its covariances (cv:
@@ -180,7 +214,7 @@ __global__ void collapse_kernel(const CalParams P, T* cov) {
 // and conj(X) G1[2a+c] to t2[2b+d]; C[u][v] (and its conjugate C[v][u])
 // adds C H2[2b+d] to h1[2a+c] and C H1[2c+a] to h2[2d+b]; only the bot
 // entries 00, 11 (real) and 01 are kept.
-template <typename T>
+template <typename T, bool SMEM>
 __device__ __forceinline__ void collapsed_terms(const T* cv, size_t stride, const J2& g1, const J2& g2,
                                                 const Herm& H1, const Herm& H2, J2& t1, J2& t2, Herm& h1,
                                                 Herm& h2) {
@@ -192,8 +226,8 @@ __device__ __forceinline__ void collapsed_terms(const T* cv, size_t stride, cons
     for (int u = 0; u < 4; u++)
 #pragma unroll
         for (int v = 0; v < 4; v++) {
-            const cplx x{(double)__ldg(cv + (size_t)(u * 4 + v) * stride),
-                         (double)__ldg(cv + (size_t)(16 + u * 4 + v) * stride)};
+            const cplx x{cov_ld<T, SMEM>(cv + (size_t)(u * 4 + v) * stride),
+                         cov_ld<T, SMEM>(cv + (size_t)(16 + u * 4 + v) * stride)};
             T1[(u >> 1) * 2 + (v >> 1)] = T1[(u >> 1) * 2 + (v >> 1)] + x * G2[(u & 1) * 2 + (v & 1)];
             T2[(u & 1) * 2 + (v & 1)] = T2[(u & 1) * 2 + (v & 1)] + conj(x) * G1[(u >> 1) * 2 + (v >> 1)];
         }
@@ -207,13 +241,13 @@ __device__ __forceinline__ void collapsed_terms(const T* cv, size_t stride, cons
         b2[(v & 1) * 2 + (u & 1)] = b2[(v & 1) * 2 + (u & 1)] + c * h1m[(v >> 1) * 2 + (u >> 1)];
     };
 #pragma unroll
-    for (int u = 0; u < 4; u++) add(u, u, cplx{(double)__ldg(cv + (size_t)(32 + u) * stride), 0.0});
+    for (int u = 0; u < 4; u++) add(u, u, cplx{cov_ld<T, SMEM>(cv + (size_t)(32 + u) * stride), 0.0});
 #pragma unroll
     for (int u = 0; u < 4; u++)
 #pragma unroll
         for (int v = u + 1; v < 4; v++) {
-            const cplx c{(double)__ldg(cv + (size_t)(36 + 2 * cpair(u, v)) * stride),
-                         (double)__ldg(cv + (size_t)(37 + 2 * cpair(u, v)) * stride)};
+            const cplx c{cov_ld<T, SMEM>(cv + (size_t)(36 + 2 * cpair(u, v)) * stride),
+                         cov_ld<T, SMEM>(cv + (size_t)(37 + 2 * cpair(u, v)) * stride)};
             add(u, v, c);
             add(v, u, conj(c));
         }
@@ -221,8 +255,28 @@ __device__ __forceinline__ void collapsed_terms(const T* cv, size_t stride, cons
     h2 = Herm{b2[0].re, b2[3].re, b2[1]};
 }
 
+// Threads per CTA of the iteration kernel: the FP32 collapsed form runs two
+// groups of 256 (one per parity of the row block) on one shared ring.
+__host__ __device__ constexpr int cal_threads(int form) { return form == HDC_CAL_COLLAPSED_F32 ? 2 * CT : CT; }
+
+// barrier 1 + grp over one group of 256 threads; true when any passed true
+__device__ __forceinline__ bool group_sync_or(bool v, int grp) {
+    int r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.b32 p, %1, 0;\n\t"
+        "bar.red.or.pred q, %2, 256, p;\n\t"
+        "selp.b32 %0, 1, 0, q;\n\t}"
+        : "=r"(r)
+        : "r"((int)v), "r"(1 + grp)
+        : "memory");
+    return r != 0;
+}
+__device__ __forceinline__ void group_sync(int grp) { asm volatile("bar.sync %0, 256;" ::"r"(1 + grp) : "memory"); }
+
 template <int FORM>
-__global__ void __launch_bounds__(CT) mitchcal_kernel(const CalParams P) {
+__global__ void __launch_bounds__(cal_threads(FORM)) mitchcal_kernel(const CalParams P) {
+    constexpr int NTH = cal_threads(FORM);
     extern __shared__ double smem[];
     const int n = P.ntiles;
     J2* G = reinterpret_cast<J2*>(smem);          // current gains
@@ -242,18 +296,42 @@ __global__ void __launch_bounds__(CT) mitchcal_kernel(const CalParams P) {
     const JonesF32* D0 = P.data + ((size_t)P.t0 * P.nchan + ch) * P.nbl;
     const JonesF32* M0 = P.model + ((size_t)P.t0 * P.nchan + ch) * P.nbl;
 
-    for (int i = tid; i < n; i += CT) {
+    // FP32 collapsed form: ring of nring covariance blocks after colbuf
+    // (16-byte aligned for the bulk copies), one mbarrier per slot
+    __shared__ alignas(8) uint64_t ring_bar[4];
+    __shared__ uint32_t ring_cnt[4];  // copies issued per slot
+    const bool use_ring = FORM == 2 && P.nring > 0;
+    float* ring = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(colbuf + 16 * 16 * 12) + 15) & ~(uintptr_t)15);
+    uint32_t jseq = 0;  // covariance blocks consumed so far (all threads alike)
+    bool abort_loop = false;
+
+    for (int i = tid; i < n; i += NTH) {
         G[i] = load_j(P.di_jones[(size_t)i * P.nchan + ch]);
         Gold[i] = jzero();
         for (int k = 0; k < 4; k++) prec[4 * i + k] = 0.0;
         failed[i] = 0;
     }
+    if (use_ring && tid == 0) {
+        for (int s = 0; s < P.nring; s++) {
+            mbar_init(&ring_bar[s], 1);
+            ring_cnt[s] = 1;  // the first copy, issued below
+        }
+        fence_barrier_init();
+    }
     __syncthreads();
+    if (use_ring && tid == 0) {
+        for (int s = 0; s < P.nring; s++) {
+            mbar_arrive_expect_tx(&ring_bar[s], NCOV * BLK * sizeof(float));
+            bulk_g2s(ring + (size_t)s * NCOV * BLK,
+                     static_cast<const float*>(P.cov) + ((size_t)ch * P.nblk + s % P.nblk) * NCOV * BLK,
+                     NCOV * BLK * sizeof(float), &ring_bar[s]);
+        }
+    }
 
     int iteration = 0;
     while (iteration < P.max_iter) {
         iteration++;
-        for (int i = tid; i < n; i += CT) {
+        for (int i = tid; i < n; i += NTH) {
             top[i] = jzero();
             bot[i] = Herm{0.0, 0.0, {0.0, 0.0}};
             if (FORM != 0) {
@@ -267,7 +345,7 @@ __global__ void __launch_bounds__(CT) mitchcal_kernel(const CalParams P) {
         // ---- accumulate top / bot (calibration_loop) ----
         if (FORM == 0) {
         const int nwarp_bl = (P.nbl + 31) & ~31;
-        for (int base = tid & ~31; base < nwarp_bl; base += CT) {
+        for (int base = tid & ~31; base < nwarp_bl; base += NTH) {
             const int bl = base + lane;
             const bool active = bl < P.nbl;
             int p = -1 - lane, q = 0;  // unique keys for inactive lanes
@@ -319,27 +397,63 @@ __global__ void __launch_bounds__(CT) mitchcal_kernel(const CalParams P) {
             }
         }
         } else {
-            // collapsed: 16 x 16 blocks of tile pairs (p, q), p < q; thread
-            // (bi, bj) takes pair (16 pb + bi, 16 qb + bj).  Tile-1 sums run
-            // along a block row (16 consecutive lanes, shuffles), tile-2 sums
-            // along a block column (through shared memory), so every
-            // accumulator entry has one writer per block and no atomics.
-            const int bi = tid >> 4, bj = tid & 15;
+            // collapsed: 16 x 16 blocks of tile pairs (p, q), p < q, in
+            // storage order (column block qb outer, row block pb inner);
+            // thread (bi, bj) takes pair (16 pb + bi, 16 qb + bj).  Tile-1
+            // (row) sums run along a block row (16 consecutive lanes,
+            // shuffles) and go to top/bot[p] from one lane; tile-2 (column)
+            // sums stay in registers over the whole block column and are
+            // reduced across rows once per column block through shared
+            // memory -- every accumulator entry has one writer at a time and
+            // no atomics.  FP32 covariances arrive through the shared-memory
+            // ring (bulk copies issued nring blocks ahead); FP64 ones are
+            // loaded directly.
+            // FORM 2 runs two groups of 256 threads: group g takes the row
+            // blocks pb = g, g + 2, ... of every column block, so the two
+            // groups consume alternate ring slots; row sums of the two
+            // groups go to different tiles, and both groups meet once per
+            // column block to reduce its column sums.
+            constexpr int NG = NTH / BLK;
+            const int grp = tid / BLK, gt = tid % BLK;
+            const int bi = gt >> 4, bj = gt & 15;
             const int nb = (n + 15) / 16;
-            for (int pb = 0; pb < nb; pb++)
-                for (int qb = pb; qb < nb; qb++) {
-                    const int p = pb * 16 + bi, q = qb * 16 + bj;
+            bool gabort = false;
+            for (int qb = 0; qb < nb; qb++) {
+                const int q = qb * 16 + bj;
+                // tile q's gain and G^H G are the same for the whole block column
+                const J2 gq = q < n ? G[q] : jzero();
+                const Herm hq = q < n ? Hs[q] : Herm{0, 0, {0, 0}};
+                J2 c2 = jzero();
+                Herm ch2{0, 0, {0, 0}};
+                for (int pb = grp; pb <= qb && !gabort; pb += NG) {
+                    const int p = pb * 16 + bi;
+                    const int blk = qb * (qb + 1) / 2 + pb;
                     J2 t1 = jzero(), t2 = jzero();
                     Herm h1{0, 0, {0, 0}}, h2{0, 0, {0, 0}};
-                    if (p < q && q < n) {
-                        const size_t bl = (size_t)baseline_index(p, q, n);
+                    if (use_ring) {
+                        const uint32_t j = jseq + (uint32_t)blk;
+                        const int st = (int)(j % (uint32_t)P.nring);
+                        const bool ok = mbar_wait_bounded(&ring_bar[st], (j / (uint32_t)P.nring) & 1u, P.err);
+                        if (NG > 1 ? group_sync_or(!ok, grp) : __syncthreads_or(!ok)) {
+                            gabort = true;
+                            break;
+                        }
+                        if (p < q && q < n)
+                            collapsed_terms<float, true>(ring + (size_t)st * NCOV * BLK + gt, BLK, G[p], gq, Hs[p], hq,
+                                                         t1, t2, h1, h2);
+                    } else if (p < q && q < n) {
+                        const size_t off = ((size_t)ch * P.nblk + blk) * NCOV * BLK + gt;
                         if (FORM == 1)
-                            collapsed_terms(static_cast<const double*>(P.cov) + (size_t)ch * NCOV * P.nbl + bl,
-                                            (size_t)P.nbl, G[p], G[q], Hs[p], Hs[q], t1, t2, h1, h2);
+                            collapsed_terms<double, false>(static_cast<const double*>(P.cov) + off, BLK, G[p], gq,
+                                                           Hs[p], hq, t1, t2, h1, h2);
                         else
-                            collapsed_terms(static_cast<const float*>(P.cov) + (size_t)ch * NCOV * P.nbl + bl,
-                                            (size_t)P.nbl, G[p], G[q], Hs[p], Hs[q], t1, t2, h1, h2);
+                            collapsed_terms<float, false>(static_cast<const float*>(P.cov) + off, BLK, G[p], gq,
+                                                          Hs[p], hq, t1, t2, h1, h2);
                     }
+                    c2 = c2 + t2;
+                    ch2.a += h2.a;
+                    ch2.d += h2.d;
+                    ch2.b = ch2.b + h2.b;
                     double v[12] = {t1.a.re, t1.a.im, t1.b.re, t1.b.im, t1.c.re, t1.c.im,
                                     t1.d.re, t1.d.im, h1.a,    h1.d,    h1.b.re, h1.b.im};
 #pragma unroll
@@ -347,10 +461,6 @@ __global__ void __launch_bounds__(CT) mitchcal_kernel(const CalParams P) {
 #pragma unroll
                         for (int o = 8; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
                     }
-                    double* cb = colbuf + (size_t)(bi * 16 + bj) * 12;
-                    cb[0] = t2.a.re, cb[1] = t2.a.im, cb[2] = t2.b.re, cb[3] = t2.b.im;
-                    cb[4] = t2.c.re, cb[5] = t2.c.im, cb[6] = t2.d.re, cb[7] = t2.d.im;
-                    cb[8] = h2.a, cb[9] = h2.d, cb[10] = h2.b.re, cb[11] = h2.b.im;
                     if (bj == 0 && p < n) {
                         double* tp = reinterpret_cast<double*>(&top[p]);
 #pragma unroll
@@ -360,35 +470,69 @@ __global__ void __launch_bounds__(CT) mitchcal_kernel(const CalParams P) {
                         bot[p].b.re += v[10];
                         bot[p].b.im += v[11];
                     }
-                    __syncthreads();
-                    if (tid < 16 * 12) {
-                        const int j = tid / 12, k = tid - j * 12;
-                        const int qq = qb * 16 + j;
-                        double sum = 0.0;
-#pragma unroll
-                        for (int i = 0; i < 16; i++) sum += colbuf[(i * 16 + j) * 12 + k];
-                        if (qq < n) {
-                            if (k < 8)
-                                reinterpret_cast<double*>(&top[qq])[k] += sum;
-                            else if (k == 8)
-                                bot[qq].a += sum;
-                            else if (k == 9)
-                                bot[qq].d += sum;
-                            else if (k == 10)
-                                bot[qq].b.re += sum;
-                            else
-                                bot[qq].b.im += sum;
+                    if (use_ring) {
+                        // the group has read this slot: refill it nring blocks ahead
+                        if (NG > 1)
+                            group_sync(grp);
+                        else
+                            __syncthreads();
+                        if (gt == 0) {
+                            const uint32_t j = jseq + (uint32_t)blk;
+                            const int st = (int)(j % (uint32_t)P.nring);
+                            const int nxt = (int)((j + (uint32_t)P.nring) % (uint32_t)P.nblk);
+                            fence_proxy_async_smem();  // generic reads of the slot before the async write
+                            atomicAdd(&ring_cnt[st], 1u);
+                            mbar_arrive_expect_tx(&ring_bar[st], NCOV * BLK * sizeof(float));
+                            bulk_g2s(ring + (size_t)st * NCOV * BLK,
+                                     static_cast<const float*>(P.cov) + ((size_t)ch * P.nblk + nxt) * NCOV * BLK,
+                                     NCOV * BLK * sizeof(float), &ring_bar[st]);
                         }
                     }
-                    __syncthreads();
                 }
+                // column sums: rows bi and bi ^ 1 share a warp; one partial per warp
+                double cv2[12] = {c2.a.re, c2.a.im, c2.b.re, c2.b.im, c2.c.re, c2.c.im,
+                                  c2.d.re, c2.d.im, ch2.a,   ch2.d,   ch2.b.re, ch2.b.im};
+#pragma unroll
+                for (int k = 0; k < 12; k++) cv2[k] += __shfl_xor_sync(0xffffffffu, cv2[k], 16);
+                if ((tid & 31) < 16) {
+                    double* cb = colbuf + ((size_t)(tid >> 5) * 16 + bj) * 12;
+#pragma unroll
+                    for (int k = 0; k < 12; k++) cb[k] = cv2[k];
+                }
+                if (__syncthreads_or(gabort)) {
+                    abort_loop = true;
+                    break;
+                }
+                if (tid < 16 * 12) {
+                    const int jq = tid / 12, k = tid - jq * 12;
+                    const int qq = qb * 16 + jq;
+                    double sum = 0.0;
+#pragma unroll
+                    for (int w = 0; w < NTH / 32; w++) sum += colbuf[(w * 16 + jq) * 12 + k];
+                    if (qq < n) {
+                        if (k < 8)
+                            reinterpret_cast<double*>(&top[qq])[k] += sum;
+                        else if (k == 8)
+                            bot[qq].a += sum;
+                        else if (k == 9)
+                            bot[qq].d += sum;
+                        else if (k == 10)
+                            bot[qq].b.re += sum;
+                        else
+                            bot[qq].b.im += sum;
+                    }
+                }
+                __syncthreads();
+            }
+            if (use_ring) jseq += (uint32_t)P.nblk;
+            if (abort_loop) break;
         }
         __syncthreads();
 
         // ---- iteration-1 check: top == bot (and zeros) (mod.rs:701-750) ----
         if (iteration == 1) {
             int eq = 1, small = 1;
-            for (int i = tid; i < n; i += CT) {
+            for (int i = tid; i < n; i += NTH) {
                 const J2 tp = top[i];
                 const Herm b = bot[i];
                 const J2 bj = J2{{b.a, 0.0}, b.b, conj(b.b), {b.d, 0.0}};
@@ -405,14 +549,14 @@ __global__ void __launch_bounds__(CT) mitchcal_kernel(const CalParams P) {
             const int all_small = __syncthreads_and(small);
             if (all_eq) {
                 if (all_small)
-                    for (int i = tid; i < n; i += CT) failed[i] = 1;
+                    for (int i = tid; i < n; i += NTH) failed[i] = 1;
                 __syncthreads();
                 break;
             }
         }
 
         // ---- new gains (mod.rs:753-778) ----
-        for (int i = tid; i < n; i += CT) {
+        for (int i = tid; i < n; i += NTH) {
             if (failed[i]) continue;
             const Herm b = bot[i];
             const J2 bj = J2{{b.a, 0.0}, b.b, conj(b.b), {b.d, 0.0}};
@@ -426,7 +570,7 @@ __global__ void __launch_bounds__(CT) mitchcal_kernel(const CalParams P) {
             }
         }
         int my_failed = 0;
-        for (int i = tid; i < n; i += CT) my_failed += failed[i];
+        for (int i = tid; i < n; i += NTH) my_failed += failed[i];
         __shared__ int s_count;
         if (tid == 0) s_count = 0;
         __syncthreads();
@@ -438,7 +582,7 @@ __global__ void __launch_bounds__(CT) mitchcal_kernel(const CalParams P) {
         // ---- even iterations: precision, average, convergence (mod.rs:787-840) ----
         if (iteration % 2 == 0) {
             int below = 1;
-            for (int i = tid; i < n; i += CT) {
+            for (int i = tid; i < n; i += NTH) {
                 if (!failed[i]) {
                     const J2 g = G[i], o = Gold[i];
                     const J2 df = g - o;
@@ -453,19 +597,26 @@ __global__ void __launch_bounds__(CT) mitchcal_kernel(const CalParams P) {
             }
             if (__syncthreads_and(below)) break;
         }
-        for (int i = tid; i < n; i += CT) Gold[i] = G[i];
+        for (int i = tid; i < n; i += NTH) Gold[i] = G[i];
         __syncthreads();
+    }
+    __syncthreads();
+    // the ring's copies still in flight land before the CTA leaves: the
+    // last copy issued to each slot (copies to one slot complete in order)
+    if (use_ring && tid == 0) {
+        for (int st = 0; st < P.nring; st++)
+            if (ring_cnt[st] > 0) mbar_wait_bounded(&ring_bar[st], (ring_cnt[st] - 1) & 1u, P.err);
     }
     __syncthreads();
 
     // ---- finalise (mod.rs:843-893) ----
-    __shared__ double s_max[CT / 32];
+    __shared__ double s_max[NTH / 32];
     __shared__ int s_nfail;
     if (tid == 0) s_nfail = 0;
     __syncthreads();
     double mx = -1.7976931348623157e308;  // f64::MIN
     int nf_local = 0;
-    for (int i = tid; i < n; i += CT) {
+    for (int i = tid; i < n; i += NTH) {
         if (failed[i]) {
             nf_local++;
             continue;
@@ -477,11 +628,11 @@ __global__ void __launch_bounds__(CT) mitchcal_kernel(const CalParams P) {
     if (nf_local) atomicAdd(&s_nfail, nf_local);
     __syncthreads();
     double max_precision = s_max[0];
-    for (int w = 1; w < CT / 32; w++) max_precision = fmax(max_precision, s_max[w]);
+    for (int w = 1; w < NTH / 32; w++) max_precision = fmax(max_precision, s_max[w]);
     const int num_failed = s_nfail;
-    const bool converged = !(n - num_failed <= 4 || max_precision > P.min_thr);
+    const bool converged = !abort_loop && !(n - num_failed <= 4 || max_precision > P.min_thr);
     const double qnan = __longlong_as_double(0x7ff8000000000000ll);
-    for (int i = tid; i < n; i += CT) {
+    for (int i = tid; i < n; i += NTH) {
         JonesF64 out;
         if (!converged || failed[i])
             out = JonesF64{qnan, qnan, qnan, qnan, qnan, qnan, qnan, qnan};
@@ -613,10 +764,27 @@ int launch_judge(const JonesF32* d_data, const JonesF32* d_model, int t0, int t1
     return HDC_OK;
 }
 
-static size_t smem_bytes(int n, int form) {
+static size_t smem_base_bytes(int n, int form) {
     const size_t base = (size_t)n * (3 * sizeof(J2) + 2 * sizeof(Herm) + 4 * sizeof(double)) +
                         sizeof(int) * (size_t)((n + 1) & ~1);
     return base + (form != HDC_CAL_PLAIN ? 16 * 16 * 12 * sizeof(double) : 0);
+}
+
+constexpr size_t SMEM_LIMIT = 227 * 1024;
+constexpr size_t RING_SLOT = (size_t)NCOV * BLK * sizeof(float);
+
+// ring depth of the FP32 collapsed form: 3 slots where they fit, else 2,
+// else direct loads
+static int ring_depth(int n, int form) {
+    if (form != HDC_CAL_COLLAPSED_F32) return 0;
+    for (int r = 3; r >= 2; r--)
+        if (smem_base_bytes(n, form) + 16 + r * RING_SLOT <= SMEM_LIMIT) return r;
+    return 0;
+}
+
+static size_t smem_bytes(int n, int form) {
+    const int r = ring_depth(n, form);
+    return smem_base_bytes(n, form) + (r ? 16 + r * RING_SLOT : 0);
 }
 
 template <int FORM>
@@ -624,7 +792,7 @@ static int launch_mitchcal_form(const CalParams& P, int nblocks, cudaStream_t s)
     const size_t sm = smem_bytes(P.ntiles, FORM);
     HDC_CUDA_RET_INT(
         cudaFuncSetAttribute(mitchcal_kernel<FORM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    mitchcal_kernel<FORM><<<nblocks, CT, sm, s>>>(P);
+    mitchcal_kernel<FORM><<<nblocks, cal_threads(FORM), sm, s>>>(P);
     count_launches(1);
     HDC_CUDA_RET_INT(cudaGetLastError());
     return HDC_OK;
@@ -635,11 +803,11 @@ static int launch_mitchcal_form(const CalParams& P, int nblocks, cudaStream_t s)
 static void launch_mitchcal_captured(const CalParams& P, int form, int nblocks, cudaStream_t s) {
     const size_t sm = smem_bytes(P.ntiles, form);
     if (form == HDC_CAL_COLLAPSED)
-        mitchcal_kernel<1><<<nblocks, CT, sm, s>>>(P);
+        mitchcal_kernel<1><<<nblocks, cal_threads(1), sm, s>>>(P);
     else if (form == HDC_CAL_COLLAPSED_F32)
-        mitchcal_kernel<2><<<nblocks, CT, sm, s>>>(P);
+        mitchcal_kernel<2><<<nblocks, cal_threads(2), sm, s>>>(P);
     else
-        mitchcal_kernel<0><<<nblocks, CT, sm, s>>>(P);
+        mitchcal_kernel<0><<<nblocks, cal_threads(0), sm, s>>>(P);
     count_launches(1);
 }
 
@@ -660,11 +828,11 @@ __global__ void identity_kernel(JonesF64* dj, size_t n) {
 }
 
 static void launch_collapse(const CalParams& P, int form, void* cov, cudaStream_t s) {
-    const dim3 grid((P.nbl + 127) / 128, P.nchan);
+    const dim3 grid(2 * P.nblk, P.nchan);
     if (form == HDC_CAL_COLLAPSED)
-        collapse_kernel<double><<<grid, 128, 0, s>>>(P, static_cast<double*>(cov));
+        collapse_kernel<double><<<grid, BLK / 2, 0, s>>>(P, static_cast<double*>(cov));
     else
-        collapse_kernel<float><<<grid, 128, 0, s>>>(P, static_cast<float*>(cov));
+        collapse_kernel<float><<<grid, BLK / 2, 0, s>>>(P, static_cast<float*>(cov));
     count_launches(1);
 }
 
@@ -827,21 +995,19 @@ extern "C" int hdc_calibrate_timeblock(const JonesF32* d_data_tfb, const JonesF3
     P.pols = pols;
     P.results = d_res;
     P.cov = nullptr;
+    P.nblk = cov_blocks(ntiles);
+    P.nring = ring_depth(ntiles, form);
+    P.err = device_error_word();
     if (form != HDC_CAL_PLAIN) {
         const size_t elem = form == HDC_CAL_COLLAPSED ? sizeof(double) : sizeof(float);
-        void* cov = covariance_buffer(elem * NCOV * (size_t)num_chanblocks * num_baselines);
+        void* cov = covariance_buffer(elem * NCOV * BLK * (size_t)num_chanblocks * P.nblk);
         if (!cov) {
             cleanup();
             set_error("hdc_calibrate_timeblock: covariance allocation failed");
             return HDC_ERR_ALLOC;
         }
         P.cov = cov;
-        const dim3 grid((num_baselines + 127) / 128, num_chanblocks);
-        if (form == HDC_CAL_COLLAPSED)
-            collapse_kernel<double><<<grid, 128, 0, s>>>(P, static_cast<double*>(cov));
-        else
-            collapse_kernel<float><<<grid, 128, 0, s>>>(P, static_cast<float*>(cov));
-        count_launches(1);
+        launch_collapse(P, form, cov, s);
         if (cudaGetLastError() != cudaSuccess) {
             cleanup();
             set_error("hdc_calibrate_timeblock: collapse launch failed");
@@ -860,6 +1026,11 @@ extern "C" int hdc_calibrate_timeblock(const JonesF32* d_data_tfb, const JonesF3
         cleanup();
         set_error("hdc_calibrate_timeblock: %s", cudaGetErrorString(cudaGetLastError()));
         return HDC_ERR_CUDA;
+    }
+    if (form == HDC_CAL_COLLAPSED_F32 && take_device_error(s)) {
+        cleanup();
+        set_error("hdc_calibrate_timeblock: a covariance copy did not arrive in time");
+        return HDC_ERR_TIMEOUT;
     }
     rc = retry_failed(P, form, res, d_list, d_pairs, s);
     if (rc) {
@@ -919,9 +1090,11 @@ extern "C" int hdc_calibrate_timeblocks(const JonesF32* d_data_tfb, const JonesF
         return HDC_ERR_ALLOC;
     }
     void* cov = nullptr;
+    const int nblk = cov_blocks(ntiles), nring = ring_depth(ntiles, form);
+    int* errw = device_error_word();
     if (form != HDC_CAL_PLAIN) {
         const size_t elem = form == HDC_CAL_COLLAPSED ? sizeof(double) : sizeof(float);
-        cov = covariance_buffer(elem * NCOV * (size_t)num_chanblocks * num_baselines);
+        cov = covariance_buffer(elem * NCOV * BLK * (size_t)num_chanblocks * nblk);
         if (!cov) {
             cleanup();
             set_error("hdc_calibrate_timeblocks: covariance allocation failed");
@@ -952,6 +1125,9 @@ extern "C" int hdc_calibrate_timeblocks(const JonesF32* d_data_tfb, const JonesF
         P.pols = pols;
         P.results = d_res + (size_t)k * num_chanblocks;
         P.cov = cov;
+        P.nblk = nblk;
+        P.nring = nring;
+        P.err = errw;
         return P;
     };
     cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
@@ -977,6 +1153,11 @@ extern "C" int hdc_calibrate_timeblocks(const JonesF32* d_data_tfb, const JonesF
         cleanup();
         set_error("hdc_calibrate_timeblocks: %s", cudaGetErrorString(e));
         return HDC_ERR_CUDA;
+    }
+    if (form == HDC_CAL_COLLAPSED_F32 && take_device_error(s)) {
+        cleanup();
+        set_error("hdc_calibrate_timeblocks: a covariance copy did not arrive in time");
+        return HDC_ERR_TIMEOUT;
     }
     for (int k = 0; k < num_timeblocks; k++) {
         std::vector<HdcCalResult> rk(res.begin() + (size_t)k * num_chanblocks,

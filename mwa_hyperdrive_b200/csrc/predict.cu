@@ -12,6 +12,7 @@
 // reference does (model/cpu.rs:341-348, gpu/model.cu:171).
 
 #include <cstdio>
+#include <vector>
 
 #include "predict.cuh"
 
@@ -544,7 +545,7 @@ static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 // Sum of per-component coefficient counts needs a device read; the drop-in
 // entry point copies the counts back (small) to size the repacked table.
 static const char* dropin_model(int type, const GroupIn g[3], const Addresses* a, const UVW* d_uvws,
-                                const JonesF64* d_beam_jones, JonesF32* d_vis_fb) {
+                                const JonesF64* d_beam_jones, void* d_vis_fb, bool out64) {
     const int nc = g[0].n + g[1].n + g[2].n;
     if (nc == 0) return NULL;
     const int nf = a->num_freqs, nbl = a->num_baselines;
@@ -636,7 +637,7 @@ static const char* dropin_model(int type, const GroupIn g[3], const Addresses* a
     p.vis = d_vis_fb;
     p.err = device_error_word();
     const bool tile_beam = d_beam_jones != nullptr;
-    HDC_CUDA_RET_STR(launch_direct(type, tile_beam, false, p, 0));
+    HDC_CUDA_RET_STR(launch_direct(type, tile_beam, out64, p, 0));
 #ifdef HDC_DEBUG_SYNC
     HDC_CUDA_RET_STR(cudaDeviceSynchronize());
 #endif
@@ -706,14 +707,101 @@ const char* points_with_workspace(const Points* comps, const Addresses* a, const
 
 using namespace hdc;
 
-extern "C" const char* model_points(const Points* comps, const Addresses* a, const UVW* d_uvws,
-                                    const JonesF64* d_beam_jones, JonesF32* d_vis_fb) {
-    GroupIn g[3] = {};
+static void point_groups(const Points* comps, GroupIn g[3]) {
     g[0] = GroupIn{comps->num_power_laws, comps->power_law_lmns, comps->power_law_fds, comps->power_law_sis};
     g[1] = GroupIn{comps->num_curved_power_laws, comps->curved_power_law_lmns, comps->curved_power_law_fds,
                    comps->curved_power_law_sis, comps->curved_power_law_qs};
     g[2] = GroupIn{comps->num_lists, comps->list_lmns, comps->list_fds};
-    return dropin_model(0, g, a, d_uvws, d_beam_jones, d_vis_fb);
+}
+
+extern "C" const char* model_points(const Points* comps, const Addresses* a, const UVW* d_uvws,
+                                    const JonesF64* d_beam_jones, JonesF32* d_vis_fb) {
+    GroupIn g[3] = {};
+    point_groups(comps, g);
+    return dropin_model(0, g, a, d_uvws, d_beam_jones, d_vis_fb, false);
+}
+
+extern "C" const char* model_points_f64out(const Points* comps, const Addresses* a, const UVW* d_uvws,
+                                           const JonesF64* d_beam_jones, JonesF64* d_vis_fb) {
+    GroupIn g[3] = {};
+    point_groups(comps, g);
+    return dropin_model(0, g, a, d_uvws, d_beam_jones, d_vis_fb, true);
+}
+
+// W [nf][nc] = B S B^H with the beam row of one unique tile
+__global__ void shared_beam_kernel(const JonesF64* S, const JonesF64* beam, int beam_tile, const int* freq_map,
+                                   int n_uniq_freq, int nc, int nf, JonesF64* W) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int f = blockIdx.y;
+    if (c >= nc || f >= nf) return;
+    const J2 b = load_j(beam[((size_t)beam_tile * n_uniq_freq + freq_map[f]) * nc + c]);
+    W[(size_t)f * nc + c] = store_j((b * load_j(S[(size_t)f * nc + c])) * herm(b));
+}
+
+extern "C" const char* model_points_tc(const Points* comps, const Addresses* a, const XYZ* d_tile_xyzs,
+                                       double lst_rad, RADec phase_centre, const JonesF64* d_beam_jones,
+                                       JonesF32* d_vis_fb) {
+    GroupIn g[3] = {};
+    point_groups(comps, g);
+    const int nc = g[0].n + g[1].n + g[2].n;
+    if (nc == 0) return NULL;
+    const int nf = a->num_freqs, nbl = a->num_baselines;
+    const int ntiles = (int)((1.0 + sqrt(1.0 + 8.0 * nbl)) / 2.0 + 0.5);
+    if (ntiles * (ntiles - 1) / 2 != nbl || !d_tile_xyzs) return "model_points_tc: invalid arguments";
+    int beam_tile = -1;
+    if (d_beam_jones) {
+        // one beam for all tiles: every tile maps to the same unique beam row
+        std::vector<int> um(ntiles), tm(ntiles);
+        if (!a->d_tile_map || !a->d_freq_map) return "model_points_tc: beam maps missing";
+        if (a->d_tile_index_to_unflagged_tile_index_map)
+            HDC_CUDA_RET_STR(cudaMemcpy(um.data(), a->d_tile_index_to_unflagged_tile_index_map, sizeof(int) * ntiles,
+                                        cudaMemcpyDeviceToHost));
+        else
+            for (int t = 0; t < ntiles; t++) um[t] = t;
+        HDC_CUDA_RET_STR(cudaMemcpy(tm.data(), a->d_tile_map, sizeof(int) * ntiles, cudaMemcpyDeviceToHost));
+        for (int t = 0; t < ntiles; t++) {
+            if (um[t] < 0 || um[t] >= ntiles) return "model_points_tc: tile map out of range";
+            const int bt = tm[um[t]];
+            if (beam_tile >= 0 && bt != beam_tile)
+                return "model_points_tc: the tensor-core form needs one beam shared by all tiles";
+            beam_tile = bt;
+        }
+    }
+    size_t off_lmn = 0;
+    size_t off_flux = align256(off_lmn + sizeof(double4) * nc);
+    size_t off_w = align256(off_flux + sizeof(JonesF64) * (size_t)nf * nc);
+    size_t off_gp = align256(off_w + (d_beam_jones ? sizeof(JonesF64) * (size_t)nf * nc : 0));
+    size_t total = align256(off_gp + sizeof(double4) * nc);
+    char* ws = (char*)device_scratch(total);
+    if (!ws) return "out of device memory";
+    PrepIn in = {};
+    for (int i = 0; i < 3; i++) in.g[i] = g[i];
+    in.nc = nc;
+    in.nf = nf;
+    in.nbl = nbl;
+    in.type = 0;
+    in.freqs = a->d_freqs;
+    in.lmn = (double4*)(ws + off_lmn);
+    in.flux = (JonesF64*)(ws + off_flux);
+    in.flux_ld = nc;
+    in.gp = (double4*)(ws + off_gp);
+    dim3 pg((nc + 127) / 128, nf);
+    dropin_prep_kernel<<<pg, 128>>>(in);
+    count_launches(1);
+    HDC_CUDA_RET_STR(cudaGetLastError());
+    const JonesF64* W = in.flux;
+    if (d_beam_jones) {
+        JonesF64* Wb = (JonesF64*)(ws + off_w);
+        shared_beam_kernel<<<pg, 128>>>(in.flux, d_beam_jones, beam_tile, a->d_freq_map, a->num_unique_beam_freqs, nc,
+                                        nf, Wb);
+        count_launches(1);
+        HDC_CUDA_RET_STR(cudaGetLastError());
+        W = Wb;
+    }
+    const int rc = launch_tensor_points(nf, nbl, ntiles, nc, a->d_freqs, d_tile_xyzs, lst_rad - phase_centre.ra,
+                                        phase_centre.dec, in.lmn, W, d_vis_fb, false, device_error_word(), 0);
+    if (rc) return hdc_last_error();
+    return NULL;
 }
 
 extern "C" const char* model_gaussians(const Gaussians* comps, const Addresses* a, const UVW* d_uvws,
@@ -724,7 +812,18 @@ extern "C" const char* model_gaussians(const Gaussians* comps, const Addresses* 
     g[1] = GroupIn{comps->num_curved_power_laws, comps->curved_power_law_lmns, comps->curved_power_law_fds,
                    comps->curved_power_law_sis, comps->curved_power_law_qs, comps->curved_power_law_gps};
     g[2] = GroupIn{comps->num_lists, comps->list_lmns, comps->list_fds, nullptr, nullptr, comps->list_gps};
-    return dropin_model(1, g, a, d_uvws, d_beam_jones, d_vis_fb);
+    return dropin_model(1, g, a, d_uvws, d_beam_jones, d_vis_fb, false);
+}
+
+extern "C" const char* model_gaussians_f64out(const Gaussians* comps, const Addresses* a, const UVW* d_uvws,
+                                              const JonesF64* d_beam_jones, JonesF64* d_vis_fb) {
+    GroupIn g[3] = {};
+    g[0] = GroupIn{comps->num_power_laws, comps->power_law_lmns, comps->power_law_fds, comps->power_law_sis, nullptr,
+                   comps->power_law_gps};
+    g[1] = GroupIn{comps->num_curved_power_laws, comps->curved_power_law_lmns, comps->curved_power_law_fds,
+                   comps->curved_power_law_sis, comps->curved_power_law_qs, comps->curved_power_law_gps};
+    g[2] = GroupIn{comps->num_lists, comps->list_lmns, comps->list_fds, nullptr, nullptr, comps->list_gps};
+    return dropin_model(1, g, a, d_uvws, d_beam_jones, d_vis_fb, true);
 }
 
 extern "C" const char* model_shapelets(const Shapelets* comps, const Addresses* a, const UVW* d_uvws,
@@ -745,7 +844,28 @@ extern "C" const char* model_shapelets(const Shapelets* comps, const Addresses* 
     g[2] = GroupIn{comps->num_lists,          comps->list_lmns,           comps->list_fds,
                    nullptr,                   nullptr,                    comps->list_gps,
                    comps->list_shapelet_uvs,  comps->list_shapelet_coeffs, comps->list_num_shapelet_coeffs};
-    return dropin_model(2, g, a, d_uvws, d_beam_jones, d_vis_fb);
+    return dropin_model(2, g, a, d_uvws, d_beam_jones, d_vis_fb, false);
+}
+
+extern "C" const char* model_shapelets_f64out(const Shapelets* comps, const Addresses* a, const UVW* d_uvws,
+                                              const JonesF64* d_beam_jones, JonesF64* d_vis_fb) {
+    GroupIn g[3] = {};
+    g[0] = GroupIn{comps->num_power_laws,           comps->power_law_lmns,          comps->power_law_fds,
+                   comps->power_law_sis,            nullptr,                        comps->power_law_gps,
+                   comps->power_law_shapelet_uvs,   comps->power_law_shapelet_coeffs, comps->power_law_num_shapelet_coeffs};
+    g[1] = GroupIn{comps->num_curved_power_laws,
+                   comps->curved_power_law_lmns,
+                   comps->curved_power_law_fds,
+                   comps->curved_power_law_sis,
+                   comps->curved_power_law_qs,
+                   comps->curved_power_law_gps,
+                   comps->curved_power_law_shapelet_uvs,
+                   comps->curved_power_law_shapelet_coeffs,
+                   comps->curved_power_law_num_shapelet_coeffs};
+    g[2] = GroupIn{comps->num_lists,          comps->list_lmns,           comps->list_fds,
+                   nullptr,                   nullptr,                    comps->list_gps,
+                   comps->list_shapelet_uvs,  comps->list_shapelet_coeffs, comps->list_num_shapelet_coeffs};
+    return dropin_model(2, g, a, d_uvws, d_beam_jones, d_vis_fb, true);
 }
 
 extern "C" const char* model_autos(int num_tiles, int num_freqs, const double* freqs, const Points* points,

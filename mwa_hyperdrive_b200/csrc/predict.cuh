@@ -49,6 +49,11 @@ struct DirectParams {
 cudaError_t launch_direct(int ty, bool tile_beam, bool out64, const DirectParams& p, cudaStream_t s,
                           bool fast = false);
 
+// The tensor-core point predict of one timestep (csrc/tensor.cu).
+int launch_tensor_points(int nf, int nbl, int ntiles, int nc, const double* d_freqs, const XYZ* d_xyzs, double ha,
+                         double dec, const double4* d_lmn, const JonesF64* d_W, void* d_vis, bool out64, int* d_err,
+                         cudaStream_t s);
+
 struct AutosParams {
     int ntiles, nf;
     int nc_total;

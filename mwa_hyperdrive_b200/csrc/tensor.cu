@@ -58,6 +58,8 @@
 #include <algorithm>
 #include <cmath>
 
+#include <mutex>
+
 #include "modeller.cuh"
 
 namespace hdc {
@@ -540,22 +542,41 @@ int Modeller::tensor_setup() {
     return HDC_OK;
 }
 
-int Modeller::tensor_points(double lst, void* d_vis, bool out64, cudaStream_t s) {
-    if (t[0].nc == 0) return HDC_OK;
+// The tensor-core point predict of one timestep over device tables: lmn
+// [nc] (turns), W [nf][nc] (B S B^H of a beam shared by all tiles), tile
+// XYZs, hour angle and declination of the phase centre; accumulates into
+// vis [nf][nbl] (JonesF32, or JonesF64 with out64).
+int launch_tensor_points(int nf, int nbl, int ntiles, int nc, const double* d_freqs, const XYZ* d_xyzs, double ha,
+                         double dec, const double4* d_lmn, const JonesF64* d_W, void* d_vis, bool out64, int* d_err,
+                         cudaStream_t s) {
+    if (nc == 0) return HDC_OK;
+    if (ntiles > tc::NT) {
+        set_error("the tensor-core predict supports up to %d tiles (have %d)", tc::NT, ntiles);
+        return HDC_ERR_UNSUPPORTED;
+    }
+    static std::once_flag once;
+    static cudaError_t attr_err = cudaSuccess;
+    std::call_once(once, [] {
+        attr_err = cudaFuncSetAttribute(tc::gram_i8_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        tc::SMEM_BYTES);
+        if (attr_err == cudaSuccess)
+            attr_err = cudaFuncSetAttribute(tc::gram_i8_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            tc::SMEM_BYTES);
+    });
+    HDC_CUDA_RET_INT(attr_err);
     tc::Params P;
     P.nf = nf;
     P.nbl = nbl;
     P.ntiles = ntiles;
-    P.nc = t[0].nc;
+    P.nc = nc;
     P.freqs = d_freqs;
     P.xyzs = d_xyzs;
-    const double ha = lst - pc.ra;
     P.s_ha = std::sin(ha);
     P.c_ha = std::cos(ha);
-    P.s_dec = std::sin(pc.dec);
-    P.c_dec = std::cos(pc.dec);
-    P.lmn = t[0].d_lmn;
-    P.W = weights(0);
+    P.s_dec = std::sin(dec);
+    P.c_dec = std::cos(dec);
+    P.lmn = d_lmn;
+    P.W = d_W;
     P.vis = d_vis;
     P.err = d_err;
     // passes of at most KPASS components accumulate into the visibilities in turn
@@ -571,6 +592,12 @@ int Modeller::tensor_points(double lst, void* d_vis, bool out64, cudaStream_t s)
         HDC_CUDA_RET_INT(cudaGetLastError());
     }
     return HDC_OK;
+}
+
+int Modeller::tensor_points(double lst, void* d_vis, bool out64, cudaStream_t s) {
+    if (t[0].nc == 0) return HDC_OK;
+    return launch_tensor_points(nf, nbl, ntiles, t[0].nc, d_freqs, d_xyzs, lst - pc.ra, pc.dec, t[0].d_lmn,
+                                weights(0), d_vis, out64, d_err, s);
 }
 
 void Modeller::tensor_release() {

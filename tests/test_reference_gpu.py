@@ -72,7 +72,7 @@ def rel(a, b):
     return np.linalg.norm(a - b) / np.linalg.norm(b)
 
 
-def dropin_inputs(oracle, ntiles, nf, ncomp_per_group, ctype, seed, ntile_beams=3, nfreq_beams=2):
+def dropin_inputs(oracle, ntiles, nf, ncomp_per_group, ctype, seed, ntile_beams=3, nfreq_beams=2, want_obs=False):
     """Device inputs of the reference's model_* FFI: 3 groups (power law,
     curved power law, list) of one component type, per-tile beam Jones."""
     pc = (0.3, math.radians(-30.0))
@@ -134,10 +134,60 @@ def dropin_inputs(oracle, ntiles, nf, ncomp_per_group, ctype, seed, ntile_beams=
                                  m, o(1), fds + m * 64, sis + m * 8, qs, gpar + m * 24, suvs[1], coeffs + 2 * m * 16,
                                  ncoef + m * 4,
                                  m, o(2), lf, gpar + 2 * m * 24, suvs[2], coeffs + 4 * m * 16, ncoef + 2 * m * 4)
+    if want_obs:
+        return comps_s, a, dev(uvws).data_ptr(), dev(beam).data_ptr(), (nf, nbl), obs
     return comps_s, a, dev(uvws).data_ptr(), dev(beam).data_ptr(), (nf, nbl)
 
 
 FN = {0: "model_points", 1: "model_gaussians", 2: "model_shapelets"}
+
+
+@pytest.mark.parametrize("ctype", [0, 1, 2])
+def test_f64out_variants(oracle, ref, ctype):
+    """model_*_f64out: the same predict with FP64 output; rounded to FP32 it
+    is the reference kernel's result (4 ulps), and it accumulates."""
+    comps, a, uvws, beam, (nf, nbl) = dropin_inputs(oracle, 21, 6, 4, ctype, 31 + ctype)
+    out_ref = torch.zeros((nf, nbl, 8), dtype=torch.float32, device="cuda")
+    _lib.check_str(getattr(ref, FN[ctype])(ctypes.byref(comps), ctypes.byref(a), uvws, beam, out_ref.data_ptr()),
+                   "reference " + FN[ctype])
+    out64 = torch.zeros((nf, nbl, 8), dtype=torch.float64, device="cuda")
+    fn = getattr(_lib.lib(), FN[ctype] + "_f64out")
+    _lib.check_str(fn(ctypes.byref(comps), ctypes.byref(a), uvws, beam, out64.data_ptr()), FN[ctype] + "_f64out")
+    torch.cuda.synchronize()
+    got = out64.cpu().numpy()
+    assert_f32_close(got.astype(np.float32), out_ref.cpu().numpy(), ulps=4)
+    _lib.check_str(fn(ctypes.byref(comps), ctypes.byref(a), uvws, beam, out64.data_ptr()), FN[ctype] + "_f64out")
+    torch.cuda.synchronize()
+    np.testing.assert_allclose(out64.cpu().numpy(), 2.0 * got, rtol=1e-15, atol=0)
+
+
+def test_model_points_tc(oracle):
+    """model_points_tc (tensor cores, per-tile XYZs) against the FP64 predict
+    of the same drop-in inputs with a beam shared by all tiles: within 1e-6
+    of the rms visibility (normwise and p99.9); a per-tile beam is refused."""
+    comps, a, uvws, beam, (nf, nbl), obs = dropin_inputs(oracle, 64, 5, 40, 0, 8, ntile_beams=1, nfreq_beams=2,
+                                                         want_obs=True)
+    ref64 = torch.zeros((nf, nbl, 8), dtype=torch.float64, device="cuda")
+    _lib.check_str(_lib.lib().model_points_f64out(ctypes.byref(comps), ctypes.byref(a), uvws, beam,
+                                                  ref64.data_ptr()), "model_points_f64out")
+    got = torch.zeros((nf, nbl, 8), dtype=torch.float32, device="cuda")
+    xyz = dev(obs.tile_xyzs)
+    pc = _lib.RADec(*obs.phase_centre)
+    _lib.check_str(_lib.lib().model_points_tc(ctypes.byref(comps), ctypes.byref(a), xyz.data_ptr(),
+                                              float(obs.lsts[0]), pc, beam, got.data_ptr()), "model_points_tc")
+    torch.cuda.synchronize()
+    r = ref64.cpu().numpy()
+    d = got.cpu().numpy().astype(np.float64) - r
+    rms = np.sqrt(np.mean(r ** 2))
+    nrm = np.sqrt(np.mean(d ** 2)) / rms
+    p999 = np.quantile(np.abs(d), 0.999) / rms
+    print(f"model_points_tc: normwise {nrm:.2e}, p99.9 {p999:.2e}")
+    assert nrm < 1e-6 and p999 < 1e-6, (nrm, p999)
+    comps3, a3, _, beam3, _, obs3 = dropin_inputs(oracle, 64, 5, 40, 0, 8, ntile_beams=3, nfreq_beams=2,
+                                                  want_obs=True)
+    msg = _lib.lib().model_points_tc(ctypes.byref(comps3), ctypes.byref(a3), dev(obs3.tile_xyzs).data_ptr(),
+                                     float(obs3.lsts[0]), _lib.RADec(*obs3.phase_centre), beam3, got.data_ptr())
+    assert msg is not None and b"one beam" in msg
 
 
 @pytest.mark.parametrize("ctype", [0, 1, 2])
