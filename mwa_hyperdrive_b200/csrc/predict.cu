@@ -96,12 +96,8 @@ __device__ __forceinline__ void shapelet_envelope_f32(const DirectParams& p, int
 // a (value, next - value) pair each), then contracted with the component's
 // signed dense coefficient matrix C (shared memory):
 //     env = sum_{n1,n2} C[n1][n2] X[n1] Y[n2],  even n1 + n2 -> re, odd -> im.
-__device__ __forceinline__ void shapelet_envelope_dense(const DirectParams& p, const float* __restrict__ cm,
-                                                        double4 g, double su, double sv, float& er, float& ei) {
-    const double x = su * g.z + sv * g.w;
-    const double y = su * g.w - sv * g.z;
-    const double x_pos = x * g.x + SBF_C;
-    const double y_pos = y * g.y + SBF_C;
+__device__ __forceinline__ void shapelet_dense_at(const DirectParams& p, const float* __restrict__ cm, double x_pos,
+                                                  double y_pos, float& er, float& ei) {
     const double fx = floor(x_pos), fy = floor(y_pos);
     const int xi = fx > 0.0 ? (int)fmin(fx, (double)(SBF_L - 2)) : 0;
     const int yi = fy > 0.0 ? (int)fmin(fy, (double)(SBF_L - 2)) : 0;
@@ -130,6 +126,13 @@ __device__ __forceinline__ void shapelet_envelope_dense(const DirectParams& p, c
     }
     er = re;
     ei = im;
+}
+
+__device__ __forceinline__ void shapelet_envelope_dense(const DirectParams& p, const float* __restrict__ cm,
+                                                        double4 g, double su, double sv, float& er, float& ei) {
+    const double x = su * g.z + sv * g.w;
+    const double y = su * g.w - sv * g.z;
+    shapelet_dense_at(p, cm, x * g.x + SBF_C, y * g.y + SBF_C, er, ei);
 }
 
 // FAST (the chosen form's Gaussians and shapelets, shared beam only): the
@@ -323,6 +326,174 @@ __global__ void __launch_bounds__(DT) direct_kernel(const DirectParams p) {
     }
 }
 
+// The chosen form's Gaussians and shapelets with FCH channels per thread: a
+// CTA covers 256 baselines of FCH consecutive channels, so each component's
+// FP64 work that does not depend on the channel -- the phase in metres, the
+// Gaussian exponent in metres^2, the shapelet coordinates, their shared-
+// memory and table-position loads -- is done once for all FCH channels and
+// only scaled per channel (lambda^-1 for the phase and positions, lambda^-2
+// for the exponent).  The arithmetic per channel is that of the FAST
+// direct_kernel above.
+constexpr int FCH = 2;
+
+template <int TYPE, bool OUT64>
+__global__ void __launch_bounds__(DT) fast_kernel(const DirectParams p) {
+    __shared__ alignas(128) double4 s_lmn[2][CH];
+    __shared__ alignas(128) JonesF64 s_flux[2][FCH][CH];
+    __shared__ alignas(128) double4 s_gp[2][CH];
+    __shared__ alignas(16) float s_wf[FCH][CH * 8];
+    __shared__ alignas(16) float s_dense[TYPE == 2 ? CH * SDN * SDN : 1];
+    __shared__ alignas(8) uint64_t bar[2];
+
+    const int f0 = blockIdx.y * FCH;
+    const int bl = blockIdx.x * DT + threadIdx.x;
+    const bool active = bl < p.nbl;
+    int t1 = 0, t2 = 1;
+    if (active) baseline_to_tiles(bl, p.ntiles, t1, t2);
+    int fr[FCH];
+    double ool[FCH];
+#pragma unroll
+    for (int i = 0; i < FCH; i++) {
+        fr[i] = min(f0 + i, p.nf - 1);  // a missing last channel repeats the previous one and is not stored
+        ool[i] = p.freqs[fr[i]] / VEL_C;
+    }
+    double um = 0.0, vm = 0.0, wm = 0.0;
+    if (active) {
+        const UVW q = p.uvws[bl];
+        um = q.u, vm = q.v, wm = q.w;
+    }
+
+    const int nchunks = (p.nc + CH - 1) / CH;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+
+    auto issue = [&](int k) {
+        const int st = k & 1;
+        const int c0 = k * CH;
+        const int n = min(CH, p.nc - c0);
+        const uint32_t bytes = n * 32u + FCH * n * 64u + n * 32u;
+        mbar_arrive_expect_tx(&bar[st], bytes);
+        bulk_g2s(s_lmn[st], p.lmn + c0, n * 32u, &bar[st]);
+#pragma unroll
+        for (int i = 0; i < FCH; i++) bulk_g2s(s_flux[st][i], p.flux + (size_t)fr[i] * p.nc + c0, n * 64u, &bar[st]);
+        bulk_g2s(s_gp[st], p.gp + c0, n * 32u, &bar[st]);
+    };
+    if (threadIdx.x == 0) {
+        fence_proxy_async_smem();
+        if (nchunks > 0) issue(0);
+        if (nchunks > 1) issue(1);
+    }
+
+    J2 acc[FCH];
+#pragma unroll
+    for (int i = 0; i < FCH; i++) acc[i] = jzero();
+    for (int k = 0; k < nchunks; k++) {
+        const int st = k & 1;
+        const bool ok = mbar_wait_bounded(&bar[st], (k >> 1) & 1, p.err);
+        if (__syncthreads_or(!ok)) break;
+        const int c0 = k * CH;
+        const int n = min(CH, p.nc - c0);
+#pragma unroll
+        for (int i = 0; i < FCH; i++) {
+            const double* src = reinterpret_cast<const double*>(s_flux[st][i]);
+            for (int e = threadIdx.x; e < n * 8; e += DT) s_wf[i][e] = (float)src[e];
+        }
+        if (TYPE == 2 && p.sdense)
+            for (int e = threadIdx.x; e < n * SDN * SDN; e += DT) s_dense[e] = __ldg(p.sdense + (size_t)c0 * SDN * SDN + e);
+        __syncthreads();
+        if (active) {
+            float a[FCH][8];
+#pragma unroll
+            for (int i = 0; i < FCH; i++)
+#pragma unroll
+                for (int e = 0; e < 8; e++) a[i][e] = 0.f;
+            for (int c = 0; c < n; c++) {
+                const double4 lmn = s_lmn[st][c];
+                const double4 g = s_gp[st][c];
+                const double tm = um * lmn.x + vm * lmn.y + wm * lmn.z;  // metres
+                double exm = 0.0, xm = 0.0, ym = 0.0, su = 0.0, sv = 0.0;
+                if (TYPE == 1) {
+                    // the exponent in FP64 (an FP32 exponent's absolute error,
+                    // ~1e-7 of its size, would become the envelope's relative error)
+                    const double kx = um * g.z + vm * g.w;
+                    const double ky = um * g.w - vm * g.z;
+                    exm = g.x * (kx * kx) + g.y * (ky * ky);
+                } else {
+                    const double2 ta = __ldg(p.suv_tile + (size_t)(c0 + c) * p.ntiles + t1);
+                    const double2 tb = __ldg(p.suv_tile + (size_t)(c0 + c) * p.ntiles + t2);
+                    su = ta.x - tb.x;
+                    sv = ta.y - tb.y;
+                    xm = su * g.z + sv * g.w;
+                    ym = su * g.w - sv * g.z;
+                }
+#pragma unroll
+                for (int i = 0; i < FCH; i++) {
+                    float sn, cs;
+                    phasor_quarter_f32(4.0 * ool[i] * tm, sn, cs);
+                    float er, ei = 0.f;
+                    if (TYPE == 1) {
+                        const double ex = exm * (ool[i] * ool[i]);
+                        const float exh = (float)ex;
+                        er = expf(exh) * (1.f + (float)(ex - (double)exh));
+                    } else if (p.sdense) {
+                        shapelet_dense_at(p, s_dense + c * SDN * SDN, xm * (ool[i] * g.x) + SBF_C,
+                                          ym * (ool[i] * g.y) + SBF_C, er, ei);
+                    } else {
+                        shapelet_envelope_f32(p, c0 + c, g, su * ool[i], sv * ool[i], er, ei);
+                    }
+                    const float zr = cs * er - sn * ei, zi = fmaf(cs, ei, sn * er);
+                    const float* wv = s_wf[i] + c * 8;
+#pragma unroll
+                    for (int e = 0; e < 4; e++) {
+                        a[i][2 * e] += fmaf(wv[2 * e], zr, -wv[2 * e + 1] * zi);
+                        a[i][2 * e + 1] += fmaf(wv[2 * e], zi, wv[2 * e + 1] * zr);
+                    }
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < FCH; i++)
+                acc[i] = acc[i] + J2{{a[i][0], a[i][1]}, {a[i][2], a[i][3]}, {a[i][4], a[i][5]}, {a[i][6], a[i][7]}};
+        }
+        __syncthreads();
+        if (threadIdx.x == 0 && k + 2 < nchunks) {
+            fence_proxy_async_smem();
+            issue(k + 2);
+        }
+    }
+
+    if (!active) return;
+#pragma unroll
+    for (int i = 0; i < FCH; i++) {
+        if (f0 + i >= p.nf) break;
+        const size_t o = (size_t)(f0 + i) * p.nbl + bl;
+        if (OUT64) {
+            double2* q = reinterpret_cast<double2*>(reinterpret_cast<JonesF64*>(p.vis) + o);
+            double2 a0 = q[0], b0 = q[1], c1 = q[2], d0 = q[3];
+            q[0] = make_double2(a0.x + acc[i].a.re, a0.y + acc[i].a.im);
+            q[1] = make_double2(b0.x + acc[i].b.re, b0.y + acc[i].b.im);
+            q[2] = make_double2(c1.x + acc[i].c.re, c1.y + acc[i].c.im);
+            q[3] = make_double2(d0.x + acc[i].d.re, d0.y + acc[i].d.im);
+        } else {
+            float4* q = reinterpret_cast<float4*>(reinterpret_cast<JonesF32*>(p.vis) + o);
+            float4 x = q[0], y = q[1];
+            x.x += (float)acc[i].a.re;
+            x.y += (float)acc[i].a.im;
+            x.z += (float)acc[i].b.re;
+            x.w += (float)acc[i].b.im;
+            y.x += (float)acc[i].c.re;
+            y.y += (float)acc[i].c.im;
+            y.z += (float)acc[i].d.re;
+            y.w += (float)acc[i].d.im;
+            q[0] = x;
+            q[1] = y;
+        }
+    }
+}
+
 template <int TYPE>
 static cudaError_t launch_t(bool tile_beam, bool out64, bool fast, const DirectParams& p, cudaStream_t s) {
     dim3 grid((p.nbl + DT - 1) / DT, p.nf);
@@ -331,6 +502,12 @@ static cudaError_t launch_t(bool tile_beam, bool out64, bool fast, const DirectP
             direct_kernel<TYPE, true, true, false><<<grid, DT, 0, s>>>(p);
         else
             direct_kernel<TYPE, true, false, false><<<grid, DT, 0, s>>>(p);
+    } else if (fast && TYPE != 0) {
+        const dim3 fgrid((p.nbl + DT - 1) / DT, (p.nf + FCH - 1) / FCH);
+        if (out64)
+            fast_kernel<TYPE == 0 ? 1 : TYPE, true><<<fgrid, DT, 0, s>>>(p);
+        else
+            fast_kernel<TYPE == 0 ? 1 : TYPE, false><<<fgrid, DT, 0, s>>>(p);
     } else if (fast) {
         if (out64)
             direct_kernel<TYPE, false, true, true><<<grid, DT, 0, s>>>(p);
