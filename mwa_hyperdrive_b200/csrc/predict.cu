@@ -337,7 +337,7 @@ __global__ void __launch_bounds__(DT) direct_kernel(const DirectParams p) {
 constexpr int FCH = 2;
 
 template <int TYPE, bool OUT64>
-__global__ void __launch_bounds__(DT) fast_kernel(const DirectParams p) {
+__global__ void __launch_bounds__(DT, TYPE == 1 ? 3 : 2) fast_kernel(const DirectParams p) {
     __shared__ alignas(128) double4 s_lmn[2][CH];
     __shared__ alignas(128) JonesF64 s_flux[2][FCH][CH];
     __shared__ alignas(128) double4 s_gp[2][CH];
