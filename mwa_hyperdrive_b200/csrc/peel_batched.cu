@@ -23,7 +23,8 @@
 //   3. apply sweep: R += sum_s conj(rot_s) M_s (iono_s(old) - iono_s(new))
 //      (the reference's subtract_iono, rotated back).
 // With one source this is the reference's sequence exactly (up to rounding:
-// FP64 throughout instead of its f32 intermediates); with several, sources
+// FP64 arithmetic with FP32 phasors after an exact FP64 range reduction,
+// instead of its f32 intermediates); with several, sources
 // fitted in the same pass do not see each other's updates until the next
 // pass.  The source models M_s (high resolution, source frame) are predicted
 // once per timeblock by the modeller and reused by every pass.
@@ -70,10 +71,14 @@ struct SweepArgs {
     int nt, nf, nbl, nsrc, favg;
 };
 
+// exp(i arg): the argument (radians) in FP64, reduced exactly in quarter
+// turns, then the FP32 quarter-turn polynomials (< 1 ulp of FP32; the
+// residual is stored in FP32, so a per-term phasor error of ~1e-7 is at its
+// rounding level)
 __device__ __forceinline__ cplx phase(double arg) {
-    double s, c;
-    sincos(arg, &s, &c);
-    return cplx{c, s};
+    float sn, cs;
+    phasor_quarter_f32(arg * 0.63661977236758134308, sn, cs);  // 2 / pi
+    return cplx{(double)cs, (double)sn};
 }
 
 // iono factor g exp(-2 pi i (u alpha + v beta) lambda), as add_model / subtract_iono
@@ -88,11 +93,15 @@ __device__ __forceinline__ JonesF32 to_f32(const J2& v) {
 }
 
 // blockDim (BX, SY): x = low-resolution bins, y = sources of this CTA's chunk
+// Grid: one dimension, source groups fastest -- the CTAs of all source
+// groups of a bin block run close together, so each residual tile comes
+// from DRAM once and from L2 for the other sources.
 template <int BX, int SY>
 __global__ void __launch_bounds__(BX* SY) accumulate_kernel(const SweepArgs A) {
     const int nlo = A.nf / A.favg;
-    const int bin = blockIdx.x * BX + threadIdx.x;
-    const int src = blockIdx.y * SY + threadIdx.y;
+    const int ngrp = (A.nsrc + SY - 1) / SY;
+    const int bin = (int)(blockIdx.x / ngrp) * BX + threadIdx.x;
+    const int src = (int)(blockIdx.x % ngrp) * SY + threadIdx.y;
     if (bin >= nlo * A.nbl || src >= A.nsrc) return;
     const int bl = bin % A.nbl, flo = bin / A.nbl;
     const IonoConsts k = A.old[src];
@@ -151,7 +160,7 @@ struct Variant {
 template <int BX, int SY>
 void launch_acc(const SweepArgs& A, cudaStream_t s) {
     const int nbins = (A.nf / A.favg) * A.nbl;
-    const dim3 grid((nbins + BX - 1) / BX, (A.nsrc + SY - 1) / SY);
+    const unsigned grid = (unsigned)((nbins + BX - 1) / BX) * (unsigned)((A.nsrc + SY - 1) / SY);
     accumulate_kernel<BX, SY><<<grid, dim3(BX, SY), 0, s>>>(A);
     count_launches(1);
 }
