@@ -17,6 +17,7 @@
 // hour angle (components/mod.rs:279-298), the beam-weighted flux
 // W = B S B^H when a beam is set, then the per-type direct kernels.
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -441,27 +442,40 @@ void Modeller::prof_collect() {
     ev_pending.clear();
 }
 
+int Modeller::model_channels(double lst, void* d_vis, bool out64, int f0, int nfc, cudaStream_t s) {
+    EvPair e{};
+    const size_t vis_off = (size_t)f0 * nbl * (out64 ? sizeof(JonesF64) : sizeof(JonesF32));
+    void* vis = static_cast<char*>(d_vis) + vis_off;
+    for (int ty = 0; ty < 3; ty++) {
+        if (t[ty].nc == 0) continue;
+        prof_begin(ty, s, e);
+        if (ty == 0 && form == HDC_PREDICT_TENSOR) {
+            const int rc = launch_tensor_points(nfc, nbl, ntiles, t[0].nc, d_freqs + f0, d_xyzs, lst - pc.ra, pc.dec,
+                                                t[0].d_lmn, weights(0) + (size_t)f0 * t[0].nc, vis, out64, d_err, s);
+            if (rc) return rc;
+        } else {
+            // the chosen (tensor) form keeps Gaussians and shapelets in the
+            // direct kernel, in its FP32 form
+            DirectParams p = direct_params(ty, vis);
+            p.nf = nfc;
+            p.freqs = d_freqs + f0;
+            p.flux = p.flux + (size_t)f0 * p.nc;
+            HDC_CUDA_RET_INT(launch_direct(ty, false, out64, p, s, form == HDC_PREDICT_TENSOR));
+        }
+        prof_end(s, e);
+    }
+    if (!out64) HDC_CUDA_RET_INT(launch_mask_pols((JonesF32*)vis, (size_t)nfc * nbl, pols, s));
+    return HDC_OK;
+}
+
 int Modeller::model(double lst, void* d_vis, bool out64, UVW* h_uvws, cudaStream_t s) {
     EvPair e{};
     prof_begin(3, s, e);
     int rc = geometry(lst, s);
     if (rc) return rc;
     prof_end(s, e);
-    for (int ty = 0; ty < 3; ty++) {
-        if (t[ty].nc == 0) continue;
-        prof_begin(ty, s, e);
-        if (ty == 0 && form == HDC_PREDICT_TENSOR) {
-            rc = tensor_points(lst, d_vis, out64, s);
-            if (rc) return rc;
-        } else {
-            // the chosen (tensor) form keeps Gaussians and shapelets in the
-            // direct kernel, in its FP32 form
-            HDC_CUDA_RET_INT(launch_direct(ty, false, out64, direct_params(ty, d_vis), s,
-                                           form == HDC_PREDICT_TENSOR));
-        }
-        prof_end(s, e);
-    }
-    if (!out64) HDC_CUDA_RET_INT(launch_mask_pols((JonesF32*)d_vis, (size_t)nf * nbl, pols, s));
+    rc = model_channels(lst, d_vis, out64, 0, nf, s);
+    if (rc) return rc;
     if (h_uvws) {
         HDC_CUDA_RET_INT(cudaMemcpyAsync(h_uvws, d_uvws, sizeof(UVW) * nbl, cudaMemcpyDeviceToHost, s));
         HDC_CUDA_RET_INT(cudaStreamSynchronize(s));
@@ -499,6 +513,10 @@ int Modeller::autos(double lst, JonesF32* d_vis, cudaStream_t s) {
 }
 
 Modeller::~Modeller() {
+    for (int i = 0; i < 3; i++)
+        if (pipe_s[i]) cudaStreamDestroy(pipe_s[i]);
+    for (auto& ev : pipe_ev)
+        if (ev) cudaEventDestroy(ev);
     for (int ty = 0; ty < 3; ty++) t[ty].release();
     dfree(d_freqs);
     dfree(d_xyzs);
@@ -615,14 +633,49 @@ extern "C" int hdc_modeller_model_timestep_with_host(HdcModeller* hm, double lst
         HDC_CUDA_RET_INT(cudaMalloc(&m->d_host_vis, bytes));
         m->host_vis_bytes = bytes;
     }
-    HDC_CUDA_RET_INT(cudaMemcpyAsync(m->d_host_vis, h_vis, bytes, cudaMemcpyHostToDevice, s));
-    int rc = m->model(lst, m->d_host_vis, false, nullptr, s);
+    return m->model_host_pipelined(lst, h_vis, h_uvws, s);
+}
+
+namespace hdc {
+// Channel chunks: chunk c is uploaded on stream 0, predicted on stream 1
+// once uploaded, and downloaded on stream 2 once predicted, so the copies of
+// one chunk overlap the predict of its neighbours.  The caller's stream
+// orders the whole call (the first upload waits for it; it waits for the
+// last download), and the call returns with the host buffer updated.
+int Modeller::model_host_pipelined(double lst, JonesF32* h_vis, UVW* h_uvws, cudaStream_t s) {
+    if (!pipe_s[0]) {
+        for (int i = 0; i < 3; i++) HDC_CUDA_RET_INT(cudaStreamCreateWithFlags(&pipe_s[i], cudaStreamNonBlocking));
+        for (auto& ev : pipe_ev) HDC_CUDA_RET_INT(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    }
+    cudaEvent_t* up = pipe_ev;                      // chunk uploaded
+    cudaEvent_t* done = pipe_ev + PIPE_CHUNKS;      // chunk predicted
+    cudaEvent_t start = pipe_ev[2 * PIPE_CHUNKS];   // caller's stream reached the call
+    cudaEvent_t fin = pipe_ev[2 * PIPE_CHUNKS + 1]; // last download issued
+    HDC_CUDA_RET_INT(cudaEventRecord(start, s));
+    for (int i = 0; i < 3; i++) HDC_CUDA_RET_INT(cudaStreamWaitEvent(pipe_s[i], start, 0));
+    int rc = geometry(lst, pipe_s[1]);
     if (rc) return rc;
-    HDC_CUDA_RET_INT(cudaMemcpyAsync(h_vis, m->d_host_vis, bytes, cudaMemcpyDeviceToHost, s));
-    if (h_uvws) HDC_CUDA_RET_INT(cudaMemcpyAsync(h_uvws, m->d_uvws, sizeof(UVW) * m->nbl, cudaMemcpyDeviceToHost, s));
-    HDC_CUDA_RET_INT(cudaStreamSynchronize(s));
+    const int nch = std::min(PIPE_CHUNKS, nf);
+    for (int c = 0; c < nch; c++) {
+        const int f0 = (int)((long long)nf * c / nch), f1 = (int)((long long)nf * (c + 1) / nch);
+        const size_t off = (size_t)f0 * nbl, n = (size_t)(f1 - f0) * nbl * sizeof(JonesF32);
+        HDC_CUDA_RET_INT(cudaMemcpyAsync(d_host_vis + off, h_vis + off, n, cudaMemcpyHostToDevice, pipe_s[0]));
+        HDC_CUDA_RET_INT(cudaEventRecord(up[c], pipe_s[0]));
+        HDC_CUDA_RET_INT(cudaStreamWaitEvent(pipe_s[1], up[c], 0));
+        rc = model_channels(lst, d_host_vis, false, f0, f1 - f0, pipe_s[1]);
+        if (rc) return rc;
+        HDC_CUDA_RET_INT(cudaEventRecord(done[c], pipe_s[1]));
+        HDC_CUDA_RET_INT(cudaStreamWaitEvent(pipe_s[2], done[c], 0));
+        HDC_CUDA_RET_INT(cudaMemcpyAsync(h_vis + off, d_host_vis + off, n, cudaMemcpyDeviceToHost, pipe_s[2]));
+    }
+    if (h_uvws)
+        HDC_CUDA_RET_INT(cudaMemcpyAsync(h_uvws, d_uvws, sizeof(UVW) * nbl, cudaMemcpyDeviceToHost, pipe_s[2]));
+    HDC_CUDA_RET_INT(cudaEventRecord(fin, pipe_s[2]));
+    HDC_CUDA_RET_INT(cudaStreamWaitEvent(s, fin, 0));
+    HDC_CUDA_RET_INT(cudaStreamSynchronize(pipe_s[2]));
     return HDC_OK;
 }
+}  // namespace hdc
 
 extern "C" int hdc_modeller_update_with_a_source(HdcModeller* hm, const HdcSkyModel* source, RADec phase_centre) {
     Modeller* m = reinterpret_cast<Modeller*>(hm);

@@ -59,6 +59,15 @@ struct Modeller {
     const JonesF64* weights(int ty) const;
     DirectParams direct_params(int ty, void* vis) const;
     int model(double lst, void* d_vis, bool out64, UVW* h_uvws, cudaStream_t s);
+    // the predict kernels of channels [f0, f0 + nfc) after geometry(); d_vis
+    // is the whole [nf][nbl] visibility array
+    int model_channels(double lst, void* d_vis, bool out64, int f0, int nfc, cudaStream_t s);
+    // host-buffer predict: upload, predict and download of channel chunks
+    // overlap on three streams
+    static constexpr int PIPE_CHUNKS = 4;
+    cudaStream_t pipe_s[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t pipe_ev[2 * PIPE_CHUNKS + 2] = {};
+    int model_host_pipelined(double lst, JonesF32* h_vis, UVW* h_uvws, cudaStream_t s);
     // model_timestep_with over baseline UVWs the caller computed (as the
     // reference's peel loop passes its own d_uvws, model/gpu.rs:1152-1166);
     // direct FP64 kernels, JonesF32 output.
