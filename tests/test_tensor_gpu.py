@@ -138,7 +138,7 @@ def test_chosen_form_shapelets_dense_and_per_coefficient(oracle, max_order):
     assert nrm < TOL and p999 < TOL, (nrm, p999, mx)
 
 
-@pytest.mark.parametrize("ntiles,npts", [(64, 4500), (24, 16500)])
+@pytest.mark.parametrize("ntiles,npts", [(64, 4500), (24, 16500), (97, 3000)])
 def test_many_components(oracle, ntiles, npts):
     """Errors must not grow with the component count; 16500 components need
     two launches (16384 + 116) that accumulate in turn."""
