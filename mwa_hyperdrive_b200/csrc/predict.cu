@@ -436,9 +436,10 @@ __global__ void __launch_bounds__(DT, TYPE == 1 ? 3 : 2) fast_kernel(const Direc
                     phasor_quarter_f32(4.0 * ool[i] * tm, sn, cs);
                     float er, ei = 0.f;
                     if (TYPE == 1) {
-                        const double ex = exm * (ool[i] * ool[i]);
-                        const float exh = (float)ex;
-                        er = expf(exh) * (1.f + (float)(ex - (double)exh));
+                        // exponent in FP64, exp in FP32: rounding the exponent
+                        // to FP32 moves the envelope by |ex| 6e-8 e^-|ex| <= 2.2e-8
+                        // of the component's flux
+                        er = expf((float)(exm * (ool[i] * ool[i])));
                     } else if (p.sdense) {
                         shapelet_dense_at(p, s_dense + c * SDN * SDN, xm * (ool[i] * g.x) + SBF_C,
                                           ym * (ool[i] * g.y) + SBF_C, er, ei);
@@ -447,10 +448,11 @@ __global__ void __launch_bounds__(DT, TYPE == 1 ? 3 : 2) fast_kernel(const Direc
                     }
                     const float zr = cs * er - sn * ei, zi = fmaf(cs, ei, sn * er);
                     const float* wv = s_wf[i] + c * 8;
+                    // a += W z, two fused multiply-adds per real part
 #pragma unroll
                     for (int e = 0; e < 4; e++) {
-                        a[i][2 * e] += fmaf(wv[2 * e], zr, -wv[2 * e + 1] * zi);
-                        a[i][2 * e + 1] += fmaf(wv[2 * e], zi, wv[2 * e + 1] * zr);
+                        a[i][2 * e] = fmaf(-wv[2 * e + 1], zi, fmaf(wv[2 * e], zr, a[i][2 * e]));
+                        a[i][2 * e + 1] = fmaf(wv[2 * e + 1], zr, fmaf(wv[2 * e], zi, a[i][2 * e + 1]));
                     }
                 }
             }
