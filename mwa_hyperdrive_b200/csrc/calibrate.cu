@@ -219,8 +219,6 @@ __device__ __forceinline__ void collapsed_terms(const T* cv, size_t stride, cons
                                                 const Herm& H1, const Herm& H2, J2& t1, J2& t2, Herm& h1,
                                                 Herm& h2) {
     const cplx G1[4] = {g1.a, g1.b, g1.c, g1.d}, G2[4] = {g2.a, g2.b, g2.c, g2.d};
-    const cplx h1m[4] = {{H1.a, 0.0}, H1.b, conj(H1.b), {H1.d, 0.0}};
-    const cplx h2m[4] = {{H2.a, 0.0}, H2.b, conj(H2.b), {H2.d, 0.0}};
     cplx T1[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}}, T2[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
 #pragma unroll
     for (int u = 0; u < 4; u++)
@@ -234,25 +232,51 @@ __device__ __forceinline__ void collapsed_terms(const T* cv, size_t stride, cons
     t1 = J2{T1[0], T1[1], T1[2], T1[3]};
     t2 = J2{T2[0], T2[1], T2[2], T2[3]};
     // bot accumulators: entry (u, v) = C[2a+b][2c+d] feeds b1[2a+c] with
-    // H2[2b+d] and, read as C[2l+j][2k+i], b2[2i+j] with H1[2k+l]
-    cplx b1[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}}, b2[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
-    auto add = [&](int u, int v, cplx c) {
-        b1[(u >> 1) * 2 + (v >> 1)] = b1[(u >> 1) * 2 + (v >> 1)] + c * h2m[(u & 1) * 2 + (v & 1)];
-        b2[(v & 1) * 2 + (u & 1)] = b2[(v & 1) * 2 + (u & 1)] + c * h1m[(v >> 1) * 2 + (u >> 1)];
+    // H2[2b+d] and, read as C[2l+j][2k+i], b2[2i+j] with H1[2k+l].  The
+    // results are Hermitian, so only entries 00 and 11 (real parts) and 01
+    // are formed; every index below is a compile-time constant once the
+    // loops are unrolled, so the unused terms are never computed.
+    double b1_00 = 0.0, b1_11 = 0.0, b2_00 = 0.0, b2_11 = 0.0;
+    cplx b1_01{0.0, 0.0}, b2_01{0.0, 0.0};
+    // r += c h for target entry i (0, 1, 3; 2 is not kept) and entry k of the
+    // Hermitian H (0, 3 real; 1 = b; 2 = conj(b)); c real when creal
+    auto acc = [](double& r00, double& r11, cplx& r01, int i, cplx c, bool creal, int k, const Herm& H) {
+        if (i == 2) return;
+        if (k == 0 || k == 3) {
+            const double hr = k == 0 ? H.a : H.d;
+            if (i == 1) {
+                r01.re += c.re * hr;
+                if (!creal) r01.im += c.im * hr;
+            } else {
+                (i == 0 ? r00 : r11) += c.re * hr;
+            }
+        } else {
+            const cplx h = k == 1 ? H.b : conj(H.b);
+            if (i == 1) {
+                r01.re += creal ? c.re * h.re : c.re * h.re - c.im * h.im;
+                r01.im += creal ? c.re * h.im : c.re * h.im + c.im * h.re;
+            } else {
+                (i == 0 ? r00 : r11) += creal ? c.re * h.re : c.re * h.re - c.im * h.im;
+            }
+        }
+    };
+    auto add = [&](int u, int v, cplx c, bool creal) {
+        acc(b1_00, b1_11, b1_01, (u >> 1) * 2 + (v >> 1), c, creal, (u & 1) * 2 + (v & 1), H2);
+        acc(b2_00, b2_11, b2_01, (v & 1) * 2 + (u & 1), c, creal, (v >> 1) * 2 + (u >> 1), H1);
     };
 #pragma unroll
-    for (int u = 0; u < 4; u++) add(u, u, cplx{cov_ld<T, SMEM>(cv + (size_t)(32 + u) * stride), 0.0});
+    for (int u = 0; u < 4; u++) add(u, u, cplx{cov_ld<T, SMEM>(cv + (size_t)(32 + u) * stride), 0.0}, true);
 #pragma unroll
     for (int u = 0; u < 4; u++)
 #pragma unroll
         for (int v = u + 1; v < 4; v++) {
             const cplx c{cov_ld<T, SMEM>(cv + (size_t)(36 + 2 * cpair(u, v)) * stride),
                          cov_ld<T, SMEM>(cv + (size_t)(37 + 2 * cpair(u, v)) * stride)};
-            add(u, v, c);
-            add(v, u, conj(c));
+            add(u, v, c, false);
+            add(v, u, conj(c), false);
         }
-    h1 = Herm{b1[0].re, b1[3].re, b1[1]};
-    h2 = Herm{b2[0].re, b2[3].re, b2[1]};
+    h1 = Herm{b1_00, b1_11, b1_01};
+    h2 = Herm{b2_00, b2_11, b2_01};
 }
 
 // Threads per CTA of the iteration kernel: the FP32 collapsed form runs two

@@ -212,8 +212,10 @@ int take_device_error(cudaStream_t s);
 // Shapelet basis table on the current device (SBF_N x SBF_L doubles).
 const double* device_shapelet_basis();
 const float* device_shapelet_basis_f32();
-// FP32 (value, next - value) pairs of the table, SBF_N x SBF_L.
-const float2* device_shapelet_basis_pairs();
+// FP32 (value, next - value) pairs of the table's orders 0 .. SDN_TABLE - 1,
+// position-major: [SBF_L][SDN_TABLE / 2] float4 (one record per position).
+constexpr int SDN_TABLE = 6;
+const float4* device_shapelet_basis_pairs();
 void host_shapelet_basis(double* out);
 // Count of kernel launches made by libhdc (diagnostics).
 void count_launches(int n);

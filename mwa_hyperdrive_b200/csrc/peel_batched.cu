@@ -112,6 +112,7 @@ __global__ void __launch_bounds__(BX* SY) accumulate_kernel(const SweepArgs A) {
     for (int t = 0; t < A.nt; t++) {
         const UVW q = A.uv_src[((size_t)src * A.nt + t) * A.nbl + bl];
         const double dw = q.w - A.uv_pc[(size_t)t * A.nbl + bl].w;
+#pragma unroll 4  // several channels' loads in flight at once
         for (int fc = flo * A.favg; fc < flo * A.favg + A.favg; fc++) {
             const size_t i = ((size_t)t * A.nf + fc) * A.nbl + bl;
             const double wt = A.w[i];

@@ -102,13 +102,16 @@ __device__ __forceinline__ void shapelet_dense_at(const DirectParams& p, const f
     const int xi = fx > 0.0 ? (int)fmin(fx, (double)(SBF_L - 2)) : 0;
     const int yi = fy > 0.0 ? (int)fmin(fy, (double)(SBF_L - 2)) : 0;
     const float xfrac = (float)(x_pos - fx), yfrac = (float)(y_pos - fy);
+    // one 48-byte record per position holds all orders' pairs
     float X[SDN], Y[SDN];
 #pragma unroll
-    for (int n = 0; n < SDN; n++) {
-        const float2 a = __ldg(p.sbfp + (size_t)SBF_L * n + xi);
-        const float2 b = __ldg(p.sbfp + (size_t)SBF_L * n + yi);
-        X[n] = fmaf(a.y, xfrac, a.x);
-        Y[n] = fmaf(b.y, yfrac, b.x);
+    for (int h = 0; h < SDN / 2; h++) {
+        const float4 a = __ldg(p.sbfp + (size_t)xi * (SDN / 2) + h);
+        const float4 b = __ldg(p.sbfp + (size_t)yi * (SDN / 2) + h);
+        X[2 * h] = fmaf(a.y, xfrac, a.x);
+        X[2 * h + 1] = fmaf(a.w, xfrac, a.z);
+        Y[2 * h] = fmaf(b.y, yfrac, b.x);
+        Y[2 * h + 1] = fmaf(b.w, yfrac, b.z);
     }
     float re = 0.f, im = 0.f;
 #pragma unroll
@@ -337,7 +340,7 @@ __global__ void __launch_bounds__(DT) direct_kernel(const DirectParams p) {
 constexpr int FCH = 2;
 
 template <int TYPE, bool OUT64>
-__global__ void __launch_bounds__(DT, TYPE == 1 ? 3 : 2) fast_kernel(const DirectParams p) {
+__global__ void __launch_bounds__(DT, 3) fast_kernel(const DirectParams p) {
     __shared__ alignas(128) double4 s_lmn[2][CH];
     __shared__ alignas(128) JonesF64 s_flux[2][FCH][CH];
     __shared__ alignas(128) double4 s_gp[2][CH];

@@ -10,7 +10,7 @@ namespace hdc {
 // is the modelling order; for the drop-in layer it is power laws, curved
 // power laws, lists (gpu/types.h:187-267), which is also the beam-direction
 // order of d_beam_jones.
-constexpr int SDN = 6;  // orders 0..5 in the dense shapelet form
+constexpr int SDN = SDN_TABLE;  // orders 0..5 in the dense shapelet form
 
 struct DirectParams {
     int nbl, nf, ntiles, nc;
@@ -29,10 +29,10 @@ struct DirectParams {
     const double* sbf;  // [SBF_N][SBF_L]
     const float* sbf32; // the same table in FP32 (chosen form), or NULL
     // chosen form, orders below SDN: the table as FP32 (value, next - value)
-    // pairs [SBF_N][SBF_L] and per component a dense SDN x SDN coefficient
+    // pairs, position-major [SBF_L][SDN / 2] float4, and per component a dense SDN x SDN coefficient
     // matrix [nc][n1][n2] with the sign of i^(n1+n2) folded in; NULL when
     // some coefficient's order is SDN or more
-    const float2* sbfp;
+    const float4* sbfp;
     const float* sdense;
     const ShapeletCoeff* coeffs;
     const int* coeff_start;
