@@ -320,6 +320,21 @@ typedef struct HdcSkyModel {
 #define HDC_BEAM_NONE 0          /* identity Jones (beam/mod.rs:255-388 NoBeam) */
 #define HDC_BEAM_ANALYTIC_DIPOLE 1 /* 4x4 dipole tile over a ground plane, shared by all tiles */
 
+/* Veto brightness of every source of a source list (srclist/veto.rs:58-129),
+ * on the device: per coarse frequency h_freqs [Hz], the sum over a source's
+ * components of the beam-attenuated flux density |(J I J^H)_XX| +
+ * |(J I J^H)_YY| (I the component's instrumental flux at that frequency, J
+ * the beam response at its Az/El for lst_rad and latitude_rad; beam_kind
+ * HDC_BEAM_NONE or HDC_BEAM_ANALYTIC_DIPOLE).  h_brightness[s] is the
+ * smallest of those sums over the frequencies, or -1 when one of the
+ * source's components lies below min_elevation_rad or farther than
+ * source_dist_cutoff_rad from the phase centre.  h_comp_source[c] is the
+ * source index of component c of sky.  The caller sorts, thresholds and
+ * keeps the top N as veto_sources does (Python: srclist_io.veto_sources). */
+int hdc_source_brightness(const HdcSkyModel *sky, const int *h_comp_source, int num_sources, const double *h_freqs,
+                          int num_freqs, double lst_rad, double latitude_rad, RADec phase_centre, int beam_kind,
+                          double source_dist_cutoff_rad, double min_elevation_rad, double *h_brightness);
+
 /* Precision form of the point-source predict. */
 #define HDC_PREDICT_DIRECT 0     /* FP64 direct per-baseline kernel (the plain form) */
 #define HDC_PREDICT_TENSOR 1     /* factored tcgen05 contraction (points only) */

@@ -154,6 +154,8 @@ SIGNATURES = {
     "hdc_modeller_set_profiling": (c_int, [c_void_p, c_int]),
     "hdc_modeller_profile": (c_int, [c_void_p, c_void_p, c_int]),
     "hdc_probe_fp64_gflops": (c_int, [ctypes.POINTER(c_double)]),
+    "hdc_source_brightness": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_int, c_double, c_double, RADec, c_int,
+                                      c_double, c_double, c_void_p]),
     "hdc_probe_fp32_gflops": (c_int, [ctypes.POINTER(c_double)]),
 }
 

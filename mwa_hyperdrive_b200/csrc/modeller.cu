@@ -534,6 +534,141 @@ Modeller::~Modeller() {
 
 using hdc::Modeller;
 
+namespace hdc {
+// Per (component, coarse frequency): the veto's tests and brightness
+// (srclist/veto.rs:58-129).  A component below the elevation limit or
+// farther than the cutoff from the phase centre marks its source vetoed;
+// otherwise its beam-attenuated flux |(J I J^H)_XX| + |(J I J^H)_YY| (I the
+// instrumental flux, J the beam; veto.rs:193-207) is added to its source's
+// total at that frequency.
+__global__ void veto_kernel(const double2* radec, const int* comp_source, int nc, const double* freqs, int nf,
+                            double lst, double lat, double pc_ra, double pc_dec, int beam_kind, double cutoff,
+                            double min_el, const JonesF64* S, double* src_fd, int* src_vetoed) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int f = blockIdx.y;
+    if (c >= nc) return;
+    const double2 rd = radec[c];
+    const int src = comp_source[c];
+    double az, el;
+    hadec_to_azel(lst - rd.x, rd.y, lat, az, el);
+    // angular separation from the phase centre (haversine)
+    const double sd = sin(0.5 * (rd.y - pc_dec)), sr = sin(0.5 * (rd.x - pc_ra));
+    const double hav = sd * sd + cos(rd.y) * cos(pc_dec) * sr * sr;
+    const double sep = 2.0 * asin(sqrt(fmin(1.0, fmax(0.0, hav))));
+    if (el < min_el || sep > cutoff) {
+        if (f == 0) atomicOr(src_vetoed + src, 1);
+        return;
+    }
+    J2 s = load_j(S[(size_t)f * nc + c]);
+    if (beam_kind == HDC_BEAM_ANALYTIC_DIPOLE) {
+        const J2 b = analytic_beam(az, el, freqs[f]);
+        s = b * (s * herm(b));
+    }
+    atomicAdd(src_fd + (size_t)src * nf + f, hypot(s.a.re, s.a.im) + hypot(s.d.re, s.d.im));
+}
+}  // namespace hdc
+
+extern "C" int hdc_source_brightness(const HdcSkyModel* sky, const int* h_comp_source, int num_sources,
+                                     const double* h_freqs, int num_freqs, double lst_rad, double latitude_rad,
+                                     RADec phase_centre, int beam_kind, double source_dist_cutoff_rad,
+                                     double min_elevation_rad, double* h_brightness) {
+    using namespace hdc;
+    if (!sky || !h_comp_source || !h_freqs || !h_brightness || num_sources < 1 || num_freqs < 1 ||
+        (beam_kind != HDC_BEAM_NONE && beam_kind != HDC_BEAM_ANALYTIC_DIPOLE)) {
+        set_error("hdc_source_brightness: invalid arguments");
+        return HDC_ERR_ARG;
+    }
+    const int nc = sky->num_components, nf = num_freqs;
+    for (int c = 0; c < nc; c++)
+        if (h_comp_source[c] < 0 || h_comp_source[c] >= num_sources) {
+            set_error("hdc_source_brightness: component %d names source %d of %d", c, h_comp_source[c], num_sources);
+            return HDC_ERR_ARG;
+        }
+    // instrumental flux per (frequency, component): lists on the host, power
+    // laws on the device, as the modeller tabulates them
+    std::vector<JonesF64> S((size_t)nf * std::max(nc, 1));
+    std::vector<FluxComp> fc(std::max(nc, 1));
+    std::vector<double2> radec(std::max(nc, 1));
+    for (int c = 0; c < nc; c++) {
+        const int ft = sky->flux_type[c];
+        if (ft < 0 || ft > 2 || sky->fd_count[c] < 1) {
+            set_error("hdc_source_brightness: component %d has an invalid flux model", c);
+            return HDC_ERR_ARG;
+        }
+        radec[c] = make_double2(sky->ra[c], sky->dec[c]);
+        FluxComp f = {};
+        f.flux_type = ft;
+        if (ft == HDC_FLUX_LIST) {
+            for (int fi = 0; fi < nf; fi++) S[(size_t)fi * nc + c] = inst_stokes(estimate_list(sky, c, h_freqs[fi]));
+        } else {
+            const Stokes r = fd_entry(sky, sky->fd_start[c]);
+            f.freq = r.freq;
+            f.i = r.i;
+            f.q = r.q;
+            f.u = r.u;
+            f.v = r.v;
+            f.si = sky->si[c];
+            f.cq = (ft == HDC_FLUX_CURVED_POWER_LAW) ? sky->q[c] : 0.0;
+        }
+        fc[c] = f;
+    }
+    std::vector<double> fd((size_t)num_sources * nf, 0.0);
+    std::vector<int> vetoed(num_sources, 0);
+    if (nc > 0) {
+        JonesF64* d_S = nullptr;
+        FluxComp* d_fc = nullptr;
+        double2* d_radec = nullptr;
+        int *d_src = nullptr, *d_vet = nullptr;
+        double *d_freqs = nullptr, *d_fd = nullptr;
+        auto release = [&]() {
+            dfree(d_S);
+            dfree(d_fc);
+            dfree(d_radec);
+            dfree(d_src);
+            dfree(d_vet);
+            dfree(d_freqs);
+            dfree(d_fd);
+        };
+        cudaError_t e = dalloc(&d_S, S.size());
+        if (e == cudaSuccess) e = dalloc(&d_fc, (size_t)nc);
+        if (e == cudaSuccess) e = dalloc(&d_radec, (size_t)nc);
+        if (e == cudaSuccess) e = dalloc(&d_src, (size_t)nc);
+        if (e == cudaSuccess) e = dalloc(&d_vet, (size_t)num_sources);
+        if (e == cudaSuccess) e = dalloc(&d_freqs, (size_t)nf);
+        if (e == cudaSuccess) e = dalloc(&d_fd, fd.size());
+        if (e == cudaSuccess) e = cudaMemcpy(d_S, S.data(), sizeof(JonesF64) * S.size(), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(d_fc, fc.data(), sizeof(FluxComp) * nc, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(d_radec, radec.data(), sizeof(double2) * nc, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(d_src, h_comp_source, sizeof(int) * nc, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(d_freqs, h_freqs, sizeof(double) * nf, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemset(d_vet, 0, sizeof(int) * num_sources);
+        if (e == cudaSuccess) e = cudaMemset(d_fd, 0, sizeof(double) * fd.size());
+        if (e == cudaSuccess) {
+            const dim3 g((nc + 127) / 128, nf);
+            flux_kernel<<<g, 128>>>(d_fc, nc, d_freqs, nf, d_S);
+            veto_kernel<<<g, 128>>>(d_radec, d_src, nc, d_freqs, nf, lst_rad, latitude_rad, phase_centre.ra,
+                                    phase_centre.dec, beam_kind, source_dist_cutoff_rad, min_elevation_rad, d_S,
+                                    d_fd, d_vet);
+            count_launches(2);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaMemcpy(fd.data(), d_fd, sizeof(double) * fd.size(), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(vetoed.data(), d_vet, sizeof(int) * num_sources, cudaMemcpyDeviceToHost);
+        release();
+        if (e != cudaSuccess) {
+            set_error("hdc_source_brightness: %s", cudaGetErrorString(e));
+            return HDC_ERR_CUDA;
+        }
+    }
+    for (int s = 0; s < num_sources; s++) {
+        double m = INFINITY;
+        for (int f = 0; f < nf; f++) m = std::min(m, fd[(size_t)s * nf + f]);
+        h_brightness[s] = vetoed[s] ? -1.0 : m;
+    }
+    return HDC_OK;
+}
+
 extern "C" int hdc_modeller_new(const HdcSkyModel* sky, int pols, const XYZ* h_xyzs, int num_tiles,
                                 const double* h_freqs, int num_freqs, RADec phase_centre, double array_latitude_rad,
                                 int beam_kind, int predict_form, HdcModeller** out) {

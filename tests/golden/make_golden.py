@@ -10,6 +10,8 @@ test time.
   power-law and curved-power-law cases (lines 351-444, 600-731, 887-1018), the
   two-component Gaussian and shapelet cases (1393-1569) and the shapelet UVWs
   (1530-1568).  Values are parsed from the Rust source text.
+* srclist_files.json -- the reference's hyperdrive-format source-list test
+  files (YAML and JSON) with their source and component counts.
 * shapelet_basis_samples.json -- samples of the shapelet basis table produced
   by the reference's generator script src/model/make_shapelet_basis_values.py
   (imported, its gen_shape_basis evaluated at the sampled points), plus the
@@ -122,6 +124,24 @@ def main(ref_root: str) -> None:
         )
     )
     del spec
+
+    # Source-list file-format vectors: the reference's hyperdrive YAML and JSON
+    # test lists (whose text its write tests reproduce from an in-code list,
+    # src/srclist/general_tests.rs:711-779) and the all-kinds list
+    # (general_tests.rs:369-385: 9 sources survive a write/read round trip),
+    # with their contents as a YAML-independent reader sees them.
+    import yaml
+
+    tf = ref / "test_files"
+    lists = {}
+    for name in ["hyperdrive_srclist.yaml", "hyperdrive_srclist.json", "srclist_all_kinds.yaml"]:
+        text = (tf / name).read_text()
+        parsed = json.loads(text) if name.endswith(".json") else yaml.safe_load(text)
+        lists[name] = {"text": text, "num_sources": len(parsed),
+                       "num_components": sum(len(v) for v in parsed.values())}
+    (HERE / "srclist_files.json").write_text(
+        json.dumps({"source": "test_files/{hyperdrive_srclist.yaml,hyperdrive_srclist.json,srclist_all_kinds.yaml}",
+                    "lists": lists}, indent=1))
 
 
 if __name__ == "__main__":
