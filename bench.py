@@ -12,6 +12,11 @@ same metric through the trait-style C-ABI call with host buffers (H2D of the
 accumulated visibilities and D2H of the result inside the timed region).
 Multi-GPU runs are independent replicas (the predict shards by timestep and
 channel with no exchange), so scaling is weak.
+
+Rank 0 of a 1-GPU run adds sections measured the same way: `dical` (DI
+calibration, all solver forms), `peel` (sequential and batched peeling),
+`warmstart` (learned warm start against identity starts) and `prep`
+(vis_average and scale_by_weights against the HBM copy bandwidth).
 """
 
 from __future__ import annotations
@@ -55,6 +60,8 @@ def parse():
     ap.add_argument("--warm-chanblocks", type=int, default=768, help="reduced warm-start case for profiling")
     ap.add_argument("--skip-warmstart", action="store_true", help="leave out the warm-start measurement")
     ap.add_argument("--peel-channels", type=int, default=384, help="reduced peel case for profiling")
+    ap.add_argument("--skip-prep", action="store_true", help="leave out the visibility-preparation measurement")
+    ap.add_argument("--prep-timesteps", type=int, default=8, help="reduced visibility-preparation case for profiling")
     args = ap.parse_args()
     global SHAPE
     SHAPE = (args.channels, args.timesteps)
@@ -515,6 +522,73 @@ def warmstart_arm(args):
     return out
 
 
+# ----------------------------------------------- visibility preparation
+PREP_WORKLOAD = ("visibility preparation before DI calibration: vis_average of one timeblock of 8 timesteps x 1536 "
+                 "channels of 20 kHz x 8128 baselines (128 tiles) into 744 chanblocks of 40 kHz (24 coarse-channel "
+                 "centre chanblocks flagged), then scale_by_weights of data and model of 8 timesteps x 744 "
+                 "chanblocks x 8128 baselines with per-baseline weights; 15 % of weights <= 0")
+
+
+def prep_arm(args):
+    import torch
+
+    from mwa_hyperdrive_b200 import calibrate as C
+
+    nt, nf, nbl, nout = args.prep_timesteps, 1536, 8128, 744
+    flagged = list(range(16, 768, 32))
+    g = torch.Generator(device="cuda").manual_seed(11)
+    vis = torch.randn((nt, nf, nbl, 8), generator=g, device="cuda")
+    w = torch.rand((nt, nf, nbl), generator=g, device="cuda") * 20.0 - 3.0
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    out = {"workload": PREP_WORKLOAD, "unit": "GB/s"}
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+
+    def timed(fn, reps=5):
+        fn()
+        best = float("inf")
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            ev[0].record()
+            fn()
+            ev[1].record()
+            torch.cuda.synchronize()
+            best = min(best, ev[0].elapsed_time(ev[1]) * 1e-3)
+        return best
+
+    # inputs (3.6 GB) exceed L2; each call reads them once
+    t_avg = timed(lambda: C.vis_average(vis, w, nout, flagged))
+    bytes_avg = nt * nout * 2 * nbl * 36 + nout * nbl * 36  # used channels read once, outputs written once
+    out["vis_average"] = {"s": t_avg, "algorithmic_bytes": bytes_avg, "achieved_gbs": bytes_avg / t_avg / 1e9,
+                          "peak_gbs": hbm, "frac": bytes_avg / t_avg / 1e9 / hbm}
+    del vis, w
+    torch.cuda.empty_cache()
+    d = torch.randn((nt, nout, nbl, 8), generator=g, device="cuda")
+    m = torch.randn((nt, nout, nbl, 8), generator=g, device="cuda")
+    wt = torch.rand((nt, nout, nbl), generator=g, device="cuda") * 20.0 - 3.0
+    bw = np.linspace(0.0, 1.0, nbl)
+    t_sc = timed(lambda: C.scale_by_weights(d, m, wt, bw))
+    bytes_sc = nt * nout * nbl * (2 * 32 * 2 + 4) + nbl * 8
+    out["scale_by_weights"] = {"s": t_sc, "algorithmic_bytes": bytes_sc, "achieved_gbs": bytes_sc / t_sc / 1e9,
+                               "peak_gbs": hbm, "frac": bytes_sc / t_sc / 1e9 / hbm}
+    out["peak_source"] = "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650 GB/s"
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+
+        O.build()
+        rng = np.random.default_rng(2)
+        sb = 1016  # a 1/8 sample of the baselines
+        hv = rng.normal(size=(nt, nf, sb, 8)).astype(np.float32)
+        hw = (rng.uniform(size=(nt, nf, sb)) * 20.0 - 3.0).astype(np.float32)
+        t0 = time.perf_counter()
+        O.vis_average(hv, hw, nout, flagged)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": dt * nbl / sb, "unit": "s per vis_average", "cores": 1, "kind": "port",
+                               "sample": f"{sb} of {nbl} baselines, scaled by {nbl / sb:.1f}"}
+        out["vis_average"]["speedup_vs_cpu"] = out["cpu_baseline"]["value"] / t_avg
+    return out
+
+
 def guarded(fn, args):
     """Run an optional bench section; a failure is reported in the line."""
     try:
@@ -689,7 +763,7 @@ def gpu_arm(args, rank, world, local_rank):
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(obs, sky, args.cpu_seconds)
-        if not (args.skip_dical and args.skip_peel and args.skip_warmstart):
+        if not (args.skip_dical and args.skip_peel and args.skip_warmstart and args.skip_prep):
             del vis, flush
             torch.cuda.empty_cache()
         if not args.skip_dical:
@@ -700,6 +774,9 @@ def gpu_arm(args, rank, world, local_rank):
             torch.cuda.empty_cache()
         if not args.skip_warmstart:
             line["warmstart"] = guarded(warmstart_arm, args)
+            torch.cuda.empty_cache()
+        if not args.skip_prep:
+            line["prep"] = guarded(prep_arm, args)
         print(json.dumps(line), flush=True)
     plain.close()
     if chosen is not plain:

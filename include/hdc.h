@@ -537,6 +537,32 @@ int hdc_peel_timeblock_batched(JonesF32 *d_resid_tfb, const float *d_weights_tfb
  * its measured time. */
 int hdc_peel_batched_tuning(int *block_bins, int *block_sources, float *ms);
 
+/* ---- Visibility preparation before DI calibration ---------------------- */
+
+/* CalVis::scale_by_weights (params/di_calibration.rs:578-625), in place on
+ * the device: data and model [timestep][chanblock][baseline] are multiplied
+ * by f64(weight) x d_baseline_weights[baseline] (NULL: 1) in FP64 and stored
+ * back as FP32; where that product is <= 0 both become 0 (flagged). */
+int hdc_scale_by_weights(JonesF32 *d_data_tfb, JonesF32 *d_model_tfb, const float *d_weights_tfb,
+                         int num_timesteps, int num_chanblocks, int num_baselines, const double *d_baseline_weights,
+                         hdcStream_t stream);
+
+/* vis_average (averaging/mod.rs:537-600) on the device: all num_timesteps of
+ * d_from_tfb / d_weights_from_tfb [timestep][freq][baseline] averaged into
+ * d_to_fb / d_weights_to_fb [chanblock][baseline].  The channels split into
+ * num_chanblocks + num_flagged chunks of ceil(num_freqs / (num_chanblocks +
+ * num_flagged)) channels; chunks listed in h_flagged_chanblocks are skipped
+ * and the others fill the outputs in order.  Each output is the FP64
+ * weight-weighted mean of its samples with weight > 0 and their weight sum,
+ * or, where no weight is > 0, the plain mean and minus the sum of |weight|
+ * (vis_average_weights_non_zero, averaging/mod.rs:606-648); results are the
+ * reference's bit for bit.  At most 8000 flagged of at most 65536 chunks
+ * (the reference's u16 chanblock indices); h_flagged_chanblocks in any
+ * order.  Asynchronous on stream; allocates nothing. */
+int hdc_vis_average(const JonesF32 *d_from_tfb, const float *d_weights_from_tfb, int num_timesteps, int num_freqs,
+                    int num_baselines, const int *h_flagged_chanblocks, int num_flagged, JonesF32 *d_to_fb,
+                    float *d_weights_to_fb, int num_chanblocks, hdcStream_t stream);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

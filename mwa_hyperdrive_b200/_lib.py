@@ -157,6 +157,9 @@ SIGNATURES = {
     "hdc_source_brightness": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_int, c_double, c_double, RADec, c_int,
                                       c_double, c_double, c_void_p]),
     "hdc_probe_fp32_gflops": (c_int, [ctypes.POINTER(c_double)]),
+    "hdc_scale_by_weights": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_void_p, c_void_p]),
+    "hdc_vis_average": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_void_p, c_int, c_void_p, c_void_p, c_int,
+                                c_void_p]),
 }
 
 # Symbols exported for tests/tools that include/hdc.h does not declare.

@@ -1288,4 +1288,72 @@ void or_weights_rts(const double* tile_uvs, int nt, int ntiles, const double* la
     }
 }
 
+// params/di_calibration.rs:578-625 (CalVis::scale_by_weights): data and model
+// [t][f][bl] times f64(weight) * baseline weight (cycled over baselines),
+// stored back as FP32; a product <= 0 zeroes both.
+int or_scale_by_weights(float* data, float* model, const float* weights, int nt, int nf, int nbl,
+                        const double* bl_weights) {
+    const size_t n = (size_t)nt * nf * nbl;
+    for (size_t i = 0; i < n; i++) {
+        const double w = (double)weights[i] * (bl_weights ? bl_weights[i % nbl] : 1.0);
+        if (w <= 0.0) {
+            for (int k = 0; k < 8; k++) data[8 * i + k] = model[8 * i + k] = 0.0f;
+        } else {
+            to_f32(jscale(from_f32(data + 8 * i), w), data + 8 * i);
+            to_f32(jscale(from_f32(model + 8 * i), w), model + 8 * i);
+        }
+    }
+    return 0;
+}
+
+// averaging/mod.rs:537-600 (vis_average) and 606-648
+// (vis_average_weights_non_zero): all nt timesteps into one; channel chunks
+// of ceil(nf / (nout + nflag)) channels with the flagged chunk indices
+// skipped; per output the FP64 sums in (t, f) order.
+int or_vis_average(const float* from, const float* wfrom, int nt, int nf, int nbl, const int* flagged, int nflag,
+                   float* to, float* wto, int nout) {
+    const int nchunks = nout + nflag;
+    const int avg_freq = (int)std::ceil((double)nf / (double)nchunks);
+    int o = 0;
+    for (int c = 0; c < nchunks && o < nout; c++) {
+        bool skip = false;
+        for (int k = 0; k < nflag; k++) skip |= flagged[k] == c;
+        if (skip) continue;
+        const int f0 = c * avg_freq, f1 = std::min(f0 + avg_freq, nf);
+        for (int b = 0; b < nbl; b++) {
+            J64 ws = jzero(), s = jzero();
+            double wsum = 0.0, fsum = 0.0;
+            bool all_flagged = true;
+            for (int t = 0; t < nt; t++)
+                for (int f = f0; f < f1; f++) {
+                    const size_t i = ((size_t)t * nf + f) * nbl + b;
+                    const J64 v = from_f32(from + 8 * i);
+                    s = jadd(s, v);
+                    const double wa = std::fabs((double)wfrom[i]);
+                    if (wfrom[i] > 0.0f) {
+                        all_flagged = false;
+                        ws = jadd(ws, jscale(v, wa));
+                        wsum += wa;
+                    } else {
+                        fsum += wa;
+                    }
+                }
+            J64 r;
+            float wr;
+            if (all_flagged || wsum <= 0.0) {
+                const double len = (double)nt * (f1 - f0);
+                for (int k = 0; k < 4; k++) r.j[k] = {s.j[k].re / len, s.j[k].im / len};
+                wr = (float)-fsum;
+            } else {
+                for (int k = 0; k < 4; k++) r.j[k] = {ws.j[k].re / wsum, ws.j[k].im / wsum};
+                wr = (float)wsum;
+            }
+            to_f32(r, to + 8 * ((size_t)o * nbl + b));
+            wto[(size_t)o * nbl + b] = wr;
+        }
+        o++;
+    }
+    return o == nout ? 0 : 1;
+}
+
 }  // extern "C"

@@ -304,6 +304,35 @@ def average(hi, w, favg):
     return lo
 
 
+def scale_by_weights(data, model, weights, baseline_weights=None):
+    """CalVis::scale_by_weights on [t][f][bl][8] FP32 arrays (returns copies)."""
+    data = np.array(data, np.float32, order="C", copy=True)
+    model = np.array(model, np.float32, order="C", copy=True)
+    weights = np.ascontiguousarray(weights, np.float32)
+    nt, nf, nbl = weights.shape
+    blw = None if baseline_weights is None else np.ascontiguousarray(baseline_weights, np.float64)
+    lib().or_scale_by_weights(_ptr(data), _ptr(model), _ptr(weights), ctypes.c_int(nt), ctypes.c_int(nf),
+                              ctypes.c_int(nbl), _ptr(blw) if blw is not None else None)
+    return data, model
+
+
+def vis_average(vis, weights, num_chanblocks, flagged=()):
+    """vis_average over one time chunk: [t][f][bl][8] -> [chanblock][bl][8]
+    and weights [chanblock][bl]."""
+    vis = np.ascontiguousarray(vis, np.float32)
+    weights = np.ascontiguousarray(weights, np.float32)
+    nt, nf, nbl = weights.shape
+    fl = np.ascontiguousarray(sorted(flagged), np.int32)
+    to = np.zeros((num_chanblocks, nbl, 8), np.float32)
+    wto = np.zeros((num_chanblocks, nbl), np.float32)
+    rc = lib().or_vis_average(_ptr(vis), _ptr(weights), ctypes.c_int(nt), ctypes.c_int(nf), ctypes.c_int(nbl),
+                              _ptr(fl) if fl.size else None, ctypes.c_int(fl.size), _ptr(to), _ptr(wto),
+                              ctypes.c_int(num_chanblocks))
+    if rc:
+        raise ValueError("vis_average: the channels do not make that many chunks")
+    return to, wto
+
+
 def iono_loop(resid, weights, model, consts, niter, uvws, lambdas, convergence):
     resid = np.ascontiguousarray(resid, np.float32)
     weights = np.ascontiguousarray(weights, np.float32)
