@@ -563,6 +563,19 @@ int hdc_vis_average(const JonesF32 *d_from_tfb, const float *d_weights_from_tfb,
                     int num_baselines, const int *h_flagged_chanblocks, int num_flagged, JonesF32 *d_to_fb,
                     float *d_weights_to_fb, int num_chanblocks, hdcStream_t stream);
 
+/* into_cal_sols (di_calibrate/mod.rs:89-176) on the device: the solver's
+ * model->data gains d_di_jones [timeblock][unflagged tile][unflagged
+ * chanblock] become the data->model solutions d_out [timeblock][tile]
+ * [chanblock] of all num_unflagged + num_flagged tiles and chanblocks: each
+ * Jones matrix inverted (marlu Jones::inv; for pols XX or YY only that
+ * entry, inverted as a complex number, the others 0), NaN for flagged tiles
+ * and chanblocks.  Flag lists in any order, at most 1024 tiles and 8000
+ * chanblocks.  Asynchronous on stream; allocates nothing. */
+int hdc_into_cal_sols(const JonesF64 *d_di_jones, int num_timeblocks, int num_unflagged_tiles,
+                      int num_unflagged_chanblocks, const int *h_flagged_tiles, int num_flagged_tiles,
+                      const int *h_flagged_chanblocks, int num_flagged_chanblocks, int pols, JonesF64 *d_out,
+                      hdcStream_t stream);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

@@ -158,6 +158,8 @@ SIGNATURES = {
                                       c_double, c_double, c_void_p]),
     "hdc_probe_fp32_gflops": (c_int, [ctypes.POINTER(c_double)]),
     "hdc_scale_by_weights": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_void_p, c_void_p]),
+    "hdc_into_cal_sols": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_int, c_void_p, c_int, c_int, c_void_p,
+                                  c_void_p]),
     "hdc_vis_average": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_void_p, c_int, c_void_p, c_void_p, c_int,
                                 c_void_p]),
 }

@@ -15,10 +15,10 @@
 // Both stream their inputs once (HBM-bound); sums run in the reference's order (time outer, channel
 // inner) so the FP32 results are the reference's bit for bit.
 
-#include <algorithm>
 #include <vector>
 
 #include "common.cuh"
+#include "flagtable.cuh"
 
 namespace hdc {
 namespace vp {
@@ -44,15 +44,9 @@ __global__ void scale_kernel(JonesF32* __restrict__ data, JonesF32* __restrict__
     d[0] = sc(d0), d[1] = sc(d1), m[0] = sc(m0), m[1] = sc(m1);
 }
 
-// The flagged chanblocks travel in the launch's parameters (no device
-// table): g[k] = flagged[k] - k over the ascending flagged indices, so output
-// o takes chunk o + #{k : g[k] <= o} (a binary search per thread).  The
-// reference indexes chanblocks with u16, hence 16-bit entries.
-template <int CAP>
-struct FlagTable {
-    int n;
-    unsigned short g[CAP];
-};
+// The flagged chanblocks travel in the launch's parameters (FlagTable, no
+// device table) as g[k] = flagged[k] - k over the ascending flagged indices,
+// so output o takes chunk o + #{k : g[k] <= o}.
 constexpr int FLAG_CAP_SMALL = 256;
 constexpr int FLAG_CAP = 8000;  // 16 KB of launch parameters (the limit is 32764 bytes)
 
@@ -76,15 +70,7 @@ __global__ void __launch_bounds__(AVG_THREADS) average_kernel(const JonesF32* __
     const int half = (int)(tid & 1);
     if (g >= (size_t)nout * nbl) return;
     const int bl = (int)(g % nbl), o = (int)(g / nbl);
-    int lo = 0, hi = tab.n;
-    while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if ((int)tab.g[mid] <= o)
-            lo = mid + 1;
-        else
-            hi = mid;
-    }
-    const int f0 = (o + lo) * avg_freq, f1 = min(f0 + avg_freq, nf);
+    const int f0 = (o + flag_count_le(tab, o)) * avg_freq, f1 = min(f0 + avg_freq, nf);
     const int navg = f1 - f0, total = nt * navg;
     double ws[4] = {0, 0, 0, 0}, s[4] = {0, 0, 0, 0};
     double wsum = 0.0, fsum = 0.0;
@@ -177,28 +163,27 @@ extern "C" int hdc_vis_average(const JonesF32* d_from_tfb, const float* d_weight
         set_error("hdc_vis_average: %d channels do not make %lld chunks", num_freqs, nchunks);
         return HDC_ERR_ARG;
     }
-    std::vector<int> fl(h_flagged_chanblocks, h_flagged_chanblocks + num_flagged);
-    std::sort(fl.begin(), fl.end());
-    for (int k = 0; k < num_flagged; k++)
-        if (fl[k] < 0 || fl[k] >= nchunks || (k > 0 && fl[k] == fl[k - 1])) {
-            set_error("hdc_vis_average: flagged chanblock %d is out of range or repeated", fl[k]);
-            return HDC_ERR_ARG;
-        }
+    bool ok;
+    const std::vector<int> fl = sorted_flags(h_flagged_chanblocks, num_flagged, (int)nchunks, &ok);
+    if (!ok) {
+        set_error("hdc_vis_average: a flagged chanblock is out of range or repeated");
+        return HDC_ERR_ARG;
+    }
     cudaStream_t s = (cudaStream_t)stream;
     const size_t n = 2 * (size_t)num_chanblocks * num_baselines;
     const unsigned blocks = (unsigned)((n + vp::AVG_THREADS - 1) / vp::AVG_THREADS);
     auto launch = [&](auto& tab) {
         tab.n = num_flagged;
-        for (int k = 0; k < num_flagged; k++) tab.g[k] = (unsigned short)(fl[k] - k);
+        for (int k = 0; k < num_flagged; k++) tab.v[k] = (unsigned short)(fl[k] - k);
         vp::average_kernel<<<blocks, vp::AVG_THREADS, 0, s>>>(d_from_tfb, d_weights_from_tfb, num_timesteps,
                                                               num_freqs, num_baselines, avg_freq, tab,
                                                               num_chanblocks, d_to_fb, d_weights_to_fb);
     };
     if (num_flagged <= vp::FLAG_CAP_SMALL) {
-        vp::FlagTable<vp::FLAG_CAP_SMALL> tab;
+        FlagTable<vp::FLAG_CAP_SMALL> tab;
         launch(tab);
     } else {
-        static thread_local vp::FlagTable<vp::FLAG_CAP> tab;  // 16 KB: off the stack
+        static thread_local FlagTable<vp::FLAG_CAP> tab;  // 16 KB: off the stack
         launch(tab);
     }
     count_launches(1);

@@ -1356,4 +1356,46 @@ int or_vis_average(const float* from, const float* wfrom, int nt, int nf, int nb
     return o == nout ? 0 : 1;
 }
 
+// di_calibrate/mod.rs:89-176 (into_cal_sols): [tb][unflagged tile][unflagged
+// chanblock] model->data gains to [tb][tile][chanblock] data->model
+// solutions; inverted as marlu Jones::inv (jinv) or, for XX / YY only data,
+// Complex::inv of that entry; NaN where a tile or chanblock is flagged.
+int or_into_cal_sols(const double* in, int ntb, int nut, int nuc, const int* ftiles, int nft, const int* fchans,
+                     int nfc, int pols, double* out) {
+    const int ntt = nut + nft, ntc = nuc + nfc;
+    std::vector<char> tf(ntt, 0), cf(ntc, 0);
+    for (int k = 0; k < nft; k++) tf[ftiles[k]] = 1;
+    for (int k = 0; k < nfc; k++) cf[fchans[k]] = 1;
+    for (int tb = 0; tb < ntb; tb++) {
+        int ut = 0;
+        for (int t = 0; t < ntt; t++) {
+            int uc = 0;
+            for (int c = 0; c < ntc; c++) {
+                double* o = out + 8 * (((size_t)tb * ntt + t) * ntc + c);
+                if (tf[t] || cf[c]) {
+                    for (int k = 0; k < 8; k++) o[k] = NAN;
+                    continue;
+                }
+                const double* p = in + 8 * (((size_t)tb * nut + ut) * nuc + uc);
+                J64 j;
+                for (int k = 0; k < 4; k++) j.j[k] = {p[2 * k], p[2 * k + 1]};
+                J64 r = jzero();
+                if (pols == 1) {
+                    const double n = cnorm_sqr(j.j[0]);
+                    r.j[0] = {j.j[0].re / n, -j.j[0].im / n};
+                } else if (pols == 2) {
+                    const double n = cnorm_sqr(j.j[3]);
+                    r.j[3] = {j.j[3].re / n, -j.j[3].im / n};
+                } else {
+                    r = jinv(j);
+                }
+                for (int k = 0; k < 4; k++) o[2 * k] = r.j[k].re, o[2 * k + 1] = r.j[k].im;
+                uc++;
+            }
+            if (!tf[t]) ut++;
+        }
+    }
+    return 0;
+}
+
 }  // extern "C"

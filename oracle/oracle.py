@@ -333,6 +333,20 @@ def vis_average(vis, weights, num_chanblocks, flagged=()):
     return to, wto
 
 
+def into_cal_sols(di_jones, flagged_tiles, flagged_chanblocks, pols=0):
+    """into_cal_sols' Jones part: [tb][unflagged tile][unflagged cb][8] ->
+    [tb][tile][cb][8] inverted, NaN where flagged."""
+    dj = np.ascontiguousarray(di_jones, np.float64)
+    ntb, nut, nuc = dj.shape[:3]
+    ft = np.ascontiguousarray(flagged_tiles, np.int32)
+    fc = np.ascontiguousarray(flagged_chanblocks, np.int32)
+    out = np.empty((ntb, nut + ft.size, nuc + fc.size, 8))
+    lib().or_into_cal_sols(_ptr(dj), ctypes.c_int(ntb), ctypes.c_int(nut), ctypes.c_int(nuc),
+                           _ptr(ft) if ft.size else None, ctypes.c_int(ft.size), _ptr(fc) if fc.size else None,
+                           ctypes.c_int(fc.size), ctypes.c_int(pols), _ptr(out))
+    return out
+
+
 def iono_loop(resid, weights, model, consts, niter, uvws, lambdas, convergence):
     resid = np.ascontiguousarray(resid, np.float32)
     weights = np.ascontiguousarray(weights, np.float32)

@@ -12,6 +12,10 @@ test time.
   (1530-1568).  Values are parsed from the Rust source text.
 * srclist_files.json -- the reference's hyperdrive-format source-list test
   files (YAML and JSON) with their source and component counts.
+* fits_srclists.json -- the reference's FITS-format source lists (written by
+  astropy through test_files/gen_fits_srclists.py), base64, with the YAML
+  lists that hold the same sources; they check the FITS reader against an
+  independent FITS writer.
 * shapelet_basis_samples.json -- samples of the shapelet basis table produced
   by the reference's generator script src/model/make_shapelet_basis_values.py
   (imported, its gen_shape_basis evaluated at the sampled points), plus the
@@ -142,6 +146,17 @@ def main(ref_root: str) -> None:
     (HERE / "srclist_files.json").write_text(
         json.dumps({"source": "test_files/{hyperdrive_srclist.yaml,hyperdrive_srclist.json,srclist_all_kinds.yaml}",
                     "lists": lists}, indent=1))
+
+    # FITS files from an independent writer (astropy), and the YAML twins of
+    # their sources.
+    import base64
+
+    fl = {}
+    for stem in ["jack", "gleam", "lobes"]:
+        fl[stem] = {"fits_base64": base64.b64encode((tf / f"{stem}.fits").read_bytes()).decode("ascii"),
+                    "yaml": (tf / f"{stem}.yaml").read_text() if (tf / f"{stem}.yaml").exists() else None}
+    (HERE / "fits_srclists.json").write_text(
+        json.dumps({"source": "test_files/{jack,gleam,lobes}.{fits,yaml}", "lists": fl}, indent=1))
 
 
 if __name__ == "__main__":
