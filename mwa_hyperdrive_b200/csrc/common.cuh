@@ -205,6 +205,9 @@ const char* cuda_msg(cudaError_t e);
 // Per-device scratch (grows on demand; used by the drop-in entry points that
 // have no workspace argument).  Returns NULL on allocation failure.
 void* device_scratch(size_t bytes);
+// Stream-ordered allocation from the library's own pool on the current device
+// (freed blocks stay mapped for reuse); release with cudaFreeAsync.
+cudaError_t pool_malloc_async(void** p, size_t bytes, cudaStream_t s);
 // Device word for kernel error flags (per device, zero-initialised).
 int* device_error_word();
 // Read and clear the device error word (synchronises the stream).

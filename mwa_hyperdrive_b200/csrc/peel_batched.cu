@@ -288,7 +288,7 @@ extern "C" int hdc_peel_timeblock_batched(JonesF32* d_resid_tfb, const float* d_
         return HDC_ERR_ALLOC;
     }
     pb::DevBuf b_lam, b_lam_lo, b_lmst, b_avg_lmst, b_xyz, b_uv_pc, b_uv_src, b_uv_lo, b_models, b_dlo, b_mlo, b_mlo_rot,
-        b_wlo, b_scr, b_old, b_new, b_stage;
+        b_wlo, b_scr, b_old, b_new;
     PB_CK(cudaMalloc(&b_lam.p, sizeof(double) * nf));
     PB_CK(cudaMalloc(&b_lam_lo.p, sizeof(double) * nlo));
     PB_CK(cudaMalloc(&b_lmst.p, sizeof(double) * nt));
@@ -313,32 +313,27 @@ extern "C" int hdc_peel_timeblock_batched(JonesF32* d_resid_tfb, const float* d_
     PB_CK(k_weights_average(d_weights_tfb, b_wlo.as<float>(), nt, nbl, nf, favg, s));
     PB_CK(k_xyzs_to_uvws(b_xyz.as<XYZ>(), b_lmst.as<double>(), b_uv_pc.as<UVW>(), phase_centre, num_tiles, nbl, nt, s));
     PB_CK(cudaMemsetAsync(b_models.p, 0, need, s));
-    if (points) PB_CK(cudaMalloc(&b_stage.p, sizeof(JonesF32) * (size_t)nf * nbl));
-    // per source: UVWs in its frame and its high-resolution model (once per timeblock)
+    // per source: UVWs in its frame and its high-resolution model (once per
+    // timeblock).  A single point at its own position has the same model on
+    // every baseline, so its table row per timestep is a one-baseline predict
+    // (tiles 0 and 1) written straight into the table.
     for (int i = 0; i < ns; i++) {
         UVW* uv = b_uv_src.as<UVW>() + (size_t)i * nt * nbl;
         PB_CK(k_xyzs_to_uvws(b_xyz.as<XYZ>(), b_lmst.as<double>(), uv, h_source_positions[i], num_tiles, nbl, nt, s));
         PB_CK(k_xyzs_to_uvws(b_xyz.as<XYZ>(), b_avg_lmst.as<double>(), b_uv_lo.as<UVW>() + (size_t)i * nbl,
                              h_source_positions[i], num_tiles, nbl, 1, s));
         HdcModeller* hm = nullptr;
-        int rc = hdc_modeller_new(&h_sources[i], 0, h_tile_xyzs, num_tiles, h_freqs, num_freqs, h_source_positions[i],
-                                  params->array_latitude_rad, params->beam_kind, HDC_PREDICT_DIRECT, &hm);
+        int rc = hdc_modeller_new(&h_sources[i], 0, h_tile_xyzs, points ? 2 : num_tiles, h_freqs, num_freqs,
+                                  h_source_positions[i], params->array_latitude_rad, params->beam_kind,
+                                  HDC_PREDICT_DIRECT, &hm);
         if (rc) return rc;
         std::unique_ptr<Modeller> m(reinterpret_cast<Modeller*>(hm));
         for (int t = 0; t < nt; t++) {
-            if (points) {
-                // predict all baselines, keep baseline 0's channel column
-                PB_CK(cudaMemsetAsync(b_stage.p, 0, sizeof(JonesF32) * (size_t)nf * nbl, s));
-                rc = m->model_uvws(h_lmsts[t], uv + (size_t)t * nbl, b_stage.as<JonesF32>(), s);
-                if (rc) return rc;
-                PB_CK(cudaMemcpy2DAsync(b_models.as<JonesF32>() + ((size_t)i * nt + t) * nf, sizeof(JonesF32),
-                                        b_stage.p, sizeof(JonesF32) * nbl, sizeof(JonesF32), nf,
-                                        cudaMemcpyDeviceToDevice, s));
-            } else {
-                rc = m->model_uvws(h_lmsts[t], uv + (size_t)t * nbl,
-                                   b_models.as<JonesF32>() + (size_t)i * nvis + (size_t)t * nf * nbl, s);
-                if (rc) return rc;
-            }
+            JonesF32* dst = points ? b_models.as<JonesF32>() + ((size_t)i * nt + t) * nf
+                                   : b_models.as<JonesF32>() + (size_t)i * nvis + (size_t)t * nf * nbl;
+            // baseline 0 of the source-frame UVWs is the (0, 1) tile pair
+            rc = m->model_uvws(h_lmsts[t], uv + (size_t)t * nbl, dst, s);
+            if (rc) return rc;
         }
     }
 

@@ -175,7 +175,7 @@ extern "C" int hdc_warmstart_features(const JonesF64* d_prev_tc, int num_tiles, 
     cudaStream_t s = (cudaStream_t)stream;
     const size_t n = (size_t)num_tiles * num_chanblocks;
     ws::Scratch sc(s);
-    HDC_CUDA_RET_INT(cudaMallocAsync(&sc.p, n * (8 * sizeof(double) + sizeof(double4)), s));
+    HDC_CUDA_RET_INT(pool_malloc_async(&sc.p, n * (8 * sizeof(double) + sizeof(double4)), s));
     double* aligned = static_cast<double*>(sc.p);
     double4* frame = reinterpret_cast<double4*>(aligned + n * 8);
     return ws::features(d_prev_tc, num_tiles, num_chanblocks, d_x, aligned, frame, s);
@@ -217,7 +217,7 @@ extern "C" int hdc_warmstart_propose(HdcMlp* mlp, const JonesF64* d_prev_tc, int
     ws::Scratch sc(s);
     const size_t bytes = n * (8 * sizeof(double) + sizeof(double4) + sizeof(float) * (ws::IN + ws::OUT)) +
                          (judge ? n * sizeof(JonesF64) : 0);
-    HDC_CUDA_RET_INT(cudaMallocAsync(&sc.p, bytes, s));
+    HDC_CUDA_RET_INT(pool_malloc_async(&sc.p, bytes, s));
     double* aligned = static_cast<double*>(sc.p);
     double4* frame = reinterpret_cast<double4*>(aligned + n * 8);
     float* x = reinterpret_cast<float*>(frame + n);
