@@ -336,11 +336,22 @@ __global__ void __launch_bounds__(DT) direct_kernel(const DirectParams p) {
 // memory and table-position loads -- is done once for all FCH channels and
 // only scaled per channel (lambda^-1 for the phase and positions, lambda^-2
 // for the exponent).  The arithmetic per channel is that of the FAST
-// direct_kernel above.
-constexpr int FCH = 2;
+// direct_kernel above.  Channels per thread and CTAs per SM by type
+// (Gaussians 1, shapelets 2).
+template <int TYPE>
+struct FastShape {
+    static constexpr int FCH = 3;
+    static constexpr int MIN_CTAS = 2;
+};
+template <>
+struct FastShape<2> {
+    static constexpr int FCH = 2;
+    static constexpr int MIN_CTAS = 3;
+};
 
 template <int TYPE, bool OUT64>
-__global__ void __launch_bounds__(DT, 3) fast_kernel(const DirectParams p) {
+__global__ void __launch_bounds__(DT, FastShape<TYPE>::MIN_CTAS) fast_kernel(const DirectParams p) {
+    constexpr int FCH = FastShape<TYPE>::FCH;
     __shared__ alignas(128) double4 s_lmn[2][CH];
     __shared__ alignas(128) JonesF64 s_flux[2][FCH][CH];
     __shared__ alignas(128) double4 s_gp[2][CH];
@@ -508,6 +519,7 @@ static cudaError_t launch_t(bool tile_beam, bool out64, bool fast, const DirectP
         else
             direct_kernel<TYPE, true, false, false><<<grid, DT, 0, s>>>(p);
     } else if (fast && TYPE != 0) {
+        constexpr int FCH = FastShape<TYPE == 0 ? 1 : TYPE>::FCH;
         const dim3 fgrid((p.nbl + DT - 1) / DT, (p.nf + FCH - 1) / FCH);
         if (out64)
             fast_kernel<TYPE == 0 ? 1 : TYPE, true><<<fgrid, DT, 0, s>>>(p);
