@@ -342,16 +342,19 @@ template <int TYPE>
 struct FastShape {
     static constexpr int FCH = 3;
     static constexpr int MIN_CTAS = 2;
+    static constexpr int CHUNK = 64;
 };
 template <>
 struct FastShape<2> {
     static constexpr int FCH = 2;
     static constexpr int MIN_CTAS = 3;
+    static constexpr int CHUNK = 64;
 };
 
 template <int TYPE, bool OUT64>
 __global__ void __launch_bounds__(DT, FastShape<TYPE>::MIN_CTAS) fast_kernel(const DirectParams p) {
     constexpr int FCH = FastShape<TYPE>::FCH;
+    constexpr int CH = FastShape<TYPE>::CHUNK;  // components per staged chunk
     __shared__ alignas(128) double4 s_lmn[2][CH];
     __shared__ alignas(128) JonesF64 s_flux[2][FCH][CH];
     __shared__ alignas(128) double4 s_gp[2][CH];
