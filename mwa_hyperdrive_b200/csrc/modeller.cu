@@ -790,9 +790,26 @@ int Modeller::model_host_pipelined(double lst, JonesF32* h_vis, UVW* h_uvws, cud
     for (int i = 0; i < 3; i++) HDC_CUDA_RET_INT(cudaStreamWaitEvent(pipe_s[i], start, 0));
     int rc = geometry(lst, pipe_s[1]);
     if (rc) return rc;
-    const int nch = std::min(PIPE_CHUNKS, nf);
+    // chunk boundaries: a short first chunk (its upload is the only one the
+    // predict waits for) and a short last chunk (its download is the only one
+    // nothing overlaps), 1/16 of the channels each; three equal chunks between
+    int bounds[PIPE_CHUNKS + 1];
+    int nch = 0;
+    const int edge = nf / 16;
+    if (edge >= 1 && nf - 2 * edge >= PIPE_CHUNKS - 2) {
+        nch = PIPE_CHUNKS;
+        bounds[0] = 0;
+        bounds[1] = edge;
+        for (int k = 1; k < PIPE_CHUNKS - 2; k++)
+            bounds[1 + k] = edge + (int)((long long)(nf - 2 * edge) * k / (PIPE_CHUNKS - 2));
+        bounds[PIPE_CHUNKS - 1] = nf - edge;
+        bounds[PIPE_CHUNKS] = nf;
+    } else {
+        nch = std::min(PIPE_CHUNKS, nf);
+        for (int k = 0; k <= nch; k++) bounds[k] = (int)((long long)nf * k / nch);
+    }
     for (int c = 0; c < nch; c++) {
-        const int f0 = (int)((long long)nf * c / nch), f1 = (int)((long long)nf * (c + 1) / nch);
+        const int f0 = bounds[c], f1 = bounds[c + 1];
         const size_t off = (size_t)f0 * nbl, n = (size_t)(f1 - f0) * nbl * sizeof(JonesF32);
         HDC_CUDA_RET_INT(cudaMemcpyAsync(d_host_vis + off, h_vis + off, n, cudaMemcpyHostToDevice, pipe_s[0]));
         HDC_CUDA_RET_INT(cudaEventRecord(up[c], pipe_s[0]));

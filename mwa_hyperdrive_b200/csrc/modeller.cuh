@@ -64,7 +64,7 @@ struct Modeller {
     int model_channels(double lst, void* d_vis, bool out64, int f0, int nfc, cudaStream_t s);
     // host-buffer predict: upload, predict and download of channel chunks
     // overlap on three streams
-    static constexpr int PIPE_CHUNKS = 4;
+    static constexpr int PIPE_CHUNKS = 5;
     cudaStream_t pipe_s[3] = {nullptr, nullptr, nullptr};
     cudaEvent_t pipe_ev[2 * PIPE_CHUNKS + 2] = {};
     int model_host_pipelined(double lst, JonesF32* h_vis, UVW* h_uvws, cudaStream_t s);
