@@ -23,8 +23,9 @@
 //   3. apply sweep: R += sum_s conj(rot_s) M_s (iono_s(old) - iono_s(new))
 //      (the reference's subtract_iono, rotated back).
 // With one source this is the reference's sequence exactly (up to rounding:
-// FP64 arithmetic with FP32 phasors after an exact FP64 range reduction,
-// instead of its f32 intermediates); with several, sources
+// FP32 products with FP32 phasors after an exact FP64 range reduction, FP64
+// sums across timesteps, as against its f32 intermediates); with several,
+// sources
 // fitted in the same pass do not see each other's updates until the next
 // pass.  The source models M_s (high resolution, source frame) are predicted
 // once per timeblock by the modeller and reused by every pass.
@@ -64,6 +65,7 @@ struct SweepArgs {
     const UVW* uv_pc;       // [nt][nbl]
     const UVW* uv_src;      // [nsrc][nt][nbl]
     const double* lambdas;  // [nf]
+    const double* inv_lambdas;  // [nf] 1 / lambda: the rotation phases multiply instead of dividing
     const IonoConsts* old;  // [nsrc]
     const IonoConsts* neu;  // [nsrc] (apply sweep)
     JonesF32* d_lo;         // [nsrc][nlo][nbl]
@@ -71,20 +73,36 @@ struct SweepArgs {
     int nt, nf, nbl, nsrc, favg;
 };
 
-// exp(i arg): the argument (radians) in FP64, reduced exactly in quarter
-// turns, then the FP32 quarter-turn polynomials (< 1 ulp of FP32; the
-// residual is stored in FP32, so a per-term phasor error of ~1e-7 is at its
-// rounding level)
-__device__ __forceinline__ cplx phase(double arg) {
+// exp(i arg) as (cos, sin): the argument (radians) in FP64, reduced exactly
+// in quarter turns, then the FP32 quarter-turn polynomials (< 1 ulp of FP32;
+// the residual is stored in FP32, so a per-term phasor error of ~1e-7 is at
+// its rounding level)
+__device__ __forceinline__ float2 phase_f(double arg) {
     float sn, cs;
     phasor_quarter_f32(arg * 0.63661977236758134308, sn, cs);  // 2 / pi
-    return cplx{(double)cs, (double)sn};
+    return make_float2(cs, sn);
 }
 
 // iono factor g exp(-2 pi i (u alpha + v beta) lambda), as add_model / subtract_iono
-__device__ __forceinline__ cplx iono(const IonoConsts& k, const UVW& q, double lam) {
-    if (k.alpha == 0.0 && k.beta == 0.0) return cplx{k.gain, 0.0};
-    return phase(-TAU * (q.u * k.alpha + q.v * k.beta) * lam) * k.gain;
+__device__ __forceinline__ float2 iono_f(const IonoConsts& k, const UVW& q, double lam) {
+    if (k.alpha == 0.0 && k.beta == 0.0) return make_float2((float)k.gain, 0.f);
+    const float2 p = phase_f(-TAU * (q.u * k.alpha + q.v * k.beta) * lam);
+    const float g = (float)k.gain;
+    return make_float2(p.x * g, p.y * g);
+}
+
+__device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
+    return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+
+// a Jones matrix as four complex FP32 numbers
+struct JF {
+    float2 v[4];
+};
+__device__ __forceinline__ JF load_jf(const JonesF32& j) {
+    const float4* p = reinterpret_cast<const float4*>(&j);
+    const float4 a = p[0], b = p[1];
+    return JF{{make_float2(a.x, a.y), make_float2(a.z, a.w), make_float2(b.x, b.y), make_float2(b.z, b.w)}};
 }
 
 __device__ __forceinline__ JonesF32 to_f32(const J2& v) {
@@ -95,7 +113,9 @@ __device__ __forceinline__ JonesF32 to_f32(const J2& v) {
 // blockDim (BX, SY): x = low-resolution bins, y = sources of this CTA's chunk
 // Grid: one dimension, source groups fastest -- the CTAs of all source
 // groups of a bin block run close together, so each residual tile comes
-// from DRAM once and from L2 for the other sources.
+// from DRAM once and from L2 for the other sources.  Products are formed in
+// FP32 (the data are FP32) and summed in FP32 over one timestep's channels
+// of the bin, then in FP64 across timesteps.
 template <int BX, int SY>
 __global__ void __launch_bounds__(BX* SY) accumulate_kernel(const SweepArgs A) {
     const int nlo = A.nf / A.favg;
@@ -107,31 +127,51 @@ __global__ void __launch_bounds__(BX* SY) accumulate_kernel(const SweepArgs A) {
     const IonoConsts k = A.old[src];
     const size_t nvis = (size_t)A.nt * A.nf * A.nbl;
     const JonesF32* M = A.ptab ? nullptr : A.models + (size_t)src * nvis;
-    J2 acc_d = jzero(), acc_m = jzero();
+    double acc_d[8] = {0, 0, 0, 0, 0, 0, 0, 0}, acc_m[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     double ws = 0.0;
     for (int t = 0; t < A.nt; t++) {
         const UVW q = A.uv_src[((size_t)src * A.nt + t) * A.nbl + bl];
         const double dw = q.w - A.uv_pc[(size_t)t * A.nbl + bl].w;
+        float2 sd[4] = {}, sm[4] = {};
+        float sw = 0.f;
 #pragma unroll 4  // several channels' loads in flight at once
         for (int fc = flo * A.favg; fc < flo * A.favg + A.favg; fc++) {
             const size_t i = ((size_t)t * A.nf + fc) * A.nbl + bl;
-            const double wt = A.w[i];
-            const double lam = A.lambdas[fc];
-            const cplx rot = phase(-TAU * dw / lam);
-            const JonesF32 mj = A.ptab ? A.ptab[((size_t)src * A.nt + t) * A.nf + fc] : M[i];
-            const J2 m = load_j32(mj) * iono(k, q, lam);
-            acc_d = acc_d + (load_j32(A.resid[i]) * rot + m) * wt;
-            acc_m = acc_m + m * wt;
-            ws += wt;
+            const float wt = A.w[i];
+            const float2 rot = phase_f(-TAU * dw * A.inv_lambdas[fc]);
+            const float2 io = iono_f(k, q, A.lambdas[fc]);
+            const JF mj = load_jf(A.ptab ? A.ptab[((size_t)src * A.nt + t) * A.nf + fc] : M[i]);
+            const JF r = load_jf(A.resid[i]);
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                const float2 m = cmulf(mj.v[e], io);
+                const float2 d = cmulf(r.v[e], rot);
+                sd[e].x = fmaf(d.x + m.x, wt, sd[e].x);
+                sd[e].y = fmaf(d.y + m.y, wt, sd[e].y);
+                sm[e].x = fmaf(m.x, wt, sm[e].x);
+                sm[e].y = fmaf(m.y, wt, sm[e].y);
+            }
+            sw += wt;
         }
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            acc_d[2 * e] += sd[e].x, acc_d[2 * e + 1] += sd[e].y;
+            acc_m[2 * e] += sm[e].x, acc_m[2 * e + 1] += sm[e].y;
+        }
+        ws += sw;
     }
-    const double d = ws > 0.0 ? ws : 1.0;
+    const double inv = 1.0 / (ws > 0.0 ? ws : 1.0);
     const size_t o = ((size_t)src * nlo + flo) * A.nbl + bl;
-    A.d_lo[o] = to_f32(acc_d * (1.0 / d));
-    A.m_lo[o] = to_f32(acc_m * (1.0 / d));
+    A.d_lo[o] = JonesF32{(float)(acc_d[0] * inv), (float)(acc_d[1] * inv), (float)(acc_d[2] * inv),
+                         (float)(acc_d[3] * inv), (float)(acc_d[4] * inv), (float)(acc_d[5] * inv),
+                         (float)(acc_d[6] * inv), (float)(acc_d[7] * inv)};
+    A.m_lo[o] = JonesF32{(float)(acc_m[0] * inv), (float)(acc_m[1] * inv), (float)(acc_m[2] * inv),
+                         (float)(acc_m[3] * inv), (float)(acc_m[4] * inv), (float)(acc_m[5] * inv),
+                         (float)(acc_m[6] * inv), (float)(acc_m[7] * inv)};
 }
 
-// one thread per high-resolution visibility; all sources' updates
+// one thread per high-resolution visibility; all sources' updates, summed in
+// FP32 and added to the residual once
 __global__ void __launch_bounds__(256) apply_kernel(JonesF32* resid, const SweepArgs A) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     const size_t nvis = (size_t)A.nt * A.nf * A.nbl;
@@ -139,18 +179,38 @@ __global__ void __launch_bounds__(256) apply_kernel(JonesF32* resid, const Sweep
     const int bl = (int)(i % A.nbl);
     const int f = (int)((i / A.nbl) % A.nf);
     const int t = (int)(i / ((size_t)A.nbl * A.nf));
-    const double lam = A.lambdas[f];
+    const double lam = A.lambdas[f], ilam = A.inv_lambdas[f];
     const double wpc = A.uv_pc[(size_t)t * A.nbl + bl].w;
-    J2 r = load_j32(resid[i]);
+    float2 dl[4] = {};
     for (int s = 0; s < A.nsrc; s++) {
         const UVW q = A.uv_src[((size_t)s * A.nt + t) * A.nbl + bl];
-        const cplx d = iono(A.old[s], q, lam) - iono(A.neu[s], q, lam);
-        if (d.re == 0.0 && d.im == 0.0) continue;
-        const cplx back = phase(TAU * (q.w - wpc) / lam);  // conj of the rotation to the source
-        const JonesF32 mj = A.ptab ? A.ptab[((size_t)s * A.nt + t) * A.nf + f] : A.models[(size_t)s * nvis + i];
-        r = r + load_j32(mj) * (back * d);
+        const float2 io = iono_f(A.old[s], q, lam), in = iono_f(A.neu[s], q, lam);
+        const float2 d = make_float2(io.x - in.x, io.y - in.y);
+        if (d.x == 0.f && d.y == 0.f) continue;
+        const float2 back = phase_f(TAU * (q.w - wpc) * ilam);  // conj of the rotation to the source
+        const float2 bd = cmulf(back, d);
+        const JF m = load_jf(A.ptab ? A.ptab[((size_t)s * A.nt + t) * A.nf + f] : A.models[(size_t)s * nvis + i]);
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            const float2 c = cmulf(m.v[e], bd);
+            dl[e].x += c.x, dl[e].y += c.y;
+        }
     }
-    resid[i] = to_f32(r);
+    float4* p = reinterpret_cast<float4*>(resid + i);
+    const float4 a = p[0], b = p[1];
+    p[0] = make_float4(a.x + dl[0].x, a.y + dl[0].y, a.z + dl[1].x, a.w + dl[1].y);
+    p[1] = make_float4(b.x + dl[2].x, b.y + dl[2].y, b.z + dl[3].x, b.w + dl[3].y);
+}
+
+// ptab[(src * nt + t) * nf + f] = W[f][src] as FP32 (W = B S B^H of the
+// combined point-source modeller at timestep t)
+__global__ void point_table_kernel(const JonesF64* __restrict__ W, int ns, int nf, int nt, int t,
+                                   JonesF32* __restrict__ ptab) {
+    const int src = blockIdx.x * blockDim.x + threadIdx.x, f = blockIdx.y;
+    if (src >= ns) return;
+    const JonesF64 w = W[(size_t)f * ns + src];
+    ptab[((size_t)src * nt + t) * nf + f] = JonesF32{(float)w.j00_re, (float)w.j00_im, (float)w.j01_re, (float)w.j01_im,
+                                                     (float)w.j10_re, (float)w.j10_im, (float)w.j11_re, (float)w.j11_im};
 }
 
 struct Variant {
@@ -211,10 +271,21 @@ int choose_variant(const SweepArgs& A, cudaStream_t s) {
     return best;
 }
 
+// call-scoped device buffers from the library's stream-ordered pool: freed
+// blocks stay mapped, so later calls reuse them without new mappings
 struct DevBuf {
     void* p = nullptr;
+    cudaStream_t s = nullptr;
+    bool pooled = false;
+    cudaError_t alloc(size_t bytes, cudaStream_t st) {
+        s = st;
+        pooled = true;
+        return pool_malloc_async(&p, bytes, st);
+    }
+    // large one-off buffers stay outside the pool, which keeps what it holds
+    cudaError_t alloc_plain(size_t bytes) { return cudaMalloc(&p, bytes); }
     ~DevBuf() {
-        if (p) cudaFree(p);
+        if (p) pooled ? cudaFreeAsync(p, s) : cudaFree(p);
     }
     template <class T>
     T* as() {
@@ -260,8 +331,9 @@ extern "C" int hdc_peel_timeblock_batched(JonesF32* d_resid_tfb, const float* d_
     const int ns = num_sources;
     const size_t nvis = (size_t)nt * nf * nbl;
 
-    std::vector<double> lam(nf), lam_lo(nlo);
+    std::vector<double> lam(2 * (size_t)nf), lam_lo(nlo);
     for (int f = 0; f < nf; f++) lam[f] = VEL_C / h_freqs[f];
+    for (int f = 0; f < nf; f++) lam[nf + f] = 1.0 / lam[f];
     for (int k = 0; k < nlo; k++) {
         double sum = 0.0;
         for (int f = k * favg; f < (k + 1) * favg; f++) sum += h_freqs[f];
@@ -289,23 +361,23 @@ extern "C" int hdc_peel_timeblock_batched(JonesF32* d_resid_tfb, const float* d_
     }
     pb::DevBuf b_lam, b_lam_lo, b_lmst, b_avg_lmst, b_xyz, b_uv_pc, b_uv_src, b_uv_lo, b_models, b_dlo, b_mlo, b_mlo_rot,
         b_wlo, b_scr, b_old, b_new;
-    PB_CK(cudaMalloc(&b_lam.p, sizeof(double) * nf));
-    PB_CK(cudaMalloc(&b_lam_lo.p, sizeof(double) * nlo));
-    PB_CK(cudaMalloc(&b_lmst.p, sizeof(double) * nt));
-    PB_CK(cudaMalloc(&b_avg_lmst.p, sizeof(double)));
-    PB_CK(cudaMalloc(&b_xyz.p, sizeof(XYZ) * xyz_t.size()));
-    PB_CK(cudaMalloc(&b_uv_pc.p, sizeof(UVW) * (size_t)nt * nbl));
-    PB_CK(cudaMalloc(&b_uv_src.p, sizeof(UVW) * (size_t)ns * nt * nbl));
-    PB_CK(cudaMalloc(&b_uv_lo.p, sizeof(UVW) * (size_t)ns * nbl));
-    PB_CK(cudaMalloc(&b_models.p, need));
-    PB_CK(cudaMalloc(&b_dlo.p, sizeof(JonesF32) * (size_t)ns * nlo * nbl));
-    PB_CK(cudaMalloc(&b_mlo.p, sizeof(JonesF32) * (size_t)ns * nlo * nbl));
-    PB_CK(cudaMalloc(&b_mlo_rot.p, sizeof(JonesF32) * (size_t)ns * nlo * nbl));
-    PB_CK(cudaMalloc(&b_wlo.p, sizeof(float) * (size_t)nlo * nbl));
-    PB_CK(cudaMalloc(&b_scr.p, iono_batched_scratch_bytes(ns, nbl, nlo)));
-    PB_CK(cudaMalloc(&b_old.p, sizeof(IonoConsts) * ns));
-    PB_CK(cudaMalloc(&b_new.p, sizeof(IonoConsts) * ns));
-    PB_CK(cudaMemcpyAsync(b_lam.p, lam.data(), sizeof(double) * nf, cudaMemcpyHostToDevice, s));
+    PB_CK(b_lam.alloc(sizeof(double) * 2 * nf, s));  // lambda, then 1 / lambda
+    PB_CK(b_lam_lo.alloc(sizeof(double) * nlo, s));
+    PB_CK(b_lmst.alloc(sizeof(double) * nt, s));
+    PB_CK(b_avg_lmst.alloc(sizeof(double), s));
+    PB_CK(b_xyz.alloc(sizeof(XYZ) * xyz_t.size(), s));
+    PB_CK(b_uv_pc.alloc(sizeof(UVW) * (size_t)nt * nbl, s));
+    PB_CK(b_uv_src.alloc(sizeof(UVW) * (size_t)ns * nt * nbl, s));
+    PB_CK(b_uv_lo.alloc(sizeof(UVW) * (size_t)ns * nbl, s));
+    PB_CK(points ? b_models.alloc(need, s) : b_models.alloc_plain(need));
+    PB_CK(b_dlo.alloc(sizeof(JonesF32) * (size_t)ns * nlo * nbl, s));
+    PB_CK(b_mlo.alloc(sizeof(JonesF32) * (size_t)ns * nlo * nbl, s));
+    PB_CK(b_mlo_rot.alloc(sizeof(JonesF32) * (size_t)ns * nlo * nbl, s));
+    PB_CK(b_wlo.alloc(sizeof(float) * (size_t)nlo * nbl, s));
+    PB_CK(b_scr.alloc(iono_batched_scratch_bytes(ns, nbl, nlo), s));
+    PB_CK(b_old.alloc(sizeof(IonoConsts) * ns, s));
+    PB_CK(b_new.alloc(sizeof(IonoConsts) * ns, s));
+    PB_CK(cudaMemcpyAsync(b_lam.p, lam.data(), sizeof(double) * 2 * nf, cudaMemcpyHostToDevice, s));
     PB_CK(cudaMemcpyAsync(b_lam_lo.p, lam_lo.data(), sizeof(double) * nlo, cudaMemcpyHostToDevice, s));
     PB_CK(cudaMemcpyAsync(b_lmst.p, h_lmsts, sizeof(double) * nt, cudaMemcpyHostToDevice, s));
     PB_CK(cudaMemcpyAsync(b_avg_lmst.p, &average_lmst, sizeof(double), cudaMemcpyHostToDevice, s));
@@ -314,26 +386,61 @@ extern "C" int hdc_peel_timeblock_batched(JonesF32* d_resid_tfb, const float* d_
     PB_CK(k_xyzs_to_uvws(b_xyz.as<XYZ>(), b_lmst.as<double>(), b_uv_pc.as<UVW>(), phase_centre, num_tiles, nbl, nt, s));
     PB_CK(cudaMemsetAsync(b_models.p, 0, need, s));
     // per source: UVWs in its frame and its high-resolution model (once per
-    // timeblock).  A single point at its own position has the same model on
-    // every baseline, so its table row per timestep is a one-baseline predict
-    // (tiles 0 and 1) written straight into the table.
+    // timeblock)
     for (int i = 0; i < ns; i++) {
         UVW* uv = b_uv_src.as<UVW>() + (size_t)i * nt * nbl;
         PB_CK(k_xyzs_to_uvws(b_xyz.as<XYZ>(), b_lmst.as<double>(), uv, h_source_positions[i], num_tiles, nbl, nt, s));
         PB_CK(k_xyzs_to_uvws(b_xyz.as<XYZ>(), b_avg_lmst.as<double>(), b_uv_lo.as<UVW>() + (size_t)i * nbl,
                              h_source_positions[i], num_tiles, nbl, 1, s));
+    }
+    if (points) {
+        // A single point at its own position has, on every baseline, the model
+        // B S B^H (phase 1).  One modeller over all the sources' components
+        // (two tiles: the weights do not depend on the baselines or the phase
+        // centre) gives B S B^H per (channel, source) after each timestep's
+        // geometry; the table kernel stores it as [source][timestep][channel].
+        std::vector<int> ctype(ns, HDC_POINT), ftype(ns), fstart(ns), fcount(ns), zero(ns, 0);
+        std::vector<double> ra(ns), dec(ns), nil(ns, 0.0), si(ns), q(ns), fds;
+        for (int i = 0; i < ns; i++) {
+            const HdcSkyModel& m = h_sources[i];
+            ra[i] = m.ra[0], dec[i] = m.dec[0], ftype[i] = m.flux_type[0], si[i] = m.si[0], q[i] = m.q[0];
+            fstart[i] = (int)(fds.size() / 5);
+            fcount[i] = m.fd_count[0];
+            fds.insert(fds.end(), m.fds + 5 * (size_t)m.fd_start[0], m.fds + 5 * (size_t)(m.fd_start[0] + m.fd_count[0]));
+        }
+        const HdcSkyModel all = {ns,          ctype.data(), ra.data(),     dec.data(),   nil.data(), nil.data(),
+                                 nil.data(),  ftype.data(), si.data(),     q.data(),     fstart.data(), fcount.data(),
+                                 fds.data(),  zero.data(),  zero.data(),   zero.data(),  zero.data(), nil.data()};
         HdcModeller* hm = nullptr;
-        int rc = hdc_modeller_new(&h_sources[i], 0, h_tile_xyzs, points ? 2 : num_tiles, h_freqs, num_freqs,
-                                  h_source_positions[i], params->array_latitude_rad, params->beam_kind,
-                                  HDC_PREDICT_DIRECT, &hm);
+        int rc = hdc_modeller_new(&all, 0, h_tile_xyzs, 2, h_freqs, num_freqs, phase_centre,
+                                  params->array_latitude_rad, params->beam_kind, HDC_PREDICT_DIRECT, &hm);
         if (rc) return rc;
         std::unique_ptr<Modeller> m(reinterpret_cast<Modeller*>(hm));
         for (int t = 0; t < nt; t++) {
-            JonesF32* dst = points ? b_models.as<JonesF32>() + ((size_t)i * nt + t) * nf
-                                   : b_models.as<JonesF32>() + (size_t)i * nvis + (size_t)t * nf * nbl;
-            // baseline 0 of the source-frame UVWs is the (0, 1) tile pair
-            rc = m->model_uvws(h_lmsts[t], uv + (size_t)t * nbl, dst, s);
+            rc = m->geometry(h_lmsts[t], s);
             if (rc) return rc;
+            pb::point_table_kernel<<<dim3((ns + 127) / 128, nf), 128, 0, s>>>(m->weights(0), ns, nf, nt, t,
+                                                                              b_models.as<JonesF32>());
+            count_launches(1);
+            PB_CK(cudaGetLastError());
+        }
+        // the modeller's tables are freed when it goes out of scope: let the
+        // table kernels finish reading them first
+        PB_CK(cudaStreamSynchronize(s));
+    } else {
+        for (int i = 0; i < ns; i++) {
+            HdcModeller* hm = nullptr;
+            int rc = hdc_modeller_new(&h_sources[i], 0, h_tile_xyzs, num_tiles, h_freqs, num_freqs,
+                                      h_source_positions[i], params->array_latitude_rad, params->beam_kind,
+                                      HDC_PREDICT_DIRECT, &hm);
+            if (rc) return rc;
+            std::unique_ptr<Modeller> m(reinterpret_cast<Modeller*>(hm));
+            const UVW* uv = b_uv_src.as<UVW>() + (size_t)i * nt * nbl;
+            for (int t = 0; t < nt; t++) {
+                rc = m->model_uvws(h_lmsts[t], uv + (size_t)t * nbl,
+                                   b_models.as<JonesF32>() + (size_t)i * nvis + (size_t)t * nf * nbl, s);
+                if (rc) return rc;
+            }
         }
     }
 
@@ -345,6 +452,7 @@ extern "C" int hdc_peel_timeblock_batched(JonesF32* d_resid_tfb, const float* d_
     A.uv_pc = b_uv_pc.as<UVW>();
     A.uv_src = b_uv_src.as<UVW>();
     A.lambdas = b_lam.as<double>();
+    A.inv_lambdas = b_lam.as<double>() + nf;
     A.old = b_old.as<IonoConsts>();
     A.neu = b_new.as<IonoConsts>();
     A.d_lo = b_dlo.as<JonesF32>();
