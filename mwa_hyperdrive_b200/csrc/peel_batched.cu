@@ -22,6 +22,10 @@
 //      (iono_loop_batched_on, the reference's arithmetic);
 //   3. apply sweep: R += sum_s conj(rot_s) M_s (iono_s(old) - iono_s(new))
 //      (the reference's subtract_iono, rotated back).
+// Every phase on a baseline is a difference of per-tile phases (uvw_pq =
+// uvw_p - uvw_q), so the rotation and ionospheric phasors come from per-tile
+// tables [source][timestep][channel][tile] -- 128 phasors where a baseline
+// loop would evaluate 8128 -- and a baseline takes tab[p] conj(tab[q]).
 // With one source this is the reference's sequence exactly (up to rounding:
 // FP32 products with FP32 phasors after an exact FP64 range reduction, FP64
 // sums across timesteps, as against its f32 intermediates); with several,
@@ -62,15 +66,18 @@ struct SweepArgs {
     const float* w;         // [nt][nf][nbl]
     const JonesF32* models; // [nsrc][nt][nf][nbl], source frames (general sources)
     const JonesF32* ptab;   // [nsrc][nt][nf]: point-at-centre sources' models, or null
-    const UVW* uv_pc;       // [nt][nbl]
-    const UVW* uv_src;      // [nsrc][nt][nbl]
-    const double* lambdas;  // [nf]
-    const double* inv_lambdas;  // [nf] 1 / lambda: the rotation phases multiply instead of dividing
+    // per-tile phasors [nsrc][nt][nf][ntiles]; a baseline's factor is
+    // tab[p] conj(tab[q]) for its tiles p, q (the phases are differences of
+    // per-tile phases, since uvw_pq = uvw_p - uvw_q)
+    const float2* rot;      // exp(-2 pi i (w_src,p - w_pc,p) / lambda): to the source frame
+    const float2* io_old;   // exp(-2 pi i (alpha u_p + beta v_p) lambda) of the old constants
+    const float2* ap_old;   // conj(rot) io_old (apply sweep)
+    const float2* ap_new;   // conj(rot) io_new (apply sweep)
     const IonoConsts* old;  // [nsrc]
     const IonoConsts* neu;  // [nsrc] (apply sweep)
     JonesF32* d_lo;         // [nsrc][nlo][nbl]
     JonesF32* m_lo;         // [nsrc][nlo][nbl]
-    int nt, nf, nbl, nsrc, favg;
+    int nt, nf, nbl, ntiles, nsrc, favg;
 };
 
 // exp(i arg) as (cos, sin): the argument (radians) in FP64, reduced exactly
@@ -83,16 +90,56 @@ __device__ __forceinline__ float2 phase_f(double arg) {
     return make_float2(cs, sn);
 }
 
-// iono factor g exp(-2 pi i (u alpha + v beta) lambda), as add_model / subtract_iono
-__device__ __forceinline__ float2 iono_f(const IonoConsts& k, const UVW& q, double lam) {
-    if (k.alpha == 0.0 && k.beta == 0.0) return make_float2((float)k.gain, 0.f);
-    const float2 p = phase_f(-TAU * (q.u * k.alpha + q.v * k.beta) * lam);
-    const float g = (float)k.gain;
-    return make_float2(p.x * g, p.y * g);
-}
-
 __device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
     return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+// a conj(b)
+__device__ __forceinline__ float2 cmulcf(float2 a, float2 b) {
+    return make_float2(fmaf(a.x, b.x, a.y * b.y), fmaf(a.y, b.x, -a.x * b.y));
+}
+
+// per-tile UVWs [frame][t][tile] in the frames of the sources (0 .. ns - 1)
+// and the phase centre (ns), as xyzs_to_uvws computes them for baselines
+__global__ void tile_uvw_kernel(const XYZ* __restrict__ xyz, const double* __restrict__ lmsts,
+                                const double2* __restrict__ radec, int nframes, int nt, int ntiles, UVW* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nframes * nt * ntiles) return;
+    const int p = i % ntiles, t = (i / ntiles) % nt, fr = i / (ntiles * nt);
+    const XYZ a = xyz[(size_t)t * ntiles + p];
+    double s_ha, c_ha, s_dec, c_dec;
+    sincos(radec[fr].y, &s_dec, &c_dec);
+    sincos(lmsts[t] - radec[fr].x, &s_ha, &c_ha);
+    out[i] = UVW{s_ha * a.x + c_ha * a.y, -s_dec * c_ha * a.x + s_dec * s_ha * a.y + c_dec * a.z,
+                 c_dec * c_ha * a.x - c_dec * s_ha * a.y + s_dec * a.z};
+}
+
+// rot[s][t][f][p] = exp(-2 pi i (w_s,p - w_pc,p) / lambda_f)
+__global__ void rot_table_kernel(const UVW* __restrict__ tuvw, const double* __restrict__ inv_lam, int ns, int nt,
+                                 int nf, int ntiles, float2* __restrict__ rot) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)ns * nt * nf * ntiles) return;
+    const int p = (int)(i % ntiles), f = (int)((i / ntiles) % nf), t = (int)((i / ((size_t)ntiles * nf)) % nt);
+    const int src = (int)(i / ((size_t)ntiles * nf * nt));
+    const double dw = tuvw[((size_t)src * nt + t) * ntiles + p].w - tuvw[((size_t)ns * nt + t) * ntiles + p].w;
+    rot[i] = phase_f(-TAU * dw * inv_lam[f]);
+}
+
+// out[s][t][f][p] = [conj(rot) x] exp(-2 pi i (alpha u_s,p + beta v_s,p) lambda_f),
+// the ionospheric phase exactly 1 when alpha = beta = 0 (as add_model skips it)
+__global__ void iono_table_kernel(const UVW* __restrict__ tuvw, const double* __restrict__ lam,
+                                  const IonoConsts* __restrict__ k, const float2* __restrict__ rot, int ns, int nt,
+                                  int nf, int ntiles, float2* __restrict__ out) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)ns * nt * nf * ntiles) return;
+    const int p = (int)(i % ntiles), f = (int)((i / ntiles) % nf), t = (int)((i / ((size_t)ntiles * nf)) % nt);
+    const int src = (int)(i / ((size_t)ntiles * nf * nt));
+    const IonoConsts c = k[src];
+    float2 v = make_float2(1.f, 0.f);
+    if (c.alpha != 0.0 || c.beta != 0.0) {
+        const UVW q = tuvw[((size_t)src * nt + t) * ntiles + p];
+        v = phase_f(-TAU * (q.u * c.alpha + q.v * c.beta) * lam[f]);
+    }
+    out[i] = rot ? cmulcf(v, rot[i]) : v;
 }
 
 // a Jones matrix as four complex FP32 numbers
@@ -124,22 +171,24 @@ __global__ void __launch_bounds__(BX* SY) accumulate_kernel(const SweepArgs A) {
     const int src = (int)(blockIdx.x % ngrp) * SY + threadIdx.y;
     if (bin >= nlo * A.nbl || src >= A.nsrc) return;
     const int bl = bin % A.nbl, flo = bin / A.nbl;
-    const IonoConsts k = A.old[src];
+    int tp, tq;
+    baseline_to_tiles(bl, A.ntiles, tp, tq);
+    const float g = (float)A.old[src].gain;
     const size_t nvis = (size_t)A.nt * A.nf * A.nbl;
     const JonesF32* M = A.ptab ? nullptr : A.models + (size_t)src * nvis;
     double acc_d[8] = {0, 0, 0, 0, 0, 0, 0, 0}, acc_m[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     double ws = 0.0;
     for (int t = 0; t < A.nt; t++) {
-        const UVW q = A.uv_src[((size_t)src * A.nt + t) * A.nbl + bl];
-        const double dw = q.w - A.uv_pc[(size_t)t * A.nbl + bl].w;
         float2 sd[4] = {}, sm[4] = {};
         float sw = 0.f;
 #pragma unroll 4  // several channels' loads in flight at once
         for (int fc = flo * A.favg; fc < flo * A.favg + A.favg; fc++) {
             const size_t i = ((size_t)t * A.nf + fc) * A.nbl + bl;
             const float wt = A.w[i];
-            const float2 rot = phase_f(-TAU * dw * A.inv_lambdas[fc]);
-            const float2 io = iono_f(k, q, A.lambdas[fc]);
+            const size_t tb = (((size_t)src * A.nt + t) * A.nf + fc) * A.ntiles;
+            const float2 rot = cmulcf(A.rot[tb + tp], A.rot[tb + tq]);
+            const float2 io1 = cmulcf(A.io_old[tb + tp], A.io_old[tb + tq]);
+            const float2 io = make_float2(io1.x * g, io1.y * g);
             const JF mj = load_jf(A.ptab ? A.ptab[((size_t)src * A.nt + t) * A.nf + fc] : M[i]);
             const JF r = load_jf(A.resid[i]);
 #pragma unroll
@@ -171,7 +220,9 @@ __global__ void __launch_bounds__(BX* SY) accumulate_kernel(const SweepArgs A) {
 }
 
 // one thread per high-resolution visibility; all sources' updates, summed in
-// FP32 and added to the residual once
+// FP32 and added to the residual once:
+//   R += sum_s M_s conj(rot_s) (g_old io_old - g_new io_new)
+// with conj(rot) io per baseline = ap[p] conj(ap[q]) from the per-tile tables
 __global__ void __launch_bounds__(256) apply_kernel(JonesF32* resid, const SweepArgs A) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     const size_t nvis = (size_t)A.nt * A.nf * A.nbl;
@@ -179,16 +230,17 @@ __global__ void __launch_bounds__(256) apply_kernel(JonesF32* resid, const Sweep
     const int bl = (int)(i % A.nbl);
     const int f = (int)((i / A.nbl) % A.nf);
     const int t = (int)(i / ((size_t)A.nbl * A.nf));
-    const double lam = A.lambdas[f], ilam = A.inv_lambdas[f];
-    const double wpc = A.uv_pc[(size_t)t * A.nbl + bl].w;
+    int tp, tq;
+    baseline_to_tiles(bl, A.ntiles, tp, tq);
     float2 dl[4] = {};
     for (int s = 0; s < A.nsrc; s++) {
-        const UVW q = A.uv_src[((size_t)s * A.nt + t) * A.nbl + bl];
-        const float2 io = iono_f(A.old[s], q, lam), in = iono_f(A.neu[s], q, lam);
-        const float2 d = make_float2(io.x - in.x, io.y - in.y);
-        if (d.x == 0.f && d.y == 0.f) continue;
-        const float2 back = phase_f(TAU * (q.w - wpc) * ilam);  // conj of the rotation to the source
-        const float2 bd = cmulf(back, d);
+        const IonoConsts ko = A.old[s], kn = A.neu[s];
+        if (ko.alpha == kn.alpha && ko.beta == kn.beta && ko.gain == kn.gain) continue;
+        const size_t tb = (((size_t)s * A.nt + t) * A.nf + f) * A.ntiles;
+        const float2 po = cmulcf(A.ap_old[tb + tp], A.ap_old[tb + tq]);
+        const float2 pn = cmulcf(A.ap_new[tb + tp], A.ap_new[tb + tq]);
+        const float go = (float)ko.gain, gn = (float)kn.gain;
+        const float2 bd = make_float2(fmaf(go, po.x, -gn * pn.x), fmaf(go, po.y, -gn * pn.y));
         const JF m = load_jf(A.ptab ? A.ptab[((size_t)s * A.nt + t) * A.nf + f] : A.models[(size_t)s * nvis + i]);
 #pragma unroll
         for (int e = 0; e < 4; e++) {
@@ -359,15 +411,22 @@ extern "C" int hdc_peel_timeblock_batched(JonesF32* d_resid_tfb, const float* d_
                   need >> 20, free_b >> 20);
         return HDC_ERR_ALLOC;
     }
-    pb::DevBuf b_lam, b_lam_lo, b_lmst, b_avg_lmst, b_xyz, b_uv_pc, b_uv_src, b_uv_lo, b_models, b_dlo, b_mlo, b_mlo_rot,
+    pb::DevBuf b_tuvw, b_radec, b_rot, b_io, b_apo, b_apn;
+    pb::DevBuf b_lam, b_lam_lo, b_lmst, b_avg_lmst, b_xyz, b_uv_src, b_uv_lo, b_models, b_dlo, b_mlo, b_mlo_rot,
         b_wlo, b_scr, b_old, b_new;
     PB_CK(b_lam.alloc(sizeof(double) * 2 * nf, s));  // lambda, then 1 / lambda
     PB_CK(b_lam_lo.alloc(sizeof(double) * nlo, s));
     PB_CK(b_lmst.alloc(sizeof(double) * nt, s));
     PB_CK(b_avg_lmst.alloc(sizeof(double), s));
     PB_CK(b_xyz.alloc(sizeof(XYZ) * xyz_t.size(), s));
-    PB_CK(b_uv_pc.alloc(sizeof(UVW) * (size_t)nt * nbl, s));
-    PB_CK(b_uv_src.alloc(sizeof(UVW) * (size_t)ns * nt * nbl, s));
+    if (!points) PB_CK(b_uv_src.alloc(sizeof(UVW) * (size_t)ns * nt * nbl, s));
+    const size_t ntab = (size_t)ns * nt * nf * num_tiles;  // per-tile phasor tables
+    PB_CK(b_tuvw.alloc(sizeof(UVW) * (size_t)(ns + 1) * nt * num_tiles, s));
+    PB_CK(b_radec.alloc(sizeof(double2) * (ns + 1), s));
+    PB_CK(b_rot.alloc(sizeof(float2) * ntab, s));
+    PB_CK(b_io.alloc(sizeof(float2) * ntab, s));
+    PB_CK(b_apo.alloc(sizeof(float2) * ntab, s));
+    PB_CK(b_apn.alloc(sizeof(float2) * ntab, s));
     PB_CK(b_uv_lo.alloc(sizeof(UVW) * (size_t)ns * nbl, s));
     PB_CK(points ? b_models.alloc(need, s) : b_models.alloc_plain(need));
     PB_CK(b_dlo.alloc(sizeof(JonesF32) * (size_t)ns * nlo * nbl, s));
@@ -383,13 +442,29 @@ extern "C" int hdc_peel_timeblock_batched(JonesF32* d_resid_tfb, const float* d_
     PB_CK(cudaMemcpyAsync(b_avg_lmst.p, &average_lmst, sizeof(double), cudaMemcpyHostToDevice, s));
     PB_CK(cudaMemcpyAsync(b_xyz.p, xyz_t.data(), sizeof(XYZ) * xyz_t.size(), cudaMemcpyHostToDevice, s));
     PB_CK(k_weights_average(d_weights_tfb, b_wlo.as<float>(), nt, nbl, nf, favg, s));
-    PB_CK(k_xyzs_to_uvws(b_xyz.as<XYZ>(), b_lmst.as<double>(), b_uv_pc.as<UVW>(), phase_centre, num_tiles, nbl, nt, s));
+    // per-tile UVWs in every source's frame and the phase centre's, and the
+    // rotation phasors to each source (fixed for the timeblock)
+    std::vector<double2> radec(ns + 1);
+    for (int i = 0; i < ns; i++) radec[i] = make_double2(h_source_positions[i].ra, h_source_positions[i].dec);
+    radec[ns] = make_double2(phase_centre.ra, phase_centre.dec);
+    PB_CK(cudaMemcpyAsync(b_radec.p, radec.data(), sizeof(double2) * (ns + 1), cudaMemcpyHostToDevice, s));
+    {
+        const int n = (ns + 1) * nt * num_tiles;
+        pb::tile_uvw_kernel<<<(n + 255) / 256, 256, 0, s>>>(b_xyz.as<XYZ>(), b_lmst.as<double>(),
+                                                            b_radec.as<double2>(), ns + 1, nt, num_tiles,
+                                                            b_tuvw.as<UVW>());
+        pb::rot_table_kernel<<<(unsigned)((ntab + 255) / 256), 256, 0, s>>>(
+            b_tuvw.as<UVW>(), b_lam.as<double>() + nf, ns, nt, nf, num_tiles, b_rot.as<float2>());
+        count_launches(2);
+        PB_CK(cudaGetLastError());
+    }
     PB_CK(cudaMemsetAsync(b_models.p, 0, need, s));
     // per source: UVWs in its frame and its high-resolution model (once per
     // timeblock)
     for (int i = 0; i < ns; i++) {
-        UVW* uv = b_uv_src.as<UVW>() + (size_t)i * nt * nbl;
-        PB_CK(k_xyzs_to_uvws(b_xyz.as<XYZ>(), b_lmst.as<double>(), uv, h_source_positions[i], num_tiles, nbl, nt, s));
+        if (!points)
+            PB_CK(k_xyzs_to_uvws(b_xyz.as<XYZ>(), b_lmst.as<double>(), b_uv_src.as<UVW>() + (size_t)i * nt * nbl,
+                                 h_source_positions[i], num_tiles, nbl, nt, s));
         PB_CK(k_xyzs_to_uvws(b_xyz.as<XYZ>(), b_avg_lmst.as<double>(), b_uv_lo.as<UVW>() + (size_t)i * nbl,
                              h_source_positions[i], num_tiles, nbl, 1, s));
     }
@@ -449,10 +524,10 @@ extern "C" int hdc_peel_timeblock_batched(JonesF32* d_resid_tfb, const float* d_
     A.w = d_weights_tfb;
     A.models = points ? nullptr : b_models.as<JonesF32>();
     A.ptab = points ? b_models.as<JonesF32>() : nullptr;
-    A.uv_pc = b_uv_pc.as<UVW>();
-    A.uv_src = b_uv_src.as<UVW>();
-    A.lambdas = b_lam.as<double>();
-    A.inv_lambdas = b_lam.as<double>() + nf;
+    A.rot = b_rot.as<float2>();
+    A.io_old = b_io.as<float2>();
+    A.ap_old = b_apo.as<float2>();
+    A.ap_new = b_apn.as<float2>();
     A.old = b_old.as<IonoConsts>();
     A.neu = b_new.as<IonoConsts>();
     A.d_lo = b_dlo.as<JonesF32>();
@@ -460,12 +535,18 @@ extern "C" int hdc_peel_timeblock_batched(JonesF32* d_resid_tfb, const float* d_
     A.nt = nt;
     A.nf = nf;
     A.nbl = nbl;
+    A.ntiles = num_tiles;
     A.nsrc = ns;
     A.favg = favg;
     const size_t nbins = (size_t)nlo * nbl;
     std::vector<IonoConsts> fit(ns), next(ns);
     for (int pass = 0; pass < params->num_passes; pass++) {
         PB_CK(cudaMemcpyAsync(b_old.p, h_iono_consts, sizeof(IonoConsts) * ns, cudaMemcpyHostToDevice, s));
+        const unsigned tgrid = (unsigned)((ntab + 255) / 256);
+        pb::iono_table_kernel<<<tgrid, 256, 0, s>>>(b_tuvw.as<UVW>(), b_lam.as<double>(), b_old.as<IonoConsts>(),
+                                                    nullptr, ns, nt, nf, num_tiles, b_io.as<float2>());
+        count_launches(1);
+        PB_CK(cudaGetLastError());
         const int v = pb::choose_variant(A, s);
         pb::kVariants[v].launch(A, s);
         PB_CK(cudaGetLastError());
@@ -486,6 +567,12 @@ extern "C" int hdc_peel_timeblock_batched(JonesF32* d_resid_tfb, const float* d_
             next[i] = c;
         }
         PB_CK(cudaMemcpyAsync(b_new.p, next.data(), sizeof(IonoConsts) * ns, cudaMemcpyHostToDevice, s));
+        pb::iono_table_kernel<<<tgrid, 256, 0, s>>>(b_tuvw.as<UVW>(), b_lam.as<double>(), b_old.as<IonoConsts>(),
+                                                    b_rot.as<float2>(), ns, nt, nf, num_tiles, b_apo.as<float2>());
+        pb::iono_table_kernel<<<tgrid, 256, 0, s>>>(b_tuvw.as<UVW>(), b_lam.as<double>(), b_new.as<IonoConsts>(),
+                                                    b_rot.as<float2>(), ns, nt, nf, num_tiles, b_apn.as<float2>());
+        count_launches(2);
+        PB_CK(cudaGetLastError());
         pb::apply_kernel<<<(unsigned)((nvis + 255) / 256), 256, 0, s>>>(d_resid_tfb, A);
         count_launches(1);
         PB_CK(cudaGetLastError());
