@@ -27,8 +27,8 @@
 // tables [source][timestep][channel][tile] -- 128 phasors where a baseline
 // loop would evaluate 8128 -- and a baseline takes tab[p] conj(tab[q]).
 // With one source this is the reference's sequence exactly (up to rounding:
-// FP32 products with FP32 phasors after an exact FP64 range reduction, FP64
-// sums across timesteps, as against its f32 intermediates); with several,
+// FP32 products and sums with FP32 phasors after an exact FP64 range
+// reduction, as against its f32 intermediates); with several,
 // sources
 // fitted in the same pass do not see each other's updates until the next
 // pass.  The source models M_s (high resolution, source frame) are predicted
@@ -160,11 +160,11 @@ __device__ __forceinline__ JonesF32 to_f32(const J2& v) {
 // blockDim (BX, SY): x = low-resolution bins, y = sources of this CTA's chunk
 // Grid: one dimension, source groups fastest -- the CTAs of all source
 // groups of a bin block run close together, so each residual tile comes
-// from DRAM once and from L2 for the other sources.  Products are formed in
-// FP32 (the data are FP32) and summed in FP32 over one timestep's channels
-// of the bin, then in FP64 across timesteps.
+// from DRAM once and from L2 for the other sources.  Products are formed and
+// summed in FP32 (the data are FP32; a bin sums nt x favg = 128 samples,
+// ~1e-7 relative rounding), at 64 registers so that 4 CTAs share an SM.
 template <int BX, int SY>
-__global__ void __launch_bounds__(BX* SY) accumulate_kernel(const SweepArgs A) {
+__global__ void __launch_bounds__(BX* SY, 4) accumulate_kernel(const SweepArgs A) {
     const int nlo = A.nf / A.favg;
     const int ngrp = (A.nsrc + SY - 1) / SY;
     const int bin = (int)(blockIdx.x / ngrp) * BX + threadIdx.x;
@@ -176,12 +176,9 @@ __global__ void __launch_bounds__(BX* SY) accumulate_kernel(const SweepArgs A) {
     const float g = (float)A.old[src].gain;
     const size_t nvis = (size_t)A.nt * A.nf * A.nbl;
     const JonesF32* M = A.ptab ? nullptr : A.models + (size_t)src * nvis;
-    double acc_d[8] = {0, 0, 0, 0, 0, 0, 0, 0}, acc_m[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    double ws = 0.0;
+    float2 sd[4] = {}, sm[4] = {};
+    float sw = 0.f;
     for (int t = 0; t < A.nt; t++) {
-        float2 sd[4] = {}, sm[4] = {};
-        float sw = 0.f;
-#pragma unroll 4  // several channels' loads in flight at once
         for (int fc = flo * A.favg; fc < flo * A.favg + A.favg; fc++) {
             const size_t i = ((size_t)t * A.nf + fc) * A.nbl + bl;
             const float wt = A.w[i];
@@ -202,13 +199,10 @@ __global__ void __launch_bounds__(BX* SY) accumulate_kernel(const SweepArgs A) {
             }
             sw += wt;
         }
-#pragma unroll
-        for (int e = 0; e < 4; e++) {
-            acc_d[2 * e] += sd[e].x, acc_d[2 * e + 1] += sd[e].y;
-            acc_m[2 * e] += sm[e].x, acc_m[2 * e + 1] += sm[e].y;
-        }
-        ws += sw;
     }
+    const double ws = sw;
+    const double acc_d[8] = {sd[0].x, sd[0].y, sd[1].x, sd[1].y, sd[2].x, sd[2].y, sd[3].x, sd[3].y};
+    const double acc_m[8] = {sm[0].x, sm[0].y, sm[1].x, sm[1].y, sm[2].x, sm[2].y, sm[3].x, sm[3].y};
     const double inv = 1.0 / (ws > 0.0 ? ws : 1.0);
     const size_t o = ((size_t)src * nlo + flo) * A.nbl + bl;
     A.d_lo[o] = JonesF32{(float)(acc_d[0] * inv), (float)(acc_d[1] * inv), (float)(acc_d[2] * inv),
