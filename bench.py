@@ -744,6 +744,16 @@ def gpu_arm(args, rank, world, local_rank):
                      "peak_source": f"{'FP32' if fast else 'FP64'} FMA probe kernel measured in this run"}
         entry.update({"achieved": flops / t_launch / 1e12, "unit": "TFLOP/s", "traffic": None,
                       "ms_per_step": per_step_ms[k]})
+        if k == 0 and form == "tensor":
+            # what the tensor pipe executes: 18 kind::i8 MMAs of 128 x 128 x 32 per 32-component stage of each
+            # (channel, polarisation, column half) CTA, against 8190 int8 MAC/clk/SM (a probe of back-to-back
+            # kind::i8 MMAs) at this run's median SM clock
+            macs = nf * 6 * ((npts + 31) // 32) * 18 * 128 * 128 * 32
+            n_sm = torch.cuda.get_device_properties(0).multi_processor_count
+            mhz = (clk or {}).get("sm_mhz") or 1965.0
+            entry["int8_mma"] = {"executed_macs_per_s": macs / t_launch,
+                                 "peak_macs_per_s": 8190.0 * n_sm * mhz * 1e6,
+                                 "frac": macs / t_launch / (8190.0 * n_sm * mhz * 1e6)}
         entry["frac"] = entry["achieved"] / entry["peak"]
         by_class[names[k]] = entry
     roofline = dict(by_class[names[dom]])
