@@ -14,6 +14,7 @@ import numpy as np
 import pytest
 
 from mwa_hyperdrive_b200 import srclist as sl
+from mwa_hyperdrive_b200 import synth
 
 GOLD = Path(__file__).resolve().parent / "golden"
 KATS = json.loads((GOLD / "model_kats.json").read_text())
@@ -216,3 +217,65 @@ def test_list_flux_edge_cases(oracle):
     si = math.log(4.0) / math.log(2.0)
     assert est([(100e6, 1.0), (200e6, 4.0)], 300e6) == pytest.approx(4.0 * 1.5 ** si, rel=1e-14)
     assert est([(100e6, 1.0), (200e6, 4.0)], 50e6) == pytest.approx(0.5 ** si, rel=1e-14)
+
+
+def _c(a):
+    """[...][8] -> [...][2][2] complex."""
+    return (a[..., 0::2] + 1j * a[..., 1::2]).reshape(a.shape[:-1] + (2, 2))
+
+
+def _mitchcal_numpy(data, model, ntiles, iters, top_then_inverse):
+    """A small MitchCal on one chanblock (di_calibrate/mod.rs:640-893 without
+    the stopping rules): G_p <- top_p bot_p^-1, top = sum_q D_pq G_q M_pq^H,
+    bot = sum_q (M_pq G_q^H)(M_pq G_q^H)^H, averaged with the previous
+    iterate every second iteration.  With top_then_inverse False the product
+    is taken the other way round, bot^-1 top."""
+    i, j = np.triu_indices(ntiles, 1)
+    D, M = _c(data.astype(np.float64)), _c(model.astype(np.float64))  # [t][bl][2][2]
+    G = np.broadcast_to(np.eye(2, dtype=complex), (ntiles, 2, 2)).copy()
+    for it in range(iters):
+        top = np.zeros_like(G)
+        bot = np.zeros_like(G)
+        for p, q, b in zip(i, j, range(len(i))):
+            for t in range(D.shape[0]):
+                # both directions of the baseline
+                z = M[t, b] @ G[q].conj().T
+                top[p] += D[t, b] @ G[q] @ M[t, b].conj().T
+                bot[p] += z @ z.conj().T
+                zq = M[t, b].conj().T @ G[p].conj().T
+                top[q] += D[t, b].conj().T @ G[p] @ M[t, b]
+                bot[q] += zq @ zq.conj().T
+        new = np.stack([top[k] @ np.linalg.inv(bot[k]) if top_then_inverse else np.linalg.inv(bot[k]) @ top[k]
+                        for k in range(ntiles)])
+        G = 0.5 * (G + new) if it % 2 == 1 else new
+    return G
+
+
+def _residual(G, data, model, ntiles):
+    i, j = np.triu_indices(ntiles, 1)
+    D, M = _c(data.astype(np.float64)), _c(model.astype(np.float64))
+    P = G[i][None] @ M @ np.conj(np.swapaxes(G[j], -1, -2))[None]
+    return np.linalg.norm(P - D) / np.linalg.norm(D)
+
+
+def test_mitchcal_division_order(oracle):
+    """The Jones "division" of the update is top . bot^-1 (marlu's Jones /,
+    di_calibrate/mod.rs:663-681).  With leaky, non-diagonal gains and a
+    polarised model the two orders differ: top . bot^-1 reproduces noiseless
+    data and bot^-1 . top does not; the oracle's solver reproduces the data
+    as the first does."""
+    rng = np.random.default_rng(21)
+    ntiles, nt, nch = 8, 2, 1
+    nbl = ntiles * (ntiles - 1) // 2
+    model = synth.polarised_model(nt, nch, nbl, rng)
+    gains = synth.truth_gains(ntiles, nch, rng, amp_sigma=0.1, leak_sigma=0.15)
+    data = synth.corrupt(model, gains)
+    d1, m1 = data[:, 0], model[:, 0]
+    right = _residual(_mitchcal_numpy(d1, m1, ntiles, 200, True), d1, m1, ntiles)
+    wrong = _residual(_mitchcal_numpy(d1, m1, ntiles, 200, False), d1, m1, ntiles)
+    assert right < 1e-5 and wrong > 1e-1, (right, wrong)
+    ident = np.zeros((ntiles, nch, 8))
+    ident[..., 0] = ident[..., 6] = 1.0
+    dj, res = oracle.calibrate_timeblock(data, model, ident, 0, nt, 200, 1e-12, 1e-4, 0)
+    G = _c(dj[:, 0])
+    assert _residual(G, d1, m1, ntiles) < 1e-5
