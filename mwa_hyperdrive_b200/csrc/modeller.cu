@@ -803,6 +803,17 @@ int Modeller::model_host_pipelined(double lst, JonesF32* h_vis, UVW* h_uvws, cud
         for (int k = 1; k < PIPE_CHUNKS - 2; k++)
             bounds[1 + k] = edge + (int)((long long)(nf - 2 * edge) * k / (PIPE_CHUNKS - 2));
         bounds[PIPE_CHUNKS - 1] = nf - edge;
+        // the tensor point predict runs one CTA per SM and six per channel:
+        // middle chunks of a whole number of waves (all but the last) leave no
+        // partly filled wave behind
+        int n_sm = 0, dev = 0;
+        if (t[0].nc > 0 && form == HDC_PREDICT_TENSOR && cudaGetDevice(&dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && n_sm >= 6) {
+            const int mid = nf - 2 * edge, per = (mid + PIPE_CHUNKS - 3) / (PIPE_CHUNKS - 2);
+            const int waves = (6 * per + n_sm - 1) / n_sm, c = waves * n_sm / 6;
+            if (c >= 1 && (long long)c * (PIPE_CHUNKS - 3) < mid)
+                for (int k = 1; k < PIPE_CHUNKS - 2; k++) bounds[1 + k] = edge + k * c;
+        }
         bounds[PIPE_CHUNKS] = nf;
     } else {
         nch = std::min(PIPE_CHUNKS, nf);
