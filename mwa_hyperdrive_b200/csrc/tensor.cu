@@ -70,6 +70,7 @@ constexpr int NH = 64;     // tile columns per CTA
 constexpr int NB = 2 * NH; // MMA N: [Re | Im] of the NH columns
 constexpr int KC = 32;     // components per stage = MMA K (bytes)
 constexpr int NSTAGE = 4;
+constexpr int CRING = NSTAGE + 2;  // component-data ring: producer warps may be NSTAGE stages apart
 constexpr int NPW = 16;    // producer / epilogue warps
 constexpr int NPT = NPW * 32;   // producer threads
 constexpr int THREADS = NPT + 32;
@@ -213,7 +214,8 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const Params P) {
     __shared__ uint32_t tmem_base_s;
     __shared__ double red_s[THREADS / 32];
     __shared__ volatile int abort_s;
-    __shared__ __align__(16) CompStage comp_s[3];
+    __shared__ __align__(16) CompStage comp_s[CRING];
+    __shared__ alignas(8) uint64_t comp_bar[CRING];
 
     unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     const int f = blockIdx.x;
@@ -233,9 +235,10 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const Params P) {
     if (lane == 0) red_s[warp] = mx;
     if (tid == 0) {
         for (int s = 0; s < NSTAGE; s++) {
-            mbar_init(&full_bar[s], 1);
+            mbar_init(&full_bar[s], NPT);  // every producer thread arrives
             mbar_init(&empty_bar[s], 1);
         }
+        for (int s = 0; s < CRING; s++) mbar_init(&comp_bar[s], KC);  // the KC stashing threads arrive
         mbar_init(&done_bar, 1);
         abort_s = 0;
         fence_barrier_init();
@@ -320,7 +323,7 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const Params P) {
         // its last reader.  Stages past the end read zeros (their values are
         // never written out).
         auto compute = [&](int k, int (&xr)[2][4], int (&xi)[2][4], int (&yr)[4], int (&yi)[4], int (&yn)[4]) {
-            const CompStage& cs_ = comp_s[k % 3];
+            const CompStage& cs_ = comp_s[k % CRING];
             double cl[4], cm[4], cn[4];
             float wr[4], wi[4];
 #pragma unroll
@@ -389,30 +392,40 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const Params P) {
         producers_sync_or(false);
         int xr[2][4], xi[2][4], yr[4], yi[4], yn[4];
         compute(0, xr, xi, yr, yi, yn);
+        // The producer warps run decoupled: each thread arrives on a stage's
+        // full barrier once its planes are written, a warp waits for the
+        // tensor core only on the buffer it is about to overwrite, and for
+        // the component data only on the ring slot it is about to read (so
+        // warps may drift up to NSTAGE stages apart; the ring has room for
+        // that).  Any timeout sets abort_s; the others leave at their next
+        // stage or their own bounded wait.
+        static_assert(KC == 32, "warp 0 stashes the component data");
         for (int k = 0; k < nchunks; k++) {
             const int st = k % NSTAGE;
             double2 na, nb, nw;  // stage k + 2's component data, in flight during this stage
             const bool pre = tid < KC;
             if (pre) fetch(k + 2, na, nb, nw);
-            int nxr[2][4], nxi[2][4], nyr[4], nyi[4], nyn[4];
-            write_planes(st, xr, xi, yr, yi, yn);
-            compute(k + 1, nxr, nxi, nyr, nyi, nyn);
-            fence_proxy_async_smem();  // make the generic-proxy stores visible to the tensor core
-            if (pre) stash((k + 2) % 3, na, nb, nw);
-            // before the barrier, thread 0 waits until the next iteration's
-            // stage has been read by the tensor core; the barrier then both
-            // publishes this stage (one arrive on its full barrier) and frees
-            // everyone to write the next.  One decision for all producers:
-            // leave together on any timeout.
-            bool bad = false;
-            if (tid == 0 && k + 1 >= NSTAGE && k + 1 < nchunks)
-                bad = !mbar_wait_bounded(&empty_bar[(k + 1) % NSTAGE], (((k + 1) / NSTAGE) - 1) & 1, P.err);
-            const bool stop = producers_sync_or(bad || abort_s != 0);
-            if (tid == 0) mbar_arrive(&full_bar[st]);
-            if (stop) {
+            if (k >= NSTAGE && !__all_sync(0xffffffffu, mbar_wait_bounded(&empty_bar[st], ((k / NSTAGE) - 1) & 1, P.err))) {
                 abort_s = 1;
                 break;
             }
+            int nxr[2][4], nxi[2][4], nyr[4], nyi[4], nyn[4];
+            write_planes(st, xr, xi, yr, yi, yn);
+            // stage k + 1's component data: stages 0 and 1 were published by
+            // the barrier above, later ones by warp 0 in its iteration k - 1
+            if (k + 1 >= 2 && !__all_sync(0xffffffffu, mbar_wait_bounded(&comp_bar[(k + 1) % CRING],
+                                                                           ((k - 1) / CRING) & 1, P.err))) {
+                abort_s = 1;
+                break;
+            }
+            compute(k + 1, nxr, nxi, nyr, nyi, nyn);
+            fence_proxy_async_smem();  // make the generic-proxy stores visible to the tensor core
+            mbar_arrive(&full_bar[st]);
+            if (pre) {
+                stash((k + 2) % CRING, na, nb, nw);
+                mbar_arrive(&comp_bar[(k + 2) % CRING]);
+            }
+            if (abort_s != 0) break;
 #pragma unroll
             for (int j = 0; j < 4; j++) {
                 xr[0][j] = nxr[0][j], xr[1][j] = nxr[1][j], xi[0][j] = nxi[0][j], xi[1][j] = nxi[1][j];
