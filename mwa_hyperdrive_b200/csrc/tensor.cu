@@ -235,10 +235,10 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const Params P) {
     if (lane == 0) red_s[warp] = mx;
     if (tid == 0) {
         for (int s = 0; s < NSTAGE; s++) {
-            mbar_init(&full_bar[s], NPT);  // every producer thread arrives
+            mbar_init(&full_bar[s], NPW);  // one arrival per producer warp
             mbar_init(&empty_bar[s], 1);
         }
-        for (int s = 0; s < CRING; s++) mbar_init(&comp_bar[s], KC);  // the KC stashing threads arrive
+        for (int s = 0; s < CRING; s++) mbar_init(&comp_bar[s], 1);  // the stashing warp arrives once
         mbar_init(&done_bar, 1);
         abort_s = 0;
         fence_barrier_init();
@@ -420,10 +420,11 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const Params P) {
             }
             compute(k + 1, nxr, nxi, nyr, nyi, nyn);
             fence_proxy_async_smem();  // make the generic-proxy stores visible to the tensor core
-            mbar_arrive(&full_bar[st]);
-            if (pre) {
-                stash((k + 2) % CRING, na, nb, nw);
-                mbar_arrive(&comp_bar[(k + 2) % CRING]);
+            if (pre) stash((k + 2) % CRING, na, nb, nw);
+            __syncwarp();  // the lanes' stores and fences before the warp's one arrival
+            if (lane == 0) {
+                mbar_arrive(&full_bar[st]);
+                if (pre) mbar_arrive(&comp_bar[(k + 2) % CRING]);
             }
             if (abort_s != 0) break;
 #pragma unroll
