@@ -138,6 +138,57 @@ __device__ __forceinline__ void shapelet_envelope_dense(const DirectParams& p, c
     shapelet_dense_at(p, cm, x * g.x + SBF_C, y * g.y + SBF_C, er, ei);
 }
 
+// shapelet_dense_at for N channels of one component at once: the basis of
+// each channel is interpolated as there, and each row of the coefficient
+// matrix is read from shared memory once (three 8-byte loads) for all N
+// channels; same arithmetic order per channel
+template <int N>
+__device__ __forceinline__ void shapelet_dense_multi(const DirectParams& p, const float* __restrict__ cm,
+                                                     const double (&x_pos)[N], const double (&y_pos)[N],
+                                                     float (&er)[N], float (&ei)[N]) {
+    float X[N][SDN], Y[N][SDN];
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        const double fx = floor(x_pos[i]), fy = floor(y_pos[i]);
+        const int xi = fx > 0.0 ? (int)fmin(fx, (double)(SBF_L - 2)) : 0;
+        const int yi = fy > 0.0 ? (int)fmin(fy, (double)(SBF_L - 2)) : 0;
+        const float xfrac = (float)(x_pos[i] - fx), yfrac = (float)(y_pos[i] - fy);
+#pragma unroll
+        for (int h = 0; h < SDN / 2; h++) {
+            const float4 a = __ldg(p.sbfp + (size_t)xi * (SDN / 2) + h);
+            const float4 b = __ldg(p.sbfp + (size_t)yi * (SDN / 2) + h);
+            X[i][2 * h] = fmaf(a.y, xfrac, a.x);
+            X[i][2 * h + 1] = fmaf(a.w, xfrac, a.z);
+            Y[i][2 * h] = fmaf(b.y, yfrac, b.x);
+            Y[i][2 * h + 1] = fmaf(b.w, yfrac, b.z);
+        }
+        er[i] = 0.f, ei[i] = 0.f;
+    }
+    const float2* row = reinterpret_cast<const float2*>(cm);
+#pragma unroll
+    for (int n1 = 0; n1 < SDN; n1++) {
+        float c[SDN];
+#pragma unroll
+        for (int h = 0; h < SDN / 2; h++) {
+            const float2 v = row[n1 * (SDN / 2) + h];
+            c[2 * h] = v.x, c[2 * h + 1] = v.y;
+        }
+#pragma unroll
+        for (int i = 0; i < N; i++) {
+            float tr = 0.f, ti = 0.f;
+#pragma unroll
+            for (int n2 = 0; n2 < SDN; n2++) {
+                if ((n1 + n2) & 1)
+                    ti = fmaf(c[n2], Y[i][n2], ti);
+                else
+                    tr = fmaf(c[n2], Y[i][n2], tr);
+            }
+            er[i] = fmaf(X[i][n1], tr, er[i]);
+            ei[i] = fmaf(X[i][n1], ti, ei[i]);
+        }
+    }
+}
+
 // FAST (the chosen form's Gaussians and shapelets, shared beam only): the
 // phasor from the FP32 quarter-turn polynomials after exact FP64 range
 // reduction, envelopes in FP32 (arguments and table positions in FP64),
@@ -447,6 +498,16 @@ __global__ void __launch_bounds__(DT, FastShape<TYPE>::MIN_CTAS) fast_kernel(con
                     xm = su * g.z + sv * g.w;
                     ym = su * g.w - sv * g.z;
                 }
+                float der[FCH], dei[FCH];  // dense shapelet envelopes of all channels
+                if (TYPE == 2 && p.sdense) {
+                    double xp[FCH], yp[FCH];
+#pragma unroll
+                    for (int i = 0; i < FCH; i++) {
+                        xp[i] = xm * (ool[i] * g.x) + SBF_C;
+                        yp[i] = ym * (ool[i] * g.y) + SBF_C;
+                    }
+                    shapelet_dense_multi<FCH>(p, s_dense + c * SDN * SDN, xp, yp, der, dei);
+                }
 #pragma unroll
                 for (int i = 0; i < FCH; i++) {
                     float sn, cs;
@@ -458,8 +519,7 @@ __global__ void __launch_bounds__(DT, FastShape<TYPE>::MIN_CTAS) fast_kernel(con
                         // of the component's flux
                         er = expf((float)(exm * (ool[i] * ool[i])));
                     } else if (p.sdense) {
-                        shapelet_dense_at(p, s_dense + c * SDN * SDN, xm * (ool[i] * g.x) + SBF_C,
-                                          ym * (ool[i] * g.y) + SBF_C, er, ei);
+                        er = der[i], ei = dei[i];
                     } else {
                         shapelet_envelope_f32(p, c0 + c, g, su * ool[i], sv * ool[i], er, ei);
                     }
