@@ -227,6 +227,7 @@ __global__ void __launch_bounds__(256) apply_kernel(JonesF32* resid, const Sweep
     int tp, tq;
     baseline_to_tiles(bl, A.ntiles, tp, tq);
     float2 dl[4] = {};
+#pragma unroll 4  // several sources' table loads in flight
     for (int s = 0; s < A.nsrc; s++) {
         const IonoConsts ko = A.old[s], kn = A.neu[s];
         if (ko.alpha == kn.alpha && ko.beta == kn.beta && ko.gain == kn.gain) continue;
