@@ -489,7 +489,9 @@ __global__ void __launch_bounds__(DT, FastShape<TYPE>::MIN_CTAS) fast_kernel(con
                     // ~1e-7 of its size, would become the envelope's relative error)
                     const double kx = um * g.z + vm * g.w;
                     const double ky = um * g.w - vm * g.z;
-                    exm = g.x * (kx * kx) + g.y * (ky * ky);
+                    // in base 2 (exp(x) = 2^(x log2 e)): the per-channel exp2f
+                    // costs fewer instructions than expf (measured)
+                    exm = (g.x * (kx * kx) + g.y * (ky * ky)) * 1.4426950408889634074;
                 } else {
                     const double2 ta = __ldg(p.suv_tile + (size_t)(c0 + c) * p.ntiles + t1);
                     const double2 tb = __ldg(p.suv_tile + (size_t)(c0 + c) * p.ntiles + t2);
@@ -514,10 +516,10 @@ __global__ void __launch_bounds__(DT, FastShape<TYPE>::MIN_CTAS) fast_kernel(con
                     phasor_quarter_f32(4.0 * ool[i] * tm, sn, cs);
                     float er, ei = 0.f;
                     if (TYPE == 1) {
-                        // exponent in FP64, exp in FP32: rounding the exponent
-                        // to FP32 moves the envelope by |ex| 6e-8 e^-|ex| <= 2.2e-8
+                        // exponent in FP64, exp2 in FP32: rounding the exponent
+                        // to FP32 moves the envelope by ln2 |x| 6e-8 2^-|x| <= 2.2e-8
                         // of the component's flux
-                        er = expf((float)(exm * (ool[i] * ool[i])));
+                        er = exp2f((float)(exm * (ool[i] * ool[i])));
                     } else if (p.sdense) {
                         er = der[i], ei = dei[i];
                     } else {
