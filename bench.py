@@ -430,7 +430,7 @@ def peel_arm(args):
            "higher_is_better": False}
     for name, batched in (("sequential", False), ("batched", True)):
         times, consts = [], None
-        for rep in range(2):  # the first run also builds the models and (batched) autotunes
+        for rep in range(3):  # the first run also builds the models and (batched) autotunes
             r = resid0.clone()
             torch.cuda.synchronize()
             t0 = time.perf_counter()
