@@ -172,39 +172,54 @@ class ClockSampler:
 
 
 # --------------------------------------------------------- reference arm
-def reference_arm(args, rank):
+def oracle_predict_samples(obs, sky, sample_s: float, samples: int):
     """The reference's CPU predictor (the oracle's C++ restatement of
-    SkyModellerCpu, OpenMP over baselines) on bounded samples of the same
-    workload: one timestep x a channel subset per step."""
-    if rank != 0:
-        return
+    SkyModellerCpu, OpenMP over baselines, all host threads) timed on bounded
+    samples of the workload: each sample is one timestep (cycling through the
+    workload's) x the first nch channels, nch sized after a warm-up so that a
+    sample takes about sample_s.  The cpu_baseline leg and the reference arm
+    both use this one rule.  Returns (work per sample, seconds per sample
+    list, nch, threads)."""
     from oracle import oracle as orc
 
     orc.build()
-    obs, sky = workload()
     threads = os.cpu_count() or 1
     orc.set_num_threads(threads)
     beam = orc.beam_struct(1)
-    nch = 2
-    # size the per-step sample to ~ a few seconds
+    orc.model_timestep(sky, obs.tile_xyzs, obs.freqs[:1], obs.phase_centre, obs.lsts[0], obs.latitude, beam=beam)
     t0 = time.perf_counter()
-    orc.model_timestep(sky, obs.tile_xyzs, obs.freqs[:nch], obs.phase_centre, obs.lsts[0], obs.latitude, beam=beam)
-    dt = time.perf_counter() - t0
-    nch = int(max(1, min(obs.freqs.size, round(nch * 3.0 / max(dt, 1e-3)))))
-    for _ in range(max(args.warmup, 0)):
-        orc.model_timestep(sky, obs.tile_xyzs, obs.freqs[:1], obs.phase_centre, obs.lsts[0], obs.latitude, beam=beam)
+    orc.model_timestep(sky, obs.tile_xyzs, obs.freqs[:2], obs.phase_centre, obs.lsts[0], obs.latitude, beam=beam)
+    per_ch = (time.perf_counter() - t0) / 2
+    nch = int(max(1, min(obs.freqs.size, round(sample_s / max(per_ch, 1e-4)))))
     times = []
-    for k in range(args.steps):
+    for k in range(samples):
         t0 = time.perf_counter()
         orc.model_timestep(sky, obs.tile_xyzs, obs.freqs[:nch], obs.phase_centre, obs.lsts[k % obs.lsts.size],
                            obs.latitude, beam=beam)
         times.append(time.perf_counter() - t0)
-    work = obs.num_baselines * nch * sky.num_components
+    return obs.num_baselines * nch * sky.num_components, times, nch, threads
+
+
+def reference_arm(args, rank):
+    """The reference's CPU predictor on bounded samples of the same workload
+    (oracle_predict_samples: one step = one sample of ~3 s)."""
+    if rank != 0:
+        return
+    obs, sky = workload()
+    from oracle import oracle as orc
+
+    orc.build()
+    orc.set_num_threads(os.cpu_count() or 1)
+    beam = orc.beam_struct(1)
+    for _ in range(max(args.warmup, 0)):
+        orc.model_timestep(sky, obs.tile_xyzs, obs.freqs[:1], obs.phase_centre, obs.lsts[0], obs.latitude, beam=beam)
+    work, times, nch, threads = oracle_predict_samples(obs, sky, 3.0, max(args.steps, 1))
     value = work * len(times) / sum(times)
-    sample = f"1 timestep x {nch} of 384 channels x 4600 components x 8128 baselines per step"
+    sample = (f"per step: 1 timestep (cycling over the 4) x {nch} of {obs.freqs.size} channels x "
+              f"{sky.num_components} components x {obs.num_baselines} baselines")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
+        "steps": len(times), "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": config_dict(obs, sky, "reference CPU (C++ restatement of SkyModellerCpu, OpenMP)"),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
@@ -214,23 +229,186 @@ def reference_arm(args, rank):
 
 
 def cpu_baseline(obs, sky, seconds):
+    """The same rule as the reference arm: samples of ~3 s, as many as fit in
+    `seconds` (at least 4, one per timestep)."""
+    samples = max(4, int(round(seconds / 3.0)))
+    work, times, nch, threads = oracle_predict_samples(obs, sky, 3.0, samples)
+    return {"value": work * len(times) / sum(times), "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{len(times)} samples of 1 timestep (cycling over the 4) x {nch} of {obs.freqs.size} channels x "
+                      f"{sky.num_components} components x {obs.num_baselines} baselines ({sum(times):.1f} s)"}
+
+
+def sampled_error(vis_tfb, obs, sky, ntiles_sample=24, seed=2024):
+    """Parity check of the timed output (the checker, run with the
+    cpu_baseline leg): the chosen form's visibilities [t][f][bl][8] of every
+    timestep and channel on a seeded sample of baselines (all baselines among
+    ntiles_sample random tiles) against the FP64 oracle; normwise error and
+    the 99.9th percentile of |dV| over the rms visibility."""
+    import torch
+
+    from mwa_hyperdrive_b200 import synth
     from oracle import oracle as orc
 
     orc.build()
-    threads = os.cpu_count() or 1
-    orc.set_num_threads(threads)
-    beam = orc.beam_struct(1)
+    orc.set_num_threads(os.cpu_count() or 1)
+    sub, bl = synth.sample_tiles(obs.num_tiles, ntiles_sample, seed)
+    got = vis_tfb.index_select(2, torch.from_numpy(bl).to(vis_tfb.device)).cpu().numpy().astype(np.float64)
     t0 = time.perf_counter()
-    orc.model_timestep(sky, obs.tile_xyzs, obs.freqs[:1], obs.phase_centre, obs.lsts[0], obs.latitude, beam=beam)
-    dt = time.perf_counter() - t0
-    nch = int(max(1, min(obs.freqs.size, math.floor(seconds / max(dt, 1e-3)))))
-    t0 = time.perf_counter()
-    orc.model_timestep(sky, obs.tile_xyzs, obs.freqs[:nch], obs.phase_centre, obs.lsts[0], obs.latitude, beam=beam)
-    dt = time.perf_counter() - t0
-    work = obs.num_baselines * nch * sky.num_components
-    return {"value": work / dt, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"1 timestep x {nch} channels x {sky.num_components} components x {obs.num_baselines} baselines "
-                      f"({dt:.1f} s)"}
+    ref = np.stack([orc.model_timestep(sky, obs.tile_xyzs[sub], obs.freqs, obs.phase_centre, float(lst), obs.latitude,
+                                       beam=orc.beam_struct(1), out_f64=True)[0] for lst in obs.lsts])
+    norm = np.linalg.norm(ref)
+    rms = norm / math.sqrt(ref.size)
+    d = np.abs(got - ref)
+    return {"normwise": float(np.linalg.norm(got - ref) / norm), "p999": float(np.percentile(d, 99.9) / rms),
+            "max": float(d.max() / rms), "bar": 1e-6, "vs": "FP64 oracle (C++ restatement of SkyModellerCpu)",
+            "sample": f"{bl.size} baselines (all among {ntiles_sample} seeded random tiles) x {obs.freqs.size} channels "
+                      f"x {obs.lsts.size} timesteps of the last timed step's output ({time.perf_counter() - t0:.1f} s)"}
+
+
+# ------------------------------------- reference GPU kernels (baseline leg)
+def dropin_inputs(obs, sky, lst, keep):
+    """The reference FFI's device inputs (gpu/types.h Points / Gaussians /
+    Shapelets / Addresses, FP64 build) for the workload's sky at one
+    timestep: components grouped power law / curved power law per type,
+    instrumental flux at 150 MHz, per-baseline UVWs and shapelet UVs, the
+    shapelet basis table, and a beam of one unique tile and frequency (random
+    Jones near identity: the same work per component as any beam)."""
+    import torch
+
+    from mwa_hyperdrive_b200 import _lib
+
+    def put(a, dt=np.float64):
+        t = torch.from_numpy(np.ascontiguousarray(a, dt)).cuda()
+        keep.append(t)
+        return t.data_ptr()
+
+    pc = obs.phase_centre
+    xyz = obs.tile_xyzs
+    i, j = np.triu_indices(obs.num_tiles, 1)
+    d = xyz[i] - xyz[j]
+
+    def uvw(ha, dec):
+        sh, ch, sd, cd = np.sin(ha), np.cos(ha), np.sin(dec), np.cos(dec)
+        return np.stack([sh * d[:, 0] + ch * d[:, 1], -sd * ch * d[:, 0] + sd * sh * d[:, 1] + cd * d[:, 2],
+                         cd * ch * d[:, 0] - cd * sh * d[:, 1] + sd * d[:, 2]], -1)
+
+    nbl, nf = obs.num_baselines, obs.freqs.size
+    sbf = np.zeros(101 * 10001)
+    _lib.lib().hdc_shapelet_basis(sbf.ctypes.data)
+    addr = _lib.Addresses(nf, nf * nbl, nbl, put(obs.freqs), put(sbf), 1, put(np.zeros(obs.num_tiles), np.int32),
+                          put(np.zeros(nf), np.int32), put(np.arange(obs.num_tiles), np.int32))
+    structs = {}
+    coeff_dt = np.dtype([("value", np.float64), ("n1", np.uint8), ("n2", np.uint8), ("pad", np.uint8, 6)])
+    rng = np.random.default_rng(9)
+    for ct in range(3):
+        idx = np.nonzero(sky.comp_type == ct)[0]
+        groups = [idx[sky.flux_type[idx] == 1], idx[sky.flux_type[idx] == 2]]
+        assert len(groups[0]) + len(groups[1]) == len(idx), "list fluxes are not part of this workload"
+        order = np.concatenate(groups)
+        nc = order.size
+        ra, dec = sky.ra[order], sky.dec[order]
+        dra = ra - pc[0]
+        l = np.cos(dec) * np.sin(dra)
+        m = np.sin(dec) * np.cos(pc[1]) - np.cos(dec) * np.sin(pc[1]) * np.cos(dra)
+        n = np.sin(dec) * np.sin(pc[1]) + np.cos(dec) * np.cos(pc[1]) * np.cos(dra)
+        lmn = 2 * np.pi * np.stack([l, m, n - 1.0], -1)
+        fd = sky.fds[sky.fd_start[order]]
+        assert np.all(fd[:, 0] == 150e6)
+        # to_inst_stokes (srclist/types/flux_density/mod.rs:58-65): XX = I - Q,
+        # XY = U - iV, YX = U + iV, YY = I + Q
+        inst = np.zeros((nc, 8))
+        inst[:, 0] = fd[:, 1] - fd[:, 2]
+        inst[:, 2], inst[:, 3] = fd[:, 3], -fd[:, 4]
+        inst[:, 4], inst[:, 5] = fd[:, 3], fd[:, 4]
+        inst[:, 6] = fd[:, 1] + fd[:, 2]
+        beam = rng.normal(size=(1, 1, nc, 8)) * 0.05
+        beam[..., 0] += 1.0
+        beam[..., 6] += 1.0
+        n0 = groups[0].size
+        lm, fdp, sis = put(lmn), put(inst), put(sky.si[order])
+        qs = put(np.concatenate([sky.q[groups[1]], [0.0]]))
+        if ct == 0:
+            st = _lib.Points(n0, lm, fdp, sis, nc - n0, lm + 24 * n0, fdp + 64 * n0, sis + 8 * n0, qs, 0, 0, 0)
+        else:
+            gp = put(np.stack([sky.maj[order], sky.min[order], sky.pa[order]], -1))
+        if ct == 1:
+            st = _lib.Gaussians(n0, lm, fdp, sis, gp, nc - n0, lm + 24 * n0, fdp + 64 * n0, sis + 8 * n0, qs,
+                                gp + 24 * n0, 0, 0, 0, 0)
+        if ct == 2:
+            suv = np.stack([uvw(lst - ra[k], dec[k])[:, :2] for k in range(nc)], 1)  # [bl][nc][2]
+            cnt = sky.coeff_count[order]
+            co = np.zeros(int(cnt.sum()), coeff_dt)
+            pos = 0
+            for k in order:
+                a, b = sky.coeff_start[k], sky.coeff_start[k] + sky.coeff_count[k]
+                co["value"][pos:pos + b - a] = sky.coeff_value[a:b]
+                co["n1"][pos:pos + b - a] = sky.coeff_n1[a:b]
+                co["n2"][pos:pos + b - a] = sky.coeff_n2[a:b]
+                pos += b - a
+            c0 = int(cnt[:n0].sum())
+            suv_p = [put(suv[:, :n0]), put(suv[:, n0:])]
+            cop, ncp = put(co.view(np.uint8), np.uint8), put(cnt, np.int32)
+            st = _lib.Shapelets(n0, lm, fdp, sis, gp, suv_p[0], cop, ncp,
+                                nc - n0, lm + 24 * n0, fdp + 64 * n0, sis + 8 * n0, qs, gp + 24 * n0, suv_p[1],
+                                cop + 16 * c0, ncp + 4 * n0, 0, 0, 0, 0, 0, 0, 0)
+        structs[ct] = (st, put(beam))
+    return structs, addr, put(uvw(lst - pc[0], pc[1]))
+
+
+def reference_gpu_leg(obs, sky):
+    """Baseline leg: mwa_hyperdrive's own GPU kernels (src/gpu/model.cu, FP64
+    build, compiled for sm_100a from the reference's sources into
+    oracle/_ref/libref_gpu.so) against libhdc's drop-in kernels on identical
+    device inputs, one timestep of the workload, CUDA events on the legacy
+    default stream both libraries launch on, best of 3 after a warm-up.  The
+    drop-in calls include their per-call table preparation and the read of
+    their kernel error word."""
+    import torch
+
+    from mwa_hyperdrive_b200 import _lib
+
+    so = ROOT / "oracle" / "_ref" / "libref_gpu.so"
+    if not so.exists():
+        return {"unavailable": "oracle/_ref/libref_gpu.so was not built (needs the reference sources)"}
+    ref = ctypes.CDLL(str(so))
+    names = {0: "model_points", 1: "model_gaussians", 2: "model_shapelets"}
+    for nm in names.values():
+        res, argt = _lib.SIGNATURES[nm]
+        getattr(ref, nm).restype, getattr(ref, nm).argtypes = res, argt
+    keep = []
+    structs, addr, uvws = dropin_inputs(obs, sky, float(obs.lsts[0]), keep)
+    nf, nbl = obs.freqs.size, obs.num_baselines
+    out = {"workload": "one timestep of the mixed-component workload (4000 points, 500 Gaussians, 100 shapelets, "
+                       "384 channels, 8128 baselines) through the reference FFI with a per-tile beam table of one "
+                       "unique tile", "unit": "ms per timestep"}
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    vis = {k: torch.zeros((nf, nbl, 8), dtype=torch.float32, device="cuda") for k in ("ref", "hdc")}
+    total = {"ref": 0.0, "hdc": 0.0}
+    for ct, nm in names.items():
+        st, beam = structs[ct]
+        row = {}
+        for who, lib in (("ref", ref), ("hdc", _lib.lib())):
+            fn = getattr(lib, nm)
+            best = float("inf")
+            for rep in range(4):
+                vis[who].zero_()
+                torch.cuda.synchronize()
+                ev[0].record(torch.cuda.default_stream())
+                _lib.check_str(fn(ctypes.byref(st), ctypes.byref(addr), uvws, beam, vis[who].data_ptr()),
+                               f"{who} {nm}")
+                ev[1].record(torch.cuda.default_stream())
+                torch.cuda.synchronize()
+                if rep:
+                    best = min(best, ev[0].elapsed_time(ev[1]))
+            row[who + "_ms"] = best
+            total[who] += best
+        a, b = vis["hdc"].double(), vis["ref"].double()
+        row["max_abs_diff_over_rms"] = float((a - b).abs().max() / b.pow(2).mean().sqrt())
+        row["speedup"] = row["ref_ms"] / row["hdc_ms"]
+        out[nm] = row
+    out["all_types"] = {"ref_ms": total["ref"], "hdc_ms": total["hdc"], "speedup": total["ref"] / total["hdc"]}
+    del keep
+    return out
 
 
 # ------------------------------------------------------ DI calibration
@@ -282,8 +460,14 @@ def dical_workload(nch):
 
 
 def dical_arm(args):
-    """Plain and collapsed DI calibration of the workload's timeblock, CPU
-    oracle on a bounded sample of its chanblocks."""
+    """DI calibration of the workload's timeblock in every solver form, each
+    timed best of 3 (CUDA-synchronised wall time of the whole call: the CUDA
+    graph of the first pass, the retry pass and the result reads).  Two
+    budgets: the stated 50 iterations (on this sky no chanblock converges in
+    50 iterations -- the CPU oracle agrees -- so every chanblock ends failed
+    and NaN-padded, as the reference does) and 200 iterations, where the
+    solver converges (mean ~130 iterations); the 200-iteration run is the
+    headline and is checked against the CPU oracle on sampled chanblocks."""
     import torch
 
     from mwa_hyperdrive_b200 import calibrate as cal
@@ -295,70 +479,83 @@ def dical_arm(args):
     ident[..., 0] = 1.0
     ident[..., 6] = 1.0
     out = {"workload": DICAL_WORKLOAD, "metric": "DI-cal s/timeblock", "unit": "s", "higher_is_better": False}
-    sols = {}
-    for form in ("plain", "collapsed", "collapsed_f32"):
-        dj = torch.from_numpy(ident.copy()).cuda()
-        cal.calibrate_timeblock(data, model, dj, (0, nt), 50, 1e-8, 1e-4, form=form)  # warm-up
-        times, res = [], None
-        for _ in range(3):
-            dj.copy_(torch.from_numpy(ident))
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            res = cal.calibrate_timeblock(data, model, dj, (0, nt), 50, 1e-8, 1e-4, form=form)
-            torch.cuda.synchronize()
-            times.append(time.perf_counter() - t0)
-        sols[form] = dj.cpu().numpy()
-        it = np.array([r.num_iterations for r in res])
-        out[form] = {"s_per_timeblock": min(times), "iterations_mean": float(it.mean()), "iterations_max": int(it.max()),
-                     "converged": int(sum(r.converged for r in res)), "chanblocks": nch}
-    ok = np.isfinite(sols["plain"])
-    for form in ("collapsed", "collapsed_f32"):
-        a, b = sols[form][ok], sols["plain"][ok]
-        out[form]["solution_rel_err_vs_plain"] = (float(np.linalg.norm(a - b) / np.linalg.norm(b)) if ok.any()
-                                                  else None)
-        out[form]["nan_pattern_equal"] = bool(np.array_equal(np.isnan(sols[form]), np.isnan(sols["plain"])))
-    # the same timeblock solved to convergence (MitchCal needs ~140 iterations on
-    # this sky; the workload's 50-iteration cap leaves every chanblock above
-    # the minimum threshold, flagged as failed, in the CPU oracle too)
-    conv = {}
-    for form in ("plain", "collapsed_f32"):
-        dj = torch.from_numpy(ident.copy()).cuda()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        res = cal.calibrate_timeblock(data, model, dj, (0, nt), 200, 1e-8, 1e-4, form=form)
-        torch.cuda.synchronize()
-        it = np.array([r.num_iterations for r in res])
-        conv[form] = {"s_per_timeblock": time.perf_counter() - t0, "iterations_mean": float(it.mean()),
-                      "converged": int(sum(r.converged for r in res))}
-        sols["conv_" + form] = dj.cpu().numpy()
-    a, b = sols["conv_collapsed_f32"], sols["conv_plain"]
-    ok = np.isfinite(b) & np.isfinite(a)
-    conv["collapsed_f32"]["solution_rel_err_vs_plain"] = (float(np.linalg.norm(a[ok] - b[ok]) / np.linalg.norm(b[ok]))
-                                                          if ok.any() else None)
+    forms = ("plain", "collapsed", "collapsed_f32")
+
+    def run(max_iter):
+        res_by_form, sols, its = {}, {}, {}
+        for form in forms:
+            dj = torch.from_numpy(ident.copy()).cuda()
+            cal.calibrate_timeblock(data, model, dj, (0, nt), max_iter, 1e-8, 1e-4, form=form)  # warm-up
+            times, res = [], None
+            for _ in range(3):
+                dj.copy_(torch.from_numpy(ident))
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                res = cal.calibrate_timeblock(data, model, dj, (0, nt), max_iter, 1e-8, 1e-4, form=form)
+                torch.cuda.synchronize()
+                times.append(time.perf_counter() - t0)
+            sols[form] = dj.cpu().numpy()
+            it = np.array([r.num_iterations for r in res])
+            its[form] = it
+            res_by_form[form] = {"s_per_timeblock": min(times), "s_all_runs": times,
+                                 "iterations_mean": float(it.mean()), "iterations_max": int(it.max()),
+                                 "converged": int(sum(r.converged for r in res)), "chanblocks": nch,
+                                 "failed_chanblocks": int(np.isnan(sols[form]).any(axis=(0, 2)).sum())}
+        ok = np.isfinite(sols["plain"])
+        for form in forms[1:]:
+            a, b = sols[form][ok], sols["plain"][ok]
+            res_by_form[form]["solution_rel_err_vs_plain"] = (float(np.linalg.norm(a - b) / np.linalg.norm(b))
+                                                              if ok.any() else None)
+            res_by_form[form]["nan_pattern_equal"] = bool(np.array_equal(np.isnan(sols[form]),
+                                                                         np.isnan(sols["plain"])))
+        return res_by_form, sols, its
+
+    out["max50"], _, _ = run(50)
+    out["max50"]["note"] = ("the stated budget: no chanblock of this sky converges within 50 iterations (the CPU "
+                            "oracle agrees), so every solution is NaN-padded as the reference does; times kept for "
+                            "the iteration cost")
+    conv, sols, its = run(200)
     out["to_convergence_max200"] = conv
     out["chosen"] = "collapsed_f32"
-    out["speedup_chosen_vs_plain"] = out["plain"]["s_per_timeblock"] / out["collapsed_f32"]["s_per_timeblock"]
-    # roofline of the chosen iteration kernel: covariance bytes per iteration
+    out["headline_s_per_timeblock"] = conv["collapsed_f32"]["s_per_timeblock"]
+    out["speedup_chosen_vs_plain"] = conv["plain"]["s_per_timeblock"] / conv["collapsed_f32"]["s_per_timeblock"]
     nbl = model.shape[2]
-    it_total = out["collapsed_f32"]["iterations_mean"] * nch
+    it_total = conv["collapsed_f32"]["iterations_mean"] * nch
     out["algorithmic"] = {"plain_bytes_per_iteration_per_chanblock": nt * nbl * 64,
                           "collapsed_f32_bytes_per_iteration_per_chanblock": nbl * 48 * 4,
                           "fp64_flop_per_visibility_iteration_plain": 368, "collapsed_iterations_total": it_total}
     if not args.no_cpu_baseline:
+        # the reference's CPU solver (oracle restatement of calibrate_timeblock,
+        # OpenMP over chanblocks as rayon) at the same 200-iteration budget on
+        # a sample of chanblocks, scaled; and every GPU form's solutions on
+        # those chanblocks against it (bar 1e-6; the plain form follows the
+        # oracle's arithmetic and agrees to ~1e-10)
         from oracle import oracle as orc
 
         orc.build()
         threads = os.cpu_count() or 1
         orc.set_num_threads(threads)
         ns = min(nch, max(threads, 8))
-        dh = data[:, :ns].cpu().numpy()
-        mh = model[:, :ns].cpu().numpy()
+        pick = np.linspace(0, nch - 1, ns).round().astype(int)
+        dh = data[:, pick].cpu().numpy()
+        mh = model[:, pick].cpu().numpy()
         t0 = time.perf_counter()
-        orc.calibrate_timeblock(dh, mh, ident[:, :ns], 0, nt, 50, 1e-8, 1e-4, 0)
+        dj_o, res_o = orc.calibrate_timeblock(dh, mh, ident[:, pick], 0, nt, 200, 1e-8, 1e-4, 0)
         dt = time.perf_counter() - t0
         out["cpu_baseline"] = {"value": dt * nch / ns, "unit": "s", "cores": threads, "kind": "port",
-                               "sample": f"{ns} of {nch} chanblocks x 14 timesteps x {nbl} baselines in {dt:.2f} s, "
-                                         f"scaled to {nch} chanblocks"}
+                               "max_iterations": 200,
+                               "sample": f"{ns} of {nch} chanblocks (evenly spaced) x 14 timesteps x {nbl} baselines "
+                                         f"in {dt:.2f} s, scaled to {nch} chanblocks"}
+        out["cpu_baseline"]["iterations_mean"] = float(np.mean([r["num_iterations"] for r in res_o]))
+        for form in forms:
+            a = sols[form][:, pick]
+            ok = np.isfinite(dj_o) & np.isfinite(a)
+            conv[form]["solution_rel_err_vs_oracle"] = (float(np.linalg.norm(a[ok] - dj_o[ok]) /
+                                                              np.linalg.norm(dj_o[ok])) if ok.any() else None)
+            conv[form]["oracle_nan_pattern_equal"] = bool(np.array_equal(np.isnan(a), np.isnan(dj_o)))
+            conv[form]["oracle_iterations_equal"] = bool(np.array_equal(its[form][pick],
+                                                                        [r["num_iterations"] for r in res_o]))
+        out["speedup_chosen_vs_cpu"] = out["cpu_baseline"]["value"] / conv["collapsed_f32"]["s_per_timeblock"]
     return out
 
 
@@ -567,8 +764,14 @@ def prep_arm(args):
     m = torch.randn((nt, nout, nbl, 8), generator=g, device="cuda")
     wt = torch.rand((nt, nout, nbl), generator=g, device="cuda") * 20.0 - 3.0
     bw = np.linspace(0.0, 1.0, nbl)
+    # count what scale_kernel moves: the weight of every entry, data and model
+    # read only where weight x baseline weight > 0 (elsewhere zeros are
+    # stored without a read), data and model written everywhere, and the
+    # baseline weights (the weights are drawn once and not changed by the call)
+    n_all = nt * nout * nbl
+    n_pos = int(((wt.double() * torch.from_numpy(bw).cuda()[None, None, :]) > 0).sum())
     t_sc = timed(lambda: C.scale_by_weights(d, m, wt, bw))
-    bytes_sc = nt * nout * nbl * (2 * 32 * 2 + 4) + nbl * 8
+    bytes_sc = n_all * 4 + n_pos * 2 * 32 + n_all * 2 * 32 + nbl * 8
     out["scale_by_weights"] = {"s": t_sc, "algorithmic_bytes": bytes_sc, "achieved_gbs": bytes_sc / t_sc / 1e9,
                                "peak_gbs": hbm, "frac": bytes_sc / t_sc / 1e9 / hbm}
     out["peak_source"] = "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650 GB/s"
@@ -595,6 +798,19 @@ def guarded(fn, args):
         return fn(args)
     except Exception as e:  # reported, not hidden: the key holds the error
         return {"error": f"{type(e).__name__}: {e}"}
+
+
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of each
+# kernel class on this workload (one timestep, 384 channels), from the ncu
+# launch list of the bench command itself (one pass: gpu__time_duration and
+# the two DRAM counters), summarised in
+# profiles/predict_launch_list_mixed_predict.md.  The visibilities alone are
+# 100 MB read + 100 MB written per launch.
+NCU_TRAFFIC_SOURCE = "ncu launch list of this bench command (profiles/predict_launch_list_mixed_predict.md)"
+NCU_DRAM_BYTES_PER_LAUNCH = {
+    ("points", "tensor"): 1202e6, ("gaussians", "tensor"): 150e6, ("shapelets", "tensor"): 153e6,
+    ("points", "direct"): 264e6, ("gaussians", "direct"): 151e6, ("shapelets", "direct"): 143e6,
+}
 
 
 # ------------------------------------------------------------ GPU arm
@@ -742,8 +958,9 @@ def gpu_arm(args, rank, world, local_rank):
                      "kernel": f"direct_kernel ({names[k]}, {'FP32 form' if fast else 'FP64'})",
                      "peak": (g32.value if fast else g64.value) / 1e3,
                      "peak_source": f"{'FP32' if fast else 'FP64'} FMA probe kernel measured in this run"}
-        entry.update({"achieved": flops / t_launch / 1e12, "unit": "TFLOP/s", "traffic": None,
-                      "ms_per_step": per_step_ms[k]})
+        traffic = NCU_DRAM_BYTES_PER_LAUNCH.get((names[k], form))
+        entry.update({"achieved": flops / t_launch / 1e12, "unit": "TFLOP/s", "traffic": traffic,
+                      "traffic_source": NCU_TRAFFIC_SOURCE if traffic else None, "ms_per_step": per_step_ms[k]})
         if k == 0 and form == "tensor":
             # what the tensor pipe executes: 18 kind::i8 MMAs of 128 x 128 x 32 per 32-component stage of each
             # (channel, polarisation, column half) CTA, against 8190 int8 MAC/clk/SM (a probe of back-to-back
@@ -773,6 +990,11 @@ def gpu_arm(args, rank, world, local_rank):
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(obs, sky, args.cpu_seconds)
+            # the checker on the timed configuration: the last timed step's
+            # output (still in `vis`) against the FP64 oracle
+            line["error"] = sampled_error(vis, obs, sky)
+            line["reference_gpu"] = guarded(lambda a: reference_gpu_leg(obs, sky), args)
+            torch.cuda.synchronize()
         if not (args.skip_dical and args.skip_peel and args.skip_warmstart and args.skip_prep):
             del vis, flush
             torch.cuda.empty_cache()

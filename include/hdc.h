@@ -179,8 +179,10 @@ const char *model_points(const Points *comps, const Addresses *a, const UVW *d_u
  * implicit device synchronisation).  Same arguments and result as
  * model_points, but its scratch is a fixed array compiled into the library
  * (HDC_NOALLOC_SCRATCH_BYTES per device, held until exit): it needs
- * 32 B per component + 64 B per (channel, component), and larger problems
- * are rejected with an error.  Every call on a device shares that array, so
+ * 64 B per component + 64 B per (channel, component), each of its three
+ * tables rounded up to 256 B (LMN 32 B and envelope 32 B per component, flux
+ * 64 B per channel and component), and larger problems are rejected with an
+ * error.  Kernel errors are read back and cleared as in model_points.  Every call on a device shares that array, so
  * calls whose kernels overlap on the GPU race and must be serialised.  The
  * first call on a device looks up the array's device address and should come
  * before any stream capture. */
@@ -259,6 +261,21 @@ const char *subtract_iono(JonesF32 *d_vis_residual, const JonesF32 *d_vis_model,
 const char *add_model(JonesF32 *d_vis_residual, const JonesF32 *d_vis_model, const IonoConsts iono_consts,
                       const double *d_lambdas_m, const UVW *d_uvws, const int num_timesteps, const int num_freqs,
                       const int num_baselines);
+
+/* Replaces gpu/utils.h:28 get_gpu_device_info (called by gpu/utils.rs:35-60
+ * for the MODELLER string of the calibration solutions): makes `device`
+ * current and reports its name, compute capability, global memory [bytes] and
+ * the CUDA driver and runtime versions (1000 * major + 10 * minor).  NULL on
+ * success, else a static error string. */
+const char *get_gpu_device_info(int device, char name[256], int *device_major, int *device_minor,
+                                size_t *total_global_mem, int *driver_version, int *runtime_version);
+
+/* Drop-in error reporting.  The drop-in model_* calls read their kernels'
+ * error word after the launch (a synchronous read on the legacy default
+ * stream) and return one of these static strings instead of NULL when a
+ * kernel reported a problem; the word is cleared first, so the next call
+ * starts clean.  A kernel whose bounded wait ran out leaves the visibilities
+ * of its baselines unchanged. */
 
 /* ---------------------------------------------------------------------- */
 /* Native layer                                                            */
@@ -380,6 +397,22 @@ int hdc_modeller_model_timestep_autos_with(HdcModeller *m, double lst_rad, Jones
 
 /* Diagnostics.  Number of kernels libhdc has launched in this process. */
 long long hdc_kernel_launches(void);
+
+/* The static message for a kernel error word (bit 0: a bounded wait ran out,
+ * HDC_ERR_TIMEOUT; bit 1: an index outside a table, HDC_ERR_ARG), NULL for 0.
+ * Native calls return the status and leave the message in hdc_last_error();
+ * a modeller's device calls are asynchronous, so its kernels' errors are
+ * reported by its next call (the host-buffer call synchronises and reports
+ * its own). */
+const char *hdc_kernel_error_string(int word);
+
+/* Failure-path testing (no counterpart in the reference): the next direct
+ * predict kernel launched in this process issues none of its component-table
+ * copies and gives each bounded wait wait_ns nanoseconds, so its first wait
+ * runs out with nothing in flight; the call then reports HDC_ERR_TIMEOUT (or
+ * the drop-in timeout string) and leaves its visibilities unchanged.  One
+ * launch only; the library stays usable. */
+int hdc_test_stall_next_predict(unsigned long long wait_ns);
 
 /* Per-kernel-class device time of a modeller's last calls, measured with
  * CUDA events on the launching stream when profiling is enabled.

@@ -151,6 +151,10 @@ SIGNATURES = {
     "hdc_warmstart_propose": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p, c_int, c_int, c_int,
                                       c_void_p, c_void_p, c_void_p]),
     "hdc_kernel_launches": (ctypes.c_longlong, []),
+    "hdc_kernel_error_string": (c_char_p, [c_int]),
+    "hdc_test_stall_next_predict": (c_int, [ctypes.c_ulonglong]),
+    "get_gpu_device_info": (c_char_p, [c_int, c_char_p, ctypes.POINTER(c_int), ctypes.POINTER(c_int),
+                                       ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(c_int), ctypes.POINTER(c_int)]),
     "hdc_modeller_set_profiling": (c_int, [c_void_p, c_int]),
     "hdc_modeller_profile": (c_int, [c_void_p, c_void_p, c_int]),
     "hdc_probe_fp64_gflops": (c_int, [ctypes.POINTER(c_double)]),

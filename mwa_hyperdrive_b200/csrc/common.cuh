@@ -157,6 +157,14 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
     return true;
 }
 
+// After a bounded wait of a two-stage bulk-copy pipeline ran out at chunk k,
+// chunks [k, issued) may still be in flight: the issuing thread waits for
+// each of them (bounded again) so that no copy lands in the shared memory of
+// a CTA that has exited.
+__device__ __forceinline__ void drain_two_stage(uint64_t* bar, int k, int issued) {
+    for (int j = k; j < issued; j++) mbar_wait_bounded(&bar[j & 1], (j >> 1) & 1, nullptr);
+}
+
 // FP64 phasor exp(2 pi i t) for a phase in turns: exact range reduction to
 // r = t - rint(t) in [-1/2, 1/2], then sincospi(2 r).
 __device__ __forceinline__ cplx phasor_turns(double t) {
@@ -212,6 +220,13 @@ cudaError_t pool_malloc_async(void** p, size_t bytes, cudaStream_t s);
 int* device_error_word();
 // Read and clear the device error word (synchronises the stream).
 int take_device_error(cudaStream_t s);
+// The drop-in layer's own kernel error word (per device), apart from the
+// native layer's so that neither sees the other's errors.
+int* dropin_error_word();
+// Read error word w after the work queued before it on the legacy default
+// stream (a synchronous copy), clear it if set and return the static message
+// for its bits (NULL when clear); `who` prefixes hdc_last_error().
+const char* take_word_sync(int* w, const char* who);
 // Shapelet basis table on the current device (SBF_N x SBF_L doubles).
 const double* device_shapelet_basis();
 const float* device_shapelet_basis_f32();

@@ -468,7 +468,33 @@ int Modeller::model_channels(double lst, void* d_vis, bool out64, int f0, int nf
     return HDC_OK;
 }
 
+int Modeller::queue_error_check(cudaStream_t s) {
+    HDC_CUDA_RET_INT(cudaMemcpyAsync(h_err, d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    HDC_CUDA_RET_INT(cudaEventRecord(err_ev, s));
+    return HDC_OK;
+}
+
+// Report the kernel error word as of the last queued copy.  wait: block until
+// that copy has landed; otherwise look only if it already has.
+int Modeller::take_error(bool wait) {
+    cudaError_t q = wait ? cudaEventSynchronize(err_ev) : cudaEventQuery(err_ev);
+    if (q == cudaErrorNotReady) return HDC_OK;
+    if (q != cudaSuccess) {
+        hdc::set_error("modeller: %s", cudaGetErrorString(q));
+        return HDC_ERR_CUDA;
+    }
+    const int w = *(volatile int*)h_err;
+    if (!w) return HDC_OK;
+    // clear both copies before reporting, so that the next call starts clean
+    HDC_CUDA_RET_INT(cudaMemset(d_err, 0, sizeof(int)));
+    *(volatile int*)h_err = 0;
+    hdc::set_error("modeller: %s", kernel_error_string(w));
+    return kernel_error_status(w);
+}
+
 int Modeller::model(double lst, void* d_vis, bool out64, UVW* h_uvws, cudaStream_t s) {
+    int rc0 = take_error(false);
+    if (rc0) return rc0;
     EvPair e{};
     prof_begin(3, s, e);
     int rc = geometry(lst, s);
@@ -476,15 +502,20 @@ int Modeller::model(double lst, void* d_vis, bool out64, UVW* h_uvws, cudaStream
     prof_end(s, e);
     rc = model_channels(lst, d_vis, out64, 0, nf, s);
     if (rc) return rc;
+    rc = queue_error_check(s);
+    if (rc) return rc;
     if (h_uvws) {
         HDC_CUDA_RET_INT(cudaMemcpyAsync(h_uvws, d_uvws, sizeof(UVW) * nbl, cudaMemcpyDeviceToHost, s));
         HDC_CUDA_RET_INT(cudaStreamSynchronize(s));
+        return take_error(true);
     }
     return HDC_OK;
 }
 
 int Modeller::model_uvws(double lst, const UVW* d_uvws_ext, JonesF32* d_vis, cudaStream_t s) {
-    int rc = geometry(lst, s);
+    int rc = take_error(false);
+    if (rc) return rc;
+    rc = geometry(lst, s);
     if (rc) return rc;
     for (int ty = 0; ty < 3; ty++) {
         if (t[ty].nc == 0) continue;
@@ -492,11 +523,13 @@ int Modeller::model_uvws(double lst, const UVW* d_uvws_ext, JonesF32* d_vis, cud
         p.uvws = d_uvws_ext;
         HDC_CUDA_RET_INT(launch_direct(ty, false, false, p, s));
     }
-    return HDC_OK;
+    return queue_error_check(s);
 }
 
 int Modeller::autos(double lst, JonesF32* d_vis, cudaStream_t s) {
-    int rc = geometry(lst, s);
+    int rc = take_error(false);
+    if (rc) return rc;
+    rc = geometry(lst, s);
     if (rc) return rc;
     for (int ty = 0; ty < 3; ty++) {
         if (t[ty].nc == 0) continue;
@@ -513,6 +546,9 @@ int Modeller::autos(double lst, JonesF32* d_vis, cudaStream_t s) {
 }
 
 Modeller::~Modeller() {
+    if (err_ev) cudaEventDestroy(err_ev);
+    if (h_err) cudaFreeHost(h_err);
+    dfree(d_err);
     for (int i = 0; i < 3; i++)
         if (pipe_s[i]) cudaStreamDestroy(pipe_s[i]);
     for (auto& ev : pipe_ev)
@@ -707,11 +743,20 @@ extern "C" int hdc_modeller_new(const HdcSkyModel* sky, int pols, const XYZ* h_x
     cudaMemcpy(m->d_freqs, h_freqs, sizeof(double) * num_freqs, cudaMemcpyHostToDevice);
     cudaMemcpy(m->d_xyzs, h_xyzs, sizeof(XYZ) * num_tiles, cudaMemcpyHostToDevice);
     m->d_sbf = hdc::device_shapelet_basis();
-    m->d_err = hdc::device_error_word();
-    if (!m->d_sbf || !m->d_err) {
+    if (!m->d_sbf) {
         hdc::set_error("hdc_modeller_new: device tables unavailable");
         return fail(HDC_ERR_ALLOC);
     }
+    if (cudaMalloc(&m->d_err, sizeof(int)) != cudaSuccess ||
+        cudaHostAlloc(&m->h_err, sizeof(int), cudaHostAllocDefault) != cudaSuccess ||
+        cudaEventCreateWithFlags(&m->err_ev, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        hdc::set_error("hdc_modeller_new: device allocation failed");
+        return fail(HDC_ERR_ALLOC);
+    }
+    cudaMemset(m->d_err, 0, sizeof(int));
+    *m->h_err = 0;
+    cudaEventRecord(m->err_ev, 0);
     rc = m->build_tables(sky);
     if (rc) return fail(rc);
     if (predict_form == HDC_PREDICT_TENSOR) {
@@ -782,6 +827,8 @@ int Modeller::model_host_pipelined(double lst, JonesF32* h_vis, UVW* h_uvws, cud
         for (int i = 0; i < 3; i++) HDC_CUDA_RET_INT(cudaStreamCreateWithFlags(&pipe_s[i], cudaStreamNonBlocking));
         for (auto& ev : pipe_ev) HDC_CUDA_RET_INT(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
     }
+    int rc0 = take_error(false);
+    if (rc0) return rc0;
     cudaEvent_t* up = pipe_ev;                      // chunk uploaded
     cudaEvent_t* done = pipe_ev + PIPE_CHUNKS;      // chunk predicted
     cudaEvent_t start = pipe_ev[2 * PIPE_CHUNKS];   // caller's stream reached the call
@@ -833,10 +880,12 @@ int Modeller::model_host_pipelined(double lst, JonesF32* h_vis, UVW* h_uvws, cud
     }
     if (h_uvws)
         HDC_CUDA_RET_INT(cudaMemcpyAsync(h_uvws, d_uvws, sizeof(UVW) * nbl, cudaMemcpyDeviceToHost, pipe_s[2]));
+    rc = queue_error_check(pipe_s[1]);
+    if (rc) return rc;
     HDC_CUDA_RET_INT(cudaEventRecord(fin, pipe_s[2]));
     HDC_CUDA_RET_INT(cudaStreamWaitEvent(s, fin, 0));
     HDC_CUDA_RET_INT(cudaStreamSynchronize(pipe_s[2]));
-    return HDC_OK;
+    return take_error(true);
 }
 }  // namespace hdc
 

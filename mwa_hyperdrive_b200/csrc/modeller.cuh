@@ -35,7 +35,16 @@ struct Modeller {
     XYZ* d_xyzs = nullptr;
     UVW* d_uvws = nullptr;
     const double* d_sbf = nullptr;
+    // This modeller's kernel error word, its pinned host copy and the event
+    // after the last copy: each call queues a copy of the word behind its
+    // kernels; a call that finds an earlier copy completed and set reports it
+    // (calls on the device are asynchronous, so an error surfaces at the next
+    // call, or at the end of the host-buffer call, which synchronises).
     int* d_err = nullptr;
+    int* h_err = nullptr;
+    cudaEvent_t err_ev = nullptr;
+    int queue_error_check(cudaStream_t s);
+    int take_error(bool wait);
     TypeTables t[3];
     JonesF32* d_host_vis = nullptr;
     size_t host_vis_bytes = 0;

@@ -12,11 +12,15 @@
 //
 // The scratch is the file-scope device array below (HDC_NOALLOC_SCRATCH_BYTES,
 // 16 MiB), which every GPU that loads the library holds until the process
-// exits.  A call needs 32 B per component plus 64 B per (channel, component),
-// rounded up; larger problems are rejected with an error before anything is
-// launched.  The array is shared by all calls on a device and keeps the
-// previous call's contents; every call rewrites all of the scratch it reads,
-// so nothing needs clearing between calls.  Calls whose kernels overlap on
+// exits.  A call needs 64 B per component (LMN and envelope tables, 32 B
+// each) plus 64 B per (channel, component) (the flux table), each table
+// rounded up to 256 B; larger problems are rejected with an error before
+// anything is launched.  After the kernels the call reads its own error word
+// (a synchronous read on the legacy default stream), clears it if set and
+// returns the message, so a call never leaves an error for the next one.
+// The array is shared by all calls on a device and keeps the previous call's
+// contents; every call rewrites all of the scratch it reads, so nothing
+// needs clearing between calls.  Calls whose kernels overlap on
 // the GPU (concurrent calls from several host threads or streams on one
 // device) race on the array and must be serialised by the caller.
 //

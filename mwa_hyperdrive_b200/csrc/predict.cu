@@ -11,6 +11,7 @@
 // accumulation is FP64 and the visibility is updated once per type, as the
 // reference does (model/cpu.rs:341-348, gpu/model.cu:171).
 
+#include <atomic>
 #include <cstdio>
 #include <vector>
 
@@ -253,17 +254,27 @@ __global__ void __launch_bounds__(DT) direct_kernel(const DirectParams p) {
         bulk_g2s(s_flux[st], p.flux + (size_t)f * p.nc + c0, n * 64u, &bar[st]);
         if (TYPE) bulk_g2s(s_gp[st], p.gp + c0, n * 32u, &bar[st]);
     };
+    int issued = 0;  // chunks whose copies thread 0 has issued
     if (threadIdx.x == 0) {
         fence_proxy_async_smem();
-        if (nchunks > 0) issue(0);
-        if (nchunks > 1) issue(1);
+        if (!p.stall) {
+            if (nchunks > 0) issue(0), issued = 1;
+            if (nchunks > 1) issue(1), issued = 2;
+        }
     }
+    const uint64_t limit = p.wait_ns ? p.wait_ns : 2000000000ull;
 
     J2 acc = jzero();
+    bool aborted = false;
     for (int k = 0; k < nchunks; k++) {
         const int st = k & 1;
-        const bool ok = mbar_wait_bounded(&bar[st], (k >> 1) & 1, p.err);
-        if (__syncthreads_or(!ok)) break;
+        const bool ok = mbar_wait_bounded(&bar[st], (k >> 1) & 1, p.err, limit);
+        if (__syncthreads_or(!ok)) {
+            // the sum is incomplete: leave the visibilities untouched
+            if (threadIdx.x == 0) drain_two_stage(bar, k, issued);
+            aborted = true;
+            break;
+        }
         const int c0 = k * CH;
         const int n = min(CH, p.nc - c0);
         if (FAST) {
@@ -352,10 +363,11 @@ __global__ void __launch_bounds__(DT) direct_kernel(const DirectParams p) {
         if (threadIdx.x == 0 && k + 2 < nchunks) {
             fence_proxy_async_smem();
             issue(k + 2);
+            issued = k + 3;
         }
     }
 
-    if (!active) return;
+    if (!active || aborted) return;
     const size_t o = (size_t)f * p.nbl + bl;
     if (OUT64) {
         double2* q = reinterpret_cast<double2*>(reinterpret_cast<JonesF64*>(p.vis) + o);
@@ -450,19 +462,29 @@ __global__ void __launch_bounds__(DT, FastShape<TYPE>::MIN_CTAS) fast_kernel(con
         for (int i = 0; i < FCH; i++) bulk_g2s(s_flux[st][i], p.flux + (size_t)fr[i] * p.nc + c0, n * 64u, &bar[st]);
         bulk_g2s(s_gp[st], p.gp + c0, n * 32u, &bar[st]);
     };
+    int issued = 0;  // chunks whose copies thread 0 has issued
     if (threadIdx.x == 0) {
         fence_proxy_async_smem();
-        if (nchunks > 0) issue(0);
-        if (nchunks > 1) issue(1);
+        if (!p.stall) {
+            if (nchunks > 0) issue(0), issued = 1;
+            if (nchunks > 1) issue(1), issued = 2;
+        }
     }
+    const uint64_t limit = p.wait_ns ? p.wait_ns : 2000000000ull;
 
     J2 acc[FCH];
 #pragma unroll
     for (int i = 0; i < FCH; i++) acc[i] = jzero();
+    bool aborted = false;
     for (int k = 0; k < nchunks; k++) {
         const int st = k & 1;
-        const bool ok = mbar_wait_bounded(&bar[st], (k >> 1) & 1, p.err);
-        if (__syncthreads_or(!ok)) break;
+        const bool ok = mbar_wait_bounded(&bar[st], (k >> 1) & 1, p.err, limit);
+        if (__syncthreads_or(!ok)) {
+            // the sum is incomplete: leave the visibilities untouched
+            if (threadIdx.x == 0) drain_two_stage(bar, k, issued);
+            aborted = true;
+            break;
+        }
         const int c0 = k * CH;
         const int n = min(CH, p.nc - c0);
 #pragma unroll
@@ -543,10 +565,11 @@ __global__ void __launch_bounds__(DT, FastShape<TYPE>::MIN_CTAS) fast_kernel(con
         if (threadIdx.x == 0 && k + 2 < nchunks) {
             fence_proxy_async_smem();
             issue(k + 2);
+            issued = k + 3;
         }
     }
 
-    if (!active) return;
+    if (!active || aborted) return;
 #pragma unroll
     for (int i = 0; i < FCH; i++) {
         if (f0 + i >= p.nf) break;
@@ -605,8 +628,35 @@ static cudaError_t launch_t(bool tile_beam, bool out64, bool fast, const DirectP
     return cudaGetLastError();
 }
 
-cudaError_t launch_direct(int ty, bool tile_beam, bool out64, const DirectParams& p, cudaStream_t s, bool fast) {
+// hdc_test_stall_next_predict: wait limit [ns] for the next direct launch,
+// which then issues no table copies (0: off).
+static std::atomic<unsigned long long> g_stall_next_ns{0};
+
+const char* kernel_error_string(int word) {
+    if (word & KERR_TIMEOUT)
+        return "a predict kernel gave up waiting for its staged component tables (bounded wait ran out); "
+               "the visibilities of the affected CTAs were left unchanged";
+    if (word & KERR_INDEX) return "a kernel found an index outside its table (shapelet order or beam map)";
+    if (word) return "a kernel reported an unknown error";
+    return NULL;
+}
+
+int kernel_error_status(int word) {
+    if (word & KERR_TIMEOUT) return HDC_ERR_TIMEOUT;
+    if (word) return HDC_ERR_ARG;
+    return HDC_OK;
+}
+
+cudaError_t launch_direct(int ty, bool tile_beam, bool out64, const DirectParams& p_in, cudaStream_t s, bool fast) {
+    DirectParams p = p_in;
     if (p.nc <= 0 || p.nbl <= 0 || p.nf <= 0) return cudaSuccess;
+    if (g_stall_next_ns.load(std::memory_order_relaxed)) {
+        const unsigned long long ns = g_stall_next_ns.exchange(0);
+        if (ns) {
+            p.stall = 1;
+            p.wait_ns = ns;
+        }
+    }
     // the FP32 form needs per-tile shapelet UVs and the FP32 basis table
     fast = fast && !tile_beam && (ty != 2 || (p.suv_tile && !p.suv_bl && p.sbf32));
     if (fast && ty == 2 && p.sdense && !p.sbfp) return cudaErrorInvalidValue;
@@ -834,6 +884,8 @@ static const char* dropin_model(int type, const GroupIn g[3], const Addresses* a
     size_t total = align256(off_co + sizeof(ShapeletCoeff) * (size_t)(total_coeffs + 1));
     char* ws = (char*)device_scratch(total);
     if (!ws) return "out of device memory";
+    int* errw = dropin_error_word();
+    if (!errw) return "device error word unavailable";
 
     PrepIn in;
     for (int i = 0; i < 3; i++) in.g[i] = g[i];
@@ -859,15 +911,13 @@ static const char* dropin_model(int type, const GroupIn g[3], const Addresses* a
         dropin_suv_kernel<<<(unsigned)((n + 255) / 256), 256>>>(in);
         count_launches(1);
         HDC_CUDA_RET_STR(cudaGetLastError());
-        int* flag = device_error_word();
-        if (!flag) return "device error word unavailable";
-        dropin_coeff_kernel<<<1, 1>>>(in, cstart, ccount, co, flag);
+        dropin_coeff_kernel<<<1, 1>>>(in, cstart, ccount, co, errw);
         count_launches(1);
         HDC_CUDA_RET_STR(cudaGetLastError());
         int h = 0;
-        HDC_CUDA_RET_STR(cudaMemcpy(&h, flag, sizeof(int), cudaMemcpyDeviceToHost));
+        HDC_CUDA_RET_STR(cudaMemcpy(&h, errw, sizeof(int), cudaMemcpyDeviceToHost));
         if (h & KERR_INDEX) {
-            cudaMemset(flag, 0, sizeof(int));
+            cudaMemset(errw, 0, sizeof(int));
             set_error("model_shapelets: a shapelet coefficient order is outside 0..%d", SBF_N - 1);
             return "model_shapelets: shapelet coefficient order outside the basis table";
         }
@@ -894,13 +944,12 @@ static const char* dropin_model(int type, const GroupIn g[3], const Addresses* a
     p.suv_bl = type == 2 ? in.suv : nullptr;
     p.suv_tile = nullptr;
     p.vis = d_vis_fb;
-    p.err = device_error_word();
+    p.err = errw;
     const bool tile_beam = d_beam_jones != nullptr;
     HDC_CUDA_RET_STR(launch_direct(type, tile_beam, out64, p, 0));
-#ifdef HDC_DEBUG_SYNC
-    HDC_CUDA_RET_STR(cudaDeviceSynchronize());
-#endif
-    return NULL;
+    // a bounded wait that ran out leaves part of d_vis_fb without this call's
+    // sum: report it (and clear the word) instead of returning success
+    return take_word_sync(errw, type == 0 ? "model_points" : type == 1 ? "model_gaussians" : "model_shapelets");
 }
 
 // Bytes of workspace the point-source drop-in path needs for nc components
@@ -959,7 +1008,7 @@ const char* points_with_workspace(const Points* comps, const Addresses* a, const
     p.vis = d_vis_fb;
     p.err = err_word;
     HDC_CUDA_RET_STR(launch_direct(0, d_beam_jones != nullptr, false, p, 0));
-    return NULL;
+    return take_word_sync(err_word, "model_points_noalloc");
 }
 
 }  // namespace hdc
@@ -1057,10 +1106,12 @@ extern "C" const char* model_points_tc(const Points* comps, const Addresses* a, 
         HDC_CUDA_RET_STR(cudaGetLastError());
         W = Wb;
     }
+    int* errw = dropin_error_word();
+    if (!errw) return "device error word unavailable";
     const int rc = launch_tensor_points(nf, nbl, ntiles, nc, a->d_freqs, d_tile_xyzs, lst_rad - phase_centre.ra,
-                                        phase_centre.dec, in.lmn, W, d_vis_fb, false, device_error_word(), 0);
+                                        phase_centre.dec, in.lmn, W, d_vis_fb, false, errw, 0);
     if (rc) return hdc_last_error();
-    return NULL;
+    return take_word_sync(errw, "model_points_tc");
 }
 
 extern "C" const char* model_gaussians(const Gaussians* comps, const Addresses* a, const UVW* d_uvws,
@@ -1195,3 +1246,10 @@ extern "C" const char* model_autos(int num_tiles, int num_freqs, const double* f
     HDC_CUDA_RET_STR(launch_autos(p, 0));
     return NULL;
 }
+
+extern "C" int hdc_test_stall_next_predict(unsigned long long wait_ns) {
+    g_stall_next_ns.store(wait_ns);
+    return HDC_OK;
+}
+
+extern "C" const char* hdc_kernel_error_string(int word) { return kernel_error_string(word); }

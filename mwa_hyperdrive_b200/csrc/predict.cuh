@@ -41,7 +41,18 @@ struct DirectParams {
     const double2* suv_tile;   // [nc][ntiles] m, or NULL (then suv = tile1 - tile2)
     void* vis;                 // [nf][nbl] JonesF32 or JonesF64, accumulated
     int* err;
+    // Limit of each bounded wait on the staged tables [ns] (0: the default
+    // 2 s).  stall != 0 (set only through hdc_test_stall_next_predict) issues
+    // none of the table copies, so that the first wait runs out with nothing
+    // in flight.
+    unsigned long long wait_ns;
+    int stall;
 };
+
+// Static message for a kernel error word (KERR_* bits), NULL for 0.
+const char* kernel_error_string(int word);
+// Status code of a kernel error word for the native layer (HDC_OK for 0).
+int kernel_error_status(int word);
 
 // Launch the direct kernel for component type ty (0 point, 1 Gaussian,
 // 2 shapelet).  tile_beam selects per-tile beam Jones; out64 an FP64 output;

@@ -9,7 +9,7 @@
 #include <mutex>
 #include <vector>
 
-#include "common.cuh"
+#include "predict.cuh"
 
 namespace hdc {
 
@@ -51,6 +51,7 @@ std::mutex g_mu;
 void* g_scratch[MAX_DEV] = {};
 size_t g_scratch_size[MAX_DEV] = {};
 int* g_errword[MAX_DEV] = {};
+int* g_dropin_err[MAX_DEV] = {};
 double* g_sbf[MAX_DEV] = {};
 float* g_sbf32[MAX_DEV] = {};
 float4* g_sbfp[MAX_DEV] = {};
@@ -124,6 +125,34 @@ int* device_error_word() {
         cudaMemset(g_errword[d], 0, sizeof(int));
     }
     return g_errword[d];
+}
+
+int* dropin_error_word() {
+    std::lock_guard<std::mutex> lk(g_mu);
+    int d = cur_dev();
+    if (d < 0) return nullptr;
+    if (!g_dropin_err[d]) {
+        if (cudaMalloc(&g_dropin_err[d], sizeof(int)) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        cudaMemset(g_dropin_err[d], 0, sizeof(int));
+    }
+    return g_dropin_err[d];
+}
+
+const char* take_word_sync(int* w, const char* who) {
+    int h = 0;
+    cudaError_t e = cudaMemcpy(&h, w, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) {
+        set_error("%s: %s", who, cudaGetErrorString(e));
+        return cudaGetErrorString(e);
+    }
+    if (!h) return NULL;
+    cudaMemset(w, 0, sizeof(int));
+    const char* msg = kernel_error_string(h);
+    set_error("%s: %s", who, msg);
+    return msg;
 }
 
 int take_device_error(cudaStream_t s) {
@@ -282,6 +311,30 @@ extern "C" int hdc_device_info(char* buf, int buf_len) {
              (double)prop.totalGlobalMem / (1024.0 * 1024.0 * 1024.0), rt / 1000, (rt % 1000) / 10, drv / 1000,
              (drv % 1000) / 10);
     return HDC_OK;
+}
+
+// The reference's device query (gpu/utils.h:28, bound by gpu/utils_bindings.rs
+// and called from gpu/utils.rs:35-60 for the solutions' MODELLER string): make
+// `device` current and report its name (NUL-terminated, at most 255
+// characters), compute capability, global memory [bytes] and the CUDA driver
+// and runtime versions as integers (1000 * major + 10 * minor).  NULL on
+// success, else the CUDA error string.
+extern "C" const char* get_gpu_device_info(int device, char name[256], int* device_major, int* device_minor,
+                                           size_t* total_global_mem, int* driver_version, int* runtime_version) {
+    cudaError_t e = cudaSetDevice(device);
+    cudaDeviceProp prop;
+    if (e == cudaSuccess) e = cudaGetDeviceProperties(&prop, device);
+    if (e == cudaSuccess) e = cudaDriverGetVersion(driver_version);
+    if (e == cudaSuccess) e = cudaRuntimeGetVersion(runtime_version);
+    if (e != cudaSuccess) {
+        hdc::set_error("get_gpu_device_info: %s", cudaGetErrorString(e));
+        return cudaGetErrorString(e);
+    }
+    snprintf(name, 256, "%s", prop.name);
+    *device_major = prop.major;
+    *device_minor = prop.minor;
+    *total_global_mem = prop.totalGlobalMem;
+    return NULL;
 }
 
 // Host copy of the shapelet basis table (for tests and for callers that

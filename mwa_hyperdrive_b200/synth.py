@@ -130,6 +130,19 @@ def config2(n_points=4000, n_gauss=500, n_shapelets=100, n_freqs=384, n_times=4)
     return obs, sl.SkyModelArrays.from_components(comps)
 
 
+def sample_tiles(ntiles: int, k: int, seed: int):
+    """A seeded random subset of k of ntiles tiles (sorted) and the indices,
+    in the full set's baseline order, of the k (k - 1) / 2 baselines among
+    them -- in the same order as the subset's own baselines.  Every baseline
+    is equally likely to be in the sample."""
+    rng = np.random.default_rng(seed)
+    sub = np.sort(rng.choice(ntiles, size=k, replace=False))
+    i, j = np.triu_indices(k, 1)
+    p, q = sub[i], sub[j]
+    bl = p * (2 * ntiles - p - 1) // 2 + (q - p - 1)
+    return sub, bl.astype(np.int64)
+
+
 def truth_gains(ntiles: int, nch: int, rng, amp_sigma=0.1, leak_sigma=0.01, phase_slope=None, freqs=None):
     """Per (tile, chanblock) Jones gains: diagonal amplitude N(1, amp_sigma),
     phase U(-pi, pi) (or a per-tile linear phase in frequency when

@@ -2,7 +2,7 @@
 known-answer tests.
 
 Run in an environment that has the mwa_hyperdrive source tree (pass its root
-as argv[1]); the outputs are committed so that nothing reads the reference at
+as argv[1] or in HDC_REFERENCE_DIR); the outputs are committed so that nothing reads the reference at
 test time.
 
 * model_kats.json  -- expected no-beam visibilities (f32, epsilon 0 in the
@@ -16,6 +16,10 @@ test time.
   astropy through test_files/gen_fits_srclists.py), base64, with the YAML
   lists that hold the same sources; they check the FITS reader against an
   independent FITS writer.
+* ref_struct_layouts.json -- sizeof/offsetof of every drop-in FFI struct
+  measured by compiling layout_probe.py's probe against the reference's
+  src/gpu/types.h (FP64 build), and the parameter types of the reference's
+  drop-in C functions as defined in src/gpu/{model,peel,utils}.cu.
 * shapelet_basis_samples.json -- samples of the shapelet basis table produced
   by the reference's generator script src/model/make_shapelet_basis_values.py
   (imported, its gen_shape_basis evaluated at the sampled points), plus the
@@ -159,5 +163,24 @@ def main(ref_root: str) -> None:
         json.dumps({"source": "test_files/{jack,gleam,lobes}.{fits,yaml}", "lists": fl}, indent=1))
 
 
+def layouts(ref_root: str) -> None:
+    spec = importlib.util.spec_from_file_location("layout_probe", HERE / "layout_probe.py")
+    lp = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(lp)
+    gpu = Path(ref_root) / "src" / "gpu"
+    protos = {}
+    for f in ["model.cu", "peel.cu", "utils.cu"]:
+        protos.update(lp.prototypes((gpu / f).read_text()))
+    (HERE / "ref_struct_layouts.json").write_text(json.dumps(
+        {"source": "src/gpu/types.h (FP64 build), src/gpu/{model,peel,utils}.cu definitions",
+         "layouts": lp.probe(gpu / "types.h"), "prototypes": protos}, indent=1) + "\n")
+
+
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    import os
+
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("HDC_REFERENCE_DIR")
+    if not root:
+        sys.exit("usage: make_golden.py <mwa_hyperdrive source root> (or set HDC_REFERENCE_DIR)")
+    main(root)
+    layouts(root)

@@ -196,6 +196,36 @@ def test_f32_output_and_accumulate(oracle):
     assert nrm < 5e-6  # f32 output rounding dominates
 
 
+@pytest.mark.parametrize("ctype,name", [(0, "points"), (1, "Gaussians"), (2, "shapelets")])
+def test_full_mixed_config_chosen_form_vs_fp64_oracle(oracle, ctype, name):
+    """The timed configuration itself: 128 tiles, all 4 timesteps and 384
+    channels, 4000 points / 500 Gaussians / 100 shapelets (20 coefficients)
+    through the analytic beam, each class predicted by the chosen form
+    (tensor-core points, FP32-form Gaussians and shapelets) with the f32
+    output the benchmark times, against the FP64 oracle on a seeded sample
+    of 276 baselines (every baseline among 24 random tiles) at every
+    (timestep, channel).  Bars: normwise and p99.9 below 1e-6."""
+    obs, sky = synth.config2()
+    cls = sky.select(sky.comp_type == ctype)
+    sub, bl = synth.sample_tiles(obs.num_tiles, 24, 2024)
+    m = SkyModeller(cls, obs.tile_xyzs, obs.freqs, obs.phase_centre, obs.latitude, beam="analytic", form="tensor")
+    vis = torch.zeros((obs.freqs.size, obs.num_baselines, 8), dtype=torch.float32, device="cuda")
+    idx = torch.from_numpy(bl).cuda()
+    got, ref = [], []
+    for t, lst in enumerate(obs.lsts):
+        vis.zero_()
+        m.model_timestep_with(float(lst), vis, return_uvws=False)
+        got.append(vis.index_select(1, idx).cpu().numpy())
+        r, _ = oracle.model_timestep(cls, obs.tile_xyzs[sub], obs.freqs, obs.phase_centre, float(lst), obs.latitude,
+                                     beam=oracle.beam_struct(1), out_f64=True)
+        ref.append(r)
+    m.close()
+    nrm, p999, mx = errors(np.stack(got), np.stack(ref))
+    print(f"config 2 {name} ({cls.num_components}), 4 x 384 x 276 sampled: normwise {nrm:.2e}, p99.9 {p999:.2e}, "
+          f"max {mx:.2e}")
+    assert nrm < TOL and p999 < TOL, (nrm, p999, mx)
+
+
 def test_unsupported_tile_count_is_refused():
     from mwa_hyperdrive_b200 import _lib
 
