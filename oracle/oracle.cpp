@@ -1398,4 +1398,196 @@ int or_into_cal_sols(const double* in, int ntb, int nut, int nuc, const int* fti
     return 0;
 }
 
+
+// ---------------------------------------------------------------------------
+// peel_cpu (params/peel/mod.rs:1121-1475), the reference's CPU peel loop, with
+// its helpers vis_rotate_tfb (:783-825), apply_iono_tfb (:829-893),
+// vis_average_tfb (:648-707), weights_average (:709-755), iono_fit
+// (:960-1076, or_iono_fit above) and unpeel_model (:897-956).  No precession
+// (the tile XYZs are used at every timestep with the given LMSTs, as
+// `no_precession`).  Arrays [t][f][bl] JonesF32 / f32 weights; the modeller is
+// SkyModellerCpu at the observation phase centre (model_timestep_with, f32
+// output).  num_passes and num_loops are the loop counts as used (the
+// reference destructures PeelLoopParams::get() with the two swapped,
+// mod.rs:1138 vs :218-224: a caller reproducing that passes them swapped).
+// The loops over timesteps run in parallel where the reference uses rayon
+// (vis_rotate_tfb, unpeel_model); everything else is sequential as there.
+// ---------------------------------------------------------------------------
+}  // extern "C"
+
+namespace {
+
+// tile (u, v, w) of every tile at hour angle ha, declination dec
+void tile_uvws(const double* xyzs, int ntiles, double ha, double dec, double* out /*[tile][3]*/) {
+    const double s_ha = std::sin(ha), c_ha = std::cos(ha), s_dec = std::sin(dec), c_dec = std::cos(dec);
+    for (int i = 0; i < ntiles; i++) uvw_from_xyz(xyzs + 3 * i, s_ha, c_ha, s_dec, c_dec, out + 3 * i);
+}
+
+// vis_rotate_fb: rot = vis * cis(-tau ((w1_to - w2_to) - (w1_from - w2_from)) / lambda)
+void rotate_fb(const float* vis, float* out, const double* tuvw_from, const double* tuvw_to, int ntiles, int nf,
+               const double* lambdas) {
+    const int nbl = ntiles * (ntiles - 1) / 2;
+    int i1 = 0, i2 = 0;
+    for (int b = 0; b < nbl; b++) {
+        i2 += 1;
+        if (i2 == ntiles) {
+            i1 += 1;
+            i2 = i1 + 1;
+        }
+        const double w_diff = (tuvw_to[3 * i1 + 2] - tuvw_to[3 * i2 + 2]) - (tuvw_from[3 * i1 + 2] - tuvw_from[3 * i2 + 2]);
+        const double arg = -TAU * w_diff;
+        for (int f = 0; f < nf; f++) {
+            const size_t step = (size_t)f * nbl + b;
+            to_f32(jmulc(from_f32(vis + 8 * step), cis(arg / lambdas[f])), out + 8 * step);
+        }
+    }
+}
+
+// apply_iono_fb over tile (u, v, w) triples
+void iono_fb(const float* vis, float* out, const double* tuvw, int ntiles, int nf, OrIono c, const double* lambdas) {
+    const int nbl = ntiles * (ntiles - 1) / 2;
+    int i1 = 0, i2 = 0;
+    for (int b = 0; b < nbl; b++) {
+        i2 += 1;
+        if (i2 == ntiles) {
+            i1 += 1;
+            i2 = i1 + 1;
+        }
+        const double u = tuvw[3 * i1] - tuvw[3 * i2], v = tuvw[3 * i1 + 1] - tuvw[3 * i2 + 1];
+        const double arg = -TAU * (u * c.alpha + v * c.beta);
+        for (int f = 0; f < nf; f++) {
+            const c64 rot = cscale(cis(arg * lambdas[f]), c.gain);
+            const size_t step = (size_t)f * nbl + b;
+            to_f32(jmulc(from_f32(vis + 8 * step), rot), out + 8 * step);
+        }
+    }
+}
+
+// vis_average_tfb into one low-res timestep: [nt][nf][nbl] -> [nf / favg][nbl]
+// (weights assumed capped at zero; an output with no weight is left as is)
+void average_tfb(const float* from, const float* w, float* to, int nt, int nf, int nbl, int favg) {
+    const int nlo = (nf + favg - 1) / favg;
+    for (int fl = 0; fl < nlo; fl++)
+        for (int b = 0; b < nbl; b++) {
+            J64 sum = jzero();
+            double ws = 0.0;
+            for (int t = 0; t < nt; t++)
+                for (int f = fl * favg; f < std::min(nf, (fl + 1) * favg); f++) {
+                    const size_t step = ((size_t)t * nf + f) * nbl + b;
+                    sum = jadd(sum, jscale(from_f32(from + 8 * step), (double)w[step]));
+                    ws += (double)w[step];
+                }
+            if (ws > 0.0) to_f32(jscale(sum, 1.0 / ws), to + 8 * ((size_t)fl * nbl + b));
+        }
+}
+
+}  // namespace
+
+extern "C" {
+
+int or_peel_cpu(float* resid, const float* weights, int nt, int nf, const double* freqs, const double* xyzs, int ntiles,
+                const double* lmsts, double average_lmst, double pc_ra, double pc_dec, int num_sources,
+                const OrSky* const* sources, const double* positions /*[src][2]*/, OrIono* consts, int num_passes,
+                int num_loops, double convergence, int favg, double lat) {
+    const int nbl = ntiles * (ntiles - 1) / 2;
+    const int nlo = (nf + favg - 1) / favg;
+    const size_t nvis = (size_t)nt * nf * nbl, slab = (size_t)nf * nbl;
+    std::vector<double> lam(nf), lam_lo(nlo);
+    for (int f = 0; f < nf; f++) lam[f] = VEL_C / freqs[f];
+    // low-res wavelengths from the mean frequency of each channel group
+    for (int fl = 0; fl < nlo; fl++) {
+        double s = 0.0;
+        int n = 0;
+        for (int f = fl * favg; f < std::min(nf, (fl + 1) * favg); f++, n++) s += freqs[f];
+        lam_lo[fl] = VEL_C / (s / n);
+    }
+    // tile UVWs at the observation phase centre, per timestep
+    std::vector<double> tuvw_obs(3 * (size_t)nt * ntiles), tuvw_src(3 * (size_t)nt * ntiles), tuv_lo(2 * (size_t)ntiles);
+    for (int t = 0; t < nt; t++) tile_uvws(xyzs, ntiles, lmsts[t] - pc_ra, pc_dec, &tuvw_obs[3 * (size_t)t * ntiles]);
+    std::vector<float> resid_src(8 * nvis), model_obs(8 * nvis), model_src(8 * nvis), model_src_iono(8 * nvis);
+    std::vector<float> resid_lo(8 * (size_t)nlo * nbl, 0.f), model_lo(8 * (size_t)nlo * nbl, 0.f);
+    // weights_average: the sum over the timeblock and each channel group, >= 0
+    std::vector<float> w_lo((size_t)nlo * nbl);
+    for (int fl = 0; fl < nlo; fl++)
+        for (int b = 0; b < nbl; b++) {
+            double s = 0.0;
+            for (int t = 0; t < nt; t++)
+                for (int f = fl * favg; f < std::min(nf, (fl + 1) * favg); f++) s += (double)weights[((size_t)t * nf + f) * nbl + b];
+            w_lo[(size_t)fl * nbl + b] = std::max((float)s, 0.f);
+        }
+    OrBeam nobeam = {};
+    for (int pass = 0; pass < num_passes; pass++) {
+        for (int s = 0; s < num_sources; s++) {
+            const OrIono old = consts[s];
+            const double src_ra = positions[2 * s], src_dec = positions[2 * s + 1];
+            // high-res model of this source at the observation phase centre
+            std::fill(model_obs.begin(), model_obs.end(), 0.f);
+            for (int t = 0; t < nt; t++) {
+                or_model_timestep(sources[s], xyzs, ntiles, freqs, nf, pc_ra, pc_dec, lmsts[t], lat, &nobeam, 0,
+                                  &model_obs[8 * t * slab], 0, nullptr);
+                tile_uvws(xyzs, ntiles, lmsts[t] - src_ra, src_dec, &tuvw_src[3 * (size_t)t * ntiles]);
+            }
+            {
+                std::vector<double> tmp(3 * (size_t)ntiles);
+                tile_uvws(xyzs, ntiles, average_lmst - src_ra, src_dec, tmp.data());
+                for (int i = 0; i < ntiles; i++) tuv_lo[2 * i] = tmp[3 * i], tuv_lo[2 * i + 1] = tmp[3 * i + 1];
+            }
+            // rotate residual and model to the source phase centre
+#pragma omp parallel for schedule(static)
+            for (int t = 0; t < nt; t++) {
+                rotate_fb(resid + 8 * t * slab, &resid_src[8 * t * slab], &tuvw_obs[3 * (size_t)t * ntiles],
+                          &tuvw_src[3 * (size_t)t * ntiles], ntiles, nf, lam.data());
+                rotate_fb(&model_obs[8 * t * slab], &model_src[8 * t * slab], &tuvw_obs[3 * (size_t)t * ntiles],
+                          &tuvw_src[3 * (size_t)t * ntiles], ntiles, nf, lam.data());
+            }
+            for (int t = 0; t < nt; t++)
+                iono_fb(&model_src[8 * t * slab], &model_src_iono[8 * t * slab], &tuvw_src[3 * (size_t)t * ntiles], ntiles,
+                        nf, consts[s], lam.data());
+            for (size_t k = 0; k < 8 * nvis; k++) resid_src[k] += model_src_iono[k];
+            average_tfb(resid_src.data(), weights, resid_lo.data(), nt, nf, nbl, favg);
+            for (int it = 0; it < num_loops; it++) {
+                for (int t = 0; t < nt; t++)
+                    iono_fb(&model_src[8 * t * slab], &model_src_iono[8 * t * slab], &tuvw_src[3 * (size_t)t * ntiles],
+                            ntiles, nf, consts[s], lam.data());
+                average_tfb(model_src_iono.data(), weights, model_lo.data(), nt, nf, nbl, favg);
+                double fit[4];
+                or_iono_fit(resid_lo.data(), w_lo.data(), model_lo.data(), lam_lo.data(), tuv_lo.data(), 1, nlo, ntiles,
+                            fit);
+                const double da = fit[0], db = fit[1], dg = fit[2] / fit[3];
+                consts[s].alpha += convergence * da;
+                consts[s].beta += convergence * db;
+                consts[s].gain *= 1. + convergence * (dg - 1.);
+                if (std::sqrt(std::pow(da, 2.) + std::pow(db, 2.) + std::pow(dg - 1., 2.)) < 1e-8) break;
+            }
+            // unpeel_model: the model at the observation phase centre with the
+            // source's tile UVs (as the reference does)
+            const OrIono c = consts[s];
+#pragma omp parallel for schedule(static)
+            for (int t = 0; t < nt; t++) {
+                const double* tu = &tuvw_src[3 * (size_t)t * ntiles];
+                int i1 = 0, i2 = 0;
+                for (int b = 0; b < nbl; b++) {
+                    i2 += 1;
+                    if (i2 == ntiles) {
+                        i1 += 1;
+                        i2 = i1 + 1;
+                    }
+                    const double u = tu[3 * i1] - tu[3 * i2], v = tu[3 * i1 + 1] - tu[3 * i2 + 1];
+                    const double arg = -TAU * (u * c.alpha + v * c.beta);
+                    const double old_arg = -TAU * (u * old.alpha + v * old.beta);
+                    for (int f = 0; f < nf; f++) {
+                        const size_t step = (size_t)t * slab + (size_t)f * nbl + b;
+                        J64 j = from_f32(resid + 8 * step);
+                        const J64 m = from_f32(&model_obs[8 * step]);
+                        j = jadd(j, jmulc(m, cscale(cis(old_arg * lam[f]), old.gain)));
+                        j = jsub(j, jmulc(m, cscale(cis(arg * lam[f]), c.gain)));
+                        to_f32(j, resid + 8 * step);
+                    }
+                }
+            }
+        }
+    }
+    return 0;
+}
+
 }  // extern "C"

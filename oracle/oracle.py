@@ -400,3 +400,24 @@ def weights_rts(tile_uvs, lambdas, sigma):
     lib().or_weights_rts(_ptr(tile_uvs), ctypes.c_int(nt), ctypes.c_int(ntiles), _ptr(lambdas),
                          ctypes.c_int(lambdas.size), ctypes.c_double(sigma), _ptr(out))
     return out
+
+
+def peel_cpu(resid, weights, freqs, xyzs, lmsts, average_lmst, pc, sources, positions, consts, num_passes, num_loops,
+             convergence, favg, lat):
+    """peel_cpu (params/peel/mod.rs:1121-1475) on the CPU: resid [t][f][bl][8]
+    float32 is peeled in place (a copy is returned), consts [(alpha, beta,
+    gain)] per source are the starting values; returns (resid, consts)."""
+    resid = np.ascontiguousarray(resid, np.float32).copy()
+    nt, nf, nbl = resid.shape[:3]
+    xyzs = np.ascontiguousarray(xyzs, np.float64)
+    structs = [sky_struct(s) for s in sources]
+    arr = (ctypes.POINTER(OrSky) * len(sources))(*[ctypes.pointer(st) for st, _ in structs])
+    pos = np.ascontiguousarray(np.asarray(positions, np.float64).reshape(-1, 2))
+    cs = (OrIono * len(sources))(*[OrIono(*c) for c in consts])
+    lib().or_peel_cpu(_ptr(resid), _ptr(np.ascontiguousarray(weights, np.float32)), ctypes.c_int(nt), ctypes.c_int(nf),
+                      _ptr(np.ascontiguousarray(freqs, np.float64)), _ptr(xyzs), ctypes.c_int(xyzs.shape[0]),
+                      _ptr(np.ascontiguousarray(lmsts, np.float64)), ctypes.c_double(average_lmst),
+                      ctypes.c_double(pc[0]), ctypes.c_double(pc[1]), ctypes.c_int(len(sources)), arr, _ptr(pos), cs,
+                      ctypes.c_int(num_passes), ctypes.c_int(num_loops), ctypes.c_double(convergence),
+                      ctypes.c_int(favg), ctypes.c_double(lat))
+    return resid, [(c.alpha, c.beta, c.gain) for c in cs]

@@ -65,7 +65,7 @@ class DropinPoints:
             self.keep.append(t)
             return t.data_ptr()
 
-        self.points = _lib.Points(nc, put(lmn), put(inst150), put([c.flux.si for c in comps]), 0, 0, 0, 0, 0, 0, 0,
+        self.points = _lib.Points(nc, put(lmn), put(inst150), put([c.flux_type.si for c in comps]), 0, 0, 0, 0, 0, 0, 0,
                                   0)
         self.addr = _lib.Addresses(nf, nf * self.nbl, self.nbl, put(obs.freqs), 0, 0, 0, 0, 0)
         self.uvws = put(uvws)
