@@ -200,10 +200,12 @@ const char *model_points_f64out(const Points *comps, const Addresses *a, const U
  * within 1e-6 of the FP64 predict).  No counterpart in the reference.  Takes
  * the per-tile XYZs (d_tile_xyzs [tile], metres, the tile order of the
  * baselines), the LST and the phase centre instead of per-baseline UVWs: the
- * predict factors per tile because uvw_pq = R (xyz_p - xyz_q).  The beam
- * must be one for all tiles: d_beam_jones NULL, or the reference's layout
- * [uniq_tile][uniq_freq][component] with every tile mapped to one row.  Up
- * to 128 tiles. */
+ * predict factors per tile because uvw_pq = R (xyz_p - xyz_q).  The beam is
+ * d_beam_jones NULL (none) or the reference's layout [uniq_tile][uniq_freq]
+ * [component] with Addresses' tile and frequency maps: when every tile maps
+ * to one row it is applied as W = B S B^H per component, otherwise per tile
+ * (the block form over twice the components, about twice the tensor-core
+ * work).  Any number of tiles (blocks of 128 x 64 tiles). */
 const char *model_points_tc(const Points *comps, const Addresses *a, const XYZ *d_tile_xyzs, double lst_rad,
                             RADec phase_centre, const JonesF64 *d_beam_jones, JonesF32 *d_vis_fb);
 
@@ -336,6 +338,7 @@ typedef struct HdcSkyModel {
 /* Beam used by the native modeller. */
 #define HDC_BEAM_NONE 0          /* identity Jones (beam/mod.rs:255-388 NoBeam) */
 #define HDC_BEAM_ANALYTIC_DIPOLE 1 /* 4x4 dipole tile over a ground plane, shared by all tiles */
+#define HDC_BEAM_ANALYTIC_PER_TILE 2 /* the same tile with each tile's own dipole gains (hdc_modeller_set_tile_beams) */
 
 /* Veto brightness of every source of a source list (srclist/veto.rs:58-129),
  * on the device: per coarse frequency h_freqs [Hz], the sum over a source's
@@ -371,6 +374,19 @@ int hdc_modeller_new(const HdcSkyModel *sky, int pols, const XYZ *h_unflagged_ti
 void hdc_modeller_free(HdcModeller *m);
 
 int hdc_modeller_set_tile_xyzs(HdcModeller *m, const XYZ *h_tile_xyzs);
+
+/* Per-tile beams (BeamGpu::calc_jones_pair, beam/mod.rs:342-367): switch the
+ * modeller to HDC_BEAM_ANALYTIC_PER_TILE with the amplitude of every dipole
+ * of every tile, h_dipole_gains [tile][2][16] (X dipoles then Y dipoles,
+ * row-major over the 4 x 4 grid from the south-west corner, 0 for a dead
+ * dipole; a tile with all 16 at 1 has the HDC_BEAM_ANALYTIC_DIPOLE beam).
+ * Tiles with equal gains share one beam (the reference's unique tiles); the
+ * beam is evaluated per timestep at the nearest multiple of freq_res_hz of
+ * each channel (1.28e6: the MWA coarse channels, the frequency resolution of
+ * the reference's FEE beam), in the reference's [uniq_tile][uniq_freq]
+ * [component] layout.  The direct form applies B_p S B_q^H per baseline; the
+ * tensor form uses its block form (twice the components). */
+int hdc_modeller_set_tile_beams(HdcModeller *m, const double *h_dipole_gains, double freq_res_hz);
 
 /* SkyModeller::model_timestep_with at a given LMST (the device-level form the
  * reference's peel loop calls, model/gpu.rs:1152-1166): d_vis_fb [freq][bl]

@@ -120,6 +120,7 @@ SIGNATURES = {
                                  ctypes.POINTER(c_void_p)]),
     "hdc_modeller_free": (None, [c_void_p]),
     "hdc_modeller_set_tile_xyzs": (c_int, [c_void_p, c_void_p]),
+    "hdc_modeller_set_tile_beams": (c_int, [c_void_p, c_void_p, c_double]),
     "hdc_modeller_model_timestep_with": (c_int, [c_void_p, c_double, c_void_p, c_void_p, c_void_p]),
     "hdc_modeller_model_timestep_with_f64": (c_int, [c_void_p, c_double, c_void_p, c_void_p, c_void_p]),
     "hdc_modeller_model_timestep_with_host": (c_int, [c_void_p, c_double, c_void_p, c_void_p, c_void_p]),

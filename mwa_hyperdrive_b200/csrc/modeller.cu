@@ -162,6 +162,46 @@ __device__ J2 analytic_beam(double az, double el, double freq) {
     return J2{amp * p00, amp * p01, amp * p01, amp * p11};
 }
 
+// The same tile with its own dipole amplitudes g [2][16] (X dipoles, then Y;
+// dipole d at east (d % 4 - 1.5) 1.1 m, north (d / 4 - 1.5) 1.1 m):
+// J = diag(ax, ay) R(az)^T diag(cos za, 1) R(az), ax = AF(g_x) GP / |GP(0)|,
+// AF(g) = (1/16) sum_d g_d exp(i k (x_d l + y_d m)).  With every g_d = 1,
+// AF = AFx(l) AFy(m) and J is analytic_beam's.
+__device__ J2 analytic_beam_tile(double az, double el, double freq, const double* g) {
+    if (el <= 0.0) return jzero();
+    const double za = FRAC_PI_2 - el;
+    const double k = TAU * freq / VEL_C;
+    double sza, cza, saz, caz;
+    sincos(za, &sza, &cza);
+    sincos(az, &saz, &caz);
+    const double l = sza * saz, m = sza * caz;
+    cplx ex[4], ey[4];
+    for (int i = 0; i < 4; i++) {
+        const double x = (i - 1.5) * 1.1;
+        double s, c;
+        sincos(k * x * l, &s, &c);
+        ex[i] = cplx{c, s};
+        sincos(k * x * m, &s, &c);
+        ey[i] = cplx{c, s};
+    }
+    cplx afx = {0.0, 0.0}, afy = {0.0, 0.0};
+    for (int d = 0; d < 16; d++) {
+        const cplx e = ex[d & 3] * ey[d >> 2];
+        afx = afx + e * g[d];
+        afy = afy + e * g[16 + d];
+    }
+    const double h = 0.278;
+    double sp, cp;
+    sincos(2.0 * k * h * cza, &sp, &cp);
+    const double gp0 = 2.0 * fabs(sin(k * h));
+    const cplx gp = cplx{1.0 - cp, sp} * (1.0 / (16.0 * gp0));
+    const cplx ax = afx * gp, ay = afy * gp;
+    const double p00 = cza * saz * saz + caz * caz;
+    const double p01 = (cza - 1.0) * saz * caz;
+    const double p11 = cza * caz * caz + saz * saz;
+    return J2{ax * p00, ax * p01, ay * p01, ay * p11};
+}
+
 // ERFA hd2ae (marlu HADec::to_azel).
 __device__ void hadec_to_azel(double ha, double dec, double lat, double& az, double& el) {
     double s_ha, c_ha, s_dec, c_dec, s_lat, c_lat;
@@ -192,6 +232,19 @@ __global__ void beam_weight_kernel(const double2* radec, int nc, const double* f
     W[(size_t)f * nc + c] = store_j((b * s) * herm(b));
 }
 
+// Per-tile beams B [uniq tile][uniq freq][nc] of one component type at this
+// timestep.
+__global__ void tile_beam_kernel(const double2* radec, int nc, const double* ufreqs, int nuf, const double* gains,
+                                 double lst, double lat, JonesF64* B) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int uf = blockIdx.y, u = blockIdx.z;
+    if (c >= nc) return;
+    const double2 rd = radec[c];
+    double az, el;
+    hadec_to_azel(lst - rd.x, rd.y, lat, az, el);
+    B[((size_t)u * nuf + uf) * nc + c] = store_j(analytic_beam_tile(az, el, ufreqs[uf], gains + 32 * u));
+}
+
 // ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
@@ -207,7 +260,16 @@ static void dfree(T*& p) {
     p = nullptr;
 }
 
+void TileBeams::release() {
+    dfree(d_gains);
+    dfree(d_tile_map);
+    dfree(d_freqs);
+    dfree(d_freq_map);
+    n_uniq_tile = n_uniq_freq = 0;
+}
+
 void TypeTables::release() {
+    dfree(d_B);
     dfree(d_lmn);
     dfree(d_S);
     dfree(d_W);
@@ -328,7 +390,7 @@ int Modeller::build_tables(const HdcSkyModel* sky) {
         if (e == cudaSuccess) e = cudaDeviceSynchronize();
         cudaFree(d_fc);
         HDC_CUDA_RET_INT(e);
-        if (beam_kind != HDC_BEAM_NONE) HDC_CUDA_RET_INT(dalloc(&tt.d_W, (size_t)nf * nc));
+        if (beam_kind == HDC_BEAM_ANALYTIC_DIPOLE) HDC_CUDA_RET_INT(dalloc(&tt.d_W, (size_t)nf * nc));
         if (ty == 2) {
             HDC_CUDA_RET_INT(dalloc(&tt.d_coeffs, coeffs.size() + 1));
             if (!coeffs.empty())
@@ -357,7 +419,63 @@ int Modeller::build_tables(const HdcSkyModel* sky) {
             }
         }
     }
+    if (tile_beams()) return alloc_tile_beam_tables();
     return HDC_OK;
+}
+
+int Modeller::alloc_tile_beam_tables() {
+    for (int ty = 0; ty < 3; ty++) {
+        dfree(t[ty].d_B);
+        if (t[ty].nc == 0) continue;
+        HDC_CUDA_RET_INT(dalloc(&t[ty].d_B, (size_t)tb.n_uniq_tile * tb.n_uniq_freq * t[ty].nc));
+    }
+    return HDC_OK;
+}
+
+int Modeller::set_tile_beams(const double* h_gains, double freq_res_hz) {
+    if (!h_gains || !(freq_res_hz > 0.0)) {
+        set_error("hdc_modeller_set_tile_beams: invalid arguments");
+        return HDC_ERR_ARG;
+    }
+    // unique tiles by their 32 gains, in order of first appearance
+    std::vector<int> tmap(ntiles);
+    std::vector<double> ugains;
+    for (int p = 0; p < ntiles; p++) {
+        const double* g = h_gains + 32 * (size_t)p;
+        int found = -1;
+        for (size_t u = 0; u < ugains.size() / 32 && found < 0; u++)
+            if (std::equal(g, g + 32, ugains.begin() + 32 * u)) found = (int)u;
+        if (found < 0) {
+            found = (int)(ugains.size() / 32);
+            ugains.insert(ugains.end(), g, g + 32);
+        }
+        tmap[p] = found;
+    }
+    // unique beam frequencies: each channel at the nearest multiple of the resolution
+    std::vector<long long> bins(nf);
+    for (int f = 0; f < nf; f++) bins[f] = std::llround(freqs[f] / freq_res_hz);
+    std::vector<long long> ub(bins);
+    std::sort(ub.begin(), ub.end());
+    ub.erase(std::unique(ub.begin(), ub.end()), ub.end());
+    std::vector<int> fmap(nf);
+    std::vector<double> ufreq(ub.size());
+    for (size_t i = 0; i < ub.size(); i++) ufreq[i] = (double)ub[i] * freq_res_hz;
+    for (int f = 0; f < nf; f++) fmap[f] = (int)(std::lower_bound(ub.begin(), ub.end(), bins[f]) - ub.begin());
+    cudaDeviceSynchronize();
+    tb.release();
+    tb.n_uniq_tile = (int)(ugains.size() / 32);
+    tb.n_uniq_freq = (int)ub.size();
+    HDC_CUDA_RET_INT(dalloc(&tb.d_gains, ugains.size()));
+    HDC_CUDA_RET_INT(dalloc(&tb.d_tile_map, ntiles));
+    HDC_CUDA_RET_INT(dalloc(&tb.d_freqs, ufreq.size()));
+    HDC_CUDA_RET_INT(dalloc(&tb.d_freq_map, nf));
+    HDC_CUDA_RET_INT(cudaMemcpy(tb.d_gains, ugains.data(), sizeof(double) * ugains.size(), cudaMemcpyHostToDevice));
+    HDC_CUDA_RET_INT(cudaMemcpy(tb.d_tile_map, tmap.data(), sizeof(int) * ntiles, cudaMemcpyHostToDevice));
+    HDC_CUDA_RET_INT(cudaMemcpy(tb.d_freqs, ufreq.data(), sizeof(double) * ufreq.size(), cudaMemcpyHostToDevice));
+    HDC_CUDA_RET_INT(cudaMemcpy(tb.d_freq_map, fmap.data(), sizeof(int) * nf, cudaMemcpyHostToDevice));
+    for (int ty = 0; ty < 3; ty++) dfree(t[ty].d_W);
+    beam_kind = HDC_BEAM_ANALYTIC_PER_TILE;
+    return alloc_tile_beam_tables();
 }
 
 int Modeller::geometry(double lst, cudaStream_t s) {
@@ -374,7 +492,16 @@ int Modeller::geometry(double lst, cudaStream_t s) {
         count_launches(1);
         HDC_CUDA_RET_INT(cudaGetLastError());
     }
-    if (beam_kind != HDC_BEAM_NONE) {
+    if (tile_beams()) {
+        for (int ty = 0; ty < 3; ty++) {
+            if (t[ty].nc == 0 || tb.n_uniq_tile == 0) continue;
+            dim3 g((t[ty].nc + 127) / 128, tb.n_uniq_freq, tb.n_uniq_tile);
+            tile_beam_kernel<<<g, 128, 0, s>>>(t[ty].d_radec, t[ty].nc, tb.d_freqs, tb.n_uniq_freq, tb.d_gains, lst,
+                                                lat, t[ty].d_B);
+            count_launches(1);
+            HDC_CUDA_RET_INT(cudaGetLastError());
+        }
+    } else if (beam_kind != HDC_BEAM_NONE) {
         for (int ty = 0; ty < 3; ty++) {
             if (t[ty].nc == 0) continue;
             dim3 g((t[ty].nc + 127) / 128, nf);
@@ -386,7 +513,11 @@ int Modeller::geometry(double lst, cudaStream_t s) {
     return HDC_OK;
 }
 
-const JonesF64* Modeller::weights(int ty) const { return beam_kind != HDC_BEAM_NONE ? t[ty].d_W : t[ty].d_S; }
+// B S B^H for a beam shared by all tiles; S when there is no beam or a beam
+// per tile (applied per baseline)
+const JonesF64* Modeller::weights(int ty) const {
+    return beam_kind == HDC_BEAM_ANALYTIC_DIPOLE ? t[ty].d_W : t[ty].d_S;
+}
 
 DirectParams Modeller::direct_params(int ty, void* vis) const {
     DirectParams p = {};
@@ -408,6 +539,13 @@ DirectParams Modeller::direct_params(int ty, void* vis) const {
     p.coeff_count = t[ty].d_ccount;
     p.suv_bl = nullptr;
     p.suv_tile = t[ty].d_suv_tile;
+    if (tile_beams()) {
+        p.beam = t[ty].d_B;
+        p.tile_map = tb.d_tile_map;
+        p.unflagged_map = nullptr;
+        p.freq_map = tb.d_freq_map;
+        p.n_uniq_freq = tb.n_uniq_freq;
+    }
     p.vis = vis;
     p.err = d_err;
     return p;
@@ -450,17 +588,25 @@ int Modeller::model_channels(double lst, void* d_vis, bool out64, int f0, int nf
         if (t[ty].nc == 0) continue;
         prof_begin(ty, s, e);
         if (ty == 0 && form == HDC_PREDICT_TENSOR) {
+            // the workspace holds planes for all nf channels; a chunk of nfc
+            // channels uses its start (chunks of one call run in order on s)
+            void* ws = tensor_workspace(out64);
+            if (!ws) return HDC_ERR_ALLOC;
+            TensorBeam tbm = {t[0].d_B, tb.d_tile_map, tb.d_freq_map + f0, tb.n_uniq_tile, tb.n_uniq_freq};
             const int rc = launch_tensor_points(nfc, nbl, ntiles, t[0].nc, d_freqs + f0, d_xyzs, lst - pc.ra, pc.dec,
-                                                t[0].d_lmn, weights(0) + (size_t)f0 * t[0].nc, vis, out64, d_err, s);
+                                                t[0].d_lmn, weights(0) + (size_t)f0 * t[0].nc,
+                                                tile_beams() ? &tbm : nullptr, vis, out64, ws, d_err, s);
             if (rc) return rc;
         } else {
             // the chosen (tensor) form keeps Gaussians and shapelets in the
-            // direct kernel, in its FP32 form
+            // direct kernel, in its FP32 form with a shared beam (FP64 with
+            // per-tile beams)
             DirectParams p = direct_params(ty, vis);
             p.nf = nfc;
             p.freqs = d_freqs + f0;
             p.flux = p.flux + (size_t)f0 * p.nc;
-            HDC_CUDA_RET_INT(launch_direct(ty, false, out64, p, s, form == HDC_PREDICT_TENSOR));
+            if (tile_beams()) p.freq_map = tb.d_freq_map + f0;
+            HDC_CUDA_RET_INT(launch_direct(ty, tile_beams(), out64, p, s, form == HDC_PREDICT_TENSOR));
         }
         prof_end(s, e);
     }
@@ -539,6 +685,13 @@ int Modeller::autos(double lst, JonesF32* d_vis, cudaStream_t s) {
         p.nc_total = t[ty].nc;
         p.flux = weights(ty);  // with a shared beam, B S B^H is already the auto term
         p.beam = nullptr;
+        if (tile_beams()) {
+            p.beam = t[ty].d_B;
+            p.tile_map = tb.d_tile_map;
+            p.unflagged_map = nullptr;
+            p.freq_map = tb.d_freq_map;
+            p.n_uniq_freq = tb.n_uniq_freq;
+        }
         p.vis = d_vis;
         HDC_CUDA_RET_INT(launch_autos(p, s));
     }
@@ -546,6 +699,7 @@ int Modeller::autos(double lst, JonesF32* d_vis, cudaStream_t s) {
 }
 
 Modeller::~Modeller() {
+    tb.release();
     if (err_ev) cudaEventDestroy(err_ev);
     if (h_err) cudaFreeHost(h_err);
     dfree(d_err);
@@ -712,7 +866,7 @@ extern "C" int hdc_modeller_new(const HdcSkyModel* sky, int pols, const XYZ* h_x
         hdc::set_error("hdc_modeller_new: invalid arguments");
         return HDC_ERR_ARG;
     }
-    if (pols < 0 || pols > 4 || beam_kind < 0 || beam_kind > 1 || predict_form < 0 || predict_form > 1) {
+    if (pols < 0 || pols > 4 || beam_kind < 0 || beam_kind > 2 || predict_form < 0 || predict_form > 1) {
         hdc::set_error("hdc_modeller_new: invalid pols/beam/form code");
         return HDC_ERR_ARG;
     }
@@ -759,12 +913,24 @@ extern "C" int hdc_modeller_new(const HdcSkyModel* sky, int pols, const XYZ* h_x
     cudaEventRecord(m->err_ev, 0);
     rc = m->build_tables(sky);
     if (rc) return fail(rc);
+    if (beam_kind == HDC_BEAM_ANALYTIC_PER_TILE) {
+        // every dipole at unit gain until hdc_modeller_set_tile_beams
+        std::vector<double> ones((size_t)32 * num_tiles, 1.0);
+        rc = m->set_tile_beams(ones.data(), 1.28e6);
+        if (rc) return fail(rc);
+    }
     if (predict_form == HDC_PREDICT_TENSOR) {
         rc = m->tensor_setup();
         if (rc) return fail(rc);
     }
     *out = reinterpret_cast<HdcModeller*>(m);
     return HDC_OK;
+}
+
+extern "C" int hdc_modeller_set_tile_beams(HdcModeller* hm, const double* h_dipole_gains, double freq_res_hz) {
+    Modeller* m = reinterpret_cast<Modeller*>(hm);
+    if (!m) return HDC_ERR_ARG;
+    return m->set_tile_beams(h_dipole_gains, freq_res_hz);
 }
 
 extern "C" void hdc_modeller_free(HdcModeller* m) { delete reinterpret_cast<Modeller*>(m); }

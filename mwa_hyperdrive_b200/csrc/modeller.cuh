@@ -19,6 +19,19 @@ struct TypeTables {
     int* d_ccount = nullptr;
     double2* d_suv_tile = nullptr;  // [nc][ntiles]
     float* d_sdense = nullptr;      // [nc][SDN][SDN] signed dense coefficients, or NULL
+    JonesF64* d_B = nullptr;        // per-tile beams: [uniq tile][uniq freq][nc] at the current timestep
+    void release();
+};
+
+// Per-tile analytic beams (hdc_modeller_set_tile_beams): the dipole gains of
+// every distinct tile, the unique row of each tile, the beam frequencies and
+// the unique column of each channel.
+struct TileBeams {
+    int n_uniq_tile = 0, n_uniq_freq = 0;
+    double* d_gains = nullptr;      // [uniq tile][2][16]
+    int* d_tile_map = nullptr;      // [tile]
+    double* d_freqs = nullptr;      // [uniq freq] Hz
+    int* d_freq_map = nullptr;      // [channel]
     void release();
 };
 
@@ -46,6 +59,7 @@ struct Modeller {
     int queue_error_check(cudaStream_t s);
     int take_error(bool wait);
     TypeTables t[3];
+    TileBeams tb;  // set when beam_kind == HDC_BEAM_ANALYTIC_PER_TILE
     JonesF32* d_host_vis = nullptr;
     size_t host_vis_bytes = 0;
     TensorState* tc = nullptr;
@@ -64,6 +78,9 @@ struct Modeller {
     void prof_collect();
 
     int build_tables(const HdcSkyModel* sky);
+    bool tile_beams() const { return beam_kind == HDC_BEAM_ANALYTIC_PER_TILE; }
+    int set_tile_beams(const double* h_gains, double freq_res_hz);
+    int alloc_tile_beam_tables();
     int geometry(double lst, cudaStream_t s);
     const JonesF64* weights(int ty) const;
     DirectParams direct_params(int ty, void* vis) const;
@@ -83,7 +100,7 @@ struct Modeller {
     int model_uvws(double lst, const UVW* d_uvws_ext, JonesF32* d_vis, cudaStream_t s);
     int autos(double lst, JonesF32* d_vis, cudaStream_t s);
     int tensor_setup();
-    int tensor_points(double lst, void* d_vis, bool out64, cudaStream_t s);
+    void* tensor_workspace(bool out64);
     void tensor_release();
     ~Modeller();
 };

@@ -1056,30 +1056,42 @@ extern "C" const char* model_points_tc(const Points* comps, const Addresses* a, 
     const int nf = a->num_freqs, nbl = a->num_baselines;
     const int ntiles = (int)((1.0 + sqrt(1.0 + 8.0 * nbl)) / 2.0 + 0.5);
     if (ntiles * (ntiles - 1) / 2 != nbl || !d_tile_xyzs) return "model_points_tc: invalid arguments";
-    int beam_tile = -1;
+    // the beam row of every tile: one row for all tiles (a shared beam, the
+    // cheaper form: W = B S B^H per component) or per-tile rows (block form)
+    int beam_tile = -1, n_uniq_tile = 0;
+    std::vector<int> row(ntiles);
     if (d_beam_jones) {
-        // one beam for all tiles: every tile maps to the same unique beam row
-        std::vector<int> um(ntiles), tm(ntiles);
+        std::vector<int> um(ntiles), tm;
         if (!a->d_tile_map || !a->d_freq_map) return "model_points_tc: beam maps missing";
         if (a->d_tile_index_to_unflagged_tile_index_map)
             HDC_CUDA_RET_STR(cudaMemcpy(um.data(), a->d_tile_index_to_unflagged_tile_index_map, sizeof(int) * ntiles,
                                         cudaMemcpyDeviceToHost));
         else
             for (int t = 0; t < ntiles; t++) um[t] = t;
-        HDC_CUDA_RET_STR(cudaMemcpy(tm.data(), a->d_tile_map, sizeof(int) * ntiles, cudaMemcpyDeviceToHost));
+        int mx = 0;
         for (int t = 0; t < ntiles; t++) {
-            if (um[t] < 0 || um[t] >= ntiles) return "model_points_tc: tile map out of range";
-            const int bt = tm[um[t]];
-            if (beam_tile >= 0 && bt != beam_tile)
-                return "model_points_tc: the tensor-core form needs one beam shared by all tiles";
-            beam_tile = bt;
+            if (um[t] < 0) return "model_points_tc: tile map out of range";
+            mx = std::max(mx, um[t]);
         }
+        tm.resize(mx + 1);
+        HDC_CUDA_RET_STR(cudaMemcpy(tm.data(), a->d_tile_map, sizeof(int) * (mx + 1), cudaMemcpyDeviceToHost));
+        bool shared = true;
+        for (int t = 0; t < ntiles; t++) {
+            row[t] = tm[um[t]];
+            if (row[t] < 0) return "model_points_tc: tile map out of range";
+            n_uniq_tile = std::max(n_uniq_tile, row[t] + 1);
+            shared = shared && row[t] == row[0];
+        }
+        if (shared) beam_tile = row[0];
     }
+    const bool tile_beam = d_beam_jones && beam_tile < 0;
     size_t off_lmn = 0;
     size_t off_flux = align256(off_lmn + sizeof(double4) * nc);
     size_t off_w = align256(off_flux + sizeof(JonesF64) * (size_t)nf * nc);
-    size_t off_gp = align256(off_w + (d_beam_jones ? sizeof(JonesF64) * (size_t)nf * nc : 0));
-    size_t total = align256(off_gp + sizeof(double4) * nc);
+    size_t off_gp = align256(off_w + (d_beam_jones && !tile_beam ? sizeof(JonesF64) * (size_t)nf * nc : 0));
+    size_t off_map = align256(off_gp + sizeof(double4) * nc);
+    size_t off_ws = align256(off_map + sizeof(int) * (size_t)ntiles);
+    size_t total = align256(off_ws + tensor_workspace_bytes(nf, nbl, false));
     char* ws = (char*)device_scratch(total);
     if (!ws) return "out of device memory";
     PrepIn in = {};
@@ -1098,18 +1110,28 @@ extern "C" const char* model_points_tc(const Points* comps, const Addresses* a, 
     count_launches(1);
     HDC_CUDA_RET_STR(cudaGetLastError());
     const JonesF64* W = in.flux;
-    if (d_beam_jones) {
+    TensorBeam tb = {};
+    if (d_beam_jones && !tile_beam) {
         JonesF64* Wb = (JonesF64*)(ws + off_w);
         shared_beam_kernel<<<pg, 128>>>(in.flux, d_beam_jones, beam_tile, a->d_freq_map, a->num_unique_beam_freqs, nc,
                                         nf, Wb);
         count_launches(1);
         HDC_CUDA_RET_STR(cudaGetLastError());
         W = Wb;
+    } else if (tile_beam) {
+        int* d_row = (int*)(ws + off_map);
+        HDC_CUDA_RET_STR(cudaMemcpy(d_row, row.data(), sizeof(int) * ntiles, cudaMemcpyHostToDevice));
+        tb.beam = d_beam_jones;
+        tb.tile_map = d_row;
+        tb.freq_map = a->d_freq_map;
+        tb.n_uniq_tile = n_uniq_tile;
+        tb.n_uniq_freq = a->num_unique_beam_freqs;
     }
     int* errw = dropin_error_word();
     if (!errw) return "device error word unavailable";
     const int rc = launch_tensor_points(nf, nbl, ntiles, nc, a->d_freqs, d_tile_xyzs, lst_rad - phase_centre.ra,
-                                        phase_centre.dec, in.lmn, W, d_vis_fb, false, errw, 0);
+                                        phase_centre.dec, in.lmn, W, tile_beam ? &tb : nullptr, d_vis_fb, false,
+                                        ws + off_ws, errw, 0);
     if (rc) return hdc_last_error();
     return take_word_sync(errw, "model_points_tc");
 }

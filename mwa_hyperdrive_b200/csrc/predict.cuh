@@ -60,10 +60,25 @@ int kernel_error_status(int word);
 cudaError_t launch_direct(int ty, bool tile_beam, bool out64, const DirectParams& p, cudaStream_t s,
                           bool fast = false);
 
-// The tensor-core point predict of one timestep (csrc/tensor.cu).
+// Per-tile beams for the tensor-core predict: beam [n_uniq_tile]
+// [n_uniq_freq][nc] (the reference's layout), the unique row of every tile
+// (any unflagged-tile map already applied) and the unique column of every
+// channel of the launch.
+struct TensorBeam {
+    const JonesF64* beam;
+    const int* tile_map;
+    const int* freq_map;
+    int n_uniq_tile;
+    int n_uniq_freq;
+};
+
+// The tensor-core point predict of one timestep (csrc/tensor.cu): d_W is
+// B S B^H [nf][nc] with a beam shared by all tiles (beam NULL), or S [nf][nc]
+// with per-tile beams.  ws: tensor_workspace_bytes(nf, nbl, out64) bytes.
+size_t tensor_workspace_bytes(int nf, int nbl, bool out64);
 int launch_tensor_points(int nf, int nbl, int ntiles, int nc, const double* d_freqs, const XYZ* d_xyzs, double ha,
-                         double dec, const double4* d_lmn, const JonesF64* d_W, void* d_vis, bool out64, int* d_err,
-                         cudaStream_t s);
+                         double dec, const double4* d_lmn, const JonesF64* d_W, const TensorBeam* beam, void* d_vis,
+                         bool out64, void* ws, int* d_err, cudaStream_t s);
 
 struct AutosParams {
     int ntiles, nf;

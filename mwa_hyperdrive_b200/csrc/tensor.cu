@@ -4,99 +4,130 @@
 // For one timestep and channel the baseline UVW is a tile difference
 // (uvw_pq = uvw_p - uvw_q, as marlu's xyzs_to_cross_uvws builds it), so the
 // point-source phasor factors: exp(2 pi i theta_pq,c) = A_pc conj(A_qc) with
-// A_pc = exp(2 pi i (u_p l_c + v_p m_c + w_p (n_c - 1)) f / c).  Each
-// polarisation ab of the visibility matrix is then a weighted Gram product
+// A_pc = exp(2 pi i (u_p l_c + v_p m_c + w_p (n_c - 1)) f / c).
+//
+// Shared beam (MODE 0).  Each polarisation ab of the visibility matrix is a
+// weighted Gram product
 //     V^ab = X Y^H,  X = A diag(W^ab),  Y = A     (tiles x tiles, over components)
-// with W = B S B^H the per-component brightness (shared beam).  W is
-// Hermitian, so V^YX = (V^XY)^H and V^XX, V^YY are Hermitian: three complex
-// products give all four correlations of every baseline.  In real form
-//     Re V = Xr Yr^T + Xi Yi^T,   Im V = Xi Yr^T + Xr (-Yi)^T.
+// with W = B S B^H the per-component brightness.  W is Hermitian, so
+// V^YX = (V^XY)^H and V^XX, V^YY are Hermitian: three complex products give
+// all four correlations of every baseline.
+//
+// Per-tile beams (MODE 1), the block form: with B_pc the beam of tile p
+// towards component c and S_c its instrumental flux,
+//     V^ab_pq = sum_{c, y} M^a_{p,(c,y)} conj(N^b_{q,(c,y)}),
+//     M^a_{p,(c,y)} = A_pc (B_pc S_c)^{ay},   N^b_{q,(c,y)} = A_qc B_qc^{by},
+// a Gram product over K = 2 x components (y the second index of S); again
+// XX, YY and XY suffice (S Hermitian: V^YX_pq = conj(V^XY_qp)).
+//
+// In real form  Re V = Xr Yr^T + Xi Yi^T,   Im V = Xi Yr^T + Xr (-Yi)^T.
 //
 // Numbers.  A tensor core accumulating in FP32 does not round to nearest, and
 // its error grows with every K step.  Here every operand is instead a
 // fixed-point integer split into balanced byte digits, and the digit planes
 // are multiplied on the integer tensor core (kind::i8, s8 x s8, s32
 // accumulators), where every sum is exact:
-//   x = rint(X sx), |x| < 2^31 - 2^24 (sx from the channel's largest |W|):
+//   x = rint(X sx), |x| < 2^31 - 2^24 (sx from the channel's largest |X|):
 //       x = d0 2^24 + d1 2^16 + d2 2^8 + d3, every d_i in [-128, 127];
-//   y = rint(A sy), |y| < 2^22: y = e0 2^16 + e1 2^8 + e2.
+//   MODE 0: y = rint(A sy), |y| < 2^22: y = e0 2^16 + e1 2^8 + e2;
+//   MODE 1: y like x (4 digits; N carries the beam's dynamic range).
 // Balanced digits are the bytes of (x + 0x808080) ^ 0x808080: adding 128 to
 // each lower digit position and flipping its top bit turns excess-128 bytes
 // into two's-complement ones (the flip is applied to four digits of a byte
-// plane at once).  They have zero mean, so the products left out
-// below do not bias the sum (unsigned lower bytes would: their dropped
-// products are all positive and grow with the number of components).
-// x y = sum_ij d_i e_j 2^(40 - 8(i + j)); the nine plane products with
-// i + j <= 3 are kept (the rest weigh < 2^-30 of full scale), each into the
-// accumulator of its class w = i + j, and the epilogue forms
-// V = sum_w D_w 2^(40 - 8w) / (sx sy) in FP64.  The only rounding is in the
-// inputs: the phase, reduced exactly in FP64 to a quadrant q and a remainder
-// r in [-1/2, 1/2] quarter-turns; sin and cos of (pi/2) r from FP32
-// polynomials (least-squares fits, mwa_hyperdrive_b200/phasor_poly.py,
-// < 0.75 ulp); X = (W sx) A in FP32; the two roundings to integers (2^-23 of A,
-// 2^-31 of the channel's largest |X|).  A launch covers at most KPASS
+// plane at once).  They have zero mean, so the products left out below do
+// not bias the sum.  x y = sum_ij d_i e_j 2^(XW + YW - 8(i + j)); the plane
+// products with i + j <= 3 are kept (9 in MODE 0, 10 in MODE 1; the rest
+// weigh < 2^-30 of full scale), each into the accumulator of its class
+// w = i + j, and the epilogue forms V = sum_w D_w 2^(XW + YW - 8w) / (sx sy)
+// in FP64.  The only rounding is in the inputs: the phase, reduced exactly
+// in FP64 to a quadrant q and a remainder r in [-1/2, 1/2] quarter-turns;
+// sin and cos of (pi/2) r from FP32 polynomials (least-squares fits,
+// mwa_hyperdrive_b200/phasor_poly.py, < 0.75 ulp); the operands formed in
+// FP32; the roundings to integers.  A launch covers at most KPASS
 // components, so no s32 sum can overflow.
 //
-// Kernel: one CTA per (channel, polarisation, half of the tile columns); M =
-// 128 tiles (rows of X), 64 tile columns (rows of Y), K = 32 components per
-// stage.  Sixteen producer warps compute the per-tile phasors, X and Y, the
-// byte planes, and write them to shared memory in the K-major core-matrix
-// layout (one warp store = one 128-byte core matrix); the stage's component data
-// (l, m, n, W) is staged in shared memory one stage ahead, so the phasor loop
-// reads no global memory.  One thread issues the 18 MMAs of a stage (9 plane
-// pairs x {Xr, Xi}, N = 128 = [Re | Im] of the 64 columns, which keeps the
-// operand bytes read from shared memory per MAC at half of what separate
-// N = 64 products would need) into 4 TMEM accumulators (one per class, 128
-// columns each = all 512 columns).  Four stages let the producers
-// run ahead of the tensor core.  The epilogue reads TMEM with tcgen05.ld,
-// combines the classes in FP64 and adds the baselines of its columns into
-// the visibilities (XX, YY: q > p; XY: q > p as XY, q < p as YX = conj).
+// Kernel: one CTA per job = (channel, polarisation, row block of 128 tiles,
+// column block of 64 tiles); the jobs of a channel are the blocks that hold a
+// baseline of that polarisation (XX, YY: some p < q; XY: all), so any number
+// of tiles is covered.  M = 128 tiles (rows of X), 64 tile columns (rows of
+// Y), K = 32 bytes per stage (32 components, or 16 components x 2 in MODE
+// 1).  Sixteen producer warps compute the per-tile phasors, X and Y, the byte
+// planes, and write them to shared memory in the K-major core-matrix layout
+// (one warp store = one 128-byte core matrix); the stage's component data is
+// staged in shared memory two stages ahead, so the phasor loop reads no
+// global memory except, in MODE 1, the beam Jones of its tiles.  One thread
+// issues the MMAs of a stage (plane pairs x {Xr, Xi}, N = 128 = [Re | Im] of
+// the 64 columns) into 4 TMEM accumulators (one per class, 128 columns each
+// = all 512 columns).  The epilogue reads TMEM with tcgen05.ld, combines the
+// classes in FP64 and stores each of its baselines' values once into a planar
+// scratch [XX, XY, YX, YY][channel][baseline] (XY of p < q as XY, of p > q as
+// YX = conj); a coalesced pass then adds the four planes into the
+// visibilities, so every Jones matrix is read and written once.
 //
 // Every mbarrier wait is bounded by the global timer; on a timeout the CTA
 // records KERR_TIMEOUT, waits (bounded) for its issued MMAs and frees TMEM.
 
 #include <algorithm>
 #include <cmath>
-
 #include <mutex>
+#include <type_traits>
+#include <vector>
 
 #include "modeller.cuh"
 
 namespace hdc {
 namespace tc {
 
-constexpr int NT = 128;    // tiles = M
-constexpr int NH = 64;     // tile columns per CTA
+constexpr int NT = 128;    // rows of a block = M
+constexpr int NH = 64;     // tile columns of a block
 constexpr int NB = 2 * NH; // MMA N: [Re | Im] of the NH columns
-constexpr int KC = 32;     // components per stage = MMA K (bytes)
-constexpr int NSTAGE = 4;
-constexpr int CRING = NSTAGE + 2;  // component-data ring: producer warps may be NSTAGE stages apart
+constexpr int KC = 32;     // K bytes per stage = MMA K
 constexpr int NPW = 16;    // producer / epilogue warps
-constexpr int NPT = NPW * 32;   // producer threads
+constexpr int NPT = NPW * 32;  // producer threads
 constexpr int THREADS = NPT + 32;
-constexpr int XDIG = 4;    // byte planes of x
-constexpr int YDIG = 3;    // byte planes of y
-constexpr int XT_BYTES = NT * KC;                           // one X plane tile, 4 KB
-constexpr int YT_BYTES = NH * KC;                           // one Y plane tile, 2 KB
-constexpr int Y_OFF = 2 * XDIG * XT_BYTES;                  // X: [re, im][4 planes]
-constexpr int STAGE_BYTES = Y_OFF + 3 * YDIG * YT_BYTES;    // Y: [re, im, -im][3 planes]
-constexpr int SMEM_BYTES = NSTAGE * STAGE_BYTES + 1024;
+constexpr int XT_BYTES = NT * KC;  // one X plane tile, 4 KB
+constexpr int YT_BYTES = NH * KC;  // one Y plane tile, 2 KB
 constexpr int LBO = 128;             // bytes between the two 16-byte K core matrices of a row group
 constexpr int SBO = (KC / 16) * 128; // bytes between 8-row groups
 constexpr int TMEM_COLS = 512;       // 4 classes x NB
-constexpr int KPASS = 16384;         // components per launch: 3 pairs x 2 x 2^14 x KPASS < 2^31
-constexpr float SY = 4128768.0f;     // 2^22 - 2^16: |A| <= 1 -> |y| < 2^22
+constexpr int MAXJOBS = 1024;        // jobs per channel in the launch parameters
+constexpr float SY0 = 4128768.0f;    // MODE 0: 2^22 - 2^16: |A| <= 1 -> |y| < 2^22
 // y + 0x8080 as FP32 bits: 1.5 * 2^23 rounds |v| < 2^22 to an integer in
 // the mantissa; the extra 0x8080 is the balancing offset of the two lower
 // digits.  The mantissa field then holds 2^22 + 0x8080 + y, so byte 2 is the
 // top digit + 0x40 and bytes 1, 0 the excess-128 lower digits.
 constexpr float YOFF = 12582912.0f + 32896.0f;
+constexpr double FULL31 = 2147483648.0 - 33554432.0;  // 2^31 - 2^25
+
+template <int MODE>
+struct Cfg;
+template <>
+struct Cfg<0> {
+    static constexpr int XDIG = 4, YDIG = 3, NSTAGE = 4, CPS = 32;  // components per stage
+    static constexpr int KPASS = 16384;  // 3 products x 2 x 2^14 x KPASS < 2^31
+};
+template <>
+struct Cfg<1> {
+    static constexpr int XDIG = 4, YDIG = 4, NSTAGE = 3, CPS = 16;
+    static constexpr int KPASS = 8000;  // 4 products x 2 x 2^14 x 2 KPASS < 2^31
+};
+template <int MODE>
+struct Lay {
+    static constexpr int Y_OFF = 2 * Cfg<MODE>::XDIG * XT_BYTES;                     // X: [re, im][digits]
+    static constexpr int STAGE_BYTES = Y_OFF + 3 * Cfg<MODE>::YDIG * YT_BYTES;       // Y: [im, re, -im][digits]
+    static constexpr int SMEM_BYTES = Cfg<MODE>::NSTAGE * STAGE_BYTES + 1024;
+    static constexpr int CRING = Cfg<MODE>::NSTAGE + 2;  // component ring: warps may be NSTAGE stages apart
+};
 
 // component data of one stage, staged in shared memory (structure of arrays
 // so that 16-byte loads of consecutive components are conflict-free)
-struct CompStage {
+struct CompStage0 {
     double l[KC], m[KC], n[KC];  // turn units (n - 1 in n)
     float2 w[KC];                // W of this polarisation times the x scale sx
+};
+struct CompStage1 {
+    double l[16], m[16], n[16];
+    float4 s[16][2];             // S (xx, xy | yx, yy as re, im) of this channel
 };
 
 struct Params {
@@ -105,9 +136,19 @@ struct Params {
     const XYZ* xyzs;
     double s_ha, c_ha, s_dec, c_dec;
     const double4* lmn;    // [nc] turn units
-    const JonesF64* W;     // [nf][nc]
-    void* vis;             // [nf][nbl]
+    const JonesF64* W;     // [nf][nc]: MODE 0 B S B^H (or S), MODE 1 S
+    // MODE 1: beam [uniq tile][uniq freq][nc], unique row of each tile and
+    // column of each channel, and per channel bounds of |B| and |S| entries
+    const JonesF64* beam;
+    const int* tile_map;
+    const int* freq_map;
+    int n_uniq_freq;
+    const double* maxb;
+    const double* maxs;
+    void* planes;          // [4][nf][nbl] float2 (or double2 with OUT64)
     int* err;
+    int njobs;
+    uint32_t jobs[MAXJOBS];  // pol | rb << 8 | cb << 20
 };
 
 __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
@@ -193,22 +234,52 @@ __device__ __forceinline__ bool producers_sync_or(bool v) {
 }
 
 // shared-memory tile offsets inside a stage; digit 0 is the signed top byte
+template <int MODE>
 __device__ __forceinline__ uint32_t x_tile(int part, int digit) {
-    return (uint32_t)((part * XDIG + digit) * XT_BYTES);
+    return (uint32_t)((part * Cfg<MODE>::XDIG + digit) * XT_BYTES);
 }
 // Y tiles of one digit lie in the order [Yi | Yr | -Yi] (64 rows each), so
 // that [Yr; -Yi] (from the Yr tile) and [Yi; Yr] (from the Yi tile) are
 // 128-row B operands: Xr [Yr; -Yi]^T + Xi [Yi; Yr]^T = [Re | Im] of X Y^H.
 // part: 0 = Yr, 1 = Yi, 2 = -Yi
+template <int MODE>
 __device__ __forceinline__ uint32_t y_tile(int part, int digit) {
     const int slot = part == 0 ? 1 : (part == 1 ? 0 : 2);
-    return (uint32_t)(Y_OFF + (digit * 3 + slot) * YT_BYTES);
+    return (uint32_t)(Lay<MODE>::Y_OFF + (digit * 3 + slot) * YT_BYTES);
 }
 // TMEM column of accumulator class w ([Re | Im], NB columns)
 __device__ __forceinline__ uint32_t acc_col(int w) { return (uint32_t)(w * NB); }
 
-template <bool OUT64>
-__global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const Params P) {
+// The tile's position in quarter-turns per unit l, m, n - 1 at this channel
+// (zero for rows beyond the array: bounded values, never written out).
+__device__ __forceinline__ void tile_uvw(const Params& P, int tile, double oq, double& u, double& v, double& w) {
+    u = v = w = 0.0;
+    if (tile < P.ntiles) {
+        const XYZ x = P.xyzs[tile];
+        u = (P.s_ha * x.x + P.c_ha * x.y) * oq;
+        v = (-P.s_dec * P.c_ha * x.x + P.s_dec * P.s_ha * x.y + P.c_dec * x.z) * oq;
+        w = (P.c_dec * P.c_ha * x.x - P.c_dec * P.s_ha * x.y + P.s_dec * x.z) * oq;
+    }
+}
+
+// one row of a beam Jones (two complex numbers, FP32) for tile `tile`,
+// component c of the pass, at unique frequency column fm
+__device__ __forceinline__ float4 beam_row(const Params& P, int tile, int c, int fm, int row) {
+    if (tile >= P.ntiles) return make_float4(0.f, 0.f, 0.f, 0.f);
+    const double2* b = reinterpret_cast<const double2*>(
+                           P.beam + ((size_t)__ldg(P.tile_map + tile) * P.n_uniq_freq + fm) * P.nc + P.c0 + c) +
+                       2 * row;
+    const double2 e0 = __ldg(b), e1 = __ldg(b + 1);
+    return make_float4((float)e0.x, (float)e0.y, (float)e1.x, (float)e1.y);
+}
+
+template <int MODE, bool OUT64>
+__global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const __grid_constant__ Params P) {
+    using C = Cfg<MODE>;
+    using L = Lay<MODE>;
+    constexpr int NSTAGE = C::NSTAGE;
+    constexpr int CRING = L::CRING;
+    using CompStage = typename std::conditional<MODE == 0, CompStage0, CompStage1>::type;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     __shared__ alignas(8) uint64_t full_bar[NSTAGE], empty_bar[NSTAGE], done_bar;
     __shared__ uint32_t tmem_base_s;
@@ -218,21 +289,28 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const Params P) {
     __shared__ alignas(8) uint64_t comp_bar[CRING];
 
     unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    const int f = blockIdx.x;
-    const int pol = blockIdx.y;   // 0: XX, 1: YY, 2: XY
-    const int hcol = blockIdx.z;  // tile columns [hcol * NH, hcol * NH + NH)
+    const int f = blockIdx.y;
+    const uint32_t job = P.jobs[blockIdx.x];
+    const int pol = (int)(job & 0xFF);          // 0: XX, 1: YY, 2: XY
+    const int rb = (int)((job >> 8) & 0xFFF);   // rows: tiles [128 rb, 128 rb + 128)
+    const int cb = (int)(job >> 20);            // columns: tiles [64 cb, 64 cb + 64)
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int arow = pol == 1 ? 1 : 0, brow = pol == 0 ? 0 : 1;  // MODE 1: beam rows a (of M) and b (of N)
     // W component of this polarisation (JonesF64 as 4 double2: xx, xy, yx, yy)
     const int wsel = pol == 0 ? 0 : (pol == 1 ? 3 : 1);
 
-    // largest |W| of the pass sets the x scale
-    double mx = 0.0;
-    for (int c = tid; c < P.cn; c += THREADS) {
-        const double2 w = __ldg(reinterpret_cast<const double2*>(P.W + (size_t)f * P.nc + P.c0 + c) + wsel);
-        mx = fmax(mx, hypot(w.x, w.y));
+    // operand scales: MODE 0 from the pass's largest |W|; MODE 1 from the
+    // channel's bounds |M| <= 2 max|B| max|S| and |N| <= max|B|
+    double bound = 0.0;
+    if (MODE == 0) {
+        double mx = 0.0;
+        for (int c = tid; c < P.cn; c += THREADS) {
+            const double2 w = __ldg(reinterpret_cast<const double2*>(P.W + (size_t)f * P.nc + P.c0 + c) + wsel);
+            mx = fmax(mx, hypot(w.x, w.y));
+        }
+        for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        if (lane == 0) red_s[warp] = mx;
     }
-    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    if (lane == 0) red_s[warp] = mx;
     if (tid == 0) {
         for (int s = 0; s < NSTAGE; s++) {
             mbar_init(&full_bar[s], NPW);  // one arrival per producer warp
@@ -244,16 +322,23 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const Params P) {
         fence_barrier_init();
     }
     __syncthreads();
-    double wmax = 0.0;
-    for (int i = 0; i < THREADS / 32; i++) wmax = fmax(wmax, red_s[i]);
+    double bmax = 1.0;
+    if (MODE == 0) {
+        for (int i = 0; i < THREADS / 32; i++) bound = fmax(bound, red_s[i]);
+    } else {
+        bmax = P.maxb[f];
+        bound = 2.0 * bmax * P.maxs[f];
+    }
+    const int n = P.ntiles;
     // A polarisation whose weights are all exactly zero (e.g. XY of a
-    // Stokes-I sky) contributes exactly zero; a column half beyond the
-    // last tile has no baselines.
-    if (!(wmax > 0.0) || hcol * NH >= P.ntiles) return;
-    const float sx = (float)((2147483648.0 - 33554432.0) / wmax);  // (2^31 - 2^25) / max|W|
-    const double inv = 1.0 / ((double)sx * (double)SY);
+    // Stokes-I sky) contributes exactly zero: its baselines get zeros.
+    const bool zero = !(bound > 0.0);
+    const float sx = zero ? 0.f : (float)(FULL31 / bound);
+    const float sy = MODE == 0 ? SY0 : (zero ? 0.f : (float)(FULL31 / bmax));
+    const double inv = zero ? 0.0 : 1.0 / ((double)sx * (double)sy);
+    const int nchunks = zero ? 0 : (P.cn + C::CPS - 1) / C::CPS;
 
-    if (warp == 0) {
+    if (!zero && warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_s)),
                      "r"(TMEM_COLS)
                      : "memory");
@@ -263,102 +348,161 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const Params P) {
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = tmem_base_s;
-    const int nchunks = (P.cn + KC - 1) / KC;
     const double freq = P.freqs[f];
+    const int fm = MODE == 1 ? __ldg(P.freq_map + f) : 0;
 
-    if (warp < NPW) {
+    if (zero) {
+        // nothing to multiply
+    } else if (warp < NPW) {
         // ------------------------------------------------ producers
-        // warp = 8 tile rows x 16 components of a stage; lane = (row rl, quad of
-        // 4 components), and every thread also takes the row 64 tiles down, so a
-        // warp's store of one byte plane is one whole 128-byte core matrix and
-        // exactly one of a thread's two rows lies in this CTA's Y half
+        // warp = 8 tile rows x 16 K bytes of a stage; lane = (row rl, quad of
+        // 4 K bytes), and every thread also takes the row 64 tiles down, so a
+        // warp's store of one byte plane is one whole 128-byte core matrix.
+        // Its Y row is column r0 of the column block: one of its two X rows
+        // when the column block lies inside the row block, else a third tile.
         const int g = warp & 7;             // rows 8g .. 8g + 7 (and + 64)
-        const int kq = warp >> 3;           // components [kq * 16, kq * 16 + 16) of a stage
+        const int kq = warp >> 3;           // K bytes [kq * 16, kq * 16 + 16) of a stage
         const int rl = lane >> 2, quad = lane & 3;
-        const int cb = kq * 16 + quad * 4;  // this thread's 4 components
-        const int r0 = 8 * g + rl;          // rows r0 and r0 + 64; Y row r0 of tile r0 + 64 hcol
-        const int ry = hcol;                // which of the two rows is the Y row
-        // Rows of tiles beyond the array get phase 0 (bounded values, so no
-        // s32 sum can overflow): their products only reach rows and columns
-        // of the accumulators that the epilogue never writes out.
-        double u[2], v[2], w[2];            // quarter-turns per unit l, m, n - 1
-#pragma unroll
-        for (int s2 = 0; s2 < 2; s2++) {
-            const int r = r0 + 64 * s2;
-            u[s2] = v[s2] = w[s2] = 0.0;
-            if (r < P.ntiles) {
-                const XYZ x = P.xyzs[r];
-                const double oq = 4.0 * freq / VEL_C;
-                u[s2] = (P.s_ha * x.x + P.c_ha * x.y) * oq;
-                v[s2] = (-P.s_dec * P.c_ha * x.x + P.s_dec * P.s_ha * x.y + P.c_dec * x.z) * oq;
-                w[s2] = (P.c_dec * P.c_ha * x.x - P.c_dec * P.s_ha * x.y + P.s_dec * x.z) * oq;
-            }
-        }
+        const int r0 = 8 * g + rl;          // rows r0 and r0 + 64 of the block
+        const int ry = cb - 2 * rb;         // the X row that is the Y tile (0 or 1), else separate
+        const bool ysep = ry != 0 && ry != 1;
+        const int prow[2] = {NT * rb + r0, NT * rb + r0 + 64};
+        const int qcol = NH * cb + r0;
+        const double oq = 4.0 * freq / VEL_C;
+        double u[3], v[3], w[3];  // quarter-turns per unit l, m, n - 1 of the two X rows and the Y tile
+        tile_uvw(P, prow[0], oq, u[0], v[0], w[0]);
+        tile_uvw(P, prow[1], oq, u[1], v[1], w[1]);
+        tile_uvw(P, qcol, oq, u[2], v[2], w[2]);
         const double4* lmn = P.lmn + P.c0;
         const JonesF64* Wf = P.W + (size_t)f * P.nc + P.c0;
-        // the first KC threads fetch a stage's component data (zeros past the end)
-        auto fetch = [&](int k, double2& a, double2& b, double2& wd) {
-            const int c = k * KC + tid;
+        // the first CPS threads fetch a stage's component data (zeros past the end)
+        auto fetch = [&](int k, double2& a, double2& b, double4& wd) {
+            const int c = k * C::CPS + tid;
             if (c < P.cn) {
                 a = __ldg(reinterpret_cast<const double2*>(lmn + c));
                 b = __ldg(reinterpret_cast<const double2*>(lmn + c) + 1);
-                wd = __ldg(reinterpret_cast<const double2*>(Wf + c) + wsel);
+                if (MODE == 0) {
+                    const double2 t = __ldg(reinterpret_cast<const double2*>(Wf + c) + wsel);
+                    wd = make_double4(t.x, t.y, 0.0, 0.0);
+                } else {
+                    wd = make_double4(0.0, 0.0, 0.0, 0.0);  // S is read at stash time
+                }
             } else {
-                a = b = wd = make_double2(0.0, 0.0);
+                a = b = make_double2(0.0, 0.0);
+                wd = make_double4(0.0, 0.0, 0.0, 0.0);
             }
         };
-        auto stash = [&](int buf, const double2& a, const double2& b, const double2& wd) {
-            comp_s[buf].l[tid] = a.x;
-            comp_s[buf].m[tid] = a.y;
-            comp_s[buf].n[tid] = b.x;
-            comp_s[buf].w[tid] = make_float2((float)(wd.x * (double)sx), (float)(wd.y * (double)sx));
+        auto stash = [&](int k, int buf, const double2& a, const double2& b, const double4& wd) {
+            CompStage& cs = comp_s[buf];
+            cs.l[tid] = a.x;
+            cs.m[tid] = a.y;
+            cs.n[tid] = b.x;
+            if constexpr (MODE == 0) {
+                cs.w[tid] = make_float2((float)(wd.x * (double)sx), (float)(wd.y * (double)sx));
+            } else {
+                const int c = k * C::CPS + tid;
+                float4 s0 = make_float4(0.f, 0.f, 0.f, 0.f), s1 = s0;
+                if (c < P.cn) {
+                    const double2* sp = reinterpret_cast<const double2*>(Wf + c);
+                    const double2 xx = __ldg(sp), xy = __ldg(sp + 1), yx = __ldg(sp + 2), yy = __ldg(sp + 3);
+                    s0 = make_float4((float)xx.x, (float)xx.y, (float)xy.x, (float)xy.y);
+                    s1 = make_float4((float)yx.x, (float)yx.y, (float)yy.x, (float)yy.y);
+                }
+                cs.s[tid][0] = s0;
+                cs.s[tid][1] = s1;
+            }
         };
         // Software pipeline: iteration k writes the byte planes of stage k
-        // from registers and computes the values of stage k + 1 (phasors, X,
-        // Y: FP64, conversion and FMA work) in the same straight-line block,
-        // so the scheduler interleaves the two kinds of work instead of every
-        // producer warp hitting the same pipe at once.  Component data goes
-        // through a 3-deep ring: stage j in comp_s[j % 3], stashed two
-        // iterations ahead, overwritten only after the barrier that follows
-        // its last reader.  Stages past the end read zeros (their values are
-        // never written out).
+        // from registers and computes the values of stage k + 1 in the same
+        // straight-line block.  Component data goes through a ring of CRING
+        // slots, stashed two stages ahead by the first CPS threads.  Stages
+        // past the end read zeros (their values are never written out).
         auto compute = [&](int k, int (&xr)[2][4], int (&xi)[2][4], int (&yr)[4], int (&yi)[4], int (&yn)[4]) {
             const CompStage& cs_ = comp_s[k % CRING];
-            double cl[4], cm[4], cn[4];
-            float wr[4], wi[4];
+            if constexpr (MODE == 0) {
+                const int cb4 = kq * 16 + quad * 4;  // this thread's 4 components
+                double cl[4], cm[4], cn[4];
+                float wr[4], wi[4];
 #pragma unroll
-            for (int h = 0; h < 2; h++) {
-                const double2 l2 = *reinterpret_cast<const double2*>(&cs_.l[cb + 2 * h]);
-                const double2 m2 = *reinterpret_cast<const double2*>(&cs_.m[cb + 2 * h]);
-                const double2 n2 = *reinterpret_cast<const double2*>(&cs_.n[cb + 2 * h]);
-                const float4 w2 = *reinterpret_cast<const float4*>(&cs_.w[cb + 2 * h]);
-                cl[2 * h] = l2.x, cl[2 * h + 1] = l2.y;
-                cm[2 * h] = m2.x, cm[2 * h + 1] = m2.y;
-                cn[2 * h] = n2.x, cn[2 * h + 1] = n2.y;
-                wr[2 * h] = w2.x, wi[2 * h] = w2.y, wr[2 * h + 1] = w2.z, wi[2 * h + 1] = w2.w;
-            }
+                for (int h = 0; h < 2; h++) {
+                    const double2 l2 = *reinterpret_cast<const double2*>(&cs_.l[cb4 + 2 * h]);
+                    const double2 m2 = *reinterpret_cast<const double2*>(&cs_.m[cb4 + 2 * h]);
+                    const double2 n2 = *reinterpret_cast<const double2*>(&cs_.n[cb4 + 2 * h]);
+                    const float4 w2 = *reinterpret_cast<const float4*>(&cs_.w[cb4 + 2 * h]);
+                    cl[2 * h] = l2.x, cl[2 * h + 1] = l2.y;
+                    cm[2 * h] = m2.x, cm[2 * h + 1] = m2.y;
+                    cn[2 * h] = n2.x, cn[2 * h + 1] = n2.y;
+                    wr[2 * h] = w2.x, wi[2 * h] = w2.y, wr[2 * h + 1] = w2.z, wi[2 * h + 1] = w2.w;
+                }
 #pragma unroll
-            for (int j = 0; j < 4; j++)
+                for (int j = 0; j < 4; j++) {
+                    float snq = 0.f, csq = 0.f;
 #pragma unroll
-                for (int s2 = 0; s2 < 2; s2++) {
-                    float sn, cs;
-                    phasor_quarter_f32(u[s2] * cl[j] + v[s2] * cm[j] + w[s2] * cn[j], sn, cs);
-                    const float Xr = fmaf(wr[j], cs, -wi[j] * sn);
-                    const float Xi = fmaf(wr[j], sn, wi[j] * cs);
-                    // x + 0x808080 (balancing offset of the three lower digits)
-                    xr[s2][j] = __float2int_rn(Xr) + 0x808080;
-                    xi[s2][j] = __float2int_rn(Xi) + 0x808080;
-                    if (s2 == ry) {
-                        // y + 0x8080 + 0x400000 in the FP32 mantissa (one rounding)
-                        yr[j] = __float_as_int(__fmaf_rn(cs, SY, YOFF));
-                        yi[j] = __float_as_int(__fmaf_rn(sn, SY, YOFF));
-                        yn[j] = __float_as_int(__fmaf_rn(-sn, SY, YOFF));
+                    for (int s2 = 0; s2 < 2; s2++) {
+                        float sn, cs;
+                        phasor_quarter_f32(u[s2] * cl[j] + v[s2] * cm[j] + w[s2] * cn[j], sn, cs);
+                        const float Xr = fmaf(wr[j], cs, -wi[j] * sn);
+                        const float Xi = fmaf(wr[j], sn, wi[j] * cs);
+                        // x + 0x808080 (balancing offset of the three lower digits)
+                        xr[s2][j] = __float2int_rn(Xr) + 0x808080;
+                        xi[s2][j] = __float2int_rn(Xi) + 0x808080;
+                        if (s2 == ry) snq = sn, csq = cs;
+                    }
+                    if (ysep) phasor_quarter_f32(u[2] * cl[j] + v[2] * cm[j] + w[2] * cn[j], snq, csq);
+                    // y + 0x8080 + 0x400000 in the FP32 mantissa (one rounding)
+                    yr[j] = __float_as_int(__fmaf_rn(csq, SY0, YOFF));
+                    yi[j] = __float_as_int(__fmaf_rn(snq, SY0, YOFF));
+                    yn[j] = __float_as_int(__fmaf_rn(-snq, SY0, YOFF));
+                }
+            } else {
+                // K bytes 4 quad .. 4 quad + 3 of this warp's 16 = components
+                // c0l, c0l + 1 (stage-local) x y in {X, Y}
+                const int c0l = kq * 8 + quad * 2;
+                const int cg = k * C::CPS + c0l;  // component of the pass
+#pragma unroll
+                for (int j = 0; j < 2; j++) {
+                    const int c = cg + j < P.cn ? cg + j : 0;  // past the end: bounded values, zero S
+                    const double cl = cs_.l[c0l + j], cm = cs_.m[c0l + j], cn = cs_.n[c0l + j];
+                    const float4 s0 = cs_.s[c0l + j][0], s1 = cs_.s[c0l + j][1];
+                    float snq = 0.f, csq = 0.f;
+#pragma unroll
+                    for (int s2 = 0; s2 < 2; s2++) {
+                        float sn, cs;
+                        phasor_quarter_f32(u[s2] * cl + v[s2] * cm + w[s2] * cn, sn, cs);
+                        if (s2 == ry) snq = sn, csq = cs;
+                        // (B S)^{a y} = B^{aX} S^{Xy} + B^{aY} S^{Yy}, then times A
+                        const float4 b = beam_row(P, prow[s2], c, fm, arow);  // (B^{aX}, B^{aY}) as re, im
+#pragma unroll
+                        for (int y = 0; y < 2; y++) {
+                            // S^{Xy}: s0 (y = 0: xx, y = 1: xy); S^{Yy}: s1 (yx, yy)
+                            const float sxr = y ? s0.z : s0.x, sxi = y ? s0.w : s0.y;
+                            const float syr = y ? s1.z : s1.x, syi = y ? s1.w : s1.y;
+                            const float tr = b.x * sxr - b.y * sxi + b.z * syr - b.w * syi;
+                            const float ti = b.x * sxi + b.y * sxr + b.z * syi + b.w * syr;
+                            const float Xr = fmaf(tr, cs, -ti * sn) * sx;
+                            const float Xi = fmaf(tr, sn, ti * cs) * sx;
+                            xr[s2][2 * j + y] = __float2int_rn(Xr) + 0x808080;
+                            xi[s2][2 * j + y] = __float2int_rn(Xi) + 0x808080;
+                        }
+                    }
+                    if (ysep) phasor_quarter_f32(u[2] * cl + v[2] * cm + w[2] * cn, snq, csq);
+                    const float4 bq = beam_row(P, qcol, c, fm, brow);
+#pragma unroll
+                    for (int y = 0; y < 2; y++) {
+                        const float br = y ? bq.z : bq.x, bi = y ? bq.w : bq.y;
+                        const float Yr = fmaf(br, csq, -bi * snq) * sy;
+                        const float Yi = fmaf(br, snq, bi * csq) * sy;
+                        const int ir = __float2int_rn(Yr), ii = __float2int_rn(Yi);
+                        yr[2 * j + y] = ir + 0x808080;
+                        yi[2 * j + y] = ii + 0x808080;
+                        yn[2 * j + y] = -ii + 0x808080;
                     }
                 }
+            }
         };
         auto write_planes = [&](int st, const int (&xr)[2][4], const int (&xi)[2][4], const int (&yr)[4],
                                 const int (&yi)[4], const int (&yn)[4]) {
-            unsigned char* sb = smem + st * STAGE_BYTES;
+            unsigned char* sb = smem + st * L::STAGE_BYTES;
             uint32_t pl[4];
             // x planes: bytes 0-2 excess-128 lower digits, byte 3 the signed top digit
 #pragma unroll
@@ -369,43 +513,53 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const Params P) {
                     byte_planes4(part ? xi[s2] : xr[s2], pl);
 #pragma unroll
                     for (int b = 0; b < 4; b++)
-                        *reinterpret_cast<uint32_t*>(sb + x_tile(part, 3 - b) + xo) = b < 3 ? pl[b] ^ 0x80808080u : pl[b];
+                        *reinterpret_cast<uint32_t*>(sb + x_tile<MODE>(part, 3 - b) + xo) =
+                            b < 3 ? pl[b] ^ 0x80808080u : pl[b];
                 }
             }
-            // y planes: bytes 0-1 excess-128, byte 2 the top digit + 64
             const uint32_t yo = chunk_off(r0, kq) + quad * 4;
 #pragma unroll
             for (int part = 0; part < 3; part++) {
                 byte_planes4(part == 0 ? yr : (part == 1 ? yi : yn), pl);
-                *reinterpret_cast<uint32_t*>(sb + y_tile(part, 2) + yo) = pl[0] ^ 0x80808080u;
-                *reinterpret_cast<uint32_t*>(sb + y_tile(part, 1) + yo) = pl[1] ^ 0x80808080u;
-                *reinterpret_cast<uint32_t*>(sb + y_tile(part, 0) + yo) = minus64(pl[2]);
+                if (MODE == 0) {
+                    // y planes: bytes 0-1 excess-128, byte 2 the top digit + 64
+                    *reinterpret_cast<uint32_t*>(sb + y_tile<MODE>(part, 2) + yo) = pl[0] ^ 0x80808080u;
+                    *reinterpret_cast<uint32_t*>(sb + y_tile<MODE>(part, 1) + yo) = pl[1] ^ 0x80808080u;
+                    *reinterpret_cast<uint32_t*>(sb + y_tile<MODE>(part, 0) + yo) = minus64(pl[2]);
+                } else {
+                    // as x: bytes 0-2 excess-128, byte 3 signed
+#pragma unroll
+                    for (int b = 0; b < 4; b++)
+                        *reinterpret_cast<uint32_t*>(sb + y_tile<MODE>(part, 3 - b) + yo) =
+                            b < 3 ? pl[b] ^ 0x80808080u : pl[b];
+                }
             }
         };
-        if (tid < KC) {
-            double2 a, b, wd;
+        if (tid < C::CPS) {
+            double2 a, b;
+            double4 wd;
             fetch(0, a, b, wd);
-            stash(0, a, b, wd);
+            stash(0, 0, a, b, wd);
             fetch(1, a, b, wd);
-            stash(1, a, b, wd);
+            stash(1, 1, a, b, wd);
         }
         producers_sync_or(false);
         int xr[2][4], xi[2][4], yr[4], yi[4], yn[4];
         compute(0, xr, xi, yr, yi, yn);
-        // The producer warps run decoupled: each thread arrives on a stage's
-        // full barrier once its planes are written, a warp waits for the
-        // tensor core only on the buffer it is about to overwrite, and for
-        // the component data only on the ring slot it is about to read (so
-        // warps may drift up to NSTAGE stages apart; the ring has room for
-        // that).  Any timeout sets abort_s; the others leave at their next
-        // stage or their own bounded wait.
-        static_assert(KC == 32, "warp 0 stashes the component data");
+        // The producer warps run decoupled: each warp arrives on a stage's
+        // full barrier once its planes are written, waits for the tensor
+        // core only on the buffer it is about to overwrite, and for the
+        // component data only on the ring slot it is about to read.  Any
+        // timeout sets abort_s; the others leave at their next stage or their
+        // own bounded wait.
         for (int k = 0; k < nchunks; k++) {
             const int st = k % NSTAGE;
-            double2 na, nb, nw;  // stage k + 2's component data, in flight during this stage
-            const bool pre = tid < KC;
+            double2 na, nb;  // stage k + 2's component data, in flight during this stage
+            double4 nw;
+            const bool pre = tid < C::CPS;
             if (pre) fetch(k + 2, na, nb, nw);
-            if (k >= NSTAGE && !__all_sync(0xffffffffu, mbar_wait_bounded(&empty_bar[st], ((k / NSTAGE) - 1) & 1, P.err))) {
+            if (k >= NSTAGE &&
+                !__all_sync(0xffffffffu, mbar_wait_bounded(&empty_bar[st], ((k / NSTAGE) - 1) & 1, P.err))) {
                 abort_s = 1;
                 break;
             }
@@ -420,7 +574,7 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const Params P) {
             }
             compute(k + 1, nxr, nxi, nyr, nyi, nyn);
             fence_proxy_async_smem();  // make the generic-proxy stores visible to the tensor core
-            if (pre) stash((k + 2) % CRING, na, nb, nw);
+            if (pre) stash(k + 2, (k + 2) % CRING, na, nb, nw);
             __syncwarp();  // the lanes' stores and fences before the warp's one arrival
             if (lane == 0) {
                 mbar_arrive(&full_bar[st]);
@@ -450,19 +604,20 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const Params P) {
                 // compile-time tile offsets (in 16-byte units, the
                 // descriptor's address field); the first product of each
                 // class in the launch's first stage overwrites its accumulator
-                const uint64_t d0 = smem_desc(sbase + st * STAGE_BYTES);
+                const uint64_t d0 = smem_desc(sbase + st * L::STAGE_BYTES);
                 const uint32_t acc0 = k > 0 ? 1u : 0u;
 #pragma unroll
-                for (int i = 0; i < XDIG; i++)
+                for (int i = 0; i < C::XDIG; i++)
 #pragma unroll
-                    for (int j = 0; j < YDIG; j++) {
+                    for (int j = 0; j < C::YDIG; j++) {
                         const int cls = i + j;
                         if (cls > 3) continue;
-                        const bool first = (i == 0) || (i == 1 && j == 2);
+                        const bool first = i == (cls - (C::YDIG - 1) > 0 ? cls - (C::YDIG - 1) : 0);
                         // [Re | Im] += Xr [Yr; -Yi]^T + Xi [Yi; Yr]^T
-                        mma_i8(tmem + acc_col(cls), d0 + (x_tile(0, i) >> 4), d0 + (y_tile(0, j) >> 4), id,
-                               first ? acc0 : 1u);
-                        mma_i8(tmem + acc_col(cls), d0 + (x_tile(1, i) >> 4), d0 + (y_tile(1, j) >> 4), id, 1u);
+                        mma_i8(tmem + acc_col(cls), d0 + (x_tile<MODE>(0, i) >> 4), d0 + (y_tile<MODE>(0, j) >> 4),
+                               id, first ? acc0 : 1u);
+                        mma_i8(tmem + acc_col(cls), d0 + (x_tile<MODE>(1, i) >> 4), d0 + (y_tile<MODE>(1, j) >> 4),
+                               id, 1u);
                     }
                 mma_commit(&empty_bar[st]);  // stage free once these MMAs have read it
             }
@@ -473,53 +628,49 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const Params P) {
     // ---------------------------------------------------- epilogue
     __syncthreads();
     const bool aborted = abort_s != 0;
-    const bool ok = mbar_wait_bounded(&done_bar, 0, P.err);
+    const bool ok = zero || mbar_wait_bounded(&done_bar, 0, P.err);
     tc_fence_after();
-    if (!aborted && ok && warp < NPW && nchunks > 0) {
+    if (!aborted && ok && warp < NPW) {
+        constexpr int XW = 8 * (C::XDIG - 1), YW = 8 * (C::YDIG - 1);
         const int lg = warp & 3;       // TMEM lane group this warp may access
         const int cq = warp >> 2;      // quarter of the NH columns
-        const int p = lg * 32 + lane;  // row: tile p
+        const int p = NT * rb + lg * 32 + lane;  // row: tile p
         const uint32_t lane_addr = tmem + ((uint32_t)(lg * 32) << 16);
-        const int n = P.ntiles;
+        const size_t plane = (size_t)P.nf * P.nbl;
         for (int c0 = cq * (NH / 4); c0 < cq * (NH / 4) + NH / 4; c0 += 8) {
             int a[8][8];  // [class * 2 + re/im][column]
+            if (!zero) {
 #pragma unroll
-            for (int g = 0; g < 8; g++)  // g = class * 2 + (0 Re, 1 Im)
-                tmem_ld8(lane_addr + acc_col(g >> 1) + (uint32_t)((g & 1) * NH + c0), a[g]);
-            tmem_wait_ld();
+                for (int g = 0; g < 8; g++)  // g = class * 2 + (0 Re, 1 Im)
+                    tmem_ld8(lane_addr + acc_col(g >> 1) + (uint32_t)((g & 1) * NH + c0), a[g]);
+                tmem_wait_ld();
+            }
             if (p >= n) continue;
 #pragma unroll
             for (int j = 0; j < 8; j++) {
-                const int q = hcol * NH + c0 + j;
+                const int q = NH * cb + c0 + j;
                 if (q == p || q >= n) continue;
                 if (pol < 2 && q < p) continue;
                 double re = 0.0, im = 0.0;
+                if (!zero) {
 #pragma unroll
-                for (int cls = 0; cls < 4; cls++) {
-                    const double wgt = ldexp(1.0, 40 - 8 * cls);
-                    re += (double)a[cls * 2][j] * wgt;
-                    im += (double)a[cls * 2 + 1][j] * wgt;
+                    for (int cls = 0; cls < 4; cls++) {
+                        const double wgt = ldexp(1.0, XW + YW - 8 * cls);
+                        re += (double)a[cls * 2][j] * wgt;
+                        im += (double)a[cls * 2 + 1][j] * wgt;
+                    }
+                    re *= inv;
+                    im *= inv;
                 }
-                re *= inv;
-                im *= inv;
                 const bool upper = q > p;
                 const size_t o = (size_t)f * P.nbl + (upper ? baseline_index(p, q, n) : baseline_index(q, p, n));
                 // XY(p, q) for q > p; YX(q, p) = conj(XY(p, q)) for q < p
                 const int slot = pol == 0 ? 0 : (pol == 1 ? 3 : (upper ? 1 : 2));
                 if (!upper) im = -im;
-                if (OUT64) {
-                    double2* vp = reinterpret_cast<double2*>(reinterpret_cast<JonesF64*>(P.vis) + o) + slot;
-                    double2 cur = *vp;
-                    cur.x += re;
-                    cur.y += im;
-                    *vp = cur;
-                } else {
-                    float2* vp = reinterpret_cast<float2*>(reinterpret_cast<JonesF32*>(P.vis) + o) + slot;
-                    float2 cur = *vp;
-                    cur.x += (float)re;
-                    cur.y += (float)im;
-                    *vp = cur;
-                }
+                if (OUT64)
+                    reinterpret_cast<double2*>(P.planes)[slot * plane + o] = make_double2(re, im);
+                else
+                    reinterpret_cast<float2*>(P.planes)[slot * plane + o] = make_float2((float)re, (float)im);
             }
         }
     }
@@ -528,57 +679,159 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const Params P) {
     }
     tc_fence_before();
     __syncthreads();
-    if (warp == 0) {
+    if (!zero && warp == 0) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
     }
 }
 
+// vis [nf][nbl] += the four planes (one thread per visibility, coalesced)
+template <bool OUT64>
+__global__ void combine_kernel(const void* planes, void* vis, size_t n) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (OUT64) {
+        const double2* pl = reinterpret_cast<const double2*>(planes);
+        double2* v = reinterpret_cast<double2*>(reinterpret_cast<JonesF64*>(vis) + i);
+#pragma unroll
+        for (int s = 0; s < 4; s++) {
+            const double2 a = pl[s * n + i];
+            double2 b = v[s];
+            b.x += a.x;
+            b.y += a.y;
+            v[s] = b;
+        }
+    } else {
+        const float2* pl = reinterpret_cast<const float2*>(planes);
+        float4* v = reinterpret_cast<float4*>(reinterpret_cast<JonesF32*>(vis) + i);
+        const float2 xx = pl[i], xy = pl[n + i], yx = pl[2 * n + i], yy = pl[3 * n + i];
+        float4 a = v[0], b = v[1];
+        a.x += xx.x, a.y += xx.y, a.z += xy.x, a.w += xy.y;
+        b.x += yx.x, b.y += yx.y, b.z += yy.x, b.w += yy.y;
+        v[0] = a;
+        v[1] = b;
+    }
+}
+
+// Per channel: the largest |entry| of the beam Jones over unique tiles and
+// components (at the channel's unique frequency) and of S (MODE 1 scales).
+__global__ void beam_bounds_kernel(const JonesF64* beam, int n_uniq_tile, const int* freq_map, int n_uniq_freq,
+                                   const JonesF64* S, int nc, int c0, int cn, double* maxb, double* maxs) {
+    const int f = blockIdx.x;
+    const int fm = freq_map[f];
+    double mb = 0.0, ms = 0.0;
+    for (int i = threadIdx.x; i < n_uniq_tile * cn; i += blockDim.x) {
+        const int u = i / cn, c = i % cn;
+        const double2* b = reinterpret_cast<const double2*>(beam + ((size_t)u * n_uniq_freq + fm) * nc + c0 + c);
+#pragma unroll
+        for (int e = 0; e < 4; e++) mb = fmax(mb, hypot(b[e].x, b[e].y));
+    }
+    for (int c = threadIdx.x; c < cn; c += blockDim.x) {
+        const double2* s = reinterpret_cast<const double2*>(S + (size_t)f * nc + c0 + c);
+#pragma unroll
+        for (int e = 0; e < 4; e++) ms = fmax(ms, hypot(s[e].x, s[e].y));
+    }
+    __shared__ double rb[2][32];
+    for (int o = 16; o > 0; o >>= 1) {
+        mb = fmax(mb, __shfl_xor_sync(0xffffffffu, mb, o));
+        ms = fmax(ms, __shfl_xor_sync(0xffffffffu, ms, o));
+    }
+    if ((threadIdx.x & 31) == 0) rb[0][threadIdx.x >> 5] = mb, rb[1][threadIdx.x >> 5] = ms;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++) mb = fmax(mb, rb[0][w]), ms = fmax(ms, rb[1][w]);
+        mb = fmax(mb, rb[0][0]);
+        ms = fmax(ms, rb[1][0]);
+        maxb[f] = mb;
+        maxs[f] = ms;
+    }
+}
+
+// The jobs of one channel: (pol, row block, column block) with a baseline of
+// that polarisation.  Returns their number (0 if more than MAXJOBS).
+int build_jobs(int ntiles, uint32_t* jobs) {
+    const int nrb = (ntiles + NT - 1) / NT, ncb = (ntiles + NH - 1) / NH;
+    int nj = 0;
+    for (int pol = 0; pol < 3; pol++)
+        for (int rb = 0; rb < nrb; rb++)
+            for (int cb = 0; cb < ncb; cb++) {
+                const int rlo = NT * rb, rhi = std::min(NT * rb + NT, ntiles) - 1;
+                const int clo = NH * cb, chi = std::min(NH * cb + NH, ntiles) - 1;
+                const bool any = pol < 2 ? chi > rlo : (rhi > rlo || chi > clo || rlo != clo);
+                if (!any) continue;
+                if (nj >= MAXJOBS) return 0;
+                jobs[nj++] = (uint32_t)pol | ((uint32_t)rb << 8) | ((uint32_t)cb << 20);
+            }
+    return nj;
+}
+
 }  // namespace tc
+
+// Bytes of device workspace the tensor predict needs for nf channels: the
+// four planes and the MODE 1 per-channel bounds.
+size_t tensor_workspace_bytes(int nf, int nbl, bool out64) {
+    const size_t planes = (size_t)4 * nf * nbl * (out64 ? 16 : 8);
+    return ((planes + 255) & ~(size_t)255) + 2 * sizeof(double) * (size_t)nf + 256;
+}
 
 struct TensorState {
     bool configured = false;
+    void* ws = nullptr;
+    size_t ws_bytes = 0;
 };
 
+int tensor_configure() {
+    static std::once_flag once;
+    static cudaError_t attr_err = cudaSuccess;
+    std::call_once(once, [] {
+        const cudaError_t e[4] = {
+            cudaFuncSetAttribute(tc::gram_i8_kernel<0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 tc::Lay<0>::SMEM_BYTES),
+            cudaFuncSetAttribute(tc::gram_i8_kernel<0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 tc::Lay<0>::SMEM_BYTES),
+            cudaFuncSetAttribute(tc::gram_i8_kernel<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 tc::Lay<1>::SMEM_BYTES),
+            cudaFuncSetAttribute(tc::gram_i8_kernel<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 tc::Lay<1>::SMEM_BYTES)};
+        for (cudaError_t x : e)
+            if (x != cudaSuccess && attr_err == cudaSuccess) attr_err = x;
+    });
+    HDC_CUDA_RET_INT(attr_err);
+    return HDC_OK;
+}
+
 int Modeller::tensor_setup() {
-    if (ntiles > tc::NT) {
-        set_error("the tensor-core predict supports up to %d tiles (have %d)", tc::NT, ntiles);
+    if (!tc) tc = new TensorState();
+    int rc = tensor_configure();
+    if (rc) return rc;
+    if (tc::build_jobs(ntiles, std::vector<uint32_t>(tc::MAXJOBS).data()) == 0) {
+        set_error("the tensor-core predict supports up to %d jobs per channel (%d tiles is too many)", tc::MAXJOBS,
+                  ntiles);
         return HDC_ERR_UNSUPPORTED;
     }
-    if (!tc) tc = new TensorState();
-    if (!tc->configured) {
-        HDC_CUDA_RET_INT(cudaFuncSetAttribute(tc::gram_i8_kernel<false>,
-                                              cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES));
-        HDC_CUDA_RET_INT(cudaFuncSetAttribute(tc::gram_i8_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              tc::SMEM_BYTES));
-        tc->configured = true;
-    }
+    tc->configured = true;
     return HDC_OK;
 }
 
 // The tensor-core point predict of one timestep over device tables: lmn
-// [nc] (turns), W [nf][nc] (B S B^H of a beam shared by all tiles), tile
-// XYZs, hour angle and declination of the phase centre; accumulates into
-// vis [nf][nbl] (JonesF32, or JonesF64 with out64).
+// [nc] (turns), W [nf][nc] (B S B^H of a beam shared by all tiles, or S with
+// per-tile beams in `beam`), tile XYZs, hour angle and declination of the
+// phase centre; accumulates into vis [nf][nbl] (JonesF32, or JonesF64 with
+// out64).  ws: tensor_workspace_bytes(nf, nbl, out64) of device memory.
 int launch_tensor_points(int nf, int nbl, int ntiles, int nc, const double* d_freqs, const XYZ* d_xyzs, double ha,
-                         double dec, const double4* d_lmn, const JonesF64* d_W, void* d_vis, bool out64, int* d_err,
-                         cudaStream_t s) {
-    if (nc == 0) return HDC_OK;
-    if (ntiles > tc::NT) {
-        set_error("the tensor-core predict supports up to %d tiles (have %d)", tc::NT, ntiles);
+                         double dec, const double4* d_lmn, const JonesF64* d_W, const TensorBeam* beam, void* d_vis,
+                         bool out64, void* ws, int* d_err, cudaStream_t s) {
+    if (nc == 0 || nf == 0) return HDC_OK;
+    int rc = tensor_configure();
+    if (rc) return rc;
+    tc::Params P;
+    P.njobs = tc::build_jobs(ntiles, P.jobs);
+    if (P.njobs == 0) {
+        set_error("the tensor-core predict supports up to %d jobs per channel (%d tiles is too many)", tc::MAXJOBS,
+                  ntiles);
         return HDC_ERR_UNSUPPORTED;
     }
-    static std::once_flag once;
-    static cudaError_t attr_err = cudaSuccess;
-    std::call_once(once, [] {
-        attr_err = cudaFuncSetAttribute(tc::gram_i8_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        tc::SMEM_BYTES);
-        if (attr_err == cudaSuccess)
-            attr_err = cudaFuncSetAttribute(tc::gram_i8_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            tc::SMEM_BYTES);
-    });
-    HDC_CUDA_RET_INT(attr_err);
-    tc::Params P;
+    const bool tile_beam = beam && beam->beam;
     P.nf = nf;
     P.nbl = nbl;
     P.ntiles = ntiles;
@@ -591,30 +844,70 @@ int launch_tensor_points(int nf, int nbl, int ntiles, int nc, const double* d_fr
     P.c_dec = std::cos(dec);
     P.lmn = d_lmn;
     P.W = d_W;
-    P.vis = d_vis;
+    P.beam = tile_beam ? beam->beam : nullptr;
+    P.tile_map = tile_beam ? beam->tile_map : nullptr;
+    P.freq_map = tile_beam ? beam->freq_map : nullptr;
+    P.n_uniq_freq = tile_beam ? beam->n_uniq_freq : 0;
+    const size_t planes_bytes = (((size_t)4 * nf * nbl * (out64 ? 16 : 8)) + 255) & ~(size_t)255;
+    P.planes = ws;
+    double* bounds = reinterpret_cast<double*>(static_cast<char*>(ws) + planes_bytes);
+    P.maxb = bounds;
+    P.maxs = bounds + nf;
     P.err = d_err;
+    const int kpass = tile_beam ? tc::Cfg<1>::KPASS : tc::Cfg<0>::KPASS;
+    const dim3 grid(P.njobs, nf);
+    const size_t nvis = (size_t)nf * nbl;
     // passes of at most KPASS components accumulate into the visibilities in turn
-    const dim3 grid(nf, 3, (ntiles + tc::NH - 1) / tc::NH);
-    for (int c0 = 0; c0 < P.nc; c0 += tc::KPASS) {
+    for (int c0 = 0; c0 < P.nc; c0 += kpass) {
         P.c0 = c0;
-        P.cn = std::min(tc::KPASS, P.nc - c0);
+        P.cn = std::min(kpass, P.nc - c0);
+        if (tile_beam) {
+            tc::beam_bounds_kernel<<<nf, 256, 0, s>>>(beam->beam, beam->n_uniq_tile, beam->freq_map,
+                                                      beam->n_uniq_freq, d_W, nc, c0, P.cn, bounds, bounds + nf);
+            count_launches(1);
+            HDC_CUDA_RET_INT(cudaGetLastError());
+            if (out64)
+                tc::gram_i8_kernel<1, true><<<grid, tc::THREADS, tc::Lay<1>::SMEM_BYTES, s>>>(P);
+            else
+                tc::gram_i8_kernel<1, false><<<grid, tc::THREADS, tc::Lay<1>::SMEM_BYTES, s>>>(P);
+        } else {
+            if (out64)
+                tc::gram_i8_kernel<0, true><<<grid, tc::THREADS, tc::Lay<0>::SMEM_BYTES, s>>>(P);
+            else
+                tc::gram_i8_kernel<0, false><<<grid, tc::THREADS, tc::Lay<0>::SMEM_BYTES, s>>>(P);
+        }
+        count_launches(1);
+        HDC_CUDA_RET_INT(cudaGetLastError());
+        const unsigned blocks = (unsigned)((nvis + 255) / 256);
         if (out64)
-            tc::gram_i8_kernel<true><<<grid, tc::THREADS, tc::SMEM_BYTES, s>>>(P);
+            tc::combine_kernel<true><<<blocks, 256, 0, s>>>(ws, d_vis, nvis);
         else
-            tc::gram_i8_kernel<false><<<grid, tc::THREADS, tc::SMEM_BYTES, s>>>(P);
+            tc::combine_kernel<false><<<blocks, 256, 0, s>>>(ws, d_vis, nvis);
         count_launches(1);
         HDC_CUDA_RET_INT(cudaGetLastError());
     }
     return HDC_OK;
 }
 
-int Modeller::tensor_points(double lst, void* d_vis, bool out64, cudaStream_t s) {
-    if (t[0].nc == 0) return HDC_OK;
-    return launch_tensor_points(nf, nbl, ntiles, t[0].nc, d_freqs, d_xyzs, lst - pc.ra, pc.dec, t[0].d_lmn,
-                                weights(0), d_vis, out64, d_err, s);
+// The modeller's workspace for the tensor predict of up to nf channels.
+void* Modeller::tensor_workspace(bool out64) {
+    const size_t need = tensor_workspace_bytes(nf, nbl, out64);
+    if (tc->ws_bytes < need) {
+        if (tc->ws) cudaFree(tc->ws);
+        tc->ws = nullptr;
+        tc->ws_bytes = 0;
+        if (cudaMalloc(&tc->ws, need) != cudaSuccess) {
+            cudaGetLastError();
+            set_error("tensor predict workspace of %zu bytes: allocation failed", need);
+            return nullptr;
+        }
+        tc->ws_bytes = need;
+    }
+    return tc->ws;
 }
 
 void Modeller::tensor_release() {
+    if (tc && tc->ws) cudaFree(tc->ws);
     delete tc;
     tc = nullptr;
 }

@@ -19,7 +19,7 @@ import numpy as np
 from . import _lib
 from .srclist import SkyModelArrays, SourceList, Source
 
-BEAMS = {"none": 0, "analytic": 1}
+BEAMS = {"none": 0, "analytic": 1, "per_tile": 2}
 FORMS = {"direct": 0, "tensor": 1}
 POLS = {"XX_XY_YX_YY": 0, "XX": 1, "YY": 2, "XX_YY": 3, "XX_YY_XY": 4}
 
@@ -51,7 +51,11 @@ class SkyModeller:
     """GPU sky modeller (SkyModellerGpu equivalent)."""
 
     def __init__(self, sky, tile_xyzs, freqs, phase_centre, array_latitude_rad: float, pols: str = "XX_XY_YX_YY",
-                 beam: str = "none", form: str = "direct"):
+                 beam: str = "none", form: str = "direct", dipole_gains=None, beam_freq_res_hz: float = 1.28e6):
+        """beam: "none", "analytic" (the dipole-array tile, shared by all
+        tiles) or "per_tile" (each tile's own dipole amplitudes,
+        ``dipole_gains`` [tile][2][16], 0 for a dead dipole; evaluated at the
+        nearest multiple of ``beam_freq_res_hz`` of each channel)."""
         self.lib = _lib.lib()
         self.sky = _as_sky(sky)
         self.tile_xyzs = np.ascontiguousarray(tile_xyzs, dtype=np.float64).reshape(-1, 3)
@@ -70,6 +74,14 @@ class SkyModeller:
                                        FORMS[form], ctypes.byref(h))
         _lib.check(rc, "hdc_modeller_new")
         self._h = h
+        if beam == "per_tile" and dipole_gains is not None:
+            self.set_tile_beams(dipole_gains, beam_freq_res_hz)
+
+    def set_tile_beams(self, dipole_gains, beam_freq_res_hz: float = 1.28e6) -> None:
+        g = np.ascontiguousarray(dipole_gains, dtype=np.float64).reshape(self.num_tiles, 2, 16)
+        _lib.check(self.lib.hdc_modeller_set_tile_beams(self._h, g.ctypes.data, float(beam_freq_res_hz)),
+                   "set_tile_beams")
+        self.beam = "per_tile"
 
     def close(self) -> None:
         if getattr(self, "_h", None):

@@ -362,6 +362,41 @@ J64 analytic_beam(double az, double el, double freq) {
     return r;
 }
 
+// The same tile with each dipole's own amplitude g [2][16] (X dipoles then
+// Y; dipole d at east (d % 4 - 1.5) 1.1 m, north (d / 4 - 1.5) 1.1 m; this
+// project's model, used for per-tile beams): J = diag(ax, ay) R(az)^T
+// diag(cos za, 1) R(az), ax = AF(g_x) GP / |GP(0)|, AF(g) = (1/16) sum_d g_d
+// exp(i k (x_d l + y_d m)).  With unit gains it is analytic_beam.
+J64 analytic_beam_tile(double az, double el, double freq, const double* g) {
+    if (el <= 0.0) return jzero();
+    double za = FRAC_PI_2 - el;
+    double k = TAU * freq / VEL_C;
+    double sza = std::sin(za), cza = std::cos(za);
+    double saz = std::sin(az), caz = std::cos(az);
+    double l = sza * saz, m = sza * caz;
+    c64 afx = {0.0, 0.0}, afy = {0.0, 0.0};
+    for (int d = 0; d < 16; d++) {
+        double x = (d % 4 - 1.5) * 1.1, y = (d / 4 - 1.5) * 1.1;
+        c64 e = cis(k * (x * l + y * m));
+        afx = cadd(afx, cscale(e, g[d]));
+        afy = cadd(afy, cscale(e, g[16 + d]));
+    }
+    const double h = 0.278;
+    double ph = 2.0 * k * h * cza;
+    c64 gp = {1.0 - std::cos(ph), std::sin(ph)};
+    double gp0 = 2.0 * std::fabs(std::sin(k * h));
+    c64 ax = cscale(cmul(afx, gp), 1.0 / (16.0 * gp0)), ay = cscale(cmul(afy, gp), 1.0 / (16.0 * gp0));
+    double p00 = cza * saz * saz + caz * caz;
+    double p01 = (cza - 1.0) * saz * caz;
+    double p11 = cza * caz * caz + saz * saz;
+    J64 r;
+    r.j[0] = cscale(ax, p00);
+    r.j[1] = cscale(ax, p01);
+    r.j[2] = cscale(ay, p01);
+    r.j[3] = cscale(ay, p11);
+    return r;
+}
+
 std::vector<double> g_sbf;  // shapelet basis table, built on first use
 
 // The reference regenerates its table with make_shapelet_basis_values.py:
@@ -477,6 +512,25 @@ void or_xyzs_to_cross_uvws(const double* xyzs, int ntiles, double ha, double dec
 void or_hadec_to_azel(double ha, double dec, double lat, double* az, double* el) { hadec_to_azel(ha, dec, lat, az, el); }
 
 void or_analytic_beam(double az, double el, double freq, double* out8) { to_f64(analytic_beam(az, el, freq), out8); }
+
+// Per-tile beam table of the components of type comp_type in sky-model
+// order: out [uniq][nuf][n_type] JonesF64 from gains [uniq][2][16] at the
+// unique frequencies ufreqs, for the given LST and latitude (the explicit
+// per-tile layout of OrBeam kind 2).
+void or_tile_beam_table(const OrSky* s, int comp_type, double lst, double lat, const double* gains, int nuniq,
+                        const double* ufreqs, int nuf, double* out) {
+    std::vector<int> idx;
+    for (int c = 0; c < s->num_components; c++)
+        if (s->comp_type[c] == comp_type) idx.push_back(c);
+    const int n = (int)idx.size();
+    for (int k = 0; k < n; k++) {
+        double az, el;
+        hadec_to_azel(lst - s->ra[idx[k]], s->dec[idx[k]], lat, &az, &el);
+        for (int u = 0; u < nuniq; u++)
+            for (int f = 0; f < nuf; f++)
+                to_f64(analytic_beam_tile(az, el, ufreqs[f], gains + 32 * u), out + 8 * (((size_t)u * nuf + f) * n + k));
+    }
+}
 
 // ---------------------------------------------------------------------------
 // Predictor: SkyModellerCpu::model_points / model_gaussians / model_shapelets

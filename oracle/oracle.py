@@ -421,3 +421,37 @@ def peel_cpu(resid, weights, freqs, xyzs, lmsts, average_lmst, pc, sources, posi
                       ctypes.c_int(num_passes), ctypes.c_int(num_loops), ctypes.c_double(convergence),
                       ctypes.c_int(favg), ctypes.c_double(lat))
     return resid, [(c.alpha, c.beta, c.gain) for c in cs]
+
+
+def tile_beam_table(sky, comp_type, lst, lat, gains, ufreqs):
+    """Per-tile analytic beam Jones [uniq][nuf][n_type][8] of the sky's
+    components of one type (this project's dipole-gain model)."""
+    s, keep = sky_struct(sky)
+    gains = np.ascontiguousarray(gains, np.float64).reshape(-1, 32)
+    ufreqs = np.ascontiguousarray(ufreqs, np.float64)
+    n = int(np.sum(np.asarray(sky.comp_type) == comp_type))
+    out = np.zeros((gains.shape[0], ufreqs.size, n, 8))
+    lib().or_tile_beam_table(ctypes.byref(s), ctypes.c_int(comp_type), ctypes.c_double(lst), ctypes.c_double(lat),
+                             _ptr(gains), ctypes.c_int(gains.shape[0]), _ptr(ufreqs), ctypes.c_int(ufreqs.size),
+                             _ptr(out))
+    return out
+
+
+def unique_tile_beams(dipole_gains, freqs, freq_res_hz=1.28e6):
+    """The unique tiles (by their 32 dipole gains, first appearance order), the
+    unique beam frequencies (nearest multiple of freq_res_hz) and the maps, as
+    the native modeller forms them."""
+    g = np.asarray(dipole_gains, np.float64).reshape(-1, 32)
+    uniq, tile_map = [], np.zeros(g.shape[0], np.int32)
+    for p in range(g.shape[0]):
+        for u, row in enumerate(uniq):
+            if np.array_equal(row, g[p]):
+                tile_map[p] = u
+                break
+        else:
+            tile_map[p] = len(uniq)
+            uniq.append(g[p])
+    bins = np.floor(np.asarray(freqs) / freq_res_hz + 0.5).astype(np.int64)  # as C's llround for positives
+    ub = np.unique(bins)
+    freq_map = np.searchsorted(ub, bins).astype(np.int32)
+    return np.array(uniq), tile_map, ub * freq_res_hz, freq_map

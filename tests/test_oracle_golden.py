@@ -279,3 +279,41 @@ def test_mitchcal_division_order(oracle):
     dj, res = oracle.calibrate_timeblock(data, model, ident, 0, nt, 200, 1e-12, 1e-4, 0)
     G = _c(dj[:, 0])
     assert _residual(G, d1, m1, ntiles) < 1e-5
+
+
+def test_per_tile_beam_with_unit_gains_is_the_shared_beam():
+    """The per-tile dipole-gain beam with every dipole at unit gain is the
+    shared analytic beam (the array factor then separates in l and m)."""
+    from oracle import oracle as O
+
+    for az, el, f in [(0.3, 1.2, 150e6), (2.0, 0.6, 182e6), (4.1, 1.5, 200e6)]:
+        ref = O.analytic_beam(az, el, f)
+        sky = _one_point_sky(az, el)
+        g = np.ones((1, 32))
+        # a component at the given (az, el): HA/Dec from an LST of 0
+        got = O.tile_beam_table(sky[0], 0, sky[1], sky[2], g, [f])[0, 0, 0]
+        np.testing.assert_allclose(got, ref, rtol=0, atol=1e-12)
+    # a dead dipole changes the beam, and only the row of its polarisation
+    sky = _one_point_sky(1.0, 0.9)
+    g = np.ones((2, 32))
+    g[1, 5] = 0.0  # X dipole 5 of the second tile
+    b = O.tile_beam_table(sky[0], 0, sky[1], sky[2], g, [170e6])[:, 0, 0]
+    assert np.abs(b[1, 0:4] - b[0, 0:4]).max() > 1e-3
+    np.testing.assert_allclose(b[1, 4:8], b[0, 4:8], rtol=0, atol=1e-15)
+
+
+def _one_point_sky(az, el, lat=-0.4660608448386394):
+    """A one-point sky at (az, el) for LST 0 and the given latitude."""
+    import math
+
+    from mwa_hyperdrive_b200 import srclist as sl
+
+    # invert hd2ae: direction cosines in the (east, north, up) frame
+    x = math.cos(el) * math.sin(az)
+    y = math.cos(el) * math.cos(az)
+    z = math.sin(el)
+    # to (HA, Dec) at latitude lat
+    dec = math.asin(y * math.cos(lat) + z * math.sin(lat))
+    ha = math.atan2(-x, -y * math.sin(lat) + z * math.cos(lat))
+    comp = sl.SourceComponent(-ha, dec, sl.Point(), sl.PowerLaw(-0.8, sl.FluxDensity(150e6, 1.0)))
+    return sl.SkyModelArrays.from_components([comp]), 0.0, lat

@@ -340,3 +340,69 @@ def test_dropin_model_functions_per_tile_beam(oracle, ctype):
     b = oracle.beam_struct(2, bj_t, tile_map, freq_map, 2)
     ref = oracle.model_type(ctype, sky, obs.tile_xyzs, obs.freqs, pc, lst, LAT, uvws, beam=b)
     assert_f32_close(vis.cpu().numpy(), ref, ulps=4)
+
+
+# ---------------------------------------------------------- per-tile beams
+def dipole_gains(ntiles, seed, damaged=0.3):
+    """[tile][2][16] dipole amplitudes: most tiles intact, a fraction with one
+    or two dead dipoles (a few distinct patterns, so tiles share beams)."""
+    rng = np.random.default_rng(seed)
+    g = np.ones((ntiles, 2, 16))
+    patterns = [(0, 5), (1, 12), (0, 3), (1, 0)]
+    for p in range(ntiles):
+        if rng.random() < damaged:
+            pol, d = patterns[rng.integers(len(patterns))]
+            g[p, pol, d] = 0.0
+            if rng.random() < 0.3:
+                g[p, 1 - pol, (d + 7) % 16] = 0.0
+    return g
+
+
+def oracle_tile_beam(oracle, sky, obs, lst, gains, res=1.28e6):
+    uniq, tmap, ufreqs, fmap = oracle.unique_tile_beams(gains, obs.freqs, res)
+    tabs = [oracle.tile_beam_table(sky, ty, lst, obs.latitude, uniq, ufreqs)
+            if np.any(np.asarray(sky.comp_type) == ty) else None for ty in range(3)]
+    return oracle.beam_struct(2, tabs, tmap, fmap, ufreqs.size), len(uniq)
+
+
+@pytest.mark.parametrize("ctype", [0, 1, 2])
+def test_per_tile_beams_direct_fp64(oracle, ctype):
+    """Per-tile beams (each tile's own dipole gains, tiles with equal gains
+    sharing one beam, evaluated at the nearest 1.28 MHz of each channel):
+    the direct FP64 form against the oracle with the same explicit per-tile
+    Jones table, within 1e-10."""
+    pc = (0.3, math.radians(-30.0))
+    obs = synth.Obs(synth.tiles_in_disk(24, 1200.0, 5), 166.4e6 + np.arange(6) * 0.64e6, pc, np.array([0.41]))
+    comps = synth.point_sky(12, pc, 8.0, 3) if ctype == 0 else \
+        synth.gaussians_and_shapelets(12 if ctype == 1 else 0, 0 if ctype == 1 else 8, pc, 4)
+    sky = sl.SkyModelArrays.from_components(comps)
+    gains = dipole_gains(obs.num_tiles, 7)
+    m = SkyModeller(sky, obs.tile_xyzs, obs.freqs, pc, obs.latitude, beam="per_tile", dipole_gains=gains)
+    vis = torch.zeros((obs.freqs.size, obs.num_baselines, 8), dtype=torch.float64, device="cuda")
+    m.model_timestep_with(obs.lsts[0], vis)
+    torch.cuda.synchronize()
+    b, nuniq = oracle_tile_beam(oracle, sky, obs, obs.lsts[0], gains)
+    assert nuniq > 2
+    ref, _ = oracle.model_timestep(sky, obs.tile_xyzs, obs.freqs, pc, obs.lsts[0], obs.latitude, beam=b,
+                                   out_f64=True)
+    nrm, mx = rel_err(vis.cpu().numpy(), ref)
+    assert nrm < 1e-10 and mx < 1e-10, (nrm, mx)
+    # the per-tile beam is not the shared one
+    vs = torch.zeros_like(vis)
+    SkyModeller(sky, obs.tile_xyzs, obs.freqs, pc, obs.latitude, beam="analytic").model_timestep_with(obs.lsts[0], vs)
+    torch.cuda.synchronize()
+    assert rel_err(vs.cpu().numpy(), ref)[0] > 1e-4
+
+
+def test_per_tile_beams_autos(oracle):
+    pc = (0.3, math.radians(-30.0))
+    obs = synth.Obs(synth.tiles_in_disk(16, 1200.0, 5), 166.4e6 + np.arange(4) * 0.64e6, pc, np.array([0.41]))
+    sky = sl.SkyModelArrays.from_components(synth.point_sky(9, pc, 8.0, 3))
+    gains = dipole_gains(obs.num_tiles, 8, damaged=0.5)
+    m = SkyModeller(sky, obs.tile_xyzs, obs.freqs, pc, obs.latitude, beam="per_tile", dipole_gains=gains)
+    v = torch.zeros((obs.freqs.size, obs.num_tiles, 8), dtype=torch.float32, device="cuda")
+    m.model_timestep_autos_with(obs.lsts[0], v)
+    torch.cuda.synchronize()
+    b, _ = oracle_tile_beam(oracle, sky, obs, obs.lsts[0], gains)
+    ref = oracle.model_autos(sky, obs.num_tiles, obs.freqs, obs.lsts[0], obs.latitude, beam=b)
+    assert_f32_close(v.cpu().numpy(), ref, ulps=4)

@@ -226,11 +226,52 @@ def test_full_mixed_config_chosen_form_vs_fp64_oracle(oracle, ctype, name):
     assert nrm < TOL and p999 < TOL, (nrm, p999, mx)
 
 
-def test_unsupported_tile_count_is_refused():
-    from mwa_hyperdrive_b200 import _lib
+@pytest.mark.parametrize("ntiles,npts", [(130, 200), (144, 300), (256, 150), (300, 64)])
+def test_more_than_128_tiles(oracle, ntiles, npts):
+    """Any tile count: the products run in blocks of 128 rows x 64 columns
+    (XX and YY only the blocks that hold a baseline p < q); every baseline is
+    written once through the planar epilogue."""
+    pc = (0.2, math.radians(-26.0))
+    obs = synth.Obs(synth.tiles_in_disk(ntiles, 1500.0, ntiles), 170e6 + np.arange(3) * 1.28e6, pc,
+                    np.array([0.25]))
+    sky = polarised_points(npts, pc, ntiles + 1)
+    got = run(sky, obs, obs.lsts[0], "tensor", beam="analytic")
+    ref, _ = oracle.model_timestep(sky, obs.tile_xyzs, obs.freqs, pc, obs.lsts[0], obs.latitude,
+                                   beam=oracle.beam_struct(1), out_f64=True)
+    nrm, p999, mx = errors(got, ref)
+    print(f"{ntiles} tiles: normwise {nrm:.2e}, p99.9 {p999:.2e}, max {mx:.2e}")
+    assert nrm < TOL and p999 < TOL, (nrm, p999, mx)
 
-    pc = (0.0, -0.5)
-    obs = synth.Obs(synth.tiles_in_disk(130, 1000.0, 1), np.array([150e6]), pc, np.array([0.0]))
-    sky = polarised_points(3, pc, 1)
-    with pytest.raises(_lib.HdcError):
-        SkyModeller(sky, obs.tile_xyzs, obs.freqs, pc, obs.latitude, form="tensor")
+
+@pytest.mark.parametrize("ntiles,npts", [(144, 200), (256, 120)])
+def test_per_tile_beams_tensor_form(oracle, ntiles, npts):
+    """Per-tile beams in the tensor form (block form over twice the
+    components) past 128 tiles, with Gaussians in the same sky (the direct
+    FP64 kernel with per-tile beams): against the oracle with the same
+    explicit per-tile Jones table, within 1e-6."""
+    pc = (0.2, math.radians(-26.0))
+    obs = synth.Obs(synth.tiles_in_disk(ntiles, 1500.0, ntiles + 3), 166.4e6 + np.arange(3) * 0.96e6, pc,
+                    np.array([0.3]))
+    sky = polarised_points(npts, pc, ntiles + 5)
+    comps = [sl.SourceComponent(float(sky.ra[k]), float(sky.dec[k]), sl.Point(),
+                                sl.PowerLaw(float(sky.si[k]), sl.FluxDensity(*sky.fds[sky.fd_start[k]])))
+             for k in range(npts) if sky.flux_type[k] == 1]
+    comps += synth.gaussians_and_shapelets(10, 0, pc, 6)
+    sky = sl.SkyModelArrays.from_components(comps)
+    rng = np.random.default_rng(ntiles)
+    gains = np.ones((ntiles, 2, 16))
+    for p in rng.choice(ntiles, ntiles // 4, replace=False):
+        gains[p, rng.integers(2), rng.integers(16)] = 0.0
+    m = SkyModeller(sky, obs.tile_xyzs, obs.freqs, pc, obs.latitude, beam="per_tile", dipole_gains=gains,
+                    form="tensor")
+    vis = torch.zeros((obs.freqs.size, obs.num_baselines, 8), dtype=torch.float64, device="cuda")
+    m.model_timestep_with(obs.lsts[0], vis)
+    torch.cuda.synchronize()
+    uniq, tmap, ufreqs, fmap = oracle.unique_tile_beams(gains, obs.freqs)
+    tabs = [oracle.tile_beam_table(sky, ty, obs.lsts[0], obs.latitude, uniq, ufreqs) if ty < 2 else None
+            for ty in range(3)]
+    ref, _ = oracle.model_timestep(sky, obs.tile_xyzs, obs.freqs, pc, obs.lsts[0], obs.latitude,
+                                   beam=oracle.beam_struct(2, tabs, tmap, fmap, ufreqs.size), out_f64=True)
+    nrm, p999, mx = errors(vis.cpu().numpy(), ref)
+    print(f"per-tile beams {ntiles} tiles, {len(uniq)} beams: normwise {nrm:.2e}, p99.9 {p999:.2e}, max {mx:.2e}")
+    assert nrm < TOL and p999 < TOL, (nrm, p999, mx)
