@@ -567,9 +567,9 @@ PEEL_WORKLOAD = ("peeling: 128 tiles (8128 baselines), 8 timesteps 8 s apart, 38
                  "convergence 1, no beam")
 
 
-def peel_workload(nch):
+def peel_workload(nch, sigma=2e-5):
     """Residual [8][nch][8128][8] float32 on the device, the 50 sources,
-    their positions and truths."""
+    their positions and truths (offsets N(0, sigma))."""
     import torch
 
     from mwa_hyperdrive_b200 import synth
@@ -592,7 +592,7 @@ def peel_workload(nch):
     for k in bright:
         sky = sl.SkyModelArrays.from_components([comps[k]])
         pos = (comps[k].ra, comps[k].dec)
-        tr = (float(rng.normal(0, 2e-5)), float(rng.normal(0, 2e-5)), float(rng.uniform(0.9, 1.1)))
+        tr = (float(rng.normal(0, sigma)), float(rng.normal(0, sigma)), float(rng.uniform(0.9, 1.1)))
         sources.append(sky)
         positions.append(pos)
         truths.append(tr)
@@ -625,26 +625,49 @@ def peel_arm(args):
     avg = float(np.median(obs.lsts))
     out = {"workload": PEEL_WORKLOAD, "metric": "peel s/timeblock (3 passes, 50 sources)", "unit": "s",
            "higher_is_better": False}
-    for name, batched in (("sequential", False), ("batched", True)):
-        times, consts = [], None
-        for rep in range(3):  # the first run also builds the models and (batched) autotunes
-            r = resid0.clone()
+    def run_arm(resid_in, truths_, batched, batch_size=0, reps=3):
+        times, consts, r = [], None, None
+        for rep in range(reps):  # the first run also builds the models and (batched) autotunes
+            r = resid_in.clone()
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             consts = P.peel_timeblock(r, weights, obs.freqs, obs.tile_xyzs, obs.lsts, avg, obs.phase_centre, sources,
                                       positions, [P.IonoConsts() for _ in sources], 3, 10, 1.0, 16,
-                                      obs.latitude, "none", batched=batched)
+                                      obs.latitude, "none", batched=batched, batch_size=batch_size)
             torch.cuda.synchronize()
             times.append(time.perf_counter() - t0)
-        err_a = max(abs(c.alpha - t[0]) for c, t in zip(consts, truths))
-        err_g = max(abs(c.gain - t[2]) for c, t in zip(consts, truths))
-        out[name] = {"s_per_timeblock": min(times), "first_call_s": times[0],
-                     "residual_rms_ratio": float(r.norm() / resid0.norm()),
-                     "max_alpha_err": err_a, "max_gain_err": err_g}
-        if batched:
-            bx, sy, ms = P.batched_tuning()
-            out[name]["autotuned_accumulate_cta"] = {"bins": bx, "sources": sy, "ms": ms}
+        err_a = [abs(c.alpha - t[0]) for c, t in zip(consts, truths_)]
+        err_g = [abs(c.gain - t[2]) for c, t in zip(consts, truths_)]
+        # a source is captured when its fitted offset is within 10 % of the
+        # injected one (or 1e-7) and its gain within 1e-3
+        cap = sum(1 for c, t in zip(consts, truths_)
+                  if abs(c.alpha - t[0]) < 0.1 * abs(t[0]) + 1e-7 and abs(c.beta - t[1]) < 0.1 * abs(t[1]) + 1e-7
+                  and abs(c.gain - t[2]) < 1e-3)
+        return {"s_per_timeblock": min(times), "first_call_s": times[0],
+                "residual_rms_ratio": float(r.norm() / resid_in.norm()),
+                "max_alpha_err": max(err_a), "max_gain_err": max(err_g), "captured": cap, "sources": len(truths_)}
+
+    out["sequential"] = run_arm(resid0, truths, False)
+    out["batched"] = run_arm(resid0, truths, True)
+    bx, sy, ms = P.batched_tuning()
+    out["batched"]["autotuned_accumulate_cta"] = {"bins": bx, "sources": sy, "ms": ms}
+    # sub-batches of 10 in the list's (brightness) order: Jacobi within, the
+    # reference's Gauss-Seidel order between them
+    out["batched_sub10"] = run_arm(resid0, truths, True, 10)
     out["speedup_batched_vs_sequential"] = out["sequential"]["s_per_timeblock"] / out["batched"]["s_per_timeblock"]
+    out["speedup_batched_sub10_vs_sequential"] = (out["sequential"]["s_per_timeblock"] /
+                                                  out["batched_sub10"]["s_per_timeblock"])
+    # the stated offsets, N(0, 2e-4): the reference's linearised fit does not
+    # capture every draw on this array (tests/test_iono_capture.py); count
+    # the captured sources of each arm (one timed run each)
+    # (same seed: the same sources and positions, other offset draws)
+    _, resid2, _, _, truths2 = peel_workload(nch, 2e-4)
+    del resid0
+    torch.cuda.empty_cache()
+    out["stated_offsets_2e-4"] = {"sequential": run_arm(resid2, truths2, False, reps=1),
+                                  "batched": run_arm(resid2, truths2, True, reps=1),
+                                  "batched_sub10": run_arm(resid2, truths2, True, 10, reps=1)}
+    del resid2
     if not args.no_cpu_baseline:
         # the reference's CPU peel loop (oracle restatement of peel_cpu,
         # params/peel/mod.rs:1121-1475, its rayon loops over timesteps as
@@ -658,7 +681,7 @@ def peel_arm(args):
         threads = os.cpu_count() or 1
         orc.set_num_threads(threads)
         ns, nchs = 4, 32
-        r_h = resid0[:, :nchs].cpu().numpy()
+        r_h = peel_workload(nchs)[1].cpu().numpy()
         w_h = np.ones(r_h.shape[:3], np.float32)
         t0 = time.perf_counter()
         orc.peel_cpu(r_h, w_h, obs.freqs[:nchs], obs.tile_xyzs, obs.lsts, avg, obs.phase_centre, sources[:ns],
@@ -670,7 +693,7 @@ def peel_arm(args):
                                          f"in {dt:.2f} s, scaled by {scale:.0f}"}
         out["speedup_batched_vs_cpu"] = out["cpu_baseline"]["value"] / out["batched"]["s_per_timeblock"]
         out["speedup_sequential_vs_cpu"] = out["cpu_baseline"]["value"] / out["sequential"]["s_per_timeblock"]
-    nvis = int(np.prod(resid0.shape[:3]))
+    nvis = int(np.prod(weights.shape))
     out["algorithmic"] = {"hi_res_vis": nvis, "hi_res_bytes": nvis * 32,
                           "batched_hi_res_bytes_per_pass": "residual read + read/write, weights, 50 model reads x 2"}
     return out

@@ -551,6 +551,7 @@ typedef struct HdcPeelParams {
     int freq_average_factor; /* high-res channels per low-res channel */
     int beam_kind;           /* HDC_BEAM_* for the per-source models */
     double array_latitude_rad;
+    int batch_size;          /* batched form: sources per sub-batch in list order (0: all in one) */
 } HdcPeelParams;
 
 /* peel_gpu (params/peel/gpu.rs:25-757): peel num_sources sources from the
@@ -568,13 +569,16 @@ int hdc_peel_timeblock(JonesF32 *d_resid_tfb, const float *d_weights_tfb, int nu
 
 /* The same timeblock peeled with every source's fit of a pass batched
  * (this project's chosen form; no counterpart in the reference): one
- * accumulation sweep over the high-resolution residual for all sources, all
- * iono fits in one launch per iteration, one sweep applying every source's
- * update.  Sources fitted in the same pass see the residual as it was at the
- * start of the pass (Jacobi) instead of each other's updates (the reference's
- * Gauss-Seidel order); with one source the two coincide.  Needs num_sources
- * x (timesteps x channels x baselines) JonesF32 of device memory for the
- * source models. */
+ * accumulation sweep over the high-resolution residual for all sources of a
+ * sub-batch, all their iono fits in one launch per iteration, one sweep
+ * applying their updates.  Sources of one sub-batch see the residual as it
+ * was when the sub-batch started (Jacobi) instead of each other's updates;
+ * sub-batches follow one another in list order (the reference's
+ * Gauss-Seidel order between them; params->batch_size sources each, 0 for
+ * one sub-batch of all).  With one source, or sub-batches of one, this is
+ * the reference's sequence.  Needs num_sources x (timesteps x channels x
+ * baselines) JonesF32 of device memory for the source models unless every
+ * source is one point at its own position. */
 int hdc_peel_timeblock_batched(JonesF32 *d_resid_tfb, const float *d_weights_tfb, int num_timesteps, int num_freqs,
                                const double *h_freqs, const XYZ *h_tile_xyzs, int num_tiles, const double *h_lmsts,
                                double average_lmst, RADec phase_centre, int num_sources, const HdcSkyModel *h_sources,

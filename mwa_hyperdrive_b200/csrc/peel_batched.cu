@@ -533,48 +533,67 @@ extern "C" int hdc_peel_timeblock_batched(JonesF32* d_resid_tfb, const float* d_
     A.ntiles = num_tiles;
     A.nsrc = ns;
     A.favg = favg;
-    const size_t nbins = (size_t)nlo * nbl;
     std::vector<IonoConsts> fit(ns), next(ns);
+    // sources in sub-batches of `batch` in list order: within a sub-batch the
+    // fits share the residual (Jacobi); each sub-batch sees the residual the
+    // earlier ones left (the reference's Gauss-Seidel order between them)
+    const int batch = params->batch_size > 0 ? std::min(params->batch_size, ns) : ns;
     for (int pass = 0; pass < params->num_passes; pass++) {
-        PB_CK(cudaMemcpyAsync(b_old.p, h_iono_consts, sizeof(IonoConsts) * ns, cudaMemcpyHostToDevice, s));
-        const unsigned tgrid = (unsigned)((ntab + 255) / 256);
-        pb::iono_table_kernel<<<tgrid, 256, 0, s>>>(b_tuvw.as<UVW>(), b_lam.as<double>(), b_old.as<IonoConsts>(),
-                                                    nullptr, ns, nt, nf, num_tiles, b_io.as<float2>());
-        count_launches(1);
-        PB_CK(cudaGetLastError());
-        const int v = pb::choose_variant(A, s);
-        pb::kVariants[v].launch(A, s);
-        PB_CK(cudaGetLastError());
-        for (int i = 0; i < ns; i++) fit[i] = IonoConsts{0.0, 0.0, 1.0};
-        const char* err = iono_loop_batched_on(b_dlo.as<JonesF32>(), b_wlo.as<float>(), b_mlo.as<JonesF32>(),
-                                               b_mlo_rot.as<JonesF32>(), b_scr.p, fit.data(), ns, nbl, nlo,
-                                               params->num_loops, b_uv_lo.as<UVW>(), b_lam_lo.as<double>(),
-                                               params->convergence, s);
-        if (err) {
-            set_error("hdc_peel_timeblock_batched: %s", err);
-            return HDC_ERR_CUDA;
+        for (int b0 = 0; b0 < ns; b0 += batch) {
+            const int nb = std::min(batch, ns - b0);
+            const size_t tab0 = (size_t)b0 * nt * nf * num_tiles, ntab_b = (size_t)nb * nt * nf * num_tiles;
+            pb::SweepArgs B = A;
+            B.nsrc = nb;
+            B.models = A.models ? A.models + (size_t)b0 * nvis : nullptr;
+            B.ptab = A.ptab ? A.ptab + (size_t)b0 * nt * nf : nullptr;
+            B.rot = A.rot + tab0;
+            B.io_old = A.io_old + tab0;
+            B.ap_old = A.ap_old + tab0;
+            B.ap_new = A.ap_new + tab0;
+            B.old = A.old + b0;
+            B.neu = A.neu + b0;
+            const UVW* tuvw_b = b_tuvw.as<UVW>() + (size_t)b0 * nt * num_tiles;
+            PB_CK(cudaMemcpyAsync(b_old.as<IonoConsts>() + b0, h_iono_consts + b0, sizeof(IonoConsts) * nb,
+                                  cudaMemcpyHostToDevice, s));
+            const unsigned tgrid = (unsigned)((ntab_b + 255) / 256);
+            pb::iono_table_kernel<<<tgrid, 256, 0, s>>>(tuvw_b, b_lam.as<double>(), B.old, nullptr, nb, nt, nf,
+                                                        num_tiles, b_io.as<float2>() + tab0);
+            count_launches(1);
+            PB_CK(cudaGetLastError());
+            const int v = pb::choose_variant(B, s);
+            pb::kVariants[v].launch(B, s);
+            PB_CK(cudaGetLastError());
+            for (int i = 0; i < nb; i++) fit[i] = IonoConsts{0.0, 0.0, 1.0};
+            const char* err = iono_loop_batched_on(b_dlo.as<JonesF32>(), b_wlo.as<float>(), b_mlo.as<JonesF32>(),
+                                                   b_mlo_rot.as<JonesF32>(), b_scr.p, fit.data(), nb, nbl, nlo,
+                                                   params->num_loops, b_uv_lo.as<UVW>() + (size_t)b0 * nbl,
+                                                   b_lam_lo.as<double>(), params->convergence, s);
+            if (err) {
+                set_error("hdc_peel_timeblock_batched: %s", err);
+                return HDC_ERR_CUDA;
+            }
+            for (int i = 0; i < nb; i++) {
+                const IonoConsts old = h_iono_consts[b0 + i];
+                IonoConsts c = {old.alpha + fit[i].alpha, old.beta + fit[i].beta, old.gain * fit[i].gain};
+                // the reference's revert rule (gpu.rs:541-627)
+                if (std::fabs(c.alpha) > 1e-3 || std::fabs(c.beta) > 1e-3 || c.gain < 0.0 || c.gain > 1.5) c = old;
+                next[b0 + i] = c;
+            }
+            PB_CK(cudaMemcpyAsync(b_new.as<IonoConsts>() + b0, next.data() + b0, sizeof(IonoConsts) * nb,
+                                  cudaMemcpyHostToDevice, s));
+            pb::iono_table_kernel<<<tgrid, 256, 0, s>>>(tuvw_b, b_lam.as<double>(), B.old, B.rot, nb, nt, nf,
+                                                        num_tiles, b_apo.as<float2>() + tab0);
+            pb::iono_table_kernel<<<tgrid, 256, 0, s>>>(tuvw_b, b_lam.as<double>(), B.neu, B.rot, nb, nt, nf,
+                                                        num_tiles, b_apn.as<float2>() + tab0);
+            count_launches(2);
+            PB_CK(cudaGetLastError());
+            pb::apply_kernel<<<(unsigned)((nvis + 255) / 256), 256, 0, s>>>(d_resid_tfb, B);
+            count_launches(1);
+            PB_CK(cudaGetLastError());
+            PB_CK(cudaStreamSynchronize(s));  // `next` is read by the copy above
+            for (int i = 0; i < nb; i++) h_iono_consts[b0 + i] = next[b0 + i];
         }
-        for (int i = 0; i < ns; i++) {
-            const IonoConsts old = h_iono_consts[i];
-            IonoConsts c = {old.alpha + fit[i].alpha, old.beta + fit[i].beta, old.gain * fit[i].gain};
-            // the reference's revert rule (gpu.rs:541-627)
-            if (std::fabs(c.alpha) > 1e-3 || std::fabs(c.beta) > 1e-3 || c.gain < 0.0 || c.gain > 1.5) c = old;
-            next[i] = c;
-        }
-        PB_CK(cudaMemcpyAsync(b_new.p, next.data(), sizeof(IonoConsts) * ns, cudaMemcpyHostToDevice, s));
-        pb::iono_table_kernel<<<tgrid, 256, 0, s>>>(b_tuvw.as<UVW>(), b_lam.as<double>(), b_old.as<IonoConsts>(),
-                                                    b_rot.as<float2>(), ns, nt, nf, num_tiles, b_apo.as<float2>());
-        pb::iono_table_kernel<<<tgrid, 256, 0, s>>>(b_tuvw.as<UVW>(), b_lam.as<double>(), b_new.as<IonoConsts>(),
-                                                    b_rot.as<float2>(), ns, nt, nf, num_tiles, b_apn.as<float2>());
-        count_launches(2);
-        PB_CK(cudaGetLastError());
-        pb::apply_kernel<<<(unsigned)((nvis + 255) / 256), 256, 0, s>>>(d_resid_tfb, A);
-        count_launches(1);
-        PB_CK(cudaGetLastError());
-        PB_CK(cudaStreamSynchronize(s));  // `next` is read by the copy above
-        for (int i = 0; i < ns; i++) h_iono_consts[i] = next[i];
     }
-    (void)nbins;
     PB_CK(cudaStreamSynchronize(s));
     return HDC_OK;
 }

@@ -321,3 +321,43 @@ def test_batched_peel_recovers_injected_iono(oracle):
         # Jacobi and Gauss-Seidel agree once the passes have converged
         assert abs(g.alpha - s_.alpha) < 0.01 * abs(s_.alpha) + 1e-7, (g, s_)
     assert after < 0.05 * before, (after, before)
+
+
+def test_batched_peel_in_sub_batches_of_one_is_the_sequential_order(oracle):
+    """Sub-batches of one source each run the reference's Gauss-Seidel order
+    (each source fitted against the residual its predecessors left): several
+    sources then give the sequential loop's constants up to rounding."""
+    rng, pc, xyzs, freqs, lmsts, lam, nbl, sources, positions, truths = make_peel_problem(seed=9, ntiles=24, nf=8,
+                                                                                           nsrc=3, points=True)
+    resid = simulate_residual(oracle, pc, xyzs, freqs, lmsts, lam, sources, positions, truths)
+    weights = np.ones(resid.shape[:3], np.float32)
+    avg_lmst = float(np.median(lmsts))
+    out = {}
+    for batched, bs in ((False, 0), (True, 1)):
+        d_resid = dev(resid, np.float32)
+        out[batched] = P.peel_timeblock(d_resid, dev(weights, np.float32), freqs, xyzs, lmsts, avg_lmst, pc, sources,
+                                        positions, [P.IonoConsts() for _ in sources], num_passes=2, num_loops=5,
+                                        convergence=1.0, freq_average_factor=4, array_latitude_rad=synth.MWA_LAT_RAD,
+                                        batched=batched, batch_size=bs)
+    for cb, cs in zip(out[True], out[False]):
+        assert abs(cb.alpha - cs.alpha) <= 1e-5 * abs(cs.alpha) + 1e-12, (cb, cs)
+        assert abs(cb.beta - cs.beta) <= 1e-5 * abs(cs.beta) + 1e-12, (cb, cs)
+        assert abs(cb.gain - cs.gain) <= 1e-6, (cb, cs)
+
+
+def test_batched_peel_sub_batches_recover_injected_iono(oracle):
+    """Sub-batches of two of six sources: every source recovered as in the
+    sequential loop."""
+    rng, pc, xyzs, freqs, lmsts, lam, nbl, sources, positions, truths = make_peel_problem(seed=11, ntiles=32, nf=16,
+                                                                                           nsrc=6, points=True)
+    resid = simulate_residual(oracle, pc, xyzs, freqs, lmsts, lam, sources, positions, truths)
+    weights = np.ones(resid.shape[:3], np.float32)
+    d_resid = dev(resid, np.float32)
+    got = P.peel_timeblock(d_resid, dev(weights, np.float32), freqs, xyzs, lmsts, float(np.median(lmsts)), pc,
+                           sources, positions, [P.IonoConsts() for _ in sources], num_passes=3, num_loops=10,
+                           convergence=1.0, freq_average_factor=4, array_latitude_rad=synth.MWA_LAT_RAD,
+                           batched=True, batch_size=2)
+    for g, tr in zip(got, truths):
+        assert abs(g.alpha - tr[0]) < 0.02 * abs(tr[0]) + 2e-7, (g, tr)
+        assert abs(g.gain - tr[2]) < 5e-3, (g, tr)
+    assert np.linalg.norm(d_resid.cpu().numpy()) < 0.05 * np.linalg.norm(resid)
