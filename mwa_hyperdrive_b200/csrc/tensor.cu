@@ -368,6 +368,18 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const __grid_consta
         const bool ysep = ry != 0 && ry != 1;
         const int prow[2] = {NT * rb + r0, NT * rb + r0 + 64};
         const int qcol = NH * cb + r0;
+        // The upper 64 rows of the block pair with no column of it when they
+        // lie beyond the array, or in an XX / YY block whose columns all lie
+        // below them: their X planes stay zero and are not produced.  (Then
+        // the Y tile is never one of them: ry != 1.)
+        const bool skip_hi = NT * rb + 64 >= n || (pol < 2 && NT * rb + 64 >= NH * cb + NH - 1);
+        if (skip_hi) {
+            for (int st = 0; st < NSTAGE; st++)
+                for (int tile = 0; tile < 2 * C::XDIG; tile++) {
+                    uint4* z = reinterpret_cast<uint4*>(smem + st * L::STAGE_BYTES + tile * XT_BYTES + XT_BYTES / 2);
+                    for (int i = tid; i < XT_BYTES / 32; i += NPT) z[i] = make_uint4(0u, 0u, 0u, 0u);
+                }
+        }
         const double oq = 4.0 * freq / VEL_C;
         double u[3], v[3], w[3];  // quarter-turns per unit l, m, n - 1 of the two X rows and the Y tile
         tile_uvw(P, prow[0], oq, u[0], v[0], w[0]);
@@ -439,6 +451,7 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const __grid_consta
                     float snq = 0.f, csq = 0.f;
 #pragma unroll
                     for (int s2 = 0; s2 < 2; s2++) {
+                        if (s2 == 1 && skip_hi) continue;
                         float sn, cs;
                         phasor_quarter_f32(u[s2] * cl[j] + v[s2] * cm[j] + w[s2] * cn[j], sn, cs);
                         const float Xr = fmaf(wr[j], cs, -wi[j] * sn);
@@ -467,6 +480,7 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const __grid_consta
                     float snq = 0.f, csq = 0.f;
 #pragma unroll
                     for (int s2 = 0; s2 < 2; s2++) {
+                        if (s2 == 1 && skip_hi) continue;
                         float sn, cs;
                         phasor_quarter_f32(u[s2] * cl + v[s2] * cm + w[s2] * cn, sn, cs);
                         if (s2 == ry) snq = sn, csq = cs;
@@ -507,6 +521,7 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const __grid_consta
             // x planes: bytes 0-2 excess-128 lower digits, byte 3 the signed top digit
 #pragma unroll
             for (int s2 = 0; s2 < 2; s2++) {
+                if (s2 == 1 && skip_hi) continue;
                 const uint32_t xo = chunk_off(r0 + 64 * s2, kq) + quad * 4;
 #pragma unroll
                 for (int part = 0; part < 2; part++) {
