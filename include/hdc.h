@@ -182,10 +182,10 @@ const char *model_points(const Points *comps, const Addresses *a, const UVW *d_u
  * 64 B per component + 64 B per (channel, component), each of its three
  * tables rounded up to 256 B (LMN 32 B and envelope 32 B per component, flux
  * 64 B per channel and component), and larger problems are rejected with an
- * error.  Kernel errors are read back and cleared as in model_points.  Every call on a device shares that array, so
- * calls whose kernels overlap on the GPU race and must be serialised.  The
- * first call on a device looks up the array's device address and should come
- * before any stream capture. */
+ * error.  Kernel errors are read back and cleared as in model_points.  Every
+ * call on a device shares that array, so calls whose kernels overlap on the
+ * GPU race and must be serialised.  The first call on a device looks up the
+ * array's device address and should come before any stream capture. */
 #define HDC_NOALLOC_SCRATCH_BYTES (16u * 1024u * 1024u)
 const char *model_points_noalloc(const Points *comps, const Addresses *a, const UVW *d_uvws,
                                  const JonesF64 *d_beam_jones, JonesF32 *d_vis_fb);
@@ -470,6 +470,20 @@ int hdc_calibrate_timeblock(const JonesF32 *d_data_tfb, const JonesF32 *d_model_
                             JonesF64 *d_di_jones, int max_iterations, double stop_threshold, double min_threshold,
                             int pols, HdcCalResult *h_results, int form, hdcStream_t stream);
 
+/* One pass of calibrate_timeblock without its retry of failed chanblocks:
+ * every chanblock when h_chanblock_list is NULL, else only the num_listed
+ * chanblocks it names (from their starts in d_di_jones; only their entries
+ * of h_results are written).  The building block of a calibration whose
+ * chanblocks are spread over several GPUs (mwa_hyperdrive_b200/shard.py):
+ * each rank runs its chanblocks' first pass, the ranks exchange results,
+ * and each re-runs its failed chanblocks from the neighbour-interpolated
+ * starts (di_calibrate/mod.rs:473-614) formed over the whole band. */
+int hdc_calibrate_chanblocks(const JonesF32 *d_data_tfb, const JonesF32 *d_model_tfb, int num_timesteps,
+                             int timeblock_start, int timeblock_end, int num_chanblocks, int num_baselines,
+                             JonesF64 *d_di_jones, int max_iterations, double stop_threshold, double min_threshold,
+                             int pols, const int *h_chanblock_list, int num_listed, HdcCalResult *h_results, int form,
+                             hdcStream_t stream);
+
 /* All timeblocks (calibrate_timeblocks, di_calibrate/mod.rs:272-361): every
  * timeblock k = [h_timeblock_bounds[2k], h_timeblock_bounds[2k+1]) starts
  * from identity; the first pass of all timeblocks runs as one CUDA graph
@@ -586,8 +600,9 @@ int hdc_peel_timeblock_batched(JonesF32 *d_resid_tfb, const float *d_weights_tfb
                                hdcStream_t stream);
 
 /* The accumulation-sweep launch shape the batched peel's autotuner chose for
- * the last new problem shape (low-resolution bins and sources per CTA) and
- * its measured time. */
+ * the last new problem shape (low-resolution bins and sources per CTA;
+ * sources 0: the variant staging 16 baselines' residual in shared memory for
+ * every source) and its measured time. */
 int hdc_peel_batched_tuning(int *block_bins, int *block_sources, float *ms);
 
 /* ---- Visibility preparation before DI calibration ---------------------- */

@@ -129,6 +129,9 @@ SIGNATURES = {
     "hdc_modeller_model_timestep_autos_with": (c_int, [c_void_p, c_double, c_void_p, c_void_p]),
     "hdc_calibrate_timeblock": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p, c_int,
                                         c_double, c_double, c_int, ctypes.POINTER(HdcCalResult), c_int, c_void_p]),
+    "hdc_calibrate_chanblocks": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p, c_int,
+                                         c_double, c_double, c_int, c_void_p, c_int, ctypes.POINTER(HdcCalResult),
+                                         c_int, c_void_p]),
     "hdc_calibrate_timeblocks": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_int, c_int, c_int, c_void_p, c_int,
                                          c_double, c_double, c_int, ctypes.POINTER(HdcCalResult), c_int, c_void_p]),
     "hdc_peel_timeblock": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p, c_int, c_void_p, c_double,

@@ -968,12 +968,14 @@ static int retry_failed(CalParams P, int form, std::vector<HdcCalResult>& res, i
 
 using namespace hdc;
 
-extern "C" int hdc_calibrate_timeblock(const JonesF32* d_data_tfb, const JonesF32* d_model_tfb, int num_timesteps,
-                                       int timeblock_start, int timeblock_end, int num_chanblocks, int num_baselines,
-                                       JonesF64* d_di_jones, int max_iterations, double stop_threshold,
-                                       double min_threshold, int pols, HdcCalResult* h_results, int form,
-                                       hdcStream_t stream) {
-    cudaStream_t s = (cudaStream_t)stream;
+// calibrate_timeblock's body: the first pass over every chanblock (or over
+// the listed ones, whose results alone are written), then -- with `retry` --
+// the retry of failed chanblocks from interpolated neighbours.
+static int calibrate_timeblock_impl(const JonesF32* d_data_tfb, const JonesF32* d_model_tfb, int num_timesteps,
+                                    int timeblock_start, int timeblock_end, int num_chanblocks, int num_baselines,
+                                    JonesF64* d_di_jones, int max_iterations, double stop_threshold,
+                                    double min_threshold, int pols, HdcCalResult* h_results, int form, bool retry,
+                                    const int* h_list, int num_listed, cudaStream_t s) {
     const int ntiles = (int)((1.0 + std::sqrt(1.0 + 8.0 * num_baselines)) / 2.0 + 0.5);
     if (ntiles * (ntiles - 1) / 2 != num_baselines || ntiles > CT || num_chanblocks <= 0 ||
         timeblock_start < 0 || timeblock_end > num_timesteps || timeblock_start >= timeblock_end || !h_results ||
@@ -1038,7 +1040,28 @@ extern "C" int hdc_calibrate_timeblock(const JonesF32* d_data_tfb, const JonesF3
             return HDC_ERR_CUDA;
         }
     }
-    rc = launch_mitchcal(P, form, num_chanblocks, s);
+    int nblocks = num_chanblocks;
+    if (h_list) {
+        for (int k = 0; k < num_listed; k++)
+            if (h_list[k] < 0 || h_list[k] >= num_chanblocks) {
+                cleanup();
+                set_error("hdc_calibrate_chanblocks: chanblock %d of the list is outside 0..%d", h_list[k],
+                          num_chanblocks - 1);
+                return HDC_ERR_ARG;
+            }
+        if (num_listed == 0) {
+            cleanup();
+            return HDC_OK;
+        }
+        if (cudaMemcpyAsync(d_list, h_list, sizeof(int) * num_listed, cudaMemcpyHostToDevice, s) != cudaSuccess) {
+            cleanup();
+            set_error("hdc_calibrate_chanblocks: %s", cudaGetErrorString(cudaGetLastError()));
+            return HDC_ERR_CUDA;
+        }
+        P.chan_list = d_list;
+        nblocks = num_listed;
+    }
+    rc = launch_mitchcal(P, form, nblocks, s);
     if (rc) {
         cleanup();
         return rc;
@@ -1056,14 +1079,50 @@ extern "C" int hdc_calibrate_timeblock(const JonesF32* d_data_tfb, const JonesF3
         set_error("hdc_calibrate_timeblock: a covariance copy did not arrive in time");
         return HDC_ERR_TIMEOUT;
     }
-    rc = retry_failed(P, form, res, d_list, d_pairs, s);
-    if (rc) {
-        cleanup();
-        return rc;
+    if (retry) {
+        rc = retry_failed(P, form, res, d_list, d_pairs, s);
+        if (rc) {
+            cleanup();
+            return rc;
+        }
     }
-    for (int c = 0; c < num_chanblocks; c++) h_results[c] = res[c];
+    if (h_list) {
+        for (int k = 0; k < num_listed; k++) {
+            HdcCalResult r = res[h_list[k]];
+            if (std::fabs(r.max_precision) > 1e100) r.max_precision = NAN;
+            h_results[h_list[k]] = r;
+        }
+    } else {
+        for (int c = 0; c < num_chanblocks; c++) h_results[c] = res[c];
+    }
     cleanup();
     return HDC_OK;
+}
+
+extern "C" int hdc_calibrate_timeblock(const JonesF32* d_data_tfb, const JonesF32* d_model_tfb, int num_timesteps,
+                                       int timeblock_start, int timeblock_end, int num_chanblocks, int num_baselines,
+                                       JonesF64* d_di_jones, int max_iterations, double stop_threshold,
+                                       double min_threshold, int pols, HdcCalResult* h_results, int form,
+                                       hdcStream_t stream) {
+    return calibrate_timeblock_impl(d_data_tfb, d_model_tfb, num_timesteps, timeblock_start, timeblock_end,
+                                    num_chanblocks, num_baselines, d_di_jones, max_iterations, stop_threshold,
+                                    min_threshold, pols, h_results, form, true, nullptr, 0, (cudaStream_t)stream);
+}
+
+extern "C" int hdc_calibrate_chanblocks(const JonesF32* d_data_tfb, const JonesF32* d_model_tfb, int num_timesteps,
+                                        int timeblock_start, int timeblock_end, int num_chanblocks,
+                                        int num_baselines, JonesF64* d_di_jones, int max_iterations,
+                                        double stop_threshold, double min_threshold, int pols,
+                                        const int* h_chanblock_list, int num_listed, HdcCalResult* h_results,
+                                        int form, hdcStream_t stream) {
+    if (h_chanblock_list == nullptr && num_listed != 0) {
+        set_error("hdc_calibrate_chanblocks: a count without a list");
+        return HDC_ERR_ARG;
+    }
+    return calibrate_timeblock_impl(d_data_tfb, d_model_tfb, num_timesteps, timeblock_start, timeblock_end,
+                                    num_chanblocks, num_baselines, d_di_jones, max_iterations, stop_threshold,
+                                    min_threshold, pols, h_results, form, false, h_chanblock_list, num_listed,
+                                    (cudaStream_t)stream);
 }
 
 // All timeblocks of an observation (calibrate_timeblocks, mod.rs:272-361):

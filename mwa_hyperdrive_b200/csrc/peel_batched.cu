@@ -260,6 +260,86 @@ __global__ void point_table_kernel(const JonesF64* __restrict__ W, int ns, int n
                                                      (float)w.j10_re, (float)w.j10_im, (float)w.j11_re, (float)w.j11_im};
 }
 
+// The same sums with the residual staged in shared memory: a CTA takes SB
+// consecutive baselines of one low-resolution channel, loads their
+// nt x favg samples of residual and weight once (coalesced), and its 256
+// threads (SB baselines x 256 / SB source lanes) then run every source of the
+// pass over them, so the residual crosses L2 once per pass instead of once per
+// source.  Shared memory: samples x SB x 36 bytes.
+constexpr int SB = 16;
+__global__ void __launch_bounds__(256) accumulate_staged_kernel(const SweepArgs A) {
+    extern __shared__ float4 st_smem[];
+    const int nlo = A.nf / A.favg, ns_samp = A.nt * A.favg;
+    const int nbb = (A.nbl + SB - 1) / SB;
+    const int flo = (int)(blockIdx.x / nbb), bl0 = (int)(blockIdx.x % nbb) * SB;
+    float4* R = st_smem;                                          // [sample][SB][2]
+    float* W = reinterpret_cast<float*>(st_smem + (size_t)ns_samp * SB * 2);  // [sample][SB]
+    for (int i = threadIdx.x; i < ns_samp * SB * 2; i += blockDim.x) {
+        const int h = i & 1, b = (i >> 1) % SB, k = (i >> 1) / SB;
+        const int t = k / A.favg, fc = flo * A.favg + k % A.favg, bl = bl0 + b;
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (bl < A.nbl) v = reinterpret_cast<const float4*>(A.resid + ((size_t)t * A.nf + fc) * A.nbl + bl)[h];
+        R[i] = v;
+    }
+    for (int i = threadIdx.x; i < ns_samp * SB; i += blockDim.x) {
+        const int b = i % SB, k = i / SB;
+        const int t = k / A.favg, fc = flo * A.favg + k % A.favg, bl = bl0 + b;
+        W[i] = bl < A.nbl ? A.w[((size_t)t * A.nf + fc) * A.nbl + bl] : 0.f;
+    }
+    __syncthreads();
+    const int b = threadIdx.x % SB, lanes = blockDim.x / SB;
+    const int bl = bl0 + b;
+    if (bl >= A.nbl) return;
+    int tp, tq;
+    baseline_to_tiles(bl, A.ntiles, tp, tq);
+    const size_t nvis = (size_t)A.nt * A.nf * A.nbl;
+    for (int src = threadIdx.x / SB; src < A.nsrc; src += lanes) {
+        const float g = (float)A.old[src].gain;
+        const JonesF32* M = A.ptab ? nullptr : A.models + (size_t)src * nvis;
+        float2 sd[4] = {}, sm[4] = {};
+        float sw = 0.f;
+        for (int k = 0; k < ns_samp; k++) {
+            const int t = k / A.favg, fc = flo * A.favg + k % A.favg;
+            const float wt = W[k * SB + b];
+            const size_t tb = (((size_t)src * A.nt + t) * A.nf + fc) * A.ntiles;
+            const float2 rot = cmulcf(A.rot[tb + tp], A.rot[tb + tq]);
+            const float2 io1 = cmulcf(A.io_old[tb + tp], A.io_old[tb + tq]);
+            const float2 io = make_float2(io1.x * g, io1.y * g);
+            const JF mj = load_jf(A.ptab ? A.ptab[((size_t)src * A.nt + t) * A.nf + fc]
+                                         : M[((size_t)t * A.nf + fc) * A.nbl + bl]);
+            const float4 r0 = R[(k * SB + b) * 2], r1 = R[(k * SB + b) * 2 + 1];
+            const JF r = {{make_float2(r0.x, r0.y), make_float2(r0.z, r0.w), make_float2(r1.x, r1.y),
+                           make_float2(r1.z, r1.w)}};
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                const float2 m = cmulf(mj.v[e], io);
+                const float2 d = cmulf(r.v[e], rot);
+                sd[e].x = fmaf(d.x + m.x, wt, sd[e].x);
+                sd[e].y = fmaf(d.y + m.y, wt, sd[e].y);
+                sm[e].x = fmaf(m.x, wt, sm[e].x);
+                sm[e].y = fmaf(m.y, wt, sm[e].y);
+            }
+            sw += wt;
+        }
+        const double inv = 1.0 / ((double)sw > 0.0 ? (double)sw : 1.0);
+        const size_t o = ((size_t)src * nlo + flo) * A.nbl + bl;
+        A.d_lo[o] = JonesF32{(float)(sd[0].x * inv), (float)(sd[0].y * inv), (float)(sd[1].x * inv),
+                             (float)(sd[1].y * inv), (float)(sd[2].x * inv), (float)(sd[2].y * inv),
+                             (float)(sd[3].x * inv), (float)(sd[3].y * inv)};
+        A.m_lo[o] = JonesF32{(float)(sm[0].x * inv), (float)(sm[0].y * inv), (float)(sm[1].x * inv),
+                             (float)(sm[1].y * inv), (float)(sm[2].x * inv), (float)(sm[2].y * inv),
+                             (float)(sm[3].x * inv), (float)(sm[3].y * inv)};
+    }
+}
+
+size_t staged_smem_bytes(const SweepArgs& A) { return (size_t)A.nt * A.favg * SB * 36; }
+
+void launch_staged(const SweepArgs& A, cudaStream_t s) {
+    const unsigned grid = (unsigned)((A.nf / A.favg) * ((A.nbl + SB - 1) / SB));
+    accumulate_staged_kernel<<<grid, 256, staged_smem_bytes(A), s>>>(A);
+    count_launches(1);
+}
+
 struct Variant {
     int bx, sy;
     void (*launch)(const SweepArgs&, cudaStream_t);
@@ -273,9 +353,15 @@ void launch_acc(const SweepArgs& A, cudaStream_t s) {
     count_launches(1);
 }
 
-const Variant kVariants[] = {
-    {256, 1, launch_acc<256, 1>}, {128, 2, launch_acc<128, 2>}, {64, 4, launch_acc<64, 4>}, {32, 8, launch_acc<32, 8>}};
+// the last variant (bins 0 in the report: one CTA per SB baselines, every
+// source) stages the residual; it runs only when its shared memory fits
+const Variant kVariants[] = {{256, 1, launch_acc<256, 1>},
+                             {128, 2, launch_acc<128, 2>},
+                             {64, 4, launch_acc<64, 4>},
+                             {32, 8, launch_acc<32, 8>},
+                             {SB, 0, launch_staged}};
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
+constexpr size_t kStagedSmemMax = 200 * 1024;
 
 std::mutex g_tune_mu;
 std::map<std::tuple<int, int, int, int, int>, int> g_tuned;  // (nt, nf, nbl, nsrc, favg) -> variant
@@ -297,7 +383,14 @@ int choose_variant(const SweepArgs& A, cudaStream_t s) {
     cudaEventCreate(&b);
     int best = 0;
     float best_ms = 1e30f;
+    const size_t st_smem = staged_smem_bytes(A);
+    const bool staged_ok =
+        st_smem <= kStagedSmemMax &&
+        cudaFuncSetAttribute(accumulate_staged_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)st_smem) ==
+            cudaSuccess;
+    cudaGetLastError();
     for (int v = 0; v < kNumVariants; v++) {
+        if (kVariants[v].sy == 0 && !staged_ok) continue;
         kVariants[v].launch(A, s);  // warm
         cudaEventRecord(a, s);
         kVariants[v].launch(A, s);

@@ -90,7 +90,8 @@ def peel_gpu(d_resid_tfb, d_weights_tfb, freqs, tile_xyzs, lmsts, average_lmst, 
 
 def batched_tuning():
     """(bins per CTA, sources per CTA, ms) the batched peel's autotuner chose
-    for the last new problem shape."""
+    for the last new problem shape; (16, 0) is the variant that stages the
+    residual of 16 baselines in shared memory for every source."""
     bx, sy, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_float()
     _lib.check(_lib.lib().hdc_peel_batched_tuning(ctypes.byref(bx), ctypes.byref(sy), ctypes.byref(ms)),
                "hdc_peel_batched_tuning")

@@ -246,3 +246,72 @@ def test_timeblocks_graph_equals_per_timeblock_calls(form):
         assert [r.num_iterations for r in results[k]] == [r.num_iterations for r in res]
         assert [r.converged for r in results[k]] == [r.converged for r in res]
         assert not res[3].converged and sum(r.converged for r in res) >= nch - 2
+
+
+def test_calibrate_chanblocks_one_pass_and_listed(oracle):
+    """hdc_calibrate_chanblocks: one pass without the retry gives the
+    oracle's per-chanblock solves; a list re-runs only the named chanblocks
+    (the building block of the chanblock-sharded calibration)."""
+    import ctypes
+
+    from mwa_hyperdrive_b200 import _lib
+
+    rng = np.random.default_rng(21)
+    ntiles, nt, nch = 12, 2, 5
+    nbl = ntiles * (ntiles - 1) // 2
+    model = synth.random_model(nt, nch, nbl, rng)
+    data = synth.corrupt(model, synth.truth_gains(ntiles, nch, rng), rng, 30.0)
+    start = identity(ntiles, nch)
+    start[:, 2] = 0.0  # fails without the retry
+    d, m = torch.from_numpy(data).cuda(), torch.from_numpy(model).cuda()
+    dj = torch.from_numpy(start.copy()).cuda()
+    res = (_lib.HdcCalResult * nch)()
+    _lib.check(_lib.lib().hdc_calibrate_chanblocks(d.data_ptr(), m.data_ptr(), nt, 0, nt, nch, nbl, dj.data_ptr(), 50,
+                                                   1e-8, 1e-4, 0, None, 0, res, 0, None), "hdc_calibrate_chanblocks")
+    got = dj.cpu().numpy()
+    for c in range(nch):
+        ref, r = oracle.calibrate(data, model, c, start[:, c], 50, 1e-8, 1e-4, 0)
+        assert res[c].num_iterations == r.num_iterations and bool(res[c].converged) == bool(r.converged)
+        np.testing.assert_array_equal(np.isnan(got[:, c]), np.isnan(ref))
+    assert not res[2].converged
+    # re-run chanblock 2 alone from its neighbours' mean: it converges, the others are untouched
+    before = got.copy()
+    seedv = 0.5 * (got[:, 1] + got[:, 3])
+    dj[:, 2] = torch.from_numpy(seedv).cuda()
+    lst = (ctypes.c_int * 1)(2)
+    _lib.check(_lib.lib().hdc_calibrate_chanblocks(d.data_ptr(), m.data_ptr(), nt, 0, nt, nch, nbl, dj.data_ptr(), 50,
+                                                   1e-8, 1e-4, 0, lst, 1, res, 0, None), "hdc_calibrate_chanblocks")
+    after = dj.cpu().numpy()
+    assert res[2].converged
+    np.testing.assert_array_equal(after[:, [0, 1, 3, 4]], before[:, [0, 1, 3, 4]])
+    ref, r = oracle.calibrate(data, model, 2, seedv, 50, 1e-8, 1e-4, 0)
+    assert res[2].num_iterations == r.num_iterations
+    assert np.max(np.abs(after[:, 2] - ref)) < 1e-10
+
+
+def test_sharded_calibration_with_the_gpu_solver(oracle, tmp_path):
+    """shard.calibrate_timeblock_sharded with the GPU chanblock solver on one
+    rank equals calibrate_timeblock (first pass and band-wide retry)."""
+    import torch.distributed as dist
+
+    from mwa_hyperdrive_b200 import shard
+
+    rng = np.random.default_rng(22)
+    ntiles, nt, nch = 12, 2, 6
+    nbl = ntiles * (ntiles - 1) // 2
+    model = synth.random_model(nt, nch, nbl, rng)
+    data = synth.corrupt(model, synth.truth_gains(ntiles, nch, rng), rng, 30.0)
+    start = identity(ntiles, nch)
+    start[:, 2] = start[:, 3] = 0.0
+    d, m = torch.from_numpy(data).cuda(), torch.from_numpy(model).cuda()
+    ref_dj, ref_res = gpu_timeblock(data, model, start, 0, nt, form="collapsed_f32")
+    dist.init_process_group("gloo", init_method=f"file://{tmp_path}/pg", rank=0, world_size=1)
+    try:
+        solver = shard.gpu_chanblock_solver(d, m, (0, nt), form="collapsed_f32")
+        sols, res = shard.calibrate_timeblock_sharded(solver, start.copy(), 0, nch)
+    finally:
+        dist.destroy_process_group()
+    np.testing.assert_array_equal(np.isnan(sols), np.isnan(ref_dj))
+    ok = ~np.isnan(ref_dj)
+    assert np.max(np.abs(sols[ok] - ref_dj[ok])) == 0.0
+    assert [r["num_iterations"] for r in res] == [r.num_iterations for r in ref_res]
