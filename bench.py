@@ -900,10 +900,13 @@ def guarded(fn, args):
 # the two DRAM counters), summarised in
 # profiles/predict_launch_list_mixed_predict.md.  The visibilities alone are
 # 100 MB read + 100 MB written per launch.
+# The tensor point predict stores each baseline once into planes that a
+# coalesced pass (combine_kernel, 245 MB per launch) adds into the
+# visibilities; the figure below is the gram kernel's own.
 NCU_TRAFFIC_SOURCE = "ncu launch list of this bench command (profiles/predict_launch_list_mixed_predict.md)"
 NCU_DRAM_BYTES_PER_LAUNCH = {
-    ("points", "tensor"): 1202e6, ("gaussians", "tensor"): 150e6, ("shapelets", "tensor"): 153e6,
-    ("points", "direct"): 264e6, ("gaussians", "direct"): 151e6, ("shapelets", "direct"): 143e6,
+    ("points", "tensor"): 156.9e6, ("gaussians", "tensor"): 150.9e6, ("shapelets", "tensor"): 164.3e6,
+    ("points", "direct"): 265.8e6, ("gaussians", "direct"): 152.6e6, ("shapelets", "direct"): 142.3e6,
 }
 
 
@@ -1088,6 +1091,15 @@ def gpu_arm(args, rank, world, local_rank):
             # output (still in `vis`) against the FP64 oracle
             line["error"] = sampled_error(vis, obs, sky)
             line["reference_gpu"] = guarded(lambda a: reference_gpu_leg(obs, sky), args)
+            rg = line["reference_gpu"]
+            if "all_types" in rg:
+                # the same timestep through the native modeller: the plain
+                # (all-FP64) and the chosen form, against the reference's kernels
+                ref_ms = rg["all_types"]["ref_ms"]
+                rg["native_plain_form"] = {"ms_per_timestep": ms_plain / nt,
+                                           "speedup_vs_reference_kernels": ref_ms / (ms_plain / nt)}
+                rg["native_chosen_form"] = {"ms_per_timestep": ms_chosen / nt,
+                                            "speedup_vs_reference_kernels": ref_ms / (ms_chosen / nt)}
             torch.cuda.synchronize()
         if not (args.skip_dical and args.skip_peel and args.skip_warmstart and args.skip_prep):
             del vis, flush

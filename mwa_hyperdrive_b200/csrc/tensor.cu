@@ -429,7 +429,11 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const __grid_consta
         // straight-line block.  Component data goes through a ring of CRING
         // slots, stashed two stages ahead by the first CPS threads.  Stages
         // past the end read zeros (their values are never written out).
-        auto compute = [&](int k, int (&xr)[2][4], int (&xi)[2][4], int (&yr)[4], int (&yi)[4], int (&yn)[4]) {
+        // compute and write_planes take SKIP (skip_hi) as a compile-time
+        // constant, so the two rows' work stays one straight-line block
+        auto compute = [&](auto skip_c, int k, int (&xr)[2][4], int (&xi)[2][4], int (&yr)[4], int (&yi)[4],
+                           int (&yn)[4]) {
+            constexpr bool SKIP = decltype(skip_c)::value;
             const CompStage& cs_ = comp_s[k % CRING];
             if constexpr (MODE == 0) {
                 const int cb4 = kq * 16 + quad * 4;  // this thread's 4 components
@@ -451,7 +455,7 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const __grid_consta
                     float snq = 0.f, csq = 0.f;
 #pragma unroll
                     for (int s2 = 0; s2 < 2; s2++) {
-                        if (s2 == 1 && skip_hi) continue;
+                        if (SKIP && s2 == 1) continue;
                         float sn, cs;
                         phasor_quarter_f32(u[s2] * cl[j] + v[s2] * cm[j] + w[s2] * cn[j], sn, cs);
                         const float Xr = fmaf(wr[j], cs, -wi[j] * sn);
@@ -480,7 +484,7 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const __grid_consta
                     float snq = 0.f, csq = 0.f;
 #pragma unroll
                     for (int s2 = 0; s2 < 2; s2++) {
-                        if (s2 == 1 && skip_hi) continue;
+                        if (SKIP && s2 == 1) continue;
                         float sn, cs;
                         phasor_quarter_f32(u[s2] * cl + v[s2] * cm + w[s2] * cn, sn, cs);
                         if (s2 == ry) snq = sn, csq = cs;
@@ -514,14 +518,15 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const __grid_consta
                 }
             }
         };
-        auto write_planes = [&](int st, const int (&xr)[2][4], const int (&xi)[2][4], const int (&yr)[4],
+        auto write_planes = [&](auto skip_c, int st, const int (&xr)[2][4], const int (&xi)[2][4], const int (&yr)[4],
                                 const int (&yi)[4], const int (&yn)[4]) {
+            constexpr bool SKIP = decltype(skip_c)::value;
             unsigned char* sb = smem + st * L::STAGE_BYTES;
             uint32_t pl[4];
             // x planes: bytes 0-2 excess-128 lower digits, byte 3 the signed top digit
 #pragma unroll
             for (int s2 = 0; s2 < 2; s2++) {
-                if (s2 == 1 && skip_hi) continue;
+                if (SKIP && s2 == 1) continue;
                 const uint32_t xo = chunk_off(r0 + 64 * s2, kq) + quad * 4;
 #pragma unroll
                 for (int part = 0; part < 2; part++) {
@@ -559,8 +564,9 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const __grid_consta
             stash(1, 1, a, b, wd);
         }
         producers_sync_or(false);
+        auto producer_loop = [&](auto skip_c) {
         int xr[2][4], xi[2][4], yr[4], yi[4], yn[4];
-        compute(0, xr, xi, yr, yi, yn);
+        compute(skip_c, 0, xr, xi, yr, yi, yn);
         // The producer warps run decoupled: each warp arrives on a stage's
         // full barrier once its planes are written, waits for the tensor
         // core only on the buffer it is about to overwrite, and for the
@@ -579,7 +585,7 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const __grid_consta
                 break;
             }
             int nxr[2][4], nxi[2][4], nyr[4], nyi[4], nyn[4];
-            write_planes(st, xr, xi, yr, yi, yn);
+            write_planes(skip_c, st, xr, xi, yr, yi, yn);
             // stage k + 1's component data: stages 0 and 1 were published by
             // the barrier above, later ones by warp 0 in its iteration k - 1
             if (k + 1 >= 2 && !__all_sync(0xffffffffu, mbar_wait_bounded(&comp_bar[(k + 1) % CRING],
@@ -587,7 +593,7 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const __grid_consta
                 abort_s = 1;
                 break;
             }
-            compute(k + 1, nxr, nxi, nyr, nyi, nyn);
+            compute(skip_c, k + 1, nxr, nxi, nyr, nyi, nyn);
             fence_proxy_async_smem();  // make the generic-proxy stores visible to the tensor core
             if (pre) stash(k + 2, (k + 2) % CRING, na, nb, nw);
             __syncwarp();  // the lanes' stores and fences before the warp's one arrival
@@ -602,6 +608,11 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const __grid_consta
                 yr[j] = nyr[j], yi[j] = nyi[j], yn[j] = nyn[j];
             }
         }
+        };
+        if (skip_hi)
+            producer_loop(std::true_type{});
+        else
+            producer_loop(std::false_type{});
     } else {
         // ------------------------------------------------ MMA issuer (one thread)
         if (lane == 0) {
