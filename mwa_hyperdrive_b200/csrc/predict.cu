@@ -1091,7 +1091,7 @@ extern "C" const char* model_points_tc(const Points* comps, const Addresses* a, 
     size_t off_gp = align256(off_w + (d_beam_jones && !tile_beam ? sizeof(JonesF64) * (size_t)nf * nc : 0));
     size_t off_map = align256(off_gp + sizeof(double4) * nc);
     size_t off_ws = align256(off_map + sizeof(int) * (size_t)ntiles);
-    size_t total = align256(off_ws + tensor_workspace_bytes(nf, nbl, false));
+    size_t total = align256(off_ws + tensor_workspace_bytes(nf, nbl, ntiles, nc, tile_beam, false));
     char* ws = (char*)device_scratch(total);
     if (!ws) return "out of device memory";
     PrepIn in = {};

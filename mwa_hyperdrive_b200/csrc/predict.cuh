@@ -74,8 +74,9 @@ struct TensorBeam {
 
 // The tensor-core point predict of one timestep (csrc/tensor.cu): d_W is
 // B S B^H [nf][nc] with a beam shared by all tiles (beam NULL), or S [nf][nc]
-// with per-tile beams.  ws: tensor_workspace_bytes(nf, nbl, out64) bytes.
-size_t tensor_workspace_bytes(int nf, int nbl, bool out64);
+// with per-tile beams.  ws: tensor_workspace_bytes(nf, nbl, ntiles, nc,
+// per-tile beams, out64) bytes.
+size_t tensor_workspace_bytes(int nf, int nbl, int ntiles, int nc, bool tile_beam, bool out64);
 int launch_tensor_points(int nf, int nbl, int ntiles, int nc, const double* d_freqs, const XYZ* d_xyzs, double ha,
                          double dec, const double4* d_lmn, const JonesF64* d_W, const TensorBeam* beam, void* d_vis,
                          bool out64, void* ws, int* d_err, cudaStream_t s);

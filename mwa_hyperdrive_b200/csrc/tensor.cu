@@ -84,7 +84,6 @@ constexpr int NB = 2 * NH; // MMA N: [Re | Im] of the NH columns
 constexpr int KC = 32;     // K bytes per stage = MMA K
 constexpr int NPW = 16;    // producer / epilogue warps
 constexpr int NPT = NPW * 32;  // producer threads
-constexpr int THREADS = NPT + 32;
 constexpr int XT_BYTES = NT * KC;  // one X plane tile, 4 KB
 constexpr int YT_BYTES = NH * KC;  // one Y plane tile, 2 KB
 constexpr int LBO = 128;             // bytes between the two 16-byte K core matrices of a row group
@@ -105,12 +104,30 @@ template <>
 struct Cfg<0> {
     static constexpr int XDIG = 4, YDIG = 3, NSTAGE = 4, CPS = 32;  // components per stage
     static constexpr int KPASS = 16384;  // 3 products x 2 x 2^14 x KPASS < 2^31
+    static constexpr int THREADS = NPT + 32;  // producers + the MMA warp
 };
 template <>
 struct Cfg<1> {
     static constexpr int XDIG = 4, YDIG = 4, NSTAGE = 3, CPS = 16;
     static constexpr int KPASS = 8000;  // 4 products x 2 x 2^14 x 2 KPASS < 2^31
+    static constexpr int THREADS = NPT + 32;
 };
+// MODE 2 (shared beam, table form): the A operand is the phasor matrix A
+// itself (3 digits, as y above), the same for every polarisation, and W
+// moves to the B side: V^ab = A (A diag(conj W^ab))^H.  The A planes and
+// the FP32 phasors come from a table written once per (channel, stage).
+template <>
+struct Cfg<2> {
+    static constexpr int XDIG = 3, YDIG = 4, NSTAGE = 4, CPS = 32;
+    static constexpr int KPASS = 16384;  // 3 products x 2 x 2^14 x KPASS < 2^31
+    static constexpr int THREADS = NPT + 64;  // producers + the MMA warp + the copy warp
+};
+// Table of one (channel, stage): the A planes of each row block ([re, im]
+// x 3 digits in the shared-memory layout, 24 KB), then the FP32 phasors
+// (cos, sin) of each column block of 64 tiles (rows of 32 components).
+constexpr int PL_BYTES = 2 * 3 * XT_BYTES;
+constexpr int PH_ROW = KC * 8;
+constexpr int PH_BYTES = NH * PH_ROW;
 template <int MODE>
 struct Lay {
     static constexpr int Y_OFF = 2 * Cfg<MODE>::XDIG * XT_BYTES;                     // X: [re, im][digits]
@@ -118,6 +135,9 @@ struct Lay {
     static constexpr int SMEM_BYTES = Cfg<MODE>::NSTAGE * STAGE_BYTES + 1024;
     static constexpr int CRING = Cfg<MODE>::NSTAGE + 2;  // component ring: warps may be NSTAGE stages apart
 };
+static_assert(Lay<2>::SMEM_BYTES <= 220 * 1024, "MODE 2 stages exceed shared memory");
+static_assert(Lay<2>::STAGE_BYTES % 16 == 0 && PH_ROW % 16 == 0, "bulk copies need 16-byte alignment");
+constexpr int PF_STAGES = 8;  // MODE 2: table blocks are prefetched into L2 this many stages ahead
 
 // component data of one stage, staged in shared memory (structure of arrays
 // so that 16-byte loads of consecutive components are conflict-free)
@@ -128,6 +148,9 @@ struct CompStage0 {
 struct CompStage1 {
     double l[16], m[16], n[16];
     float4 s[16][2];             // S (xx, xy | yx, yy as re, im) of this channel
+};
+struct CompStage2 {
+    float2 w[KC];                // W of this polarisation times sx
 };
 
 struct Params {
@@ -147,6 +170,16 @@ struct Params {
     const double* maxs;
     void* planes;          // [4][nf][nbl] float2 (or double2 with OUT64)
     int* err;
+    // MODE 2: channels f0 + blockIdx.y; the table of channel f0 + i at
+    // table + i * tab_chan, its stage k at + k * tab_block (row-block planes
+    // first, the column-block phasors from tab_ph_off)
+    int f0;
+    const unsigned char* table;
+    size_t tab_chan, tab_block, tab_ph_off;
+    // per channel after its stages: W sx of each polarisation (XX, YY, XY)
+    // [3][stages x 32] float2, then the three bounds max |W| (double)
+    size_t tab_w_off, tab_bound_off;
+    int ncb;
     int njobs;
     uint32_t jobs[MAXJOBS];  // pol | rb << 8 | cb << 20
 };
@@ -274,22 +307,25 @@ __device__ __forceinline__ float4 beam_row(const Params& P, int tile, int c, int
 }
 
 template <int MODE, bool OUT64>
-__global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const __grid_constant__ Params P) {
+__global__ void __launch_bounds__(Cfg<MODE>::THREADS, 1) gram_i8_kernel(const __grid_constant__ Params P) {
     using C = Cfg<MODE>;
     using L = Lay<MODE>;
     constexpr int NSTAGE = C::NSTAGE;
     constexpr int CRING = L::CRING;
-    using CompStage = typename std::conditional<MODE == 0, CompStage0, CompStage1>::type;
+    constexpr int NTHR = C::THREADS;
+    using CompStage = typename std::conditional<
+        MODE == 0, CompStage0, typename std::conditional<MODE == 1, CompStage1, CompStage2>::type>::type;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     __shared__ alignas(8) uint64_t full_bar[NSTAGE], empty_bar[NSTAGE], done_bar;
+    __shared__ alignas(8) uint64_t copy_bar[NSTAGE];  // MODE 2: the stage's A planes have landed
     __shared__ uint32_t tmem_base_s;
-    __shared__ double red_s[THREADS / 32];
+    __shared__ double red_s[NTHR / 32];
     __shared__ volatile int abort_s;
     __shared__ __align__(16) CompStage comp_s[CRING];
     __shared__ alignas(8) uint64_t comp_bar[CRING];
 
     unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    const int f = blockIdx.y;
+    const int f = P.f0 + blockIdx.y;  // channel (planes, W, frequency)
     const uint32_t job = P.jobs[blockIdx.x];
     const int pol = (int)(job & 0xFF);          // 0: XX, 1: YY, 2: XY
     const int rb = (int)((job >> 8) & 0xFFF);   // rows: tiles [128 rb, 128 rb + 128)
@@ -304,7 +340,7 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const __grid_consta
     double bound = 0.0;
     if (MODE == 0) {
         double mx = 0.0;
-        for (int c = tid; c < P.cn; c += THREADS) {
+        for (int c = tid; c < P.cn; c += NTHR) {
             const double2 w = __ldg(reinterpret_cast<const double2*>(P.W + (size_t)f * P.nc + P.c0 + c) + wsel);
             mx = fmax(mx, hypot(w.x, w.y));
         }
@@ -317,6 +353,8 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const __grid_consta
             mbar_init(&empty_bar[s], 1);
         }
         for (int s = 0; s < CRING; s++) mbar_init(&comp_bar[s], 1);  // the stashing warp arrives once
+        if (MODE == 2)
+            for (int s = 0; s < NSTAGE; s++) mbar_init(&copy_bar[s], 1);  // the copy thread's expect_tx
         mbar_init(&done_bar, 1);
         abort_s = 0;
         fence_barrier_init();
@@ -324,7 +362,9 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const __grid_consta
     __syncthreads();
     double bmax = 1.0;
     if (MODE == 0) {
-        for (int i = 0; i < THREADS / 32; i++) bound = fmax(bound, red_s[i]);
+        for (int i = 0; i < NTHR / 32; i++) bound = fmax(bound, red_s[i]);
+    } else if (MODE == 2) {
+        bound = reinterpret_cast<const double*>(P.table + (size_t)blockIdx.y * P.tab_chan + P.tab_bound_off)[pol];
     } else {
         bmax = P.maxb[f];
         bound = 2.0 * bmax * P.maxs[f];
@@ -334,7 +374,7 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const __grid_consta
     // Stokes-I sky) contributes exactly zero: its baselines get zeros.
     const bool zero = !(bound > 0.0);
     const float sx = zero ? 0.f : (float)(FULL31 / bound);
-    const float sy = MODE == 0 ? SY0 : (zero ? 0.f : (float)(FULL31 / bmax));
+    const float sy = MODE != 1 ? SY0 : (zero ? 0.f : (float)(FULL31 / bmax));
     const double inv = zero ? 0.0 : 1.0 / ((double)sx * (double)sy);
     const int nchunks = zero ? 0 : (P.cn + C::CPS - 1) / C::CPS;
 
@@ -355,6 +395,87 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const __grid_consta
         // nothing to multiply
     } else if (warp < NPW) {
         // ------------------------------------------------ producers
+        if constexpr (MODE == 2) {
+            // Table form: warp (g, kq), lane (rl, quad) forms the B operand
+            // of column-block row r = 8 g + rl for the stage's components
+            // 16 kq + 4 quad .. + 3, Y = A_qc conj(W_c) sx in 4 digits, from
+            // the table's FP32 phasors (read from L2 into registers one stage
+            // ahead; the copy warp prefetches them into L2).
+            const int g = warp & 7, kq = warp >> 3, rl = lane >> 2, quad = lane & 3;
+            const int r = 8 * g + rl;
+            const int cl0 = kq * 16 + quad * 4;
+            const uint32_t yo = chunk_off(r, kq) + quad * 4;
+            const unsigned char* tch = P.table + (size_t)blockIdx.y * P.tab_chan;
+            const unsigned char* phq = tch + P.tab_ph_off + (size_t)cb * PH_BYTES + r * PH_ROW + cl0 * 8;
+            const float2* wq = reinterpret_cast<const float2*>(tch + P.tab_w_off) + (size_t)pol * nchunks * KC + cl0;
+            // stage k's phasors and W sx of this thread's four components
+            // (the copy warp prefetches the phasor blocks into L2; past the
+            // end: zeros)
+            auto load_ph = [&](int k, float4& x, float4& y, float4& u, float4& v) {
+                if (k < nchunks) {
+                    const float4* q = reinterpret_cast<const float4*>(phq + (size_t)k * P.tab_block);
+                    x = __ldg(q);
+                    y = __ldg(q + 1);
+                    const float4* wv = reinterpret_cast<const float4*>(wq + (size_t)k * KC);
+                    u = __ldg(wv);
+                    v = __ldg(wv + 1);
+                } else {
+                    x = y = u = v = make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+            };
+            // one lane polls a barrier for its warp; the others follow it
+            // past __syncwarp
+            auto warp_wait = [&](uint64_t* bar, uint32_t parity) {
+                int ok = 1;
+                if (lane == 0) ok = mbar_wait_bounded(bar, parity, P.err);
+                ok = __shfl_sync(0xffffffffu, ok, 0);
+                __syncwarp();
+                return ok != 0;
+            };
+            float4 a01, a23, w01, w23;
+            load_ph(0, a01, a23, w01, w23);
+            for (int k = 0; k < nchunks; k++) {
+                const int st = k % NSTAGE;
+                float4 n01, n23, m01, m23;
+                load_ph(k + 1, n01, n23, m01, m23);  // stage k + 1's inputs, in flight during this stage
+                const float ac[4] = {a01.x, a01.z, a23.x, a23.z}, as[4] = {a01.y, a01.w, a23.y, a23.w};
+                const float wr[4] = {w01.x, w01.z, w23.x, w23.z}, wi[4] = {w01.y, w01.w, w23.y, w23.w};
+                int yv[3][4];  // Yr, Yi, -Yi (+ 0x808080, the balancing offset of the three lower digits)
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const int ir = __float2int_rn(fmaf(wr[j], ac[j], wi[j] * as[j]));
+                    const int ii = __float2int_rn(fmaf(wr[j], as[j], -(wi[j] * ac[j])));
+                    yv[0][j] = ir + 0x808080;
+                    yv[1][j] = ii + 0x808080;
+                    yv[2][j] = -ii + 0x808080;
+                }
+                // the stage buffer's B planes are free once the tensor core
+                // is done with stage k - NSTAGE
+                if (k >= NSTAGE && !warp_wait(&empty_bar[st], ((k / NSTAGE) - 1) & 1)) {
+                    abort_s = 1;
+                    break;
+                }
+                unsigned char* sb = smem + st * L::STAGE_BYTES;
+                uint32_t pl[4];
+#pragma unroll
+                for (int part = 0; part < 3; part++) {
+                    byte_planes4(yv[part], pl);
+                    // bytes 0-2 excess-128 lower digits, byte 3 the signed top digit
+#pragma unroll
+                    for (int b = 0; b < 4; b++)
+                        *reinterpret_cast<uint32_t*>(sb + y_tile<MODE>(part, 3 - b) + yo) =
+                            b < 3 ? pl[b] ^ 0x80808080u : pl[b];
+                }
+                fence_proxy_async_smem();  // make the generic-proxy stores visible to the tensor core
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&full_bar[st]);
+                if (abort_s != 0) break;
+                a01 = n01;
+                a23 = n23;
+                w01 = m01;
+                w23 = m23;
+            }
+        } else {
         // warp = 8 tile rows x 16 K bytes of a stage; lane = (row rl, quad of
         // 4 K bytes), and every thread also takes the row 64 tiles down, so a
         // warp's store of one byte plane is one whole 128-byte core matrix.
@@ -613,14 +734,18 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const __grid_consta
             producer_loop(std::true_type{});
         else
             producer_loop(std::false_type{});
-    } else {
+        }
+    } else if (warp == NPW) {
         // ------------------------------------------------ MMA issuer (one thread)
         if (lane == 0) {
             const uint32_t sbase = smem_u32(smem);
             const uint32_t id = idesc_s8();
             for (int k = 0; k < nchunks; k++) {
                 const int st = k % NSTAGE;
-                const bool ok = mbar_wait_bounded(&full_bar[st], (k / NSTAGE) & 1, P.err);
+                bool ok = mbar_wait_bounded(&full_bar[st], (k / NSTAGE) & 1, P.err);
+                // MODE 2: the A planes came by bulk copy (complete before
+                // the producers arrived; observed here as well)
+                if (MODE == 2 && ok) ok = mbar_wait_bounded(&copy_bar[st], (k / NSTAGE) & 1, P.err);
                 if (!ok) {
                     abort_s = 1;
                     break;
@@ -648,6 +773,42 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const __grid_consta
                 mma_commit(&empty_bar[st]);  // stage free once these MMAs have read it
             }
             mma_commit(&done_bar);
+        }
+    } else if (MODE == 2) {
+        // ------------------------------------------------ table copies (one thread)
+        // Stage k's A planes (this row block) go into stage buffer k %
+        // NSTAGE once the tensor core is done with stage k - NSTAGE.  The
+        // A planes and the producers' phasors are prefetched into L2
+        // PF_STAGES stages ahead.
+        if (lane == 0) {
+            const unsigned char* tch = P.table + (size_t)blockIdx.y * P.tab_chan;
+            auto a_src = [&](int k) { return tch + (size_t)k * P.tab_block + (size_t)rb * PL_BYTES; };
+            auto p_src = [&](int k) { return tch + (size_t)k * P.tab_block + P.tab_ph_off + (size_t)cb * PH_BYTES; };
+            auto copy_a = [&](int k) {
+                mbar_arrive_expect_tx(&copy_bar[k % NSTAGE], PL_BYTES);
+                bulk_g2s(smem + (k % NSTAGE) * L::STAGE_BYTES, a_src(k), PL_BYTES, &copy_bar[k % NSTAGE]);
+            };
+            for (int k = 0; k < nchunks && k < PF_STAGES; k++) {
+                prefetch_l2(a_src(k), PL_BYTES);
+                prefetch_l2(p_src(k), PH_BYTES);
+            }
+            int na = 0;  // copies issued
+            for (; na < nchunks && na < NSTAGE; na++) copy_a(na);
+            for (int k = 0; na < nchunks; k++) {
+                if (k + PF_STAGES < nchunks) {
+                    prefetch_l2(a_src(k + PF_STAGES), PL_BYTES);
+                    prefetch_l2(p_src(k + PF_STAGES), PH_BYTES);
+                }
+                if (!mbar_wait_bounded(&empty_bar[k % NSTAGE], (k / NSTAGE) & 1, P.err) || abort_s != 0) {
+                    abort_s = 1;
+                    break;
+                }
+                copy_a(na++);
+            }
+            // no copy may still be in flight when the CTA leaves: wait
+            // (bounded) for the last one into each buffer
+            for (int j = na > NSTAGE ? na - NSTAGE : 0; j < na; j++)
+                mbar_wait_bounded(&copy_bar[j % NSTAGE], (j / NSTAGE) & 1, nullptr);
         }
     }
 
@@ -708,6 +869,137 @@ __global__ void __launch_bounds__(THREADS, 1) gram_i8_kernel(const __grid_consta
     if (!zero && warp == 0) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+    }
+}
+
+// MODE 2 operand bounds of one pass: grid (channels of the chunk), 1024
+// threads.  For each polarisation (XX, YY, XY) the pass's largest |W| (the
+// operand scale sx = (2^31 - 2^25) / max |W|, as in the other forms).
+constexpr int BOUND_THREADS = 1024;
+__global__ void __launch_bounds__(BOUND_THREADS) weight_bound_kernel(const __grid_constant__ Params P) {
+    const int fl = blockIdx.x, f = P.f0 + fl;
+    const JonesF64* Wf = P.W + (size_t)f * P.nc + P.c0;
+    __shared__ double red[3][BOUND_THREADS / 32];
+    double mx[3] = {0.0, 0.0, 0.0};
+    for (int c = threadIdx.x; c < P.cn; c += BOUND_THREADS) {
+        const double2* w = reinterpret_cast<const double2*>(Wf + c);
+        const double2 xx = __ldg(w), xy = __ldg(w + 1), yy = __ldg(w + 3);
+        mx[0] = fmax(mx[0], hypot(xx.x, xx.y));
+        mx[1] = fmax(mx[1], hypot(yy.x, yy.y));
+        mx[2] = fmax(mx[2], hypot(xy.x, xy.y));
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+    for (int p = 0; p < 3; p++) {
+        for (int o = 16; o > 0; o >>= 1) mx[p] = fmax(mx[p], __shfl_xor_sync(0xffffffffu, mx[p], o));
+        if (lane == 0) red[p][warp] = mx[p];
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        double bound = 0.0;
+        for (int i = 0; i < BOUND_THREADS / 32; i++) bound = fmax(bound, red[threadIdx.x][i]);
+        reinterpret_cast<double*>(const_cast<unsigned char*>(P.table) + (size_t)fl * P.tab_chan +
+                                  P.tab_bound_off)[threadIdx.x] = bound;
+    }
+}
+
+// MODE 2 table of one pass: grid (stages, row blocks, channels of the
+// chunk), 256 threads.  Thread (row, kh) takes tile 128 rb + row and the
+// stage's components 16 kh .. 16 kh + 15: their phasors A (the same FP64
+// phase and FP32 polynomials as the in-kernel forms), the 16-byte chunk
+// (row, kh) of each of the six A planes (3 digits of re and im, as y of
+// MODE 0), and the FP32 (cos, sin) row of the tile's column block, staged
+// in shared memory (rows padded to 272 bytes: conflict-free) so that every
+// warp store to the table is 512 contiguous bytes.  The CTAs of row block 0
+// also write the stage's W sx of each polarisation.
+constexpr int TROW = PH_ROW + 16;
+__global__ void __launch_bounds__(256) phasor_table_kernel(const __grid_constant__ Params P) {
+    __shared__ __align__(16) unsigned char phs[NT * TROW];
+    __shared__ double2 lm_s[KC];
+    __shared__ double n_s[KC];
+    const int k = blockIdx.x, rb = blockIdx.y, fl = blockIdx.z;
+    const int f = P.f0 + fl;
+    const int t = threadIdx.x;
+    const int row = t >> 1, kh = t & 1;
+    const int tile = NT * rb + row;
+    const double oq = 4.0 * P.freqs[f] / VEL_C;
+    double u, v, w;
+    tile_uvw(P, tile, oq, u, v, w);
+    unsigned char* tch = const_cast<unsigned char*>(P.table) + (size_t)fl * P.tab_chan;
+    unsigned char* blk = tch + (size_t)k * P.tab_block;
+    const JonesF64* Wf = P.W + (size_t)f * P.nc + P.c0;
+    // the stage's component positions, once per CTA (past the end: A = 1,
+    // whose W is zero)
+    if (t < KC) {
+        const int c = k * KC + t;
+        double2 a = make_double2(0.0, 0.0);
+        double nn = 0.0;
+        if (c < P.cn) {
+            const double4* lmn = P.lmn + P.c0;
+            a = __ldg(reinterpret_cast<const double2*>(lmn + c));
+            nn = __ldg(reinterpret_cast<const double*>(lmn + c) + 2);
+        }
+        lm_s[t] = a;
+        n_s[t] = nn;
+    } else if (rb == 0 && t >= 128 && t < 128 + 3 * KC) {
+        // W sx of polarisation p (XX, YY, XY) for component t % 32 of the stage
+        const int p = (t - 128) / KC, cl = (t - 128) % KC, c = k * KC + cl;
+        const double bound = reinterpret_cast<const double*>(tch + P.tab_bound_off)[p];
+        const float sx = bound > 0.0 ? (float)(FULL31 / bound) : 0.f;
+        float2 o = make_float2(0.f, 0.f);
+        if (c < P.cn) {
+            const double2 wv = __ldg(reinterpret_cast<const double2*>(Wf + c) + (p == 0 ? 0 : (p == 1 ? 3 : 1)));
+            o = make_float2((float)(wv.x * (double)sx), (float)(wv.y * (double)sx));
+        }
+        const int nstg = (P.cn + KC - 1) / KC;
+        reinterpret_cast<float2*>(tch + P.tab_w_off)[((size_t)p * nstg + k) * KC + cl] = o;
+    }
+    __syncthreads();
+    int yr[16], yi[16];
+#pragma unroll
+    for (int j = 0; j < 16; j += 2) {
+        float2 ph[2];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const double2 a = lm_s[kh * 16 + j + h];
+            const double cn = n_s[kh * 16 + j + h];
+            float sn, cs;
+            phasor_quarter_f32(u * a.x + v * a.y + w * cn, sn, cs);
+            // y + 0x8080 + 0x400000 in the FP32 mantissa (one rounding)
+            yr[j + h] = __float_as_int(__fmaf_rn(cs, SY0, YOFF));
+            yi[j + h] = __float_as_int(__fmaf_rn(sn, SY0, YOFF));
+            ph[h] = make_float2(cs, sn);
+        }
+        *reinterpret_cast<float4*>(phs + row * TROW + kh * 128 + j * 8) = make_float4(ph[0].x, ph[0].y, ph[1].x, ph[1].y);
+    }
+    unsigned char* pb = blk + (size_t)rb * PL_BYTES + chunk_off(row, kh);
+#pragma unroll
+    for (int part = 0; part < 2; part++) {
+        uint32_t d[3][4];  // [digit][word of 4 components]
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            uint32_t pl[4];
+            byte_planes4((part ? yi : yr) + 4 * q, pl);
+            // bytes 0-1 excess-128, byte 2 the top digit + 64
+            d[2][q] = pl[0] ^ 0x80808080u;
+            d[1][q] = pl[1] ^ 0x80808080u;
+            d[0][q] = minus64(pl[2]);
+        }
+#pragma unroll
+        for (int dg = 0; dg < 3; dg++)
+            *reinterpret_cast<uint4*>(pb + (part * 3 + dg) * XT_BYTES) = make_uint4(d[dg][0], d[dg][1], d[dg][2], d[dg][3]);
+    }
+    __syncthreads();
+    // phasor rows of column blocks 2 rb and 2 rb + 1 (those that exist):
+    // 16-byte unit i of the 128 rows x 256 bytes
+    const int nrows = (P.ncb - 2 * rb) * NH < NT ? (P.ncb - 2 * rb) * NH : NT;
+    unsigned char* pdst = blk + P.tab_ph_off + (size_t)(2 * rb) * PH_BYTES;
+#pragma unroll
+    for (int i = t; i < NT * (PH_ROW / 16); i += 256) {
+        const int rr = i / (PH_ROW / 16), uu = i % (PH_ROW / 16);
+        if (rr < nrows)
+            *reinterpret_cast<float4*>(pdst + (size_t)rr * PH_ROW + uu * 16) =
+                *reinterpret_cast<const float4*>(phs + rr * TROW + uu * 16);
     }
 }
 
@@ -791,13 +1083,49 @@ int build_jobs(int ntiles, uint32_t* jobs) {
     return nj;
 }
 
+// The MODE 2 table of a pass: bytes per (channel, stage) and per channel,
+// and the channels of one chunk: as many as fit in TABLE_CAP, rounded down
+// to a multiple that fills whole waves of the SMs with jobs.
+constexpr size_t TABLE_CAP = (size_t)1 << 30;
+
+struct TableShape {
+    int nrb, ncb, nstg, chunk;
+    size_t block, chan;
+};
+
+static int gcd_int(int a, int b) { return b == 0 ? a : gcd_int(b, a % b); }
+
+static TableShape table_shape(int nf, int ntiles, int cn, int njobs) {
+    TableShape t;
+    t.nrb = (ntiles + NT - 1) / NT;
+    t.ncb = (ntiles + NH - 1) / NH;
+    t.nstg = (cn + KC - 1) / KC;
+    t.block = (size_t)t.nrb * PL_BYTES + (size_t)t.ncb * PH_BYTES;
+    t.chan = (size_t)t.nstg * t.block + (size_t)3 * t.nstg * KC * sizeof(float2) + 32;
+    int sms = 148, dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaGetLastError();
+    const int fit = (int)std::max<size_t>(1, TABLE_CAP / std::max<size_t>(t.chan, 1));
+    const int q = sms / gcd_int(sms, std::max(njobs, 1));  // channels per whole number of waves
+    t.chunk = std::min(nf, fit >= q ? fit / q * q : fit);
+    return t;
+}
+
 }  // namespace tc
 
-// Bytes of device workspace the tensor predict needs for nf channels: the
-// four planes and the MODE 1 per-channel bounds.
-size_t tensor_workspace_bytes(int nf, int nbl, bool out64) {
+// Bytes of device workspace the tensor predict needs for nf channels of
+// nc components: the four planes, the MODE 1 per-channel bounds and, with
+// a shared beam, the MODE 2 table of one chunk of channels.
+size_t tensor_workspace_bytes(int nf, int nbl, int ntiles, int nc, bool tile_beam, bool out64) {
     const size_t planes = (size_t)4 * nf * nbl * (out64 ? 16 : 8);
-    return ((planes + 255) & ~(size_t)255) + 2 * sizeof(double) * (size_t)nf + 256;
+    size_t bytes = ((planes + 255) & ~(size_t)255) + ((2 * sizeof(double) * (size_t)nf + 255) & ~(size_t)255);
+    if (!tile_beam && nc > 0 && nf > 0) {
+        std::vector<uint32_t> jobs(tc::MAXJOBS);
+        const int nj = tc::build_jobs(ntiles, jobs.data());
+        const tc::TableShape t = tc::table_shape(nf, ntiles, std::min(nc, tc::Cfg<2>::KPASS), nj);
+        bytes += (size_t)t.chunk * t.chan;
+    }
+    return bytes + 256;
 }
 
 struct TensorState {
@@ -810,7 +1138,7 @@ int tensor_configure() {
     static std::once_flag once;
     static cudaError_t attr_err = cudaSuccess;
     std::call_once(once, [] {
-        const cudaError_t e[4] = {
+        const cudaError_t e[6] = {
             cudaFuncSetAttribute(tc::gram_i8_kernel<0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  tc::Lay<0>::SMEM_BYTES),
             cudaFuncSetAttribute(tc::gram_i8_kernel<0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -818,7 +1146,11 @@ int tensor_configure() {
             cudaFuncSetAttribute(tc::gram_i8_kernel<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  tc::Lay<1>::SMEM_BYTES),
             cudaFuncSetAttribute(tc::gram_i8_kernel<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 tc::Lay<1>::SMEM_BYTES)};
+                                 tc::Lay<1>::SMEM_BYTES),
+            cudaFuncSetAttribute(tc::gram_i8_kernel<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 tc::Lay<2>::SMEM_BYTES),
+            cudaFuncSetAttribute(tc::gram_i8_kernel<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 tc::Lay<2>::SMEM_BYTES)};
         for (cudaError_t x : e)
             if (x != cudaSuccess && attr_err == cudaSuccess) attr_err = x;
     });
@@ -843,7 +1175,8 @@ int Modeller::tensor_setup() {
 // [nc] (turns), W [nf][nc] (B S B^H of a beam shared by all tiles, or S with
 // per-tile beams in `beam`), tile XYZs, hour angle and declination of the
 // phase centre; accumulates into vis [nf][nbl] (JonesF32, or JonesF64 with
-// out64).  ws: tensor_workspace_bytes(nf, nbl, out64) of device memory.
+// out64).  ws: tensor_workspace_bytes(nf, nbl, ntiles, nc, per-tile beams,
+// out64) bytes of device memory.
 int launch_tensor_points(int nf, int nbl, int ntiles, int nc, const double* d_freqs, const XYZ* d_xyzs, double ha,
                          double dec, const double4* d_lmn, const JonesF64* d_W, const TensorBeam* beam, void* d_vis,
                          bool out64, void* ws, int* d_err, cudaStream_t s) {
@@ -880,8 +1213,12 @@ int launch_tensor_points(int nf, int nbl, int ntiles, int nc, const double* d_fr
     P.maxb = bounds;
     P.maxs = bounds + nf;
     P.err = d_err;
-    const int kpass = tile_beam ? tc::Cfg<1>::KPASS : tc::Cfg<0>::KPASS;
-    const dim3 grid(P.njobs, nf);
+    P.f0 = 0;
+    P.table = static_cast<const unsigned char*>(ws) + planes_bytes +
+              ((2 * sizeof(double) * (size_t)nf + 255) & ~(size_t)255);
+    P.tab_chan = P.tab_block = P.tab_ph_off = P.tab_w_off = P.tab_bound_off = 0;
+    P.ncb = 0;
+    const int kpass = tile_beam ? tc::Cfg<1>::KPASS : tc::Cfg<2>::KPASS;
     const size_t nvis = (size_t)nf * nbl;
     // passes of at most KPASS components accumulate into the visibilities in turn
     for (int c0 = 0; c0 < P.nc; c0 += kpass) {
@@ -892,18 +1229,43 @@ int launch_tensor_points(int nf, int nbl, int ntiles, int nc, const double* d_fr
                                                       beam->n_uniq_freq, d_W, nc, c0, P.cn, bounds, bounds + nf);
             count_launches(1);
             HDC_CUDA_RET_INT(cudaGetLastError());
+            const dim3 grid(P.njobs, nf);
             if (out64)
-                tc::gram_i8_kernel<1, true><<<grid, tc::THREADS, tc::Lay<1>::SMEM_BYTES, s>>>(P);
+                tc::gram_i8_kernel<1, true><<<grid, tc::Cfg<1>::THREADS, tc::Lay<1>::SMEM_BYTES, s>>>(P);
             else
-                tc::gram_i8_kernel<1, false><<<grid, tc::THREADS, tc::Lay<1>::SMEM_BYTES, s>>>(P);
+                tc::gram_i8_kernel<1, false><<<grid, tc::Cfg<1>::THREADS, tc::Lay<1>::SMEM_BYTES, s>>>(P);
+            count_launches(1);
+            HDC_CUDA_RET_INT(cudaGetLastError());
         } else {
-            if (out64)
-                tc::gram_i8_kernel<0, true><<<grid, tc::THREADS, tc::Lay<0>::SMEM_BYTES, s>>>(P);
-            else
-                tc::gram_i8_kernel<0, false><<<grid, tc::THREADS, tc::Lay<0>::SMEM_BYTES, s>>>(P);
+            // the table of a chunk of channels, then their Gram products
+            // (one stream: the next chunk's table waits for these products)
+            const tc::TableShape t = tc::table_shape(nf, ntiles, std::min(nc, kpass), P.njobs);
+            const int nstg = (P.cn + tc::KC - 1) / tc::KC;
+            P.tab_block = t.block;
+            P.tab_w_off = (size_t)nstg * t.block;
+            P.tab_bound_off = P.tab_w_off + (size_t)3 * nstg * tc::KC * sizeof(float2);
+            P.tab_chan = P.tab_bound_off + 32;
+            P.tab_ph_off = (size_t)t.nrb * tc::PL_BYTES;
+            P.ncb = t.ncb;
+            for (int f0 = 0; f0 < nf; f0 += t.chunk) {
+                const int nch = std::min(t.chunk, nf - f0);
+                P.f0 = f0;
+                tc::weight_bound_kernel<<<nch, tc::BOUND_THREADS, 0, s>>>(P);
+                count_launches(1);
+                HDC_CUDA_RET_INT(cudaGetLastError());
+                tc::phasor_table_kernel<<<dim3(nstg, t.nrb, nch), 256, 0, s>>>(P);
+                count_launches(1);
+                HDC_CUDA_RET_INT(cudaGetLastError());
+                const dim3 grid(P.njobs, nch);
+                if (out64)
+                    tc::gram_i8_kernel<2, true><<<grid, tc::Cfg<2>::THREADS, tc::Lay<2>::SMEM_BYTES, s>>>(P);
+                else
+                    tc::gram_i8_kernel<2, false><<<grid, tc::Cfg<2>::THREADS, tc::Lay<2>::SMEM_BYTES, s>>>(P);
+                count_launches(1);
+                HDC_CUDA_RET_INT(cudaGetLastError());
+            }
+            P.f0 = 0;
         }
-        count_launches(1);
-        HDC_CUDA_RET_INT(cudaGetLastError());
         const unsigned blocks = (unsigned)((nvis + 255) / 256);
         if (out64)
             tc::combine_kernel<true><<<blocks, 256, 0, s>>>(ws, d_vis, nvis);
@@ -917,7 +1279,7 @@ int launch_tensor_points(int nf, int nbl, int ntiles, int nc, const double* d_fr
 
 // The modeller's workspace for the tensor predict of up to nf channels.
 void* Modeller::tensor_workspace(bool out64) {
-    const size_t need = tensor_workspace_bytes(nf, nbl, out64);
+    const size_t need = tensor_workspace_bytes(nf, nbl, ntiles, t[0].nc, tile_beams(), out64);
     if (tc->ws_bytes < need) {
         if (tc->ws) cudaFree(tc->ws);
         tc->ws = nullptr;
