@@ -163,6 +163,30 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
     return true;
 }
 
+// As mbar_wait_bounded, but each try suspends the thread in hardware until
+// the phase completes or about a millisecond passes (no polling traffic on
+// the shared-memory pipe while it waits).
+__device__ __forceinline__ bool mbar_wait_sleep(uint64_t* bar, uint32_t parity, int* err,
+                                                uint64_t limit_ns = 2000000000ull) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = global_timer_ns();
+    for (;;) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(smem_u32(bar)), "r"(parity), "r"(1000000u)
+            : "memory");
+        if (ok) return true;
+        if (global_timer_ns() - t0 > limit_ns) {
+            if (err) atomicOr(err, KERR_TIMEOUT);
+            return false;
+        }
+    }
+}
+
 // After a bounded wait of a two-stage bulk-copy pipeline ran out at chunk k,
 // chunks [k, issued) may still be in flight: the issuing thread waits for
 // each of them (bounded again) so that no copy lands in the shared memory of

@@ -6,37 +6,44 @@
 // point-source phasor factors: exp(2 pi i theta_pq,c) = A_pc conj(A_qc) with
 // A_pc = exp(2 pi i (u_p l_c + v_p m_c + w_p (n_c - 1)) f / c).
 //
-// Shared beam (MODE 0).  Each polarisation ab of the visibility matrix is a
-// weighted Gram product
-//     V^ab = X Y^H,  X = A diag(W^ab),  Y = A     (tiles x tiles, over components)
+// Shared beam (MODE 2, the table form).  Each polarisation ab of the
+// visibility matrix is a weighted Gram product
+//     V^ab = A (A diag(conj W^ab))^H       (tiles x tiles, over components)
 // with W = B S B^H the per-component brightness.  W is Hermitian, so
 // V^YX = (V^XY)^H and V^XX, V^YY are Hermitian: three complex products give
-// all four correlations of every baseline.
+// all four correlations of every baseline.  The left operand A is the same
+// for every polarisation and column block, so its digit planes (and the
+// FP32 phasors the right operand is formed from) are computed once per
+// (channel, stage of 32 components) into a table in device memory, which
+// the Gram CTAs read with bulk copies (TMA) and L2 loads.
 //
 // Per-tile beams (MODE 1), the block form: with B_pc the beam of tile p
 // towards component c and S_c its instrumental flux,
 //     V^ab_pq = sum_{c, y} M^a_{p,(c,y)} conj(N^b_{q,(c,y)}),
 //     M^a_{p,(c,y)} = A_pc (B_pc S_c)^{ay},   N^b_{q,(c,y)} = A_qc B_qc^{by},
 // a Gram product over K = 2 x components (y the second index of S); again
-// XX, YY and XY suffice (S Hermitian: V^YX_pq = conj(V^XY_qp)).
+// XX, YY and XY suffice (S Hermitian: V^YX_pq = conj(V^XY_qp)).  Both
+// operands carry the beam, so they are formed in the Gram CTA itself.
 //
-// In real form  Re V = Xr Yr^T + Xi Yi^T,   Im V = Xi Yr^T + Xr (-Yi)^T.
+// With X the left and Y the right operand, in real form
+//     Re V = Xr Yr^T + Xi Yi^T,   Im V = Xi Yr^T + Xr (-Yi)^T.
 //
 // Numbers.  A tensor core accumulating in FP32 does not round to nearest, and
 // its error grows with every K step.  Here every operand is instead a
 // fixed-point integer split into balanced byte digits, and the digit planes
 // are multiplied on the integer tensor core (kind::i8, s8 x s8, s32
 // accumulators), where every sum is exact:
-//   x = rint(X sx), |x| < 2^31 - 2^24 (sx from the channel's largest |X|):
+//   an operand with dynamic range (A conj(W) in MODE 2, M and N in MODE 1):
+//       x = rint(X sx), |x| < 2^31 - 2^24 (sx from the channel's largest |X|),
 //       x = d0 2^24 + d1 2^16 + d2 2^8 + d3, every d_i in [-128, 127];
-//   MODE 0: y = rint(A sy), |y| < 2^22: y = e0 2^16 + e1 2^8 + e2;
-//   MODE 1: y like x (4 digits; N carries the beam's dynamic range).
+//   the unit phasor A (MODE 2): y = rint(A sy), |y| < 2^22,
+//       y = e0 2^16 + e1 2^8 + e2.
 // Balanced digits are the bytes of (x + 0x808080) ^ 0x808080: adding 128 to
 // each lower digit position and flipping its top bit turns excess-128 bytes
 // into two's-complement ones (the flip is applied to four digits of a byte
 // plane at once).  They have zero mean, so the products left out below do
 // not bias the sum.  x y = sum_ij d_i e_j 2^(XW + YW - 8(i + j)); the plane
-// products with i + j <= 3 are kept (9 in MODE 0, 10 in MODE 1; the rest
+// products with i + j <= 3 are kept (9 in MODE 2, 10 in MODE 1; the rest
 // weigh < 2^-30 of full scale), each into the accumulator of its class
 // w = i + j, and the epilogue forms V = sum_w D_w 2^(XW + YW - 8w) / (sx sy)
 // in FP64.  The only rounding is in the inputs: the phase, reduced exactly
@@ -51,21 +58,24 @@
 // baseline of that polarisation (XX, YY: some p < q; XY: all), so any number
 // of tiles is covered.  M = 128 tiles (rows of X), 64 tile columns (rows of
 // Y), K = 32 bytes per stage (32 components, or 16 components x 2 in MODE
-// 1).  Sixteen producer warps compute the per-tile phasors, X and Y, the byte
-// planes, and write them to shared memory in the K-major core-matrix layout
-// (one warp store = one 128-byte core matrix); the stage's component data is
-// staged in shared memory two stages ahead, so the phasor loop reads no
-// global memory except, in MODE 1, the beam Jones of its tiles.  One thread
-// issues the MMAs of a stage (plane pairs x {Xr, Xi}, N = 128 = [Re | Im] of
-// the 64 columns) into 4 TMEM accumulators (one per class, 128 columns each
-// = all 512 columns).  The epilogue reads TMEM with tcgen05.ld, combines the
-// classes in FP64 and stores each of its baselines' values once into a planar
-// scratch [XX, XY, YX, YY][channel][baseline] (XY of p < q as XY, of p > q as
-// YX = conj); a coalesced pass then adds the four planes into the
-// visibilities, so every Jones matrix is read and written once.
+// 1).  MODE 2: a copy warp brings each stage's A planes from the table
+// (one bulk copy, prefetched into L2 eight stages ahead) and sixteen
+// producer warps form Y = A conj(W) sx from the table's phasors and weights
+// and write its byte planes.  MODE 1: the sixteen producer warps compute
+// the phasors, beams, X and Y and write all planes.  Planes are in the
+// K-major no-swizzle core-matrix layout (one warp store = one 128-byte core
+// matrix).  One thread issues the MMAs of a stage (plane pairs x {Xr, Xi},
+// N = 128 = [Re | Im] of the 64 columns) into 4 TMEM accumulators (one per
+// class, 128 columns each = all 512 columns).  The epilogue reads TMEM with
+// tcgen05.ld, combines the classes in FP64 and stores each of its baselines'
+// values once into a planar scratch [XX, XY, YX, YY][channel][baseline] (XY
+// of p < q as XY, of p > q as YX = conj); a coalesced pass then adds the four
+// planes into the visibilities, so every Jones matrix is read and written
+// once.
 //
 // Every mbarrier wait is bounded by the global timer; on a timeout the CTA
-// records KERR_TIMEOUT, waits (bounded) for its issued MMAs and frees TMEM.
+// records KERR_TIMEOUT, waits (bounded) for its issued MMAs and copies and
+// frees TMEM.
 
 #include <algorithm>
 #include <cmath>
@@ -90,7 +100,7 @@ constexpr int LBO = 128;             // bytes between the two 16-byte K core mat
 constexpr int SBO = (KC / 16) * 128; // bytes between 8-row groups
 constexpr int TMEM_COLS = 512;       // 4 classes x NB
 constexpr int MAXJOBS = 1024;        // jobs per channel in the launch parameters
-constexpr float SY0 = 4128768.0f;    // MODE 0: 2^22 - 2^16: |A| <= 1 -> |y| < 2^22
+constexpr float SY0 = 4128768.0f;    // MODE 2: 2^22 - 2^16: |A| <= 1 -> |y| < 2^22
 // y + 0x8080 as FP32 bits: 1.5 * 2^23 rounds |v| < 2^22 to an integer in
 // the mantissa; the extra 0x8080 is the balancing offset of the two lower
 // digits.  The mantissa field then holds 2^22 + 0x8080 + y, so byte 2 is the
@@ -101,16 +111,10 @@ constexpr double FULL31 = 2147483648.0 - 33554432.0;  // 2^31 - 2^25
 template <int MODE>
 struct Cfg;
 template <>
-struct Cfg<0> {
-    static constexpr int XDIG = 4, YDIG = 3, NSTAGE = 4, CPS = 32;  // components per stage
-    static constexpr int KPASS = 16384;  // 3 products x 2 x 2^14 x KPASS < 2^31
-    static constexpr int THREADS = NPT + 32;  // producers + the MMA warp
-};
-template <>
 struct Cfg<1> {
-    static constexpr int XDIG = 4, YDIG = 4, NSTAGE = 3, CPS = 16;
+    static constexpr int XDIG = 4, YDIG = 4, NSTAGE = 3, CPS = 16;  // components per stage
     static constexpr int KPASS = 8000;  // 4 products x 2 x 2^14 x 2 KPASS < 2^31
-    static constexpr int THREADS = NPT + 32;
+    static constexpr int THREADS = NPT + 32;  // producers + the MMA warp
 };
 // MODE 2 (shared beam, table form): the A operand is the phasor matrix A
 // itself (3 digits, as y above), the same for every polarisation, and W
@@ -139,18 +143,12 @@ static_assert(Lay<2>::SMEM_BYTES <= 220 * 1024, "MODE 2 stages exceed shared mem
 static_assert(Lay<2>::STAGE_BYTES % 16 == 0 && PH_ROW % 16 == 0, "bulk copies need 16-byte alignment");
 constexpr int PF_STAGES = 8;  // MODE 2: table blocks are prefetched into L2 this many stages ahead
 
-// component data of one stage, staged in shared memory (structure of arrays
-// so that 16-byte loads of consecutive components are conflict-free)
-struct CompStage0 {
-    double l[KC], m[KC], n[KC];  // turn units (n - 1 in n)
-    float2 w[KC];                // W of this polarisation times the x scale sx
-};
+// MODE 1 component data of one stage, staged in shared memory (structure
+// of arrays so that 16-byte loads of consecutive components are
+// conflict-free)
 struct CompStage1 {
-    double l[16], m[16], n[16];
+    double l[16], m[16], n[16];  // turn units (n - 1 in n)
     float4 s[16][2];             // S (xx, xy | yx, yy as re, im) of this channel
-};
-struct CompStage2 {
-    float2 w[KC];                // W of this polarisation times sx
 };
 
 struct Params {
@@ -159,7 +157,7 @@ struct Params {
     const XYZ* xyzs;
     double s_ha, c_ha, s_dec, c_dec;
     const double4* lmn;    // [nc] turn units
-    const JonesF64* W;     // [nf][nc]: MODE 0 B S B^H (or S), MODE 1 S
+    const JonesF64* W;     // [nf][nc]: MODE 2 B S B^H (or S), MODE 1 S
     // MODE 1: beam [uniq tile][uniq freq][nc], unique row of each tile and
     // column of each channel, and per channel bounds of |B| and |S| entries
     const JonesF64* beam;
@@ -313,16 +311,14 @@ __global__ void __launch_bounds__(Cfg<MODE>::THREADS, 1) gram_i8_kernel(const __
     constexpr int NSTAGE = C::NSTAGE;
     constexpr int CRING = L::CRING;
     constexpr int NTHR = C::THREADS;
-    using CompStage = typename std::conditional<
-        MODE == 0, CompStage0, typename std::conditional<MODE == 1, CompStage1, CompStage2>::type>::type;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     __shared__ alignas(8) uint64_t full_bar[NSTAGE], empty_bar[NSTAGE], done_bar;
     __shared__ alignas(8) uint64_t copy_bar[NSTAGE];  // MODE 2: the stage's A planes have landed
     __shared__ uint32_t tmem_base_s;
-    __shared__ double red_s[NTHR / 32];
     __shared__ volatile int abort_s;
-    __shared__ __align__(16) CompStage comp_s[CRING];
-    __shared__ alignas(8) uint64_t comp_bar[CRING];
+    // MODE 1: the ring of component data
+    __shared__ __align__(16) CompStage1 comp_s[MODE == 1 ? CRING : 1];
+    __shared__ alignas(8) uint64_t comp_bar[MODE == 1 ? CRING : 1];
 
     unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     const int f = P.f0 + blockIdx.y;  // channel (planes, W, frequency)
@@ -332,27 +328,17 @@ __global__ void __launch_bounds__(Cfg<MODE>::THREADS, 1) gram_i8_kernel(const __
     const int cb = (int)(job >> 20);            // columns: tiles [64 cb, 64 cb + 64)
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int arow = pol == 1 ? 1 : 0, brow = pol == 0 ? 0 : 1;  // MODE 1: beam rows a (of M) and b (of N)
-    // W component of this polarisation (JonesF64 as 4 double2: xx, xy, yx, yy)
-    const int wsel = pol == 0 ? 0 : (pol == 1 ? 3 : 1);
 
-    // operand scales: MODE 0 from the pass's largest |W|; MODE 1 from the
-    // channel's bounds |M| <= 2 max|B| max|S| and |N| <= max|B|
-    double bound = 0.0;
-    if (MODE == 0) {
-        double mx = 0.0;
-        for (int c = tid; c < P.cn; c += NTHR) {
-            const double2 w = __ldg(reinterpret_cast<const double2*>(P.W + (size_t)f * P.nc + P.c0 + c) + wsel);
-            mx = fmax(mx, hypot(w.x, w.y));
-        }
-        for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-        if (lane == 0) red_s[warp] = mx;
-    }
+    // operand scales: MODE 2 from the pass's largest |W| of this
+    // polarisation (in the table); MODE 1 from the channel's bounds
+    // |M| <= 2 max|B| max|S| and |N| <= max|B|
     if (tid == 0) {
         for (int s = 0; s < NSTAGE; s++) {
             mbar_init(&full_bar[s], NPW);  // one arrival per producer warp
             mbar_init(&empty_bar[s], 1);
         }
-        for (int s = 0; s < CRING; s++) mbar_init(&comp_bar[s], 1);  // the stashing warp arrives once
+        if (MODE == 1)
+            for (int s = 0; s < CRING; s++) mbar_init(&comp_bar[s], 1);  // the stashing warp arrives once
         if (MODE == 2)
             for (int s = 0; s < NSTAGE; s++) mbar_init(&copy_bar[s], 1);  // the copy thread's expect_tx
         mbar_init(&done_bar, 1);
@@ -360,10 +346,8 @@ __global__ void __launch_bounds__(Cfg<MODE>::THREADS, 1) gram_i8_kernel(const __
         fence_barrier_init();
     }
     __syncthreads();
-    double bmax = 1.0;
-    if (MODE == 0) {
-        for (int i = 0; i < NTHR / 32; i++) bound = fmax(bound, red_s[i]);
-    } else if (MODE == 2) {
+    double bound, bmax = 1.0;
+    if (MODE == 2) {
         bound = reinterpret_cast<const double*>(P.table + (size_t)blockIdx.y * P.tab_chan + P.tab_bound_off)[pol];
     } else {
         bmax = P.maxb[f];
@@ -374,7 +358,7 @@ __global__ void __launch_bounds__(Cfg<MODE>::THREADS, 1) gram_i8_kernel(const __
     // Stokes-I sky) contributes exactly zero: its baselines get zeros.
     const bool zero = !(bound > 0.0);
     const float sx = zero ? 0.f : (float)(FULL31 / bound);
-    const float sy = MODE != 1 ? SY0 : (zero ? 0.f : (float)(FULL31 / bmax));
+    const float sy = MODE == 2 ? SY0 : (zero ? 0.f : (float)(FULL31 / bmax));
     const double inv = zero ? 0.0 : 1.0 / ((double)sx * (double)sy);
     const int nchunks = zero ? 0 : (P.cn + C::CPS - 1) / C::CPS;
 
@@ -427,7 +411,7 @@ __global__ void __launch_bounds__(Cfg<MODE>::THREADS, 1) gram_i8_kernel(const __
             // past __syncwarp
             auto warp_wait = [&](uint64_t* bar, uint32_t parity) {
                 int ok = 1;
-                if (lane == 0) ok = mbar_wait_bounded(bar, parity, P.err);
+                if (lane == 0) ok = mbar_wait_sleep(bar, parity, P.err);
                 ok = __shfl_sync(0xffffffffu, ok, 0);
                 __syncwarp();
                 return ok != 0;
@@ -509,41 +493,31 @@ __global__ void __launch_bounds__(Cfg<MODE>::THREADS, 1) gram_i8_kernel(const __
         const double4* lmn = P.lmn + P.c0;
         const JonesF64* Wf = P.W + (size_t)f * P.nc + P.c0;
         // the first CPS threads fetch a stage's component data (zeros past the end)
-        auto fetch = [&](int k, double2& a, double2& b, double4& wd) {
+        auto fetch = [&](int k, double2& a, double2& b) {
             const int c = k * C::CPS + tid;
             if (c < P.cn) {
                 a = __ldg(reinterpret_cast<const double2*>(lmn + c));
                 b = __ldg(reinterpret_cast<const double2*>(lmn + c) + 1);
-                if (MODE == 0) {
-                    const double2 t = __ldg(reinterpret_cast<const double2*>(Wf + c) + wsel);
-                    wd = make_double4(t.x, t.y, 0.0, 0.0);
-                } else {
-                    wd = make_double4(0.0, 0.0, 0.0, 0.0);  // S is read at stash time
-                }
             } else {
                 a = b = make_double2(0.0, 0.0);
-                wd = make_double4(0.0, 0.0, 0.0, 0.0);
             }
         };
-        auto stash = [&](int k, int buf, const double2& a, const double2& b, const double4& wd) {
-            CompStage& cs = comp_s[buf];
+        // S is read at stash time
+        auto stash = [&](int k, int buf, const double2& a, const double2& b) {
+            CompStage1& cs = comp_s[buf];
             cs.l[tid] = a.x;
             cs.m[tid] = a.y;
             cs.n[tid] = b.x;
-            if constexpr (MODE == 0) {
-                cs.w[tid] = make_float2((float)(wd.x * (double)sx), (float)(wd.y * (double)sx));
-            } else {
-                const int c = k * C::CPS + tid;
-                float4 s0 = make_float4(0.f, 0.f, 0.f, 0.f), s1 = s0;
-                if (c < P.cn) {
-                    const double2* sp = reinterpret_cast<const double2*>(Wf + c);
-                    const double2 xx = __ldg(sp), xy = __ldg(sp + 1), yx = __ldg(sp + 2), yy = __ldg(sp + 3);
-                    s0 = make_float4((float)xx.x, (float)xx.y, (float)xy.x, (float)xy.y);
-                    s1 = make_float4((float)yx.x, (float)yx.y, (float)yy.x, (float)yy.y);
-                }
-                cs.s[tid][0] = s0;
-                cs.s[tid][1] = s1;
+            const int c = k * C::CPS + tid;
+            float4 s0 = make_float4(0.f, 0.f, 0.f, 0.f), s1 = s0;
+            if (c < P.cn) {
+                const double2* sp = reinterpret_cast<const double2*>(Wf + c);
+                const double2 xx = __ldg(sp), xy = __ldg(sp + 1), yx = __ldg(sp + 2), yy = __ldg(sp + 3);
+                s0 = make_float4((float)xx.x, (float)xx.y, (float)xy.x, (float)xy.y);
+                s1 = make_float4((float)yx.x, (float)yx.y, (float)yy.x, (float)yy.y);
             }
+            cs.s[tid][0] = s0;
+            cs.s[tid][1] = s1;
         };
         // Software pipeline: iteration k writes the byte planes of stage k
         // from registers and computes the values of stage k + 1 in the same
@@ -555,44 +529,8 @@ __global__ void __launch_bounds__(Cfg<MODE>::THREADS, 1) gram_i8_kernel(const __
         auto compute = [&](auto skip_c, int k, int (&xr)[2][4], int (&xi)[2][4], int (&yr)[4], int (&yi)[4],
                            int (&yn)[4]) {
             constexpr bool SKIP = decltype(skip_c)::value;
-            const CompStage& cs_ = comp_s[k % CRING];
-            if constexpr (MODE == 0) {
-                const int cb4 = kq * 16 + quad * 4;  // this thread's 4 components
-                double cl[4], cm[4], cn[4];
-                float wr[4], wi[4];
-#pragma unroll
-                for (int h = 0; h < 2; h++) {
-                    const double2 l2 = *reinterpret_cast<const double2*>(&cs_.l[cb4 + 2 * h]);
-                    const double2 m2 = *reinterpret_cast<const double2*>(&cs_.m[cb4 + 2 * h]);
-                    const double2 n2 = *reinterpret_cast<const double2*>(&cs_.n[cb4 + 2 * h]);
-                    const float4 w2 = *reinterpret_cast<const float4*>(&cs_.w[cb4 + 2 * h]);
-                    cl[2 * h] = l2.x, cl[2 * h + 1] = l2.y;
-                    cm[2 * h] = m2.x, cm[2 * h + 1] = m2.y;
-                    cn[2 * h] = n2.x, cn[2 * h + 1] = n2.y;
-                    wr[2 * h] = w2.x, wi[2 * h] = w2.y, wr[2 * h + 1] = w2.z, wi[2 * h + 1] = w2.w;
-                }
-#pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    float snq = 0.f, csq = 0.f;
-#pragma unroll
-                    for (int s2 = 0; s2 < 2; s2++) {
-                        if (SKIP && s2 == 1) continue;
-                        float sn, cs;
-                        phasor_quarter_f32(u[s2] * cl[j] + v[s2] * cm[j] + w[s2] * cn[j], sn, cs);
-                        const float Xr = fmaf(wr[j], cs, -wi[j] * sn);
-                        const float Xi = fmaf(wr[j], sn, wi[j] * cs);
-                        // x + 0x808080 (balancing offset of the three lower digits)
-                        xr[s2][j] = __float2int_rn(Xr) + 0x808080;
-                        xi[s2][j] = __float2int_rn(Xi) + 0x808080;
-                        if (s2 == ry) snq = sn, csq = cs;
-                    }
-                    if (ysep) phasor_quarter_f32(u[2] * cl[j] + v[2] * cm[j] + w[2] * cn[j], snq, csq);
-                    // y + 0x8080 + 0x400000 in the FP32 mantissa (one rounding)
-                    yr[j] = __float_as_int(__fmaf_rn(csq, SY0, YOFF));
-                    yi[j] = __float_as_int(__fmaf_rn(snq, SY0, YOFF));
-                    yn[j] = __float_as_int(__fmaf_rn(-snq, SY0, YOFF));
-                }
-            } else {
+            const CompStage1& cs_ = comp_s[k % CRING];
+            {
                 // K bytes 4 quad .. 4 quad + 3 of this warp's 16 = components
                 // c0l, c0l + 1 (stage-local) x y in {X, Y}
                 const int c0l = kq * 8 + quad * 2;
@@ -662,27 +600,19 @@ __global__ void __launch_bounds__(Cfg<MODE>::THREADS, 1) gram_i8_kernel(const __
 #pragma unroll
             for (int part = 0; part < 3; part++) {
                 byte_planes4(part == 0 ? yr : (part == 1 ? yi : yn), pl);
-                if (MODE == 0) {
-                    // y planes: bytes 0-1 excess-128, byte 2 the top digit + 64
-                    *reinterpret_cast<uint32_t*>(sb + y_tile<MODE>(part, 2) + yo) = pl[0] ^ 0x80808080u;
-                    *reinterpret_cast<uint32_t*>(sb + y_tile<MODE>(part, 1) + yo) = pl[1] ^ 0x80808080u;
-                    *reinterpret_cast<uint32_t*>(sb + y_tile<MODE>(part, 0) + yo) = minus64(pl[2]);
-                } else {
-                    // as x: bytes 0-2 excess-128, byte 3 signed
+                // as x: bytes 0-2 excess-128, byte 3 signed
 #pragma unroll
-                    for (int b = 0; b < 4; b++)
-                        *reinterpret_cast<uint32_t*>(sb + y_tile<MODE>(part, 3 - b) + yo) =
-                            b < 3 ? pl[b] ^ 0x80808080u : pl[b];
-                }
+                for (int b = 0; b < 4; b++)
+                    *reinterpret_cast<uint32_t*>(sb + y_tile<MODE>(part, 3 - b) + yo) =
+                        b < 3 ? pl[b] ^ 0x80808080u : pl[b];
             }
         };
         if (tid < C::CPS) {
             double2 a, b;
-            double4 wd;
-            fetch(0, a, b, wd);
-            stash(0, 0, a, b, wd);
-            fetch(1, a, b, wd);
-            stash(1, 1, a, b, wd);
+            fetch(0, a, b);
+            stash(0, 0, a, b);
+            fetch(1, a, b);
+            stash(1, 1, a, b);
         }
         producers_sync_or(false);
         auto producer_loop = [&](auto skip_c) {
@@ -697,9 +627,8 @@ __global__ void __launch_bounds__(Cfg<MODE>::THREADS, 1) gram_i8_kernel(const __
         for (int k = 0; k < nchunks; k++) {
             const int st = k % NSTAGE;
             double2 na, nb;  // stage k + 2's component data, in flight during this stage
-            double4 nw;
             const bool pre = tid < C::CPS;
-            if (pre) fetch(k + 2, na, nb, nw);
+            if (pre) fetch(k + 2, na, nb);
             if (k >= NSTAGE &&
                 !__all_sync(0xffffffffu, mbar_wait_bounded(&empty_bar[st], ((k / NSTAGE) - 1) & 1, P.err))) {
                 abort_s = 1;
@@ -716,7 +645,7 @@ __global__ void __launch_bounds__(Cfg<MODE>::THREADS, 1) gram_i8_kernel(const __
             }
             compute(skip_c, k + 1, nxr, nxi, nyr, nyi, nyn);
             fence_proxy_async_smem();  // make the generic-proxy stores visible to the tensor core
-            if (pre) stash(k + 2, (k + 2) % CRING, na, nb, nw);
+            if (pre) stash(k + 2, (k + 2) % CRING, na, nb);
             __syncwarp();  // the lanes' stores and fences before the warp's one arrival
             if (lane == 0) {
                 mbar_arrive(&full_bar[st]);
@@ -742,10 +671,11 @@ __global__ void __launch_bounds__(Cfg<MODE>::THREADS, 1) gram_i8_kernel(const __
             const uint32_t id = idesc_s8();
             for (int k = 0; k < nchunks; k++) {
                 const int st = k % NSTAGE;
-                bool ok = mbar_wait_bounded(&full_bar[st], (k / NSTAGE) & 1, P.err);
+                bool ok = MODE == 2 ? mbar_wait_sleep(&full_bar[st], (k / NSTAGE) & 1, P.err)
+                                    : mbar_wait_bounded(&full_bar[st], (k / NSTAGE) & 1, P.err);
                 // MODE 2: the A planes came by bulk copy (complete before
                 // the producers arrived; observed here as well)
-                if (MODE == 2 && ok) ok = mbar_wait_bounded(&copy_bar[st], (k / NSTAGE) & 1, P.err);
+                if (MODE == 2 && ok) ok = mbar_wait_sleep(&copy_bar[st], (k / NSTAGE) & 1, P.err);
                 if (!ok) {
                     abort_s = 1;
                     break;
@@ -799,7 +729,7 @@ __global__ void __launch_bounds__(Cfg<MODE>::THREADS, 1) gram_i8_kernel(const __
                     prefetch_l2(a_src(k + PF_STAGES), PL_BYTES);
                     prefetch_l2(p_src(k + PF_STAGES), PH_BYTES);
                 }
-                if (!mbar_wait_bounded(&empty_bar[k % NSTAGE], (k / NSTAGE) & 1, P.err) || abort_s != 0) {
+                if (!mbar_wait_sleep(&empty_bar[k % NSTAGE], (k / NSTAGE) & 1, P.err) || abort_s != 0) {
                     abort_s = 1;
                     break;
                 }
@@ -815,7 +745,7 @@ __global__ void __launch_bounds__(Cfg<MODE>::THREADS, 1) gram_i8_kernel(const __
     // ---------------------------------------------------- epilogue
     __syncthreads();
     const bool aborted = abort_s != 0;
-    const bool ok = zero || mbar_wait_bounded(&done_bar, 0, P.err);
+    const bool ok = zero || mbar_wait_sleep(&done_bar, 0, P.err);
     tc_fence_after();
     if (!aborted && ok && warp < NPW) {
         constexpr int XW = 8 * (C::XDIG - 1), YW = 8 * (C::YDIG - 1);
@@ -907,8 +837,8 @@ __global__ void __launch_bounds__(BOUND_THREADS) weight_bound_kernel(const __gri
 // chunk), 256 threads.  Thread (row, kh) takes tile 128 rb + row and the
 // stage's components 16 kh .. 16 kh + 15: their phasors A (the same FP64
 // phase and FP32 polynomials as the in-kernel forms), the 16-byte chunk
-// (row, kh) of each of the six A planes (3 digits of re and im, as y of
-// MODE 0), and the FP32 (cos, sin) row of the tile's column block, staged
+// (row, kh) of each of the six A planes (3 digits of re and im, the
+// encoding of y above), and the FP32 (cos, sin) row of the tile's column block, staged
 // in shared memory (rows padded to 272 bytes: conflict-free) so that every
 // warp store to the table is 512 contiguous bytes.  The CTAs of row block 0
 // also write the stage's W sx of each polarisation.
@@ -1138,11 +1068,7 @@ int tensor_configure() {
     static std::once_flag once;
     static cudaError_t attr_err = cudaSuccess;
     std::call_once(once, [] {
-        const cudaError_t e[6] = {
-            cudaFuncSetAttribute(tc::gram_i8_kernel<0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 tc::Lay<0>::SMEM_BYTES),
-            cudaFuncSetAttribute(tc::gram_i8_kernel<0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 tc::Lay<0>::SMEM_BYTES),
+        const cudaError_t e[4] = {
             cudaFuncSetAttribute(tc::gram_i8_kernel<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  tc::Lay<1>::SMEM_BYTES),
             cudaFuncSetAttribute(tc::gram_i8_kernel<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
