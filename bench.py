@@ -900,13 +900,14 @@ def guarded(fn, args):
 # the two DRAM counters), summarised in
 # profiles/predict_launch_list_mixed_predict.md.  The visibilities alone are
 # 100 MB read + 100 MB written per launch.
-# The tensor point predict stores each baseline once into planes that a
-# coalesced pass (combine_kernel, 245 MB per launch) adds into the
-# visibilities; the figure below is the gram kernel's own.
+# The tensor point predict of one timestep runs in chunks of channels; the
+# figure is its Gram kernels' DRAM over the timestep: they read the table of
+# A planes and phasors (written by phasor_table_kernel, 2.42 GB per
+# timestep) once from DRAM.
 NCU_TRAFFIC_SOURCE = "ncu launch list of this bench command (profiles/predict_launch_list_mixed_predict.md)"
 NCU_DRAM_BYTES_PER_LAUNCH = {
-    ("points", "tensor"): 156.9e6, ("gaussians", "tensor"): 150.9e6, ("shapelets", "tensor"): 164.3e6,
-    ("points", "direct"): 265.8e6, ("gaussians", "direct"): 152.6e6, ("shapelets", "direct"): 142.3e6,
+    ("points", "tensor"): 2927e6, ("gaussians", "tensor"): 152.0e6, ("shapelets", "tensor"): 164.5e6,
+    ("points", "direct"): 268.0e6, ("gaussians", "direct"): 152.0e6, ("shapelets", "direct"): 142.0e6,
 }
 
 
@@ -1060,7 +1061,7 @@ def gpu_arm(args, rank, world, local_rank):
                       "traffic_source": NCU_TRAFFIC_SOURCE if traffic else None, "ms_per_step": per_step_ms[k]})
         if k == 0 and form == "tensor":
             # what the tensor pipe executes: 18 kind::i8 MMAs of 128 x 128 x 32 per 32-component stage of each
-            # (channel, polarisation, column half) CTA, against 8190 int8 MAC/clk/SM (a probe of back-to-back
+            # (channel, polarisation, column block) CTA, against 8190 int8 MAC/clk/SM (a probe of back-to-back
             # kind::i8 MMAs) at this run's median SM clock
             macs = nf * 6 * ((npts + 31) // 32) * 18 * 128 * 128 * 32
             n_sm = torch.cuda.get_device_properties(0).multi_processor_count
