@@ -399,7 +399,8 @@ __global__ void __launch_bounds__(DT) direct_kernel(const DirectParams p) {
 // memory and table-position loads -- is done once for all FCH channels and
 // only scaled per channel (lambda^-1 for the phase and positions, lambda^-2
 // for the exponent).  The arithmetic per channel is that of the FAST
-// direct_kernel above.  Channels per thread and CTAs per SM by type
+// direct_kernel above, except that the accumulation uses W's Hermitian
+// symmetry (a shared beam).  Channels per thread and CTAs per SM by type
 // (Gaussians 1, shapelets 2).
 template <int TYPE>
 struct FastShape {
@@ -421,7 +422,10 @@ __global__ void __launch_bounds__(DT, FastShape<TYPE>::MIN_CTAS) fast_kernel(con
     __shared__ alignas(128) double4 s_lmn[2][CH];
     __shared__ alignas(128) JonesF64 s_flux[2][FCH][CH];
     __shared__ alignas(128) double4 s_gp[2][CH];
-    __shared__ alignas(16) float s_wf[FCH][CH * 8];
+    // W of each channel as (XX, YY, Re XY, Im XY): this kernel runs with a
+    // beam shared by all tiles (or none), where W = B S B^H is Hermitian
+    // (XX and YY real, YX = conj XY)
+    __shared__ alignas(16) float s_wf[FCH][CH * 4];
     __shared__ alignas(16) float s_dense[TYPE == 2 ? CH * SDN * SDN : 1];
     __shared__ alignas(8) uint64_t bar[2];
 
@@ -490,7 +494,10 @@ __global__ void __launch_bounds__(DT, FastShape<TYPE>::MIN_CTAS) fast_kernel(con
 #pragma unroll
         for (int i = 0; i < FCH; i++) {
             const double* src = reinterpret_cast<const double*>(s_flux[st][i]);
-            for (int e = threadIdx.x; e < n * 8; e += DT) s_wf[i][e] = (float)src[e];
+            for (int e = threadIdx.x; e < n * 4; e += DT) {
+                const int q = e & 3;  // XX re (0), YY re (6), XY re (2), XY im (3) of the component's 8
+                s_wf[i][e] = (float)src[(e >> 2) * 8 + (q == 0 ? 0 : (q == 1 ? 6 : q))];
+            }
         }
         if (TYPE == 2 && p.sdense)
             for (int e = threadIdx.x; e < n * SDN * SDN; e += DT) s_dense[e] = __ldg(p.sdense + (size_t)c0 * SDN * SDN + e);
@@ -547,14 +554,25 @@ __global__ void __launch_bounds__(DT, FastShape<TYPE>::MIN_CTAS) fast_kernel(con
                     } else {
                         shapelet_envelope_f32(p, c0 + c, g, su * ool[i], sv * ool[i], er, ei);
                     }
-                    const float zr = cs * er - sn * ei, zi = fmaf(cs, ei, sn * er);
-                    const float* wv = s_wf[i] + c * 8;
-                    // a += W z, two fused multiply-adds per real part
-#pragma unroll
-                    for (int e = 0; e < 4; e++) {
-                        a[i][2 * e] = fmaf(-wv[2 * e + 1], zi, fmaf(wv[2 * e], zr, a[i][2 * e]));
-                        a[i][2 * e + 1] = fmaf(wv[2 * e + 1], zr, fmaf(wv[2 * e], zi, a[i][2 * e + 1]));
+                    // z = envelope x phasor (a Gaussian's envelope is real)
+                    float zr, zi;
+                    if (TYPE == 1) {
+                        zr = cs * er;
+                        zi = sn * er;
+                    } else {
+                        zr = cs * er - sn * ei;
+                        zi = fmaf(cs, ei, sn * er);
                     }
+                    // a += W z with W Hermitian: 12 fused multiply-adds
+                    const float4 wv = *reinterpret_cast<const float4*>(s_wf[i] + c * 4);
+                    a[i][0] = fmaf(wv.x, zr, a[i][0]);
+                    a[i][1] = fmaf(wv.x, zi, a[i][1]);
+                    a[i][2] = fmaf(-wv.w, zi, fmaf(wv.z, zr, a[i][2]));
+                    a[i][3] = fmaf(wv.w, zr, fmaf(wv.z, zi, a[i][3]));
+                    a[i][4] = fmaf(wv.w, zi, fmaf(wv.z, zr, a[i][4]));
+                    a[i][5] = fmaf(-wv.w, zr, fmaf(wv.z, zi, a[i][5]));
+                    a[i][6] = fmaf(wv.y, zr, a[i][6]);
+                    a[i][7] = fmaf(wv.y, zi, a[i][7]);
                 }
             }
 #pragma unroll
