@@ -279,6 +279,27 @@ __device__ __forceinline__ void collapsed_terms(const T* cv, size_t stride, cons
     h2 = Herm{b2_00, b2_11, b2_01};
 }
 
+// Sum of 12 values (t's 8 reals, then h's a, d, b.re, b.im) over the 16
+// lanes of a half-warp, reduced and scattered: each round halves the values
+// a lane keeps (it sends the half its partner keeps), so after four rounds
+// lane j of the half-warp holds the total of value j (zero for j >= 12).
+// Every value is summed in the same pairing order on every lane.
+__device__ __forceinline__ double row_reduce_scatter16(const J2& t, const Herm& h, int j) {
+    double v[16] = {t.a.re, t.a.im, t.b.re, t.b.im, t.c.re, t.c.im, t.d.re, t.d.im,
+                    h.a,    h.d,    h.b.re, h.b.im, 0.0,    0.0,    0.0,    0.0};
+#pragma unroll
+    for (int half = 8; half > 0; half >>= 1) {
+        const bool hi = (j & half) != 0;
+#pragma unroll
+        for (int k = 0; k < half; k++) {
+            const double send = hi ? v[k] : v[k + half];
+            const double keep = hi ? v[k + half] : v[k];
+            v[k] = keep + __shfl_xor_sync(0xffffffffu, send, half);
+        }
+    }
+    return v[0];
+}
+
 // Threads per CTA of the iteration kernel: the FP32 collapsed form runs two
 // groups of 256 (one per parity of the row block) on one shared ring.
 __host__ __device__ constexpr int cal_threads(int form) { return form == HDC_CAL_COLLAPSED_F32 ? 2 * CT : CT; }
@@ -478,21 +499,21 @@ __global__ void __launch_bounds__(cal_threads(FORM)) mitchcal_kernel(const CalPa
                     ch2.a += h2.a;
                     ch2.d += h2.d;
                     ch2.b = ch2.b + h2.b;
-                    double v[12] = {t1.a.re, t1.a.im, t1.b.re, t1.b.im, t1.c.re, t1.c.im,
-                                    t1.d.re, t1.d.im, h1.a,    h1.d,    h1.b.re, h1.b.im};
-#pragma unroll
-                    for (int k = 0; k < 12; k++) {
-#pragma unroll
-                        for (int o = 8; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
-                    }
-                    if (bj == 0 && p < n) {
-                        double* tp = reinterpret_cast<double*>(&top[p]);
-#pragma unroll
-                        for (int k = 0; k < 8; k++) tp[k] += v[k];
-                        bot[p].a += v[8];
-                        bot[p].d += v[9];
-                        bot[p].b.re += v[10];
-                        bot[p].b.im += v[11];
+                    // row sums over the 16 lanes of the block row, reduced
+                    // and scattered: after the four halving rounds lane bj
+                    // holds the total of value bj (15 shuffles instead of 48)
+                    const double rs = row_reduce_scatter16(t1, h1, bj);
+                    if (bj < 12 && p < n) {
+                        if (bj < 8)
+                            reinterpret_cast<double*>(&top[p])[bj] += rs;
+                        else if (bj == 8)
+                            bot[p].a += rs;
+                        else if (bj == 9)
+                            bot[p].d += rs;
+                        else if (bj == 10)
+                            bot[p].b.re += rs;
+                        else
+                            bot[p].b.im += rs;
                     }
                     if (use_ring) {
                         // the group has read this slot: refill it nring blocks ahead
