@@ -360,8 +360,13 @@ def _pad(b: bytes, fill: bytes = b"\0") -> bytes:
     return b + fill * ((-len(b)) % BLOCK)
 
 
-def encode(primary: Header, hdus: Sequence[HDU]) -> bytes:
+def encode(primary: Header, hdus: Sequence[HDU], primary_data: Optional[np.ndarray] = None) -> bytes:
+    """The file's bytes: the primary header (and its data -- e.g. random
+    groups [GCOUNT][PCOUNT + values] -- big-endian) then each extension."""
     out = [primary.encode()]
+    if primary_data is not None:
+        a = np.asarray(primary_data)
+        out.append(_pad(np.ascontiguousarray(a.astype(a.dtype.newbyteorder(">"))).tobytes()))
     for hdu in hdus:
         out.append(hdu.header.encode())
         if hdu.kind == "IMAGE":
@@ -375,8 +380,9 @@ def encode(primary: Header, hdus: Sequence[HDU]) -> bytes:
     return b"".join(out)
 
 
-def write(path: Union[str, Path], primary: Header, hdus: Sequence[HDU]) -> None:
-    Path(path).write_bytes(encode(primary, hdus))
+def write(path: Union[str, Path], primary: Header, hdus: Sequence[HDU],
+          primary_data: Optional[np.ndarray] = None) -> None:
+    Path(path).write_bytes(encode(primary, hdus, primary_data))
 
 
 # -------------------------------------------------------------- reading
@@ -394,8 +400,11 @@ def decode(buf: bytes) -> Tuple[Header, List[HDU]]:
         naxis = int(h.get("NAXIS", 0))
         dims = [int(h[f"NAXIS{i + 1}"]) for i in range(naxis)]
         bitpix = int(h["BITPIX"])
-        nbytes = (abs(bitpix) // 8) * int(h.get("GCOUNT", 1)) * (int(h.get("PCOUNT", 0)) +
-                                                                 (int(np.prod(dims)) if dims else 0))
+        # random groups (uvfits): NAXIS1 = 0, each of GCOUNT groups holds
+        # PCOUNT parameters then the product of NAXIS2.. values
+        groups = h.get("GROUPS") is True and naxis >= 1 and dims[0] == 0
+        gsize = int(h.get("PCOUNT", 0)) + ((int(np.prod(dims[1:])) if groups else int(np.prod(dims))) if dims else 0)
+        nbytes = (abs(bitpix) // 8) * int(h.get("GCOUNT", 1)) * gsize
         raw = buf[pos:pos + nbytes]
         if len(raw) < nbytes:
             raise FitsError("truncated data")
@@ -405,7 +414,11 @@ def decode(buf: bytes) -> Tuple[Header, List[HDU]]:
             if h.get("SIMPLE") is not True:
                 raise FitsError("not a FITS file (no SIMPLE = T)")
             primary = h
-            if dims:
+            if groups:
+                # [GCOUNT][PCOUNT + values]; parameters unscaled (PSCAL / PZERO are the caller's)
+                hdus.append(HDU(h, np.frombuffer(raw, _BITPIX[bitpix]).reshape(int(h.get("GCOUNT", 1)), gsize).astype(
+                    np.dtype(_BITPIX[bitpix]).newbyteorder("=")), "GROUPS"))
+            elif dims:
                 hdus.append(HDU(h, np.frombuffer(raw, _BITPIX[bitpix]).reshape(dims[::-1]).astype(
                     np.dtype(_BITPIX[bitpix]).newbyteorder("=")), "PRIMARY"))
             continue

@@ -20,6 +20,13 @@ test time.
   measured by compiling layout_probe.py's probe against the reference's
   src/gpu/types.h (FP64 build), and the parameter types of the reference's
   drop-in C functions as defined in src/gpu/{model,peel,utils}.cu.
+* uvfits_sdc3.json -- the content of the reference's one uvfits test file
+  (test_files/sdc3/sdc3_0000.uvfits: one timestep, one channel, XX only, one
+  cross-correlation, 512 stations of SKA-Low with ARRAYX/Y/Z zero as casacore
+  writes them) as its primary header card images, the group's values, and the
+  AN table's keywords and the three columns a reader uses (ANNAME, STABXYZ,
+  NOSTA), so that the test can rebuild the file; with the reference's expected
+  values from src/io/read/uvfits/tests.rs:909-958 (test_sdc3).
 * shapelet_basis_samples.json -- samples of the shapelet basis table produced
   by the reference's generator script src/model/make_shapelet_basis_values.py
   (imported, its gen_shape_basis evaluated at the sampled points), plus the
@@ -176,6 +183,40 @@ def layouts(ref_root: str) -> None:
          "layouts": lp.probe(gpu / "types.h"), "prototypes": protos}, indent=1) + "\n")
 
 
+def uvfits_sdc3(ref_root):
+    """The sdc3 uvfits file's headers, data and AN rows (see the module
+    docstring), read with this package's FITS layer."""
+    sys.path.insert(0, str(HERE.parents[1]))
+    from mwa_hyperdrive_b200 import fits
+
+    path = Path(ref_root) / "test_files" / "sdc3" / "sdc3_0000.uvfits"
+    raw = path.read_bytes()
+    h, hdus = fits.decode(raw)
+    cards = []
+    for k in range(0, len(h.encode()), 80):
+        c = h.encode()[k:k + 80].decode("ascii")
+        if c.strip():
+            cards.append(c)
+    # the AN table's keywords (its column definitions are rebuilt from the
+    # three columns a reader needs) and rows; the FQ table is not needed
+    an = fits.find(hdus, "AIPS AN")
+    hc = [an.header.encode()[k:k + 80].decode("ascii") for k in range(0, len(an.header.encode()), 80)]
+    skip = ("XTENSION", "BITPIX", "NAXIS", "PCOUNT", "GCOUNT", "TFIELDS", "TTYPE", "TFORM", "TUNIT", "EXTNAME", "END")
+    keys = [c for c in hc if c.strip() and not c.startswith(skip)]
+    tables = [{"name": "AIPS AN", "cards": keys,
+               "columns": [["ANNAME", "8A"], ["STABXYZ", "3D"], ["NOSTA", "1J"]],
+               "data": {"ANNAME": list(an.data["ANNAME"]), "STABXYZ": np.asarray(an.data["STABXYZ"]).tolist(),
+                        "NOSTA": np.asarray(an.data["NOSTA"]).tolist()}}]
+    groups = [x for x in hdus if x.kind == "GROUPS"][0]
+    (HERE / "uvfits_sdc3.json").write_text(json.dumps({
+        "source": "test_files/sdc3/sdc3_0000.uvfits; expected values: src/io/read/uvfits/tests.rs:909-958",
+        "primary_cards": cards, "groups": groups.data.astype(np.float64).tolist(), "tables": tables,
+        "expected": {"num_timestamps": 1, "num_fine_chans": 1, "longitude_deg": 116.76372382627274,
+                     "latitude_deg": -26.824419317822766, "height_m": -10.401579822123448, "epsilon": 1e-8,
+                     "polarisations": "XX", "flagged_tiles": list(range(2, 512)),
+                     "vis_xx": [-8.517027, -7.5777674], "weight": 1.0}}) + "\n")
+
+
 if __name__ == "__main__":
     import os
 
@@ -184,3 +225,4 @@ if __name__ == "__main__":
         sys.exit("usage: make_golden.py <mwa_hyperdrive source root> (or set HDC_REFERENCE_DIR)")
     main(root)
     layouts(root)
+    uvfits_sdc3(root)
