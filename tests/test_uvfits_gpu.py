@@ -59,7 +59,9 @@ def test_uvfits_to_solutions(tmp_path, ant2_minus_ant1):
                                 torch.from_numpy(model.astype(np.float32)).cuda(), dj, (0, nt), 200, 1e-8, 1e-4,
                                 form="plain")
         sols.append(dj.cpu().numpy())
-    np.testing.assert_array_equal(sols[0], sols[1])
+    # the same inputs: equal up to the order of the solver's shared-memory
+    # atomic sums (not fixed from run to run)
+    np.testing.assert_allclose(sols[0], sols[1], rtol=1e-12, atol=1e-15)
     ref, _ = O.calibrate_timeblock(data.astype(np.float64), model.astype(np.float32).astype(np.float64), start, 0, nt,
                                    200, 1e-8, 1e-4, 0)
     fin = np.isfinite(ref)
