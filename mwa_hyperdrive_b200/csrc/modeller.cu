@@ -595,7 +595,7 @@ int Modeller::model_channels(double lst, void* d_vis, bool out64, int f0, int nf
             TensorBeam tbm = {t[0].d_B, tb.d_tile_map, tb.d_freq_map + f0, tb.n_uniq_tile, tb.n_uniq_freq};
             const int rc = launch_tensor_points(nfc, nbl, ntiles, t[0].nc, d_freqs + f0, d_xyzs, lst - pc.ra, pc.dec,
                                                 t[0].d_lmn, weights(0) + (size_t)f0 * t[0].nc,
-                                                tile_beams() ? &tbm : nullptr, vis, out64, ws, d_err, s);
+                                                tile_beams() ? &tbm : nullptr, vis, out64, ws, d_err, s, tensor_sync());
             if (rc) return rc;
         } else {
             // the chosen (tensor) form keeps Gaussians and shapelets in the

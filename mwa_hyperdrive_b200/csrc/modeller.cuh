@@ -101,6 +101,7 @@ struct Modeller {
     int autos(double lst, JonesF32* d_vis, cudaStream_t s);
     int tensor_setup();
     void* tensor_workspace(bool out64);
+    TensorSync* tensor_sync();  // the tensor predict's second stream (NULL: none)
     void tensor_release();
     ~Modeller();
 };

@@ -1109,7 +1109,7 @@ extern "C" const char* model_points_tc(const Points* comps, const Addresses* a, 
     size_t off_gp = align256(off_w + (d_beam_jones && !tile_beam ? sizeof(JonesF64) * (size_t)nf * nc : 0));
     size_t off_map = align256(off_gp + sizeof(double4) * nc);
     size_t off_ws = align256(off_map + sizeof(int) * (size_t)ntiles);
-    size_t total = align256(off_ws + tensor_workspace_bytes(nf, nbl, ntiles, nc, tile_beam, false));
+    size_t total = align256(off_ws + tensor_workspace_bytes(nf, nbl, ntiles, nc, tile_beam, false, false));
     char* ws = (char*)device_scratch(total);
     if (!ws) return "out of device memory";
     PrepIn in = {};
@@ -1149,7 +1149,7 @@ extern "C" const char* model_points_tc(const Points* comps, const Addresses* a, 
     if (!errw) return "device error word unavailable";
     const int rc = launch_tensor_points(nf, nbl, ntiles, nc, a->d_freqs, d_tile_xyzs, lst_rad - phase_centre.ra,
                                         phase_centre.dec, in.lmn, W, tile_beam ? &tb : nullptr, d_vis_fb, false,
-                                        ws + off_ws, errw, 0);
+                                        ws + off_ws, errw, 0, nullptr);
     if (rc) return hdc_last_error();
     return take_word_sync(errw, "model_points_tc");
 }

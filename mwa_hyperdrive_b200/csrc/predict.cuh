@@ -72,14 +72,26 @@ struct TensorBeam {
     int n_uniq_freq;
 };
 
+// A second stream and its events, with which the tensor predict of a shared
+// beam writes the next chunk's table while the Gram kernel of the current
+// chunk runs (two tables in the workspace).  One per caller: not shared
+// between concurrent calls.
+struct TensorSync {
+    cudaStream_t ts = nullptr;
+    cudaEvent_t start = nullptr, table_done[2] = {nullptr, nullptr}, gram_done[2] = {nullptr, nullptr};
+};
+int tensor_sync_init(TensorSync& t);
+void tensor_sync_free(TensorSync& t);
+
 // The tensor-core point predict of one timestep (csrc/tensor.cu): d_W is
 // B S B^H [nf][nc] with a beam shared by all tiles (beam NULL), or S [nf][nc]
 // with per-tile beams.  ws: tensor_workspace_bytes(nf, nbl, ntiles, nc,
-// per-tile beams, out64) bytes.
-size_t tensor_workspace_bytes(int nf, int nbl, int ntiles, int nc, bool tile_beam, bool out64);
+// per-tile beams, out64, sync != NULL) bytes; sync NULL runs every kernel
+// on s in turn.
+size_t tensor_workspace_bytes(int nf, int nbl, int ntiles, int nc, bool tile_beam, bool out64, bool two_tables);
 int launch_tensor_points(int nf, int nbl, int ntiles, int nc, const double* d_freqs, const XYZ* d_xyzs, double ha,
                          double dec, const double4* d_lmn, const JonesF64* d_W, const TensorBeam* beam, void* d_vis,
-                         bool out64, void* ws, int* d_err, cudaStream_t s);
+                         bool out64, void* ws, int* d_err, cudaStream_t s, TensorSync* sync);
 
 struct AutosParams {
     int ntiles, nf;

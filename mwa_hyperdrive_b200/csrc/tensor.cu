@@ -833,25 +833,31 @@ __global__ void __launch_bounds__(BOUND_THREADS) weight_bound_kernel(const __gri
     }
 }
 
-// MODE 2 table of one pass: grid (stages, row blocks, channels of the
-// chunk), 256 threads.  Thread (row, kh) takes tile 128 rb + row and the
-// stage's components 16 kh .. 16 kh + 15: their phasors A (the same FP64
-// phase and FP32 polynomials as the in-kernel forms), the 16-byte chunk
-// (row, kh) of each of the six A planes (3 digits of re and im, the
-// encoding of y above), and the FP32 (cos, sin) row of the tile's column block, staged
-// in shared memory (rows padded to 272 bytes: conflict-free) so that every
-// warp store to the table is 512 contiguous bytes.  The CTAs of row block 0
-// also write the stage's W sx of each polarisation.
+// MODE 2 table of one pass: grid (stages, 2 x row blocks, channels of the
+// chunk), TT = 128 threads; CTA (k, 2 rb + half, f) takes the 64 tiles
+// 128 rb + 64 half .. of stage k, i.e. one column block.  Thread (row, kh)
+// takes tile 128 rb + 64 half + row and the stage's components 16 kh ..
+// 16 kh + 15: their phasors A (the same FP64 phase and FP32 polynomials as
+// the in-kernel forms), the 16-byte chunk of each of the six A planes (3
+// digits of re and im, the encoding of y above), and the FP32 (cos, sin) row
+// of the tile, staged in shared memory (rows padded to 272 bytes:
+// conflict-free) so that every warp store to the table is 512 contiguous
+// bytes.  The first CTAs of a stage also write its W sx of each
+// polarisation.  A CTA this small (17 KB of shared memory) fits on an SM
+// beside a Gram CTA, so the next chunk's table can be written while the
+// Gram kernel of this one runs.
+constexpr int TT = 128;
 constexpr int TROW = PH_ROW + 16;
-__global__ void __launch_bounds__(256) phasor_table_kernel(const __grid_constant__ Params P) {
-    __shared__ __align__(16) unsigned char phs[NT * TROW];
+__global__ void __launch_bounds__(TT) phasor_table_kernel(const __grid_constant__ Params P) {
+    __shared__ __align__(16) unsigned char phs[NH * TROW];
     __shared__ double2 lm_s[KC];
     __shared__ double n_s[KC];
-    const int k = blockIdx.x, rb = blockIdx.y, fl = blockIdx.z;
+    const int k = blockIdx.x, rb = blockIdx.y >> 1, half = blockIdx.y & 1, fl = blockIdx.z;
     const int f = P.f0 + fl;
     const int t = threadIdx.x;
-    const int row = t >> 1, kh = t & 1;
-    const int tile = NT * rb + row;
+    const int row = t >> 1, kh = t & 1;            // row of the 64
+    const int brow = NH * half + row;              // row of the 128-row block
+    const int tile = NT * rb + brow;
     const double oq = 4.0 * P.freqs[f] / VEL_C;
     double u, v, w;
     tile_uvw(P, tile, oq, u, v, w);
@@ -871,9 +877,9 @@ __global__ void __launch_bounds__(256) phasor_table_kernel(const __grid_constant
         }
         lm_s[t] = a;
         n_s[t] = nn;
-    } else if (rb == 0 && t >= 128 && t < 128 + 3 * KC) {
-        // W sx of polarisation p (XX, YY, XY) for component t % 32 of the stage
-        const int p = (t - 128) / KC, cl = (t - 128) % KC, c = k * KC + cl;
+    } else if (blockIdx.y == 0 && t < KC + 3 * KC) {
+        // W sx of polarisation p (XX, YY, XY) for component cl of the stage
+        const int p = (t - KC) / KC, cl = (t - KC) % KC, c = k * KC + cl;
         const double bound = reinterpret_cast<const double*>(tch + P.tab_bound_off)[p];
         const float sx = bound > 0.0 ? (float)(FULL31 / bound) : 0.f;
         float2 o = make_float2(0.f, 0.f);
@@ -902,7 +908,7 @@ __global__ void __launch_bounds__(256) phasor_table_kernel(const __grid_constant
         }
         *reinterpret_cast<float4*>(phs + row * TROW + kh * 128 + j * 8) = make_float4(ph[0].x, ph[0].y, ph[1].x, ph[1].y);
     }
-    unsigned char* pb = blk + (size_t)rb * PL_BYTES + chunk_off(row, kh);
+    unsigned char* pb = blk + (size_t)rb * PL_BYTES + chunk_off(brow, kh);
 #pragma unroll
     for (int part = 0; part < 2; part++) {
         uint32_t d[3][4];  // [digit][word of 4 components]
@@ -920,16 +926,17 @@ __global__ void __launch_bounds__(256) phasor_table_kernel(const __grid_constant
             *reinterpret_cast<uint4*>(pb + (part * 3 + dg) * XT_BYTES) = make_uint4(d[dg][0], d[dg][1], d[dg][2], d[dg][3]);
     }
     __syncthreads();
-    // phasor rows of column blocks 2 rb and 2 rb + 1 (those that exist):
-    // 16-byte unit i of the 128 rows x 256 bytes
-    const int nrows = (P.ncb - 2 * rb) * NH < NT ? (P.ncb - 2 * rb) * NH : NT;
-    unsigned char* pdst = blk + P.tab_ph_off + (size_t)(2 * rb) * PH_BYTES;
+    // the phasor rows of column block 2 rb + half (if it exists): 16-byte
+    // unit i of its 64 rows x 256 bytes
+    const int cbt = 2 * rb + half;
+    if (cbt < P.ncb) {
+        unsigned char* pdst = blk + P.tab_ph_off + (size_t)cbt * PH_BYTES;
 #pragma unroll
-    for (int i = t; i < NT * (PH_ROW / 16); i += 256) {
-        const int rr = i / (PH_ROW / 16), uu = i % (PH_ROW / 16);
-        if (rr < nrows)
+        for (int i = t; i < NH * (PH_ROW / 16); i += TT) {
+            const int rr = i / (PH_ROW / 16), uu = i % (PH_ROW / 16);
             *reinterpret_cast<float4*>(pdst + (size_t)rr * PH_ROW + uu * 16) =
                 *reinterpret_cast<const float4*>(phs + rr * TROW + uu * 16);
+        }
     }
 }
 
@@ -1046,14 +1053,14 @@ static TableShape table_shape(int nf, int ntiles, int cn, int njobs) {
 // Bytes of device workspace the tensor predict needs for nf channels of
 // nc components: the four planes, the MODE 1 per-channel bounds and, with
 // a shared beam, the MODE 2 table of one chunk of channels.
-size_t tensor_workspace_bytes(int nf, int nbl, int ntiles, int nc, bool tile_beam, bool out64) {
+size_t tensor_workspace_bytes(int nf, int nbl, int ntiles, int nc, bool tile_beam, bool out64, bool two_tables) {
     const size_t planes = (size_t)4 * nf * nbl * (out64 ? 16 : 8);
     size_t bytes = ((planes + 255) & ~(size_t)255) + ((2 * sizeof(double) * (size_t)nf + 255) & ~(size_t)255);
     if (!tile_beam && nc > 0 && nf > 0) {
         std::vector<uint32_t> jobs(tc::MAXJOBS);
         const int nj = tc::build_jobs(ntiles, jobs.data());
         const tc::TableShape t = tc::table_shape(nf, ntiles, std::min(nc, tc::Cfg<2>::KPASS), nj);
-        bytes += (size_t)t.chunk * t.chan;
+        bytes += (two_tables && t.chunk < nf ? 2 : 1) * (size_t)t.chunk * t.chan;
     }
     return bytes + 256;
 }
@@ -1062,7 +1069,29 @@ struct TensorState {
     bool configured = false;
     void* ws = nullptr;
     size_t ws_bytes = 0;
+    TensorSync sync;
+    bool sync_ok = false, sync_failed = false;
 };
+
+int tensor_sync_init(TensorSync& t) {
+    HDC_CUDA_RET_INT(cudaStreamCreateWithFlags(&t.ts, cudaStreamNonBlocking));
+    HDC_CUDA_RET_INT(cudaEventCreateWithFlags(&t.start, cudaEventDisableTiming));
+    for (int b = 0; b < 2; b++) {
+        HDC_CUDA_RET_INT(cudaEventCreateWithFlags(&t.table_done[b], cudaEventDisableTiming));
+        HDC_CUDA_RET_INT(cudaEventCreateWithFlags(&t.gram_done[b], cudaEventDisableTiming));
+    }
+    return HDC_OK;
+}
+
+void tensor_sync_free(TensorSync& t) {
+    for (int b = 0; b < 2; b++) {
+        if (t.table_done[b]) cudaEventDestroy(t.table_done[b]);
+        if (t.gram_done[b]) cudaEventDestroy(t.gram_done[b]);
+    }
+    if (t.start) cudaEventDestroy(t.start);
+    if (t.ts) cudaStreamDestroy(t.ts);
+    t = TensorSync();
+}
 
 int tensor_configure() {
     static std::once_flag once;
@@ -1102,10 +1131,14 @@ int Modeller::tensor_setup() {
 // per-tile beams in `beam`), tile XYZs, hour angle and declination of the
 // phase centre; accumulates into vis [nf][nbl] (JonesF32, or JonesF64 with
 // out64).  ws: tensor_workspace_bytes(nf, nbl, ntiles, nc, per-tile beams,
-// out64) bytes of device memory.
+// out64, sync != NULL) bytes of device memory.  With sync, the tables of a
+// shared beam alternate between two buffers and are written on sync->ts,
+// each chunk's Gram kernel (on s) waiting for its table and each table for
+// the Gram kernel that last read its buffer, so that writing the next
+// chunk's table overlaps the current Gram kernel.
 int launch_tensor_points(int nf, int nbl, int ntiles, int nc, const double* d_freqs, const XYZ* d_xyzs, double ha,
                          double dec, const double4* d_lmn, const JonesF64* d_W, const TensorBeam* beam, void* d_vis,
-                         bool out64, void* ws, int* d_err, cudaStream_t s) {
+                         bool out64, void* ws, int* d_err, cudaStream_t s, TensorSync* sync) {
     if (nc == 0 || nf == 0) return HDC_OK;
     int rc = tensor_configure();
     if (rc) return rc;
@@ -1140,8 +1173,9 @@ int launch_tensor_points(int nf, int nbl, int ntiles, int nc, const double* d_fr
     P.maxs = bounds + nf;
     P.err = d_err;
     P.f0 = 0;
-    P.table = static_cast<const unsigned char*>(ws) + planes_bytes +
-              ((2 * sizeof(double) * (size_t)nf + 255) & ~(size_t)255);
+    const unsigned char* table0 = static_cast<const unsigned char*>(ws) + planes_bytes +
+                                  ((2 * sizeof(double) * (size_t)nf + 255) & ~(size_t)255);
+    P.table = table0;
     P.tab_chan = P.tab_block = P.tab_ph_off = P.tab_w_off = P.tab_bound_off = 0;
     P.ncb = 0;
     const int kpass = tile_beam ? tc::Cfg<1>::KPASS : tc::Cfg<2>::KPASS;
@@ -1163,8 +1197,9 @@ int launch_tensor_points(int nf, int nbl, int ntiles, int nc, const double* d_fr
             count_launches(1);
             HDC_CUDA_RET_INT(cudaGetLastError());
         } else {
-            // the table of a chunk of channels, then their Gram products
-            // (one stream: the next chunk's table waits for these products)
+            // the table of a chunk of channels, then their Gram products;
+            // with sync the tables alternate between two buffers on the
+            // second stream
             const tc::TableShape t = tc::table_shape(nf, ntiles, std::min(nc, kpass), P.njobs);
             const int nstg = (P.cn + tc::KC - 1) / tc::KC;
             P.tab_block = t.block;
@@ -1173,15 +1208,30 @@ int launch_tensor_points(int nf, int nbl, int ntiles, int nc, const double* d_fr
             P.tab_chan = P.tab_bound_off + 32;
             P.tab_ph_off = (size_t)t.nrb * tc::PL_BYTES;
             P.ncb = t.ncb;
-            for (int f0 = 0; f0 < nf; f0 += t.chunk) {
+            const bool two = sync != nullptr && t.chunk < nf;
+            const unsigned char* buf[2] = {table0, table0 + (size_t)t.chunk * t.chan};
+            if (two) {
+                HDC_CUDA_RET_INT(cudaEventRecord(sync->start, s));
+                HDC_CUDA_RET_INT(cudaStreamWaitEvent(sync->ts, sync->start, 0));
+            }
+            for (int f0 = 0, i = 0; f0 < nf; f0 += t.chunk, i++) {
                 const int nch = std::min(t.chunk, nf - f0);
+                const int b = two ? (i & 1) : 0;
+                cudaStream_t tsx = two ? sync->ts : s;
                 P.f0 = f0;
-                tc::weight_bound_kernel<<<nch, tc::BOUND_THREADS, 0, s>>>(P);
+                P.table = buf[b];
+                // the buffer's previous reader is done
+                if (two && i >= 2) HDC_CUDA_RET_INT(cudaStreamWaitEvent(sync->ts, sync->gram_done[b], 0));
+                tc::weight_bound_kernel<<<nch, tc::BOUND_THREADS, 0, tsx>>>(P);
                 count_launches(1);
                 HDC_CUDA_RET_INT(cudaGetLastError());
-                tc::phasor_table_kernel<<<dim3(nstg, t.nrb, nch), 256, 0, s>>>(P);
+                tc::phasor_table_kernel<<<dim3(nstg, 2 * t.nrb, nch), tc::TT, 0, tsx>>>(P);
                 count_launches(1);
                 HDC_CUDA_RET_INT(cudaGetLastError());
+                if (two) {
+                    HDC_CUDA_RET_INT(cudaEventRecord(sync->table_done[b], sync->ts));
+                    HDC_CUDA_RET_INT(cudaStreamWaitEvent(s, sync->table_done[b], 0));
+                }
                 const dim3 grid(P.njobs, nch);
                 if (out64)
                     tc::gram_i8_kernel<2, true><<<grid, tc::Cfg<2>::THREADS, tc::Lay<2>::SMEM_BYTES, s>>>(P);
@@ -1189,6 +1239,7 @@ int launch_tensor_points(int nf, int nbl, int ntiles, int nc, const double* d_fr
                     tc::gram_i8_kernel<2, false><<<grid, tc::Cfg<2>::THREADS, tc::Lay<2>::SMEM_BYTES, s>>>(P);
                 count_launches(1);
                 HDC_CUDA_RET_INT(cudaGetLastError());
+                if (two) HDC_CUDA_RET_INT(cudaEventRecord(sync->gram_done[b], s));
             }
             P.f0 = 0;
         }
@@ -1205,7 +1256,7 @@ int launch_tensor_points(int nf, int nbl, int ntiles, int nc, const double* d_fr
 
 // The modeller's workspace for the tensor predict of up to nf channels.
 void* Modeller::tensor_workspace(bool out64) {
-    const size_t need = tensor_workspace_bytes(nf, nbl, ntiles, t[0].nc, tile_beams(), out64);
+    const size_t need = tensor_workspace_bytes(nf, nbl, ntiles, t[0].nc, tile_beams(), out64, tensor_sync() != nullptr);
     if (tc->ws_bytes < need) {
         if (tc->ws) cudaFree(tc->ws);
         tc->ws = nullptr;
@@ -1220,7 +1271,25 @@ void* Modeller::tensor_workspace(bool out64) {
     return tc->ws;
 }
 
+// The modeller's second stream for the tensor predict (created on first
+// use; NULL if that failed: the predict then runs on one stream).
+TensorSync* Modeller::tensor_sync() {
+    if (!tc) return nullptr;
+    if (!tc->sync_ok) {
+        if (tc->sync_failed) return nullptr;
+        if (tensor_sync_init(tc->sync) != HDC_OK) {
+            cudaGetLastError();
+            tensor_sync_free(tc->sync);
+            tc->sync_failed = true;
+            return nullptr;
+        }
+        tc->sync_ok = true;
+    }
+    return &tc->sync;
+}
+
 void Modeller::tensor_release() {
+    if (tc && tc->sync_ok) tensor_sync_free(tc->sync);
     if (tc && tc->ws) cudaFree(tc->ws);
     delete tc;
     tc = nullptr;
