@@ -401,10 +401,11 @@ __global__ void __launch_bounds__(DT) direct_kernel(const DirectParams p) {
 // for the exponent).  The arithmetic per channel is that of the FAST
 // direct_kernel above, except that the accumulation uses W's Hermitian
 // symmetry (a shared beam).  Channels per thread and CTAs per SM by type
-// (Gaussians 1, shapelets 2).
+// (Gaussians 1: 4 channels, 2 CTAs per SM; shapelets 2: 2 channels, 3 CTAs
+// per SM; chosen by timing).
 template <int TYPE>
 struct FastShape {
-    static constexpr int FCH = 3;
+    static constexpr int FCH = 4;
     static constexpr int MIN_CTAS = 2;
     static constexpr int CHUNK = 64;
 };
