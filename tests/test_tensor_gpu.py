@@ -226,6 +226,30 @@ def test_full_mixed_config_chosen_form_vs_fp64_oracle(oracle, ctype, name):
     assert nrm < TOL and p999 < TOL, (nrm, p999, mx)
 
 
+def test_host_buffer_call_equals_device_call():
+    """The trait's host-buffer call -- the channels in five chunks pipelined
+    over three streams, the points' tables on a second stream -- accumulates
+    exactly the device call's visibilities into the caller's buffer (the
+    timed configuration, one timestep, every component class)."""
+    obs, sky = synth.config2()
+    m = SkyModeller(sky, obs.tile_xyzs, obs.freqs, obs.phase_centre, obs.latitude, beam="analytic", form="tensor")
+    lst = float(obs.lsts[1])
+    dev = torch.zeros((obs.freqs.size, obs.num_baselines, 8), dtype=torch.float32, device="cuda")
+    m.model_timestep_with(lst, dev, return_uvws=False)
+    want = dev.cpu().numpy()
+    host = np.zeros((obs.freqs.size, obs.num_baselines, 8), np.float32)
+    m.model_timestep_with_host(lst, host)
+    np.testing.assert_array_equal(host, want)
+    # accumulation into what the buffer held: the additions' order differs
+    # from the device call's, so equal to FP32 rounding at the visibilities'
+    # scale (2 ulp of the largest magnitude)
+    host = np.full((obs.freqs.size, obs.num_baselines, 8), 0.5, np.float32)
+    m.model_timestep_with_host(lst, host)
+    m.close()
+    tol = 2 * float(np.spacing(np.float32(np.abs(want).max())))
+    np.testing.assert_allclose(host, want + np.float32(0.5), rtol=0, atol=tol)
+
+
 @pytest.mark.parametrize("ntiles,npts", [(130, 200), (144, 300), (256, 150), (300, 64)])
 def test_more_than_128_tiles(oracle, ntiles, npts):
     """Any tile count: the products run in blocks of 128 rows x 64 columns
