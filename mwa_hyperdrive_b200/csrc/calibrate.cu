@@ -304,21 +304,6 @@ __device__ __forceinline__ double row_reduce_scatter16(const J2& t, const Herm& 
 // groups of 256 (one per parity of the row block) on one shared ring.
 __host__ __device__ constexpr int cal_threads(int form) { return form == HDC_CAL_COLLAPSED_F32 ? 2 * CT : CT; }
 
-// barrier 1 + grp over one group of 256 threads; true when any passed true
-__device__ __forceinline__ bool group_sync_or(bool v, int grp) {
-    int r;
-    asm volatile(
-        "{\n\t.reg .pred p, q;\n\t"
-        "setp.ne.b32 p, %1, 0;\n\t"
-        "bar.red.or.pred q, %2, 256, p;\n\t"
-        "selp.b32 %0, 1, 0, q;\n\t}"
-        : "=r"(r)
-        : "r"((int)v), "r"(1 + grp)
-        : "memory");
-    return r != 0;
-}
-__device__ __forceinline__ void group_sync(int grp) { asm volatile("bar.sync %0, 256;" ::"r"(1 + grp) : "memory"); }
-
 template <int FORM>
 __global__ void __launch_bounds__(cal_threads(FORM)) mitchcal_kernel(const CalParams P) {
     constexpr int NTH = cal_threads(FORM);
@@ -343,8 +328,16 @@ __global__ void __launch_bounds__(cal_threads(FORM)) mitchcal_kernel(const CalPa
 
     // FP32 collapsed form: ring of nring covariance blocks after colbuf
     // (16-byte aligned for the bulk copies), one mbarrier per slot
+    // slot s holds sequence number ring_tag[s] (blocks are numbered in
+    // consumption order over all iterations): a waiter checks the tag before
+    // the phase parity, because the warps of one group can reach the next
+    // use of a slot while the other group's use in between is still pending,
+    // and a parity alone cannot tell two phases apart.  ring_rel counts the
+    // warps that have finished reading the slot's current block: the last of
+    // the group's warps refills it.
     __shared__ alignas(8) uint64_t ring_bar[4];
     __shared__ uint32_t ring_cnt[4];  // copies issued per slot
+    __shared__ uint32_t ring_tag[4], ring_rel[4];
     const bool use_ring = FORM == 2 && P.nring > 0;
     float* ring = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(colbuf + 16 * 16 * 12) + 15) & ~(uintptr_t)15);
     uint32_t jseq = 0;  // covariance blocks consumed so far (all threads alike)
@@ -360,6 +353,8 @@ __global__ void __launch_bounds__(cal_threads(FORM)) mitchcal_kernel(const CalPa
         for (int s = 0; s < P.nring; s++) {
             mbar_init(&ring_bar[s], 1);
             ring_cnt[s] = 1;  // the first copy, issued below
+            ring_tag[s] = (uint32_t)s;
+            ring_rel[s] = 0;
         }
         fence_barrier_init();
     }
@@ -457,7 +452,9 @@ __global__ void __launch_bounds__(cal_threads(FORM)) mitchcal_kernel(const CalPa
             // blocks pb = g, g + 2, ... of every column block, so the two
             // groups consume alternate ring slots; row sums of the two
             // groups go to different tiles, and both groups meet once per
-            // column block to reduce its column sums.
+            // column block to reduce its column sums.  Within a column block
+            // the warps do not meet: a row of the block belongs to one warp
+            // in every block, so each top/bot entry still has one writer.
             constexpr int NG = NTH / BLK;
             const int grp = tid / BLK, gt = tid % BLK;
             const int bi = gt >> 4, bj = gt & 15;
@@ -475,11 +472,12 @@ __global__ void __launch_bounds__(cal_threads(FORM)) mitchcal_kernel(const CalPa
                     const int blk = qb * (qb + 1) / 2 + pb;
                     J2 t1 = jzero(), t2 = jzero();
                     Herm h1{0, 0, {0, 0}}, h2{0, 0, {0, 0}};
+                    const uint32_t j = jseq + (uint32_t)blk;
+                    const int st = use_ring ? (int)(j % (uint32_t)P.nring) : 0;
                     if (use_ring) {
-                        const uint32_t j = jseq + (uint32_t)blk;
-                        const int st = (int)(j % (uint32_t)P.nring);
-                        const bool ok = mbar_wait_bounded(&ring_bar[st], (j / (uint32_t)P.nring) & 1u, P.err);
-                        if (NG > 1 ? group_sync_or(!ok, grp) : __syncthreads_or(!ok)) {
+                        const bool ok = tag_wait_bounded(&ring_tag[st], j, P.err) &&
+                                        mbar_wait_bounded(&ring_bar[st], (j / (uint32_t)P.nring) & 1u, P.err);
+                        if (__any_sync(0xffffffffu, !ok)) {
                             gabort = true;
                             break;
                         }
@@ -516,21 +514,24 @@ __global__ void __launch_bounds__(cal_threads(FORM)) mitchcal_kernel(const CalPa
                             bot[p].b.im += rs;
                     }
                     if (use_ring) {
-                        // the group has read this slot: refill it nring blocks ahead
-                        if (NG > 1)
-                            group_sync(grp);
-                        else
-                            __syncthreads();
-                        if (gt == 0) {
-                            const uint32_t j = jseq + (uint32_t)blk;
-                            const int st = (int)(j % (uint32_t)P.nring);
-                            const int nxt = (int)((j + (uint32_t)P.nring) % (uint32_t)P.nblk);
-                            fence_proxy_async_smem();  // generic reads of the slot before the async write
-                            atomicAdd(&ring_cnt[st], 1u);
-                            mbar_arrive_expect_tx(&ring_bar[st], NCOV * BLK * sizeof(float));
-                            bulk_g2s(ring + (size_t)st * NCOV * BLK,
-                                     static_cast<const float*>(P.cov) + ((size_t)ch * P.nblk + nxt) * NCOV * BLK,
-                                     NCOV * BLK * sizeof(float), &ring_bar[st]);
+                        // this warp has read the slot; the group's last warp
+                        // to finish it refills it nring blocks ahead (no
+                        // barrier: the other warps go on to their next block)
+                        __syncwarp();
+                        if (lane == 0) {
+                            __threadfence_block();  // this warp's reads before its count
+                            if (atomicAdd(&ring_rel[st], 1u) == (uint32_t)(BLK / 32 - 1)) {
+                                __threadfence_block();  // every warp's reads before the refill
+                                ring_rel[st] = 0;
+                                const int nxt = (int)((j + (uint32_t)P.nring) % (uint32_t)P.nblk);
+                                fence_proxy_async_smem();  // generic reads of the slot before the async write
+                                ring_cnt[st] += 1u;
+                                mbar_arrive_expect_tx(&ring_bar[st], NCOV * BLK * sizeof(float));
+                                bulk_g2s(ring + (size_t)st * NCOV * BLK,
+                                         static_cast<const float*>(P.cov) + ((size_t)ch * P.nblk + nxt) * NCOV * BLK,
+                                         NCOV * BLK * sizeof(float), &ring_bar[st]);
+                                st_release_smem(&ring_tag[st], j + (uint32_t)P.nring);
+                            }
                         }
                     }
                 }

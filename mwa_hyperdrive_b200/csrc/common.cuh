@@ -187,6 +187,32 @@ __device__ __forceinline__ bool mbar_wait_sleep(uint64_t* bar, uint32_t parity, 
     }
 }
 
+// A shared-memory word written with release and read with acquire (CTA
+// scope): a slot tag that says which sequence number a ring slot holds.
+__device__ __forceinline__ uint32_t ld_acquire_smem(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.acquire.cta.shared::cta.u32 %0, [%1];" : "=r"(v) : "r"(smem_u32(p)) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_smem(uint32_t* p, uint32_t v) {
+    asm volatile("st.release.cta.shared::cta.u32 [%0], %1;" ::"r"(smem_u32(p)), "r"(v) : "memory");
+}
+
+// Wait (bounded, as mbar_wait_bounded) until *tag == want.
+__device__ __forceinline__ bool tag_wait_bounded(const uint32_t* tag, uint32_t want, int* err,
+                                                 uint64_t limit_ns = 2000000000ull) {
+    if (ld_acquire_smem(tag) == want) return true;
+    const uint64_t t0 = global_timer_ns();
+    while (ld_acquire_smem(tag) != want) {
+        if (global_timer_ns() - t0 > limit_ns) {
+            if (err) atomicOr(err, KERR_TIMEOUT);
+            return false;
+        }
+        __nanosleep(32);
+    }
+    return true;
+}
+
 // After a bounded wait of a two-stage bulk-copy pipeline ran out at chunk k,
 // chunks [k, issued) may still be in flight: the issuing thread waits for
 // each of them (bounded again) so that no copy lands in the shared memory of
