@@ -198,36 +198,61 @@ __global__ void __launch_bounds__(BLK / 2) collapse_kernel(const CalParams P, T*
     }
 }
 
-template <typename T, bool SMEM>
-__device__ __forceinline__ double cov_ld(const T* p) {
-    if (SMEM)
-        return (double)*p;
-    else
-        return (double)__ldg(p);
+// Covariance component k of one lane: from global memory (read-only path),
+// or from a ring slot in shared memory through its 32-bit shared address
+// (explicit ld.shared: the slot's address is computed at run time, where a
+// generic load would be issued otherwise).
+template <typename T>
+struct CovGlobal {
+    const T* cv;
+    __device__ __forceinline__ double operator()(int k) const { return (double)__ldg(cv + (size_t)k * BLK); }
+};
+struct CovShared {
+    uint32_t base;  // shared address of component 0 of this lane
+    __device__ __forceinline__ double operator()(int k) const {
+        float v;
+        asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(base + (uint32_t)(k * BLK * sizeof(float))));
+        return (double)v;
+    }
+};
+
+// acc += x g (first: acc = x g), as two fused multiply-adds per part
+__device__ __forceinline__ void cmac(cplx& acc, cplx x, cplx g, bool first) {
+    acc.re = first ? x.re * g.re : fma(x.re, g.re, acc.re);
+    acc.im = first ? x.re * g.im : fma(x.re, g.im, acc.im);
+    acc.re = fma(-x.im, g.im, acc.re);
+    acc.im = fma(x.im, g.re, acc.im);
+}
+// acc += conj(x) g (first: acc = conj(x) g)
+__device__ __forceinline__ void cmac_conj(cplx& acc, cplx x, cplx g, bool first) {
+    acc.re = first ? x.re * g.re : fma(x.re, g.re, acc.re);
+    acc.im = first ? x.re * g.im : fma(x.re, g.im, acc.im);
+    acc.re = fma(x.im, g.im, acc.re);
+    acc.im = fma(-x.im, g.re, acc.im);
 }
 
-// One baseline's tile1 and tile2 contributions from its covariances (cv:
-// component k at cv[k * stride]), each entry read once:
+// One baseline's tile1 and tile2 contributions from its covariances
+// (component k from ld(k)), each entry read once:
 //   t1_ij = sum_kl X[ik][jl] G2_kl        t2_ij = sum_kl conj(X[ki][lj]) G1_kl
 //   h1_ij = sum_kl C[ik][jl] H2_kl        h2_ij = sum_kl C[lj][ki] H1_kl
 // With u = 2a + b, v = 2c + d an entry X[u][v] adds X G2[2b+d] to t1[2a+c]
 // and conj(X) G1[2a+c] to t2[2b+d]; C[u][v] (and its conjugate C[v][u])
 // adds C H2[2b+d] to h1[2a+c] and C H1[2c+a] to h2[2d+b]; only the bot
-// entries 00, 11 (real) and 01 are kept.
-template <typename T, bool SMEM>
-__device__ __forceinline__ void collapsed_terms(const T* cv, size_t stride, const J2& g1, const J2& g2,
-                                                const Herm& H1, const Herm& H2, J2& t1, J2& t2, Herm& h1,
-                                                Herm& h2) {
+// entries 00, 11 (real) and 01 are kept.  Every product is added with a
+// fused multiply-add; each accumulator starts from its first product.
+template <class LD>
+__device__ __forceinline__ void collapsed_terms(const LD& ld, const J2& g1, const J2& g2, const Herm& H1,
+                                                const Herm& H2, J2& t1, J2& t2, Herm& h1, Herm& h2) {
     const cplx G1[4] = {g1.a, g1.b, g1.c, g1.d}, G2[4] = {g2.a, g2.b, g2.c, g2.d};
-    cplx T1[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}}, T2[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
+    cplx T1[4], T2[4];
 #pragma unroll
     for (int u = 0; u < 4; u++)
 #pragma unroll
         for (int v = 0; v < 4; v++) {
-            const cplx x{cov_ld<T, SMEM>(cv + (size_t)(u * 4 + v) * stride),
-                         cov_ld<T, SMEM>(cv + (size_t)(16 + u * 4 + v) * stride)};
-            T1[(u >> 1) * 2 + (v >> 1)] = T1[(u >> 1) * 2 + (v >> 1)] + x * G2[(u & 1) * 2 + (v & 1)];
-            T2[(u & 1) * 2 + (v & 1)] = T2[(u & 1) * 2 + (v & 1)] + conj(x) * G1[(u >> 1) * 2 + (v >> 1)];
+            const cplx x{ld(u * 4 + v), ld(16 + u * 4 + v)};
+            // T1[2a+c] is first reached at b = d = 0, T2[2b+d] at a = c = 0
+            cmac(T1[(u >> 1) * 2 + (v >> 1)], x, G2[(u & 1) * 2 + (v & 1)], (u & 1) == 0 && (v & 1) == 0);
+            cmac_conj(T2[(u & 1) * 2 + (v & 1)], x, G1[(u >> 1) * 2 + (v >> 1)], u < 2 && v < 2);
         }
     t1 = J2{T1[0], T1[1], T1[2], T1[3]};
     t2 = J2{T2[0], T2[1], T2[2], T2[3]};
@@ -245,18 +270,25 @@ __device__ __forceinline__ void collapsed_terms(const T* cv, size_t stride, cons
         if (k == 0 || k == 3) {
             const double hr = k == 0 ? H.a : H.d;
             if (i == 1) {
-                r01.re += c.re * hr;
-                if (!creal) r01.im += c.im * hr;
+                r01.re = fma(c.re, hr, r01.re);
+                if (!creal) r01.im = fma(c.im, hr, r01.im);
             } else {
-                (i == 0 ? r00 : r11) += c.re * hr;
+                double& r = i == 0 ? r00 : r11;
+                r = fma(c.re, hr, r);
             }
         } else {
             const cplx h = k == 1 ? H.b : conj(H.b);
             if (i == 1) {
-                r01.re += creal ? c.re * h.re : c.re * h.re - c.im * h.im;
-                r01.im += creal ? c.re * h.im : c.re * h.im + c.im * h.re;
+                r01.re = fma(c.re, h.re, r01.re);
+                r01.im = fma(c.re, h.im, r01.im);
+                if (!creal) {
+                    r01.re = fma(-c.im, h.im, r01.re);
+                    r01.im = fma(c.im, h.re, r01.im);
+                }
             } else {
-                (i == 0 ? r00 : r11) += creal ? c.re * h.re : c.re * h.re - c.im * h.im;
+                double& r = i == 0 ? r00 : r11;
+                r = fma(c.re, h.re, r);
+                if (!creal) r = fma(-c.im, h.im, r);
             }
         }
     };
@@ -265,13 +297,12 @@ __device__ __forceinline__ void collapsed_terms(const T* cv, size_t stride, cons
         acc(b2_00, b2_11, b2_01, (v & 1) * 2 + (u & 1), c, creal, (v >> 1) * 2 + (u >> 1), H1);
     };
 #pragma unroll
-    for (int u = 0; u < 4; u++) add(u, u, cplx{cov_ld<T, SMEM>(cv + (size_t)(32 + u) * stride), 0.0}, true);
+    for (int u = 0; u < 4; u++) add(u, u, cplx{ld(32 + u), 0.0}, true);
 #pragma unroll
     for (int u = 0; u < 4; u++)
 #pragma unroll
         for (int v = u + 1; v < 4; v++) {
-            const cplx c{cov_ld<T, SMEM>(cv + (size_t)(36 + 2 * cpair(u, v)) * stride),
-                         cov_ld<T, SMEM>(cv + (size_t)(37 + 2 * cpair(u, v)) * stride)};
+            const cplx c{ld(36 + 2 * cpair(u, v)), ld(37 + 2 * cpair(u, v))};
             add(u, v, c, false);
             add(v, u, conj(c), false);
         }
@@ -482,16 +513,16 @@ __global__ void __launch_bounds__(cal_threads(FORM)) mitchcal_kernel(const CalPa
                             break;
                         }
                         if (p < q && q < n)
-                            collapsed_terms<float, true>(ring + (size_t)st * NCOV * BLK + gt, BLK, G[p], gq, Hs[p], hq,
-                                                         t1, t2, h1, h2);
+                            collapsed_terms(CovShared{smem_u32(ring + (size_t)st * NCOV * BLK + gt)}, G[p], gq, Hs[p],
+                                            hq, t1, t2, h1, h2);
                     } else if (p < q && q < n) {
                         const size_t off = ((size_t)ch * P.nblk + blk) * NCOV * BLK + gt;
                         if (FORM == 1)
-                            collapsed_terms<double, false>(static_cast<const double*>(P.cov) + off, BLK, G[p], gq,
-                                                           Hs[p], hq, t1, t2, h1, h2);
+                            collapsed_terms(CovGlobal<double>{static_cast<const double*>(P.cov) + off}, G[p], gq,
+                                            Hs[p], hq, t1, t2, h1, h2);
                         else
-                            collapsed_terms<float, false>(static_cast<const float*>(P.cov) + off, BLK, G[p], gq,
-                                                          Hs[p], hq, t1, t2, h1, h2);
+                            collapsed_terms(CovGlobal<float>{static_cast<const float*>(P.cov) + off}, G[p], gq, Hs[p],
+                                            hq, t1, t2, h1, h2);
                     }
                     c2 = c2 + t2;
                     ch2.a += h2.a;
