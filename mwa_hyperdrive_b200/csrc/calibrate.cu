@@ -88,6 +88,8 @@ struct Herm {  // [a b; conj(b) d], a and d real
     double a, d;
     cplx b;
 };
+// the iteration kernel adds row and column sums to a Herm as doubles 0..3
+static_assert(offsetof(Herm, d) == 8 && offsetof(Herm, b) == 16 && sizeof(Herm) == 32, "Herm layout");
 
 __device__ __forceinline__ J2 load_vis(const JonesF32* p) {
     const float4* q = reinterpret_cast<const float4*>(p);
@@ -239,30 +241,32 @@ __device__ __forceinline__ void cmac_conj(cplx& acc, cplx x, cplx g, bool first)
 // and conj(X) G1[2a+c] to t2[2b+d]; C[u][v] (and its conjugate C[v][u])
 // adds C H2[2b+d] to h1[2a+c] and C H1[2c+a] to h2[2d+b]; only the bot
 // entries 00, 11 (real) and 01 are kept.  Every product is added with a
-// fused multiply-add; each accumulator starts from its first product.
+// fused multiply-add.  t1 and h1 are this baseline's (each accumulator
+// starts from its first product); t2 and h2 are added straight into the
+// caller's running column sums c2 and ch2.
 template <class LD>
 __device__ __forceinline__ void collapsed_terms(const LD& ld, const J2& g1, const J2& g2, const Herm& H1,
-                                                const Herm& H2, J2& t1, J2& t2, Herm& h1, Herm& h2) {
+                                                const Herm& H2, J2& t1, Herm& h1, J2& c2, Herm& ch2) {
     const cplx G1[4] = {g1.a, g1.b, g1.c, g1.d}, G2[4] = {g2.a, g2.b, g2.c, g2.d};
-    cplx T1[4], T2[4];
+    cplx T1[4], T2[4] = {c2.a, c2.b, c2.c, c2.d};
 #pragma unroll
     for (int u = 0; u < 4; u++)
 #pragma unroll
         for (int v = 0; v < 4; v++) {
             const cplx x{ld(u * 4 + v), ld(16 + u * 4 + v)};
-            // T1[2a+c] is first reached at b = d = 0, T2[2b+d] at a = c = 0
+            // T1[2a+c] is first reached at b = d = 0
             cmac(T1[(u >> 1) * 2 + (v >> 1)], x, G2[(u & 1) * 2 + (v & 1)], (u & 1) == 0 && (v & 1) == 0);
-            cmac_conj(T2[(u & 1) * 2 + (v & 1)], x, G1[(u >> 1) * 2 + (v >> 1)], u < 2 && v < 2);
+            cmac_conj(T2[(u & 1) * 2 + (v & 1)], x, G1[(u >> 1) * 2 + (v >> 1)], false);
         }
     t1 = J2{T1[0], T1[1], T1[2], T1[3]};
-    t2 = J2{T2[0], T2[1], T2[2], T2[3]};
+    c2 = J2{T2[0], T2[1], T2[2], T2[3]};
     // bot accumulators: entry (u, v) = C[2a+b][2c+d] feeds b1[2a+c] with
     // H2[2b+d] and, read as C[2l+j][2k+i], b2[2i+j] with H1[2k+l].  The
     // results are Hermitian, so only entries 00 and 11 (real parts) and 01
     // are formed; every index below is a compile-time constant once the
     // loops are unrolled, so the unused terms are never computed.
-    double b1_00 = 0.0, b1_11 = 0.0, b2_00 = 0.0, b2_11 = 0.0;
-    cplx b1_01{0.0, 0.0}, b2_01{0.0, 0.0};
+    double b1_00 = 0.0, b1_11 = 0.0, b2_00 = ch2.a, b2_11 = ch2.d;
+    cplx b1_01{0.0, 0.0}, b2_01 = ch2.b;
     // r += c h for target entry i (0, 1, 3; 2 is not kept) and entry k of the
     // Hermitian H (0, 3 real; 1 = b; 2 = conj(b)); c real when creal
     auto acc = [](double& r00, double& r11, cplx& r01, int i, cplx c, bool creal, int k, const Herm& H) {
@@ -307,7 +311,7 @@ __device__ __forceinline__ void collapsed_terms(const LD& ld, const J2& g1, cons
             add(v, u, conj(c), false);
         }
     h1 = Herm{b1_00, b1_11, b1_01};
-    h2 = Herm{b2_00, b2_11, b2_01};
+    ch2 = Herm{b2_00, b2_11, b2_01};
 }
 
 // Sum of 12 values (t's 8 reals, then h's a, d, b.re, b.im) over the 16
@@ -329,6 +333,38 @@ __device__ __forceinline__ double row_reduce_scatter16(const J2& t, const Herm& 
         }
     }
     return v[0];
+}
+
+// The same sums (lane j of each half-warp gets the total of value j, j <
+// 12) through shared memory: the warp's own 128-byte segments of components
+// 0..23 of the ring slot it has just read (wbase: shared address of the
+// segment of component 0) hold the 12 values of its 32 lanes as rows of 16
+// doubles (row k + 12 r for value k of half-warp r); lane j of half-warp r
+// sums row j + 12 r, starting at column j so that the 12 lanes of a
+// half-warp hit different banks.  12 stores and 16 loads per lane in place
+// of the shuffles' 15 exchanges and 60 selects.
+__device__ __forceinline__ double row_sum_via_slot(uint32_t wbase, const J2& t, const Herm& h, int lane) {
+    const int r = lane >> 4, c = lane & 15;
+    const double v[12] = {t.a.re, t.a.im, t.b.re, t.b.im, t.c.re, t.c.im, t.d.re, t.d.im, h.a, h.d, h.b.re, h.b.im};
+    constexpr uint32_t ROW = BLK * sizeof(float);  // one component of the slot
+    __syncwarp();  // every lane's covariance reads before the stores over them
+#pragma unroll
+    for (int k = 0; k < 12; k++)
+        asm volatile("st.shared.f64 [%0], %1;" ::"r"(wbase + (uint32_t)(k + 12 * r) * ROW + (uint32_t)c * 8u),
+                     "d"(v[k])
+                     : "memory");
+    __syncwarp();
+    double s = 0.0;
+    if (c < 12) {
+        const uint32_t row = wbase + (uint32_t)(c + 12 * r) * ROW;
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            double x;
+            asm volatile("ld.shared.f64 %0, [%1];" : "=d"(x) : "r"(row + (uint32_t)((c + i) & 15) * 8u) : "memory");
+            s = i == 0 ? x : s + x;
+        }
+    }
+    return s;
 }
 
 // Threads per CTA of the iteration kernel: the FP32 collapsed form runs two
@@ -501,49 +537,40 @@ __global__ void __launch_bounds__(cal_threads(FORM)) mitchcal_kernel(const CalPa
                 for (int pb = grp; pb <= qb && !gabort; pb += NG) {
                     const int p = pb * 16 + bi;
                     const int blk = qb * (qb + 1) / 2 + pb;
-                    J2 t1 = jzero(), t2 = jzero();
-                    Herm h1{0, 0, {0, 0}}, h2{0, 0, {0, 0}};
+                    J2 t1 = jzero();
+                    Herm h1{0, 0, {0, 0}};
                     const uint32_t j = jseq + (uint32_t)blk;
-                    const int st = use_ring ? (int)(j % (uint32_t)P.nring) : 0;
+                    // the ring is 3 or 2 slots deep: constant divisors
+                    const int st = !use_ring ? 0 : P.nring == 3 ? (int)(j % 3u) : (int)(j & 1u);
                     if (use_ring) {
+                        const uint32_t ph = (P.nring == 3 ? j / 3u : j >> 1) & 1u;
                         const bool ok = tag_wait_bounded(&ring_tag[st], j, P.err) &&
-                                        mbar_wait_bounded(&ring_bar[st], (j / (uint32_t)P.nring) & 1u, P.err);
+                                        mbar_wait_bounded(&ring_bar[st], ph, P.err);
                         if (__any_sync(0xffffffffu, !ok)) {
                             gabort = true;
                             break;
                         }
                         if (p < q && q < n)
                             collapsed_terms(CovShared{smem_u32(ring + (size_t)st * NCOV * BLK + gt)}, G[p], gq, Hs[p],
-                                            hq, t1, t2, h1, h2);
+                                            hq, t1, h1, c2, ch2);
                     } else if (p < q && q < n) {
                         const size_t off = ((size_t)ch * P.nblk + blk) * NCOV * BLK + gt;
                         if (FORM == 1)
                             collapsed_terms(CovGlobal<double>{static_cast<const double*>(P.cov) + off}, G[p], gq,
-                                            Hs[p], hq, t1, t2, h1, h2);
+                                            Hs[p], hq, t1, h1, c2, ch2);
                         else
                             collapsed_terms(CovGlobal<float>{static_cast<const float*>(P.cov) + off}, G[p], gq, Hs[p],
-                                            hq, t1, t2, h1, h2);
+                                            hq, t1, h1, c2, ch2);
                     }
-                    c2 = c2 + t2;
-                    ch2.a += h2.a;
-                    ch2.d += h2.d;
-                    ch2.b = ch2.b + h2.b;
-                    // row sums over the 16 lanes of the block row, reduced
-                    // and scattered: after the four halving rounds lane bj
-                    // holds the total of value bj (15 shuffles instead of 48)
-                    const double rs = row_reduce_scatter16(t1, h1, bj);
-                    if (bj < 12 && p < n) {
-                        if (bj < 8)
-                            reinterpret_cast<double*>(&top[p])[bj] += rs;
-                        else if (bj == 8)
-                            bot[p].a += rs;
-                        else if (bj == 9)
-                            bot[p].d += rs;
-                        else if (bj == 10)
-                            bot[p].b.re += rs;
-                        else
-                            bot[p].b.im += rs;
-                    }
+                    // row sums over the 16 lanes of the block row: lane bj
+                    // gets the total of value bj (top's 8 reals, then bot's
+                    // a, d, b.re, b.im, which is Herm's field order)
+                    const double rs =
+                        use_ring ? row_sum_via_slot(smem_u32(ring + (size_t)st * NCOV * BLK + (gt & ~31)), t1, h1, lane)
+                                 : row_reduce_scatter16(t1, h1, bj);
+                    if (bj < 12 && p < n)
+                        *(bj < 8 ? reinterpret_cast<double*>(&top[p]) + bj : reinterpret_cast<double*>(&bot[p]) + (bj - 8)) +=
+                            rs;
                     if (use_ring) {
                         // this warp has read the slot; the group's last warp
                         // to finish it refills it nring blocks ahead (no
@@ -586,18 +613,9 @@ __global__ void __launch_bounds__(cal_threads(FORM)) mitchcal_kernel(const CalPa
                     double sum = 0.0;
 #pragma unroll
                     for (int w = 0; w < NTH / 32; w++) sum += colbuf[(w * 16 + jq) * 12 + k];
-                    if (qq < n) {
-                        if (k < 8)
-                            reinterpret_cast<double*>(&top[qq])[k] += sum;
-                        else if (k == 8)
-                            bot[qq].a += sum;
-                        else if (k == 9)
-                            bot[qq].d += sum;
-                        else if (k == 10)
-                            bot[qq].b.re += sum;
-                        else
-                            bot[qq].b.im += sum;
-                    }
+                    if (qq < n)
+                        *(k < 8 ? reinterpret_cast<double*>(&top[qq]) + k : reinterpret_cast<double*>(&bot[qq]) + (k - 8)) +=
+                            sum;
                 }
                 __syncthreads();
             }
