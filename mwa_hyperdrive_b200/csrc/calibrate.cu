@@ -367,6 +367,31 @@ __device__ __forceinline__ double row_sum_via_slot(uint32_t wbase, const J2& t, 
     return s;
 }
 
+// Barrier over one group of the iteration kernel (the whole CTA when it has
+// one group; else named barrier 1 + grp over its 256 threads); the _or form
+// returns true when any thread of the group passed true.
+template <int NG>
+__device__ __forceinline__ bool group_sync_or(bool v, int grp) {
+    if (NG == 1) return __syncthreads_or(v);
+    int r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.b32 p, %1, 0;\n\t"
+        "bar.red.or.pred q, %2, 256, p;\n\t"
+        "selp.b32 %0, 1, 0, q;\n\t}"
+        : "=r"(r)
+        : "r"((int)v), "r"(1 + grp)
+        : "memory");
+    return r != 0;
+}
+template <int NG>
+__device__ __forceinline__ void group_sync(int grp) {
+    if (NG == 1)
+        __syncthreads();
+    else
+        asm volatile("bar.sync %0, 256;" ::"r"(1 + grp) : "memory");
+}
+
 // Threads per CTA of the iteration kernel: the FP32 collapsed form runs two
 // groups of 256 (one per parity of the row block) on one shared ring.
 __host__ __device__ constexpr int cal_threads(int form) { return form == HDC_CAL_COLLAPSED_F32 ? 2 * CT : CT; }
@@ -385,6 +410,10 @@ __global__ void __launch_bounds__(cal_threads(FORM)) mitchcal_kernel(const CalPa
     int* failed = reinterpret_cast<int*>(prec + 4 * n);
     // collapsed form: 16 x 16 x 12 block-column partial sums (8-byte aligned)
     double* colbuf = reinterpret_cast<double*>(failed + ((n + 1) & ~1));
+    // FP32 collapsed form: the second group's own accumulators, added into
+    // top/bot once both groups have swept the blocks
+    J2* top1 = reinterpret_cast<J2*>(colbuf + 16 * 16 * 12);
+    Herm* bot1 = reinterpret_cast<Herm*>(top1 + (FORM == 2 ? n : 0));
 
     const int ch = P.chan_list ? P.chan_list[blockIdx.x] : blockIdx.x;
     const int tid = threadIdx.x, lane = tid & 31;
@@ -406,7 +435,7 @@ __global__ void __launch_bounds__(cal_threads(FORM)) mitchcal_kernel(const CalPa
     __shared__ uint32_t ring_cnt[4];  // copies issued per slot
     __shared__ uint32_t ring_tag[4], ring_rel[4];
     const bool use_ring = FORM == 2 && P.nring > 0;
-    float* ring = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(colbuf + 16 * 16 * 12) + 15) & ~(uintptr_t)15);
+    float* ring = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(bot1 + (FORM == 2 ? n : 0)) + 15) & ~(uintptr_t)15);
     uint32_t jseq = 0;  // covariance blocks consumed so far (all threads alike)
     bool abort_loop = false;
 
@@ -441,6 +470,10 @@ __global__ void __launch_bounds__(cal_threads(FORM)) mitchcal_kernel(const CalPa
         for (int i = tid; i < n; i += NTH) {
             top[i] = jzero();
             bot[i] = Herm{0.0, 0.0, {0.0, 0.0}};
+            if (FORM == 2) {
+                top1[i] = jzero();
+                bot1[i] = Herm{0.0, 0.0, {0.0, 0.0}};
+            }
             if (FORM != 0) {
                 Herm h{0.0, 0.0, {0.0, 0.0}};
                 add_zhz(h, G[i]);
@@ -515,17 +548,21 @@ __global__ void __launch_bounds__(cal_threads(FORM)) mitchcal_kernel(const CalPa
             // no atomics.  FP32 covariances arrive through the shared-memory
             // ring (bulk copies issued nring blocks ahead); FP64 ones are
             // loaded directly.
-            // FORM 2 runs two groups of 256 threads: group g takes the row
-            // blocks pb = g, g + 2, ... of every column block, so the two
-            // groups consume alternate ring slots; row sums of the two
-            // groups go to different tiles, and both groups meet once per
-            // column block to reduce its column sums.  Within a column block
-            // the warps do not meet: a row of the block belongs to one warp
-            // in every block, so each top/bot entry still has one writer.
+            // FORM 2 runs two groups of 256 threads: group g takes the
+            // blocks of odd or even storage index (18 each for 128 tiles),
+            // so the two groups consume alternate ring slots, and sums into
+            // its own accumulators (group 1: top1/bot1, added to top/bot
+            // after the sweep).  A group's warps meet once per column block
+            // to reduce its column sums (named barrier 1 + g); the groups
+            // meet only at the end of the sweep.  Within a column block the
+            // warps do not meet: a row of the block belongs to one warp in
+            // every block, so each accumulator entry has one writer.
             constexpr int NG = NTH / BLK;
             const int grp = tid / BLK, gt = tid % BLK;
             const int bi = gt >> 4, bj = gt & 15;
             const int nb = (n + 15) / 16;
+            J2* tacc = FORM == 2 && grp == 1 ? top1 : top;
+            Herm* bacc = FORM == 2 && grp == 1 ? bot1 : bot;
             bool gabort = false;
             for (int qb = 0; qb < nb; qb++) {
                 const int q = qb * 16 + bj;
@@ -534,7 +571,8 @@ __global__ void __launch_bounds__(cal_threads(FORM)) mitchcal_kernel(const CalPa
                 const Herm hq = q < n ? Hs[q] : Herm{0, 0, {0, 0}};
                 J2 c2 = jzero();
                 Herm ch2{0, 0, {0, 0}};
-                for (int pb = grp; pb <= qb && !gabort; pb += NG) {
+                // this group's blocks of the column: storage index = grp mod NG
+                for (int pb = NG == 1 ? 0 : (grp - qb * (qb + 1) / 2) & 1; pb <= qb && !gabort; pb += NG) {
                     const int p = pb * 16 + bi;
                     const int blk = qb * (qb + 1) / 2 + pb;
                     J2 t1 = jzero();
@@ -569,7 +607,7 @@ __global__ void __launch_bounds__(cal_threads(FORM)) mitchcal_kernel(const CalPa
                         use_ring ? row_sum_via_slot(smem_u32(ring + (size_t)st * NCOV * BLK + (gt & ~31)), t1, h1, lane)
                                  : row_reduce_scatter16(t1, h1, bj);
                     if (bj < 12 && p < n)
-                        *(bj < 8 ? reinterpret_cast<double*>(&top[p]) + bj : reinterpret_cast<double*>(&bot[p]) + (bj - 8)) +=
+                        *(bj < 8 ? reinterpret_cast<double*>(&tacc[p]) + bj : reinterpret_cast<double*>(&bacc[p]) + (bj - 8)) +=
                             rs;
                     if (use_ring) {
                         // this warp has read the slot; the group's last warp
@@ -603,21 +641,32 @@ __global__ void __launch_bounds__(cal_threads(FORM)) mitchcal_kernel(const CalPa
 #pragma unroll
                     for (int k = 0; k < 12; k++) cb[k] = cv2[k];
                 }
-                if (__syncthreads_or(gabort)) {
-                    abort_loop = true;
+                if (group_sync_or<NG>(gabort, grp)) {
+                    gabort = true;
                     break;
                 }
-                if (tid < 16 * 12) {
-                    const int jq = tid / 12, k = tid - jq * 12;
+                if (gt < 16 * 12) {
+                    const int jq = gt / 12, k = gt - jq * 12;
                     const int qq = qb * 16 + jq;
                     double sum = 0.0;
 #pragma unroll
-                    for (int w = 0; w < NTH / 32; w++) sum += colbuf[(w * 16 + jq) * 12 + k];
+                    for (int w = 0; w < BLK / 32; w++) sum += colbuf[((grp * (BLK / 32) + w) * 16 + jq) * 12 + k];
                     if (qq < n)
-                        *(k < 8 ? reinterpret_cast<double*>(&top[qq]) + k : reinterpret_cast<double*>(&bot[qq]) + (k - 8)) +=
+                        *(k < 8 ? reinterpret_cast<double*>(&tacc[qq]) + k : reinterpret_cast<double*>(&bacc[qq]) + (k - 8)) +=
                             sum;
                 }
-                __syncthreads();
+                group_sync<NG>(grp);
+            }
+            // both groups' sweeps done: fold group 1's sums into top/bot
+            if (__syncthreads_or(gabort)) {
+                abort_loop = true;
+            } else if (FORM == 2) {
+                for (int i = tid; i < n; i += NTH) {
+                    top[i] = top[i] + top1[i];
+                    bot[i].a += bot1[i].a;
+                    bot[i].d += bot1[i].d;
+                    bot[i].b = bot[i].b + bot1[i].b;
+                }
             }
             if (use_ring) jseq += (uint32_t)P.nblk;
             if (abort_loop) break;
@@ -862,7 +911,9 @@ int launch_judge(const JonesF32* d_data, const JonesF32* d_model, int t0, int t1
 static size_t smem_base_bytes(int n, int form) {
     const size_t base = (size_t)n * (3 * sizeof(J2) + 2 * sizeof(Herm) + 4 * sizeof(double)) +
                         sizeof(int) * (size_t)((n + 1) & ~1);
-    return base + (form != HDC_CAL_PLAIN ? 16 * 16 * 12 * sizeof(double) : 0);
+    // collapsed forms: column partial sums; FP32 form: group 1's accumulators
+    return base + (form != HDC_CAL_PLAIN ? 16 * 16 * 12 * sizeof(double) : 0) +
+           (form == HDC_CAL_COLLAPSED_F32 ? (size_t)n * (sizeof(J2) + sizeof(Herm)) : 0);
 }
 
 constexpr size_t SMEM_LIMIT = 227 * 1024;
