@@ -190,8 +190,13 @@ def compare_collapsed(oracle, data, model, dj0, t0, t1, form, max_iter=50, stop=
     return err
 
 
+# tile counts: one block (8), an odd number of blocks (20: 3), 128 (36 blocks,
+# a 3-slot shared-memory ring in the FP32 form), and above 155 tiles, where
+# the FP32 form's ring is 2 slots deep (200: 91 blocks; 256, the largest
+# array the kernel takes: 136 blocks)
 @pytest.mark.parametrize("form,tol", [("collapsed", 1e-9), ("collapsed_f32", 1e-6)])
-@pytest.mark.parametrize("ntiles,nt,nch,snr", [(8, 2, 5, None), (20, 4, 6, 10.0), (128, 14, 3, 10.0)])
+@pytest.mark.parametrize("ntiles,nt,nch,snr", [(8, 2, 5, None), (20, 4, 6, 10.0), (128, 14, 3, 10.0),
+                                               (200, 2, 2, 10.0), (256, 2, 2, 10.0)])
 def test_collapsed_forms_match_oracle(oracle, form, tol, ntiles, nt, nch, snr):
     rng = np.random.default_rng(ntiles + nt)
     nbl = ntiles * (ntiles - 1) // 2
