@@ -580,12 +580,20 @@ void Modeller::prof_collect() {
     ev_pending.clear();
 }
 
-int Modeller::model_channels(double lst, void* d_vis, bool out64, int f0, int nfc, cudaStream_t s) {
+int Modeller::model_channels(double lst, void* d_vis, bool out64, int f0, int nfc, cudaStream_t s, int types,
+                             bool mask) {
     EvPair e{};
     const size_t vis_off = (size_t)f0 * nbl * (out64 ? sizeof(JonesF64) : sizeof(JonesF32));
     void* vis = static_cast<char*>(d_vis) + vis_off;
-    for (int ty = 0; ty < 3; ty++) {
-        if (t[ty].nc == 0) continue;
+    // the reference's order (points, Gaussians, shapelets: the FP32 sums
+    // round as its do); the tensor form adds Gaussians, shapelets, then
+    // points, as its host-buffer call does (that call stages the first two and
+    // adds the points chunk by chunk)
+    static constexpr int REF_ORDER[3] = {0, 1, 2}, TENSOR_ORDER[3] = {1, 2, 0};
+    const int* order = form == HDC_PREDICT_TENSOR ? TENSOR_ORDER : REF_ORDER;
+    for (int k = 0; k < 3; k++) {
+        const int ty = order[k];
+        if (t[ty].nc == 0 || !(types & (1 << ty))) continue;
         prof_begin(ty, s, e);
         if (ty == 0 && form == HDC_PREDICT_TENSOR) {
             // the workspace holds planes for all nf channels; a chunk of nfc
@@ -610,7 +618,7 @@ int Modeller::model_channels(double lst, void* d_vis, bool out64, int f0, int nf
         }
         prof_end(s, e);
     }
-    if (!out64) HDC_CUDA_RET_INT(launch_mask_pols((JonesF32*)vis, (size_t)nfc * nbl, pols, s));
+    if (!out64 && mask) HDC_CUDA_RET_INT(launch_mask_pols((JonesF32*)vis, (size_t)nfc * nbl, pols, s));
     return HDC_OK;
 }
 
@@ -712,6 +720,7 @@ Modeller::~Modeller() {
     dfree(d_xyzs);
     dfree(d_uvws);
     dfree(d_host_vis);
+    dfree(d_host_model);
     tensor_release();
     for (EvPair& e : ev_pending) ev_free.push_back(e);
     for (EvPair& e : ev_free) {
@@ -979,6 +988,17 @@ extern "C" int hdc_modeller_model_timestep_with_host(HdcModeller* hm, double lst
         HDC_CUDA_RET_INT(cudaMalloc(&m->d_host_vis, bytes));
         m->host_vis_bytes = bytes;
     }
+    if (m->form == HDC_PREDICT_TENSOR && !m->tile_beams() && m->t[0].nc > 0 &&
+        m->t[0].nc <= hdc::tensor_single_pass() && (m->t[1].nc > 0 || m->t[2].nc > 0)) {
+        if (m->host_model_bytes < bytes) {
+            if (m->d_host_model) cudaFree(m->d_host_model);
+            m->d_host_model = nullptr;
+            m->host_model_bytes = 0;
+            HDC_CUDA_RET_INT(cudaMalloc(&m->d_host_model, bytes));
+            m->host_model_bytes = bytes;
+        }
+        return m->model_host_points_last(lst, h_vis, h_uvws, s);
+    }
     return m->model_host_pipelined(lst, h_vis, h_uvws, s);
 }
 
@@ -1044,6 +1064,73 @@ int Modeller::model_host_pipelined(double lst, JonesF32* h_vis, UVW* h_uvws, cud
         HDC_CUDA_RET_INT(cudaStreamWaitEvent(pipe_s[2], done[c], 0));
         HDC_CUDA_RET_INT(cudaMemcpyAsync(h_vis + off, d_host_vis + off, n, cudaMemcpyDeviceToHost, pipe_s[2]));
     }
+    if (h_uvws)
+        HDC_CUDA_RET_INT(cudaMemcpyAsync(h_uvws, d_uvws, sizeof(UVW) * nbl, cudaMemcpyDeviceToHost, pipe_s[2]));
+    rc = queue_error_check(pipe_s[1]);
+    if (rc) return rc;
+    HDC_CUDA_RET_INT(cudaEventRecord(fin, pipe_s[2]));
+    HDC_CUDA_RET_INT(cudaStreamWaitEvent(s, fin, 0));
+    HDC_CUDA_RET_INT(cudaStreamSynchronize(pipe_s[2]));
+    return take_error(true);
+}
+}  // namespace hdc
+
+namespace hdc {
+namespace {
+struct PointsLastCtx {
+    Modeller* m;
+    JonesF32* h_vis;
+    cudaEvent_t ev;
+};
+// a chunk's points are in: mask its pols, then download it on stream 2
+int points_last_chunk_done(void* vctx, int f0, int nch) {
+    PointsLastCtx* c = static_cast<PointsLastCtx*>(vctx);
+    Modeller* m = c->m;
+    const size_t off = (size_t)f0 * m->nbl, n = (size_t)nch * m->nbl;
+    HDC_CUDA_RET_INT(launch_mask_pols(m->d_host_vis + off, n, m->pols, m->pipe_s[1]));
+    // one event serves every chunk: a wait takes the record made before it
+    HDC_CUDA_RET_INT(cudaEventRecord(c->ev, m->pipe_s[1]));
+    HDC_CUDA_RET_INT(cudaStreamWaitEvent(m->pipe_s[2], c->ev, 0));
+    HDC_CUDA_RET_INT(cudaMemcpyAsync(c->h_vis + off, m->d_host_vis + off, n * sizeof(JonesF32),
+                                     cudaMemcpyDeviceToHost, m->pipe_s[2]));
+    return HDC_OK;
+}
+}  // namespace
+
+// Tensor form, shared beam: stream 0 uploads the whole buffer while stream 1
+// predicts the Gaussians and shapelets of every channel into d_host_model
+// (full-size grids); then the points run in their table chunks (whole waves
+// of the Gram kernel), each chunk's visibilities become buffer + staged
+// model + points and go back on stream 2 while the next chunk computes.
+int Modeller::model_host_points_last(double lst, JonesF32* h_vis, UVW* h_uvws, cudaStream_t s) {
+    if (!pipe_s[0]) {
+        for (int i = 0; i < 3; i++) HDC_CUDA_RET_INT(cudaStreamCreateWithFlags(&pipe_s[i], cudaStreamNonBlocking));
+        for (auto& ev : pipe_ev) HDC_CUDA_RET_INT(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    }
+    int rc = take_error(false);
+    if (rc) return rc;
+    cudaEvent_t start = pipe_ev[0], up = pipe_ev[1], fin = pipe_ev[2];
+    HDC_CUDA_RET_INT(cudaEventRecord(start, s));
+    for (int i = 0; i < 3; i++) HDC_CUDA_RET_INT(cudaStreamWaitEvent(pipe_s[i], start, 0));
+    const size_t bytes = (size_t)nf * nbl * sizeof(JonesF32);
+    HDC_CUDA_RET_INT(cudaMemcpyAsync(d_host_vis, h_vis, bytes, cudaMemcpyHostToDevice, pipe_s[0]));
+    HDC_CUDA_RET_INT(cudaEventRecord(up, pipe_s[0]));
+    rc = geometry(lst, pipe_s[1]);
+    if (rc) return rc;
+    HDC_CUDA_RET_INT(cudaMemsetAsync(d_host_model, 0, bytes, pipe_s[1]));
+    rc = model_channels(lst, d_host_model, false, 0, nf, pipe_s[1], 2 | 4, false);
+    if (rc) return rc;
+    HDC_CUDA_RET_INT(cudaStreamWaitEvent(pipe_s[1], up, 0));
+    void* ws = tensor_workspace(false);
+    if (!ws) return HDC_ERR_ALLOC;
+    PointsLastCtx ctx{this, h_vis, pipe_ev[3]};
+    const TensorChunkOut out{d_host_model, points_last_chunk_done, &ctx};
+    EvPair e{};
+    prof_begin(0, pipe_s[1], e);
+    rc = launch_tensor_points(nf, nbl, ntiles, t[0].nc, d_freqs, d_xyzs, lst - pc.ra, pc.dec, t[0].d_lmn, weights(0),
+                              nullptr, d_host_vis, false, ws, d_err, pipe_s[1], tensor_sync(), &out);
+    if (rc) return rc;
+    prof_end(pipe_s[1], e);
     if (h_uvws)
         HDC_CUDA_RET_INT(cudaMemcpyAsync(h_uvws, d_uvws, sizeof(UVW) * nbl, cudaMemcpyDeviceToHost, pipe_s[2]));
     rc = queue_error_check(pipe_s[1]);

@@ -62,6 +62,8 @@ struct Modeller {
     TileBeams tb;  // set when beam_kind == HDC_BEAM_ANALYTIC_PER_TILE
     JonesF32* d_host_vis = nullptr;
     size_t host_vis_bytes = 0;
+    JonesF32* d_host_model = nullptr;  // host-buffer call: Gaussians + shapelets staged here
+    size_t host_model_bytes = 0;
     TensorState* tc = nullptr;
 
     // Optional CUDA-event timing of each kernel class on the launching stream:
@@ -86,14 +88,23 @@ struct Modeller {
     DirectParams direct_params(int ty, void* vis) const;
     int model(double lst, void* d_vis, bool out64, UVW* h_uvws, cudaStream_t s);
     // the predict kernels of channels [f0, f0 + nfc) after geometry(); d_vis
-    // is the whole [nf][nbl] visibility array
-    int model_channels(double lst, void* d_vis, bool out64, int f0, int nfc, cudaStream_t s);
+    // is the whole [nf][nbl] visibility array.  Classes (types bit-set: 1
+    // points, 2 Gaussians, 4 shapelets) are added in the reference's order,
+    // or Gaussians, shapelets, points in the tensor form; the pol mask
+    // follows when mask is set.
+    int model_channels(double lst, void* d_vis, bool out64, int f0, int nfc, cudaStream_t s, int types = 7,
+                       bool mask = true);
     // host-buffer predict: upload, predict and download of channel chunks
     // overlap on three streams
     static constexpr int PIPE_CHUNKS = 5;
     cudaStream_t pipe_s[3] = {nullptr, nullptr, nullptr};
     cudaEvent_t pipe_ev[2 * PIPE_CHUNKS + 2] = {};
     int model_host_pipelined(double lst, JonesF32* h_vis, UVW* h_uvws, cudaStream_t s);
+    // the same for the tensor form with a shared beam: Gaussians and
+    // shapelets over all channels into d_host_model while the buffer
+    // uploads, then the points chunk by chunk, each chunk downloaded as soon
+    // as its points are in
+    int model_host_points_last(double lst, JonesF32* h_vis, UVW* h_uvws, cudaStream_t s);
     // model_timestep_with over baseline UVWs the caller computed (as the
     // reference's peel loop passes its own d_uvws, model/gpu.rs:1152-1166);
     // direct FP64 kernels, JonesF32 output.

@@ -89,9 +89,21 @@ void tensor_sync_free(TensorSync& t);
 // per-tile beams, out64, sync != NULL) bytes; sync NULL runs every kernel
 // on s in turn.
 size_t tensor_workspace_bytes(int nf, int nbl, int ntiles, int nc, bool tile_beam, bool out64, bool two_tables);
+// Per-chunk output of the table form (shared beam, nc <= tensor_single_pass()
+// components, JonesF32 output): after the Gram products of channels
+// [f0, f0 + nch) the chunk's visibilities become vis + model + planes (model:
+// [nf][nbl], added before the planes), and done(ctx, f0, nch) is called to
+// queue the chunk's further work on s; no whole-array combine follows.
+struct TensorChunkOut {
+    const JonesF32* model;
+    int (*done)(void* ctx, int f0, int nch);
+    void* ctx;
+};
+int tensor_single_pass();
 int launch_tensor_points(int nf, int nbl, int ntiles, int nc, const double* d_freqs, const XYZ* d_xyzs, double ha,
                          double dec, const double4* d_lmn, const JonesF64* d_W, const TensorBeam* beam, void* d_vis,
-                         bool out64, void* ws, int* d_err, cudaStream_t s, TensorSync* sync);
+                         bool out64, void* ws, int* d_err, cudaStream_t s, TensorSync* sync,
+                         const TensorChunkOut* chunk_out = nullptr);
 
 struct AutosParams {
     int ntiles, nf;

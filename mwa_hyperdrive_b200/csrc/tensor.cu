@@ -968,6 +968,28 @@ __global__ void combine_kernel(const void* planes, void* vis, size_t n) {
     }
 }
 
+// vis[i] = (vis[i] + model[i]) + the four planes, for i in [i0, i0 + cnt)
+// of n (the host-buffer call's chunks: the other classes' sum, staged in
+// model, goes in before the points, as the device call adds them first)
+__global__ void combine_model_kernel(const void* planes, JonesF32* vis, const JonesF32* model, size_t n, size_t i0,
+                                     size_t cnt) {
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= cnt) return;
+    const size_t i = i0 + k;
+    const float2* pl = reinterpret_cast<const float2*>(planes);
+    float4* v = reinterpret_cast<float4*>(vis + i);
+    const float4* m = reinterpret_cast<const float4*>(model + i);
+    const float2 xx = pl[i], xy = pl[n + i], yx = pl[2 * n + i], yy = pl[3 * n + i];
+    float4 a = v[0], b = v[1];
+    const float4 ma = m[0], mb = m[1];
+    a.x += ma.x, a.y += ma.y, a.z += ma.z, a.w += ma.w;
+    b.x += mb.x, b.y += mb.y, b.z += mb.z, b.w += mb.w;
+    a.x += xx.x, a.y += xx.y, a.z += xy.x, a.w += xy.y;
+    b.x += yx.x, b.y += yx.y, b.z += yy.x, b.w += yy.y;
+    v[0] = a;
+    v[1] = b;
+}
+
 // Per channel: the largest |entry| of the beam Jones over unique tiles and
 // components (at the channel's unique frequency) and of S (MODE 1 scales).
 __global__ void beam_bounds_kernel(const JonesF64* beam, int n_uniq_tile, const int* freq_map, int n_uniq_freq,
@@ -1136,10 +1158,17 @@ int Modeller::tensor_setup() {
 // each chunk's Gram kernel (on s) waiting for its table and each table for
 // the Gram kernel that last read its buffer, so that writing the next
 // chunk's table overlaps the current Gram kernel.
+int tensor_single_pass() { return tc::Cfg<2>::KPASS; }
+
 int launch_tensor_points(int nf, int nbl, int ntiles, int nc, const double* d_freqs, const XYZ* d_xyzs, double ha,
                          double dec, const double4* d_lmn, const JonesF64* d_W, const TensorBeam* beam, void* d_vis,
-                         bool out64, void* ws, int* d_err, cudaStream_t s, TensorSync* sync) {
+                         bool out64, void* ws, int* d_err, cudaStream_t s, TensorSync* sync,
+                         const TensorChunkOut* chunk_out) {
     if (nc == 0 || nf == 0) return HDC_OK;
+    if (chunk_out && (out64 || (beam && beam->beam) || nc > tc::Cfg<2>::KPASS)) {
+        set_error("launch_tensor_points: per-chunk output needs the shared-beam table form, one pass, JonesF32");
+        return HDC_ERR_ARG;
+    }
     int rc = tensor_configure();
     if (rc) return rc;
     tc::Params P;
@@ -1240,8 +1269,18 @@ int launch_tensor_points(int nf, int nbl, int ntiles, int nc, const double* d_fr
                 count_launches(1);
                 HDC_CUDA_RET_INT(cudaGetLastError());
                 if (two) HDC_CUDA_RET_INT(cudaEventRecord(sync->gram_done[b], s));
+                if (chunk_out) {
+                    const size_t i0 = (size_t)f0 * nbl, cnt = (size_t)nch * nbl;
+                    tc::combine_model_kernel<<<(unsigned)((cnt + 255) / 256), 256, 0, s>>>(
+                        ws, static_cast<JonesF32*>(d_vis), chunk_out->model, nvis, i0, cnt);
+                    count_launches(1);
+                    HDC_CUDA_RET_INT(cudaGetLastError());
+                    rc = chunk_out->done(chunk_out->ctx, f0, nch);
+                    if (rc) return rc;
+                }
             }
             P.f0 = 0;
+            if (chunk_out) return HDC_OK;
         }
         const unsigned blocks = (unsigned)((nvis + 255) / 256);
         if (out64)
