@@ -226,14 +226,7 @@ def test_full_mixed_config_chosen_form_vs_fp64_oracle(oracle, ctype, name):
     assert nrm < TOL and p999 < TOL, (nrm, p999, mx)
 
 
-def test_host_buffer_call_equals_device_call():
-    """The trait's host-buffer call -- the channels in five chunks pipelined
-    over three streams, the points' tables on a second stream -- accumulates
-    exactly the device call's visibilities into the caller's buffer (the
-    timed configuration, one timestep, every component class)."""
-    obs, sky = synth.config2()
-    m = SkyModeller(sky, obs.tile_xyzs, obs.freqs, obs.phase_centre, obs.latitude, beam="analytic", form="tensor")
-    lst = float(obs.lsts[1])
+def host_buffer_matches_device(m, obs, lst):
     dev = torch.zeros((obs.freqs.size, obs.num_baselines, 8), dtype=torch.float32, device="cuda")
     m.model_timestep_with(lst, dev, return_uvws=False)
     want = dev.cpu().numpy()
@@ -245,9 +238,35 @@ def test_host_buffer_call_equals_device_call():
     # scale (2 ulp of the largest magnitude)
     host = np.full((obs.freqs.size, obs.num_baselines, 8), 0.5, np.float32)
     m.model_timestep_with_host(lst, host)
-    m.close()
     tol = 2 * float(np.spacing(np.float32(np.abs(want).max())))
-    np.testing.assert_allclose(host, want + np.float32(0.5), rtol=0, atol=tol)
+    # a masked pol is zero after either call, the buffer's 0.5 included
+    masked = np.all(want == 0, axis=(0, 1))
+    np.testing.assert_allclose(host, np.where(masked, np.float32(0), want + np.float32(0.5)), rtol=0, atol=tol)
+
+
+def test_host_buffer_call_equals_device_call():
+    """The trait's host-buffer call -- the Gaussians and shapelets of every
+    channel staged while the buffer uploads, then the points chunk by chunk
+    with each chunk's download behind them -- accumulates exactly the device
+    call's visibilities into the caller's buffer (the timed configuration,
+    one timestep, every component class)."""
+    obs, sky = synth.config2()
+    m = SkyModeller(sky, obs.tile_xyzs, obs.freqs, obs.phase_centre, obs.latitude, beam="analytic", form="tensor")
+    host_buffer_matches_device(m, obs, float(obs.lsts[1]))
+    m.close()
+
+
+@pytest.mark.parametrize("pols,ng,ns", [("XX_YY", 60, 0), ("XX", 0, 12), ("XX_YY_XY", 30, 6), ("XX_XY_YX_YY", 0, 0)])
+def test_host_buffer_call_chunks_and_masks(pols, ng, ns):
+    """The same at 160 channels (three tables of points: 74 + 74 + 12
+    channels, each downloaded behind its own Gram products) for points with
+    Gaussians, with shapelets, with both, and alone (the five-chunk pipeline
+    of the other forms), under every pol mask."""
+    obs, sky = synth.config2(n_gauss=ng, n_shapelets=ns, n_freqs=160, n_times=1)
+    m = SkyModeller(sky, obs.tile_xyzs, obs.freqs, obs.phase_centre, obs.latitude, pols=pols, beam="analytic",
+                    form="tensor")
+    host_buffer_matches_device(m, obs, float(obs.lsts[0]))
+    m.close()
 
 
 @pytest.mark.parametrize("ntiles,npts", [(130, 200), (144, 300), (256, 150), (300, 64)])
