@@ -1053,7 +1053,7 @@ def gpu_arm(args, rank, world, local_rank):
             flops = fl_per * nbl * nf * ncomp
             fast = form == "tensor"
             entry = {"bound": "fp32" if fast else "fp64",
-                     "kernel": f"direct_kernel ({names[k]}, {'FP32 form' if fast else 'FP64'})",
+                     "kernel": f"fast_kernel ({names[k]}, FP32 form)" if fast else f"direct_kernel ({names[k]}, FP64)",
                      "peak": (g32.value if fast else g64.value) / 1e3,
                      "peak_source": f"{'FP32' if fast else 'FP64'} FMA probe kernel measured in this run"}
         traffic = NCU_DRAM_BYTES_PER_LAUNCH.get((names[k], form))
