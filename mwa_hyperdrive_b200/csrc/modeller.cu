@@ -997,9 +997,9 @@ extern "C" int hdc_modeller_model_timestep_with_host(HdcModeller* hm, double lst
             HDC_CUDA_RET_INT(cudaMalloc(&m->d_host_model, bytes));
             m->host_model_bytes = bytes;
         }
-        return m->model_host_points_last(lst, h_vis, h_uvws, s);
+        return m->host_call_drained(m->model_host_points_last(lst, h_vis, h_uvws, s));
     }
-    return m->model_host_pipelined(lst, h_vis, h_uvws, s);
+    return m->host_call_drained(m->model_host_pipelined(lst, h_vis, h_uvws, s));
 }
 
 namespace hdc {
@@ -1076,6 +1076,16 @@ int Modeller::model_host_pipelined(double lst, JonesF32* h_vis, UVW* h_uvws, cud
 }  // namespace hdc
 
 namespace hdc {
+// An error return of a host-buffer call may leave copies of the caller's
+// buffer queued: wait for the pipeline's streams first, so that nothing
+// reads or writes that buffer after the call returns.
+int Modeller::host_call_drained(int rc) {
+    if (rc)
+        for (auto st : pipe_s)
+            if (st) cudaStreamSynchronize(st);
+    return rc;
+}
+
 namespace {
 struct PointsLastCtx {
     Modeller* m;

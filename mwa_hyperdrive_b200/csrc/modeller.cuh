@@ -105,6 +105,8 @@ struct Modeller {
     // uploads, then the points chunk by chunk, each chunk downloaded as soon
     // as its points are in
     int model_host_points_last(double lst, JonesF32* h_vis, UVW* h_uvws, cudaStream_t s);
+    // rc, after waiting for the pipeline's streams when rc reports an error
+    int host_call_drained(int rc);
     // model_timestep_with over baseline UVWs the caller computed (as the
     // reference's peel loop passes its own d_uvws, model/gpu.rs:1152-1166);
     // direct FP64 kernels, JonesF32 output.
