@@ -393,7 +393,8 @@ __device__ __forceinline__ void group_sync(int grp) {
 }
 
 // Threads per CTA of the iteration kernel: the FP32 collapsed form runs two
-// groups of 256 (one per parity of the row block) on one shared ring.
+// groups of 256 (one per parity of the block's storage index) on one
+// shared ring.
 __host__ __device__ constexpr int cal_threads(int form) { return form == HDC_CAL_COLLAPSED_F32 ? 2 * CT : CT; }
 
 template <int FORM>
