@@ -15,8 +15,9 @@ channel with no exchange), so scaling is weak.
 
 Rank 0 of a 1-GPU run adds sections measured the same way: `dical` (DI
 calibration, all solver forms), `peel` (sequential and batched peeling),
-`warmstart` (learned warm start against identity starts) and `prep`
-(vis_average and scale_by_weights against the HBM copy bandwidth).
+`warmstart` (learned warm start against identity starts), `prep`
+(vis_average and scale_by_weights against the HBM copy bandwidth) and `fee`
+(the FEE beam's per-tile Jones against the FP64 FMA rate).
 """
 
 from __future__ import annotations
@@ -62,6 +63,8 @@ def parse():
     ap.add_argument("--peel-channels", type=int, default=384, help="reduced peel case for profiling")
     ap.add_argument("--skip-prep", action="store_true", help="leave out the visibility-preparation measurement")
     ap.add_argument("--prep-timesteps", type=int, default=8, help="reduced visibility-preparation case for profiling")
+    ap.add_argument("--skip-fee", action="store_true", help="leave out the FEE beam measurement")
+    ap.add_argument("--fee-directions", type=int, default=4600, help="reduced FEE case for profiling")
     args = ap.parse_args()
     global SHAPE
     SHAPE = (args.channels, args.timesteps)
@@ -886,6 +889,90 @@ def prep_arm(args):
     return out
 
 
+FEE_NMAX = 16
+FEE_WORKLOAD = ("FEE beam Jones (norm to zenith, parallactic rotation) at the mixed configuration's 4600 "
+                "component directions for 128 tiles (24 unique: one pointing, 23 dead-dipole patterns) x 384 "
+                "channels (their 25 closest file frequencies), synthetic coefficients with the beam file's "
+                f"layout up to degree {FEE_NMAX} ({FEE_NMAX * (FEE_NMAX + 2)} modes per polarisation)")
+FEE_FLOP_PER_MODE = 56  # both polarisations: theta and phi sums, 2 x (6 + 6 + 8 + 8)
+
+
+def fee_arm(args):
+    import torch
+
+    from mwa_hyperdrive_b200 import _lib, synth
+    from mwa_hyperdrive_b200.fee import FeeBeam
+
+    lib = _lib.lib()
+    file_f = (166.4e6 + np.arange(27) * 1.28e6).astype(np.uint32)
+    coeffs = synth.fee_coeffs(file_f, FEE_NMAX, seed=21)
+    chans = 167.00e6 + np.arange(384) * 0.08e6
+    ntiles = 128
+    base = np.array([(d % 4) * 3 + (d // 4) for d in range(16)], np.uint32)
+    delays = np.tile(base, (ntiles, 1))
+    for t in range(1, 24):  # tiles 1..23 each with its own dead dipole; the rest intact
+        delays[t, (t * 5) % 16] = 32
+        if t > 16:
+            delays[t, (t * 3 + 1) % 16] = 32
+    amps = np.ones((ntiles, 32))
+    beam = FeeBeam(coeffs, chans, delays, amps, norm_to_zenith=True)
+    nu, nuf = beam.num_unique_tiles(), beam.num_unique_freqs()
+    n = args.fee_directions
+    rng = np.random.default_rng(5)
+    az = torch.from_numpy(rng.uniform(0.0, 2 * math.pi, n)).cuda()
+    za = torch.from_numpy(np.arccos(rng.uniform(0.05, 1.0, n))).cuda()
+    lat = torch.tensor([-0.4660608448386394], dtype=torch.float64, device="cuda")
+    out = torch.empty((nu, nuf, n, 8), dtype=torch.float64, device="cuda")  # > L2 at the full size
+    stream = torch.cuda.current_stream()
+    st = ctypes.c_void_p(stream.cuda_stream)
+
+    def call():
+        _lib.check(lib.hdc_fee_calc_jones(beam.handle, az.data_ptr(), za.data_ptr(), n, lat.data_ptr(), 0,
+                                          out.data_ptr(), st), "hdc_fee_calc_jones")
+
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    for _ in range(3):
+        call()
+    times = []
+    for _ in range(5):
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        call()
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        times.append(ev[0].elapsed_time(ev[1]) * 1e-3)
+    t = statistics.median(times)
+    modes = FEE_NMAX * (FEE_NMAX + 2)
+    jones = nu * nuf * n
+    flop = jones * modes * FEE_FLOP_PER_MODE
+    g = ctypes.c_double()
+    _lib.check(lib.hdc_probe_fp64_gflops(ctypes.byref(g)), "hdc_probe_fp64_gflops")
+    res = {"workload": FEE_WORKLOAD, "unique_tiles": nu, "unique_freqs": nuf,
+           "directions": n, "s_per_call": t, "jones_per_s": jones / t, "jones_modes_per_s": jones * modes / t,
+           "roofline": {"bound": "fp64", "kernel": "fee_jones_kernel", "achieved": flop / t / 1e12,
+                        "peak": g.value / 1e3, "unit": "TFLOP/s", "frac": flop / t / 1e9 / g.value,
+                        "peak_source": "FP64 FMA probe kernel measured in this run",
+                        "flop_per_launch": flop,
+                        "flop_rule": f"{FEE_FLOP_PER_MODE} FLOP per mode per direction per (unique tile, "
+                                     "unique frequency); the Legendre recurrences are not counted"}}
+    if not args.no_cpu_baseline:
+        from oracle import fee_ref as fr
+
+        k = 2  # sets in the sample
+        azh, zah = az.cpu().numpy(), za.cpu().numpy()
+        t0 = time.perf_counter()
+        for i in range(k):
+            fr.calc_jones(coeffs, azh, zah, chans[i * 100], delays[i], amps[i], norm_to_zenith=True,
+                          latitude=-0.4660608448386394)
+        dt = time.perf_counter() - t0
+        res["cpu_baseline"] = {"value": dt * (nu * nuf) / k, "unit": "s per call", "cores": 1, "kind": "port",
+                               "sample": f"{k} of {nu * nuf} (tile, frequency) sets x {n} directions "
+                                         f"(numpy restatement, {dt:.1f} s), scaled"}
+        res["speedup_vs_cpu"] = res["cpu_baseline"]["value"] / t
+    beam.close()
+    return res
+
+
 def guarded(fn, args):
     """Run an optional bench section; a failure is reported in the line."""
     try:
@@ -1102,7 +1189,7 @@ def gpu_arm(args, rank, world, local_rank):
                 rg["native_chosen_form"] = {"ms_per_timestep": ms_chosen / nt,
                                             "speedup_vs_reference_kernels": ref_ms / (ms_chosen / nt)}
             torch.cuda.synchronize()
-        if not (args.skip_dical and args.skip_peel and args.skip_warmstart and args.skip_prep):
+        if not (args.skip_dical and args.skip_peel and args.skip_warmstart and args.skip_prep and args.skip_fee):
             del vis, flush
             torch.cuda.empty_cache()
         if not args.skip_dical:
@@ -1116,6 +1203,9 @@ def gpu_arm(args, rank, world, local_rank):
             torch.cuda.empty_cache()
         if not args.skip_prep:
             line["prep"] = guarded(prep_arm, args)
+            torch.cuda.empty_cache()
+        if not args.skip_fee:
+            line["fee"] = guarded(fee_arm, args)
         print(json.dumps(line), flush=True)
     plain.close()
     if chosen is not plain:

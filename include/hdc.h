@@ -339,6 +339,7 @@ typedef struct HdcSkyModel {
 #define HDC_BEAM_NONE 0          /* identity Jones (beam/mod.rs:255-388 NoBeam) */
 #define HDC_BEAM_ANALYTIC_DIPOLE 1 /* 4x4 dipole tile over a ground plane, shared by all tiles */
 #define HDC_BEAM_ANALYTIC_PER_TILE 2 /* the same tile with each tile's own dipole gains (hdc_modeller_set_tile_beams) */
+#define HDC_BEAM_FEE 3               /* the MWA FEE beam per tile (hdc_modeller_set_fee_beam) */
 
 /* Veto brightness of every source of a source list (srclist/veto.rs:58-129),
  * on the device: per coarse frequency h_freqs [Hz], the sum over a source's
@@ -387,6 +388,66 @@ int hdc_modeller_set_tile_xyzs(HdcModeller *m, const XYZ *h_tile_xyzs);
  * [component] layout.  The direct form applies B_p S B_q^H per baseline; the
  * tensor form uses its block form (twice the components). */
 int hdc_modeller_set_tile_beams(HdcModeller *m, const double *h_dipole_gains, double freq_res_hz);
+
+/* ---------------------------------------------------------------------- */
+/* MWA FEE beam on the device                                             */
+/* ---------------------------------------------------------------------- */
+/* The reference takes its per-tile beam Jones from mwa_hyperbeam 0.11.0's
+ * FEE model (beam/fee.rs:307-369: FEEBeam::gpu_prepare(freqs, delays, gains,
+ * norm_to_zenith = true), then calc_jones_device_pair_inner(az, za, latitude,
+ * iau_order = false) into [uniq tile][uniq freq][direction], with the tile
+ * and frequency maps and unique counts of beam/mod.rs:342-367).  The model
+ * is the spherical-wave expansion of each dipole's embedded element pattern
+ * (Sokolowski et al. 2017, PASA 34, e062).  HDF5 is not linked: the caller
+ * reads the beam file (mwa_full_embedded_element_pattern.h5) and passes its
+ * arrays here. */
+typedef struct HdcFeeCoeffs {
+    int num_freqs;                 /* frequencies of the file */
+    const uint32_t *freqs_hz;      /* [num_freqs] */
+    int num_modes;                 /* columns of the file's "modes" data set */
+    const int32_t *modes;          /* [3][num_modes]: s (1 or 2), m, n of each column */
+    const int32_t *num_freq_modes; /* [num_freqs]: columns of that frequency's data sets (the first ones of modes) */
+    const double *q;               /* [num_freqs][2: X, Y][16 dipoles][num_modes][2]: complex coefficient (re, im)
+                                      of each column; the file holds amplitude and phase [deg] */
+} HdcFeeCoeffs;
+
+typedef struct HdcFeeBeam HdcFeeBeam;
+
+/* FEEBeam::gpu_prepare: each tile's dipole delays h_delays [num_tiles][16]
+ * (steps of 435 ps; 32 marks a dead dipole, whose amplitudes become 0) and
+ * amplitudes h_amps [num_tiles][num_amps] (num_amps 32: X dipoles then Y;
+ * 16: the same for both), each of h_freqs_hz [num_freqs] taken at the file's
+ * closest frequency.  Tiles with equal delays and amplitudes share one beam,
+ * as do channels with the same closest frequency.  The dipole sums of every
+ * unique (tile, frequency) are formed on the host and uploaded; with
+ * norm_to_zenith each Jones element is divided by the magnitude of the
+ * zenith-pointed (all delays 0, amplitudes 1) beam's element at zenith. */
+int hdc_fee_beam_new(const HdcFeeCoeffs *file, const uint32_t *h_freqs_hz, int num_freqs, const uint32_t *h_delays,
+                     const double *h_amps, int num_tiles, int num_amps, int norm_to_zenith, HdcFeeBeam **out);
+void hdc_fee_beam_free(HdcFeeBeam *b);
+/* BeamGpu::get_num_unique_tiles / get_num_unique_freqs / get_tile_map /
+ * get_freq_map (beam/mod.rs:355-367); the maps are device pointers owned by
+ * the beam ([num_tiles] and [num_freqs]). */
+int hdc_fee_beam_num_unique_tiles(const HdcFeeBeam *b);
+int hdc_fee_beam_num_unique_freqs(const HdcFeeBeam *b);
+const int *hdc_fee_beam_tile_map(const HdcFeeBeam *b);
+const int *hdc_fee_beam_freq_map(const HdcFeeBeam *b);
+/* Host copies of the two maps (h_tile_map [num_tiles], h_freq_map
+ * [num_freqs]; either may be NULL).  No counterpart in the reference. */
+int hdc_fee_beam_host_maps(const HdcFeeBeam *b, int *h_tile_map, int *h_freq_map);
+/* calc_jones_device_pair_inner (beam/fee.rs:330-349): for directions
+ * d_az_rad, d_za_rad [num_directions] write d_jones [uniq tile][uniq freq]
+ * [num_directions].  d_latitude_rad (a device pointer to one value, or NULL)
+ * applies the parallactic-angle rotation; iau_order must be 0 (the order the
+ * reference asks for).  Asynchronous on stream. */
+int hdc_fee_calc_jones(const HdcFeeBeam *b, const double *d_az_rad, const double *d_za_rad, int num_directions,
+                       const double *d_latitude_rad, int iau_order, JonesF64 *d_jones, hdcStream_t stream);
+/* Use an FEE beam for every tile of the modeller (HDC_BEAM_FEE): its
+ * per-tile Jones are evaluated per timestep at each component's Az/ZA, with
+ * the parallactic rotation at the modeller's latitude.  The beam must have
+ * been prepared for the modeller's channel frequencies and tile count, and
+ * must stay alive while the modeller uses it. */
+int hdc_modeller_set_fee_beam(HdcModeller *m, const HdcFeeBeam *b);
 
 /* SkyModeller::model_timestep_with at a given LMST (the device-level form the
  * reference's peel loop calls, model/gpu.rs:1152-1166): d_vis_fb [freq][bl]

@@ -41,6 +41,11 @@ class HdcPeelParams(ctypes.Structure):
                 ("batch_size", c_int)]
 
 
+class HdcFeeCoeffs(ctypes.Structure):
+    _fields_ = [("num_freqs", c_int), ("freqs_hz", c_void_p), ("num_modes", c_int), ("modes", c_void_p),
+                ("num_freq_modes", c_void_p), ("q", c_void_p)]
+
+
 class HdcCalResult(ctypes.Structure):
     _fields_ = [("num_iterations", c_int), ("converged", c_int), ("max_precision", c_double), ("num_failed", c_int)]
 
@@ -122,6 +127,16 @@ SIGNATURES = {
     "hdc_modeller_free": (None, [c_void_p]),
     "hdc_modeller_set_tile_xyzs": (c_int, [c_void_p, c_void_p]),
     "hdc_modeller_set_tile_beams": (c_int, [c_void_p, c_void_p, c_double]),
+    "hdc_modeller_set_fee_beam": (c_int, [c_void_p, c_void_p]),
+    "hdc_fee_beam_new": (c_int, [ctypes.POINTER(HdcFeeCoeffs), c_void_p, c_int, c_void_p, c_void_p, c_int, c_int,
+                                 c_int, ctypes.POINTER(c_void_p)]),
+    "hdc_fee_beam_free": (None, [c_void_p]),
+    "hdc_fee_beam_num_unique_tiles": (c_int, [c_void_p]),
+    "hdc_fee_beam_num_unique_freqs": (c_int, [c_void_p]),
+    "hdc_fee_beam_tile_map": (c_void_p, [c_void_p]),
+    "hdc_fee_beam_freq_map": (c_void_p, [c_void_p]),
+    "hdc_fee_beam_host_maps": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "hdc_fee_calc_jones": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p]),
     "hdc_modeller_model_timestep_with": (c_int, [c_void_p, c_double, c_void_p, c_void_p, c_void_p]),
     "hdc_modeller_model_timestep_with_f64": (c_int, [c_void_p, c_double, c_void_p, c_void_p, c_void_p]),
     "hdc_modeller_model_timestep_with_host": (c_int, [c_void_p, c_double, c_void_p, c_void_p, c_void_p]),

@@ -221,6 +221,21 @@ __device__ __forceinline__ void drain_two_stage(uint64_t* bar, int k, int issued
     for (int j = k; j < issued; j++) mbar_wait_bounded(&bar[j & 1], (j >> 1) & 1, nullptr);
 }
 
+// ERFA hd2ae (marlu HADec::to_azel).
+__device__ __forceinline__ void hadec_to_azel(double ha, double dec, double lat, double& az, double& el) {
+    double s_ha, c_ha, s_dec, c_dec, s_lat, c_lat;
+    sincos(ha, &s_ha, &c_ha);
+    sincos(dec, &s_dec, &c_dec);
+    sincos(lat, &s_lat, &c_lat);
+    const double x = -s_ha * c_dec;
+    const double y = -c_ha * c_dec * s_lat + s_dec * c_lat;
+    const double z = c_ha * c_dec * c_lat + s_dec * s_lat;
+    const double r = hypot(x, y);
+    const double a = (r == 0.0) ? 0.0 : atan2(x, y);
+    az = (a < 0.0) ? a + TAU : a;
+    el = atan2(z, r);
+}
+
 // FP64 phasor exp(2 pi i t) for a phase in turns: exact range reduction to
 // r = t - rint(t) in [-1/2, 1/2], then sincospi(2 r).
 __device__ __forceinline__ cplx phasor_turns(double t) {

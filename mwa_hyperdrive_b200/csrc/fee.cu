@@ -1,0 +1,572 @@
+// MWA FEE beam on the device: per-tile Jones matrices from the
+// spherical-wave expansion of the dipoles' embedded element patterns.
+//
+// The reference takes them from mwa_hyperbeam 0.11.0 (a crates.io
+// dependency, not part of the reference tree): FEEBeam::gpu_prepare and
+// FEEBeamGpu::calc_jones_device_pair_inner, called from beam/fee.rs:307-349
+// and read by the predict kernels as [uniq tile][uniq freq][direction]
+// (model/gpu.rs:889-910, gpu/model.cu:114-123).  The model is that of
+// Sokolowski et al. 2017 (PASA 34, e062).  For one polarisation with the
+// beamformed coefficients Q1_mn, Q2_mn (the file's s = 1 and s = 2 modes,
+// summed over the 16 dipoles with each dipole's amplitude and delay phase
+// exp(-2 pi i f tau), tau = delay x 435 ps):
+//   sigma_T = sum_mn K_mn e^{i m phi} (P1sin (|m| Q2 u - m Q1) + Q2 P1)
+//   sigma_P = sum_mn K_mn e^{i m phi} j (P1sin (m Q2 - |m| Q1 u) - Q1 P1)
+//   K_mn = C_mn (-m/|m|)^m j^n / sqrt(n (n + 1)),
+//   C_mn = sqrt((2n + 1)/2 (n - |m|)! / (n + |m|)!)
+// with u = cos theta, theta = za, phi = pi/2 - az, P1sin = P_n^|m|(u) /
+// sin theta and P1 = dP_n^|m|(cos theta) / d theta (associated Legendre
+// functions with the Condon-Shortley phase; (-m/|m|)^m is 1 for m <= 0).
+// The polarisation's Jones row is (sigma_T, -sigma_P); rows X then Y.  With
+// norm_to_zenith every element is divided by the magnitude of the same
+// element of the zenith-pointed beam at the zenith, taken at the azimuth
+// where it peaks (phi = 0, -pi/2, pi/2, 0).  With a latitude the matrix is
+// rotated by the parallactic angle + pi/2 (ERFA ae2hd and hd2pa, as marlu's
+// AzEl::to_hadec and HADec::get_parallactic_angle).
+//
+// Device layout.  K_mn is folded into the coefficients on the host and the
+// modes of a (tile, frequency) set are stored in the order the kernel visits
+// them (|m| outer, n inner, +m before -m), so a thread walks one array front
+// to back and every thread of a block reads the same 64-byte record at the
+// same time (one L1 broadcast per warp).  Per direction a thread runs three
+// upward Legendre recurrences in n, for columns |m| - 1, |m|, |m| + 1 of
+// R_n^c = P_n^c / sin^c theta (polynomials in u, finite at the zenith), so
+//   P1sin = sin^{|m|-1} R_n^|m|,
+//   P1 = (sin^{|m|+1} R_n^{|m|+1} - (n+|m|)(n-|m|+1) sin^{|m|-1} R_n^{|m|-1}) / 2
+//   (P1 = sin R_n^1 for m = 0)
+// hold at every theta, the zenith included, with no division.  The
+// recurrence coefficients (2n-1)/(n-c) and (n+c-1)/(n-c) come from a small
+// table.  The work is FP64 arithmetic: about 56 FLOPs per mode per
+// direction for both polarisations.
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+
+namespace hdc {
+
+constexpr int FEE_MAX_N = 64;              // largest mode degree n supported
+constexpr int FEE_REC_W = FEE_MAX_N + 2;   // recurrence table row: columns 0 .. n_max + 1
+constexpr double FEE_DELAY_STEP = 435e-12; // seconds per delay step
+constexpr uint32_t FEE_DEAD_DELAY = 32;    // delay value marking a dead dipole
+constexpr int FEE_BLOCK = 128;
+
+// One mode in kernel order: the s = 1 and s = 2 coefficients of the X and Y
+// polarisations with K_mn folded in.
+struct FeeMode {
+    double2 q1x, q2x, q1y, q2y;
+};
+
+// Modes of a set whose largest degree is nmax: n = 1..nmax, m = -n..n.
+inline int fee_num_modes(int nmax) { return nmax * (nmax + 2); }
+
+// Position of mode (m, n) in kernel order for largest degree nmax.
+inline int fee_kernel_index(int nmax, int m, int n) {
+    const int a = m < 0 ? -m : m;
+    if (a == 0) return n - 1;
+    const int k = a - 1;  // blocks of |m| = 1 .. a - 1 before this one, after the m = 0 block
+    return nmax + 2 * k * (nmax + 1) - k * (k + 1) + 2 * (n - a) + (m < 0 ? 1 : 0);
+}
+
+struct FeeSums {
+    cplx tx, px, ty, py;  // sigma_T and sigma_P / j of the X and Y rows
+};
+
+__device__ __forceinline__ void cmac(cplx& acc, cplx e, double tr, double ti) {
+    acc.re = fma(e.re, tr, fma(-e.im, ti, acc.re));
+    acc.im = fma(e.re, ti, fma(e.im, tr, acc.im));
+}
+
+// sigma_T += e (a q1 + b q2), sigma_P / j += e (b q1 + a q2), both rows.
+__device__ __forceinline__ void fee_mode_add(const FeeMode* __restrict__ p, double a, double b, cplx e, FeeSums& s) {
+    const double2 q1x = __ldg(&p->q1x), q2x = __ldg(&p->q2x), q1y = __ldg(&p->q1y), q2y = __ldg(&p->q2y);
+    cmac(s.tx, e, fma(a, q1x.x, b * q2x.x), fma(a, q1x.y, b * q2x.y));
+    cmac(s.px, e, fma(b, q1x.x, a * q2x.x), fma(b, q1x.y, a * q2x.y));
+    cmac(s.ty, e, fma(a, q1y.x, b * q2y.x), fma(a, q1y.y, b * q2y.y));
+    cmac(s.py, e, fma(b, q1y.x, a * q2y.x), fma(b, q1y.y, a * q2y.y));
+}
+
+// The mode sums of one coefficient set at (theta, phi).  (Reading the
+// coefficient records one mode ahead in registers measured slower: 122
+// registers instead of 88 cost a fifth of the resident warps.)
+__device__ void fee_sums(double theta, double phi, const FeeMode* __restrict__ q, int nmax,
+                         const double2* __restrict__ rec, FeeSums& out) {
+    double s, x, sph, cph;
+    sincos(theta, &s, &x);
+    sincos(phi, &sph, &cph);
+    FeeSums acc = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
+    const cplx e1 = {cph, sph};
+    cplx em = {1.0, 0.0};            // e^{i |m| phi}
+    double rd = 1.0, rd_prev = 0.0;  // R_|m|^|m| and R_{|m|-1}^{|m|-1}: R_0^0 = 1, R_{c+1}^{c+1} = -(2c+1) R_c^c
+    double sm1 = 0.0, sm = 1.0;      // sin^{|m|-1}, sin^{|m|}
+    const FeeMode* p = q;
+    for (int ma = 0; ma <= nmax; ma++) {
+        const double rd_next = -(2.0 * ma + 1.0) * rd;
+        const double smp1 = sm * s;
+        // the three columns at n = ma (previous, current)
+        double pa = rd_prev, ca = x * (2.0 * ma - 1.0) * rd_prev;  // column ma - 1 (ma >= 1)
+        double pb = 0.0, cb = rd;                                  // column ma
+        double pc = 0.0, cc = 0.0;                                 // column ma + 1 (zero below its diagonal)
+        auto advance = [&](int n1) {
+            if (ma >= 1) {
+                const double2 r = __ldg(&rec[n1 * FEE_REC_W + ma - 1]);
+                const double t = fma(r.x * x, ca, -r.y * pa);
+                pa = ca;
+                ca = t;
+            }
+            {
+                const double2 r = __ldg(&rec[n1 * FEE_REC_W + ma]);
+                const double t = fma(r.x * x, cb, -r.y * pb);
+                pb = cb;
+                cb = t;
+            }
+            if (n1 == ma + 1) {
+                pc = 0.0;
+                cc = rd_next;
+            } else {
+                const double2 r = __ldg(&rec[n1 * FEE_REC_W + ma + 1]);
+                const double t = fma(r.x * x, cc, -r.y * pc);
+                pc = cc;
+                cc = t;
+            }
+        };
+        int n = ma;
+        if (ma == 0) {
+            advance(1);
+            n = 1;
+        }
+        for (; n <= nmax; n++) {
+            const double p1sin = ma >= 1 ? sm1 * cb : 0.0;
+            const double p1 = ma == 0 ? s * cc : 0.5 * fma(smp1, cc, -(double)((n + ma) * (n - ma + 1)) * sm1 * ca);
+            const double b = fma(ma * x, p1sin, p1);
+            const double a = -ma * p1sin;  // for +m; -m takes -a
+            fee_mode_add(p++, a, b, em, acc);
+            if (ma > 0) fee_mode_add(p++, -a, b, conj(em), acc);
+            if (n < nmax) advance(n + 1);
+        }
+        rd_prev = rd;
+        rd = rd_next;
+        sm1 = sm;
+        sm = smp1;
+        em = em * e1;
+    }
+    out = acc;
+}
+
+__device__ __forceinline__ J2 fee_jones(const FeeSums& s) {
+    // rows (sigma_T, -sigma_P) with sigma_P = j (sigma_P / j)
+    return J2{s.tx, cplx{-s.px.im, s.px.re}, s.ty, cplx{-s.py.im, s.py.re}};
+}
+
+// Rotation by the parallactic angle + pi/2 of direction (az, za) at latitude
+// lat: ERFA ae2hd (Az/El -> HA/Dec), then hd2pa.
+__device__ __forceinline__ J2 fee_parallactic(const J2& j, double az, double za, double lat) {
+    double sa, ca, se, ce, sp, cp;
+    sincos(az, &sa, &ca);
+    sincos(FRAC_PI_2 - za, &se, &ce);
+    sincos(lat, &sp, &cp);
+    const double x = -ca * ce * sp + se * cp;
+    const double y = -sa * ce;
+    const double z = ca * ce * cp + se * sp;
+    const double r = sqrt(x * x + y * y);
+    const double ha = r != 0.0 ? atan2(y, x) : 0.0;
+    const double dec = atan2(z, r);
+    double sh, ch, sd, cd;
+    sincos(ha, &sh, &ch);
+    sincos(dec, &sd, &cd);
+    const double sqsz = cp * sh;
+    const double cqsz = sp * cd - cp * sd * ch;
+    const double pa = (sqsz != 0.0 || cqsz != 0.0) ? atan2(sqsz, cqsz) : 0.0;
+    double sr, cr;
+    sincos(pa + FRAC_PI_2, &sr, &cr);
+    return J2{j.a * cr - j.b * sr, j.a * sr + j.b * cr, j.c * cr - j.d * sr, j.c * sr + j.d * cr};
+}
+
+struct FeeArgs {
+    const FeeMode* sets;  // [uniq tile][uniq freq][stride]
+    int stride;
+    const int* nmax;      // [uniq freq]
+    const double* norm;   // [uniq freq][4], or NULL
+    const double2* rec;   // [FEE_MAX_N + 1][FEE_REC_W]
+    int n_uniq_freq;
+    int n_dirs;
+    JonesF64* out;        // [uniq tile][uniq freq][n_dirs]
+};
+
+// One thread per direction of one (unique tile, unique frequency) set.
+// RADEC: directions from (RA, Dec) at the LST and latitude given (the
+// modeller's components; rotation always applied); otherwise from (az, za)
+// arrays, rotated when d_lat is set.
+template <bool RADEC>
+__global__ void __launch_bounds__(FEE_BLOCK) fee_jones_kernel(FeeArgs a, const double* __restrict__ az_in,
+                                                             const double* __restrict__ za_in,
+                                                             const double2* __restrict__ radec, double lst,
+                                                             double lat_v, const double* __restrict__ d_lat) {
+    const int d = blockIdx.x * blockDim.x + threadIdx.x;
+    const int uf = blockIdx.y, u = blockIdx.z;
+    if (d >= a.n_dirs) return;
+    double az, za, lat = 0.0;
+    bool rot;
+    if (RADEC) {
+        const double2 rd = radec[d];
+        double el;
+        hadec_to_azel(lst - rd.x, rd.y, lat_v, az, el);
+        za = FRAC_PI_2 - el;
+        rot = true;
+        lat = lat_v;
+    } else {
+        az = az_in[d];
+        za = za_in[d];
+        rot = d_lat != nullptr;
+        if (rot) lat = *d_lat;
+    }
+    const size_t set = (size_t)u * a.n_uniq_freq + uf;
+    FeeSums s;
+    fee_sums(za, FRAC_PI_2 - az, a.sets + set * a.stride, a.nmax[uf], a.rec, s);
+    J2 j = fee_jones(s);
+    if (a.norm) {
+        const double* nm = a.norm + 4 * uf;
+        j.a = cplx{j.a.re / nm[0], j.a.im / nm[0]};
+        j.b = cplx{j.b.re / nm[1], j.b.im / nm[1]};
+        j.c = cplx{j.c.re / nm[2], j.c.im / nm[2]};
+        j.d = cplx{j.d.re / nm[3], j.d.im / nm[3]};
+    }
+    if (rot) j = fee_parallactic(j, az, za, lat);
+    a.out[set * a.n_dirs + d] = store_j(j);
+}
+
+// Zenith normalisation: |element k| of the zenith-pointed beam at the zenith,
+// at the azimuth where that element peaks (phi = 0, -pi/2, pi/2, 0).
+__global__ void fee_norm_kernel(const FeeMode* __restrict__ ideal, int stride, const int* __restrict__ nmax,
+                                const double2* __restrict__ rec, int n_uniq_freq, double* __restrict__ norm) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 4 * n_uniq_freq) return;
+    const int uf = t >> 2, k = t & 3;
+    const double phi = (k == 1) ? -FRAC_PI_2 : (k == 2) ? FRAC_PI_2 : 0.0;
+    FeeSums s;
+    fee_sums(0.0, phi, ideal + (size_t)uf * stride, nmax[uf], rec, s);
+    const J2 j = fee_jones(s);
+    const cplx e = k == 0 ? j.a : k == 1 ? j.b : k == 2 ? j.c : j.d;
+    norm[t] = hypot(e.re, e.im);
+}
+
+}  // namespace hdc
+
+struct HdcFeeBeam {
+    int device = 0;
+    int ntiles = 0, nfreqs = 0, n_uniq_tile = 0, n_uniq_freq = 0, stride = 0;
+    hdc::FeeMode* d_sets = nullptr;
+    int* d_nmax = nullptr;
+    double* d_norm = nullptr;
+    double2* d_rec = nullptr;
+    int* d_tile_map = nullptr;
+    int* d_freq_map = nullptr;
+    std::vector<int> tile_map, freq_map;  // host copies
+};
+
+namespace hdc {
+namespace {
+
+using zc = std::complex<double>;
+
+void fee_release(HdcFeeBeam* b) {
+    cudaFree(b->d_sets);
+    cudaFree(b->d_nmax);
+    cudaFree(b->d_norm);
+    cudaFree(b->d_rec);
+    cudaFree(b->d_tile_map);
+    cudaFree(b->d_freq_map);
+    b->d_sets = nullptr;
+    b->d_nmax = b->d_tile_map = b->d_freq_map = nullptr;
+    b->d_norm = nullptr;
+    b->d_rec = nullptr;
+}
+
+// K_mn in kernel order for largest degree nmax.
+std::vector<zc> fee_factors(int nmax) {
+    std::vector<zc> k(fee_num_modes(nmax));
+    static const zc jpow[4] = {zc(1, 0), zc(0, 1), zc(-1, 0), zc(0, -1)};
+    for (int n = 1; n <= nmax; n++)
+        for (int m = -n; m <= n; m++) {
+            const int a = std::abs(m);
+            double ratio = 1.0;  // (n - |m|)! / (n + |m|)!
+            for (int t = n - a + 1; t <= n + a; t++) ratio /= (double)t;
+            const double c_mn = std::sqrt(0.5 * (2.0 * n + 1.0) * ratio);
+            const double sgn = (m > 0 && (m & 1)) ? -1.0 : 1.0;
+            k[fee_kernel_index(nmax, m, n)] = jpow[n & 3] * (c_mn * sgn / std::sqrt((double)n * (n + 1.0)));
+        }
+    return k;
+}
+
+// The beamformed coefficients of one set (file frequency k, one tile's
+// amplitudes [32] and delays [16], dead dipoles already zeroed) into
+// out[0 .. fee_num_modes(nmax)) in kernel order.
+void fee_set(const HdcFeeCoeffs* f, int k, const double* amps, const uint32_t* delays, int nmax,
+             const std::vector<zc>& kf, FeeMode* out) {
+    const int nm = f->num_freq_modes[k];
+    const int M = fee_num_modes(nmax);
+    std::vector<zc> q1[2], q2[2];
+    for (int p = 0; p < 2; p++) {
+        q1[p].assign(M, zc(0, 0));
+        q2[p].assign(M, zc(0, 0));
+        zc w[16];
+        for (int d = 0; d < 16; d++) {
+            const double ph = -TAU * (double)f->freqs_hz[k] * (double)delays[d] * FEE_DELAY_STEP;
+            w[d] = std::polar(amps[16 * p + d], ph);
+        }
+        const double* qk = f->q + (((size_t)k * 2 + p) * 16) * (size_t)f->num_modes * 2;
+        for (int col = 0; col < nm; col++) {
+            const int s = f->modes[col], m = f->modes[f->num_modes + col], n = f->modes[2 * f->num_modes + col];
+            zc acc(0, 0);
+            for (int d = 0; d < 16; d++) {
+                const double* c = qk + ((size_t)d * f->num_modes + col) * 2;
+                acc += w[d] * zc(c[0], c[1]);
+            }
+            const int i = fee_kernel_index(nmax, m, n);
+            (s == 1 ? q1[p] : q2[p])[i] += acc;
+        }
+    }
+    for (int i = 0; i < M; i++) {
+        const zc a = q1[0][i] * kf[i], b = q2[0][i] * kf[i], c = q1[1][i] * kf[i], d = q2[1][i] * kf[i];
+        out[i] = FeeMode{make_double2(a.real(), a.imag()), make_double2(b.real(), b.imag()),
+                         make_double2(c.real(), c.imag()), make_double2(d.real(), d.imag())};
+    }
+}
+
+int fee_check_file(const HdcFeeCoeffs* f) {
+    if (!f || f->num_freqs < 1 || !f->freqs_hz || f->num_modes < 1 || !f->modes || !f->num_freq_modes || !f->q) {
+        set_error("hdc_fee_beam_new: incomplete coefficient arrays");
+        return HDC_ERR_ARG;
+    }
+    for (int k = 0; k < f->num_freqs; k++)
+        if (f->num_freq_modes[k] < 1 || f->num_freq_modes[k] > f->num_modes) {
+            set_error("hdc_fee_beam_new: frequency %d has %d modes of %d", k, f->num_freq_modes[k], f->num_modes);
+            return HDC_ERR_ARG;
+        }
+    for (int c = 0; c < f->num_modes; c++) {
+        const int s = f->modes[c], m = f->modes[f->num_modes + c], n = f->modes[2 * f->num_modes + c];
+        if ((s != 1 && s != 2) || n < 1 || n > FEE_MAX_N || std::abs(m) > n) {
+            set_error("hdc_fee_beam_new: mode column %d (s %d, m %d, n %d) is outside s in {1, 2}, 1 <= n <= %d, "
+                      "|m| <= n", c, s, m, n, FEE_MAX_N);
+            return HDC_ERR_ARG;
+        }
+    }
+    return HDC_OK;
+}
+
+}  // namespace
+
+// Directions from (RA, Dec) at an LST (the modeller's per-timestep beam).
+int fee_launch_radec(const HdcFeeBeam* b, const double2* d_radec, int n, double lst, double lat, JonesF64* d_out,
+                     cudaStream_t s) {
+    if (n <= 0) return HDC_OK;
+    FeeArgs a{b->d_sets, b->stride, b->d_nmax, b->d_norm, b->d_rec, b->n_uniq_freq, n, d_out};
+    dim3 g((n + FEE_BLOCK - 1) / FEE_BLOCK, b->n_uniq_freq, b->n_uniq_tile);
+    fee_jones_kernel<true><<<g, FEE_BLOCK, 0, s>>>(a, nullptr, nullptr, d_radec, lst, lat, nullptr);
+    count_launches(1);
+    HDC_CUDA_RET_INT(cudaGetLastError());
+    return HDC_OK;
+}
+
+int fee_num_tiles(const HdcFeeBeam* b) { return b->ntiles; }
+int fee_num_freqs(const HdcFeeBeam* b) { return b->nfreqs; }
+int fee_device(const HdcFeeBeam* b) { return b->device; }
+
+}  // namespace hdc
+
+using namespace hdc;
+
+extern "C" int hdc_fee_beam_new(const HdcFeeCoeffs* file, const uint32_t* h_freqs_hz, int num_freqs,
+                                const uint32_t* h_delays, const double* h_amps, int num_tiles, int num_amps,
+                                int norm_to_zenith, HdcFeeBeam** out) {
+    if (!out) {
+        set_error("hdc_fee_beam_new: NULL output");
+        return HDC_ERR_ARG;
+    }
+    *out = nullptr;
+    int rc = fee_check_file(file);
+    if (rc) return rc;
+    if (!h_freqs_hz || num_freqs < 1 || !h_delays || !h_amps || num_tiles < 1 || (num_amps != 16 && num_amps != 32)) {
+        set_error("hdc_fee_beam_new: invalid arguments (num_freqs %d, num_tiles %d, num_amps %d)", num_freqs,
+                  num_tiles, num_amps);
+        return HDC_ERR_ARG;
+    }
+    // channels -> the file's closest frequency (the first on a tie), unique in order of first appearance
+    std::vector<int> fmap(num_freqs), ufile;
+    for (int f = 0; f < num_freqs; f++) {
+        int best = 0;
+        long long bd = -1;
+        for (int k = 0; k < file->num_freqs; k++) {
+            const long long dd = std::llabs((long long)file->freqs_hz[k] - (long long)h_freqs_hz[f]);
+            if (bd < 0 || dd < bd) {
+                bd = dd;
+                best = k;
+            }
+        }
+        auto it = std::find(ufile.begin(), ufile.end(), best);
+        fmap[f] = (int)(it - ufile.begin());
+        if (it == ufile.end()) ufile.push_back(best);
+    }
+    // tiles -> unique (delays, amplitudes), dead dipoles (delay 32) at amplitude 0 and delay 0
+    std::vector<int> tmap(num_tiles);
+    std::vector<std::vector<double>> uamp;
+    std::vector<std::vector<uint32_t>> udel;
+    for (int t = 0; t < num_tiles; t++) {
+        std::vector<double> a(32);
+        std::vector<uint32_t> dl(16);
+        for (int d = 0; d < 16; d++) {
+            const uint32_t v = h_delays[16 * (size_t)t + d];
+            if (v > FEE_DEAD_DELAY) {
+                set_error("hdc_fee_beam_new: tile %d dipole %d has delay %u (at most 32)", t, d, v);
+                return HDC_ERR_ARG;
+            }
+            const bool dead = v == FEE_DEAD_DELAY;
+            dl[d] = dead ? 0u : v;
+            const double ax = h_amps[(size_t)num_amps * t + d];
+            const double ay = h_amps[(size_t)num_amps * t + (num_amps == 32 ? 16 + d : d)];
+            a[d] = dead ? 0.0 : ax;
+            a[16 + d] = dead ? 0.0 : ay;
+        }
+        int found = -1;
+        for (size_t u = 0; u < uamp.size() && found < 0; u++)
+            if (uamp[u] == a && udel[u] == dl) found = (int)u;
+        if (found < 0) {
+            found = (int)uamp.size();
+            uamp.push_back(a);
+            udel.push_back(dl);
+        }
+        tmap[t] = found;
+    }
+    const int nu = (int)uamp.size(), nuf = (int)ufile.size();
+    std::vector<int> nmax(nuf, 1);
+    int nmax_all = 1;
+    for (int i = 0; i < nuf; i++) {
+        const int k = ufile[i];
+        for (int c = 0; c < file->num_freq_modes[k]; c++) nmax[i] = std::max(nmax[i], (int)file->modes[2 * file->num_modes + c]);
+        nmax_all = std::max(nmax_all, nmax[i]);
+    }
+    const int stride = fee_num_modes(nmax_all);
+    std::vector<FeeMode> sets((size_t)nu * nuf * stride);
+    std::vector<std::vector<zc>> kf(nuf);
+    for (int i = 0; i < nuf; i++) kf[i] = fee_factors(nmax[i]);
+    for (int u = 0; u < nu; u++)
+        for (int i = 0; i < nuf; i++)
+            fee_set(file, ufile[i], uamp[u].data(), udel[u].data(), nmax[i], kf[i],
+                    sets.data() + ((size_t)u * nuf + i) * stride);
+    // recurrence coefficients (2n-1)/(n-c), (n+c-1)/(n-c) for c < n
+    std::vector<double2> rec((size_t)(FEE_MAX_N + 1) * FEE_REC_W, make_double2(0.0, 0.0));
+    for (int n = 1; n <= FEE_MAX_N; n++)
+        for (int c = 0; c < n && c < FEE_REC_W; c++)
+            rec[(size_t)n * FEE_REC_W + c] = make_double2((2.0 * n - 1.0) / (n - c), (n + c - 1.0) / (n - c));
+
+    HdcFeeBeam* b = new HdcFeeBeam();
+    cudaGetDevice(&b->device);
+    b->ntiles = num_tiles;
+    b->nfreqs = num_freqs;
+    b->n_uniq_tile = nu;
+    b->n_uniq_freq = nuf;
+    b->stride = stride;
+    b->tile_map = tmap;
+    b->freq_map = fmap;
+    auto fail = [&](cudaError_t e, const char* what) {
+        set_error("hdc_fee_beam_new: %s: %s", what, cudaGetErrorString(e));
+        fee_release(b);
+        delete b;
+        return e == cudaErrorMemoryAllocation ? HDC_ERR_ALLOC : HDC_ERR_CUDA;
+    };
+    cudaError_t e;
+    if ((e = cudaMalloc(&b->d_sets, sizeof(FeeMode) * sets.size())) != cudaSuccess) return fail(e, "cudaMalloc");
+    if ((e = cudaMalloc(&b->d_nmax, sizeof(int) * nuf)) != cudaSuccess) return fail(e, "cudaMalloc");
+    if ((e = cudaMalloc(&b->d_rec, sizeof(double2) * rec.size())) != cudaSuccess) return fail(e, "cudaMalloc");
+    if ((e = cudaMalloc(&b->d_tile_map, sizeof(int) * num_tiles)) != cudaSuccess) return fail(e, "cudaMalloc");
+    if ((e = cudaMalloc(&b->d_freq_map, sizeof(int) * num_freqs)) != cudaSuccess) return fail(e, "cudaMalloc");
+    if ((e = cudaMemcpy(b->d_sets, sets.data(), sizeof(FeeMode) * sets.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
+        return fail(e, "cudaMemcpy");
+    if ((e = cudaMemcpy(b->d_nmax, nmax.data(), sizeof(int) * nuf, cudaMemcpyHostToDevice)) != cudaSuccess)
+        return fail(e, "cudaMemcpy");
+    if ((e = cudaMemcpy(b->d_rec, rec.data(), sizeof(double2) * rec.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
+        return fail(e, "cudaMemcpy");
+    if ((e = cudaMemcpy(b->d_tile_map, tmap.data(), sizeof(int) * num_tiles, cudaMemcpyHostToDevice)) != cudaSuccess)
+        return fail(e, "cudaMemcpy");
+    if ((e = cudaMemcpy(b->d_freq_map, fmap.data(), sizeof(int) * num_freqs, cudaMemcpyHostToDevice)) != cudaSuccess)
+        return fail(e, "cudaMemcpy");
+    if (norm_to_zenith) {
+        // the zenith-pointed beam of every unique frequency: all delays 0, amplitudes 1
+        std::vector<FeeMode> ideal((size_t)nuf * stride);
+        const std::vector<double> ones(32, 1.0);
+        const std::vector<uint32_t> zeros(16, 0u);
+        for (int i = 0; i < nuf; i++)
+            fee_set(file, ufile[i], ones.data(), zeros.data(), nmax[i], kf[i], ideal.data() + (size_t)i * stride);
+        FeeMode* d_ideal = nullptr;
+        if ((e = cudaMalloc(&d_ideal, sizeof(FeeMode) * ideal.size())) != cudaSuccess) return fail(e, "cudaMalloc");
+        if ((e = cudaMalloc(&b->d_norm, sizeof(double) * 4 * nuf)) != cudaSuccess) {
+            cudaFree(d_ideal);
+            return fail(e, "cudaMalloc");
+        }
+        e = cudaMemcpy(d_ideal, ideal.data(), sizeof(FeeMode) * ideal.size(), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) {
+            fee_norm_kernel<<<(4 * nuf + 127) / 128, 128>>>(d_ideal, stride, b->d_nmax, b->d_rec, nuf, b->d_norm);
+            count_launches(1);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+        cudaFree(d_ideal);
+        if (e != cudaSuccess) return fail(e, "zenith normalisation");
+    }
+    *out = b;
+    return HDC_OK;
+}
+
+extern "C" void hdc_fee_beam_free(HdcFeeBeam* b) {
+    if (!b) return;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != b->device) cudaSetDevice(b->device);
+    fee_release(b);
+    if (cur != b->device) cudaSetDevice(cur);
+    delete b;
+}
+
+extern "C" int hdc_fee_beam_num_unique_tiles(const HdcFeeBeam* b) { return b ? b->n_uniq_tile : 0; }
+extern "C" int hdc_fee_beam_num_unique_freqs(const HdcFeeBeam* b) { return b ? b->n_uniq_freq : 0; }
+extern "C" const int* hdc_fee_beam_tile_map(const HdcFeeBeam* b) { return b ? b->d_tile_map : nullptr; }
+extern "C" const int* hdc_fee_beam_freq_map(const HdcFeeBeam* b) { return b ? b->d_freq_map : nullptr; }
+
+extern "C" int hdc_fee_beam_host_maps(const HdcFeeBeam* b, int* h_tile_map, int* h_freq_map) {
+    if (!b) return HDC_ERR_ARG;
+    if (h_tile_map) std::copy(b->tile_map.begin(), b->tile_map.end(), h_tile_map);
+    if (h_freq_map) std::copy(b->freq_map.begin(), b->freq_map.end(), h_freq_map);
+    return HDC_OK;
+}
+
+extern "C" int hdc_fee_calc_jones(const HdcFeeBeam* b, const double* d_az_rad, const double* d_za_rad,
+                                  int num_directions, const double* d_latitude_rad, int iau_order, JonesF64* d_jones,
+                                  hdcStream_t stream) {
+    if (!b || num_directions < 0 || (num_directions > 0 && (!d_az_rad || !d_za_rad || !d_jones))) {
+        set_error("hdc_fee_calc_jones: invalid arguments");
+        return HDC_ERR_ARG;
+    }
+    if (iau_order) {
+        set_error("hdc_fee_calc_jones: iau_order = 1 is not supported (the reference asks for 0)");
+        return HDC_ERR_UNSUPPORTED;
+    }
+    int dev = 0;
+    HDC_CUDA_RET_INT(cudaGetDevice(&dev));
+    if (dev != b->device) {
+        set_error("hdc_fee_calc_jones: the beam was prepared on device %d, the current device is %d", b->device, dev);
+        return HDC_ERR_ARG;
+    }
+    if (num_directions == 0) return HDC_OK;
+    FeeArgs a{b->d_sets, b->stride, b->d_nmax, b->d_norm, b->d_rec, b->n_uniq_freq, num_directions, d_jones};
+    dim3 g((num_directions + FEE_BLOCK - 1) / FEE_BLOCK, b->n_uniq_freq, b->n_uniq_tile);
+    fee_jones_kernel<false><<<g, FEE_BLOCK, 0, (cudaStream_t)stream>>>(a, d_az_rad, d_za_rad, nullptr, 0.0, 0.0,
+                                                                       d_latitude_rad);
+    count_launches(1);
+    HDC_CUDA_RET_INT(cudaGetLastError());
+    return HDC_OK;
+}

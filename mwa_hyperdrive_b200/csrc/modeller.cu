@@ -202,21 +202,6 @@ __device__ J2 analytic_beam_tile(double az, double el, double freq, const double
     return J2{ax * p00, ax * p01, ay * p01, ay * p11};
 }
 
-// ERFA hd2ae (marlu HADec::to_azel).
-__device__ void hadec_to_azel(double ha, double dec, double lat, double& az, double& el) {
-    double s_ha, c_ha, s_dec, c_dec, s_lat, c_lat;
-    sincos(ha, &s_ha, &c_ha);
-    sincos(dec, &s_dec, &c_dec);
-    sincos(lat, &s_lat, &c_lat);
-    const double x = -s_ha * c_dec;
-    const double y = -c_ha * c_dec * s_lat + s_dec * c_lat;
-    const double z = c_ha * c_dec * c_lat + s_dec * s_lat;
-    const double r = hypot(x, y);
-    const double a = (r == 0.0) ? 0.0 : atan2(x, y);
-    az = (a < 0.0) ? a + TAU : a;
-    el = atan2(z, r);
-}
-
 // W[f][c] = B S B^H for a beam shared by all tiles (model/cpu.rs:187-230,
 // 336-337 with B1 == B2).
 __global__ void beam_weight_kernel(const double2* radec, int nc, const double* freqs, int nf, double lst, double lat,
@@ -265,6 +250,7 @@ void TileBeams::release() {
     dfree(d_tile_map);
     dfree(d_freqs);
     dfree(d_freq_map);
+    fee = nullptr;
     n_uniq_tile = n_uniq_freq = 0;
 }
 
@@ -478,6 +464,27 @@ int Modeller::set_tile_beams(const double* h_gains, double freq_res_hz) {
     return alloc_tile_beam_tables();
 }
 
+int Modeller::set_fee_beam(const HdcFeeBeam* b) {
+    if (!b || fee_num_tiles(b) != ntiles || fee_num_freqs(b) != nf || fee_device(b) != device) {
+        set_error("hdc_modeller_set_fee_beam: the beam was not prepared for this modeller's %d tiles and %d channels "
+                  "on device %d", ntiles, nf, device);
+        return HDC_ERR_ARG;
+    }
+    cudaDeviceSynchronize();
+    tb.release();
+    tb.n_uniq_tile = hdc_fee_beam_num_unique_tiles(b);
+    tb.n_uniq_freq = hdc_fee_beam_num_unique_freqs(b);
+    HDC_CUDA_RET_INT(dalloc(&tb.d_tile_map, ntiles));
+    HDC_CUDA_RET_INT(dalloc(&tb.d_freq_map, nf));
+    HDC_CUDA_RET_INT(cudaMemcpy(tb.d_tile_map, hdc_fee_beam_tile_map(b), sizeof(int) * ntiles,
+                                cudaMemcpyDeviceToDevice));
+    HDC_CUDA_RET_INT(cudaMemcpy(tb.d_freq_map, hdc_fee_beam_freq_map(b), sizeof(int) * nf, cudaMemcpyDeviceToDevice));
+    tb.fee = b;
+    for (int ty = 0; ty < 3; ty++) dfree(t[ty].d_W);
+    beam_kind = HDC_BEAM_FEE;
+    return alloc_tile_beam_tables();
+}
+
 int Modeller::geometry(double lst, cudaStream_t s) {
     const double ha = lst - pc.ra;
     const double s_ha = std::sin(ha), c_ha = std::cos(ha);
@@ -495,6 +502,11 @@ int Modeller::geometry(double lst, cudaStream_t s) {
     if (tile_beams()) {
         for (int ty = 0; ty < 3; ty++) {
             if (t[ty].nc == 0 || tb.n_uniq_tile == 0) continue;
+            if (tb.fee) {
+                const int rc = fee_launch_radec(tb.fee, t[ty].d_radec, t[ty].nc, lst, lat, t[ty].d_B, s);
+                if (rc) return rc;
+                continue;
+            }
             dim3 g((t[ty].nc + 127) / 128, tb.n_uniq_freq, tb.n_uniq_tile);
             tile_beam_kernel<<<g, 128, 0, s>>>(t[ty].d_radec, t[ty].nc, tb.d_freqs, tb.n_uniq_freq, tb.d_gains, lst,
                                                 lat, t[ty].d_B);
@@ -940,6 +952,12 @@ extern "C" int hdc_modeller_set_tile_beams(HdcModeller* hm, const double* h_dipo
     Modeller* m = reinterpret_cast<Modeller*>(hm);
     if (!m) return HDC_ERR_ARG;
     return m->set_tile_beams(h_dipole_gains, freq_res_hz);
+}
+
+extern "C" int hdc_modeller_set_fee_beam(HdcModeller* hm, const HdcFeeBeam* b) {
+    Modeller* m = reinterpret_cast<Modeller*>(hm);
+    if (!m) return HDC_ERR_ARG;
+    return m->set_fee_beam(b);
 }
 
 extern "C" void hdc_modeller_free(HdcModeller* m) { delete reinterpret_cast<Modeller*>(m); }

@@ -32,8 +32,18 @@ struct TileBeams {
     int* d_tile_map = nullptr;      // [tile]
     double* d_freqs = nullptr;      // [uniq freq] Hz
     int* d_freq_map = nullptr;      // [channel]
+    const HdcFeeBeam* fee = nullptr;  // HDC_BEAM_FEE: the caller's beam (the maps above are copies of its maps)
     void release();
 };
+
+// The FEE beam's per-timestep evaluation for the modeller (csrc/fee.cu):
+// Jones [uniq tile][uniq freq][n] of the directions d_radec at the LST, with
+// the parallactic rotation at latitude lat.
+int fee_launch_radec(const HdcFeeBeam* b, const double2* d_radec, int n, double lst, double lat, JonesF64* d_out,
+                     cudaStream_t s);
+int fee_num_tiles(const HdcFeeBeam* b);
+int fee_num_freqs(const HdcFeeBeam* b);
+int fee_device(const HdcFeeBeam* b);
 
 struct TensorState;
 
@@ -59,7 +69,7 @@ struct Modeller {
     int queue_error_check(cudaStream_t s);
     int take_error(bool wait);
     TypeTables t[3];
-    TileBeams tb;  // set when beam_kind == HDC_BEAM_ANALYTIC_PER_TILE
+    TileBeams tb;  // set when beam_kind == HDC_BEAM_ANALYTIC_PER_TILE or HDC_BEAM_FEE
     JonesF32* d_host_vis = nullptr;
     size_t host_vis_bytes = 0;
     JonesF32* d_host_model = nullptr;  // host-buffer call: Gaussians + shapelets staged here
@@ -80,8 +90,9 @@ struct Modeller {
     void prof_collect();
 
     int build_tables(const HdcSkyModel* sky);
-    bool tile_beams() const { return beam_kind == HDC_BEAM_ANALYTIC_PER_TILE; }
+    bool tile_beams() const { return beam_kind == HDC_BEAM_ANALYTIC_PER_TILE || beam_kind == HDC_BEAM_FEE; }
     int set_tile_beams(const double* h_gains, double freq_res_hz);
+    int set_fee_beam(const HdcFeeBeam* b);
     int alloc_tile_beam_tables();
     int geometry(double lst, cudaStream_t s);
     const JonesF64* weights(int ty) const;

@@ -19,7 +19,7 @@ import numpy as np
 from . import _lib
 from .srclist import SkyModelArrays, SourceList, Source
 
-BEAMS = {"none": 0, "analytic": 1, "per_tile": 2}
+BEAMS = {"none": 0, "analytic": 1, "per_tile": 2, "fee": 3}
 FORMS = {"direct": 0, "tensor": 1}
 POLS = {"XX_XY_YX_YY": 0, "XX": 1, "YY": 2, "XX_YY": 3, "XX_YY_XY": 4}
 
@@ -51,11 +51,14 @@ class SkyModeller:
     """GPU sky modeller (SkyModellerGpu equivalent)."""
 
     def __init__(self, sky, tile_xyzs, freqs, phase_centre, array_latitude_rad: float, pols: str = "XX_XY_YX_YY",
-                 beam: str = "none", form: str = "direct", dipole_gains=None, beam_freq_res_hz: float = 1.28e6):
+                 beam: str = "none", form: str = "direct", dipole_gains=None, beam_freq_res_hz: float = 1.28e6,
+                 fee_beam=None):
         """beam: "none", "analytic" (the dipole-array tile, shared by all
-        tiles) or "per_tile" (each tile's own dipole amplitudes,
+        tiles), "per_tile" (each tile's own dipole amplitudes,
         ``dipole_gains`` [tile][2][16], 0 for a dead dipole; evaluated at the
-        nearest multiple of ``beam_freq_res_hz`` of each channel)."""
+        nearest multiple of ``beam_freq_res_hz`` of each channel) or "fee"
+        (``fee_beam``, a :class:`mwa_hyperdrive_b200.fee.FeeBeam` prepared for
+        these tiles and channels, kept alive by this modeller)."""
         self.lib = _lib.lib()
         self.sky = _as_sky(sky)
         self.tile_xyzs = np.ascontiguousarray(tile_xyzs, dtype=np.float64).reshape(-1, 3)
@@ -70,12 +73,24 @@ class SkyModeller:
         h = ctypes.c_void_p()
         rc = self.lib.hdc_modeller_new(ctypes.byref(self.sky.struct()), POLS[pols], self.tile_xyzs.ctypes.data,
                                        self.num_tiles, self.freqs.ctypes.data, self.num_freqs,
-                                       _lib.RADec(*self.phase_centre), float(array_latitude_rad), BEAMS[beam],
+                                       _lib.RADec(*self.phase_centre), float(array_latitude_rad),
+                                       BEAMS["none"] if beam == "fee" else BEAMS[beam],
                                        FORMS[form], ctypes.byref(h))
         _lib.check(rc, "hdc_modeller_new")
         self._h = h
         if beam == "per_tile" and dipole_gains is not None:
             self.set_tile_beams(dipole_gains, beam_freq_res_hz)
+        if beam == "fee":
+            if fee_beam is None:
+                raise ValueError('beam="fee" needs fee_beam')
+            self.set_fee_beam(fee_beam)
+
+    def set_fee_beam(self, fee_beam) -> None:
+        """Use the FEE beam for every tile (its per-tile Jones are evaluated
+        per timestep at each component's Az/ZA)."""
+        _lib.check(self.lib.hdc_modeller_set_fee_beam(self._h, fee_beam.handle), "set_fee_beam")
+        self._fee = fee_beam
+        self.beam = "fee"
 
     def set_tile_beams(self, dipole_gains, beam_freq_res_hz: float = 1.28e6) -> None:
         g = np.ascontiguousarray(dipole_gains, dtype=np.float64).reshape(self.num_tiles, 2, 16)

@@ -263,3 +263,33 @@ def random_model(nt, nch, nbl, rng):
     m[..., 7] = m[..., 1] * 0.95
     m[..., 2:6] = rng.normal(0.0, 0.02, (nt, nch, nbl, 4)) * amp[..., None]
     return m.astype(np.float32)
+
+
+def fee_coeffs(freqs_hz, nmax, seed: int = 11) -> dict:
+    """Seeded stand-in for the MWA FEE beam file (the file is not in this
+    image), in the layout HdcFeeCoeffs takes: ``freqs_hz`` [nf] (uint32),
+    ``modes`` [3][M] (s, m, n; sorted by n, then s, then m, so that the first
+    2 n_k (n_k + 2) columns hold every mode up to degree n_k), ``num_freq_modes``
+    [nf] and ``q`` [nf][2 pols][16 dipoles][M][2] complex coefficients.
+    ``nmax`` is one largest degree for all frequencies or one per frequency.
+    Magnitudes fall as exp(-0.4 (n - 1)) with seeded random phases; each
+    dipole's coefficients are a shared pattern plus a 20 % dipole-specific
+    part."""
+    freqs = np.asarray(freqs_hz, np.uint32)
+    nf = freqs.size
+    nmx = np.broadcast_to(np.asarray(nmax, np.int32), (nf,)).copy()
+    top = int(nmx.max())
+    cols = [(s, m, n) for n in range(1, top + 1) for s in (1, 2) for m in range(-n, n + 1)]
+    modes = np.array(cols, np.int32).T.copy()
+    M = modes.shape[1]
+    rng = np.random.default_rng(seed)
+    n_of = modes[2].astype(np.float64)
+    scale = np.exp(-0.4 * (n_of - 1.0))
+    base = (rng.normal(size=(nf, 2, 1, M)) + 1j * rng.normal(size=(nf, 2, 1, M))) * scale
+    own = (rng.normal(size=(nf, 2, 16, M)) + 1j * rng.normal(size=(nf, 2, 16, M))) * scale * 0.2
+    qc = base + own
+    q = np.stack([qc.real, qc.imag], -1)
+    num = np.array([2 * k * (k + 2) for k in nmx], np.int32)
+    for f in range(nf):  # columns past a frequency's own modes are unused (zero, as padding in a file)
+        q[f, :, :, num[f]:, :] = 0.0
+    return {"freqs_hz": freqs, "modes": modes, "num_freq_modes": num, "q": np.ascontiguousarray(q)}
