@@ -24,20 +24,28 @@
 // rotated by the parallactic angle + pi/2 (ERFA ae2hd and hd2pa, as marlu's
 // AzEl::to_hadec and HADec::get_parallactic_angle).
 //
-// Device layout.  K_mn is folded into the coefficients on the host and the
+// Device layout.  K_mn is folded into the coefficients on the host, and the
 // modes of a (tile, frequency) set are stored in the order the kernel visits
-// them (|m| outer, n inner, +m before -m), so a thread walks one array front
-// to back and every thread of a block reads the same 64-byte record at the
-// same time (one L1 broadcast per warp).  Per direction a thread runs three
-// upward Legendre recurrences in n, for columns |m| - 1, |m|, |m| + 1 of
+// them (|m| outer, n inner), every set laid out for the beam's largest
+// degree.  The modes +m and -m of one degree share P1sin, P1 and
+// e^{-i m phi} = conj(e^{i m phi}), so they are stored as the sums and
+// differences of their coefficients and added together:
+//   e (a q1+ + b q2+) + conj(e) (-a q1- + b q2-)
+//     = Re(e) (a M1 + b P2) + i Im(e) (a P1 + b M2),  P = q+ + q-, M = q+ - q-
+// (a = -|m| P1sin, b = |m| u P1sin + P1), 24 FP64 instructions per
+// polarisation for the two modes instead of 32; m = 0 modes (e = 1, a = 0)
+// take 4.  A thread sums one set at two directions, so every coefficient
+// record it loads (all threads of a block read the same one: one L1
+// broadcast per warp) serves both.  Per direction it runs three upward
+// Legendre recurrences in n, for columns |m| - 1, |m|, |m| + 1 of
 // R_n^c = P_n^c / sin^c theta (polynomials in u, finite at the zenith), so
 //   P1sin = sin^{|m|-1} R_n^|m|,
 //   P1 = (sin^{|m|+1} R_n^{|m|+1} - (n+|m|)(n-|m|+1) sin^{|m|-1} R_n^{|m|-1}) / 2
 //   (P1 = sin R_n^1 for m = 0)
 // hold at every theta, the zenith included, with no division.  The
 // recurrence coefficients (2n-1)/(n-c) and (n+c-1)/(n-c) come from a small
-// table.  The work is FP64 arithmetic: about 56 FLOPs per mode per
-// direction for both polarisations.
+// table.  The work is FP64 arithmetic; the roofline counts the published
+// sum's 56 FLOPs per mode per direction (both polarisations).
 
 #include <algorithm>
 #include <cmath>
@@ -56,10 +64,14 @@ constexpr double FEE_DELAY_STEP = 435e-12; // seconds per delay step
 constexpr uint32_t FEE_DEAD_DELAY = 32;    // delay value marking a dead dipole
 constexpr int FEE_BLOCK = 128;
 
-// One mode in kernel order: the s = 1 and s = 2 coefficients of the X and Y
-// polarisations with K_mn folded in.
+// One 64-byte coefficient record in kernel order (K_mn folded in).  An m = 0
+// mode is one record (q1 X, q2 X, q1 Y, q2 Y); the modes +m and -m of one
+// degree are a pair of records, X then Y, each (P1, M1, P2, M2) with
+// P = q(+m) + q(-m) and M = q(+m) - q(-m): the two modes share P1sin, P1 and
+// e^{-i m phi} = conj(e^{i m phi}), so with the sums and differences stored
+// their contribution is Re(e) (s) + i Im(e) (d) (below).
 struct FeeMode {
-    double2 q1x, q2x, q1y, q2y;
+    double2 c0, c1, c2, c3;
 };
 
 // Modes of a set whose largest degree is nmax: n = 1..nmax, m = -n..n.
@@ -77,62 +89,101 @@ struct FeeSums {
     cplx tx, px, ty, py;  // sigma_T and sigma_P / j of the X and Y rows
 };
 
-__device__ __forceinline__ void cmac(cplx& acc, cplx e, double tr, double ti) {
-    acc.re = fma(e.re, tr, fma(-e.im, ti, acc.re));
-    acc.im = fma(e.re, ti, fma(e.im, tr, acc.im));
+__device__ __forceinline__ FeeMode ld_mode(const FeeMode* __restrict__ p) {
+    return FeeMode{__ldg(&p->c0), __ldg(&p->c1), __ldg(&p->c2), __ldg(&p->c3)};
 }
 
-// sigma_T += e (a q1 + b q2), sigma_P / j += e (b q1 + a q2), both rows.
-__device__ __forceinline__ void fee_mode_add(const FeeMode* __restrict__ p, double a, double b, cplx e, FeeSums& s) {
-    const double2 q1x = __ldg(&p->q1x), q2x = __ldg(&p->q2x), q1y = __ldg(&p->q1y), q2y = __ldg(&p->q2y);
-    cmac(s.tx, e, fma(a, q1x.x, b * q2x.x), fma(a, q1x.y, b * q2x.y));
-    cmac(s.px, e, fma(b, q1x.x, a * q2x.x), fma(b, q1x.y, a * q2x.y));
-    cmac(s.ty, e, fma(a, q1y.x, b * q2y.x), fma(a, q1y.y, b * q2y.y));
-    cmac(s.py, e, fma(b, q1y.x, a * q2y.x), fma(b, q1y.y, a * q2y.y));
+// An m = 0 mode (e = 1, a = 0): sigma_T += b q2, sigma_P / j += b q1.
+__device__ __forceinline__ void fee_m0_add(const FeeMode& r, double b, FeeSums& s) {
+    s.tx.re = fma(b, r.c1.x, s.tx.re);
+    s.tx.im = fma(b, r.c1.y, s.tx.im);
+    s.px.re = fma(b, r.c0.x, s.px.re);
+    s.px.im = fma(b, r.c0.y, s.px.im);
+    s.ty.re = fma(b, r.c3.x, s.ty.re);
+    s.ty.im = fma(b, r.c3.y, s.ty.im);
+    s.py.re = fma(b, r.c2.x, s.py.re);
+    s.py.im = fma(b, r.c2.y, s.py.im);
 }
 
-// The mode sums of one coefficient set at (theta, phi).  (Reading the
-// coefficient records one mode ahead in registers measured slower: 122
-// registers instead of 88 cost a fifth of the resident warps.)
-__device__ void fee_sums(double theta, double phi, const FeeMode* __restrict__ q, int nmax,
-                         const double2* __restrict__ rec, FeeSums& out) {
-    double s, x, sph, cph;
-    sincos(theta, &s, &x);
-    sincos(phi, &sph, &cph);
-    FeeSums acc = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
-    const cplx e1 = {cph, sph};
-    cplx em = {1.0, 0.0};            // e^{i |m| phi}
+// The pair +m, -m of one polarisation, record (P1, M1, P2, M2), a = -|m|
+// P1sin, e = e^{i |m| phi}:
+//   sigma_T     += Re(e) (a M1 + b P2) + i Im(e) (a P1 + b M2)
+//   sigma_P / j += Re(e) (b P1 + a M2) + i Im(e) (b M1 + a P2)
+__device__ __forceinline__ void fee_pair_add(const FeeMode& r, double a, double b, cplx e, cplx& t, cplx& ph) {
+    const double2 p1 = r.c0, m1 = r.c1, p2 = r.c2, m2 = r.c3;
+    const double str = fma(a, m1.x, b * p2.x), sti = fma(a, m1.y, b * p2.y);
+    const double dtr = fma(a, p1.x, b * m2.x), dti = fma(a, p1.y, b * m2.y);
+    t.re = fma(e.re, str, fma(-e.im, dti, t.re));
+    t.im = fma(e.re, sti, fma(e.im, dtr, t.im));
+    const double spr = fma(b, p1.x, a * m2.x), spi = fma(b, p1.y, a * m2.y);
+    const double dpr = fma(b, m1.x, a * p2.x), dpi = fma(b, m1.y, a * p2.y);
+    ph.re = fma(e.re, spr, fma(-e.im, dpi, ph.re));
+    ph.im = fma(e.re, spi, fma(e.im, dpr, ph.im));
+}
+
+// The mode sums of one coefficient set at D directions (theta[k], phi[k]):
+// every coefficient record and recurrence coefficient a thread loads serves
+// its D directions, whose D independent accumulations also hide each other's
+// latency.  (Measured alternatives, not kept: one thread summing up to four
+// unique frequencies' sets at one direction, which shares the Legendre work
+// but not the loads, no faster; reading the coefficient records one mode
+// ahead in registers, slower.)
+template <int D>
+__device__ void fee_sums(const double (&theta)[D], const double (&phi)[D], const FeeMode* __restrict__ q, int nmax,
+                         const double2* __restrict__ rec, FeeSums (&out)[D]) {
+    double s[D], x[D], sm1[D], sm[D], smp1[D];
+    cplx e1[D], em[D];
+    FeeSums acc[D];
+#pragma unroll
+    for (int k = 0; k < D; k++) {
+        double sph, cph;
+        sincos(theta[k], &s[k], &x[k]);
+        sincos(phi[k], &sph, &cph);
+        e1[k] = cplx{cph, sph};
+        em[k] = cplx{1.0, 0.0};  // e^{i |m| phi}
+        sm1[k] = 0.0;            // sin^{|m|-1}
+        sm[k] = 1.0;             // sin^{|m|}
+        acc[k] = FeeSums{{0, 0}, {0, 0}, {0, 0}, {0, 0}};
+    }
     double rd = 1.0, rd_prev = 0.0;  // R_|m|^|m| and R_{|m|-1}^{|m|-1}: R_0^0 = 1, R_{c+1}^{c+1} = -(2c+1) R_c^c
-    double sm1 = 0.0, sm = 1.0;      // sin^{|m|-1}, sin^{|m|}
     const FeeMode* p = q;
     for (int ma = 0; ma <= nmax; ma++) {
         const double rd_next = -(2.0 * ma + 1.0) * rd;
-        const double smp1 = sm * s;
-        // the three columns at n = ma (previous, current)
-        double pa = rd_prev, ca = x * (2.0 * ma - 1.0) * rd_prev;  // column ma - 1 (ma >= 1)
-        double pb = 0.0, cb = rd;                                  // column ma
-        double pc = 0.0, cc = 0.0;                                 // column ma + 1 (zero below its diagonal)
+        // the three columns at n = ma (previous, current) per direction
+        double pa[D], ca[D], pb[D], cb[D], pc[D], cc[D];
+#pragma unroll
+        for (int k = 0; k < D; k++) {
+            smp1[k] = sm[k] * s[k];
+            pa[k] = rd_prev;
+            ca[k] = x[k] * (2.0 * ma - 1.0) * rd_prev;  // column ma - 1 (ma >= 1)
+            pb[k] = 0.0;
+            cb[k] = rd;  // column ma
+            pc[k] = 0.0;
+            cc[k] = 0.0;  // column ma + 1 (zero below its diagonal)
+        }
         auto advance = [&](int n1) {
-            if (ma >= 1) {
-                const double2 r = __ldg(&rec[n1 * FEE_REC_W + ma - 1]);
-                const double t = fma(r.x * x, ca, -r.y * pa);
-                pa = ca;
-                ca = t;
-            }
-            {
-                const double2 r = __ldg(&rec[n1 * FEE_REC_W + ma]);
-                const double t = fma(r.x * x, cb, -r.y * pb);
-                pb = cb;
-                cb = t;
-            }
-            if (n1 == ma + 1) {
-                pc = 0.0;
-                cc = rd_next;
-            } else {
-                const double2 r = __ldg(&rec[n1 * FEE_REC_W + ma + 1]);
-                const double t = fma(r.x * x, cc, -r.y * pc);
-                pc = cc;
-                cc = t;
+            const double2* row = rec + n1 * FEE_REC_W;
+            const double2 ra = ma >= 1 ? __ldg(row + ma - 1) : make_double2(0.0, 0.0);
+            const double2 rb = __ldg(row + ma);
+            const double2 rc = n1 > ma + 1 ? __ldg(row + ma + 1) : make_double2(0.0, 0.0);
+#pragma unroll
+            for (int k = 0; k < D; k++) {
+                if (ma >= 1) {
+                    const double t = fma(ra.x * x[k], ca[k], -ra.y * pa[k]);
+                    pa[k] = ca[k];
+                    ca[k] = t;
+                }
+                const double tb = fma(rb.x * x[k], cb[k], -rb.y * pb[k]);
+                pb[k] = cb[k];
+                cb[k] = tb;
+                if (n1 == ma + 1) {
+                    pc[k] = 0.0;
+                    cc[k] = rd_next;
+                } else {
+                    const double t = fma(rc.x * x[k], cc[k], -rc.y * pc[k]);
+                    pc[k] = cc[k];
+                    cc[k] = t;
+                }
             }
         };
         int n = ma;
@@ -141,21 +192,41 @@ __device__ void fee_sums(double theta, double phi, const FeeMode* __restrict__ q
             n = 1;
         }
         for (; n <= nmax; n++) {
-            const double p1sin = ma >= 1 ? sm1 * cb : 0.0;
-            const double p1 = ma == 0 ? s * cc : 0.5 * fma(smp1, cc, -(double)((n + ma) * (n - ma + 1)) * sm1 * ca);
-            const double b = fma(ma * x, p1sin, p1);
-            const double a = -ma * p1sin;  // for +m; -m takes -a
-            fee_mode_add(p++, a, b, em, acc);
-            if (ma > 0) fee_mode_add(p++, -a, b, conj(em), acc);
+            double a[D], b[D];
+#pragma unroll
+            for (int k = 0; k < D; k++) {
+                const double p1sin = ma >= 1 ? sm1[k] * cb[k] : 0.0;
+                const double p1 = ma == 0 ? s[k] * cc[k]
+                                          : 0.5 * fma(smp1[k], cc[k], -(double)((n + ma) * (n - ma + 1)) * sm1[k] * ca[k]);
+                b[k] = fma(ma * x[k], p1sin, p1);
+                a[k] = -ma * p1sin;  // for +m (-m has -a)
+            }
+            if (ma == 0) {
+                const FeeMode r = ld_mode(p++);
+#pragma unroll
+                for (int k = 0; k < D; k++) fee_m0_add(r, b[k], acc[k]);
+            } else {
+                const FeeMode rx = ld_mode(p), ry = ld_mode(p + 1);
+                p += 2;
+#pragma unroll
+                for (int k = 0; k < D; k++) {
+                    fee_pair_add(rx, a[k], b[k], em[k], acc[k].tx, acc[k].px);
+                    fee_pair_add(ry, a[k], b[k], em[k], acc[k].ty, acc[k].py);
+                }
+            }
             if (n < nmax) advance(n + 1);
         }
         rd_prev = rd;
         rd = rd_next;
-        sm1 = sm;
-        sm = smp1;
-        em = em * e1;
+#pragma unroll
+        for (int k = 0; k < D; k++) {
+            sm1[k] = sm[k];
+            sm[k] = smp1[k];
+            em[k] = em[k] * e1[k];
+        }
     }
-    out = acc;
+#pragma unroll
+    for (int k = 0; k < D; k++) out[k] = acc[k];
 }
 
 __device__ __forceinline__ J2 fee_jones(const FeeSums& s) {
@@ -188,9 +259,9 @@ __device__ __forceinline__ J2 fee_parallactic(const J2& j, double az, double za,
 }
 
 struct FeeArgs {
-    const FeeMode* sets;  // [uniq tile][uniq freq][stride]
+    const FeeMode* sets;  // [uniq tile][uniq freq][stride], every set laid out for degree nmax
     int stride;
-    const int* nmax;      // [uniq freq]
+    int nmax;
     const double* norm;   // [uniq freq][4], or NULL
     const double2* rec;   // [FEE_MAX_N + 1][FEE_REC_W]
     int n_uniq_freq;
@@ -198,59 +269,82 @@ struct FeeArgs {
     JonesF64* out;        // [uniq tile][uniq freq][n_dirs]
 };
 
-// One thread per direction of one (unique tile, unique frequency) set.
-// RADEC: directions from (RA, Dec) at the LST and latitude given (the
-// modeller's components; rotation always applied); otherwise from (az, za)
-// arrays, rotated when d_lat is set.
-template <bool RADEC>
+// D directions (d0 + k * FEE_BLOCK) of one (unique tile blockIdx.z, unique
+// frequency blockIdx.y) set per thread; a block covers D * FEE_BLOCK
+// directions.  RADEC: directions from (RA, Dec) at the LST and latitude
+// given (the modeller's components; rotation always applied); otherwise from
+// (az, za) arrays, rotated when d_lat is set.  Directions past the end repeat
+// the last one and are not written.
+template <int D, bool RADEC>
 __global__ void __launch_bounds__(FEE_BLOCK) fee_jones_kernel(FeeArgs a, const double* __restrict__ az_in,
                                                              const double* __restrict__ za_in,
                                                              const double2* __restrict__ radec, double lst,
                                                              double lat_v, const double* __restrict__ d_lat) {
-    const int d = blockIdx.x * blockDim.x + threadIdx.x;
+    const int d0 = blockIdx.x * (D * FEE_BLOCK) + threadIdx.x;
     const int uf = blockIdx.y, u = blockIdx.z;
-    if (d >= a.n_dirs) return;
-    double az, za, lat = 0.0;
-    bool rot;
-    if (RADEC) {
-        const double2 rd = radec[d];
-        double el;
-        hadec_to_azel(lst - rd.x, rd.y, lat_v, az, el);
-        za = FRAC_PI_2 - el;
-        rot = true;
-        lat = lat_v;
-    } else {
-        az = az_in[d];
-        za = za_in[d];
-        rot = d_lat != nullptr;
-        if (rot) lat = *d_lat;
+    if (d0 >= a.n_dirs) return;
+    double az[D], za[D], theta[D], phi[D];
+    const bool rot = RADEC || d_lat != nullptr;
+    const double lat = RADEC ? lat_v : (d_lat ? *d_lat : 0.0);
+#pragma unroll
+    for (int k = 0; k < D; k++) {
+        const int d = min(d0 + k * FEE_BLOCK, a.n_dirs - 1);
+        if (RADEC) {
+            const double2 rd = radec[d];
+            double el;
+            hadec_to_azel(lst - rd.x, rd.y, lat_v, az[k], el);
+            za[k] = FRAC_PI_2 - el;
+        } else {
+            az[k] = az_in[d];
+            za[k] = za_in[d];
+        }
+        theta[k] = za[k];
+        phi[k] = FRAC_PI_2 - az[k];
     }
     const size_t set = (size_t)u * a.n_uniq_freq + uf;
-    FeeSums s;
-    fee_sums(za, FRAC_PI_2 - az, a.sets + set * a.stride, a.nmax[uf], a.rec, s);
-    J2 j = fee_jones(s);
-    if (a.norm) {
-        const double* nm = a.norm + 4 * uf;
-        j.a = cplx{j.a.re / nm[0], j.a.im / nm[0]};
-        j.b = cplx{j.b.re / nm[1], j.b.im / nm[1]};
-        j.c = cplx{j.c.re / nm[2], j.c.im / nm[2]};
-        j.d = cplx{j.d.re / nm[3], j.d.im / nm[3]};
+    FeeSums sums[D];
+    fee_sums<D>(theta, phi, a.sets + set * a.stride, a.nmax, a.rec, sums);
+#pragma unroll
+    for (int k = 0; k < D; k++) {
+        const int d = d0 + k * FEE_BLOCK;
+        if (d >= a.n_dirs) break;
+        J2 j = fee_jones(sums[k]);
+        if (a.norm) {
+            const double* nm = a.norm + 4 * uf;
+            j.a = cplx{j.a.re / nm[0], j.a.im / nm[0]};
+            j.b = cplx{j.b.re / nm[1], j.b.im / nm[1]};
+            j.c = cplx{j.c.re / nm[2], j.c.im / nm[2]};
+            j.d = cplx{j.d.re / nm[3], j.d.im / nm[3]};
+        }
+        if (rot) j = fee_parallactic(j, az[k], za[k], lat);
+        a.out[set * a.n_dirs + d] = store_j(j);
     }
-    if (rot) j = fee_parallactic(j, az, za, lat);
-    a.out[set * a.n_dirs + d] = store_j(j);
+}
+
+// Directions per thread.
+constexpr int FEE_DIRS_PER_THREAD = 2;
+
+template <bool RADEC>
+cudaError_t fee_launch(const FeeArgs& a, int n_uniq_tile, const double* az, const double* za, const double2* radec,
+                       double lst, double lat, const double* d_lat, cudaStream_t s) {
+    constexpr int D = FEE_DIRS_PER_THREAD;
+    dim3 g((a.n_dirs + D * FEE_BLOCK - 1) / (D * FEE_BLOCK), a.n_uniq_freq, n_uniq_tile);
+    fee_jones_kernel<D, RADEC><<<g, FEE_BLOCK, 0, s>>>(a, az, za, radec, lst, lat, d_lat);
+    return cudaGetLastError();
 }
 
 // Zenith normalisation: |element k| of the zenith-pointed beam at the zenith,
 // at the azimuth where that element peaks (phi = 0, -pi/2, pi/2, 0).
-__global__ void fee_norm_kernel(const FeeMode* __restrict__ ideal, int stride, const int* __restrict__ nmax,
+__global__ void fee_norm_kernel(const FeeMode* __restrict__ ideal, int stride, int nmax,
                                 const double2* __restrict__ rec, int n_uniq_freq, double* __restrict__ norm) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= 4 * n_uniq_freq) return;
     const int uf = t >> 2, k = t & 3;
-    const double phi = (k == 1) ? -FRAC_PI_2 : (k == 2) ? FRAC_PI_2 : 0.0;
-    FeeSums s;
-    fee_sums(0.0, phi, ideal + (size_t)uf * stride, nmax[uf], rec, s);
-    const J2 j = fee_jones(s);
+    const double theta[1] = {0.0};
+    const double phi[1] = {(k == 1) ? -FRAC_PI_2 : (k == 2) ? FRAC_PI_2 : 0.0};
+    FeeSums s[1];
+    fee_sums<1>(theta, phi, ideal + (size_t)uf * stride, nmax, rec, s);
+    const J2 j = fee_jones(s[0]);
     const cplx e = k == 0 ? j.a : k == 1 ? j.b : k == 2 ? j.c : j.d;
     norm[t] = hypot(e.re, e.im);
 }
@@ -259,9 +353,8 @@ __global__ void fee_norm_kernel(const FeeMode* __restrict__ ideal, int stride, c
 
 struct HdcFeeBeam {
     int device = 0;
-    int ntiles = 0, nfreqs = 0, n_uniq_tile = 0, n_uniq_freq = 0, stride = 0;
+    int ntiles = 0, nfreqs = 0, n_uniq_tile = 0, n_uniq_freq = 0, stride = 0, nmax = 1;
     hdc::FeeMode* d_sets = nullptr;
-    int* d_nmax = nullptr;
     double* d_norm = nullptr;
     double2* d_rec = nullptr;
     int* d_tile_map = nullptr;
@@ -276,13 +369,12 @@ using zc = std::complex<double>;
 
 void fee_release(HdcFeeBeam* b) {
     cudaFree(b->d_sets);
-    cudaFree(b->d_nmax);
     cudaFree(b->d_norm);
     cudaFree(b->d_rec);
     cudaFree(b->d_tile_map);
     cudaFree(b->d_freq_map);
     b->d_sets = nullptr;
-    b->d_nmax = b->d_tile_map = b->d_freq_map = nullptr;
+    b->d_tile_map = b->d_freq_map = nullptr;
     b->d_norm = nullptr;
     b->d_rec = nullptr;
 }
@@ -331,11 +423,15 @@ void fee_set(const HdcFeeCoeffs* f, int k, const double* amps, const uint32_t* d
             (s == 1 ? q1[p] : q2[p])[i] += acc;
         }
     }
-    for (int i = 0; i < M; i++) {
-        const zc a = q1[0][i] * kf[i], b = q2[0][i] * kf[i], c = q1[1][i] * kf[i], d = q2[1][i] * kf[i];
-        out[i] = FeeMode{make_double2(a.real(), a.imag()), make_double2(b.real(), b.imag()),
-                         make_double2(c.real(), c.imag()), make_double2(d.real(), d.imag())};
-    }
+    auto d2 = [](zc z) { return make_double2(z.real(), z.imag()); };
+    for (int i = 0; i < nmax; i++)  // m = 0: (q1 X, q2 X, q1 Y, q2 Y)
+        out[i] = FeeMode{d2(q1[0][i] * kf[i]), d2(q2[0][i] * kf[i]), d2(q1[1][i] * kf[i]), d2(q2[1][i] * kf[i])};
+    for (int i = nmax; i < M; i += 2)  // +m at i, -m at i + 1 -> (P1, M1, P2, M2) of X at i, of Y at i + 1
+        for (int pol = 0; pol < 2; pol++) {
+            const zc a1 = q1[pol][i] * kf[i], b1 = q1[pol][i + 1] * kf[i + 1];
+            const zc a2 = q2[pol][i] * kf[i], b2 = q2[pol][i + 1] * kf[i + 1];
+            out[i + pol] = FeeMode{d2(a1 + b1), d2(a1 - b1), d2(a2 + b2), d2(a2 - b2)};
+        }
 }
 
 int fee_check_file(const HdcFeeCoeffs* f) {
@@ -365,11 +461,9 @@ int fee_check_file(const HdcFeeCoeffs* f) {
 int fee_launch_radec(const HdcFeeBeam* b, const double2* d_radec, int n, double lst, double lat, JonesF64* d_out,
                      cudaStream_t s) {
     if (n <= 0) return HDC_OK;
-    FeeArgs a{b->d_sets, b->stride, b->d_nmax, b->d_norm, b->d_rec, b->n_uniq_freq, n, d_out};
-    dim3 g((n + FEE_BLOCK - 1) / FEE_BLOCK, b->n_uniq_freq, b->n_uniq_tile);
-    fee_jones_kernel<true><<<g, FEE_BLOCK, 0, s>>>(a, nullptr, nullptr, d_radec, lst, lat, nullptr);
+    FeeArgs a{b->d_sets, b->stride, b->nmax, b->d_norm, b->d_rec, b->n_uniq_freq, n, d_out};
+    HDC_CUDA_RET_INT(fee_launch<true>(a, b->n_uniq_tile, nullptr, nullptr, d_radec, lst, lat, nullptr, s));
     count_launches(1);
-    HDC_CUDA_RET_INT(cudaGetLastError());
     return HDC_OK;
 }
 
@@ -443,21 +537,20 @@ extern "C" int hdc_fee_beam_new(const HdcFeeCoeffs* file, const uint32_t* h_freq
         tmap[t] = found;
     }
     const int nu = (int)uamp.size(), nuf = (int)ufile.size();
-    std::vector<int> nmax(nuf, 1);
-    int nmax_all = 1;
+    // every set is laid out for the largest degree of all the unique
+    // frequencies (zero coefficients above a frequency's own): one stride and
+    // one loop for all sets
+    int nmax = 1;
     for (int i = 0; i < nuf; i++) {
         const int k = ufile[i];
-        for (int c = 0; c < file->num_freq_modes[k]; c++) nmax[i] = std::max(nmax[i], (int)file->modes[2 * file->num_modes + c]);
-        nmax_all = std::max(nmax_all, nmax[i]);
+        for (int c = 0; c < file->num_freq_modes[k]; c++) nmax = std::max(nmax, (int)file->modes[2 * file->num_modes + c]);
     }
-    const int stride = fee_num_modes(nmax_all);
+    const int stride = fee_num_modes(nmax);
     std::vector<FeeMode> sets((size_t)nu * nuf * stride);
-    std::vector<std::vector<zc>> kf(nuf);
-    for (int i = 0; i < nuf; i++) kf[i] = fee_factors(nmax[i]);
+    const std::vector<zc> kf = fee_factors(nmax);
     for (int u = 0; u < nu; u++)
         for (int i = 0; i < nuf; i++)
-            fee_set(file, ufile[i], uamp[u].data(), udel[u].data(), nmax[i], kf[i],
-                    sets.data() + ((size_t)u * nuf + i) * stride);
+            fee_set(file, ufile[i], uamp[u].data(), udel[u].data(), nmax, kf, sets.data() + ((size_t)u * nuf + i) * stride);
     // recurrence coefficients (2n-1)/(n-c), (n+c-1)/(n-c) for c < n
     std::vector<double2> rec((size_t)(FEE_MAX_N + 1) * FEE_REC_W, make_double2(0.0, 0.0));
     for (int n = 1; n <= FEE_MAX_N; n++)
@@ -471,6 +564,7 @@ extern "C" int hdc_fee_beam_new(const HdcFeeCoeffs* file, const uint32_t* h_freq
     b->n_uniq_tile = nu;
     b->n_uniq_freq = nuf;
     b->stride = stride;
+    b->nmax = nmax;
     b->tile_map = tmap;
     b->freq_map = fmap;
     auto fail = [&](cudaError_t e, const char* what) {
@@ -481,13 +575,10 @@ extern "C" int hdc_fee_beam_new(const HdcFeeCoeffs* file, const uint32_t* h_freq
     };
     cudaError_t e;
     if ((e = cudaMalloc(&b->d_sets, sizeof(FeeMode) * sets.size())) != cudaSuccess) return fail(e, "cudaMalloc");
-    if ((e = cudaMalloc(&b->d_nmax, sizeof(int) * nuf)) != cudaSuccess) return fail(e, "cudaMalloc");
     if ((e = cudaMalloc(&b->d_rec, sizeof(double2) * rec.size())) != cudaSuccess) return fail(e, "cudaMalloc");
     if ((e = cudaMalloc(&b->d_tile_map, sizeof(int) * num_tiles)) != cudaSuccess) return fail(e, "cudaMalloc");
     if ((e = cudaMalloc(&b->d_freq_map, sizeof(int) * num_freqs)) != cudaSuccess) return fail(e, "cudaMalloc");
     if ((e = cudaMemcpy(b->d_sets, sets.data(), sizeof(FeeMode) * sets.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
-        return fail(e, "cudaMemcpy");
-    if ((e = cudaMemcpy(b->d_nmax, nmax.data(), sizeof(int) * nuf, cudaMemcpyHostToDevice)) != cudaSuccess)
         return fail(e, "cudaMemcpy");
     if ((e = cudaMemcpy(b->d_rec, rec.data(), sizeof(double2) * rec.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
         return fail(e, "cudaMemcpy");
@@ -501,7 +592,7 @@ extern "C" int hdc_fee_beam_new(const HdcFeeCoeffs* file, const uint32_t* h_freq
         const std::vector<double> ones(32, 1.0);
         const std::vector<uint32_t> zeros(16, 0u);
         for (int i = 0; i < nuf; i++)
-            fee_set(file, ufile[i], ones.data(), zeros.data(), nmax[i], kf[i], ideal.data() + (size_t)i * stride);
+            fee_set(file, ufile[i], ones.data(), zeros.data(), nmax, kf, ideal.data() + (size_t)i * stride);
         FeeMode* d_ideal = nullptr;
         if ((e = cudaMalloc(&d_ideal, sizeof(FeeMode) * ideal.size())) != cudaSuccess) return fail(e, "cudaMalloc");
         if ((e = cudaMalloc(&b->d_norm, sizeof(double) * 4 * nuf)) != cudaSuccess) {
@@ -510,7 +601,7 @@ extern "C" int hdc_fee_beam_new(const HdcFeeCoeffs* file, const uint32_t* h_freq
         }
         e = cudaMemcpy(d_ideal, ideal.data(), sizeof(FeeMode) * ideal.size(), cudaMemcpyHostToDevice);
         if (e == cudaSuccess) {
-            fee_norm_kernel<<<(4 * nuf + 127) / 128, 128>>>(d_ideal, stride, b->d_nmax, b->d_rec, nuf, b->d_norm);
+            fee_norm_kernel<<<(4 * nuf + 127) / 128, 128>>>(d_ideal, stride, nmax, b->d_rec, nuf, b->d_norm);
             count_launches(1);
             e = cudaGetLastError();
         }
@@ -562,11 +653,9 @@ extern "C" int hdc_fee_calc_jones(const HdcFeeBeam* b, const double* d_az_rad, c
         return HDC_ERR_ARG;
     }
     if (num_directions == 0) return HDC_OK;
-    FeeArgs a{b->d_sets, b->stride, b->d_nmax, b->d_norm, b->d_rec, b->n_uniq_freq, num_directions, d_jones};
-    dim3 g((num_directions + FEE_BLOCK - 1) / FEE_BLOCK, b->n_uniq_freq, b->n_uniq_tile);
-    fee_jones_kernel<false><<<g, FEE_BLOCK, 0, (cudaStream_t)stream>>>(a, d_az_rad, d_za_rad, nullptr, 0.0, 0.0,
-                                                                       d_latitude_rad);
+    FeeArgs a{b->d_sets, b->stride, b->nmax, b->d_norm, b->d_rec, b->n_uniq_freq, num_directions, d_jones};
+    HDC_CUDA_RET_INT(fee_launch<false>(a, b->n_uniq_tile, d_az_rad, d_za_rad, nullptr, 0.0, 0.0, d_latitude_rad,
+                                       (cudaStream_t)stream));
     count_launches(1);
-    HDC_CUDA_RET_INT(cudaGetLastError());
     return HDC_OK;
 }
