@@ -448,6 +448,15 @@ int hdc_fee_calc_jones(const HdcFeeBeam *b, const double *d_az_rad, const double
  * been prepared for the modeller's channel frequencies and tile count, and
  * must stay alive while the modeller uses it. */
 int hdc_modeller_set_fee_beam(HdcModeller *m, const HdcFeeBeam *b);
+/* hdc_source_brightness with the FEE beam, as veto_sources evaluates it
+ * (srclist/veto.rs:99-104: calc_jones with no tile, i.e. the observation's
+ * ideal delays and unit gains, beam/fee.rs:287-292): beam is prepared for
+ * one tile with those delays and gains and for the num_freqs frequencies
+ * h_freqs. */
+int hdc_source_brightness_fee(const HdcSkyModel *sky, const int *h_comp_source, int num_sources,
+                              const double *h_freqs, int num_freqs, double lst_rad, double latitude_rad,
+                              RADec phase_centre, const HdcFeeBeam *beam, double source_dist_cutoff_rad,
+                              double min_elevation_rad, double *h_brightness);
 
 /* SkyModeller::model_timestep_with at a given LMST (the device-level form the
  * reference's peel loop calls, model/gpu.rs:1152-1166): d_vis_fb [freq][bl]

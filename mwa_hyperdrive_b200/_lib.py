@@ -180,6 +180,8 @@ SIGNATURES = {
     "hdc_probe_fp64_gflops": (c_int, [ctypes.POINTER(c_double)]),
     "hdc_source_brightness": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_int, c_double, c_double, RADec, c_int,
                                       c_double, c_double, c_void_p]),
+    "hdc_source_brightness_fee": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_int, c_double, c_double, RADec, c_void_p,
+                                      c_double, c_double, c_void_p]),
     "hdc_probe_fp32_gflops": (c_int, [ctypes.POINTER(c_double)]),
     "hdc_scale_by_weights": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_void_p, c_void_p]),
     "hdc_into_cal_sols": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_int, c_void_p, c_int, c_int, c_void_p,

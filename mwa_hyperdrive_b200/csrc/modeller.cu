@@ -754,7 +754,8 @@ namespace hdc {
 // total at that frequency.
 __global__ void veto_kernel(const double2* radec, const int* comp_source, int nc, const double* freqs, int nf,
                             double lst, double lat, double pc_ra, double pc_dec, int beam_kind, double cutoff,
-                            double min_el, const JonesF64* S, double* src_fd, int* src_vetoed) {
+                            double min_el, const JonesF64* S, const JonesF64* B, const int* bmap, double* src_fd,
+                            int* src_vetoed) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     const int f = blockIdx.y;
     if (c >= nc) return;
@@ -774,19 +775,33 @@ __global__ void veto_kernel(const double2* radec, const int* comp_source, int nc
     if (beam_kind == HDC_BEAM_ANALYTIC_DIPOLE) {
         const J2 b = analytic_beam(az, el, freqs[f]);
         s = b * (s * herm(b));
+    } else if (beam_kind == HDC_BEAM_FEE) {
+        // the FEE table [unique frequency][component] of the one beam
+        const J2 b = load_j(B[(size_t)bmap[f] * nc + c]);
+        s = b * (s * herm(b));
     }
     atomicAdd(src_fd + (size_t)src * nf + f, hypot(s.a.re, s.a.im) + hypot(s.d.re, s.d.im));
 }
 }  // namespace hdc
 
-extern "C" int hdc_source_brightness(const HdcSkyModel* sky, const int* h_comp_source, int num_sources,
-                                     const double* h_freqs, int num_freqs, double lst_rad, double latitude_rad,
-                                     RADec phase_centre, int beam_kind, double source_dist_cutoff_rad,
-                                     double min_elevation_rad, double* h_brightness) {
-    using namespace hdc;
+namespace hdc {
+// hdc_source_brightness and hdc_source_brightness_fee: fee is the FEE beam
+// when beam_kind is HDC_BEAM_FEE.
+static int source_brightness(const HdcSkyModel* sky, const int* h_comp_source, int num_sources, const double* h_freqs,
+                             int num_freqs, double lst_rad, double latitude_rad, RADec phase_centre, int beam_kind,
+                             const HdcFeeBeam* fee, double source_dist_cutoff_rad, double min_elevation_rad,
+                             double* h_brightness) {
     if (!sky || !h_comp_source || !h_freqs || !h_brightness || num_sources < 1 || num_freqs < 1 ||
-        (beam_kind != HDC_BEAM_NONE && beam_kind != HDC_BEAM_ANALYTIC_DIPOLE)) {
+        (beam_kind != HDC_BEAM_NONE && beam_kind != HDC_BEAM_ANALYTIC_DIPOLE && beam_kind != HDC_BEAM_FEE)) {
         set_error("hdc_source_brightness: invalid arguments");
+        return HDC_ERR_ARG;
+    }
+    int dev = 0;
+    HDC_CUDA_RET_INT(cudaGetDevice(&dev));
+    if (beam_kind == HDC_BEAM_FEE &&
+        (!fee || fee_num_freqs(fee) != num_freqs || hdc_fee_beam_num_unique_tiles(fee) != 1 || fee_device(fee) != dev)) {
+        set_error("hdc_source_brightness_fee: the beam must be prepared on the current device for one tile (the "
+                  "ideal delays, unit gains) and the %d frequencies given", num_freqs);
         return HDC_ERR_ARG;
     }
     const int nc = sky->num_components, nf = num_freqs;
@@ -831,7 +846,11 @@ extern "C" int hdc_source_brightness(const HdcSkyModel* sky, const int* h_comp_s
         double2* d_radec = nullptr;
         int *d_src = nullptr, *d_vet = nullptr;
         double *d_freqs = nullptr, *d_fd = nullptr;
+        JonesF64* d_B = nullptr;
+        int* d_bmap = nullptr;
         auto release = [&]() {
+            dfree(d_B);
+            dfree(d_bmap);
             dfree(d_S);
             dfree(d_fc);
             dfree(d_radec);
@@ -854,14 +873,28 @@ extern "C" int hdc_source_brightness(const HdcSkyModel* sky, const int* h_comp_s
         if (e == cudaSuccess) e = cudaMemcpy(d_freqs, h_freqs, sizeof(double) * nf, cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = cudaMemset(d_vet, 0, sizeof(int) * num_sources);
         if (e == cudaSuccess) e = cudaMemset(d_fd, 0, sizeof(double) * fd.size());
-        if (e == cudaSuccess) {
+        int rc_fee = HDC_OK;
+        if (e == cudaSuccess && beam_kind == HDC_BEAM_FEE) {
+            // the beam's Jones at every component for each unique frequency
+            // (on the legacy stream, ahead of the veto kernel)
+            e = dalloc(&d_B, (size_t)hdc_fee_beam_num_unique_freqs(fee) * nc);
+            if (e == cudaSuccess) e = dalloc(&d_bmap, (size_t)nf);
+            if (e == cudaSuccess)
+                e = cudaMemcpy(d_bmap, hdc_fee_beam_freq_map(fee), sizeof(int) * nf, cudaMemcpyDeviceToDevice);
+            if (e == cudaSuccess) rc_fee = fee_launch_radec(fee, d_radec, nc, lst_rad, latitude_rad, d_B, 0);
+        }
+        if (e == cudaSuccess && rc_fee == HDC_OK) {
             const dim3 g((nc + 127) / 128, nf);
             flux_kernel<<<g, 128>>>(d_fc, nc, d_freqs, nf, d_S);
             veto_kernel<<<g, 128>>>(d_radec, d_src, nc, d_freqs, nf, lst_rad, latitude_rad, phase_centre.ra,
                                     phase_centre.dec, beam_kind, source_dist_cutoff_rad, min_elevation_rad, d_S,
-                                    d_fd, d_vet);
+                                    d_B, d_bmap, d_fd, d_vet);
             count_launches(2);
             e = cudaGetLastError();
+        }
+        if (rc_fee != HDC_OK) {
+            release();
+            return rc_fee;
         }
         if (e == cudaSuccess) e = cudaMemcpy(fd.data(), d_fd, sizeof(double) * fd.size(), cudaMemcpyDeviceToHost);
         if (e == cudaSuccess)
@@ -878,6 +911,29 @@ extern "C" int hdc_source_brightness(const HdcSkyModel* sky, const int* h_comp_s
         h_brightness[s] = vetoed[s] ? -1.0 : m;
     }
     return HDC_OK;
+}
+}  // namespace hdc
+
+extern "C" int hdc_source_brightness(const HdcSkyModel* sky, const int* h_comp_source, int num_sources,
+                                     const double* h_freqs, int num_freqs, double lst_rad, double latitude_rad,
+                                     RADec phase_centre, int beam_kind, double source_dist_cutoff_rad,
+                                     double min_elevation_rad, double* h_brightness) {
+    if (beam_kind == HDC_BEAM_FEE) {
+        hdc::set_error("hdc_source_brightness: the FEE beam goes through hdc_source_brightness_fee");
+        return HDC_ERR_ARG;
+    }
+    return hdc::source_brightness(sky, h_comp_source, num_sources, h_freqs, num_freqs, lst_rad, latitude_rad,
+                                  phase_centre, beam_kind, nullptr, source_dist_cutoff_rad, min_elevation_rad,
+                                  h_brightness);
+}
+
+extern "C" int hdc_source_brightness_fee(const HdcSkyModel* sky, const int* h_comp_source, int num_sources,
+                                         const double* h_freqs, int num_freqs, double lst_rad, double latitude_rad,
+                                         RADec phase_centre, const HdcFeeBeam* beam, double source_dist_cutoff_rad,
+                                         double min_elevation_rad, double* h_brightness) {
+    return hdc::source_brightness(sky, h_comp_source, num_sources, h_freqs, num_freqs, lst_rad, latitude_rad,
+                                  phase_centre, HDC_BEAM_FEE, beam, source_dist_cutoff_rad, min_elevation_rad,
+                                  h_brightness);
 }
 
 extern "C" int hdc_modeller_new(const HdcSkyModel* sky, int pols, const XYZ* h_xyzs, int num_tiles,

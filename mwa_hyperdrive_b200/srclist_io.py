@@ -273,7 +273,7 @@ def veto_sources(source_list: sl.SourceList, phase_centre, lst_rad: float, array
                  freqs_hz, beam: str = "none", num_sources: Optional[int] = None,
                  source_dist_cutoff_deg: float = DEFAULT_CUTOFF_DISTANCE_DEG,
                  veto_threshold: float = DEFAULT_VETO_THRESHOLD_JY,
-                 min_elevation_deg: float = DEFAULT_ELEVATION_LIMIT_DEG) -> sl.SourceList:
+                 min_elevation_deg: float = DEFAULT_ELEVATION_LIMIT_DEG, fee_beam=None) -> sl.SourceList:
     """veto_sources (srclist/veto.rs:44-188): a new list without the sources
     that have a component below the elevation limit or farther than the
     cutoff from the phase centre, or whose beam-attenuated brightness (XX +
@@ -281,7 +281,11 @@ def veto_sources(source_list: sl.SourceList, phase_centre, lst_rad: float, array
     ``freqs_hz``; sorted brightest first (by that smallest brightness) and cut
     to the first ``num_sources``.  The brightness is computed on the GPU
     (hdc_source_brightness).  Raises if fewer than ``num_sources`` remain.
-    The predictor then models the list in reverse, dimmest first."""
+    The predictor then models the list in reverse, dimmest first.  ``beam`` is
+    "none", "analytic" or "fee"; for "fee", ``fee_beam`` is a
+    :class:`mwa_hyperdrive_b200.fee.FeeBeam` prepared for one tile with the
+    observation's ideal delays and unit gains at ``freqs_hz`` (the reference
+    asks its beam for no tile, beam/fee.rs:287-292)."""
     import ctypes
 
     from . import _lib
@@ -299,14 +303,24 @@ def veto_sources(source_list: sl.SourceList, phase_centre, lst_rad: float, array
     freqs = np.ascontiguousarray(freqs_hz, np.float64)
     out = np.zeros(len(names))
     beams = {"none": 0, "analytic": 1}
-    if beam not in beams:
+    if beam == "fee":
+        if fee_beam is None:
+            raise SourceListError('beam "fee" needs fee_beam')
+        rc = _lib.lib().hdc_source_brightness_fee(ctypes.byref(sky.struct()), comp_source.ctypes.data, len(names),
+                                                  freqs.ctypes.data, freqs.size, float(lst_rad),
+                                                  float(array_latitude_rad), _lib.RADec(*phase_centre),
+                                                  fee_beam.handle, math.radians(source_dist_cutoff_deg),
+                                                  math.radians(min_elevation_deg), out.ctypes.data)
+        _lib.check(rc, "hdc_source_brightness_fee")
+    elif beam in beams:
+        rc = _lib.lib().hdc_source_brightness(ctypes.byref(sky.struct()), comp_source.ctypes.data, len(names),
+                                              freqs.ctypes.data, freqs.size, float(lst_rad), float(array_latitude_rad),
+                                              _lib.RADec(*phase_centre), beams[beam],
+                                              math.radians(source_dist_cutoff_deg), math.radians(min_elevation_deg),
+                                              out.ctypes.data)
+        _lib.check(rc, "hdc_source_brightness")
+    else:
         raise SourceListError(f"unknown beam {beam!r}")
-    rc = _lib.lib().hdc_source_brightness(ctypes.byref(sky.struct()), comp_source.ctypes.data, len(names),
-                                          freqs.ctypes.data, freqs.size, float(lst_rad), float(array_latitude_rad),
-                                          _lib.RADec(*phase_centre), beams[beam],
-                                          math.radians(source_dist_cutoff_deg), math.radians(min_elevation_deg),
-                                          out.ctypes.data)
-    _lib.check(rc, "hdc_source_brightness")
     keep = [(out[k], n) for k, n in enumerate(names) if out[k] >= 0.0 and out[k] >= veto_threshold]
     keep.sort(key=lambda t: -t[0])  # brightest first
     if num_sources is not None:

@@ -188,3 +188,61 @@ def test_modeller_with_fee_beam_tensor_form(oracle):
     got = vis.cpu().numpy()
     nrm = np.linalg.norm(got - ref) / np.linalg.norm(ref)
     assert nrm < 1e-6, nrm
+
+
+def test_veto_brightness_with_the_fee_beam(oracle):
+    """hdc_source_brightness_fee (veto_sources with the FEE beam: no tile, so
+    the ideal delays and unit gains) against the oracle's flux estimates and
+    FEE Jones, and veto_sources' beam="fee" path."""
+    from mwa_hyperdrive_b200 import srclist_io as io
+
+    rng = np.random.default_rng(8)
+    pc = (0.2, math.radians(-27.0))
+    lst = 0.25
+    s = sl.SourceList()
+    for k in range(25):
+        comps = []
+        for _ in range(int(rng.integers(1, 4))):
+            ra = (math.degrees(pc[0]) + rng.uniform(-25, 25)) % 360.0
+            dec = math.degrees(pc[1]) + rng.uniform(-25, 25)
+            fd = sl.FluxDensity(150e6, float(rng.lognormal()), 0.0, 0.0, 0.0)
+            comps.append(sl.SourceComponent(math.radians(ra), math.radians(dec), sl.Point(), sl.PowerLaw(-0.8, fd)))
+        s[f"s{k}"] = sl.Source(comps)
+    freqs = np.array([166.4e6, 168.96e6, 170.24e6])
+    ideal = np.array([(d % 4) + (d // 4) for d in range(16)], np.uint32)
+    beam = FeeBeam(FILE, freqs, ideal[None, :], np.ones((1, 32)))
+    names = list(s.keys())
+    comps, owner = [], []
+    for k, n in enumerate(names):
+        for c in s[n].components:
+            comps.append(c)
+            owner.append(k)
+    sky = sl.SkyModelArrays.from_components(comps)
+    owner = np.ascontiguousarray(owner, np.int32)
+    got = np.zeros(len(names))
+    _lib.check(_lib.lib().hdc_source_brightness_fee(ctypes.byref(sky.struct()), owner.ctypes.data, len(names),
+                                                    freqs.ctypes.data, freqs.size, lst, LAT, _lib.RADec(*pc),
+                                                    beam.handle, math.radians(180.0), 0.0, got.ctypes.data),
+               "hdc_source_brightness_fee")
+    exp = np.zeros(len(names))
+    inst = oracle.inst_flux(sky, freqs)  # [f][c][8]
+    tot = np.zeros((len(names), freqs.size))
+    for c, comp in enumerate(comps):
+        az, el = oracle.hadec_to_azel(lst - comp.ra, comp.dec, LAT)
+        for f, nu in enumerate(freqs):
+            j = fr.calc_jones(FILE, az, math.pi / 2 - el, nu, ideal, np.ones(32), latitude=LAT)[0]
+            J = j.reshape(2, 2)
+            i = inst[f, c]
+            inst_j = np.array([[i[0] + 1j * i[1], i[2] + 1j * i[3]], [i[4] + 1j * i[5], i[6] + 1j * i[7]]])
+            m = J @ inst_j @ J.conj().T
+            tot[owner[c], f] += abs(m[0, 0]) + abs(m[1, 1])
+    below = np.array([any(oracle.hadec_to_azel(lst - c.ra, c.dec, LAT)[1] < 0.0 for c in s[n].components)
+                      for n in names])
+    exp = np.where(below, -1.0, tot.min(axis=1))
+    np.testing.assert_allclose(got, exp, rtol=1e-11)
+    out = io.veto_sources(s, pc, lst, LAT, freqs, beam="fee", fee_beam=beam, veto_threshold=0.05)
+    keep = sorted([(exp[k], n) for k, n in enumerate(names) if exp[k] >= 0.05], key=lambda t: -t[0])
+    assert list(out.keys()) == [n for _, n in keep]
+    with pytest.raises(_lib.HdcError):  # a beam of two tiles is not the reference's tile-less beam
+        two = FeeBeam(FILE, freqs, np.stack([ideal, ideal + 1]), np.ones((2, 32)))
+        io.veto_sources(s, pc, lst, LAT, freqs, beam="fee", fee_beam=two)

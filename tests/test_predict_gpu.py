@@ -258,7 +258,13 @@ def _rime_tables(sky_arr, obs, beam_tiles=None, seed=0):
 
 
 @pytest.mark.parametrize("ctype", [0, 1, 2])
-def test_dropin_model_functions_per_tile_beam(oracle, ctype):
+@pytest.mark.parametrize("fee", [False, True])
+def test_dropin_model_functions_per_tile_beam(oracle, ctype, fee):
+    """The drop-in model_* with a per-tile beam table [uniq tile][uniq freq]
+    [component] and its maps: a random table, or (fee) the reference's own
+    flow, where BeamGpu::calc_jones_pair fills the table and the Addresses
+    carry the beam's device tile and frequency maps (model/gpu.rs:889-910),
+    here hdc_fee_calc_jones and hdc_fee_beam_tile_map / _freq_map."""
     obs = small_obs(12, 5)
     rng = np.random.default_rng(11 + ctype)
     pc = obs.phase_centre
@@ -283,6 +289,20 @@ def test_dropin_model_functions_per_tile_beam(oracle, ctype):
     beam = (rng.normal(size=(3, 2, 9, 8)) * 0.3)
     beam[..., 0] += 1.0
     beam[..., 6] += 1.0
+    n_uniq_freq = 2
+    if fee:
+        from mwa_hyperdrive_b200.fee import FeeBeam
+
+        delays = np.tile(np.arange(16, dtype=np.uint32) % 4, (nt, 1))
+        delays[1, 3] = delays[4, 9] = 32  # dead dipoles: three unique tiles
+        fb = FeeBeam(synth.fee_coeffs([160000000, 161280000, 162560000, 163840000], 7, seed=2), obs.freqs, delays,
+                     np.ones((nt, 32)))
+        tile_map, freq_map = fb.maps()
+        n_uniq_freq = fb.num_unique_freqs()
+        azza = [oracle.hadec_to_azel(lst - c.ra, c.dec, LAT) for c in comps]
+        az = np.array([a for a, _ in azza])
+        za = np.array([math.pi / 2 - e for _, e in azza])
+        beam = fb.calc_jones(az, za, latitude_rad=LAT).cpu().numpy()
     lmn = np.array([oracle.lmn_rime(c.ra, c.dec, *pc) for c in comps])
     inst150 = oracle.inst_flux(sky, [150e6])[0]
     list_fds = oracle.inst_flux(sky, obs.freqs)[:, 6:9]  # [nf][3][8]
@@ -317,7 +337,9 @@ def test_dropin_model_functions_per_tile_beam(oracle, ctype):
     bj = put("beam", beam)
     d_uvws = put("uvws", uvws)
     vis = torch.zeros((nf, nbl, 8), dtype=torch.float32, device="cuda")
-    a = _lib.Addresses(nf, nf * nbl, nbl, freqs, 0, 2, tm, fm, um)
+    if fee:  # the beam's own device maps, as the reference's Addresses carry them
+        tm, fm = _lib.lib().hdc_fee_beam_tile_map(fb.handle), _lib.lib().hdc_fee_beam_freq_map(fb.handle)
+    a = _lib.Addresses(nf, nf * nbl, nbl, freqs, 0, n_uniq_freq, tm, fm, um)
     L = _lib.lib()
     o3 = lambda off: lm + off * 24  # noqa: E731
     if ctype == 0:
@@ -337,7 +359,7 @@ def test_dropin_model_functions_per_tile_beam(oracle, ctype):
     # oracle with the explicit per-tile beam
     bj_t = [None, None, None]
     bj_t[ctype] = beam
-    b = oracle.beam_struct(2, bj_t, tile_map, freq_map, 2)
+    b = oracle.beam_struct(2, bj_t, tile_map, freq_map, n_uniq_freq)
     ref = oracle.model_type(ctype, sky, obs.tile_xyzs, obs.freqs, pc, lst, LAT, uvws, beam=b)
     assert_f32_close(vis.cpu().numpy(), ref, ulps=4)
 
