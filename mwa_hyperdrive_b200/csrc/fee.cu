@@ -59,31 +59,29 @@
 namespace hdc {
 
 constexpr int FEE_MAX_N = 64;              // largest mode degree n supported
-constexpr int FEE_REC_W = FEE_MAX_N + 2;   // recurrence table row: columns 0 .. n_max + 1
 constexpr double FEE_DELAY_STEP = 435e-12; // seconds per delay step
 constexpr uint32_t FEE_DEAD_DELAY = 32;    // delay value marking a dead dipole
 constexpr int FEE_BLOCK = 128;
 
-// One 64-byte coefficient record in kernel order (K_mn folded in).  An m = 0
-// mode is one record (q1 X, q2 X, q1 Y, q2 Y); the modes +m and -m of one
-// degree are a pair of records, X then Y, each (P1, M1, P2, M2) with
-// P = q(+m) + q(-m) and M = q(+m) - q(-m): the two modes share P1sin, P1 and
-// e^{-i m phi} = conj(e^{i m phi}), so with the sums and differences stored
-// their contribution is Re(e) (s) + i Im(e) (d) (below).
+// One 64-byte coefficient record (K_mn folded in).  The records of a set are
+// stored in the order the kernel visits them: for |m| = 1 .. nmax, for
+// n = |m| .. nmax: (for |m| = 1 only) the m = 0 mode of degree n as
+// (q1 X, q2 X, q1 Y, q2 Y), then the pair +|m|, -|m| of degree n as two
+// records, X then Y, each (P1, M1, P2, M2) with P = q(+m) + q(-m) and
+// M = q(+m) - q(-m).
 struct FeeMode {
     double2 c0, c1, c2, c3;
 };
 
-// Modes of a set whose largest degree is nmax: n = 1..nmax, m = -n..n.
+// Records of a set whose largest degree is nmax: n = 1..nmax, m = -n..n.
 inline int fee_num_modes(int nmax) { return nmax * (nmax + 2); }
 
-// Position of mode (m, n) in kernel order for largest degree nmax.
-inline int fee_kernel_index(int nmax, int m, int n) {
-    const int a = m < 0 ? -m : m;
-    if (a == 0) return n - 1;
-    const int k = a - 1;  // blocks of |m| = 1 .. a - 1 before this one, after the m = 0 block
-    return nmax + 2 * k * (nmax + 1) - k * (k + 1) + 2 * (n - a) + (m < 0 ? 1 : 0);
-}
+// Per (n, |m|) constants of the column recurrence: n + 1 and n - |m| + 1 (the
+// derivative identity) and the coefficients that take R^|m| from degrees
+// n, n + 1 to n + 2: (2n+3)/(n+2-|m|) and (n+1+|m|)/(n+2-|m|).
+struct FeeRec {
+    double c1, c2, al, be;
+};
 
 struct FeeSums {
     cplx tx, px, ty, py;  // sigma_T and sigma_P / j of the X and Y rows
@@ -93,7 +91,8 @@ __device__ __forceinline__ FeeMode ld_mode(const FeeMode* __restrict__ p) {
     return FeeMode{__ldg(&p->c0), __ldg(&p->c1), __ldg(&p->c2), __ldg(&p->c3)};
 }
 
-// An m = 0 mode (e = 1, a = 0): sigma_T += b q2, sigma_P / j += b q1.
+// An m = 0 mode (e = 1, a = 0, b = P1 = P_n^1): sigma_T += b q2,
+// sigma_P / j += b q1.
 __device__ __forceinline__ void fee_m0_add(const FeeMode& r, double b, FeeSums& s) {
     s.tx.re = fma(b, r.c1.x, s.tx.re);
     s.tx.im = fma(b, r.c1.y, s.tx.im);
@@ -105,33 +104,35 @@ __device__ __forceinline__ void fee_m0_add(const FeeMode& r, double b, FeeSums& 
     s.py.im = fma(b, r.c2.y, s.py.im);
 }
 
-// The pair +m, -m of one polarisation, record (P1, M1, P2, M2), a = -|m|
-// P1sin, e = e^{i |m| phi}:
+// The pair +m, -m of one polarisation, record (P1, M1, P2, M2), with
+// ra = Re(e) a, rb = Re(e) b, ia = Im(e) a, ib = Im(e) b (e = e^{i |m| phi},
+// a = -|m| P1sin):
 //   sigma_T     += Re(e) (a M1 + b P2) + i Im(e) (a P1 + b M2)
 //   sigma_P / j += Re(e) (b P1 + a M2) + i Im(e) (b M1 + a P2)
-__device__ __forceinline__ void fee_pair_add(const FeeMode& r, double a, double b, cplx e, cplx& t, cplx& ph) {
+// 16 fused multiply-adds.
+__device__ __forceinline__ void fee_pair_add(const FeeMode& r, double ra, double rb, double ia, double ib, cplx& t,
+                                             cplx& ph) {
     const double2 p1 = r.c0, m1 = r.c1, p2 = r.c2, m2 = r.c3;
-    const double str = fma(a, m1.x, b * p2.x), sti = fma(a, m1.y, b * p2.y);
-    const double dtr = fma(a, p1.x, b * m2.x), dti = fma(a, p1.y, b * m2.y);
-    t.re = fma(e.re, str, fma(-e.im, dti, t.re));
-    t.im = fma(e.re, sti, fma(e.im, dtr, t.im));
-    const double spr = fma(b, p1.x, a * m2.x), spi = fma(b, p1.y, a * m2.y);
-    const double dpr = fma(b, m1.x, a * p2.x), dpi = fma(b, m1.y, a * p2.y);
-    ph.re = fma(e.re, spr, fma(-e.im, dpi, ph.re));
-    ph.im = fma(e.re, spi, fma(e.im, dpr, ph.im));
+    t.re = fma(ra, m1.x, fma(rb, p2.x, fma(-ia, p1.y, fma(-ib, m2.y, t.re))));
+    t.im = fma(ra, m1.y, fma(rb, p2.y, fma(ia, p1.x, fma(ib, m2.x, t.im))));
+    ph.re = fma(rb, p1.x, fma(ra, m2.x, fma(-ib, m1.y, fma(-ia, p2.y, ph.re))));
+    ph.im = fma(rb, p1.y, fma(ra, m2.y, fma(ib, m1.x, fma(ia, p2.x, ph.im))));
 }
 
-// The mode sums of one coefficient set at D directions (theta[k], phi[k]):
-// every coefficient record and recurrence coefficient a thread loads serves
-// its D directions, whose D independent accumulations also hide each other's
-// latency.  (Measured alternatives, not kept: one thread summing up to four
-// unique frequencies' sets at one direction, which shares the Legendre work
-// but not the loads, no faster; reading the coefficient records one mode
-// ahead in registers, slower.)
+// The mode sums of one coefficient set at D directions (theta[k], phi[k]).
+// For each |m| one column of R_n^|m| = P_n^|m| / sin^|m| theta runs one
+// degree ahead, and with x = cos theta, s = sin theta:
+//   P1sin = s^{|m|-1} R_n,
+//   P1 = dP_n^|m|/d theta = s^{|m|-1} ((n - |m| + 1) R_{n+1} - (n + 1) x R_n)
+// (from (1 - x^2) dP_n^m/dx = (n + 1) x P_n^m - (n - m + 1) P_{n+1}^m), and
+// the m = 0 modes take P1 = P_n^1 = s R_n^1 from the |m| = 1 column: one
+// recurrence per (n, |m|), no division, exact at the zenith.  Every record
+// and table entry a thread loads serves its D directions.  (Measured
+// alternatives are listed with the kernel's profile.)
 template <int D>
 __device__ void fee_sums(const double (&theta)[D], const double (&phi)[D], const FeeMode* __restrict__ q, int nmax,
-                         const double2* __restrict__ rec, FeeSums (&out)[D]) {
-    double s[D], x[D], sm1[D], sm[D], smp1[D];
+                         const FeeRec* __restrict__ rec, FeeSums (&out)[D]) {
+    double s[D], x[D], sm1[D];
     cplx e1[D], em[D];
     FeeSums acc[D];
 #pragma unroll
@@ -140,88 +141,48 @@ __device__ void fee_sums(const double (&theta)[D], const double (&phi)[D], const
         sincos(theta[k], &s[k], &x[k]);
         sincos(phi[k], &sph, &cph);
         e1[k] = cplx{cph, sph};
-        em[k] = cplx{1.0, 0.0};  // e^{i |m| phi}
-        sm1[k] = 0.0;            // sin^{|m|-1}
-        sm[k] = 1.0;             // sin^{|m|}
+        em[k] = e1[k];  // e^{i |m| phi}, |m| = 1
+        sm1[k] = 1.0;   // s^{|m|-1}
         acc[k] = FeeSums{{0, 0}, {0, 0}, {0, 0}, {0, 0}};
     }
-    double rd = 1.0, rd_prev = 0.0;  // R_|m|^|m| and R_{|m|-1}^{|m|-1}: R_0^0 = 1, R_{c+1}^{c+1} = -(2c+1) R_c^c
+    double rd = -1.0;  // R_|m|^|m| = (-1)^|m| (2|m|-1)!!
     const FeeMode* p = q;
-    for (int ma = 0; ma <= nmax; ma++) {
-        const double rd_next = -(2.0 * ma + 1.0) * rd;
-        // the three columns at n = ma (previous, current) per direction
-        double pa[D], ca[D], pb[D], cb[D], pc[D], cc[D];
+    for (int ma = 1; ma <= nmax; ma++) {
+        double cur[D], nxt[D];  // R_n and R_{n+1} of column |m|
 #pragma unroll
         for (int k = 0; k < D; k++) {
-            smp1[k] = sm[k] * s[k];
-            pa[k] = rd_prev;
-            ca[k] = x[k] * (2.0 * ma - 1.0) * rd_prev;  // column ma - 1 (ma >= 1)
-            pb[k] = 0.0;
-            cb[k] = rd;  // column ma
-            pc[k] = 0.0;
-            cc[k] = 0.0;  // column ma + 1 (zero below its diagonal)
+            cur[k] = rd;
+            nxt[k] = x[k] * (2.0 * ma + 1.0) * rd;
         }
-        auto advance = [&](int n1) {
-            const double2* row = rec + n1 * FEE_REC_W;
-            const double2 ra = ma >= 1 ? __ldg(row + ma - 1) : make_double2(0.0, 0.0);
-            const double2 rb = __ldg(row + ma);
-            const double2 rc = n1 > ma + 1 ? __ldg(row + ma + 1) : make_double2(0.0, 0.0);
+        const FeeRec* r = rec + ma * (FEE_MAX_N + 1) + ma;  // row n = ma, column |m|
+        for (int n = ma; n <= nmax; n++, r += FEE_MAX_N + 1) {
+            const double2 c01 = __ldg(reinterpret_cast<const double2*>(r));  // (n + 1, n - |m| + 1)
+            const double2 c23 = __ldg(reinterpret_cast<const double2*>(r) + 1);  // (al, be)
+            const double4 c = make_double4(c01.x, c01.y, c23.x, c23.y);
+            FeeMode m0;
+            if (ma == 1) m0 = ld_mode(p++);
+            const FeeMode rx = ld_mode(p), ry = ld_mode(p + 1);
+            p += 2;
 #pragma unroll
             for (int k = 0; k < D; k++) {
-                if (ma >= 1) {
-                    const double t = fma(ra.x * x[k], ca[k], -ra.y * pa[k]);
-                    pa[k] = ca[k];
-                    ca[k] = t;
-                }
-                const double tb = fma(rb.x * x[k], cb[k], -rb.y * pb[k]);
-                pb[k] = cb[k];
-                cb[k] = tb;
-                if (n1 == ma + 1) {
-                    pc[k] = 0.0;
-                    cc[k] = rd_next;
-                } else {
-                    const double t = fma(rc.x * x[k], cc[k], -rc.y * pc[k]);
-                    pc[k] = cc[k];
-                    cc[k] = t;
-                }
+                const double p1sin = sm1[k] * cur[k];
+                const double p1 = sm1[k] * fma(c.y, nxt[k], -c.x * x[k] * cur[k]);
+                const double a = -ma * p1sin;
+                const double b = fma(ma * x[k], p1sin, p1);
+                if (ma == 1) fee_m0_add(m0, s[k] * cur[k], acc[k]);
+                const double ra = em[k].re * a, rb = em[k].re * b, ia = em[k].im * a, ib = em[k].im * b;
+                fee_pair_add(rx, ra, rb, ia, ib, acc[k].tx, acc[k].px);
+                fee_pair_add(ry, ra, rb, ia, ib, acc[k].ty, acc[k].py);
+                // R_{n+2} = al x R_{n+1} - be R_n
+                const double t = fma(c.z * x[k], nxt[k], -c.w * cur[k]);
+                cur[k] = nxt[k];
+                nxt[k] = t;
             }
-        };
-        int n = ma;
-        if (ma == 0) {
-            advance(1);
-            n = 1;
         }
-        for (; n <= nmax; n++) {
-            double a[D], b[D];
-#pragma unroll
-            for (int k = 0; k < D; k++) {
-                const double p1sin = ma >= 1 ? sm1[k] * cb[k] : 0.0;
-                const double p1 = ma == 0 ? s[k] * cc[k]
-                                          : 0.5 * fma(smp1[k], cc[k], -(double)((n + ma) * (n - ma + 1)) * sm1[k] * ca[k]);
-                b[k] = fma(ma * x[k], p1sin, p1);
-                a[k] = -ma * p1sin;  // for +m (-m has -a)
-            }
-            if (ma == 0) {
-                const FeeMode r = ld_mode(p++);
-#pragma unroll
-                for (int k = 0; k < D; k++) fee_m0_add(r, b[k], acc[k]);
-            } else {
-                const FeeMode rx = ld_mode(p), ry = ld_mode(p + 1);
-                p += 2;
-#pragma unroll
-                for (int k = 0; k < D; k++) {
-                    fee_pair_add(rx, a[k], b[k], em[k], acc[k].tx, acc[k].px);
-                    fee_pair_add(ry, a[k], b[k], em[k], acc[k].ty, acc[k].py);
-                }
-            }
-            if (n < nmax) advance(n + 1);
-        }
-        rd_prev = rd;
-        rd = rd_next;
+        rd *= -(2.0 * ma + 1.0);
 #pragma unroll
         for (int k = 0; k < D; k++) {
-            sm1[k] = sm[k];
-            sm[k] = smp1[k];
+            sm1[k] *= s[k];
             em[k] = em[k] * e1[k];
         }
     }
@@ -263,7 +224,7 @@ struct FeeArgs {
     int stride;
     int nmax;
     const double* norm;   // [uniq freq][4], or NULL
-    const double2* rec;   // [FEE_MAX_N + 1][FEE_REC_W]
+    const FeeRec* rec;    // [FEE_MAX_N + 1][FEE_MAX_N + 1], (n, |m|)
     int n_uniq_freq;
     int n_dirs;
     JonesF64* out;        // [uniq tile][uniq freq][n_dirs]
@@ -336,7 +297,7 @@ cudaError_t fee_launch(const FeeArgs& a, int n_uniq_tile, const double* az, cons
 // Zenith normalisation: |element k| of the zenith-pointed beam at the zenith,
 // at the azimuth where that element peaks (phi = 0, -pi/2, pi/2, 0).
 __global__ void fee_norm_kernel(const FeeMode* __restrict__ ideal, int stride, int nmax,
-                                const double2* __restrict__ rec, int n_uniq_freq, double* __restrict__ norm) {
+                                const FeeRec* __restrict__ rec, int n_uniq_freq, double* __restrict__ norm) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= 4 * n_uniq_freq) return;
     const int uf = t >> 2, k = t & 3;
@@ -356,7 +317,7 @@ struct HdcFeeBeam {
     int ntiles = 0, nfreqs = 0, n_uniq_tile = 0, n_uniq_freq = 0, stride = 0, nmax = 1;
     hdc::FeeMode* d_sets = nullptr;
     double* d_norm = nullptr;
-    double2* d_rec = nullptr;
+    hdc::FeeRec* d_rec = nullptr;
     int* d_tile_map = nullptr;
     int* d_freq_map = nullptr;
     std::vector<int> tile_map, freq_map;  // host copies
@@ -379,33 +340,27 @@ void fee_release(HdcFeeBeam* b) {
     b->d_rec = nullptr;
 }
 
-// K_mn in kernel order for largest degree nmax.
-std::vector<zc> fee_factors(int nmax) {
-    std::vector<zc> k(fee_num_modes(nmax));
+// K_mn = C_mn (-m/|m|)^m j^n / sqrt(n (n + 1)).
+zc fee_factor(int m, int n) {
     static const zc jpow[4] = {zc(1, 0), zc(0, 1), zc(-1, 0), zc(0, -1)};
-    for (int n = 1; n <= nmax; n++)
-        for (int m = -n; m <= n; m++) {
-            const int a = std::abs(m);
-            double ratio = 1.0;  // (n - |m|)! / (n + |m|)!
-            for (int t = n - a + 1; t <= n + a; t++) ratio /= (double)t;
-            const double c_mn = std::sqrt(0.5 * (2.0 * n + 1.0) * ratio);
-            const double sgn = (m > 0 && (m & 1)) ? -1.0 : 1.0;
-            k[fee_kernel_index(nmax, m, n)] = jpow[n & 3] * (c_mn * sgn / std::sqrt((double)n * (n + 1.0)));
-        }
-    return k;
+    const int a = std::abs(m);
+    double ratio = 1.0;  // (n - |m|)! / (n + |m|)!
+    for (int t = n - a + 1; t <= n + a; t++) ratio /= (double)t;
+    const double c_mn = std::sqrt(0.5 * (2.0 * n + 1.0) * ratio);
+    const double sgn = (m > 0 && (m & 1)) ? -1.0 : 1.0;
+    return jpow[n & 3] * (c_mn * sgn / std::sqrt((double)n * (n + 1.0)));
 }
 
 // The beamformed coefficients of one set (file frequency k, one tile's
-// amplitudes [32] and delays [16], dead dipoles already zeroed) into
-// out[0 .. fee_num_modes(nmax)) in kernel order.
-void fee_set(const HdcFeeCoeffs* f, int k, const double* amps, const uint32_t* delays, int nmax,
-             const std::vector<zc>& kf, FeeMode* out) {
+// amplitudes [32] and delays [16], dead dipoles already zeroed) as the
+// fee_num_modes(nmax) records of the kernel's order in out.
+void fee_set(const HdcFeeCoeffs* f, int k, const double* amps, const uint32_t* delays, int nmax, FeeMode* out) {
     const int nm = f->num_freq_modes[k];
-    const int M = fee_num_modes(nmax);
+    const size_t dense = (size_t)(nmax + 1) * (nmax + 1);  // (n, m) at n^2 + n + m
     std::vector<zc> q1[2], q2[2];
     for (int p = 0; p < 2; p++) {
-        q1[p].assign(M, zc(0, 0));
-        q2[p].assign(M, zc(0, 0));
+        q1[p].assign(dense, zc(0, 0));
+        q2[p].assign(dense, zc(0, 0));
         zc w[16];
         for (int d = 0; d < 16; d++) {
             const double ph = -TAU * (double)f->freqs_hz[k] * (double)delays[d] * FEE_DELAY_STEP;
@@ -419,18 +374,22 @@ void fee_set(const HdcFeeCoeffs* f, int k, const double* amps, const uint32_t* d
                 const double* c = qk + ((size_t)d * f->num_modes + col) * 2;
                 acc += w[d] * zc(c[0], c[1]);
             }
-            const int i = fee_kernel_index(nmax, m, n);
-            (s == 1 ? q1[p] : q2[p])[i] += acc;
+            const size_t i = (size_t)n * n + n + m;
+            (s == 1 ? q1[p] : q2[p])[i] += acc * fee_factor(m, n);
         }
     }
     auto d2 = [](zc z) { return make_double2(z.real(), z.imag()); };
-    for (int i = 0; i < nmax; i++)  // m = 0: (q1 X, q2 X, q1 Y, q2 Y)
-        out[i] = FeeMode{d2(q1[0][i] * kf[i]), d2(q2[0][i] * kf[i]), d2(q1[1][i] * kf[i]), d2(q2[1][i] * kf[i])};
-    for (int i = nmax; i < M; i += 2)  // +m at i, -m at i + 1 -> (P1, M1, P2, M2) of X at i, of Y at i + 1
-        for (int pol = 0; pol < 2; pol++) {
-            const zc a1 = q1[pol][i] * kf[i], b1 = q1[pol][i + 1] * kf[i + 1];
-            const zc a2 = q2[pol][i] * kf[i], b2 = q2[pol][i + 1] * kf[i + 1];
-            out[i + pol] = FeeMode{d2(a1 + b1), d2(a1 - b1), d2(a2 + b2), d2(a2 - b2)};
+    FeeMode* o = out;
+    for (int ma = 1; ma <= nmax; ma++)
+        for (int n = ma; n <= nmax; n++) {
+            if (ma == 1) {
+                const size_t i0 = (size_t)n * n + n;
+                *o++ = FeeMode{d2(q1[0][i0]), d2(q2[0][i0]), d2(q1[1][i0]), d2(q2[1][i0])};
+            }
+            const size_t ip = (size_t)n * n + n + ma, im = (size_t)n * n + n - ma;
+            for (int p = 0; p < 2; p++)
+                *o++ = FeeMode{d2(q1[p][ip] + q1[p][im]), d2(q1[p][ip] - q1[p][im]), d2(q2[p][ip] + q2[p][im]),
+                               d2(q2[p][ip] - q2[p][im])};
         }
 }
 
@@ -547,15 +506,15 @@ extern "C" int hdc_fee_beam_new(const HdcFeeCoeffs* file, const uint32_t* h_freq
     }
     const int stride = fee_num_modes(nmax);
     std::vector<FeeMode> sets((size_t)nu * nuf * stride);
-    const std::vector<zc> kf = fee_factors(nmax);
     for (int u = 0; u < nu; u++)
         for (int i = 0; i < nuf; i++)
-            fee_set(file, ufile[i], uamp[u].data(), udel[u].data(), nmax, kf, sets.data() + ((size_t)u * nuf + i) * stride);
-    // recurrence coefficients (2n-1)/(n-c), (n+c-1)/(n-c) for c < n
-    std::vector<double2> rec((size_t)(FEE_MAX_N + 1) * FEE_REC_W, make_double2(0.0, 0.0));
+            fee_set(file, ufile[i], uamp[u].data(), udel[u].data(), nmax, sets.data() + ((size_t)u * nuf + i) * stride);
+    // the column recurrence's constants per (n, |m|), |m| <= n
+    std::vector<FeeRec> rec((size_t)(FEE_MAX_N + 1) * (FEE_MAX_N + 1), FeeRec{0.0, 0.0, 0.0, 0.0});
     for (int n = 1; n <= FEE_MAX_N; n++)
-        for (int c = 0; c < n && c < FEE_REC_W; c++)
-            rec[(size_t)n * FEE_REC_W + c] = make_double2((2.0 * n - 1.0) / (n - c), (n + c - 1.0) / (n - c));
+        for (int ma = 1; ma <= n; ma++)
+            rec[(size_t)n * (FEE_MAX_N + 1) + ma] =
+                FeeRec{n + 1.0, n - ma + 1.0, (2.0 * n + 3.0) / (n + 2.0 - ma), (n + 1.0 + ma) / (n + 2.0 - ma)};
 
     HdcFeeBeam* b = new HdcFeeBeam();
     cudaGetDevice(&b->device);
@@ -575,12 +534,12 @@ extern "C" int hdc_fee_beam_new(const HdcFeeCoeffs* file, const uint32_t* h_freq
     };
     cudaError_t e;
     if ((e = cudaMalloc(&b->d_sets, sizeof(FeeMode) * sets.size())) != cudaSuccess) return fail(e, "cudaMalloc");
-    if ((e = cudaMalloc(&b->d_rec, sizeof(double2) * rec.size())) != cudaSuccess) return fail(e, "cudaMalloc");
+    if ((e = cudaMalloc(&b->d_rec, sizeof(FeeRec) * rec.size())) != cudaSuccess) return fail(e, "cudaMalloc");
     if ((e = cudaMalloc(&b->d_tile_map, sizeof(int) * num_tiles)) != cudaSuccess) return fail(e, "cudaMalloc");
     if ((e = cudaMalloc(&b->d_freq_map, sizeof(int) * num_freqs)) != cudaSuccess) return fail(e, "cudaMalloc");
     if ((e = cudaMemcpy(b->d_sets, sets.data(), sizeof(FeeMode) * sets.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
         return fail(e, "cudaMemcpy");
-    if ((e = cudaMemcpy(b->d_rec, rec.data(), sizeof(double2) * rec.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
+    if ((e = cudaMemcpy(b->d_rec, rec.data(), sizeof(FeeRec) * rec.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
         return fail(e, "cudaMemcpy");
     if ((e = cudaMemcpy(b->d_tile_map, tmap.data(), sizeof(int) * num_tiles, cudaMemcpyHostToDevice)) != cudaSuccess)
         return fail(e, "cudaMemcpy");
@@ -592,7 +551,7 @@ extern "C" int hdc_fee_beam_new(const HdcFeeCoeffs* file, const uint32_t* h_freq
         const std::vector<double> ones(32, 1.0);
         const std::vector<uint32_t> zeros(16, 0u);
         for (int i = 0; i < nuf; i++)
-            fee_set(file, ufile[i], ones.data(), zeros.data(), nmax, kf, ideal.data() + (size_t)i * stride);
+            fee_set(file, ufile[i], ones.data(), zeros.data(), nmax, ideal.data() + (size_t)i * stride);
         FeeMode* d_ideal = nullptr;
         if ((e = cudaMalloc(&d_ideal, sizeof(FeeMode) * ideal.size())) != cudaSuccess) return fail(e, "cudaMalloc");
         if ((e = cudaMalloc(&b->d_norm, sizeof(double) * 4 * nuf)) != cudaSuccess) {
