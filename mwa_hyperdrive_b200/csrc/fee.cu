@@ -25,27 +25,26 @@
 // AzEl::to_hadec and HADec::get_parallactic_angle).
 //
 // Device layout.  K_mn is folded into the coefficients on the host, and the
-// modes of a (tile, frequency) set are stored in the order the kernel visits
-// them (|m| outer, n inner), every set laid out for the beam's largest
+// records of a (tile, frequency) set are stored in the order the kernel
+// visits them (|m| outer, n inner), every set laid out for the beam's largest
 // degree.  The modes +m and -m of one degree share P1sin, P1 and
 // e^{-i m phi} = conj(e^{i m phi}), so they are stored as the sums and
 // differences of their coefficients and added together:
 //   e (a q1+ + b q2+) + conj(e) (-a q1- + b q2-)
 //     = Re(e) (a M1 + b P2) + i Im(e) (a P1 + b M2),  P = q+ + q-, M = q+ - q-
-// (a = -|m| P1sin, b = |m| u P1sin + P1), 24 FP64 instructions per
-// polarisation for the two modes instead of 32; m = 0 modes (e = 1, a = 0)
-// take 4.  A thread sums one set at two directions, so every coefficient
+// (a = -|m| P1sin, b = |m| u P1sin + P1), which with Re(e) a, Re(e) b,
+// Im(e) a and Im(e) b formed once is 16 fused multiply-adds per polarisation
+// for the two modes.  A thread sums one set at two directions, so every
 // record it loads (all threads of a block read the same one: one L1
-// broadcast per warp) serves both.  Per direction it runs three upward
-// Legendre recurrences in n, for columns |m| - 1, |m|, |m| + 1 of
-// R_n^c = P_n^c / sin^c theta (polynomials in u, finite at the zenith), so
-//   P1sin = sin^{|m|-1} R_n^|m|,
-//   P1 = (sin^{|m|+1} R_n^{|m|+1} - (n+|m|)(n-|m|+1) sin^{|m|-1} R_n^{|m|-1}) / 2
-//   (P1 = sin R_n^1 for m = 0)
-// hold at every theta, the zenith included, with no division.  The
-// recurrence coefficients (2n-1)/(n-c) and (n+c-1)/(n-c) come from a small
-// table.  The work is FP64 arithmetic; the roofline counts the published
-// sum's 56 FLOPs per mode per direction (both polarisations).
+// broadcast per warp) serves both.  Per direction and |m| it runs one upward
+// Legendre recurrence in n of R_n^|m| = P_n^|m| / sin^|m| theta (a
+// polynomial in u, finite at the zenith), one degree ahead, for
+//   P1sin = sin^{|m|-1} R_n,
+//   P1 = sin^{|m|-1} ((n - |m| + 1) R_{n+1} - (n + 1) u R_n)
+// (the m = 0 modes: P1 = P_n^1 = sin theta R_n^1), with no division.  The
+// recurrence constants come from a small table.  The work is FP64
+// arithmetic; the roofline counts the published sum's 56 FLOPs per mode per
+// direction (both polarisations).
 
 #include <algorithm>
 #include <cmath>
