@@ -1189,22 +1189,26 @@ def gpu_arm(args, rank, world, local_rank):
                 rg["native_chosen_form"] = {"ms_per_timestep": ms_chosen / nt,
                                             "speedup_vs_reference_kernels": ref_ms / (ms_chosen / nt)}
             torch.cuda.synchronize()
-        if not (args.skip_dical and args.skip_peel and args.skip_warmstart and args.skip_prep and args.skip_fee):
+        # the sections of a 1-GPU run (a multi-GPU run measures the replicated
+        # predict only)
+        single = world == 1
+        if single and not (args.skip_dical and args.skip_peel and args.skip_warmstart and args.skip_prep
+                           and args.skip_fee):
             del vis, flush
             torch.cuda.empty_cache()
-        if not args.skip_dical:
+        if single and not args.skip_dical:
             line["dical"] = guarded(dical_arm, args)
             torch.cuda.empty_cache()
-        if not args.skip_peel:
+        if single and not args.skip_peel:
             line["peel"] = guarded(peel_arm, args)
             torch.cuda.empty_cache()
-        if not args.skip_warmstart:
+        if single and not args.skip_warmstart:
             line["warmstart"] = guarded(warmstart_arm, args)
             torch.cuda.empty_cache()
-        if not args.skip_prep:
+        if single and not args.skip_prep:
             line["prep"] = guarded(prep_arm, args)
             torch.cuda.empty_cache()
-        if not args.skip_fee:
+        if single and not args.skip_fee:
             line["fee"] = guarded(fee_arm, args)
         print(json.dumps(line), flush=True)
     plain.close()
