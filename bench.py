@@ -955,6 +955,36 @@ def fee_arm(args):
                         "flop_per_launch": flop,
                         "flop_rule": f"{FEE_FLOP_PER_MODE} FLOP per mode per direction per (unique tile, "
                                      "unique frequency); the Legendre recurrences are not counted"}}
+    # the predict of one timestep of the mixed configuration with this beam per
+    # tile (chosen form: tensor block form for the points, the FP64 per-tile
+    # direct kernel for Gaussians and shapelets) beside the shared analytic
+    # beam, per kernel class (the modeller's CUDA events)
+    if n == 4600:
+        from mwa_hyperdrive_b200.model import SkyModeller
+
+        obs, sky = workload()
+        if obs.num_tiles == ntiles and np.allclose(obs.freqs, chans):
+            vis = torch.zeros((obs.freqs.size, obs.num_baselines, 8), dtype=torch.float32, device="cuda")
+            per = {}
+            for name, bm in (("fee_per_tile", "fee"), ("analytic_shared", "analytic")):
+                m = SkyModeller(sky, obs.tile_xyzs, obs.freqs, obs.phase_centre, obs.latitude, form="tensor", beam=bm,
+                                fee_beam=beam if bm == "fee" else None)
+                m.model_timestep_with(obs.lsts[0], vis, return_uvws=False)
+                lib.hdc_modeller_set_profiling(m._h, 1)
+                prof = (ctypes.c_double * 4)()
+                runs = []
+                for _ in range(3):
+                    lib.hdc_modeller_profile(m._h, prof, 1)
+                    m.model_timestep_with(obs.lsts[0], vis, return_uvws=False)
+                    torch.cuda.synchronize()
+                    lib.hdc_modeller_profile(m._h, prof, 1)
+                    runs.append(list(prof))
+                med = [statistics.median(r[i] for r in runs) for i in range(4)]
+                per[name] = {"ms_per_timestep": sum(med), "points": med[0], "gaussians": med[1],
+                             "shapelets": med[2], "geometry_and_beam": med[3]}
+                m.close()
+            res["predict_one_timestep"] = per
+            del vis
     if not args.no_cpu_baseline:
         from oracle import fee_ref as fr
 

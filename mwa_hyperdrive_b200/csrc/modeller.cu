@@ -557,6 +557,7 @@ DirectParams Modeller::direct_params(int ty, void* vis) const {
         p.unflagged_map = nullptr;
         p.freq_map = tb.d_freq_map;
         p.n_uniq_freq = tb.n_uniq_freq;
+        p.n_uniq_tile = tb.n_uniq_tile;
     }
     p.vis = vis;
     p.err = d_err;

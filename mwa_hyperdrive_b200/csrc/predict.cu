@@ -617,10 +617,254 @@ __global__ void __launch_bounds__(DT, FastShape<TYPE>::MIN_CTAS) fast_kernel(con
     }
 }
 
+// The chosen form's Gaussians and shapelets with a beam per tile: each
+// thread takes one baseline (p, q) and FT_FCH consecutive channels, as
+// fast_kernel does.  Per staged chunk of components the CTA forms, in FP64
+// shared memory, G = B_u S and H = B_u for every unique tile u and each of its
+// channels (B the tile's beam Jones at the channel's beam frequency, S the
+// component's instrumental flux), laid out [channel][component][unique
+// tile] so that a warp's threads, which share tile p and mostly share the
+// unique beam of tile q, read the same or neighbouring records.  A
+// visibility term is then z G_p H_q^H = B_p (z S) B_q^H: the phasor and
+// envelope z in FP32 exactly as fast_kernel computes them, the products in
+// FP64 (16 + 32 operations).  FP32 products (measured) put the
+// cross-polarisation terms' cancellation at FP32 precision of the parallel
+// hands and the p99.9 error at 1.0-1.15e-6; in FP64 the terms keep the
+// shared-beam form's error structure (W = B S B^H rounded once, relative to
+// each element).
+constexpr int FT_FCH = 2;      // channels per thread
+constexpr int FT_CH = 16;      // components per staged chunk
+constexpr int FT_MAX_NU = 32;  // unique tiles (more: the FP64 per-tile kernel)
+
+inline size_t fast_tile_smem_bytes(int nu) { return (size_t)FT_FCH * FT_CH * nu * 8 * sizeof(double2); }
+
+template <int TYPE, bool OUT64>
+__global__ void __launch_bounds__(DT, 1) fast_tile_kernel(const DirectParams p) {
+    constexpr int FCH = FT_FCH;
+    constexpr int CH = FT_CH;
+    __shared__ alignas(128) double4 s_lmn[2][CH];
+    __shared__ alignas(128) JonesF64 s_flux[2][FCH][CH];
+    __shared__ alignas(128) double4 s_gp[2][CH];
+    __shared__ alignas(16) float s_dense[TYPE == 2 ? CH * SDN * SDN : 1];
+    __shared__ alignas(8) uint64_t bar[2];
+    // [FCH][CH][nu] records of 8 double2: G (a, b, c, d) then H (a, b, c, d)
+    extern __shared__ double2 s_gh[];
+    const int nu = p.n_uniq_tile;
+
+    const int f0 = blockIdx.y * FCH;
+    const int bl = blockIdx.x * DT + threadIdx.x;
+    const bool active = bl < p.nbl;
+    int t1 = 0, t2 = 1;
+    if (active) baseline_to_tiles(bl, p.ntiles, t1, t2);
+    const int u1 = active ? p.tile_map[t1] : 0, u2 = active ? p.tile_map[t2] : 0;
+    int fr[FCH], col[FCH];
+    double ool[FCH];
+#pragma unroll
+    for (int i = 0; i < FCH; i++) {
+        fr[i] = min(f0 + i, p.nf - 1);  // a missing last channel repeats the previous one and is not stored
+        ool[i] = p.freqs[fr[i]] / VEL_C;
+        col[i] = p.freq_map[fr[i]];
+    }
+    double um = 0.0, vm = 0.0, wm = 0.0;
+    if (active) {
+        const UVW q = p.uvws[bl];
+        um = q.u, vm = q.v, wm = q.w;
+    }
+
+    const int nchunks = (p.nc + CH - 1) / CH;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+
+    auto issue = [&](int k) {
+        const int st = k & 1;
+        const int c0 = k * CH;
+        const int n = min(CH, p.nc - c0);
+        const uint32_t bytes = n * 32u + FCH * n * 64u + n * 32u;
+        mbar_arrive_expect_tx(&bar[st], bytes);
+        bulk_g2s(s_lmn[st], p.lmn + c0, n * 32u, &bar[st]);
+#pragma unroll
+        for (int i = 0; i < FCH; i++) bulk_g2s(s_flux[st][i], p.flux + (size_t)fr[i] * p.nc + c0, n * 64u, &bar[st]);
+        bulk_g2s(s_gp[st], p.gp + c0, n * 32u, &bar[st]);
+    };
+    int issued = 0;
+    if (threadIdx.x == 0) {
+        fence_proxy_async_smem();
+        if (!p.stall) {
+            if (nchunks > 0) issue(0), issued = 1;
+            if (nchunks > 1) issue(1), issued = 2;
+        }
+    }
+    const uint64_t limit = p.wait_ns ? p.wait_ns : 2000000000ull;
+
+    J2 acc[FCH];
+#pragma unroll
+    for (int i = 0; i < FCH; i++) acc[i] = jzero();
+    bool aborted = false;
+    for (int k = 0; k < nchunks; k++) {
+        const int st = k & 1;
+        const bool ok = mbar_wait_bounded(&bar[st], (k >> 1) & 1, p.err, limit);
+        if (__syncthreads_or(!ok)) {
+            if (threadIdx.x == 0) drain_two_stage(bar, k, issued);
+            aborted = true;
+            break;
+        }
+        const int c0 = k * CH;
+        const int n = min(CH, p.nc - c0);
+        // G = B S and H = B of every (channel, component, unique tile)
+        for (int e = threadIdx.x; e < FCH * CH * nu; e += DT) {
+            const int u = e % nu, c = (e / nu) % CH, i = e / (nu * CH);
+            if (c >= n) continue;
+            const J2 b = ldg_j(p.beam + ((size_t)u * p.n_uniq_freq + col[i]) * p.nc + c0 + c);
+            const J2 g = b * load_j(s_flux[st][i][c]);
+            double2* r = s_gh + (size_t)e * 8;
+            r[0] = make_double2(g.a.re, g.a.im);
+            r[1] = make_double2(g.b.re, g.b.im);
+            r[2] = make_double2(g.c.re, g.c.im);
+            r[3] = make_double2(g.d.re, g.d.im);
+            r[4] = make_double2(b.a.re, b.a.im);
+            r[5] = make_double2(b.b.re, b.b.im);
+            r[6] = make_double2(b.c.re, b.c.im);
+            r[7] = make_double2(b.d.re, b.d.im);
+        }
+        if (TYPE == 2 && p.sdense)
+            for (int e = threadIdx.x; e < n * SDN * SDN; e += DT) s_dense[e] = __ldg(p.sdense + (size_t)c0 * SDN * SDN + e);
+        __syncthreads();
+        if (active) {
+            for (int c = 0; c < n; c++) {
+                const double4 lmn = s_lmn[st][c];
+                const double4 g = s_gp[st][c];
+                const double tm = um * lmn.x + vm * lmn.y + wm * lmn.z;  // metres
+                double exm = 0.0, xm = 0.0, ym = 0.0, su = 0.0, sv = 0.0;
+                if (TYPE == 1) {
+                    const double kx = um * g.z + vm * g.w;
+                    const double ky = um * g.w - vm * g.z;
+                    exm = (g.x * (kx * kx) + g.y * (ky * ky)) * 1.4426950408889634074;
+                } else {
+                    const double2 ta = __ldg(p.suv_tile + (size_t)(c0 + c) * p.ntiles + t1);
+                    const double2 tb = __ldg(p.suv_tile + (size_t)(c0 + c) * p.ntiles + t2);
+                    su = ta.x - tb.x;
+                    sv = ta.y - tb.y;
+                    xm = su * g.z + sv * g.w;
+                    ym = su * g.w - sv * g.z;
+                }
+                float der[FCH], dei[FCH];
+                if (TYPE == 2 && p.sdense) {
+                    double xp[FCH], yp[FCH];
+#pragma unroll
+                    for (int i = 0; i < FCH; i++) {
+                        xp[i] = xm * (ool[i] * g.x) + SBF_C;
+                        yp[i] = ym * (ool[i] * g.y) + SBF_C;
+                    }
+                    shapelet_dense_multi<FCH>(p, s_dense + c * SDN * SDN, xp, yp, der, dei);
+                }
+#pragma unroll
+                for (int i = 0; i < FCH; i++) {
+                    float sn, cs;
+                    phasor_quarter_f32(4.0 * ool[i] * tm, sn, cs);
+                    float er, ei = 0.f;
+                    if (TYPE == 1) {
+                        er = exp2f((float)(exm * (ool[i] * ool[i])));
+                    } else if (p.sdense) {
+                        er = der[i], ei = dei[i];
+                    } else {
+                        shapelet_envelope_f32(p, c0 + c, g, su * ool[i], sv * ool[i], er, ei);
+                    }
+                    float zr, zi;
+                    if (TYPE == 1) {
+                        zr = cs * er;
+                        zi = sn * er;
+                    } else {
+                        zr = cs * er - sn * ei;
+                        zi = fmaf(cs, ei, sn * er);
+                    }
+                    const cplx z = {(double)zr, (double)zi};
+                    const double2* rg = s_gh + ((size_t)(i * CH + c) * nu + u1) * 8;
+                    const double2* rh = s_gh + ((size_t)(i * CH + c) * nu + u2) * 8 + 4;
+                    // zG = z G_p, then acc += zG H_q^H: M[r][s] = sum_k zG[r][k] conj(H[s][k])
+                    const cplx za = z * cplx{rg[0].x, rg[0].y}, zb = z * cplx{rg[1].x, rg[1].y};
+                    const cplx zc = z * cplx{rg[2].x, rg[2].y}, zd = z * cplx{rg[3].x, rg[3].y};
+                    const double2 ha = rh[0], hb = rh[1], hc = rh[2], hd = rh[3];
+                    J2& m = acc[i];
+                    m.a.re = fma(za.re, ha.x, fma(za.im, ha.y, fma(zb.re, hb.x, fma(zb.im, hb.y, m.a.re))));
+                    m.a.im = fma(za.im, ha.x, fma(-za.re, ha.y, fma(zb.im, hb.x, fma(-zb.re, hb.y, m.a.im))));
+                    m.b.re = fma(za.re, hc.x, fma(za.im, hc.y, fma(zb.re, hd.x, fma(zb.im, hd.y, m.b.re))));
+                    m.b.im = fma(za.im, hc.x, fma(-za.re, hc.y, fma(zb.im, hd.x, fma(-zb.re, hd.y, m.b.im))));
+                    m.c.re = fma(zc.re, ha.x, fma(zc.im, ha.y, fma(zd.re, hb.x, fma(zd.im, hb.y, m.c.re))));
+                    m.c.im = fma(zc.im, ha.x, fma(-zc.re, ha.y, fma(zd.im, hb.x, fma(-zd.re, hb.y, m.c.im))));
+                    m.d.re = fma(zc.re, hc.x, fma(zc.im, hc.y, fma(zd.re, hd.x, fma(zd.im, hd.y, m.d.re))));
+                    m.d.im = fma(zc.im, hc.x, fma(-zc.re, hc.y, fma(zd.im, hd.x, fma(-zd.re, hd.y, m.d.im))));
+                }
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0 && k + 2 < nchunks) {
+            fence_proxy_async_smem();
+            issue(k + 2);
+            issued = k + 3;
+        }
+    }
+
+    if (!active || aborted) return;
+#pragma unroll
+    for (int i = 0; i < FCH; i++) {
+        if (f0 + i >= p.nf) break;
+        const size_t o = (size_t)(f0 + i) * p.nbl + bl;
+        if (OUT64) {
+            double2* q = reinterpret_cast<double2*>(reinterpret_cast<JonesF64*>(p.vis) + o);
+            double2 a0 = q[0], b0 = q[1], c1 = q[2], d0 = q[3];
+            q[0] = make_double2(a0.x + acc[i].a.re, a0.y + acc[i].a.im);
+            q[1] = make_double2(b0.x + acc[i].b.re, b0.y + acc[i].b.im);
+            q[2] = make_double2(c1.x + acc[i].c.re, c1.y + acc[i].c.im);
+            q[3] = make_double2(d0.x + acc[i].d.re, d0.y + acc[i].d.im);
+        } else {
+            float4* q = reinterpret_cast<float4*>(reinterpret_cast<JonesF32*>(p.vis) + o);
+            float4 x = q[0], y = q[1];
+            x.x += (float)acc[i].a.re;
+            x.y += (float)acc[i].a.im;
+            x.z += (float)acc[i].b.re;
+            x.w += (float)acc[i].b.im;
+            y.x += (float)acc[i].c.re;
+            y.y += (float)acc[i].c.im;
+            y.z += (float)acc[i].d.re;
+            y.w += (float)acc[i].d.im;
+            q[0] = x;
+            q[1] = y;
+        }
+    }
+}
+
+template <int TYPE, bool OUT64>
+static cudaError_t launch_fast_tile(const DirectParams& p, cudaStream_t s) {
+    const size_t smem = fast_tile_smem_bytes(p.n_uniq_tile);
+    // the opt-in above 48 KB of dynamic shared memory, once per device
+    static std::atomic<bool> attr[64];
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (!attr[dev].load(std::memory_order_relaxed)) {
+        e = cudaFuncSetAttribute(fast_tile_kernel<TYPE, OUT64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)fast_tile_smem_bytes(FT_MAX_NU));
+        if (e != cudaSuccess) return e;
+        attr[dev].store(true, std::memory_order_relaxed);
+    }
+    const dim3 grid((p.nbl + DT - 1) / DT, (p.nf + FT_FCH - 1) / FT_FCH);
+    fast_tile_kernel<TYPE, OUT64><<<grid, DT, smem, s>>>(p);
+    return cudaSuccess;
+}
+
 template <int TYPE>
 static cudaError_t launch_t(bool tile_beam, bool out64, bool fast, const DirectParams& p, cudaStream_t s) {
     dim3 grid((p.nbl + DT - 1) / DT, p.nf);
-    if (tile_beam) {
+    if (tile_beam && fast && TYPE != 0) {
+        const cudaError_t e = out64 ? launch_fast_tile<TYPE == 0 ? 1 : TYPE, true>(p, s)
+                                    : launch_fast_tile<TYPE == 0 ? 1 : TYPE, false>(p, s);
+        if (e != cudaSuccess) return e;
+    } else if (tile_beam) {
         if (out64)
             direct_kernel<TYPE, true, true, false><<<grid, DT, 0, s>>>(p);
         else
@@ -676,8 +920,11 @@ cudaError_t launch_direct(int ty, bool tile_beam, bool out64, const DirectParams
             p.wait_ns = ns;
         }
     }
-    // the FP32 form needs per-tile shapelet UVs and the FP32 basis table
-    fast = fast && !tile_beam && (ty != 2 || (p.suv_tile && !p.suv_bl && p.sbf32));
+    // the FP32 form needs per-tile shapelet UVs and the FP32 basis table, and
+    // with per-tile beams a unique-tile count it can stage (not the points,
+    // whose chosen form is the tensor kernel)
+    fast = fast && (ty != 2 || (p.suv_tile && !p.suv_bl && p.sbf32)) &&
+           (!tile_beam || (ty != 0 && p.n_uniq_tile > 0 && p.n_uniq_tile <= FT_MAX_NU && !p.unflagged_map));
     if (fast && ty == 2 && p.sdense && !p.sbfp) return cudaErrorInvalidValue;
     if (ty == 0) return launch_t<0>(tile_beam, out64, fast, p, s);
     if (ty == 1) return launch_t<1>(tile_beam, out64, fast, p, s);

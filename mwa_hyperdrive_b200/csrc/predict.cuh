@@ -25,6 +25,7 @@ struct DirectParams {
     const int* unflagged_map;
     const int* freq_map;
     int n_uniq_freq;
+    int n_uniq_tile;  // rows of beam (the chosen form's per-tile kernel stages them; 0: not known)
     // shapelets
     const double* sbf;  // [SBF_N][SBF_L]
     const float* sbf32; // the same table in FP32 (chosen form), or NULL
@@ -116,6 +117,7 @@ struct AutosParams {
     const int* unflagged_map;
     const int* freq_map;
     int n_uniq_freq;
+    int n_uniq_tile;  // rows of beam (the chosen form's per-tile kernel stages them; 0: not known)
     JonesF32* vis;  // [nf][ntiles]
 };
 cudaError_t launch_autos(const AutosParams& p, cudaStream_t s);

@@ -168,11 +168,13 @@ def test_modeller_with_fee_beam_fp64(oracle, ctype):
 
 
 def test_modeller_with_fee_beam_tensor_form(oracle):
-    """The tensor-core point predict (block form for per-tile beams) with the
-    FEE beam, against the same oracle, within 1e-6."""
+    """The chosen form with the FEE beam per tile -- the tensor-core points
+    (block form), the FP32 per-tile Gaussians and shapelets -- against the
+    same oracle, within 1e-6."""
     pc = (0.3, math.radians(-30.0))
     obs = synth.Obs(synth.tiles_in_disk(40, 1500.0, 6), 166.4e6 + np.arange(4) * 0.64e6, pc, np.array([0.37]))
-    sky = sl.SkyModelArrays.from_components(synth.point_sky(64, pc, 8.0, 7))
+    sky = sl.SkyModelArrays.from_components(synth.point_sky(64, pc, 8.0, 7) +
+                                            synth.gaussians_and_shapelets(20, 6, pc, 5))
     delays, amps = tile_settings(obs.num_tiles, 10)
     beam = FeeBeam(FILE, obs.freqs, delays, amps)
     tmap, fmap = beam.maps()
@@ -180,9 +182,11 @@ def test_modeller_with_fee_beam_tensor_form(oracle):
     vis = torch.zeros((obs.freqs.size, obs.num_baselines, 8), dtype=torch.float64, device="cuda")
     m.model_timestep_with(obs.lsts[0], vis)
     torch.cuda.synchronize()
-    az, za = comp_azza(oracle, sky, 0, obs.lsts[0], obs.latitude)
-    tab = oracle_tables(FILE, az, za, obs.freqs, delays, amps, tmap, fmap, True, obs.latitude)
-    b = oracle.beam_struct(2, [tab, None, None], tmap, fmap, beam.num_unique_freqs())
+    tabs = []
+    for ty in range(3):
+        az, za = comp_azza(oracle, sky, ty, obs.lsts[0], obs.latitude)
+        tabs.append(oracle_tables(FILE, az, za, obs.freqs, delays, amps, tmap, fmap, True, obs.latitude))
+    b = oracle.beam_struct(2, tabs, tmap, fmap, beam.num_unique_freqs())
     ref, _ = oracle.model_timestep(sky, obs.tile_xyzs, obs.freqs, pc, obs.lsts[0], obs.latitude, beam=b,
                                    out_f64=True)
     got = vis.cpu().numpy()

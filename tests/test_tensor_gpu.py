@@ -289,9 +289,9 @@ def test_more_than_128_tiles(oracle, ntiles, npts):
 @pytest.mark.parametrize("ntiles,npts", [(144, 200), (256, 120)])
 def test_per_tile_beams_tensor_form(oracle, ntiles, npts):
     """Per-tile beams in the tensor form (block form over twice the
-    components) past 128 tiles, with Gaussians in the same sky (the direct
-    FP64 kernel with per-tile beams): against the oracle with the same
-    explicit per-tile Jones table, within 1e-6."""
+    components) past 128 tiles, with Gaussians in the same sky (the chosen
+    form's per-tile kernel up to 32 unique beams, here 18 and 30): against
+    the oracle with the same explicit per-tile Jones table, within 1e-6."""
     pc = (0.2, math.radians(-26.0))
     obs = synth.Obs(synth.tiles_in_disk(ntiles, 1500.0, ntiles + 3), 166.4e6 + np.arange(3) * 0.96e6, pc,
                     np.array([0.3]))
@@ -318,3 +318,40 @@ def test_per_tile_beams_tensor_form(oracle, ntiles, npts):
     nrm, p999, mx = errors(vis.cpu().numpy(), ref)
     print(f"per-tile beams {ntiles} tiles, {len(uniq)} beams: normwise {nrm:.2e}, p99.9 {p999:.2e}, max {mx:.2e}")
     assert nrm < TOL and p999 < TOL, (nrm, p999, mx)
+
+
+@pytest.mark.parametrize("ctype", [1, 2])
+def test_chosen_form_per_tile_beams_gaussians_and_shapelets(oracle, ctype):
+    """With a beam per tile and at most 32 unique tiles, the chosen form's
+    Gaussians and shapelets run in the per-tile kernel of the chosen form
+    (FP32 phasor and envelope; G = B_p S and H = B_q staged per chunk, the
+    products in FP64): against the oracle with the same explicit per-tile
+    Jones table within 1e-6, and not the FP64 per-tile kernel's result (a
+    different kernel ran)."""
+    pc = (0.2, math.radians(-26.0))
+    obs = synth.Obs(synth.tiles_in_disk(48, 1500.0, 7), 166.4e6 + np.arange(5) * 0.64e6, pc, np.array([0.3]))
+    comps = synth.gaussians_and_shapelets(60 if ctype == 1 else 0, 0 if ctype == 1 else 12, pc, 8)
+    sky = sl.SkyModelArrays.from_components(comps)
+    rng = np.random.default_rng(3)
+    gains = np.ones((obs.num_tiles, 2, 16))
+    for p in rng.choice(obs.num_tiles, 12, replace=False):
+        gains[p, rng.integers(2), rng.integers(16)] = 0.0
+    out = {}
+    for form in ("tensor", "direct"):
+        m = SkyModeller(sky, obs.tile_xyzs, obs.freqs, pc, obs.latitude, beam="per_tile", dipole_gains=gains,
+                        form=form)
+        vis = torch.zeros((obs.freqs.size, obs.num_baselines, 8), dtype=torch.float64, device="cuda")
+        m.model_timestep_with(obs.lsts[0], vis)
+        torch.cuda.synchronize()
+        out[form] = vis.cpu().numpy()
+    uniq, tmap, ufreqs, fmap = oracle.unique_tile_beams(gains, obs.freqs)
+    assert 2 < len(uniq) <= 32
+    tabs = [oracle.tile_beam_table(sky, ty, obs.lsts[0], obs.latitude, uniq, ufreqs) if ty == ctype else None
+            for ty in range(3)]
+    ref, _ = oracle.model_timestep(sky, obs.tile_xyzs, obs.freqs, pc, obs.lsts[0], obs.latitude,
+                                   beam=oracle.beam_struct(2, tabs, tmap, fmap, ufreqs.size), out_f64=True)
+    nrm, p999, mx = errors(out["tensor"], ref)
+    print(f"per-tile chosen form, type {ctype}, {len(uniq)} beams: normwise {nrm:.2e}, p99.9 {p999:.2e}, max {mx:.2e}")
+    assert nrm < TOL and p999 < TOL, (nrm, p999, mx)
+    assert errors(out["direct"], ref)[0] < 1e-10
+    assert errors(out["tensor"], out["direct"])[0] > 1e-12
