@@ -956,9 +956,9 @@ def fee_arm(args):
                         "flop_rule": f"{FEE_FLOP_PER_MODE} FLOP per mode per direction per (unique tile, "
                                      "unique frequency); the Legendre recurrences are not counted"}}
     # the predict of one timestep of the mixed configuration with this beam per
-    # tile (chosen form: tensor block form for the points, the FP64 per-tile
-    # direct kernel for Gaussians and shapelets) beside the shared analytic
-    # beam, per kernel class (the modeller's CUDA events)
+    # tile (chosen form: tensor block form for the points, the per-tile kernel
+    # of the chosen form for Gaussians and shapelets) beside the shared
+    # analytic beam, per kernel class (the modeller's CUDA events)
     if n == 4600:
         from mwa_hyperdrive_b200.model import SkyModeller
 
