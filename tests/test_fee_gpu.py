@@ -250,3 +250,30 @@ def test_veto_brightness_with_the_fee_beam(oracle):
     with pytest.raises(_lib.HdcError):  # a beam of two tiles is not the reference's tile-less beam
         two = FeeBeam(FILE, freqs, np.stack([ideal, ideal + 1]), np.ones((2, 32)))
         io.veto_sources(s, pc, lst, LAT, freqs, beam="fee", fee_beam=two)
+
+
+def test_autos_with_fee_beam(oracle):
+    """model_timestep_autos_with with the FEE beam per tile against the
+    oracle's autos given the oracle's FEE tables (f32 output within 4 ulps of
+    the oracle's identically demoted result)."""
+    pc = (0.3, math.radians(-30.0))
+    obs = synth.Obs(synth.tiles_in_disk(12, 1000.0, 4), 166.4e6 + np.arange(4) * 0.64e6, pc, np.array([0.41]))
+    sky = sl.SkyModelArrays.from_components(synth.point_sky(8, pc, 8.0, 3) +
+                                            synth.gaussians_and_shapelets(4, 2, pc, 6))
+    delays, amps = tile_settings(obs.num_tiles, 12)
+    beam = FeeBeam(FILE, obs.freqs, delays, amps)
+    tmap, fmap = beam.maps()
+    m = SkyModeller(sky, obs.tile_xyzs, obs.freqs, pc, obs.latitude, beam="fee", fee_beam=beam)
+    v = torch.zeros((obs.freqs.size, obs.num_tiles, 8), dtype=torch.float32, device="cuda")
+    m.model_timestep_autos_with(obs.lsts[0], v)
+    torch.cuda.synchronize()
+    tabs = []
+    for ty in range(3):
+        az, za = comp_azza(oracle, sky, ty, obs.lsts[0], obs.latitude)
+        tabs.append(oracle_tables(FILE, az, za, obs.freqs, delays, amps, tmap, fmap, True, obs.latitude))
+    b = oracle.beam_struct(2, tabs, tmap, fmap, beam.num_unique_freqs())
+    ref = oracle.model_autos(sky, obs.num_tiles, obs.freqs, obs.lsts[0], obs.latitude, beam=b)
+    got = v.cpu().numpy().astype(np.float32)
+    ref = np.asarray(ref, np.float32)
+    scale = np.maximum(np.abs(ref), np.float32(np.max(np.abs(ref)) * 1e-6 + 1e-30))
+    assert not (np.abs(got - ref) > 4 * np.spacing(scale)).any(), np.max(np.abs(got - ref))
