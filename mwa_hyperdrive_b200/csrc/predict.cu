@@ -392,6 +392,102 @@ __global__ void __launch_bounds__(DT) direct_kernel(const DirectParams p) {
     }
 }
 
+// The channel-independent FP64 work of one Gaussian or shapelet term of the
+// chosen form at baseline (um, vm, wm) [m] (tiles t1, t2): the phase in
+// metres, the Gaussian exponent in metres^2 (base 2) or the shapelet
+// coordinates, and the dense shapelet envelopes of the FCH channels (cm:
+// the component's dense coefficient matrix in shared memory, or NULL).
+template <int TYPE, int FCH>
+struct FastTerm {
+    double tm, exm, su, sv;
+    float der[FCH], dei[FCH];
+};
+
+template <int TYPE, int FCH>
+__device__ __forceinline__ void fast_term(const DirectParams& p, double4 lmn, double4 g, double um, double vm, double wm,
+                                          int cglob, int t1, int t2, const double (&ool)[FCH], const float* cm,
+                                          FastTerm<TYPE, FCH>& f) {
+    f.tm = um * lmn.x + vm * lmn.y + wm * lmn.z;
+    f.exm = f.su = f.sv = 0.0;
+    if (TYPE == 1) {
+        // the exponent in FP64 (an FP32 exponent's absolute error, ~1e-7 of
+        // its size, would become the envelope's relative error), in base 2
+        // (exp(x) = 2^(x log2 e)): the per-channel exp2f costs fewer
+        // instructions than expf (measured)
+        const double kx = um * g.z + vm * g.w;
+        const double ky = um * g.w - vm * g.z;
+        f.exm = (g.x * (kx * kx) + g.y * (ky * ky)) * 1.4426950408889634074;
+    } else {
+        const double2 ta = __ldg(p.suv_tile + (size_t)cglob * p.ntiles + t1);
+        const double2 tb = __ldg(p.suv_tile + (size_t)cglob * p.ntiles + t2);
+        f.su = ta.x - tb.x;
+        f.sv = ta.y - tb.y;
+        if (cm) {
+            const double xm = f.su * g.z + f.sv * g.w;
+            const double ym = f.su * g.w - f.sv * g.z;
+            double xp[FCH], yp[FCH];
+#pragma unroll
+            for (int i = 0; i < FCH; i++) {
+                xp[i] = xm * (ool[i] * g.x) + SBF_C;
+                yp[i] = ym * (ool[i] * g.y) + SBF_C;
+            }
+            shapelet_dense_multi<FCH>(p, cm, xp, yp, f.der, f.dei);
+        }
+    }
+}
+
+// z = envelope x phasor of channel i of a FastTerm (ool_i = its frequency / c).
+template <int TYPE, int FCH>
+__device__ __forceinline__ void fast_z(const DirectParams& p, const FastTerm<TYPE, FCH>& f, int i, double ool_i,
+                                       int cglob, double4 g, bool dense, float& zr, float& zi) {
+    float sn, cs;
+    phasor_quarter_f32(4.0 * ool_i * f.tm, sn, cs);
+    if (TYPE == 1) {
+        // exponent in FP64, exp2 in FP32: rounding the exponent to FP32 moves
+        // the envelope by ln2 |x| 6e-8 2^-|x| <= 2.2e-8 of the component's flux;
+        // a Gaussian's envelope is real
+        const float er = exp2f((float)(f.exm * (ool_i * ool_i)));
+        zr = cs * er;
+        zi = sn * er;
+    } else {
+        float er, ei;
+        if (dense) {
+            er = f.der[i];
+            ei = f.dei[i];
+        } else {
+            shapelet_envelope_f32(p, cglob, g, f.su * ool_i, f.sv * ool_i, er, ei);
+        }
+        zr = cs * er - sn * ei;
+        zi = fmaf(cs, ei, sn * er);
+    }
+}
+
+// vis[o] += acc (JonesF64 or JonesF32 [channel][baseline] at element o).
+template <bool OUT64>
+__device__ __forceinline__ void add_vis(void* vis, size_t o, const J2& acc) {
+    if (OUT64) {
+        double2* q = reinterpret_cast<double2*>(reinterpret_cast<JonesF64*>(vis) + o);
+        const double2 a0 = q[0], b0 = q[1], c0 = q[2], d0 = q[3];
+        q[0] = make_double2(a0.x + acc.a.re, a0.y + acc.a.im);
+        q[1] = make_double2(b0.x + acc.b.re, b0.y + acc.b.im);
+        q[2] = make_double2(c0.x + acc.c.re, c0.y + acc.c.im);
+        q[3] = make_double2(d0.x + acc.d.re, d0.y + acc.d.im);
+    } else {
+        float4* q = reinterpret_cast<float4*>(reinterpret_cast<JonesF32*>(vis) + o);
+        float4 x = q[0], y = q[1];
+        x.x += (float)acc.a.re;
+        x.y += (float)acc.a.im;
+        x.z += (float)acc.b.re;
+        x.w += (float)acc.b.im;
+        y.x += (float)acc.c.re;
+        y.y += (float)acc.c.im;
+        y.z += (float)acc.d.re;
+        y.w += (float)acc.d.im;
+        q[0] = x;
+        q[1] = y;
+    }
+}
+
 // The chosen form's Gaussians and shapelets with FCH channels per thread: a
 // CTA covers 256 baselines of FCH consecutive channels, so each component's
 // FP64 work that does not depend on the channel -- the phase in metres, the
@@ -510,60 +606,14 @@ __global__ void __launch_bounds__(DT, FastShape<TYPE>::MIN_CTAS) fast_kernel(con
 #pragma unroll
                 for (int e = 0; e < 8; e++) a[i][e] = 0.f;
             for (int c = 0; c < n; c++) {
-                const double4 lmn = s_lmn[st][c];
                 const double4 g = s_gp[st][c];
-                const double tm = um * lmn.x + vm * lmn.y + wm * lmn.z;  // metres
-                double exm = 0.0, xm = 0.0, ym = 0.0, su = 0.0, sv = 0.0;
-                if (TYPE == 1) {
-                    // the exponent in FP64 (an FP32 exponent's absolute error,
-                    // ~1e-7 of its size, would become the envelope's relative error)
-                    const double kx = um * g.z + vm * g.w;
-                    const double ky = um * g.w - vm * g.z;
-                    // in base 2 (exp(x) = 2^(x log2 e)): the per-channel exp2f
-                    // costs fewer instructions than expf (measured)
-                    exm = (g.x * (kx * kx) + g.y * (ky * ky)) * 1.4426950408889634074;
-                } else {
-                    const double2 ta = __ldg(p.suv_tile + (size_t)(c0 + c) * p.ntiles + t1);
-                    const double2 tb = __ldg(p.suv_tile + (size_t)(c0 + c) * p.ntiles + t2);
-                    su = ta.x - tb.x;
-                    sv = ta.y - tb.y;
-                    xm = su * g.z + sv * g.w;
-                    ym = su * g.w - sv * g.z;
-                }
-                float der[FCH], dei[FCH];  // dense shapelet envelopes of all channels
-                if (TYPE == 2 && p.sdense) {
-                    double xp[FCH], yp[FCH];
-#pragma unroll
-                    for (int i = 0; i < FCH; i++) {
-                        xp[i] = xm * (ool[i] * g.x) + SBF_C;
-                        yp[i] = ym * (ool[i] * g.y) + SBF_C;
-                    }
-                    shapelet_dense_multi<FCH>(p, s_dense + c * SDN * SDN, xp, yp, der, dei);
-                }
+                FastTerm<TYPE, FCH> term;
+                fast_term<TYPE, FCH>(p, s_lmn[st][c], g, um, vm, wm, c0 + c, t1, t2, ool,
+                                     TYPE == 2 && p.sdense ? s_dense + c * SDN * SDN : nullptr, term);
 #pragma unroll
                 for (int i = 0; i < FCH; i++) {
-                    float sn, cs;
-                    phasor_quarter_f32(4.0 * ool[i] * tm, sn, cs);
-                    float er, ei = 0.f;
-                    if (TYPE == 1) {
-                        // exponent in FP64, exp2 in FP32: rounding the exponent
-                        // to FP32 moves the envelope by ln2 |x| 6e-8 2^-|x| <= 2.2e-8
-                        // of the component's flux
-                        er = exp2f((float)(exm * (ool[i] * ool[i])));
-                    } else if (p.sdense) {
-                        er = der[i], ei = dei[i];
-                    } else {
-                        shapelet_envelope_f32(p, c0 + c, g, su * ool[i], sv * ool[i], er, ei);
-                    }
-                    // z = envelope x phasor (a Gaussian's envelope is real)
                     float zr, zi;
-                    if (TYPE == 1) {
-                        zr = cs * er;
-                        zi = sn * er;
-                    } else {
-                        zr = cs * er - sn * ei;
-                        zi = fmaf(cs, ei, sn * er);
-                    }
+                    fast_z<TYPE, FCH>(p, term, i, ool[i], c0 + c, g, p.sdense != nullptr, zr, zi);
                     // a += W z with W Hermitian: 12 fused multiply-adds
                     const float4 wv = *reinterpret_cast<const float4*>(s_wf[i] + c * 4);
                     a[i][0] = fmaf(wv.x, zr, a[i][0]);
@@ -592,28 +642,7 @@ __global__ void __launch_bounds__(DT, FastShape<TYPE>::MIN_CTAS) fast_kernel(con
 #pragma unroll
     for (int i = 0; i < FCH; i++) {
         if (f0 + i >= p.nf) break;
-        const size_t o = (size_t)(f0 + i) * p.nbl + bl;
-        if (OUT64) {
-            double2* q = reinterpret_cast<double2*>(reinterpret_cast<JonesF64*>(p.vis) + o);
-            double2 a0 = q[0], b0 = q[1], c1 = q[2], d0 = q[3];
-            q[0] = make_double2(a0.x + acc[i].a.re, a0.y + acc[i].a.im);
-            q[1] = make_double2(b0.x + acc[i].b.re, b0.y + acc[i].b.im);
-            q[2] = make_double2(c1.x + acc[i].c.re, c1.y + acc[i].c.im);
-            q[3] = make_double2(d0.x + acc[i].d.re, d0.y + acc[i].d.im);
-        } else {
-            float4* q = reinterpret_cast<float4*>(reinterpret_cast<JonesF32*>(p.vis) + o);
-            float4 x = q[0], y = q[1];
-            x.x += (float)acc[i].a.re;
-            x.y += (float)acc[i].a.im;
-            x.z += (float)acc[i].b.re;
-            x.w += (float)acc[i].b.im;
-            y.x += (float)acc[i].c.re;
-            y.y += (float)acc[i].c.im;
-            y.z += (float)acc[i].d.re;
-            y.w += (float)acc[i].d.im;
-            q[0] = x;
-            q[1] = y;
-        }
+        add_vis<OUT64>(p.vis, (size_t)(f0 + i) * p.nbl + bl, acc[i]);
     }
 }
 
@@ -735,52 +764,14 @@ __global__ void __launch_bounds__(DT, 1) fast_tile_kernel(const DirectParams p) 
         __syncthreads();
         if (active) {
             for (int c = 0; c < n; c++) {
-                const double4 lmn = s_lmn[st][c];
                 const double4 g = s_gp[st][c];
-                const double tm = um * lmn.x + vm * lmn.y + wm * lmn.z;  // metres
-                double exm = 0.0, xm = 0.0, ym = 0.0, su = 0.0, sv = 0.0;
-                if (TYPE == 1) {
-                    const double kx = um * g.z + vm * g.w;
-                    const double ky = um * g.w - vm * g.z;
-                    exm = (g.x * (kx * kx) + g.y * (ky * ky)) * 1.4426950408889634074;
-                } else {
-                    const double2 ta = __ldg(p.suv_tile + (size_t)(c0 + c) * p.ntiles + t1);
-                    const double2 tb = __ldg(p.suv_tile + (size_t)(c0 + c) * p.ntiles + t2);
-                    su = ta.x - tb.x;
-                    sv = ta.y - tb.y;
-                    xm = su * g.z + sv * g.w;
-                    ym = su * g.w - sv * g.z;
-                }
-                float der[FCH], dei[FCH];
-                if (TYPE == 2 && p.sdense) {
-                    double xp[FCH], yp[FCH];
-#pragma unroll
-                    for (int i = 0; i < FCH; i++) {
-                        xp[i] = xm * (ool[i] * g.x) + SBF_C;
-                        yp[i] = ym * (ool[i] * g.y) + SBF_C;
-                    }
-                    shapelet_dense_multi<FCH>(p, s_dense + c * SDN * SDN, xp, yp, der, dei);
-                }
+                FastTerm<TYPE, FCH> term;
+                fast_term<TYPE, FCH>(p, s_lmn[st][c], g, um, vm, wm, c0 + c, t1, t2, ool,
+                                     TYPE == 2 && p.sdense ? s_dense + c * SDN * SDN : nullptr, term);
 #pragma unroll
                 for (int i = 0; i < FCH; i++) {
-                    float sn, cs;
-                    phasor_quarter_f32(4.0 * ool[i] * tm, sn, cs);
-                    float er, ei = 0.f;
-                    if (TYPE == 1) {
-                        er = exp2f((float)(exm * (ool[i] * ool[i])));
-                    } else if (p.sdense) {
-                        er = der[i], ei = dei[i];
-                    } else {
-                        shapelet_envelope_f32(p, c0 + c, g, su * ool[i], sv * ool[i], er, ei);
-                    }
                     float zr, zi;
-                    if (TYPE == 1) {
-                        zr = cs * er;
-                        zi = sn * er;
-                    } else {
-                        zr = cs * er - sn * ei;
-                        zi = fmaf(cs, ei, sn * er);
-                    }
+                    fast_z<TYPE, FCH>(p, term, i, ool[i], c0 + c, g, p.sdense != nullptr, zr, zi);
                     const cplx z = {(double)zr, (double)zi};
                     const double2* rg = s_gh + ((size_t)(i * CH + c) * nu + u1) * 8;
                     const double2* rh = s_gh + ((size_t)(i * CH + c) * nu + u2) * 8 + 4;
@@ -812,28 +803,7 @@ __global__ void __launch_bounds__(DT, 1) fast_tile_kernel(const DirectParams p) 
 #pragma unroll
     for (int i = 0; i < FCH; i++) {
         if (f0 + i >= p.nf) break;
-        const size_t o = (size_t)(f0 + i) * p.nbl + bl;
-        if (OUT64) {
-            double2* q = reinterpret_cast<double2*>(reinterpret_cast<JonesF64*>(p.vis) + o);
-            double2 a0 = q[0], b0 = q[1], c1 = q[2], d0 = q[3];
-            q[0] = make_double2(a0.x + acc[i].a.re, a0.y + acc[i].a.im);
-            q[1] = make_double2(b0.x + acc[i].b.re, b0.y + acc[i].b.im);
-            q[2] = make_double2(c1.x + acc[i].c.re, c1.y + acc[i].c.im);
-            q[3] = make_double2(d0.x + acc[i].d.re, d0.y + acc[i].d.im);
-        } else {
-            float4* q = reinterpret_cast<float4*>(reinterpret_cast<JonesF32*>(p.vis) + o);
-            float4 x = q[0], y = q[1];
-            x.x += (float)acc[i].a.re;
-            x.y += (float)acc[i].a.im;
-            x.z += (float)acc[i].b.re;
-            x.w += (float)acc[i].b.im;
-            y.x += (float)acc[i].c.re;
-            y.y += (float)acc[i].c.im;
-            y.z += (float)acc[i].d.re;
-            y.w += (float)acc[i].d.im;
-            q[0] = x;
-            q[1] = y;
-        }
+        add_vis<OUT64>(p.vis, (size_t)(f0 + i) * p.nbl + bl, acc[i]);
     }
 }
 
