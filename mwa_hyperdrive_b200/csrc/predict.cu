@@ -648,24 +648,25 @@ __global__ void __launch_bounds__(DT, FastShape<TYPE>::MIN_CTAS) fast_kernel(con
 
 // The chosen form's Gaussians and shapelets with a beam per tile: each
 // thread takes one baseline (p, q) and FT_FCH consecutive channels, as
-// fast_kernel does.  Per staged chunk of components the CTA forms, in FP64
-// shared memory, G = B_u S and H = B_u for every unique tile u and each of its
-// channels (B the tile's beam Jones at the channel's beam frequency, S the
-// component's instrumental flux), laid out [channel][component][unique
+// fast_kernel does.  Per staged chunk of components the CTA forms in shared
+// memory G = B_u S (FP32) and H = B_u (FP64) for every unique tile u and each
+// of its channels (B the tile's beam Jones at the channel's beam frequency,
+// S the component's instrumental flux), laid out [channel][component][unique
 // tile] so that a warp's threads, which share tile p and mostly share the
 // unique beam of tile q, read the same or neighbouring records.  A
 // visibility term is then z G_p H_q^H = B_p (z S) B_q^H: the phasor and
-// envelope z in FP32 exactly as fast_kernel computes them, the products in
-// FP64 (16 + 32 operations).  FP32 products (measured) put the
-// cross-polarisation terms' cancellation at FP32 precision of the parallel
-// hands and the p99.9 error at 1.0-1.15e-6; in FP64 the terms keep the
-// shared-beam form's error structure (W = B S B^H rounded once, relative to
-// each element).
+// envelope z in FP32 exactly as fast_kernel computes them, z G_p in FP32,
+// and its product with H_q^H accumulated in FP64 (32 fused multiply-adds).
+// All-FP32 products (measured) put the cross-polarisation terms'
+// cancellation at FP32 precision of the parallel hands and the p99.9 error
+// at 1.0-1.15e-6; accumulating in FP64 keeps each element's rounding
+// relative to its own size, as the shared-beam form's W = B S B^H rounded
+// once does (p99.9 3.4e-7 and 5.3e-7 on the tests' skies).
 constexpr int FT_FCH = 2;      // channels per thread
 constexpr int FT_CH = 16;      // components per staged chunk
 constexpr int FT_MAX_NU = 32;  // unique tiles (more: the FP64 per-tile kernel)
 
-inline size_t fast_tile_smem_bytes(int nu) { return (size_t)FT_FCH * FT_CH * nu * 8 * sizeof(double2); }
+inline size_t fast_tile_smem_bytes(int nu) { return (size_t)FT_FCH * FT_CH * nu * 6 * sizeof(float4); }
 
 template <int TYPE, bool OUT64>
 __global__ void __launch_bounds__(DT, 1) fast_tile_kernel(const DirectParams p) {
@@ -676,8 +677,9 @@ __global__ void __launch_bounds__(DT, 1) fast_tile_kernel(const DirectParams p) 
     __shared__ alignas(128) double4 s_gp[2][CH];
     __shared__ alignas(16) float s_dense[TYPE == 2 ? CH * SDN * SDN : 1];
     __shared__ alignas(8) uint64_t bar[2];
-    // [FCH][CH][nu] records of 8 double2: G (a, b, c, d) then H (a, b, c, d)
-    extern __shared__ double2 s_gh[];
+    // [FCH][CH][nu] records of 96 bytes: G (2 float4: a, b | c, d), then H
+    // (4 double2: a, b, c, d)
+    extern __shared__ float4 s_gh[];
     const int nu = p.n_uniq_tile;
 
     const int f0 = blockIdx.y * FCH;
@@ -749,15 +751,14 @@ __global__ void __launch_bounds__(DT, 1) fast_tile_kernel(const DirectParams p) 
             if (c >= n) continue;
             const J2 b = ldg_j(p.beam + ((size_t)u * p.n_uniq_freq + col[i]) * p.nc + c0 + c);
             const J2 g = b * load_j(s_flux[st][i][c]);
-            double2* r = s_gh + (size_t)e * 8;
-            r[0] = make_double2(g.a.re, g.a.im);
-            r[1] = make_double2(g.b.re, g.b.im);
-            r[2] = make_double2(g.c.re, g.c.im);
-            r[3] = make_double2(g.d.re, g.d.im);
-            r[4] = make_double2(b.a.re, b.a.im);
-            r[5] = make_double2(b.b.re, b.b.im);
-            r[6] = make_double2(b.c.re, b.c.im);
-            r[7] = make_double2(b.d.re, b.d.im);
+            float4* rf = s_gh + (size_t)e * 6;
+            rf[0] = make_float4((float)g.a.re, (float)g.a.im, (float)g.b.re, (float)g.b.im);
+            rf[1] = make_float4((float)g.c.re, (float)g.c.im, (float)g.d.re, (float)g.d.im);
+            double2* r = reinterpret_cast<double2*>(rf + 2);
+            r[0] = make_double2(b.a.re, b.a.im);
+            r[1] = make_double2(b.b.re, b.b.im);
+            r[2] = make_double2(b.c.re, b.c.im);
+            r[3] = make_double2(b.d.re, b.d.im);
         }
         if (TYPE == 2 && p.sdense)
             for (int e = threadIdx.x; e < n * SDN * SDN; e += DT) s_dense[e] = __ldg(p.sdense + (size_t)c0 * SDN * SDN + e);
@@ -772,12 +773,13 @@ __global__ void __launch_bounds__(DT, 1) fast_tile_kernel(const DirectParams p) 
                 for (int i = 0; i < FCH; i++) {
                     float zr, zi;
                     fast_z<TYPE, FCH>(p, term, i, ool[i], c0 + c, g, p.sdense != nullptr, zr, zi);
-                    const cplx z = {(double)zr, (double)zi};
-                    const double2* rg = s_gh + ((size_t)(i * CH + c) * nu + u1) * 8;
-                    const double2* rh = s_gh + ((size_t)(i * CH + c) * nu + u2) * 8 + 4;
-                    // zG = z G_p, then acc += zG H_q^H: M[r][s] = sum_k zG[r][k] conj(H[s][k])
-                    const cplx za = z * cplx{rg[0].x, rg[0].y}, zb = z * cplx{rg[1].x, rg[1].y};
-                    const cplx zc = z * cplx{rg[2].x, rg[2].y}, zd = z * cplx{rg[3].x, rg[3].y};
+                    const float4* rg = s_gh + ((size_t)(i * CH + c) * nu + u1) * 6;
+                    const double2* rh = reinterpret_cast<const double2*>(s_gh + ((size_t)(i * CH + c) * nu + u2) * 6 + 2);
+                    const float4 g0 = rg[0], g1 = rg[1];
+                    const cplx za = {(double)(zr * g0.x - zi * g0.y), (double)fmaf(zr, g0.y, zi * g0.x)};
+                    const cplx zb = {(double)(zr * g0.z - zi * g0.w), (double)fmaf(zr, g0.w, zi * g0.z)};
+                    const cplx zc = {(double)(zr * g1.x - zi * g1.y), (double)fmaf(zr, g1.y, zi * g1.x)};
+                    const cplx zd = {(double)(zr * g1.z - zi * g1.w), (double)fmaf(zr, g1.w, zi * g1.z)};
                     const double2 ha = rh[0], hb = rh[1], hc = rh[2], hd = rh[3];
                     J2& m = acc[i];
                     m.a.re = fma(za.re, ha.x, fma(za.im, ha.y, fma(zb.re, hb.x, fma(zb.im, hb.y, m.a.re))));
