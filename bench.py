@@ -1015,13 +1015,13 @@ def guarded(fn, args):
 # kernel class on this workload (one timestep, 384 channels), from the ncu
 # launch list of the bench command itself (one pass: gpu__time_duration and
 # the two DRAM counters), summarised in
-# profiles/predict_launch_list_mixed_predict.md.  The visibilities alone are
+# the launch-list summary of the predict kernels.  The visibilities alone are
 # 100 MB read + 100 MB written per launch.
 # The tensor point predict of one timestep runs in chunks of channels; the
 # figure is its Gram kernels' DRAM over the timestep: they read the table of
 # A planes and phasors (written by phasor_table_kernel, 2.42 GB per
 # timestep) once from DRAM.
-NCU_TRAFFIC_SOURCE = "ncu launch list of this bench command (profiles/predict_launch_list_mixed_predict.md)"
+NCU_TRAFFIC_SOURCE = "ncu launch list of this bench command (launch-list summary of the predict kernels)"
 NCU_DRAM_BYTES_PER_LAUNCH = {
     ("points", "tensor"): 2927e6, ("gaussians", "tensor"): 156.0e6, ("shapelets", "tensor"): 164.5e6,
     ("points", "direct"): 268.0e6, ("gaussians", "direct"): 152.0e6, ("shapelets", "direct"): 142.0e6,

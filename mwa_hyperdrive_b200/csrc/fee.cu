@@ -126,8 +126,11 @@ __device__ __forceinline__ void fee_pair_add(const FeeMode& r, double ra, double
 // (from (1 - x^2) dP_n^m/dx = (n + 1) x P_n^m - (n - m + 1) P_{n+1}^m), and
 // the m = 0 modes take P1 = P_n^1 = s R_n^1 from the |m| = 1 column: one
 // recurrence per (n, |m|), no division, exact at the zenith.  Every record
-// and table entry a thread loads serves its D directions.  (Measured
-// alternatives are listed with the kernel's profile.)
+// and table entry a thread loads serves its D directions.  (Measured and
+// not kept, on 4600 directions x 600 sets at degree 16: three Legendre
+// columns per |m|, 3.3 ms; the coefficient records read one mode ahead in
+// registers, 3.5 ms; four unique frequencies per thread at one direction,
+// 3.3 ms; three directions per thread, 2.3 ms; this form, 1.74 ms.)
 template <int D>
 __device__ void fee_sums(const double (&theta)[D], const double (&phi)[D], const FeeMode* __restrict__ q, int nmax,
                          const FeeRec* __restrict__ rec, FeeSums (&out)[D]) {
