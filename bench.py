@@ -1014,9 +1014,8 @@ def guarded(fn, args):
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of each
 # kernel class on this workload (one timestep, 384 channels), from the ncu
 # launch list of the bench command itself (one pass: gpu__time_duration and
-# the two DRAM counters), summarised in
-# the launch-list summary of the predict kernels.  The visibilities alone are
-# 100 MB read + 100 MB written per launch.
+# the two DRAM counters).  The visibilities alone are 100 MB read + 100 MB
+# written per launch.
 # The tensor point predict of one timestep runs in chunks of channels; the
 # figure is its Gram kernels' DRAM over the timestep: they read the table of
 # A planes and phasors (written by phasor_table_kernel, 2.42 GB per
