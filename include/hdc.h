@@ -636,6 +636,7 @@ typedef struct HdcPeelParams {
     int beam_kind;           /* HDC_BEAM_* for the per-source models */
     double array_latitude_rad;
     int batch_size;          /* batched form: sources per sub-batch in list order (0: all in one) */
+    const HdcFeeBeam *fee_beam; /* beam_kind HDC_BEAM_FEE: the beam, prepared for these tiles and channels */
 } HdcPeelParams;
 
 /* peel_gpu (params/peel/gpu.rs:25-757): peel num_sources sources from the

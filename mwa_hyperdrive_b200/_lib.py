@@ -38,7 +38,7 @@ class IonoConsts(ctypes.Structure):
 class HdcPeelParams(ctypes.Structure):
     _fields_ = [("num_passes", c_int), ("num_loops", c_int), ("convergence", c_double),
                 ("freq_average_factor", c_int), ("beam_kind", c_int), ("array_latitude_rad", c_double),
-                ("batch_size", c_int)]
+                ("batch_size", c_int), ("fee_beam", c_void_p)]
 
 
 class HdcFeeCoeffs(ctypes.Structure):

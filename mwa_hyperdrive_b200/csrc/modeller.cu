@@ -688,7 +688,7 @@ int Modeller::model_uvws(double lst, const UVW* d_uvws_ext, JonesF32* d_vis, cud
         if (t[ty].nc == 0) continue;
         DirectParams p = direct_params(ty, d_vis);
         p.uvws = d_uvws_ext;
-        HDC_CUDA_RET_INT(launch_direct(ty, false, false, p, s));
+        HDC_CUDA_RET_INT(launch_direct(ty, tile_beams(), false, p, s));
     }
     return queue_error_check(s);
 }
@@ -1004,6 +1004,26 @@ extern "C" int hdc_modeller_new(const HdcSkyModel* sky, int pols, const XYZ* h_x
     *out = reinterpret_cast<HdcModeller*>(m);
     return HDC_OK;
 }
+
+namespace hdc {
+int peel_modeller_new(const HdcSkyModel* sky, const XYZ* h_xyzs, int num_tiles, const double* h_freqs, int num_freqs,
+                      RADec phase_centre, const HdcPeelParams* params, HdcModeller** out) {
+    const bool fee = params->beam_kind == HDC_BEAM_FEE;
+    if (fee && !params->fee_beam) {
+        set_error("peel: beam_kind HDC_BEAM_FEE needs fee_beam");
+        return HDC_ERR_ARG;
+    }
+    int rc = hdc_modeller_new(sky, 0, h_xyzs, num_tiles, h_freqs, num_freqs, phase_centre, params->array_latitude_rad,
+                              fee ? HDC_BEAM_NONE : params->beam_kind, HDC_PREDICT_DIRECT, out);
+    if (rc || !fee) return rc;
+    rc = hdc_modeller_set_fee_beam(*out, params->fee_beam);
+    if (rc) {
+        hdc_modeller_free(*out);
+        *out = nullptr;
+    }
+    return rc;
+}
+}  // namespace hdc
 
 extern "C" int hdc_modeller_set_tile_beams(HdcModeller* hm, const double* h_dipole_gains, double freq_res_hz) {
     Modeller* m = reinterpret_cast<Modeller*>(hm);

@@ -44,6 +44,10 @@ int fee_launch_radec(const HdcFeeBeam* b, const double2* d_radec, int n, double 
 int fee_num_tiles(const HdcFeeBeam* b);
 int fee_num_freqs(const HdcFeeBeam* b);
 int fee_device(const HdcFeeBeam* b);
+// A peel loop's per-source modeller (direct FP64 form) with the loop's beam:
+// params->beam_kind, or the FEE beam params->fee_beam.
+int peel_modeller_new(const HdcSkyModel* sky, const XYZ* h_xyzs, int num_tiles, const double* h_freqs, int num_freqs,
+                      RADec phase_centre, const HdcPeelParams* params, HdcModeller** out);
 
 struct TensorState;
 

@@ -485,7 +485,9 @@ extern "C" int hdc_peel_timeblock_batched(JonesF32* d_resid_tfb, const float* d_
 
     // point-at-centre sources keep a (timestep, channel) table; otherwise
     // the models need ns x nvis JonesF32 of device memory
-    bool points = true;
+    // (with a beam shared by all tiles, or none: per-tile beams make a
+    // point's model depend on the baseline)
+    bool points = params->beam_kind == HDC_BEAM_NONE || params->beam_kind == HDC_BEAM_ANALYTIC_DIPOLE;
     for (int i = 0; i < ns && points; i++) {
         const HdcSkyModel& m = h_sources[i];
         points = m.num_components == 1 && m.comp_type[0] == 0 && std::fabs(m.ra[0] - h_source_positions[i].ra) < 1e-12 &&
@@ -593,9 +595,8 @@ extern "C" int hdc_peel_timeblock_batched(JonesF32* d_resid_tfb, const float* d_
     } else {
         for (int i = 0; i < ns; i++) {
             HdcModeller* hm = nullptr;
-            int rc = hdc_modeller_new(&h_sources[i], 0, h_tile_xyzs, num_tiles, h_freqs, num_freqs,
-                                      h_source_positions[i], params->array_latitude_rad, params->beam_kind,
-                                      HDC_PREDICT_DIRECT, &hm);
+            int rc = peel_modeller_new(&h_sources[i], h_tile_xyzs, num_tiles, h_freqs, num_freqs,
+                                       h_source_positions[i], params, &hm);
             if (rc) return rc;
             std::unique_ptr<Modeller> m(reinterpret_cast<Modeller*>(hm));
             const UVW* uv = b_uv_src.as<UVW>() + (size_t)i * nt * nbl;

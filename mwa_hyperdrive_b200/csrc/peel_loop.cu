@@ -131,8 +131,8 @@ extern "C" int hdc_peel_timeblock(JonesF32* d_resid_tfb, const float* d_weights_
     std::vector<std::unique_ptr<Modeller>> models;
     for (int i = 0; i < num_sources; i++) {
         HdcModeller* hm = nullptr;
-        int rc = hdc_modeller_new(&h_sources[i], 0, h_tile_xyzs, num_tiles, h_freqs, num_freqs, h_source_positions[i],
-                                  params->array_latitude_rad, params->beam_kind, HDC_PREDICT_DIRECT, &hm);
+        int rc = peel_modeller_new(&h_sources[i], h_tile_xyzs, num_tiles, h_freqs, num_freqs, h_source_positions[i],
+                                   params, &hm);
         if (rc) return rc;
         models.emplace_back(reinterpret_cast<Modeller*>(hm));
     }

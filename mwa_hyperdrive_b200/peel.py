@@ -42,13 +42,15 @@ class PeelLoopParams:
 def peel_timeblock(d_resid_tfb, d_weights_tfb, freqs, tile_xyzs, lmsts, average_lmst, phase_centre, sources,
                    source_positions, iono_consts: Sequence[IonoConsts], num_passes: int, num_loops: int,
                    convergence: float, freq_average_factor: int, array_latitude_rad: float, beam: str = "none",
-                   stream=None, batched: bool = False, batch_size: int = 0) -> List[IonoConsts]:
+                   stream=None, batched: bool = False, batch_size: int = 0, fee_beam=None) -> List[IonoConsts]:
     """Peel ``sources`` (a list of SourceList / Source / SkyModelArrays, one per
     source) with explicit pass and loop counts.  ``batched`` selects
     hdc_peel_timeblock_batched (the sources of a sub-batch fitted together
     against the residual at the start of the sub-batch; sub-batches of
     ``batch_size`` sources in list order, 0 for all in one) instead of the
-    reference's source-by-source order."""
+    reference's source-by-source order.  ``beam`` "fee" models the sources
+    with ``fee_beam`` (a :class:`mwa_hyperdrive_b200.fee.FeeBeam` prepared
+    for these tiles and channels), as the reference's peel uses its beam."""
     nt, nf, nbl = (int(x) for x in d_resid_tfb.shape[:3])
     freqs = np.ascontiguousarray(freqs, np.float64)
     xyzs = np.ascontiguousarray(tile_xyzs, np.float64).reshape(-1, 3)
@@ -62,8 +64,11 @@ def peel_timeblock(d_resid_tfb, d_weights_tfb, freqs, tile_xyzs, lmsts, average_
         structs[i] = sk.struct()
     pos = (_lib.RADec * max(n, 1))(*[_lib.RADec(*p) for p in source_positions])
     consts = (_lib.IonoConsts * max(n, 1))(*[_lib.IonoConsts(c.alpha, c.beta, c.gain) for c in iono_consts])
+    if beam == "fee" and fee_beam is None:
+        raise ValueError('beam "fee" needs fee_beam')
     params = _lib.HdcPeelParams(int(num_passes), int(num_loops), float(convergence), int(freq_average_factor),
-                                BEAMS[beam], float(array_latitude_rad), int(batch_size))
+                                BEAMS[beam], float(array_latitude_rad), int(batch_size),
+                                fee_beam.handle if beam == "fee" else None)
     fn = _lib.lib().hdc_peel_timeblock_batched if batched else _lib.lib().hdc_peel_timeblock
     rc = fn(d_resid_tfb.data_ptr(), d_weights_tfb.data_ptr(), nt, nf, freqs.ctypes.data, xyzs.ctypes.data,
             xyzs.shape[0], lmsts.ctypes.data, float(average_lmst), _lib.RADec(*phase_centre), n,

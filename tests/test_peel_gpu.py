@@ -172,25 +172,28 @@ def make_peel_problem(seed=3, ntiles=20, nt=2, nf=8, nsrc=3, inject=True, points
     return rng, pc, xyzs, freqs, lmsts, lam, nbl, sources, positions, truths
 
 
-def simulate_residual(oracle, pc, xyzs, freqs, lmsts, lam, sources, positions, truths):
+def simulate_residual(oracle, pc, xyzs, freqs, lmsts, lam, sources, positions, truths, beam_for=None):
     """data = sum_s model_s * iono_s (uv at the source position); residual =
-    data - sum_s model_s, everything at the observation phase centre."""
+    data - sum_s model_s, everything at the observation phase centre;
+    beam_for(sky, lst) gives the oracle's per-tile beam tables (or none)."""
     nt, nf = lmsts.size, freqs.size
     n = xyzs.shape[0]
     nbl = n * (n - 1) // 2
     resid = np.zeros((nt, nf, nbl, 8), np.float64)
     for sky, pos, tr in zip(sources, positions, truths):
         for t in range(nt):
-            m, _ = oracle.model_timestep(sky, xyzs, freqs, pc, lmsts[t], synth.MWA_LAT_RAD, out_f64=True)
+            m, _ = oracle.model_timestep(sky, xyzs, freqs, pc, lmsts[t], synth.MWA_LAT_RAD, out_f64=True,
+                                         beam=beam_for(sky, lmsts[t]) if beam_for else None)
             uvw_src = oracle.xyzs_to_cross_uvws(xyzs, lmsts[t] - pos[0], pos[1])
             resid[t] += iono_rotate(m, uvw_src, tr, lam).astype(np.float64) - m
     return resid.astype(np.float32)
 
 
 def oracle_peel(oracle, resid, weights, pc, xyzs, freqs, lmsts, avg_lmst, sources, positions, consts, num_passes,
-                num_loops, conv, favg):
+                num_loops, conv, favg, beam_for=None):
     """The native loop's sequence (peel_gpu, params/peel/gpu.rs:355-757)
-    composed from the oracle's kernels."""
+    composed from the oracle's kernels (beam_for(sky, lst): the sources'
+    per-tile beam tables, or none)."""
     resid = resid.copy()
     nt, nf, nbl = resid.shape[:3]
     n = xyzs.shape[0]
@@ -212,7 +215,7 @@ def oracle_peel(oracle, resid, weights, pc, xyzs, freqs, lmsts, avg_lmst, source
                 for ty in range(3):
                     if np.any(np.asarray(sky.comp_type) == ty):
                         oracle.model_type(ty, sky, xyzs, freqs, pos, lmsts[t], synth.MWA_LAT_RAD, to[t],
-                                          vis=model[t])
+                                          vis=model[t], beam=beam_for(sky, lmsts[t]) if beam_for else None)
             rsrc = oracle.add_model(resid, model, old, lam, to)
             mrot = oracle.add_model(np.zeros_like(model), model, old, lam, to)
             rlo = oracle.average(rsrc, weights, favg)
@@ -362,3 +365,89 @@ def test_batched_peel_sub_batches_recover_injected_iono(oracle):
         assert abs(g.alpha - tr[0]) < 0.02 * abs(tr[0]) + 2e-7, (g, tr)
         assert abs(g.gain - tr[2]) < 5e-3, (g, tr)
     assert np.linalg.norm(d_resid.cpu().numpy()) < 0.05 * np.linalg.norm(resid)
+
+
+# ------------------------------------------------------------ the FEE beam
+def fee_peel_beam(oracle, xyzs, freqs, seed=4):
+    """An FEE beam per tile (synthetic coefficients at the channels, two tiles
+    with a dead dipole) and beam_for(sky, lst): the oracle's FEE tables of a
+    source's components in the library's unique order."""
+    from mwa_hyperdrive_b200.fee import FeeBeam
+    from oracle import fee_ref as fr
+
+    n = xyzs.shape[0]
+    file = synth.fee_coeffs(np.round(freqs).astype(np.uint32), 6, seed=seed)
+    delays = np.tile(np.arange(16, dtype=np.uint32) % 3, (n, 1))
+    delays[2, 5] = delays[7, 11] = 32
+    amps = np.ones((n, 32))
+    beam = FeeBeam(file, freqs, delays, amps)
+    tmap, fmap = beam.maps()
+    nu, nuf = int(tmap.max()) + 1, int(fmap.max()) + 1
+
+    def beam_for(sky, lst):
+        tabs = []
+        for ty in range(3):
+            sel = np.asarray(sky.comp_type) == ty
+            if not sel.any():
+                tabs.append(None)
+                continue
+            azel = [oracle.hadec_to_azel(lst - ra, dec, synth.MWA_LAT_RAD) for ra, dec in zip(sky.ra[sel], sky.dec[sel])]
+            az = np.array([a for a, _ in azel])
+            za = np.array([math.pi / 2 - e for _, e in azel])
+            out = np.zeros((nu, nuf, az.size, 8))
+            for u in range(nu):
+                t = int(np.argmax(tmap == u))
+                for uf in range(nuf):
+                    f = int(np.argmax(fmap == uf))
+                    out[u, uf] = fr.as_jones8(fr.calc_jones(file, az, za, freqs[f], delays[t], amps[t],
+                                                            latitude=synth.MWA_LAT_RAD))
+            tabs.append(out)
+        return oracle.beam_struct(2, tabs, tmap, fmap, nuf)
+
+    return beam, beam_for
+
+
+def test_native_peel_with_fee_beam_matches_oracle_loop(oracle):
+    """The peel loop with the FEE beam per tile (the reference's peel_gpu
+    models its sources through the same beam) against the oracle's loop
+    given the oracle's FEE tables."""
+    rng, pc, xyzs, freqs, lmsts, lam, nbl, sources, positions, truths = make_peel_problem(seed=5)
+    beam, beam_for = fee_peel_beam(oracle, xyzs, freqs)
+    resid = simulate_residual(oracle, pc, xyzs, freqs, lmsts, lam, sources, positions, truths, beam_for)
+    weights = np.ones(resid.shape[:3], np.float32)
+    avg_lmst = float(np.median(lmsts))
+    d_resid = dev(resid, np.float32)
+    got = P.peel_timeblock(d_resid, dev(weights, np.float32), freqs, xyzs, lmsts, avg_lmst, pc, sources, positions,
+                           [P.IonoConsts() for _ in sources], num_passes=2, num_loops=5, convergence=1.0,
+                           freq_average_factor=4, array_latitude_rad=synth.MWA_LAT_RAD, beam="fee", fee_beam=beam)
+    ref_resid, ref_consts = oracle_peel(oracle, resid, weights, pc, xyzs, freqs, lmsts, avg_lmst, sources, positions,
+                                        [(0.0, 0.0, 1.0)] * len(sources), 2, 5, 1.0, 4, beam_for)
+    for g, r in zip(got, ref_consts):
+        assert abs(g.alpha - r[0]) <= 1e-5 * abs(r[0]) + 1e-12
+        assert abs(g.beta - r[1]) <= 1e-5 * abs(r[1]) + 1e-12
+        assert abs(g.gain - r[2]) <= 1e-6
+    assert rel(d_resid.cpu().numpy(), ref_resid) < 1e-4
+
+
+def test_batched_peel_with_fee_beam_recovers_injected_iono(oracle):
+    """Both peel forms with the FEE beam recover the offsets injected through
+    that beam (the batched form's shared-weights shortcut for points does not
+    apply to per-tile beams)."""
+    rng, pc, xyzs, freqs, lmsts, lam, nbl, sources, positions, truths = make_peel_problem(seed=7, ntiles=24, nf=16,
+                                                                                           nsrc=2, points=True)
+    beam, beam_for = fee_peel_beam(oracle, xyzs, freqs, seed=6)
+    resid = simulate_residual(oracle, pc, xyzs, freqs, lmsts, lam, sources, positions, truths, beam_for)
+    before = np.linalg.norm(resid)
+    weights = np.ones(resid.shape[:3], np.float32)
+    for batched in (False, True):
+        d_resid = dev(resid, np.float32)
+        got = P.peel_timeblock(d_resid, dev(weights, np.float32), freqs, xyzs, lmsts, float(np.median(lmsts)), pc,
+                               sources, positions, [P.IonoConsts() for _ in sources], num_passes=3, num_loops=10,
+                               convergence=1.0, freq_average_factor=4, array_latitude_rad=synth.MWA_LAT_RAD,
+                               batched=batched, beam="fee", fee_beam=beam)
+        after = np.linalg.norm(d_resid.cpu().numpy())
+        for g, tr in zip(got, truths):
+            assert abs(g.alpha - tr[0]) < 0.02 * abs(tr[0]) + 2e-7, (batched, g, tr)
+            assert abs(g.beta - tr[1]) < 0.02 * abs(tr[1]) + 2e-7, (batched, g, tr)
+            assert abs(g.gain - tr[2]) < 5e-3, (batched, g, tr)
+        assert after < 0.05 * before, (batched, after, before)
