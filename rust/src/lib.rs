@@ -10,8 +10,9 @@
 //! unchanged once `build.rs` links libhdc instead of compiling src/gpu/*.cu.
 //!
 //! The safe wrappers below cover the native layer's trait-shaped entry
-//! points: [`Modeller`] (the `SkyModeller` trait, model/mod.rs:123-204) and
-//! [`calibrate_timeblock`] (di_calibrate/mod.rs:387-618).
+//! points: [`Modeller`] (the `SkyModeller` trait, model/mod.rs:123-204),
+//! [`calibrate_timeblock`] (di_calibrate/mod.rs:387-618) and [`FeeBeam`]
+//! (the `FEEBeamGpu` calls of beam/fee.rs:307-369).
 
 pub mod ffi;
 pub use ffi::*;
@@ -122,6 +123,78 @@ impl Drop for Modeller {
 // (model/gpu.rs:140); the native modeller is likewise used from one thread
 // at a time.
 unsafe impl Send for Modeller {}
+
+/// The MWA FEE beam prepared on the current device (FEEBeam::gpu_prepare,
+/// beam/fee.rs:307-320): the caller reads the beam file into `HdcFeeCoeffs`
+/// (the `hdf5` crate; complex coefficients from the file's amplitude and
+/// phase rows).
+pub struct FeeBeam {
+    raw: *mut HdcFeeBeam,
+    pub num_tiles: usize,
+    pub num_freqs: usize,
+}
+
+impl FeeBeam {
+    /// `delays` [tile][16] (32: a dead dipole), `amps` [tile][32] (X then Y)
+    /// or [tile][16]; `freqs_hz` the channels.
+    pub fn new(file: &HdcFeeCoeffs, freqs_hz: &[u32], delays: &[[u32; 16]], amps: &[f64], num_amps: usize,
+               norm_to_zenith: bool) -> Result<Self, HdcError> {
+        assert!(num_amps == 16 || num_amps == 32);
+        assert_eq!(amps.len(), delays.len() * num_amps);
+        let mut raw = null_mut();
+        check(unsafe {
+            hdc_fee_beam_new(file, freqs_hz.as_ptr(), freqs_hz.len() as c_int, delays.as_ptr() as *const u32,
+                             amps.as_ptr(), delays.len() as c_int, num_amps as c_int, norm_to_zenith as c_int,
+                             &mut raw)
+        })?;
+        Ok(FeeBeam { raw, num_tiles: delays.len(), num_freqs: freqs_hz.len() })
+    }
+
+    /// BeamGpu::get_num_unique_tiles / get_num_unique_freqs.
+    pub fn num_unique(&self) -> (usize, usize) {
+        unsafe {
+            (hdc_fee_beam_num_unique_tiles(self.raw) as usize, hdc_fee_beam_num_unique_freqs(self.raw) as usize)
+        }
+    }
+
+    /// BeamGpu::get_tile_map / get_freq_map: device pointers owned by the beam.
+    pub fn device_maps(&self) -> (*const c_int, *const c_int) {
+        unsafe { (hdc_fee_beam_tile_map(self.raw), hdc_fee_beam_freq_map(self.raw)) }
+    }
+
+    /// BeamGpu::calc_jones_pair (iau_order false): `d_jones` gets
+    /// [uniq tile][uniq freq][direction].
+    ///
+    /// # Safety
+    /// `d_az_rad` and `d_za_rad` are device arrays of `n` directions,
+    /// `d_latitude_rad` a device pointer to one value (or null), `d_jones`
+    /// holds unique tiles x unique frequencies x `n` JonesF64.
+    pub unsafe fn calc_jones_pair(&self, d_az_rad: *const f64, d_za_rad: *const f64, n: usize,
+                                  d_latitude_rad: *const f64, d_jones: *mut JonesF64,
+                                  stream: *mut CUstream_st) -> Result<(), HdcError> {
+        check(hdc_fee_calc_jones(self.raw, d_az_rad, d_za_rad, n as c_int, d_latitude_rad, 0, d_jones, stream))
+    }
+
+    pub fn as_ptr(&self) -> *const HdcFeeBeam {
+        self.raw
+    }
+}
+
+impl Drop for FeeBeam {
+    fn drop(&mut self) {
+        unsafe { hdc_fee_beam_free(self.raw) }
+    }
+}
+
+unsafe impl Send for FeeBeam {}
+
+impl Modeller {
+    /// The FEE beam for every tile (HDC_BEAM_FEE); `beam` must outlive the
+    /// modeller's use of it.
+    pub fn set_fee_beam(&mut self, beam: &FeeBeam) -> Result<(), HdcError> {
+        check(unsafe { hdc_modeller_set_fee_beam(self.raw, beam.as_ptr()) })
+    }
+}
 
 /// calibrate_timeblock (di_calibrate/mod.rs:387-618) on device buffers:
 /// `d_di_jones` [tile][chanblock] holds the starting gains in and the
