@@ -277,3 +277,27 @@ def test_autos_with_fee_beam(oracle):
     ref = np.asarray(ref, np.float32)
     scale = np.maximum(np.abs(ref), np.float32(np.max(np.abs(ref)) * 1e-6 + 1e-30))
     assert not (np.abs(got - ref) > 4 * np.spacing(scale)).any(), np.max(np.abs(got - ref))
+
+
+def test_calc_jones_at_degree_30(oracle):
+    """Degrees up to 30, where the recurrences' dynamic range is largest
+    ((2m - 1)!! against the small C_mn): within 1e-8 of the largest element.
+    The bar is the oracle's own: its Legendre series (numpy's) agrees with
+    scipy's lpmv to 1.5e-9 of a column's largest value at degree 40 and
+    loses digits with degree."""
+    file = synth.fee_coeffs([167680000, 168960000], [28, 30], seed=9)
+    rng = np.random.default_rng(4)
+    n = 64
+    az = rng.uniform(0.0, 2 * math.pi, n)
+    za = rng.uniform(0.0, 1.5, n)
+    freqs = np.array([167.68e6, 168.96e6])
+    delays = np.stack([np.arange(16, dtype=np.uint32) % 5, np.full(16, 3, np.uint32)])
+    delays[1, 6] = 32
+    amps = np.ones((2, 32))
+    beam = FeeBeam(file, freqs, delays, amps)
+    tmap, fmap = beam.maps()
+    got = beam.calc_jones(az, za, latitude_rad=LAT).cpu().numpy()
+    torch.cuda.synchronize()
+    ref = oracle_tables(file, az, za, freqs, delays, amps, tmap, fmap, True, LAT)
+    err = np.max(np.abs(got - ref)) / np.max(np.abs(ref))
+    assert err < 1e-8, err
