@@ -571,6 +571,20 @@ extern "C" int hdc_fee_beam_new(const HdcFeeCoeffs* file, const uint32_t* h_freq
         if (e == cudaSuccess) e = cudaDeviceSynchronize();
         cudaFree(d_ideal);
         if (e != cudaSuccess) return fail(e, "zenith normalisation");
+        // every element divides by its norm: a zero or non-finite one (a
+        // coefficient set without that element at the zenith) is refused
+        std::vector<double> h_norm((size_t)4 * nuf);
+        if ((e = cudaMemcpy(h_norm.data(), b->d_norm, sizeof(double) * h_norm.size(), cudaMemcpyDeviceToHost)) !=
+            cudaSuccess)
+            return fail(e, "cudaMemcpy");
+        for (size_t i = 0; i < h_norm.size(); i++)
+            if (!(h_norm[i] > 0.0) || !std::isfinite(h_norm[i])) {
+                set_error("hdc_fee_beam_new: the zenith-pointed beam's element %d at %u Hz is %g at the zenith; it "
+                          "cannot normalise", (int)(i % 4), file->freqs_hz[ufile[i / 4]], h_norm[i]);
+                fee_release(b);
+                delete b;
+                return HDC_ERR_ARG;
+            }
     }
     *out = b;
     return HDC_OK;

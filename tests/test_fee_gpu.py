@@ -301,3 +301,16 @@ def test_calc_jones_at_degree_30(oracle):
     ref = oracle_tables(file, az, za, freqs, delays, amps, tmap, fmap, True, LAT)
     err = np.max(np.abs(got - ref)) / np.max(np.abs(ref))
     assert err < 1e-8, err
+
+
+def test_zero_zenith_norm_is_refused():
+    """A coefficient set whose zenith-pointed beam has a zero element at the
+    zenith cannot be normalised to it: hdc_fee_beam_new refuses it (and the
+    same set without normalisation is accepted)."""
+    file = synth.fee_coeffs([167680000], 4, seed=2)
+    file["q"] = file["q"].copy()
+    file["q"][0, 0] = 0.0  # no X coefficients at all
+    delays = np.zeros((1, 16), np.uint32)
+    with pytest.raises(_lib.HdcError, match="cannot normalise"):
+        FeeBeam(file, [167.68e6], delays, np.ones((1, 32)), norm_to_zenith=True)
+    FeeBeam(file, [167.68e6], delays, np.ones((1, 32)), norm_to_zenith=False).close()
