@@ -293,13 +293,19 @@ __device__ __forceinline__ void tile_uvw(const Params& P, int tile, double oq, d
     }
 }
 
-// one row of a beam Jones (two complex numbers, FP32) for tile `tile`,
-// component c of the pass, at unique frequency column fm
-__device__ __forceinline__ float4 beam_row(const Params& P, int tile, int c, int fm, int row) {
-    if (tile >= P.ntiles) return make_float4(0.f, 0.f, 0.f, 0.f);
-    const double2* b = reinterpret_cast<const double2*>(
-                           P.beam + ((size_t)__ldg(P.tile_map + tile) * P.n_uniq_freq + fm) * P.nc + P.c0 + c) +
-                       2 * row;
+// the beam table row of a tile (its unique tile at unique frequency column
+// fm: unique tile x unique frequencies + fm), looked up once per thread; -1
+// past the array
+__device__ __forceinline__ int beam_base(const Params& P, int tile, int fm) {
+    if (tile >= P.ntiles) return -1;
+    return __ldg(P.tile_map + tile) * P.n_uniq_freq + fm;
+}
+
+// one row of a beam Jones (two complex numbers, FP32): component c of the
+// pass in beam table row `base`
+__device__ __forceinline__ float4 beam_row(const Params& P, int base, int c, int row) {
+    if (base < 0) return make_float4(0.f, 0.f, 0.f, 0.f);
+    const double2* b = reinterpret_cast<const double2*>(P.beam + (size_t)base * P.nc + P.c0 + c) + 2 * row;
     const double2 e0 = __ldg(b), e1 = __ldg(b + 1);
     return make_float4((float)e0.x, (float)e0.y, (float)e1.x, (float)e1.y);
 }
@@ -473,6 +479,9 @@ __global__ void __launch_bounds__(Cfg<MODE>::THREADS, 1) gram_i8_kernel(const __
         const bool ysep = ry != 0 && ry != 1;
         const int prow[2] = {NT * rb + r0, NT * rb + r0 + 64};
         const int qcol = NH * cb + r0;
+        // the three tiles' beam row blocks (MODE 1), looked up once
+        const int bbase[3] = {MODE == 1 ? beam_base(P, prow[0], fm) : -1, MODE == 1 ? beam_base(P, prow[1], fm) : -1,
+                              MODE == 1 ? beam_base(P, qcol, fm) : -1};
         // The upper 64 rows of the block pair with no column of it when they
         // lie beyond the array, or in an XX / YY block whose columns all lie
         // below them: their X planes stay zero and are not produced.  (Then
@@ -548,7 +557,7 @@ __global__ void __launch_bounds__(Cfg<MODE>::THREADS, 1) gram_i8_kernel(const __
                         phasor_quarter_f32(u[s2] * cl + v[s2] * cm + w[s2] * cn, sn, cs);
                         if (s2 == ry) snq = sn, csq = cs;
                         // (B S)^{a y} = B^{aX} S^{Xy} + B^{aY} S^{Yy}, then times A
-                        const float4 b = beam_row(P, prow[s2], c, fm, arow);  // (B^{aX}, B^{aY}) as re, im
+                        const float4 b = beam_row(P, bbase[s2], c, arow);  // (B^{aX}, B^{aY}) as re, im
 #pragma unroll
                         for (int y = 0; y < 2; y++) {
                             // S^{Xy}: s0 (y = 0: xx, y = 1: xy); S^{Yy}: s1 (yx, yy)
@@ -563,7 +572,7 @@ __global__ void __launch_bounds__(Cfg<MODE>::THREADS, 1) gram_i8_kernel(const __
                         }
                     }
                     if (ysep) phasor_quarter_f32(u[2] * cl + v[2] * cm + w[2] * cn, snq, csq);
-                    const float4 bq = beam_row(P, qcol, c, fm, brow);
+                    const float4 bq = beam_row(P, bbase[2], c, brow);
 #pragma unroll
                     for (int y = 0; y < 2; y++) {
                         const float br = y ? bq.z : bq.x, bi = y ? bq.w : bq.y;
