@@ -217,6 +217,17 @@ __global__ void beam_weight_kernel(const double2* radec, int nc, const double* f
     W[(size_t)f * nc + c] = store_j((b * s) * herm(b));
 }
 
+// FP32 copy of a per-tile beam table (n Jones matrices).
+__global__ void jones_to_f32_kernel(const JonesF64* __restrict__ in, size_t n, JonesF32* __restrict__ out) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double4* a = reinterpret_cast<const double4*>(in + i);
+    const double4 x = a[0], y = a[1];
+    float4* o = reinterpret_cast<float4*>(out + i);
+    o[0] = make_float4((float)x.x, (float)x.y, (float)x.z, (float)x.w);
+    o[1] = make_float4((float)y.x, (float)y.y, (float)y.z, (float)y.w);
+}
+
 // Per-tile beams B [uniq tile][uniq freq][nc] of one component type at this
 // timestep.
 __global__ void tile_beam_kernel(const double2* radec, int nc, const double* ufreqs, int nuf, const double* gains,
@@ -256,6 +267,7 @@ void TileBeams::release() {
 
 void TypeTables::release() {
     dfree(d_B);
+    dfree(d_B32);
     dfree(d_lmn);
     dfree(d_S);
     dfree(d_W);
@@ -412,8 +424,11 @@ int Modeller::build_tables(const HdcSkyModel* sky) {
 int Modeller::alloc_tile_beam_tables() {
     for (int ty = 0; ty < 3; ty++) {
         dfree(t[ty].d_B);
+        dfree(t[ty].d_B32);
         if (t[ty].nc == 0) continue;
         HDC_CUDA_RET_INT(dalloc(&t[ty].d_B, (size_t)tb.n_uniq_tile * tb.n_uniq_freq * t[ty].nc));
+        if (ty == 0 && form == HDC_PREDICT_TENSOR)
+            HDC_CUDA_RET_INT(dalloc(&t[ty].d_B32, (size_t)tb.n_uniq_tile * tb.n_uniq_freq * t[ty].nc));
     }
     return HDC_OK;
 }
@@ -510,6 +525,13 @@ int Modeller::geometry(double lst, cudaStream_t s) {
             dim3 g((t[ty].nc + 127) / 128, tb.n_uniq_freq, tb.n_uniq_tile);
             tile_beam_kernel<<<g, 128, 0, s>>>(t[ty].d_radec, t[ty].nc, tb.d_freqs, tb.n_uniq_freq, tb.d_gains, lst,
                                                 lat, t[ty].d_B);
+            count_launches(1);
+            HDC_CUDA_RET_INT(cudaGetLastError());
+        }
+        // the points' table in FP32 for the tensor form's producers
+        if (t[0].d_B32) {
+            const size_t n = (size_t)tb.n_uniq_tile * tb.n_uniq_freq * t[0].nc;
+            jones_to_f32_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(t[0].d_B, n, t[0].d_B32);
             count_launches(1);
             HDC_CUDA_RET_INT(cudaGetLastError());
         }
@@ -613,7 +635,8 @@ int Modeller::model_channels(double lst, void* d_vis, bool out64, int f0, int nf
             // channels uses its start (chunks of one call run in order on s)
             void* ws = tensor_workspace(out64);
             if (!ws) return HDC_ERR_ALLOC;
-            TensorBeam tbm = {t[0].d_B, tb.d_tile_map, tb.d_freq_map + f0, tb.n_uniq_tile, tb.n_uniq_freq};
+            TensorBeam tbm = {t[0].d_B, t[0].d_B32, tb.d_tile_map, tb.d_freq_map + f0, tb.n_uniq_tile,
+                              tb.n_uniq_freq};
             const int rc = launch_tensor_points(nfc, nbl, ntiles, t[0].nc, d_freqs + f0, d_xyzs, lst - pc.ra, pc.dec,
                                                 t[0].d_lmn, weights(0) + (size_t)f0 * t[0].nc,
                                                 tile_beams() ? &tbm : nullptr, vis, out64, ws, d_err, s, tensor_sync());

@@ -20,6 +20,7 @@ struct TypeTables {
     double2* d_suv_tile = nullptr;  // [nc][ntiles]
     float* d_sdense = nullptr;      // [nc][SDN][SDN] signed dense coefficients, or NULL
     JonesF64* d_B = nullptr;        // per-tile beams: [uniq tile][uniq freq][nc] at the current timestep
+    JonesF32* d_B32 = nullptr;      // the same in FP32 (points in the tensor form: its producers' reads)
     void release();
 };
 

@@ -67,6 +67,7 @@ cudaError_t launch_direct(int ty, bool tile_beam, bool out64, const DirectParams
 // channel of the launch.
 struct TensorBeam {
     const JonesF64* beam;
+    const JonesF32* beam32;  // the same table in FP32 (the producers' reads), or NULL
     const int* tile_map;
     const int* freq_map;
     int n_uniq_tile;

@@ -161,6 +161,7 @@ struct Params {
     // MODE 1: beam [uniq tile][uniq freq][nc], unique row of each tile and
     // column of each channel, and per channel bounds of |B| and |S| entries
     const JonesF64* beam;
+    const JonesF32* beam32;  // MODE 1: the beam table in FP32, or NULL (then read from beam)
     const int* tile_map;
     const int* freq_map;
     int n_uniq_freq;
@@ -305,6 +306,7 @@ __device__ __forceinline__ int beam_base(const Params& P, int tile, int fm) {
 // pass in beam table row `base`
 __device__ __forceinline__ float4 beam_row(const Params& P, int base, int c, int row) {
     if (base < 0) return make_float4(0.f, 0.f, 0.f, 0.f);
+    if (P.beam32) return __ldg(reinterpret_cast<const float4*>(P.beam32 + (size_t)base * P.nc + P.c0 + c) + row);
     const double2* b = reinterpret_cast<const double2*>(P.beam + (size_t)base * P.nc + P.c0 + c) + 2 * row;
     const double2 e0 = __ldg(b), e1 = __ldg(b + 1);
     return make_float4((float)e0.x, (float)e0.y, (float)e1.x, (float)e1.y);
@@ -1201,6 +1203,7 @@ int launch_tensor_points(int nf, int nbl, int ntiles, int nc, const double* d_fr
     P.lmn = d_lmn;
     P.W = d_W;
     P.beam = tile_beam ? beam->beam : nullptr;
+    P.beam32 = tile_beam ? beam->beam32 : nullptr;
     P.tile_map = tile_beam ? beam->tile_map : nullptr;
     P.freq_map = tile_beam ? beam->freq_map : nullptr;
     P.n_uniq_freq = tile_beam ? beam->n_uniq_freq : 0;
