@@ -657,11 +657,10 @@ __global__ void __launch_bounds__(DT, FastShape<TYPE>::MIN_CTAS) fast_kernel(con
 // visibility term is then z G_p H_q^H = B_p (z S) B_q^H: the phasor and
 // envelope z in FP32 exactly as fast_kernel computes them, z G_p in FP32,
 // and its product with H_q^H accumulated in FP64 (32 fused multiply-adds).
-// All-FP32 products (measured) put the cross-polarisation terms'
-// cancellation at FP32 precision of the parallel hands and the p99.9 error
-// at 1.0-1.15e-6; accumulating in FP64 keeps each element's rounding
-// relative to its own size, as the shared-beam form's W = B S B^H rounded
-// once does (p99.9 3.4e-7 and 5.3e-7 on the tests' skies).
+// Measured on the tests' skies (p99.9 of the error, Gaussians / shapelets):
+// this form 3.4e-7 / 5.3e-7; FP32 two-product sums added into FP64
+// accumulators 4.2e-7 / 5.9e-7 (7 % faster Gaussians); everything in FP32,
+// chunk sums included, 1.0-1.15e-6, over the 1e-6 bar.
 constexpr int FT_FCH = 2;      // channels per thread
 constexpr int FT_CH = 16;      // components per staged chunk
 constexpr int FT_MAX_NU = 32;  // unique tiles (more: the FP64 per-tile kernel)
