@@ -148,22 +148,33 @@ __device__ __forceinline__ void shapelet_dense_multi(const DirectParams& p, cons
                                                      const double (&x_pos)[N], const double (&y_pos)[N],
                                                      float (&er)[N], float (&ei)[N]) {
     float X[N][SDN], Y[N][SDN];
+    int xi[N], yi[N];
+    float xfrac[N], yfrac[N];
 #pragma unroll
     for (int i = 0; i < N; i++) {
         const double fx = floor(x_pos[i]), fy = floor(y_pos[i]);
-        const int xi = fx > 0.0 ? (int)fmin(fx, (double)(SBF_L - 2)) : 0;
-        const int yi = fy > 0.0 ? (int)fmin(fy, (double)(SBF_L - 2)) : 0;
-        const float xfrac = (float)(x_pos[i] - fx), yfrac = (float)(y_pos[i] - fy);
-#pragma unroll
-        for (int h = 0; h < SDN / 2; h++) {
-            const float4 a = __ldg(p.sbfp + (size_t)xi * (SDN / 2) + h);
-            const float4 b = __ldg(p.sbfp + (size_t)yi * (SDN / 2) + h);
-            X[i][2 * h] = fmaf(a.y, xfrac, a.x);
-            X[i][2 * h + 1] = fmaf(a.w, xfrac, a.z);
-            Y[i][2 * h] = fmaf(b.y, yfrac, b.x);
-            Y[i][2 * h + 1] = fmaf(b.w, yfrac, b.z);
-        }
+        xi[i] = fx > 0.0 ? (int)fmin(fx, (double)(SBF_L - 2)) : 0;
+        yi[i] = fy > 0.0 ? (int)fmin(fy, (double)(SBF_L - 2)) : 0;
+        xfrac[i] = (float)(x_pos[i] - fx);
+        yfrac[i] = (float)(y_pos[i] - fy);
         er[i] = 0.f, ei[i] = 0.f;
+    }
+    // A thread's channels usually share a table interval (their positions
+    // differ by the channels' relative frequency spacing): a channel whose
+    // interval equals the previous channel's takes its records instead of
+    // gathering them again, so only lanes with a new interval load.
+#pragma unroll
+    for (int h = 0; h < SDN / 2; h++) {
+        float4 a, b;
+#pragma unroll
+        for (int i = 0; i < N; i++) {
+            if (i == 0 || xi[i] != xi[i - 1]) a = __ldg(p.sbfp + (size_t)xi[i] * (SDN / 2) + h);
+            if (i == 0 || yi[i] != yi[i - 1]) b = __ldg(p.sbfp + (size_t)yi[i] * (SDN / 2) + h);
+            X[i][2 * h] = fmaf(a.y, xfrac[i], a.x);
+            X[i][2 * h + 1] = fmaf(a.w, xfrac[i], a.z);
+            Y[i][2 * h] = fmaf(b.y, yfrac[i], b.x);
+            Y[i][2 * h + 1] = fmaf(b.w, yfrac[i], b.z);
+        }
     }
     const float2* row = reinterpret_cast<const float2*>(cm);
 #pragma unroll
