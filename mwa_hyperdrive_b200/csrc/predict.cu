@@ -661,7 +661,7 @@ __global__ void __launch_bounds__(DT, FastShape<TYPE>::MIN_CTAS) fast_kernel(con
 }
 
 // The chosen form's Gaussians and shapelets with a beam per tile: each
-// thread takes one baseline (p, q) and FT_FCH consecutive channels, as
+// thread takes one baseline (p, q) and FastTileShape::FCH consecutive channels, as
 // fast_kernel does.  Per staged chunk of components the CTA forms in shared
 // memory G = B_u S (FP32) and H = B_u (FP64) for every unique tile u and each
 // of its channels (B the tile's beam Jones at the channel's beam frequency,
@@ -675,16 +675,33 @@ __global__ void __launch_bounds__(DT, FastShape<TYPE>::MIN_CTAS) fast_kernel(con
 // this form 3.4e-7 / 5.3e-7; FP32 two-product sums added into FP64
 // accumulators 4.2e-7 / 5.9e-7 (7 % faster Gaussians); everything in FP32,
 // chunk sums included, 1.0-1.15e-6, over the 1e-6 bar.
-constexpr int FT_FCH = 2;      // channels per thread
-constexpr int FT_CH = 16;      // components per staged chunk
+// Channels per thread and components per staged chunk by type, chosen by
+// timing on 17 unique tiles (one timestep, 128 tiles, 384 channels):
+// Gaussians (1) 2 x 16 (4 x 8: 9.4 -> 10.8 ms, 156 registers); shapelets (2)
+// 4 x 8, whose channels then share more gathered basis records (2 x 16: 5.4
+// ms, 4 x 8: 4.6 ms, bit-identical).  Both stage 32 (channel, component)
+// records per unique tile, so the shared memory does not depend on the type.
+template <int TYPE>
+struct FastTileShape {
+    static constexpr int FCH = 2;
+    static constexpr int CH = 16;
+};
+template <>
+struct FastTileShape<2> {
+    static constexpr int FCH = 4;
+    static constexpr int CH = 8;
+};
+constexpr int FT_RECS = 32;    // FCH x CH of every type
 constexpr int FT_MAX_NU = 32;  // unique tiles (more: the FP64 per-tile kernel)
+static_assert(FastTileShape<1>::FCH * FastTileShape<1>::CH == FT_RECS, "per-tile records");
+static_assert(FastTileShape<2>::FCH * FastTileShape<2>::CH == FT_RECS, "per-tile records");
 
-inline size_t fast_tile_smem_bytes(int nu) { return (size_t)FT_FCH * FT_CH * nu * 6 * sizeof(float4); }
+inline size_t fast_tile_smem_bytes(int nu) { return (size_t)FT_RECS * nu * 6 * sizeof(float4); }
 
 template <int TYPE, bool OUT64>
 __global__ void __launch_bounds__(DT, 1) fast_tile_kernel(const DirectParams p) {
-    constexpr int FCH = FT_FCH;
-    constexpr int CH = FT_CH;
+    constexpr int FCH = FastTileShape<TYPE>::FCH;
+    constexpr int CH = FastTileShape<TYPE>::CH;
     __shared__ alignas(128) double4 s_lmn[2][CH];
     __shared__ alignas(128) JonesF64 s_flux[2][FCH][CH];
     __shared__ alignas(128) double4 s_gp[2][CH];
@@ -837,7 +854,7 @@ static cudaError_t launch_fast_tile(const DirectParams& p, cudaStream_t s) {
         if (e != cudaSuccess) return e;
         attr[dev].store(true, std::memory_order_relaxed);
     }
-    const dim3 grid((p.nbl + DT - 1) / DT, (p.nf + FT_FCH - 1) / FT_FCH);
+    const dim3 grid((p.nbl + DT - 1) / DT, (p.nf + FastTileShape<TYPE>::FCH - 1) / FastTileShape<TYPE>::FCH);
     fast_tile_kernel<TYPE, OUT64><<<grid, DT, smem, s>>>(p);
     return cudaSuccess;
 }
